@@ -1,0 +1,465 @@
+"""Input-deck tooling: seeded synthetic meshes and reference-format deck files.
+
+A GiftBTE run reads three keyword files from ``./input`` (CONTROL, GEOMETRY,
+PHONON), a boundary-condition table, a mesh file and a material band table.
+This module builds the meshes used by the parity tests and the benchmark and
+writes them in exactly those formats, so the same deck can be handed to the
+reference binary and to this library.
+
+File formats follow the readers of the reference:
+  * CONTROL / GEOMETRY / PHONON: keyword line, value on the next line
+    (``src/BTEMain.cpp:87-315``).
+  * BC table: count line, two header lines, then ``index type value``
+    (``src/BTEBoundaryCondition/BTEBoundaryCondition.cpp:8-31``).
+  * COMSOL ``.mphtxt`` 2D mesh (``src/BTEMesh/ReadinMesh.cpp:228-400``):
+    vertex block, then ``vtx``/``edg``/``tri``/``quad`` element types each
+    followed by their geometric-entity indices (0-based in the file; the
+    reader adds 1 to edge tags and subtracts 1 from domain indices).
+  * gmsh MSH 4.1 2D mesh (``src/BTEMesh/ReadinMesh.cpp:407-534``).
+  * DATABASE band table: one line per band, ``|v| tau C lattice_ratio
+    heat_ratio`` (``src/BTEBand/BTEBand.cpp:64-79``).
+"""
+from __future__ import annotations
+
+import dataclasses
+import os
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+
+# ----------------------------------------------------------------------------
+# meshes
+# ----------------------------------------------------------------------------
+@dataclasses.dataclass
+class Mesh2D:
+    """A 2D mesh in unit coordinates (multiplied by ScaleX/ScaleY on read).
+
+    nodes:      (Nn, 2) float64
+    cells:      list of vertex tuples (3 = triangle, 4 = quad in COMSOL
+                "Z" order v0 v1 v2 v3 with faces v0-v1, v1-v3, v3-v2, v2-v0)
+    edges:      (Ne, 2) int boundary edges
+    edge_tags:  (Ne,) int boundary tags (1-based, as the BC file names them)
+    cell_region:(Nc,) int region index (0-based, GeometryMaterialType row - 1)
+    """
+
+    nodes: np.ndarray
+    cells: np.ndarray
+    edges: np.ndarray
+    edge_tags: np.ndarray
+    cell_region: np.ndarray
+
+    @property
+    def n_cells(self) -> int:
+        return int(self.cells.shape[0])
+
+
+def square_tri_mesh(nx: int, ny: int) -> Mesh2D:
+    """Structured nx x ny grid on [0,1]^2, each square split into 2 triangles
+    along its (0,0)-(1,1) diagonal. Boundary tags: 1 left, 2 right,
+    3 bottom, 4 top."""
+    xs = np.linspace(0.0, 1.0, nx + 1)
+    ys = np.linspace(0.0, 1.0, ny + 1)
+    X, Y = np.meshgrid(xs, ys, indexing="ij")
+    nodes = np.stack([X.ravel(), Y.ravel()], axis=1)
+
+    def nid(i, j):
+        return i * (ny + 1) + j
+
+    tris = []
+    for i in range(nx):
+        for j in range(ny):
+            n00, n10, n01, n11 = nid(i, j), nid(i + 1, j), nid(i, j + 1), nid(i + 1, j + 1)
+            tris.append((n00, n10, n11))
+            tris.append((n00, n11, n01))
+    edges, tags = [], []
+    for j in range(ny):
+        edges.append((nid(0, j), nid(0, j + 1))); tags.append(1)
+        edges.append((nid(nx, j), nid(nx, j + 1))); tags.append(2)
+    for i in range(nx):
+        edges.append((nid(i, 0), nid(i + 1, 0))); tags.append(3)
+        edges.append((nid(i, ny), nid(i + 1, ny))); tags.append(4)
+    return Mesh2D(nodes=nodes, cells=np.asarray(tris, dtype=np.int64),
+                  edges=np.asarray(edges, dtype=np.int64),
+                  edge_tags=np.asarray(tags, dtype=np.int64),
+                  cell_region=np.zeros(len(tris), dtype=np.int64))
+
+
+def square_quad_mesh(nx: int, ny: int) -> Mesh2D:
+    """Structured quad grid on [0,1]^2 (COMSOL vertex order), tags as in
+    :func:`square_tri_mesh`."""
+    xs = np.linspace(0.0, 1.0, nx + 1)
+    ys = np.linspace(0.0, 1.0, ny + 1)
+    X, Y = np.meshgrid(xs, ys, indexing="ij")
+    nodes = np.stack([X.ravel(), Y.ravel()], axis=1)
+
+    def nid(i, j):
+        return i * (ny + 1) + j
+
+    quads = []
+    for i in range(nx):
+        for j in range(ny):
+            quads.append((nid(i, j), nid(i + 1, j), nid(i, j + 1), nid(i + 1, j + 1)))
+    m = square_tri_mesh(nx, ny)
+    return Mesh2D(nodes=nodes, cells=np.asarray(quads, dtype=np.int64), edges=m.edges,
+                  edge_tags=m.edge_tags, cell_region=np.zeros(len(quads), dtype=np.int64))
+
+
+def jitter_interior(mesh: Mesh2D, amount: float, seed: int) -> Mesh2D:
+    """Move interior nodes by a uniform random offset in [-amount, amount]^2
+    (unit coordinates); boundary nodes stay on the boundary."""
+    rng = np.random.default_rng(seed)
+    nodes = mesh.nodes.copy()
+    bnd = np.zeros(len(nodes), dtype=bool)
+    bnd[mesh.edges.ravel()] = True
+    d = rng.uniform(-amount, amount, size=nodes.shape)
+    nodes[~bnd] += d[~bnd]
+    return dataclasses.replace(mesh, nodes=nodes)
+
+
+def _poisson_disk(rng, h, inside, bbox, k=20):
+    """Bridson-style Poisson-disk sample with spacing h inside bbox."""
+    (x0, y0), (x1, y1) = bbox
+    cell = h / np.sqrt(2.0)
+    gw, gh = int(np.ceil((x1 - x0) / cell)) + 1, int(np.ceil((y1 - y0) / cell)) + 1
+    grid = -np.ones((gw, gh), dtype=np.int64)
+    pts: List[Tuple[float, float]] = []
+    active: List[int] = []
+
+    def fits(p):
+        gi, gj = int((p[0] - x0) / cell), int((p[1] - y0) / cell)
+        for a in range(max(gi - 2, 0), min(gi + 3, gw)):
+            for b in range(max(gj - 2, 0), min(gj + 3, gh)):
+                q = grid[a, b]
+                if q >= 0 and (pts[q][0] - p[0]) ** 2 + (pts[q][1] - p[1]) ** 2 < h * h:
+                    return False
+        return True
+
+    def add(p):
+        pts.append(p)
+        grid[int((p[0] - x0) / cell), int((p[1] - y0) / cell)] = len(pts) - 1
+        active.append(len(pts) - 1)
+
+    while True:
+        p = (rng.uniform(x0, x1), rng.uniform(y0, y1))
+        if inside(p):
+            add(p)
+            break
+    while active:
+        idx = active[rng.integers(len(active))]
+        base = pts[idx]
+        placed = False
+        for _ in range(k):
+            r = rng.uniform(h, 2 * h)
+            t = rng.uniform(0, 2 * np.pi)
+            p = (base[0] + r * np.cos(t), base[1] + r * np.sin(t))
+            if x0 <= p[0] < x1 and y0 <= p[1] < y1 and inside(p) and fits(p):
+                add(p)
+                placed = True
+                break
+        if not placed:
+            active.remove(idx)
+    return np.asarray(pts, dtype=np.float64)
+
+
+def porous_cell_mesh(h: float, pores: Sequence[Tuple[float, float, float]], seed: int,
+                     side: float = 1.0) -> Mesh2D:
+    """Periodic square cell [0,side]^2 with circular pores (cx, cy, r), all
+    in unit coordinates, meshed as a Delaunay triangulation of Poisson-disk
+    interior points plus evenly spaced boundary points.
+
+    The x- and y-faces carry identical node positions (translation-matched),
+    which the reference's nearest-face-centre periodic pairing needs
+    (``src/BTEMesh/BTEMesh.cpp:905-924``). Tags: 1 left, 2 right, 3 bottom,
+    4 top, 5 + k for the wall of pore k.
+    """
+    from scipy.spatial import Delaunay
+
+    rng = np.random.default_rng(seed)
+    n_side = max(int(round(side / h)), 2)
+    s = np.linspace(0.0, side, n_side + 1)
+    bpts = []
+    for v in s[:-1]:
+        bpts += [(v, 0.0), (side, v), (side - v, side), (0.0, side - v)]
+    pore_pts = []
+    for (cx, cy, r) in pores:
+        m = max(int(round(2 * np.pi * r / h)), 8)
+        t = np.arange(m) * 2 * np.pi / m
+        pore_pts.append(np.stack([cx + r * np.cos(t), cy + r * np.sin(t)], axis=1))
+
+    margin = 0.6 * h
+
+    def inside(p):
+        if p[0] < margin or p[0] > side - margin or p[1] < margin or p[1] > side - margin:
+            return False
+        for (cx, cy, r) in pores:
+            if (p[0] - cx) ** 2 + (p[1] - cy) ** 2 < (r + margin) ** 2:
+                return False
+        return True
+
+    ipts = _poisson_disk(rng, h, inside, ((0.0, 0.0), (side, side)))
+    pts = np.concatenate([np.asarray(bpts)] + pore_pts + [ipts], axis=0)
+    tri = Delaunay(pts)
+    simp = tri.simplices
+    cent = pts[simp].mean(axis=1)
+    keep = np.ones(len(simp), dtype=bool)
+    for (cx, cy, r) in pores:
+        keep &= (cent[:, 0] - cx) ** 2 + (cent[:, 1] - cy) ** 2 > r * r
+    simp = simp[keep]
+    # drop unused nodes (none expected) and renumber
+    used = np.unique(simp)
+    remap = -np.ones(len(pts), dtype=np.int64)
+    remap[used] = np.arange(len(used))
+    pts = pts[used]
+    simp = remap[simp]
+    # boundary edges = edges used by exactly one triangle
+    e = np.concatenate([simp[:, [1, 2]], simp[:, [2, 0]], simp[:, [0, 1]]], axis=0)
+    es = np.sort(e, axis=1)
+    uniq, cnt = np.unique(es, axis=0, return_counts=True)
+    bedges = uniq[cnt == 1]
+    tags = np.zeros(len(bedges), dtype=np.int64)
+    mid = pts[bedges].mean(axis=1)
+    tol = 1e-9 * side
+    tags[np.abs(mid[:, 0]) < tol] = 1
+    tags[np.abs(mid[:, 0] - side) < tol] = 2
+    tags[np.abs(mid[:, 1]) < tol] = 3
+    tags[np.abs(mid[:, 1] - side) < tol] = 4
+    for k, (cx, cy, r) in enumerate(pores):
+        d = np.hypot(mid[:, 0] - cx, mid[:, 1] - cy)
+        tags[(tags == 0) & (d < r + 0.5 * h)] = 5 + k
+    if np.any(tags == 0):
+        raise RuntimeError("porous_cell_mesh: unclassified boundary edge")
+    return Mesh2D(nodes=pts, cells=simp.astype(np.int64), edges=bedges.astype(np.int64),
+                  edge_tags=tags, cell_region=np.zeros(len(simp), dtype=np.int64))
+
+
+# ----------------------------------------------------------------------------
+# bands
+# ----------------------------------------------------------------------------
+@dataclasses.dataclass
+class BandTable:
+    """Per-band properties of one material (DATABASE columns)."""
+
+    v: np.ndarray          # |group velocity| m/s
+    tau: np.ndarray        # relaxation time s
+    C: np.ndarray          # heat capacity J/m^3K
+    lattice_ratio: np.ndarray
+    heat_ratio: np.ndarray
+
+    @property
+    def n_bands(self) -> int:
+        return int(len(self.v))
+
+
+def gray_band(v: float, mfp: float, C: float) -> BandTable:
+    one = np.ones(1)
+    return BandTable(v=one * v, tau=one * (mfp / v), C=one * C, lattice_ratio=one.copy(),
+                     heat_ratio=one.copy())
+
+
+HBAR = 1.054571817e-34
+KB = 1.380649e-23
+
+
+def sine_dispersion_bands(n_bands: int, T: float = 300.0, kmax: float = 1.1e10,
+                          wmax_la: float = 7.0e13, wmax_ta: float = 2.8e13,
+                          n_k: int = 4000) -> BandTable:
+    """Isotropic sine dispersion (1 LA + 2 TA branches, w = wmax sin(pi k /
+    2 kmax)), binned into n_bands equal-frequency bands.
+
+    Per mode: v = dw/dk, C = Bose-Einstein mode heat capacity at T with a
+    spherical-shell density of states k^2 dk / (2 pi^2), and
+    tau^-1 = 1.3e-45 w^4 + 1.7e-19 w^2 T exp(-137/T).
+    Band aggregation: C_b = sum C, v_b = sum C v / C_b,
+    tau_b = sum C v^2 tau / (C_b v_b^2), lattice_ratio = heat_ratio = C_b / C.
+    """
+    k = (np.arange(n_k) + 0.5) * kmax / n_k
+    dk = kmax / n_k
+    wmax_all = max(wmax_la, wmax_ta)
+    edges = np.linspace(0.0, wmax_all, n_bands + 1)
+    Cb = np.zeros(n_bands); Cv = np.zeros(n_bands); Cv2t = np.zeros(n_bands)
+    for wmax, mult in ((wmax_la, 1), (wmax_ta, 2)):
+        w = wmax * np.sin(0.5 * np.pi * k / kmax)
+        v = wmax * 0.5 * np.pi / kmax * np.cos(0.5 * np.pi * k / kmax)
+        x = HBAR * w / (KB * T)
+        cm = KB * x * x * np.exp(x) / np.expm1(x) ** 2 * k * k * dk / (2 * np.pi ** 2) * mult
+        tau = 1.0 / (1.3e-45 * w ** 4 + 1.7e-19 * w ** 2 * T * np.exp(-137.0 / T))
+        idx = np.clip(np.searchsorted(edges, w, side="right") - 1, 0, n_bands - 1)
+        np.add.at(Cb, idx, cm)
+        np.add.at(Cv, idx, cm * v)
+        np.add.at(Cv2t, idx, cm * v * v * tau)
+    vb = Cv / Cb
+    taub = Cv2t / (Cb * vb * vb)
+    ratio = Cb / Cb.sum()
+    # renormalise so the ratios sum to one at 17 significant digits
+    ratio = ratio / ratio.sum()
+    return BandTable(v=vb, tau=taub, C=Cb, lattice_ratio=ratio, heat_ratio=ratio.copy())
+
+
+# ----------------------------------------------------------------------------
+# writers
+# ----------------------------------------------------------------------------
+def write_mphtxt(path: str, mesh: Mesh2D) -> None:
+    """COMSOL text mesh, 2D, in the layout the reference parser expects."""
+    nn = len(mesh.nodes)
+    out = ["# Created by COMSOL Multiphysics.", "", "# Major & minor version", "0 1 ",
+           "1 # number of tags", "# Tags", "5 mesh1 ", "1 # number of types", "# Types",
+           "3 obj ", "", "# --------- Object 0 ----------", "", "0 0 1 ", "4 Mesh # class",
+           "4 # version", "2 # sdim", f"{nn} # number of mesh vertices",
+           "0 # lowest mesh vertex index", "", "# Mesh vertex coordinates"]
+    out += [f"{x:.17g} {y:.17g} " for x, y in mesh.nodes]
+    by_nv: Dict[int, List[int]] = {}
+    for i, c in enumerate(mesh.cells):
+        by_nv.setdefault(len(c), []).append(i)
+    types = [("edg", 2, mesh.edges, mesh.edge_tags - 1)]
+    for nv, name in ((3, "tri"), (4, "quad")):
+        if nv in by_nv:
+            ids = by_nv[nv]
+            types.append((name, nv, np.asarray(mesh.cells)[ids], np.asarray(mesh.cell_region)[ids] + 1))
+    out += ["", f"{len(types)} # number of element types"]
+    for t, (name, nv, elems, ent) in enumerate(types):
+        out += ["", f"# Type #{t}", "", f"3 {name} # type name", "", "",
+                f"{nv} # number of vertices per element", f"{len(elems)} # number of elements",
+                "# Elements"]
+        out += [" ".join(str(int(v)) for v in e) + " " for e in elems]
+        out += ["", f"{len(elems)} # number of geometric entity indices",
+                "# Geometric entity indices"]
+        out += [f"{int(v)} " for v in ent]
+    with open(path, "w") as f:
+        f.write("\n".join(out) + "\n")
+
+
+def write_msh41(path: str, mesh: Mesh2D) -> None:
+    """gmsh MSH 4.1 ASCII, 2D: one node block, line elements tagged by their
+    boundary tag (entity tag), triangle/quad elements in entity (region+1)."""
+    nn = len(mesh.nodes)
+    lines = ["$MeshFormat", "4.1 0 8", "$EndMeshFormat", "$Nodes",
+             f"1 {nn} 1 {nn}", f"2 1 0 {nn}"]
+    lines += [str(i + 1) for i in range(nn)]
+    lines += [f"{x:.17g} {y:.17g} 0" for x, y in mesh.nodes]
+    lines += ["$EndNodes", "$Elements"]
+    blocks = []
+    tags = np.unique(mesh.edge_tags)
+    for t in tags:
+        sel = mesh.edges[mesh.edge_tags == t]
+        blocks.append((1, int(t), 1, sel))
+    for reg in np.unique(mesh.cell_region):
+        cs = np.asarray(mesh.cells)[np.asarray(mesh.cell_region) == reg]
+        tri = [c for c in cs if len(c) == 3]
+        quad = [c for c in cs if len(c) == 4]
+        if tri:
+            blocks.append((2, int(reg) + 1, 2, np.asarray(tri)))
+        if quad:
+            # gmsh quads are counter-clockwise; the reader maps a0 a1 a3 a2
+            q = np.asarray(quad)[:, [0, 1, 3, 2]]
+            blocks.append((2, int(reg) + 1, 3, q))
+    total = sum(len(b[3]) for b in blocks)
+    lines.append(f"{len(blocks)} {total} 1 {total}")
+    eid = 1
+    for dim, tag, typ, els in blocks:
+        lines.append(f"{dim} {tag} {typ} {len(els)}")
+        for e in els:
+            lines.append(f"{eid} " + " ".join(str(int(v) + 1) for v in e))
+            eid += 1
+    lines.append("$EndElements")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def write_band_database(path: str, bands: BandTable) -> None:
+    with open(path, "w") as f:
+        for i in range(bands.n_bands):
+            f.write(f"{bands.v[i]:.17g} {bands.tau[i]:.17g} {bands.C[i]:.17g} "
+                    f"{bands.lattice_ratio[i]:.17g} {bands.heat_ratio[i]:.17g}\n")
+
+
+@dataclasses.dataclass
+class BC:
+    tag: int
+    type: int      # 1 isothermal, 2 diffuse, 3 specular, <0 periodic (partner = -type)
+    value: float   # wall temperature / periodic temperature jump
+
+
+@dataclasses.dataclass
+class Deck:
+    """A complete steady synthetic-BTE input deck."""
+
+    mesh: Mesh2D
+    bands: BandTable
+    bcs: List[BC]
+    scale: Tuple[float, float] = (1e-6, 1e-6)
+    material_dim: int = 2
+    angle_method: int = 1
+    n_theta: int = 4
+    n_phi: int = 8
+    tref: float = 300.0
+    residual_temp: float = 1e-8
+    residual_flux: float = 1e-8
+    max_iter: int = 10000
+    order: str = "2"
+    heat_source: Optional[float] = None   # uniform volumetric heat (W/m^3)
+    mesh_format: str = "COMSOL"           # COMSOL or MSH
+
+    def write(self, root: str) -> str:
+        """Write ``root/input/*``; returns the input directory."""
+        d = os.path.join(root, "input")
+        os.makedirs(d, exist_ok=True)
+        mesh_name = "mesh.mphtxt" if self.mesh_format == "COMSOL" else "mesh.msh"
+        if self.mesh_format == "COMSOL":
+            write_mphtxt(os.path.join(d, mesh_name), self.mesh)
+        else:
+            write_msh41(os.path.join(d, mesh_name), self.mesh)
+        write_band_database(os.path.join(d, "bands.dat"), self.bands)
+        with open(os.path.join(d, "bc.dat"), "w") as f:
+            f.write(f"{len(self.bcs)} #Number of boundaries\n\n")
+            f.write("BoundaryIndex BoundaryType BoundaryValue\n")
+            for b in self.bcs:
+                f.write(f"{b.tag} {b.type} {b.value:.17g}\n")
+        with open(os.path.join(d, "CONTROL"), "w") as f:
+            f.write("State=\nSteady\nOrder=\n%s\nIterativeScheme=\nSynthetic\nMatrixSolver=\nLU\n"
+                    "Tref=\n%.17g\nMaxNumIter=\n%d\nResidualTemp=\n%.17g\nResidualFlux=\n%.17g\n"
+                    % (self.order, self.tref, self.max_iter, self.residual_temp, self.residual_flux))
+        with open(os.path.join(d, "GEOMETRY"), "w") as f:
+            f.write("GeometryDimension=\n2\nScaleX=\n%.17g\nScaleY=\n%.17g\nBCFile=\ninput/bc.dat\n"
+                    "MeshType=\n%s\nMeshFile=\ninput/%s\n"
+                    % (self.scale[0], self.scale[1], self.mesh_format, mesh_name))
+            if self.heat_source is not None:
+                f.write("UniformHeat=\n%.17g\n" % self.heat_source)
+        with open(os.path.join(d, "PHONON"), "w") as f:
+            f.write("MaterialNumber=\n1\nBandNumber=\n%d\n\nMaterialFile 1= DATABASE\ninput/bands.dat\n\n"
+                    "GeometryMaterialType=\n1 1\n\nMaterialDimension=\n%d\nAngle_method=\n%d\n"
+                    "Ntheta=\n%d\nNphi=\n%d\n"
+                    % (self.bands.n_bands, self.material_dim, self.angle_method,
+                       self.n_theta, self.n_phi))
+        return d
+
+
+# ----------------------------------------------------------------------------
+# the named workloads
+# ----------------------------------------------------------------------------
+def config1_deck(n: int = 40, **kw) -> Deck:
+    """Gray 2D square, 1 um x 1 um, n x n squares split into 2 triangles,
+    |v| = 6400 m/s, MFP 100 nm, C = 1.66e6 J/m^3K, 32 CADOM directions,
+    left 301 K / right 299 K isothermal, top/bottom diffuse."""
+    mesh = square_tri_mesh(n, n)
+    bands = gray_band(6400.0, 1e-7, 1.66e6)
+    bcs = [BC(1, 1, 301.0), BC(2, 1, 299.0), BC(3, 2, 0.0), BC(4, 2, 0.0)]
+    kw.setdefault("n_phi", 8)
+    kw.setdefault("angle_method", 1)
+    return Deck(mesh=mesh, bands=bands, bcs=bcs, scale=(1e-6, 1e-6), **kw)
+
+
+def config2_deck(h_nm: float = 3.0, n_bands: int = 40, n_phi: int = 16, seed: int = 0,
+                 **kw) -> Deck:
+    """Non-gray 2D nanoporous periodic cell: 300 nm square with a centred
+    r = 100 nm pore (diffuse wall), Poisson-disk Delaunay mesh with spacing
+    h, sine-dispersion bands binned to n_bands, 4*n_phi directions,
+    x-periodic with a 1 K jump, y-periodic."""
+    L = 300e-9
+    mesh = porous_cell_mesh(h_nm * 1e-9 / L, [(0.5, 0.5, 100e-9 / L)], seed)
+    bands = sine_dispersion_bands(n_bands)
+    bcs = [BC(1, -2, 1.0), BC(2, -1, 0.0), BC(3, -4, 0.0), BC(4, -3, 0.0), BC(5, 2, 0.0)]
+    kw.setdefault("n_phi", n_phi)
+    kw.setdefault("angle_method", 1)
+    kw.setdefault("tref", 0.0)
+    return Deck(mesh=mesh, bands=bands, bcs=bcs, scale=(L, L), **kw)
