@@ -1,0 +1,285 @@
+"""giftbte_b200 — B200-native steady synthetic phonon-BTE solver.
+
+Python binding of the C ABI in ``include/giftbte.h`` (the library itself is
+C++/CUDA: ``giftbte_b200/_build/libgiftbte_b200.so``). The class
+:class:`StaticBTESynthetic` mirrors the reference's solver object
+(``includes/StaticBTESynthetic/StaticBTESynthetic.h:24-261``): it is built
+from a mesh, boundary conditions, band table and angular quadrature, takes an
+initial temperature, and ``solve(max_iter, err_T, err_q)`` runs the outer
+source iteration; afterwards ``temperature`` (the macro lattice temperature),
+``total_energy`` (Temperature.dat), ``heat_flux`` and ``temperature_band``
+hold the results.
+
+There is no CPU fallback: without the compiled library or a CUDA device the
+constructor raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libgiftbte_b200.so")
+
+GBTE_OK = 0
+GBTE_ERR_NOT_CONVERGED = 1
+GBTE_FP64 = 0
+GBTE_FP32_MIXED = 1
+
+STATUS = {0: "ok", -1: "invalid argument", -2: "input/output error", -3: "CUDA error", -4: "diverged",
+          -5: "device wait timed out", -6: "out of memory", -7: "mesh topology error", -8: "unsupported input",
+          1: "not converged within max_iter"}
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+_c_dbl_p = ctypes.POINTER(ctypes.c_double)
+
+
+class MeshView(ctypes.Structure):
+    _fields_ = [("dimension", ctypes.c_int), ("num_nodes", ctypes.c_int), ("num_cells", ctypes.c_int),
+                ("num_boundary_elements", ctypes.c_int), ("node_xyz", _c_dbl_p), ("cell_ptr", _c_int_p),
+                ("cell_verts", _c_int_p), ("cell_region", _c_int_p), ("belem_ptr", _c_int_p),
+                ("belem_verts", _c_int_p), ("belem_tag", _c_int_p), ("scale_x", ctypes.c_double),
+                ("scale_y", ctypes.c_double), ("scale_z", ctypes.c_double)]
+
+
+class BandTableC(ctypes.Structure):
+    _fields_ = [("num_materials", ctypes.c_int), ("num_bands", ctypes.c_int), ("group_velocity", _c_dbl_p),
+                ("relaxation_time", _c_dbl_p), ("heat_capacity", _c_dbl_p), ("lattice_ratio", _c_dbl_p),
+                ("heat_ratio", _c_dbl_p), ("num_regions", ctypes.c_int), ("region_material", _c_int_p),
+                ("material_dimension", ctypes.c_int)]
+
+
+class BCTable(ctypes.Structure):
+    _fields_ = [("num", ctypes.c_int), ("tag", _c_int_p), ("type", _c_int_p), ("value", _c_dbl_p)]
+
+
+class AngleSpec(ctypes.Structure):
+    _fields_ = [("method", ctypes.c_int), ("n_theta", ctypes.c_int), ("n_phi", ctypes.c_int)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("use_limiter", ctypes.c_int), ("max_iter", ctypes.c_int),
+                ("err_temp", ctypes.c_double), ("err_flux", ctypes.c_double), ("cell_heat", _c_dbl_p),
+                ("stream", ctypes.c_void_p), ("device", ctypes.c_int), ("verbose", ctypes.c_int),
+                ("macro_rtol", ctypes.c_double)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("err_temp", ctypes.c_double), ("err_flux", ctypes.c_double),
+                ("solve_ms", ctypes.c_double), ("setup_ms", ctypes.c_double), ("transport_ms", ctypes.c_double),
+                ("macro_ms", ctypes.c_double), ("macro_cg_iterations", ctypes.c_longlong),
+                ("updates", ctypes.c_longlong), ("num_directions", ctypes.c_int), ("num_bands", ctypes.c_int),
+                ("num_cells", ctypes.c_int), ("max_levels", ctypes.c_int), ("lagged_faces", ctypes.c_int),
+                ("inner_iterations", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+EXPORTS = ["gbte_default_options", "gbte_create", "gbte_create_from_deck", "gbte_set_initial",
+           "gbte_fourier_initial", "gbte_solve", "gbte_get_fields", "gbte_write_outputs", "gbte_get_sizes",
+           "gbte_get_geometry", "gbte_last_error", "gbte_status_string", "gbte_destroy"]
+
+_lib = None
+
+
+def library():
+    """Load the compiled library (building it first if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            from . import build as _build
+            _build.build()
+        lib = ctypes.CDLL(LIB_PATH)
+        lib.gbte_last_error.restype = ctypes.c_char_p
+        lib.gbte_last_error.argtypes = [ctypes.c_void_p]
+        lib.gbte_status_string.restype = ctypes.c_char_p
+        lib.gbte_create.argtypes = [ctypes.POINTER(MeshView), ctypes.POINTER(BandTableC), ctypes.POINTER(BCTable),
+                                    ctypes.POINTER(AngleSpec), ctypes.POINTER(Options),
+                                    ctypes.POINTER(ctypes.c_void_p)]
+        lib.gbte_create_from_deck.argtypes = [ctypes.c_char_p, ctypes.POINTER(Options),
+                                              ctypes.POINTER(ctypes.c_void_p)]
+        lib.gbte_set_initial.argtypes = [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, _c_dbl_p]
+        lib.gbte_solve.argtypes = [ctypes.c_void_p, ctypes.POINTER(Stats)]
+        lib.gbte_get_fields.argtypes = [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, _c_dbl_p, _c_dbl_p]
+        lib.gbte_write_outputs.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        lib.gbte_get_sizes.argtypes = [ctypes.c_void_p] + [_c_int_p] * 4
+        lib.gbte_get_geometry.argtypes = [ctypes.c_void_p, _c_dbl_p, _c_dbl_p]
+        lib.gbte_destroy.argtypes = [ctypes.c_void_p]
+        lib.gbte_fourier_initial.argtypes = [ctypes.c_void_p]
+        _lib = lib
+    return _lib
+
+
+class GBTEError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(ctypes.POINTER(t)) if a is not None else None
+
+
+def default_options(precision: int = GBTE_FP64, **kw) -> Options:
+    o = Options()
+    library().gbte_default_options(ctypes.byref(o))
+    o.precision = precision
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class StaticBTESynthetic:
+    """One solver instance on one GPU (see module docstring)."""
+
+    def __init__(self, handle: ctypes.c_void_p, keep=()):
+        self._h = handle
+        self._keep = keep
+        lib = library()
+        nc, nb, nd, nbs = (ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int())
+        lib.gbte_get_sizes(self._h, ctypes.byref(nc), ctypes.byref(nb), ctypes.byref(nd), ctypes.byref(nbs))
+        self.num_cells, self.num_bands, self.num_directions, self.num_boundary_sides = (
+            nc.value, nb.value, nd.value, nbs.value)
+        self.stats: Optional[dict] = None
+
+    # --- construction -----------------------------------------------------
+    @classmethod
+    def from_deck_dir(cls, path: str, precision: int = GBTE_FP64, device: int = 0, verbose: int = 0,
+                      **opt) -> "StaticBTESynthetic":
+        lib = library()
+        o = default_options(precision, device=device, verbose=verbose, **opt)
+        h = ctypes.c_void_p()
+        rc = lib.gbte_create_from_deck(path.encode(), ctypes.byref(o), ctypes.byref(h))
+        if rc != GBTE_OK:
+            raise GBTEError(rc, lib.gbte_last_error(None).decode())
+        return cls(h)
+
+    @classmethod
+    def from_deck(cls, deck, precision: int = GBTE_FP64, device: int = 0, verbose: int = 0,
+                  cell_heat: Optional[np.ndarray] = None, **opt) -> "StaticBTESynthetic":
+        """Build from a :class:`giftbte_b200.decks.Deck` held in memory."""
+        lib = library()
+        m = deck.mesh
+        nc = m.n_cells
+        nn = len(m.nodes)
+        xyz = np.zeros((nn, 3))
+        xyz[:, 0] = m.nodes[:, 0] * deck.scale[0]
+        xyz[:, 1] = m.nodes[:, 1] * deck.scale[1]
+        if m.nodes.shape[1] > 2:
+            xyz[:, 2] = m.nodes[:, 2] * (deck.scale[2] if len(deck.scale) > 2 else deck.scale[0])
+        cells = [np.asarray(c) for c in m.cells]
+        cptr = np.zeros(nc + 1, dtype=np.int32)
+        cptr[1:] = np.cumsum([len(c) for c in cells])
+        cverts = np.ascontiguousarray(np.concatenate(cells), dtype=np.int32)
+        creg = np.ascontiguousarray(m.cell_region, dtype=np.int32)
+        edges = np.asarray(m.edges)
+        nbe = len(edges)
+        bptr = (np.arange(nbe + 1) * edges.shape[1]).astype(np.int32)
+        bverts = np.ascontiguousarray(edges.ravel(), dtype=np.int32)
+        btag = np.ascontiguousarray(m.edge_tags, dtype=np.int32)
+        dim = 3 if (m.nodes.shape[1] > 2) else 2
+        mv = MeshView(dim, nn, nc, nbe, _ptr(xyz, ctypes.c_double), _ptr(cptr, ctypes.c_int),
+                      _ptr(cverts, ctypes.c_int), _ptr(creg, ctypes.c_int), _ptr(bptr, ctypes.c_int),
+                      _ptr(bverts, ctypes.c_int), _ptr(btag, ctypes.c_int), deck.scale[0], deck.scale[1],
+                      deck.scale[2] if len(deck.scale) > 2 else 1.0)
+        B = deck.bands
+        arrs = [np.ascontiguousarray(getattr(B, k), dtype=np.float64)
+                for k in ("v", "tau", "C", "lattice_ratio", "heat_ratio")]
+        reg = np.zeros(max(1, int(np.max(creg)) + 1), dtype=np.int32)
+        bt = BandTableC(1, B.n_bands, *[_ptr(a, ctypes.c_double) for a in arrs], len(reg),
+                        _ptr(reg, ctypes.c_int), deck.material_dim)
+        tags = np.asarray([b.tag for b in deck.bcs], dtype=np.int32)
+        types = np.asarray([b.type for b in deck.bcs], dtype=np.int32)
+        vals = np.asarray([b.value for b in deck.bcs], dtype=np.float64)
+        bc = BCTable(len(deck.bcs), _ptr(tags, ctypes.c_int), _ptr(types, ctypes.c_int), _ptr(vals, ctypes.c_double))
+        an = AngleSpec(deck.angle_method, deck.n_theta, deck.n_phi)
+        if cell_heat is None and deck.heat_source is not None:
+            cell_heat = np.full(nc, float(deck.heat_source))
+        heat = np.ascontiguousarray(cell_heat, dtype=np.float64) if cell_heat is not None else None
+        o = default_options(precision, device=device, verbose=verbose, max_iter=deck.max_iter,
+                            err_temp=deck.residual_temp, err_flux=deck.residual_flux, **opt)
+        o.cell_heat = _ptr(heat, ctypes.c_double)
+        h = ctypes.c_void_p()
+        rc = lib.gbte_create(ctypes.byref(mv), ctypes.byref(bt), ctypes.byref(bc), ctypes.byref(an), ctypes.byref(o),
+                             ctypes.byref(h))
+        if rc != GBTE_OK:
+            raise GBTEError(rc, lib.gbte_last_error(None).decode())
+        s = cls(h)
+        s.set_initial(np.full(nc, deck.tref))
+        return s
+
+    # --- the reference's solve interface ----------------------------------
+    def set_initial(self, T0: np.ndarray, q0: Optional[np.ndarray] = None,
+                    boundary_thermal: Optional[np.ndarray] = None) -> None:
+        T0 = np.ascontiguousarray(T0, dtype=np.float64)
+        q0 = np.ascontiguousarray(q0, dtype=np.float64) if q0 is not None else None
+        bt = np.ascontiguousarray(boundary_thermal, dtype=np.float64) if boundary_thermal is not None else None
+        self._check(library().gbte_set_initial(self._h, _ptr(T0, ctypes.c_double), _ptr(q0, ctypes.c_double),
+                                               _ptr(bt, ctypes.c_double)))
+
+    def solve(self, allow_not_converged: bool = True) -> dict:
+        st = Stats()
+        rc = library().gbte_solve(self._h, ctypes.byref(st))
+        self.stats = st.as_dict()
+        if rc == GBTE_ERR_NOT_CONVERGED and allow_not_converged:
+            return self.stats
+        self._check(rc)
+        return self.stats
+
+    def fields(self) -> dict:
+        nc, nb = self.num_cells, self.num_bands
+        TE = np.zeros(nc); TL = np.zeros(nc); q = np.zeros(3 * nc); TB = np.zeros(nb * nc)
+        self._check(library().gbte_get_fields(self._h, _ptr(TE, ctypes.c_double), _ptr(TL, ctypes.c_double),
+                                              _ptr(q, ctypes.c_double), _ptr(TB, ctypes.c_double)))
+        return {"E": TE, "T": TL, "q": q.reshape(nc, 3), "Tband": TB.reshape(nb, nc)}
+
+    @property
+    def temperature(self):
+        return self.fields()["T"]
+
+    @property
+    def total_energy(self):
+        return self.fields()["E"]
+
+    @property
+    def heat_flux(self):
+        return self.fields()["q"]
+
+    @property
+    def temperature_band(self):
+        return self.fields()["Tband"]
+
+    def geometry(self):
+        nc = self.num_cells
+        c = np.zeros(3 * nc); v = np.zeros(nc)
+        self._check(library().gbte_get_geometry(self._h, _ptr(c, ctypes.c_double), _ptr(v, ctypes.c_double)))
+        return c.reshape(nc, 3), v
+
+    def write_outputs(self, path: str) -> None:
+        self._check(library().gbte_write_outputs(self._h, path.encode()))
+
+    def close(self) -> None:
+        if self._h:
+            library().gbte_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int) -> None:
+        if rc != GBTE_OK:
+            raise GBTEError(rc, library().gbte_last_error(self._h).decode())
+
+
+def effective_conductivity(q: np.ndarray, volumes: np.ndarray, length: float, delta_T: float, axis: int = 0) -> float:
+    """k_eff = <q_axis>_V * L / dT, the volume-averaged flux over the
+    temperature difference (the reference computes it in post-processing,
+    bin/examples/cross-plane/verify_kappa_crossplane.m:7)."""
+    return float(np.sum(q[:, axis] * volumes) / np.sum(volumes) * length / delta_T)

@@ -1,0 +1,404 @@
+// C ABI of the B200 solver (include/giftbte.h). Converts the plain-pointer
+// views into host structures, builds the flat mesh and the device solver,
+// and maps every failure to a status code plus a per-handle message; nothing
+// here exits the process or lets an exception cross the boundary.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "../../include/giftbte.h"
+#include "gbte_internal.h"
+#include "solver.cuh"
+
+struct gbte_handle {
+    gbte::Solver solver;
+    gbte::FlatMesh *mesh() { return &solver.mesh; }
+    std::string err;
+    double setup_ms = 0;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int fail(gbte_handle *h, const gbte::Error &e) {
+    if (h) h->err = e.msg;
+    g_create_error = e.msg;
+    return e.code;
+}
+
+int status_of(int code) {
+    switch (code) {
+    case 0: return GBTE_OK;
+    case 1: return GBTE_ERR_NOT_CONVERGED;
+    case -1: return GBTE_ERR_ARG;
+    case -2: return GBTE_ERR_IO;
+    case -3: return GBTE_ERR_CUDA;
+    case -4: return GBTE_ERR_DIVERGED;
+    case -5: return GBTE_ERR_TIMEOUT;
+    case -6: return GBTE_ERR_NOMEM;
+    case -7: return GBTE_ERR_MESH;
+    case -8: return GBTE_ERR_UNSUPPORTED;
+    default: return GBTE_ERR_ARG;
+    }
+}
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+int create_common(const gbte::RawMesh &raw, const gbte::Bands &bands_in, const gbte::BCs &bcs, const gbte_angle_spec &as,
+                  const gbte_options &opt, const std::vector<double> &cell_heat, gbte_handle **out) {
+    double t0 = now_ms();
+    std::unique_ptr<gbte_handle> h(new (std::nothrow) gbte_handle());
+    if (!h) {
+        g_create_error = "host allocation failed";
+        return GBTE_ERR_NOMEM;
+    }
+    gbte::Bands bands = bands_in;
+    bands.kappa.assign(bands.nmat, 0.0);
+    bands.capb.assign(bands.nmat, 0.0);
+    for (int m = 0; m < bands.nmat; m++) {  // BTEBand.cpp:791-819
+        double sl = 0, sh = 0;
+        for (int b = 0; b < bands.nb; b++) {
+            int i = m * bands.nb + b;
+            double k = bands.C[i] * bands.v[i] * bands.v[i] * bands.tau[i];
+            bands.kappa[m] += (bands.material_dim == 2) ? k / 2 : k / 3;
+            bands.capb[m] += bands.C[i];
+            sl += bands.lat[i];
+            sh += bands.hr[i];
+        }
+        if (std::isnan(bands.kappa[m])) return fail(nullptr, {-1, "mistake in phonon properties, nan"}), GBTE_ERR_ARG;
+        if (std::fabs(sl - 1.0) > 1e-6)
+            return fail(nullptr, {-1, "lattice ratios of a material do not sum to 1"}), GBTE_ERR_ARG;
+        for (int b = 0; b < bands.nb; b++)
+            if (!(bands.C[m * bands.nb + b] > 0) || !(bands.v[m * bands.nb + b] > 0) || !(bands.tau[m * bands.nb + b] > 0))
+                return fail(nullptr, {-1, "band heat capacity, group velocity and relaxation time must be positive"}),
+                       GBTE_ERR_ARG;
+    }
+    gbte::Angles ang;
+    gbte::Error e = gbte::make_angles(as.method, as.n_theta, as.n_phi, bands.material_dim, ang);
+    if (e.code) return fail(nullptr, e), status_of(e.code);
+    gbte::FlatMesh fm;
+    e = gbte::build_flat_mesh(raw, bcs, bands, fm);
+    if (e.code) return fail(nullptr, e), status_of(e.code);
+    gbte::SolverConfig cfg;
+    cfg.precision = opt.precision;
+    cfg.use_limiter = opt.use_limiter;
+    cfg.max_iter = opt.max_iter;
+    cfg.err_temp = opt.err_temp;
+    cfg.err_flux = opt.err_flux;
+    cfg.macro_rtol = opt.macro_rtol > 0 ? opt.macro_rtol : 1e-13;
+    cfg.verbose = opt.verbose;
+    cfg.device = opt.device;
+    cfg.stream = (cudaStream_t)opt.stream;
+    if (opt.precision != GBTE_FP64 && opt.precision != GBTE_FP32_MIXED)
+        return fail(nullptr, {-1, "precision must be GBTE_FP64 or GBTE_FP32_MIXED"}), GBTE_ERR_ARG;
+    std::vector<double> heat = cell_heat;
+    e = h->solver.init(fm, bands, ang, heat, cfg);
+    if (e.code) return fail(nullptr, e), status_of(e.code);
+    h->setup_ms = now_ms() - t0;
+    *out = h.release();
+    return GBTE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void gbte_default_options(gbte_options *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->precision = GBTE_FP64;
+    o->max_iter = 10000;
+    o->err_temp = 1e-6;
+    o->err_flux = 1e-4;
+    o->macro_rtol = 1e-13;
+}
+
+int gbte_create(const gbte_mesh_view *mv, const gbte_band_table *bt, const gbte_bc_table *bc, const gbte_angle_spec *as,
+                const gbte_options *opt, gbte_handle **out) {
+    try {
+        if (!mv || !bt || !bc || !as || !opt || !out) return fail(nullptr, {-1, "null argument"}), GBTE_ERR_ARG;
+        *out = nullptr;
+        if (mv->num_nodes <= 0 || mv->num_cells <= 0 || !mv->node_xyz || !mv->cell_ptr || !mv->cell_verts ||
+            !mv->cell_region || (mv->num_boundary_elements > 0 && (!mv->belem_ptr || !mv->belem_verts || !mv->belem_tag)))
+            return fail(nullptr, {-1, "incomplete mesh view"}), GBTE_ERR_ARG;
+        if (bt->num_materials <= 0 || bt->num_bands <= 0 || !bt->group_velocity || !bt->relaxation_time ||
+            !bt->heat_capacity || !bt->lattice_ratio || !bt->heat_ratio || bt->num_regions <= 0 || !bt->region_material)
+            return fail(nullptr, {-1, "incomplete band table"}), GBTE_ERR_ARG;
+        if (bc->num < 0 || (bc->num > 0 && (!bc->tag || !bc->type || !bc->value)))
+            return fail(nullptr, {-1, "incomplete BC table"}), GBTE_ERR_ARG;
+        gbte::RawMesh raw;
+        raw.dim = mv->dimension;
+        raw.xyz.assign(mv->node_xyz, mv->node_xyz + 3 * (size_t)mv->num_nodes);
+        raw.cptr.assign(mv->cell_ptr, mv->cell_ptr + mv->num_cells + 1);
+        if (raw.cptr[0] != 0) return fail(nullptr, {-1, "cell_ptr must start at 0"}), GBTE_ERR_ARG;
+        for (int i = 0; i < mv->num_cells; i++)
+            if (raw.cptr[i + 1] < raw.cptr[i]) return fail(nullptr, {-1, "cell_ptr must be non-decreasing"}), GBTE_ERR_ARG;
+        raw.cverts.assign(mv->cell_verts, mv->cell_verts + raw.cptr.back());
+        raw.creg.assign(mv->cell_region, mv->cell_region + mv->num_cells);
+        raw.bptr.assign(1, 0);
+        if (mv->num_boundary_elements > 0) {
+            raw.bptr.assign(mv->belem_ptr, mv->belem_ptr + mv->num_boundary_elements + 1);
+            if (raw.bptr[0] != 0) return fail(nullptr, {-1, "belem_ptr must start at 0"}), GBTE_ERR_ARG;
+            for (int i = 0; i < mv->num_boundary_elements; i++)
+                if (raw.bptr[i + 1] < raw.bptr[i]) return fail(nullptr, {-1, "belem_ptr must be non-decreasing"}), GBTE_ERR_ARG;
+            raw.bverts.assign(mv->belem_verts, mv->belem_verts + raw.bptr.back());
+            raw.btag.assign(mv->belem_tag, mv->belem_tag + mv->num_boundary_elements);
+        }
+        raw.Lx = mv->scale_x > 0 ? mv->scale_x : 1.0;
+        raw.Ly = mv->scale_y;
+        raw.Lz = mv->scale_z;
+        gbte::Bands B;
+        B.nmat = bt->num_materials;
+        B.nb = bt->num_bands;
+        B.material_dim = bt->material_dimension;
+        size_t n = (size_t)B.nmat * B.nb;
+        B.v.assign(bt->group_velocity, bt->group_velocity + n);
+        B.tau.assign(bt->relaxation_time, bt->relaxation_time + n);
+        B.C.assign(bt->heat_capacity, bt->heat_capacity + n);
+        B.lat.assign(bt->lattice_ratio, bt->lattice_ratio + n);
+        B.hr.assign(bt->heat_ratio, bt->heat_ratio + n);
+        B.region_material.assign(bt->region_material, bt->region_material + bt->num_regions);
+        for (int r : B.region_material)
+            if (r < 0 || r >= B.nmat) return fail(nullptr, {-1, "region_material out of range"}), GBTE_ERR_ARG;
+        gbte::BCs bcs;
+        for (int i = 0; i < bc->num; i++) {
+            bcs.tag.push_back(bc->tag[i]);
+            bcs.type.push_back(bc->type[i]);
+            bcs.value.push_back(bc->value[i]);
+        }
+        std::vector<double> heat;
+        if (opt->cell_heat) heat.assign(opt->cell_heat, opt->cell_heat + mv->num_cells);
+        return create_common(raw, B, bcs, *as, *opt, heat, out);
+    } catch (const std::bad_alloc &) {
+        g_create_error = "host allocation failed";
+        return GBTE_ERR_NOMEM;
+    } catch (const std::exception &ex) {
+        g_create_error = ex.what();
+        return GBTE_ERR_ARG;
+    }
+}
+
+int gbte_create_from_deck(const char *dir, const gbte_options *opt_in, gbte_handle **out) {
+    try {
+        if (!dir || !out) return fail(nullptr, {-1, "null argument"}), GBTE_ERR_ARG;
+        *out = nullptr;
+        gbte_options opt;
+        if (opt_in)
+            opt = *opt_in;
+        else
+            gbte_default_options(&opt);
+        gbte::Deck deck;
+        gbte::Error e = gbte::read_deck(dir, deck);
+        if (e.code) return fail(nullptr, e), status_of(e.code);
+        if (deck.order == "2limit")
+            opt.use_limiter = 1;
+        else if (deck.order != "2")
+            return fail(nullptr, {-8, "only Order=2 / 2limit (second-order synthetic) is implemented"}), GBTE_ERR_UNSUPPORTED;
+        if (deck.method != "Synthetic")
+            return fail(nullptr, {-8, "only IterativeScheme=Synthetic is implemented"}), GBTE_ERR_UNSUPPORTED;
+        opt.max_iter = deck.max_iter;
+        opt.err_temp = deck.err_temp;
+        opt.err_flux = deck.err_flux;
+        gbte_angle_spec as{deck.angle_method, deck.n_theta, deck.n_phi};
+        int rc = create_common(deck.mesh, deck.bands, deck.bcs, as, opt, deck.cell_heat, out);
+        if (rc == GBTE_OK) {
+            // Tref as the initial temperature; gbte_fourier_initial / gbte_set_initial may replace it
+            std::vector<double> T0(deck.mesh.nc(), deck.tref);
+            gbte::Error e2 = (*out)->solver.set_initial(T0.data(), nullptr, nullptr);
+            if (e2.code) {
+                delete *out;
+                *out = nullptr;
+                return fail(nullptr, e2), status_of(e2.code);
+            }
+        }
+        return rc;
+    } catch (const std::bad_alloc &) {
+        g_create_error = "host allocation failed";
+        return GBTE_ERR_NOMEM;
+    } catch (const std::exception &ex) {
+        g_create_error = ex.what();
+        return GBTE_ERR_ARG;
+    }
+}
+
+int gbte_set_initial(gbte_handle *h, const double *T0, const double *q0, const double *bth) {
+    if (!h) return GBTE_ERR_ARG;
+    try {
+        gbte::Error e = h->solver.set_initial(T0, q0, bth);
+        if (e.code) return fail(h, e), status_of(e.code);
+        return GBTE_OK;
+    } catch (const std::exception &ex) {
+        h->err = ex.what();
+        return GBTE_ERR_ARG;
+    }
+}
+
+int gbte_fourier_initial(gbte_handle *h) {
+    if (!h) return GBTE_ERR_ARG;
+    gbte::Error e = h->solver.fourier_initial();
+    if (e.code) return fail(h, e), status_of(e.code);
+    return GBTE_OK;
+}
+
+int gbte_solve(gbte_handle *h, gbte_stats *st) {
+    if (!h) return GBTE_ERR_ARG;
+    try {
+        gbte::SolveStats s;
+        gbte::Error e = h->solver.solve(s);
+        if (st) {
+            std::memset(st, 0, sizeof(*st));
+            st->iterations = s.iterations;
+            st->err_temp = s.err_temp;
+            st->err_flux = s.err_flux;
+            st->solve_ms = s.solve_ms;
+            st->setup_ms = h->setup_ms;
+            st->transport_ms = s.transport_ms;
+            st->macro_ms = s.macro_ms;
+            st->macro_cg_iterations = s.cg_iterations;
+            st->updates = s.updates;
+            st->num_directions = h->solver.ang.nd;
+            st->num_bands = h->solver.bands.nb;
+            st->num_cells = h->solver.mesh.nc;
+            st->max_levels = h->solver.sched.max_levels;
+            st->lagged_faces = h->solver.sched.lagged_faces;
+            st->inner_iterations = s.inner_iterations;
+        }
+        if (e.code) {
+            if (e.code > 0) {
+                h->err = e.msg;
+                return status_of(e.code);
+            }
+            return fail(h, e), status_of(e.code);
+        }
+        return GBTE_OK;
+    } catch (const std::exception &ex) {
+        h->err = ex.what();
+        return GBTE_ERR_ARG;
+    }
+}
+
+int gbte_get_fields(gbte_handle *h, double *TE, double *TL, double *q, double *TB) {
+    if (!h) return GBTE_ERR_ARG;
+    gbte::Error e = h->solver.get_fields(TE, TL, q, TB);
+    if (e.code) return fail(h, e), status_of(e.code);
+    return GBTE_OK;
+}
+
+int gbte_get_sizes(gbte_handle *h, int *nc, int *nb, int *nd, int *nbs) {
+    if (!h) return GBTE_ERR_ARG;
+    if (nc) *nc = h->solver.mesh.nc;
+    if (nb) *nb = h->solver.bands.nb;
+    if (nd) *nd = h->solver.ang.nd;
+    if (nbs) *nbs = h->solver.mesh.nbs();
+    return GBTE_OK;
+}
+
+int gbte_get_geometry(gbte_handle *h, double *centers, double *volumes) {
+    if (!h) return GBTE_ERR_ARG;
+    const gbte::FlatMesh &m = h->solver.mesh;
+    for (int c = 0; c < m.nc; c++) {
+        if (centers) {
+            centers[3 * c] = m.cx[c];
+            centers[3 * c + 1] = m.cy[c];
+            centers[3 * c + 2] = m.cz[c];
+        }
+        if (volumes) volumes[c] = m.vol[c];
+    }
+    return GBTE_OK;
+}
+
+int gbte_write_outputs(gbte_handle *h, const char *dir) {
+    if (!h || !dir) return GBTE_ERR_ARG;
+    const gbte::FlatMesh &m = h->solver.mesh;
+    const int nc = m.nc, nb = h->solver.bands.nb;
+    std::vector<double> TE(nc), TL(nc), q(3 * (size_t)nc), TB((size_t)nb * nc);
+    int rc = gbte_get_fields(h, TE.data(), TL.data(), q.data(), TB.data());
+    if (rc != GBTE_OK) return rc;
+    std::string d(dir);
+    auto open = [&](const char *name, std::ofstream &f) {
+        f.open(d + "/" + name);
+        f << std::setprecision(17);
+        return f.is_open();
+    };
+    std::ofstream f;
+    // TempLattice.dat / Tempband.dat / Temperature.dat / HeatFlux.dat (StaticBTESynthetic.cpp:2613-2653)
+    if (!open("TempLattice.dat", f)) return fail(h, {-2, "cannot write TempLattice.dat"}), GBTE_ERR_IO;
+    for (int i = 0; i < nc; i++) f << m.cx[i] << " " << m.cy[i] << " " << m.cz[i] << " " << TL[i] << "\n";
+    f.close();
+    if (!open("Tempband.dat", f)) return fail(h, {-2, "cannot write Tempband.dat"}), GBTE_ERR_IO;
+    for (int j = 0; j < nb; j++)
+        for (int i = 0; i < nc; i++)
+            f << j + 1 << " " << m.cx[i] << " " << m.cy[i] << " " << m.cz[i] << " " << TB[(size_t)j * nc + i] << "\n";
+    f.close();
+    if (!open("Temperature.dat", f)) return fail(h, {-2, "cannot write Temperature.dat"}), GBTE_ERR_IO;
+    for (int i = 0; i < nc; i++) f << m.cx[i] << " " << m.cy[i] << " " << m.cz[i] << " " << TE[i] << "\n";
+    f.close();
+    if (!open("HeatFlux.dat", f)) return fail(h, {-2, "cannot write HeatFlux.dat"}), GBTE_ERR_IO;
+    for (int i = 0; i < nc; i++) {
+        double v[6] = {m.cx[i], m.cy[i], m.cz[i], q[3 * i], q[3 * i + 1], q[3 * i + 2]};
+        for (double x : v) f << " " << std::setw(24) << x;
+        f << "\n";
+    }
+    f.close();
+    // Result.vtk (Solution.cpp:163-220): legacy ASCII, nodes divided by the scales
+    if (!open("Result.vtk", f)) return fail(h, {-2, "cannot write Result.vtk"}), GBTE_ERR_IO;
+    f << "# vtk DataFile Version 2.0\nRESULT\nASCII\nDATASET UNSTRUCTURED_GRID\n";
+    f << "POINTS " << m.nn << " float\n";
+    for (int i = 0; i < m.nn; i++) f << m.node_x[i] / m.Lx << " " << m.node_y[i] / m.Lx << " " << m.node_z[i] / m.Lx << "\n";
+    size_t total = 0;
+    for (int c = 0; c < nc; c++) total += m.cptr[c + 1] - m.cptr[c] + 1;
+    f << "\nCELLS " << nc << " " << total << "\n";
+    for (int c = 0; c < nc; c++) {
+        f << m.cptr[c + 1] - m.cptr[c];
+        for (int k = m.cptr[c]; k < m.cptr[c + 1]; k++) f << " " << m.cverts[k];
+        f << "\n";
+    }
+    f << "\nCELL_TYPES " << nc << "\n";
+    for (int c = 0; c < nc; c++) {
+        int nv = m.cptr[c + 1] - m.cptr[c];
+        f << (m.dim == 2 ? (nv == 4 ? 8 : 5) : 10) << "\n";
+    }
+    f << "\nCELL_DATA " << nc << "\nSCALARS Temperature float 1\nLOOKUP_TABLE default\n";
+    for (int c = 0; c < nc; c++) f << TE[c] << "\n";
+    f << "VECTORS HeatFLux float\n";
+    for (int c = 0; c < nc; c++) f << q[3 * c] << " " << q[3 * c + 1] << " " << q[3 * c + 2] << "\n";
+    f.close();
+    return GBTE_OK;
+}
+
+const char *gbte_last_error(const gbte_handle *h) {
+    if (!h) return g_create_error.c_str();
+    return h->err.c_str();
+}
+
+const char *gbte_status_string(int s) {
+    switch (s) {
+    case GBTE_OK: return "ok";
+    case GBTE_ERR_ARG: return "invalid argument";
+    case GBTE_ERR_IO: return "input/output error";
+    case GBTE_ERR_CUDA: return "CUDA error";
+    case GBTE_ERR_DIVERGED: return "diverged";
+    case GBTE_ERR_TIMEOUT: return "device wait timed out";
+    case GBTE_ERR_NOMEM: return "out of memory";
+    case GBTE_ERR_MESH: return "mesh topology error";
+    case GBTE_ERR_UNSUPPORTED: return "unsupported input";
+    case GBTE_ERR_NOT_CONVERGED: return "not converged within max_iter";
+    default: return "unknown status";
+    }
+}
+
+int gbte_destroy(gbte_handle *h) {
+    delete h;
+    return GBTE_OK;
+}
+
+}  // extern "C"

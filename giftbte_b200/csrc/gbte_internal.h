@@ -1,0 +1,116 @@
+// Host-side data structures of the B200 solver (not part of the C ABI).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace gbte {
+
+struct Error {
+    int code;
+    std::string msg;
+};
+
+// Raw mesh as read from a deck (coordinates in metres).
+struct RawMesh {
+    int dim = 2;
+    std::vector<double> xyz;               // [nn*3]
+    std::vector<int> cptr, cverts, creg;   // cells
+    std::vector<int> bptr, bverts, btag;   // boundary elements
+    double Lx = 1, Ly = 1, Lz = 1;
+    int nn() const { return (int)(xyz.size() / 3); }
+    int nc() const { return (int)cptr.size() - 1; }
+    int nbe() const { return (int)bptr.size() - 1; }
+};
+
+struct Bands {
+    int nmat = 1, nb = 0, material_dim = 3;
+    std::vector<double> v, tau, C, lat, hr;  // [m*nb + b]
+    std::vector<int> region_material;
+    std::vector<double> kappa, capb;         // per material (BTEBand.cpp:791-803)
+};
+
+struct BCs {
+    std::vector<int> tag, type;
+    std::vector<double> value;
+};
+
+struct Angles {
+    int nd = 0;
+    double solid = 0;
+    std::vector<double> sx, sy, sz, w;  // direction cosines, weight / SolidAngle
+};
+
+// Flattened mesh in structure-of-arrays / CSR form. Cell faces keep the
+// reference's per-cell face order (BTEMesh.cpp:722-772); boundaries keep the
+// reference's boundary order and (boundary, side) numbering, so a boundary
+// side is s = 2*ib + icell exactly like ebound[...][ib*2+icell].
+struct FlatMesh {
+    int dim = 2, nc = 0, nn = 0, nmat = 1;
+    double Lx = 1;
+    // cells
+    std::vector<int> matter;
+    std::vector<double> vol, cx, cy, cz;
+    std::vector<int> cf_ptr;  // [nc+1]
+    // cell faces (k = cf_ptr[c] + j)
+    std::vector<double> cf_area, cf_nx, cf_ny, cf_nz, cf_fx, cf_fy, cf_fz;
+    std::vector<int> cf_nbr, cf_bside, cf_bound, cf_face;
+    std::vector<int> cf_v;  // [ncf*3] face vertices (third = -1 in 2D)
+    // global faces (Element_Faces order, BTEMesh.cpp:987-1021)
+    std::vector<int> f_cell0, f_cf0, f_cell1, f_cf1, f_bound;
+    // vertex-neighbour least-squares stencil (StaticBTESynthetic.cpp:453-465,
+    // 967-1025); weights already include the 1/ScaleX factors
+    std::vector<int> nbr_ptr, nbr_idx;
+    std::vector<double> lsq_w;  // [entry*3]
+    // 3D face tangential LSQ (FaceMatrix, StaticBTESynthetic.cpp:1617-1649), [f*9]
+    std::vector<double> face_w;
+    // boundaries (after BC matching, BTEMesh.cpp:845-866)
+    std::vector<int> b_type, b_connect, b_tag;
+    std::vector<double> b_T;
+    std::vector<int> bs_cell, bs_cf;  // [2*nbd], -1 if absent
+    // node slots (node*nmat + matter): inverse-distance interpolation.
+    // e-interpolation with boundary override (StaticBTESynthetic.cpp:1541-1616):
+    // src >= 0 is a cell, src < 0 is boundary side (-1 - src)
+    std::vector<int> nv_ptr, nv_src;
+    std::vector<double> nv_w;
+    // temperature interpolation over cells only (:2276-2305)
+    std::vector<int> nt_ptr, nt_src;
+    std::vector<double> nt_w;
+    std::vector<double> node_x, node_y, node_z;
+    // raw cell vertex lists (for output)
+    std::vector<int> cptr, cverts;
+
+    int ncf() const { return (int)cf_area.size(); }
+    int nbd() const { return (int)b_type.size(); }
+    int nbs() const { return 2 * nbd(); }
+    int nf() const { return (int)f_cell0.size(); }
+};
+
+// Per-direction upwind schedule: cells in level order.
+struct Schedule {
+    std::vector<int> lvl_cells;   // [nd*nc]
+    std::vector<int> lvl_ptr;     // concatenated level offsets
+    std::vector<int> dir_lvl_off; // [nd+1] offsets into lvl_ptr (levels of d: lvl_ptr[dir_lvl_off[d] .. +1])
+    std::vector<uint8_t> lag;     // [nd*nc] bit j set: face j of the cell is lagged (empty if none)
+    int max_levels = 0;
+    int lagged_faces = 0;
+};
+
+// Read a deck directory (reference file formats).
+struct Deck {
+    RawMesh mesh;
+    Bands bands;
+    BCs bcs;
+    int angle_method = 2, n_theta = 4, n_phi = 4;
+    std::string order = "2", method = "Sequential", matrix = "LU";
+    int max_iter = 10000;
+    double err_temp = 1e-6, err_flux = 1e-4, tref = 300, uniform_heat = 0;
+    std::vector<double> cell_heat;
+};
+Error read_deck(const std::string &dir, Deck &deck);
+
+Error make_angles(int method, int ntheta, int nphi, int material_dim, Angles &out);
+Error build_flat_mesh(const RawMesh &raw, const BCs &bcs, const Bands &bands, FlatMesh &out);
+void build_schedule(const FlatMesh &m, const Angles &a, Schedule &out, int nthreads);
+
+}  // namespace gbte

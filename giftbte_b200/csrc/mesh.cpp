@@ -1,0 +1,585 @@
+// Mesh flattening: raw cells/boundary elements + BC table -> FlatMesh.
+//
+// Topology semantics follow GiftBTE's BTEMesh (src/BTEMesh/BTEMesh.cpp):
+//   * 2D cell geometry, face vertex order and outward normals :668-772
+//     (triangles: face j = (v[j+1], v[j+2]); COMSOL quads: v0-v1, v1-v3,
+//     v3-v2, v2-v0; area by Heron's formula as get_tri_area)
+//   * face neighbour = last other cell around the face's first vertex that
+//     holds all face vertices :782-806
+//   * boundary element -> (cell, face) sides :808-834
+//   * boundaries kept in mesh order when their tag is in the BC table;
+//     tags that are in no BC row become isothermal at 0 K unless the element
+//     has two cells (Distribute.cpp:150-197)
+//   * periodic partner = nearest face centre among boundaries whose type
+//     names this tag :903-925
+//   * global face list in cell/face order :987-1021
+// 3D tetrahedra (stripped from the reference's public release) use face j =
+// the three vertices other than vertex j, area by Heron, outward normal.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <queue>
+#include <thread>
+
+#include "gbte_internal.h"
+
+namespace gbte {
+namespace {
+
+inline double sq(double x) { return x * x; }
+inline double dist3(double ax, double ay, double az, double bx, double by, double bz) {
+    return std::sqrt(std::pow(ax - bx, 2) + std::pow(ay - by, 2) + std::pow(az - bz, 2));
+}
+double heron(const double *a, const double *b, const double *c) {
+    double la = dist3(a[0], a[1], a[2], b[0], b[1], b[2]);
+    double lb = dist3(b[0], b[1], b[2], c[0], c[1], c[2]);
+    double lc = dist3(a[0], a[1], a[2], c[0], c[1], c[2]);
+    double p = (la + lb + lc) / 2;
+    return std::sqrt(p * (p - la) * (p - lb) * (p - lc));
+}
+
+// (J^T J)^-1 J^T for k rows of dimension dim -> out[r*k + j], r < 3
+void lsq_pinv(const std::vector<double> &J, int k, int dim, std::vector<double> &out) {
+    out.assign(3 * (size_t)k, 0.0);
+    double M[3][3] = {{0}}, N[3][3] = {{0}};
+    for (int i = 0; i < dim; i++)
+        for (int j = 0; j < dim; j++)
+            for (int r = 0; r < k; r++) M[i][j] += J[r * 3 + i] * J[r * 3 + j];
+    if (dim == 2) {
+        double det = M[0][0] * M[1][1] - M[0][1] * M[1][0];
+        N[0][0] = M[1][1] / det;
+        N[0][1] = -M[0][1] / det;
+        N[1][1] = M[0][0] / det;
+        N[1][0] = -M[1][0] / det;
+    } else {
+        double det = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) + M[0][1] * (M[1][2] * M[2][0] - M[1][0] * M[2][2]) +
+                     M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+        N[0][0] = 1.0 / det * (M[1][1] * M[2][2] - M[1][2] * M[2][1]);
+        N[1][0] = 1.0 / det * (M[0][2] * M[2][1] - M[0][1] * M[2][2]);
+        N[2][0] = 1.0 / det * (M[0][1] * M[1][2] - M[0][2] * M[1][1]);
+        N[0][1] = 1.0 / det * (M[1][2] * M[2][0] - M[1][0] * M[2][2]);
+        N[1][1] = 1.0 / det * (M[0][0] * M[2][2] - M[0][2] * M[2][0]);
+        N[2][1] = 1.0 / det * (M[1][0] * M[0][2] - M[0][0] * M[1][2]);
+        N[0][2] = 1.0 / det * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+        N[1][2] = 1.0 / det * (M[0][1] * M[2][0] - M[0][0] * M[2][1]);
+        N[2][2] = 1.0 / det * (M[0][0] * M[1][1] - M[1][0] * M[0][1]);
+    }
+    for (int i = 0; i < dim; i++)
+        for (int j = 0; j < k; j++) {
+            double s = 0;
+            for (int q = 0; q < dim; q++) s += N[i][q] * J[j * 3 + q];
+            out[i * (size_t)k + j] = s;
+        }
+}
+
+}  // namespace
+
+Error build_flat_mesh(const RawMesh &raw, const BCs &bcs, const Bands &bands, FlatMesh &m) {
+    const int dim = raw.dim, nc = raw.nc(), nn = raw.nn(), nbe = raw.nbe();
+    if (dim != 2 && dim != 3) return {-1, "dimension must be 2 or 3"};
+    if (nc <= 0 || nn <= 0) return {-1, "empty mesh"};
+    m = FlatMesh();
+    m.dim = dim;
+    m.nc = nc;
+    m.nn = nn;
+    m.nmat = bands.nmat;
+    m.Lx = raw.Lx;
+    m.node_x.resize(nn);
+    m.node_y.resize(nn);
+    m.node_z.resize(nn);
+    for (int i = 0; i < nn; i++) {
+        m.node_x[i] = raw.xyz[3 * i];
+        m.node_y[i] = raw.xyz[3 * i + 1];
+        m.node_z[i] = dim == 2 ? 0.0 : raw.xyz[3 * i + 2];
+    }
+    auto P = [&](int v, double *p) {
+        p[0] = m.node_x[v];
+        p[1] = m.node_y[v];
+        p[2] = m.node_z[v];
+    };
+    m.cptr = raw.cptr;
+    m.cverts = raw.cverts;
+    m.matter.resize(nc);
+    m.vol.resize(nc);
+    m.cx.resize(nc);
+    m.cy.resize(nc);
+    m.cz.resize(nc);
+    m.cf_ptr.assign(nc + 1, 0);
+    for (int c = 0; c < nc; c++) {
+        int r = raw.creg[c];
+        if (r < 0 || r >= (int)bands.region_material.size())
+            return {-1, "cell region " + std::to_string(r) + " has no material (GeometryMaterialType)"};
+        m.matter[c] = bands.region_material[r];
+        int nv = raw.cptr[c + 1] - raw.cptr[c];
+        int nfc = (dim == 2) ? nv : 4;
+        if (dim == 2 && nv != 3 && nv != 4) return {-1, "2D cells must be triangles or quads"};
+        if (dim == 3 && nv != 4) return {-8, "3D cells must be tetrahedra"};
+        m.cf_ptr[c + 1] = m.cf_ptr[c] + nfc;
+    }
+    const int ncf = m.cf_ptr[nc];
+    m.cf_area.resize(ncf);
+    m.cf_nx.resize(ncf);
+    m.cf_ny.resize(ncf);
+    m.cf_nz.resize(ncf);
+    m.cf_fx.resize(ncf);
+    m.cf_fy.resize(ncf);
+    m.cf_fz.resize(ncf);
+    m.cf_nbr.assign(ncf, -1);
+    m.cf_bside.assign(ncf, -1);
+    m.cf_bound.assign(ncf, -1);
+    m.cf_face.assign(ncf, -1);
+    m.cf_v.assign(3 * (size_t)ncf, -1);
+    for (int c = 0; c < nc; c++) {
+        const int *v = &raw.cverts[raw.cptr[c]];
+        int nv = raw.cptr[c + 1] - raw.cptr[c];
+        double p[4][3];
+        for (int k = 0; k < std::min(nv, 4); k++) P(v[k], p[k]);
+        int k0 = m.cf_ptr[c];
+        if (dim == 2) {
+            if (nv == 3) {
+                m.vol[c] = heron(p[0], p[1], p[2]);
+                m.cx[c] = ((p[0][0] + p[1][0]) + p[2][0]) / 3;
+                m.cy[c] = ((p[0][1] + p[1][1]) + p[2][1]) / 3;
+                m.cz[c] = ((p[0][2] + p[1][2]) + p[2][2]) / 3;
+                for (int j = 0; j < 3; j++) {
+                    m.cf_v[3 * (k0 + j)] = v[(j + 1) % 3];
+                    m.cf_v[3 * (k0 + j) + 1] = v[(j + 2) % 3];
+                }
+            } else {
+                m.vol[c] = heron(p[0], p[1], p[2]) + heron(p[1], p[2], p[3]);
+                m.cx[c] = ((p[0][0] + p[1][0]) + p[2][0] + p[3][0]) / 4;
+                m.cy[c] = ((p[0][1] + p[1][1]) + p[2][1] + p[3][1]) / 4;
+                m.cz[c] = ((p[0][2] + p[1][2]) + p[2][2] + p[3][2]) / 4;
+                const int qf[4][2] = {{0, 1}, {1, 3}, {3, 2}, {2, 0}};
+                for (int j = 0; j < 4; j++) {
+                    m.cf_v[3 * (k0 + j)] = v[qf[j][0]];
+                    m.cf_v[3 * (k0 + j) + 1] = v[qf[j][1]];
+                }
+            }
+            for (int j = 0; j < nv; j++) {
+                int k = k0 + j;
+                double a0[3], a1[3];
+                P(m.cf_v[3 * k], a0);
+                P(m.cf_v[3 * k + 1], a1);
+                double area = dist3(a0[0], a0[1], a0[2], a1[0], a1[1], a1[2]);
+                m.cf_area[k] = area;
+                m.cf_fx[k] = (a0[0] + a1[0]) / 2;
+                m.cf_fy[k] = (a0[1] + a1[1]) / 2;
+                m.cf_fz[k] = (a0[2] + a1[2]) / 2;
+                double ax = (a0[0] - a1[0]) / area, ay = (a0[1] - a1[1]) / area;
+                double nx = ay, ny = -ax;
+                double dx = m.cx[c] - m.cf_fx[k], dy = m.cy[c] - m.cf_fy[k], dz = m.cz[c] - m.cf_fz[k];
+                if (dx * nx + dy * ny + dz * 0.0 > 0) {
+                    nx = -nx;
+                    ny = -ny;
+                }
+                m.cf_nx[k] = nx;
+                m.cf_ny[k] = ny;
+                m.cf_nz[k] = 0;
+            }
+        } else {
+            double a[3] = {p[1][0] - p[0][0], p[1][1] - p[0][1], p[1][2] - p[0][2]};
+            double b[3] = {p[2][0] - p[0][0], p[2][1] - p[0][1], p[2][2] - p[0][2]};
+            double d[3] = {p[3][0] - p[0][0], p[3][1] - p[0][1], p[3][2] - p[0][2]};
+            double det = a[0] * (b[1] * d[2] - b[2] * d[1]) - a[1] * (b[0] * d[2] - b[2] * d[0]) + a[2] * (b[0] * d[1] - b[1] * d[0]);
+            m.vol[c] = std::fabs(det) / 6.0;
+            m.cx[c] = (p[0][0] + p[1][0] + p[2][0] + p[3][0]) / 4;
+            m.cy[c] = (p[0][1] + p[1][1] + p[2][1] + p[3][1]) / 4;
+            m.cz[c] = (p[0][2] + p[1][2] + p[2][2] + p[3][2]) / 4;
+            for (int j = 0; j < 4; j++) {
+                int k = k0 + j;
+                int fv[3] = {v[(j + 1) % 4], v[(j + 2) % 4], v[(j + 3) % 4]};
+                double q[3][3];
+                for (int t = 0; t < 3; t++) {
+                    m.cf_v[3 * k + t] = fv[t];
+                    P(fv[t], q[t]);
+                }
+                m.cf_area[k] = heron(q[0], q[1], q[2]);
+                m.cf_fx[k] = (q[0][0] + q[1][0] + q[2][0]) / 3;
+                m.cf_fy[k] = (q[0][1] + q[1][1] + q[2][1]) / 3;
+                m.cf_fz[k] = (q[0][2] + q[1][2] + q[2][2]) / 3;
+                double u[3] = {q[1][0] - q[0][0], q[1][1] - q[0][1], q[1][2] - q[0][2]};
+                double w[3] = {q[2][0] - q[0][0], q[2][1] - q[0][1], q[2][2] - q[0][2]};
+                double cr[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
+                double l = std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+                double nx = cr[0] / l, ny = cr[1] / l, nz = cr[2] / l;
+                if ((m.cx[c] - m.cf_fx[k]) * nx + (m.cy[c] - m.cf_fy[k]) * ny + (m.cz[c] - m.cf_fz[k]) * nz > 0) {
+                    nx = -nx;
+                    ny = -ny;
+                    nz = -nz;
+                }
+                m.cf_nx[k] = nx;
+                m.cf_ny[k] = ny;
+                m.cf_nz[k] = nz;
+            }
+        }
+    }
+    // node -> cells (in cell order)
+    std::vector<int> nc_ptr(nn + 1, 0), nc_idx;
+    for (int c = 0; c < nc; c++)
+        for (int q = raw.cptr[c]; q < raw.cptr[c + 1]; q++) {
+            int vtx = raw.cverts[q];
+            if (vtx < 0 || vtx >= nn) return {-1, "cell vertex index out of range"};
+            nc_ptr[vtx + 1]++;
+        }
+    for (int i = 0; i < nn; i++) nc_ptr[i + 1] += nc_ptr[i];
+    nc_idx.resize(nc_ptr[nn]);
+    {
+        std::vector<int> fill(nc_ptr.begin(), nc_ptr.end() - 1);
+        for (int c = 0; c < nc; c++)
+            for (int q = raw.cptr[c]; q < raw.cptr[c + 1]; q++) nc_idx[fill[raw.cverts[q]]++] = c;
+    }
+    auto cell_has = [&](int c, int vtx) {
+        for (int q = raw.cptr[c]; q < raw.cptr[c + 1]; q++)
+            if (raw.cverts[q] == vtx) return true;
+        return false;
+    };
+    const int fnv = (dim == 2) ? 2 : 3;
+    // face neighbours
+    for (int c = 0; c < nc; c++)
+        for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+            int v0 = m.cf_v[3 * k];
+            for (int q = nc_ptr[v0]; q < nc_ptr[v0 + 1]; q++) {
+                int o = nc_idx[q];
+                if (o == c) continue;
+                bool all = true;
+                for (int t = 0; t < fnv; t++) all = all && cell_has(o, m.cf_v[3 * k + t]);
+                if (all) m.cf_nbr[k] = o;
+            }
+        }
+    // boundary elements -> sides
+    std::vector<std::vector<std::pair<int, int>>> bsides(nbe);
+    for (int i = 0; i < nbe; i++) {
+        int nv = raw.bptr[i + 1] - raw.bptr[i];
+        if (nv != fnv) return {-1, "boundary element vertex count does not match the dimension"};
+        const int *bv = &raw.bverts[raw.bptr[i]];
+        for (int t = 0; t < nv; t++)
+            if (bv[t] < 0 || bv[t] >= nn) return {-1, "boundary vertex index out of range"};
+        for (int q = nc_ptr[bv[0]]; q < nc_ptr[bv[0] + 1]; q++) {
+            int c = nc_idx[q];
+            for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+                bool all = true;
+                for (int t = 0; t < nv; t++) {
+                    bool in = false;
+                    for (int u = 0; u < fnv; u++) in = in || m.cf_v[3 * k + u] == bv[t];
+                    all = all && in;
+                }
+                if (all) bsides[i].push_back({c, k - m.cf_ptr[c]});
+            }
+        }
+    }
+    // BC rows + undefined tags
+    std::vector<int> tags = bcs.tag, types = bcs.type;
+    std::vector<double> vals = bcs.value;
+    std::vector<int> nodefine;
+    for (int i = 0; i < nbe; i++) {
+        int t = raw.btag[i];
+        bool set = std::find(tags.begin(), tags.end(), t) != tags.end() || bsides[i].size() == 2;
+        if (!set && std::find(nodefine.begin(), nodefine.end(), t) == nodefine.end()) nodefine.push_back(t);
+    }
+    for (int t : nodefine) {
+        tags.push_back(t);
+        types.push_back(1);
+        vals.push_back(0.0);
+    }
+    std::vector<int> b_row;
+    std::vector<std::vector<std::pair<int, int>>> b_sides;
+    for (int i = 0; i < nbe; i++)
+        for (int j = 0; j < (int)tags.size(); j++)
+            if (raw.btag[i] == tags[j]) {
+                if (bsides[i].size() > 2) return {-7, "boundary element shared by more than two cells"};
+                b_row.push_back(j);
+                b_sides.push_back(bsides[i]);
+            }
+    const int nbd = (int)b_row.size();
+    m.b_type.resize(nbd);
+    m.b_T.resize(nbd);
+    m.b_tag.resize(nbd);
+    m.b_connect.assign(nbd, -1);
+    m.bs_cell.assign(2 * nbd, -1);
+    m.bs_cf.assign(2 * nbd, -1);
+    for (int ib = 0; ib < nbd; ib++) {
+        m.b_type[ib] = types[b_row[ib]];
+        m.b_T[ib] = vals[b_row[ib]];
+        m.b_tag[ib] = tags[b_row[ib]];
+        for (int ic = 0; ic < (int)b_sides[ib].size(); ic++) {
+            int c = b_sides[ib][ic].first, k = m.cf_ptr[c] + b_sides[ib][ic].second;
+            m.bs_cell[2 * ib + ic] = c;
+            m.bs_cf[2 * ib + ic] = k;
+            m.cf_bound[k] = ib;
+            m.cf_bside[k] = 2 * ib + ic;
+        }
+    }
+    for (int k = 0; k < ncf; k++)
+        if (m.cf_bound[k] < 0 && m.cf_nbr[k] < 0) return {-7, "a face is neither an interior face nor on a boundary in the BC table"};
+    for (int k = 0; k < ncf; k++)
+        if (m.cf_bound[k] >= 0) m.cf_nbr[k] = m.cf_nbr[k];  // boundary faces keep their neighbour for the face list
+    // periodic partners
+    for (int ib = 0; ib < nbd; ib++) {
+        if (types[b_row[ib]] >= 0) continue;
+        double best = 1000;
+        int k0 = m.bs_cf[2 * ib];
+        if (k0 < 0) return {-7, "periodic boundary without a cell"};
+        for (int j = 0; j < nbd; j++) {
+            if (tags[b_row[ib]] != -types[b_row[j]]) continue;
+            int k1 = m.bs_cf[2 * j];
+            if (k1 < 0) continue;
+            double d1 = dist3(m.cf_fx[k0], m.cf_fy[k0], m.cf_fz[k0], m.cf_fx[k1], m.cf_fy[k1], m.cf_fz[k1]);
+            if (d1 < best) {
+                best = d1;
+                m.b_connect[ib] = j;
+            }
+        }
+        if (m.b_connect[ib] < 0) return {-7, "periodic boundary tag " + std::to_string(tags[b_row[ib]]) + " has no partner"};
+    }
+    // global face list
+    {
+        std::vector<char> done(ncf, 0);
+        for (int c = 0; c < nc; c++)
+            for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+                if (done[k]) continue;
+                int f = (int)m.f_cell0.size();
+                m.cf_face[k] = f;
+                done[k] = 1;
+                int c1 = -1, k1 = -1;
+                if (m.cf_bound[k] == -1) {
+                    int o = m.cf_nbr[k];
+                    c1 = o;
+                    for (int q = m.cf_ptr[o]; q < m.cf_ptr[o + 1]; q++)
+                        if (m.cf_nbr[q] == c && m.cf_bound[q] == -1) {
+                            k1 = q;
+                            done[q] = 1;
+                            m.cf_face[q] = f;
+                        }
+                }
+                m.f_cell0.push_back(c);
+                m.f_cf0.push_back(k);
+                m.f_cell1.push_back(c1);
+                m.f_cf1.push_back(k1);
+                m.f_bound.push_back(m.cf_bound[k]);
+            }
+    }
+    // vertex-neighbour LSQ stencil
+    m.nbr_ptr.assign(nc + 1, 0);
+    {
+        std::vector<std::vector<int>> lists(nc);
+        std::vector<int> mark(nc, -1);
+        for (int c = 0; c < nc; c++) {
+            for (int q = raw.cptr[c]; q < raw.cptr[c + 1]; q++) {
+                int vtx = raw.cverts[q];
+                for (int t = nc_ptr[vtx]; t < nc_ptr[vtx + 1]; t++) {
+                    int o = nc_idx[t];
+                    if (o != c && mark[o] != c && m.matter[o] == m.matter[c]) {
+                        mark[o] = c;
+                        lists[c].push_back(o);
+                    }
+                }
+            }
+            m.nbr_ptr[c + 1] = m.nbr_ptr[c] + (int)lists[c].size();
+        }
+        m.nbr_idx.resize(m.nbr_ptr[nc]);
+        m.lsq_w.assign(3 * (size_t)m.nbr_ptr[nc], 0.0);
+        std::vector<double> J, W;
+        for (int c = 0; c < nc; c++) {
+            int k = (int)lists[c].size();
+            std::copy(lists[c].begin(), lists[c].end(), m.nbr_idx.begin() + m.nbr_ptr[c]);
+            if (k < 3) continue;  // zero gradient (StaticBTESynthetic.cpp:1290)
+            J.assign(3 * (size_t)k, 0.0);
+            for (int j = 0; j < k; j++) {
+                int o = lists[c][j];
+                J[3 * j] = 1.0 / m.Lx * (m.cx[o] - m.cx[c]);
+                J[3 * j + 1] = 1.0 / m.Lx * (m.cy[o] - m.cy[c]);
+                J[3 * j + 2] = dim == 3 ? 1.0 / m.Lx * (m.cz[o] - m.cz[c]) : 0.0;
+            }
+            lsq_pinv(J, k, dim, W);
+            bool bad = false;
+            for (double x : W) bad = bad || !std::isfinite(x);
+            if (bad) continue;  // singular stencil: the reference's NaN check zeroes the gradient
+            for (int j = 0; j < k; j++)
+                for (int r = 0; r < dim; r++) m.lsq_w[3 * (size_t)(m.nbr_ptr[c] + j) + r] = W[r * (size_t)k + j] / m.Lx;
+        }
+    }
+    // 3D face tangential LSQ
+    if (dim == 3) {
+        const int nf = m.nf();
+        m.face_w.assign(9 * (size_t)nf, 0.0);
+        std::vector<double> J(9), W;
+        for (int f = 0; f < nf; f++) {
+            int k = m.f_cf0[f];
+            J[0] = m.cf_nx[k];
+            J[1] = m.cf_ny[k];
+            J[2] = m.cf_nz[k];
+            for (int t = 0; t < 2; t++) {
+                int a = m.cf_v[3 * k + t + 1], b = m.cf_v[3 * k + t];
+                J[3 * (t + 1)] = 1.0 / m.Lx * (m.node_x[a] - m.node_x[b]);
+                J[3 * (t + 1) + 1] = 1.0 / m.Lx * (m.node_y[a] - m.node_y[b]);
+                J[3 * (t + 1) + 2] = 1.0 / m.Lx * (m.node_z[a] - m.node_z[b]);
+            }
+            lsq_pinv(J, 3, 3, W);
+            for (int i = 0; i < 9; i++) m.face_w[9 * (size_t)f + i] = W[i];
+        }
+    }
+    // node-slot interpolation weights
+    const int M = m.nmat, nslot = nn * M;
+    {
+        std::vector<std::vector<std::pair<int, double>>> ev(nslot), tv(nslot);
+        for (int c = 0; c < nc; c++)
+            for (int q = raw.cptr[c]; q < raw.cptr[c + 1]; q++) {
+                int vtx = raw.cverts[q];
+                double ds = dist3(m.node_x[vtx], m.node_y[vtx], m.node_z[vtx], m.cx[c], m.cy[c], m.cz[c]);
+                ev[vtx * M + m.matter[c]].push_back({c, 1.0 / ds});
+                tv[vtx * M + m.matter[c]].push_back({c, 1.0 / ds});
+            }
+        for (int s = 0; s < 2 * nbd; s++) {
+            int c = m.bs_cell[s];
+            if (c < 0) continue;
+            int k = m.bs_cf[s];
+            for (int t = 0; t < fnv; t++) ev[m.cf_v[3 * k + t] * M + m.matter[c]].clear();
+        }
+        for (int s = 0; s < 2 * nbd; s++) {
+            int c = m.bs_cell[s];
+            if (c < 0) continue;
+            int k = m.bs_cf[s];
+            for (int t = 0; t < fnv; t++) {
+                int vtx = m.cf_v[3 * k + t];
+                double ds = dist3(m.node_x[vtx], m.node_y[vtx], m.node_z[vtx], m.cf_fx[k], m.cf_fy[k], m.cf_fz[k]);
+                ev[vtx * M + m.matter[c]].push_back({-1 - s, 1.0 / ds});
+            }
+        }
+        auto pack = [&](std::vector<std::vector<std::pair<int, double>>> &lst, std::vector<int> &ptr, std::vector<int> &src,
+                        std::vector<double> &w) {
+            ptr.assign(nslot + 1, 0);
+            for (int i = 0; i < nslot; i++) ptr[i + 1] = ptr[i] + (int)lst[i].size();
+            src.resize(ptr[nslot]);
+            w.resize(ptr[nslot]);
+            for (int i = 0; i < nslot; i++) {
+                double tot = 0;
+                for (auto &e : lst[i]) tot += e.second;
+                for (size_t j = 0; j < lst[i].size(); j++) {
+                    src[ptr[i] + j] = lst[i][j].first;
+                    w[ptr[i] + j] = lst[i][j].second / tot;
+                }
+            }
+        };
+        pack(ev, m.nv_ptr, m.nv_src, m.nv_w);
+        pack(tv, m.nt_ptr, m.nt_src, m.nt_w);
+    }
+    return {0, ""};
+}
+
+// Upwind level schedule per direction (Kahn's algorithm). Cell c depends on
+// interior neighbour o across face k when s_d . n_k < 0. Faces that close a
+// cycle (possible on distorted 3D tetrahedra) are lagged: the sweep treats
+// the neighbour's correction as zero, which changes only the convergence
+// rate of the defect correction, not its fixed point.
+void build_schedule(const FlatMesh &m, const Angles &a, Schedule &s, int nthreads) {
+    const int nc = m.nc, nd = a.nd;
+    s.lvl_cells.assign((size_t)nd * nc, 0);
+    std::vector<std::vector<int>> dir_ptr(nd);
+    std::vector<std::vector<uint8_t>> dir_lag(nd);
+    std::vector<int> dir_lagged(nd, 0);
+    auto work = [&](int d) {
+        std::vector<int> indeg(nc, 0), level(nc, 0);
+        std::vector<uint8_t> lag(nc, 0);
+        std::vector<int> out_ptr(nc + 1, 0), out_idx;
+        for (int c = 0; c < nc; c++)
+            for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+                if (m.cf_bound[k] != -1) continue;
+                double dp = a.sx[d] * m.cf_nx[k] + a.sy[d] * m.cf_ny[k] + a.sz[d] * m.cf_nz[k];
+                if (dp < 0) {
+                    indeg[c]++;
+                    out_ptr[m.cf_nbr[k] + 1]++;
+                }
+            }
+        for (int c = 0; c < nc; c++) out_ptr[c + 1] += out_ptr[c];
+        out_idx.resize(out_ptr[nc]);
+        {
+            std::vector<int> fill(out_ptr.begin(), out_ptr.end() - 1);
+            for (int c = 0; c < nc; c++)
+                for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+                    if (m.cf_bound[k] != -1) continue;
+                    double dp = a.sx[d] * m.cf_nx[k] + a.sy[d] * m.cf_ny[k] + a.sz[d] * m.cf_nz[k];
+                    if (dp < 0) out_idx[fill[m.cf_nbr[k]]++] = c;
+                }
+        }
+        std::vector<int> order;
+        order.reserve(nc);
+        std::vector<char> done(nc, 0);
+        std::vector<int> frontier;
+        for (int c = 0; c < nc; c++)
+            if (indeg[c] == 0) frontier.push_back(c);
+        int next_seed = 0, lagged = 0;
+        while ((int)order.size() < nc) {
+            if (frontier.empty()) {
+                // cycle: lag every not-yet-swept upwind face of the lowest pending cell
+                while (done[next_seed] || indeg[next_seed] == 0) next_seed++;
+                int c = next_seed;
+                int j = 0, lvl = 0;
+                for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++, j++) {
+                    if (m.cf_bound[k] != -1) continue;
+                    double dp = a.sx[d] * m.cf_nx[k] + a.sy[d] * m.cf_ny[k] + a.sz[d] * m.cf_nz[k];
+                    if (!(dp < 0)) continue;
+                    if (done[m.cf_nbr[k]])
+                        lvl = std::max(lvl, level[m.cf_nbr[k]] + 1);
+                    else {
+                        lag[c] |= (uint8_t)(1u << j);
+                        lagged++;
+                        indeg[c]--;
+                    }
+                }
+                level[c] = lvl;
+                frontier.push_back(c);
+                continue;
+            }
+            std::vector<int> nxt;
+            for (int c : frontier) {
+                done[c] = 1;
+                order.push_back(c);
+                for (int q = out_ptr[c]; q < out_ptr[c + 1]; q++) {
+                    int o = out_idx[q];
+                    if (done[o]) continue;
+                    level[o] = std::max(level[o], level[c] + 1);
+                    if (--indeg[o] == 0) nxt.push_back(o);
+                }
+            }
+            frontier.swap(nxt);
+        }
+        // group by level (stable within a level)
+        int nl = 0;
+        for (int c = 0; c < nc; c++) nl = std::max(nl, level[c] + 1);
+        std::vector<int> cnt(nl + 1, 0);
+        for (int c = 0; c < nc; c++) cnt[level[c] + 1]++;
+        for (int l = 0; l < nl; l++) cnt[l + 1] += cnt[l];
+        std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+        int *dst = &s.lvl_cells[(size_t)d * nc];
+        for (int c : order) dst[fill[level[c]]++] = c;
+        dir_ptr[d] = cnt;
+        dir_lag[d] = lag;
+        dir_lagged[d] = lagged;
+    };
+    nthreads = std::max(1, std::min(nthreads, nd));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthreads; t++)
+        pool.emplace_back([&, t]() {
+            for (int d = t; d < nd; d += nthreads) work(d);
+        });
+    for (auto &th : pool) th.join();
+    s.dir_lvl_off.assign(nd + 1, 0);
+    s.lvl_ptr.clear();
+    s.max_levels = 0;
+    s.lagged_faces = 0;
+    for (int d = 0; d < nd; d++) {
+        s.dir_lvl_off[d] = (int)s.lvl_ptr.size();
+        s.lvl_ptr.insert(s.lvl_ptr.end(), dir_ptr[d].begin(), dir_ptr[d].end());
+        s.max_levels = std::max(s.max_levels, (int)dir_ptr[d].size() - 1);
+        s.lagged_faces += dir_lagged[d];
+    }
+    s.dir_lvl_off[nd] = (int)s.lvl_ptr.size();
+    if (s.lagged_faces > 0) {
+        s.lag.assign((size_t)nd * nc, 0);
+        for (int d = 0; d < nd; d++) std::copy(dir_lag[d].begin(), dir_lag[d].end(), s.lag.begin() + (size_t)d * nc);
+    } else
+        s.lag.clear();
+}
+
+}  // namespace gbte

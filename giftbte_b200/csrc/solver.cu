@@ -1,0 +1,1224 @@
+// B200 (sm_100a) kernels and host driver of the steady synthetic phonon BTE.
+//
+// One outer iteration of StaticBTESynthetic::solve
+// (src/StaticBTESynthetic/StaticBTESyntheticSolver.cpp:63-218) is, for all
+// (band, direction) pairs at once (they are independent within an iteration:
+// temperatureOld is frozen by copy() and incoming boundary values are only
+// refreshed after the pair loop):
+//   k_gradient   LSQ gradient over the vertex-neighbour stencil
+//                (_get_gradient_larger, StaticBTESynthetic.cpp:1243-1424)
+//   k_residual   second-order upwind defect R(e) (_get_Re, :1427-1500)
+//   k_sweep      d = A^-1 R with A the first-order upwind operator
+//                (_get_coefficient :784-840), by a level-scheduled wavefront
+//                sweep per direction instead of a sparse LU; e += d
+//   k_bound_out  outgoing boundary values (_get_bound_ee, :1502-1539)
+//   k_moments    T, T_band, E, q (:2487-2520) plus the two moments the
+//                synthetic source needs
+//   k_remacro    the non-Fourier source (_set_vertex_energydensity,
+//                _get_face_gradient, _get_non_fourier, :1541-1937), evaluated
+//                from cell/boundary moments: every term is linear in e with
+//                band/direction weights that factor out of the face and
+//                vertex stencils, so the per-pair face pass collapses into
+//                one pass over cells per iteration
+//   k_gather     incoming boundary values by wall type (_set_bound_ee_1,
+//                :2083-2232)
+//   macro        boundary temperatures (:2234-2274), Picard loop of FP64
+//                Jacobi-preconditioned CG solves of the Fourier system
+//                (_marco_solution :2692-2734, _get_Re_macro :2307-2407)
+//   margins      (_get_magin_check_error, :2565-2611)
+// Band intensities are stored as a deviation from C_b * T_base[c]; the FP64
+// form keeps T_base = 0 (plain e), the FP32 form keeps the initial
+// temperature as base so that FP32 holds only the small deviation.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <thread>
+
+#include "solver.cuh"
+
+namespace cgrp = cooperative_groups;
+
+namespace gbte {
+
+#define CUDA_TRY(x)                                                                                \
+    do {                                                                                           \
+        cudaError_t e_ = (x);                                                                      \
+        if (e_ != cudaSuccess) return Error{-3, std::string(#x) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ size_t gtid() { return blockIdx.x * (size_t)blockDim.x + threadIdx.x; }
+__device__ __forceinline__ size_t gstride() { return (size_t)gridDim.x * blockDim.x; }
+
+int grid_for(size_t total, int threads = kThreads) {
+    size_t g = (total + threads - 1) / threads;
+    return (int)std::max<size_t>(1, std::min<size_t>(g, 148 * 64));
+}
+
+// ---------------------------------------------------------------- kernels --
+
+template <typename S>
+__global__ void k_init_eps(DMesh m, DPhys p, const double *__restrict__ T0, const double *__restrict__ Tb,
+                           S *__restrict__ eps) {
+    const size_t total = (size_t)p.nd * m.nc * p.nb;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        int b = (int)(t % p.nb);
+        int c = (int)((t / p.nb) % m.nc);
+        eps[t] = (S)(p.C[b] * T0[c] - p.C[b] * Tb[c]);
+    }
+}
+
+// g[d][c][r][b] = sum_k w_ck (eps_k - eps_c)
+template <typename S>
+__global__ void k_gradient(DMesh m, DPhys p, const S *__restrict__ eps, S *__restrict__ g) {
+    const int nb = p.nb, nc = m.nc;
+    const size_t total = (size_t)p.nd * nc * nb;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b = (int)(t % nb);
+        const size_t dc = t / nb;
+        const int c = (int)(dc % nc);
+        const S *ed = eps + (dc - c) * nb;
+        const S ec = ed[(size_t)c * nb + b];
+        S gx = 0, gy = 0, gz = 0;
+        const int q1 = m.nbr_ptr[c + 1];
+        for (int q = m.nbr_ptr[c]; q < q1; q++) {
+            const S de = ed[(size_t)m.nbr_idx[q] * nb + b] - ec;
+            gx += (S)m.lsq_w[3 * q] * de;
+            gy += (S)m.lsq_w[3 * q + 1] * de;
+            gz += (S)m.lsq_w[3 * q + 2] * de;
+        }
+        S *gp = g + dc * 3 * nb + b;
+        gp[0] = gx;
+        gp[nb] = gy;
+        gp[2 * nb] = gz;
+    }
+}
+
+template <typename S>
+struct EView {
+    const S *eps, *g;
+    const double *Tb, *gTb;
+    int nb, nc;
+    __device__ __forceinline__ double e(size_t d, int c, int b, double Cb) const {
+        return Cb * Tb[c] + (double)eps[(d * nc + c) * nb + b];
+    }
+    __device__ __forceinline__ double gdot(size_t d, int c, int b, double Cb, double rx, double ry, double rz) const {
+        const S *gp = g + (d * nc + c) * 3 * nb + b;
+        return ((double)gp[0] + Cb * gTb[3 * c]) * rx + ((double)gp[nb] + Cb * gTb[3 * c + 1]) * ry +
+               ((double)gp[2 * nb] + Cb * gTb[3 * c + 2]) * rz;
+    }
+};
+
+// R = C_b T_old + Q hr tau - e - sum_f tau (v.n) A/V x_f  (second-order upwind x_f)
+template <typename S>
+__global__ void k_residual(DMesh m, DPhys p, EView<S> ev, const double *__restrict__ Told, const double *__restrict__ eb,
+                           S *__restrict__ R) {
+    const int nb = p.nb, nc = m.nc;
+    const size_t total = (size_t)p.nd * nc * nb;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b = (int)(t % nb);
+        const size_t dc = t / nb;
+        const int c = (int)(dc % nc);
+        const size_t d = dc / nc;
+        const double Cb = p.C[b], tau = p.tau[b], vm = p.vmag[b];
+        const double vx = vm * p.sx[d], vy = vm * p.sy[d], vz = vm * p.sz[d];
+        const double ec = ev.e(d, c, b, Cb);
+        const double cx = m.cx[c], cy = m.cy[c], cz = m.cz[c], vol = m.vol[c];
+        double acc = 0;
+        for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+            const double vn = vx * m.cf_nx[k] + vy * m.cf_ny[k] + vz * m.cf_nz[k];
+            const double temp = tau * m.cf_area[k] / vol * vn;
+            double x;
+            if (vn >= 0) {
+                x = ec + ev.gdot(d, c, b, Cb, m.cf_fx[k] - cx, m.cf_fy[k] - cy, m.cf_fz[k] - cz);
+            } else if (m.cf_bound[k] < 0) {
+                const int j = m.cf_nbr[k];
+                x = ev.e(d, j, b, Cb) + ev.gdot(d, j, b, Cb, m.cf_fx[k] - m.cx[j], m.cf_fy[k] - m.cy[j], m.cf_fz[k] - m.cz[j]);
+            } else {
+                x = eb[(d * m.nbs + m.cf_bside[k]) * nb + b];
+            }
+            acc += temp * x;
+        }
+        const double r = Cb * Told[c] + m.heat[c] * p.hr[b] * tau - ec - acc;
+        R[t] = (S)r;
+    }
+}
+
+// Level-scheduled upwind sweep: one CTA per (direction, band chunk). Cells
+// of a level depend only on cells of earlier levels of the same direction,
+// so a __syncthreads between levels orders the whole sweep. R is
+// overwritten in place by the correction d, and eps += d.
+template <typename S>
+__global__ void __launch_bounds__(256) k_sweep(DMesh m, DPhys p, int nbc, const int *__restrict__ lvl_cells,
+                                               const int *__restrict__ lvl_ptr, const int *__restrict__ dir_lvl_off,
+                                               const unsigned char *__restrict__ lag, S *R, S *eps) {
+    const int nb = p.nb, nc = m.nc;
+    const int nchunks = (nb + nbc - 1) / nbc;
+    const int d = blockIdx.x / nchunks, chunk = blockIdx.x % nchunks;
+    const int b0 = chunk * nbc, nbl = min(nbc, nb - b0);
+    const double sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
+    const int *cells = lvl_cells + (size_t)d * nc;
+    const int *lp = lvl_ptr + dir_lvl_off[d];
+    const int nlev = dir_lvl_off[d + 1] - dir_lvl_off[d] - 1;
+    S *Rd = R + (size_t)d * nc * nb;
+    S *ed = eps + (size_t)d * nc * nb;
+    for (int l = 0; l < nlev; l++) {
+        const int c0 = lp[l], items = (lp[l + 1] - c0) * nbl;
+        for (int t = threadIdx.x; t < items; t += blockDim.x) {
+            const int c = cells[c0 + t / nbl];
+            const int b = b0 + t % nbl;
+            const double kb = p.tau[b] * p.vmag[b];
+            const double vol = m.vol[c];
+            const unsigned lm = lag ? lag[(size_t)d * nc + c] : 0u;
+            S acc = Rd[(size_t)c * nb + b];
+            double sig = 0;
+            int j = 0;
+            for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++, j++) {
+                const double dpn = sx * m.cf_nx[k] + sy * m.cf_ny[k] + sz * m.cf_nz[k];
+                const double a = m.cf_area[k] / vol * dpn;
+                if (dpn >= 0)
+                    sig += a;
+                else if (m.cf_bound[k] < 0 && !((lm >> j) & 1u))
+                    acc -= (S)(kb * a) * Rd[(size_t)m.cf_nbr[k] * nb + b];
+            }
+            const S dl = acc / (S)(1.0 + kb * sig);
+            Rd[(size_t)c * nb + b] = dl;
+            ed[(size_t)c * nb + b] += dl;
+        }
+        __syncthreads();
+    }
+}
+
+// outgoing boundary values: e_c(new) + g_c(pre-sweep) . (x_f - x_c)
+template <typename S>
+__global__ void k_bound_out(DMesh m, DPhys p, EView<S> ev, double *__restrict__ eb) {
+    const int nb = p.nb;
+    const size_t total = (size_t)p.nd * m.nbs * nb;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b = (int)(t % nb);
+        const int s = (int)((t / nb) % m.nbs);
+        const size_t d = t / ((size_t)nb * m.nbs);
+        const int c = m.bs_cell[s];
+        if (c < 0) continue;
+        const int k = m.bs_cf[s];
+        const double vm = p.vmag[b];
+        const double vn = vm * p.sx[d] * m.cf_nx[k] + vm * p.sy[d] * m.cf_ny[k] + vm * p.sz[d] * m.cf_nz[k];
+        if (vn >= 0) {
+            const double Cb = p.C[b];
+            eb[t] = ev.e(d, c, b, Cb) +
+                    ev.gdot(d, c, b, Cb, m.cf_fx[k] - m.cx[c], m.cf_fy[k] - m.cy[c], m.cf_fz[k] - m.cz[c]);
+        }
+    }
+}
+
+// Per-cell moments over all (b, d). LPC lanes cooperate on one cell.
+//   Tlat = sum lat w e / C          (temperature, :2493)
+//   Tband[b] = sum_d w e / C        (:2494)
+//   E = sum w e / C_bulk             (:2504)
+//   q = sum v w e                    (:2515-2517)
+//   Th = kappa sum_{hr>0} lat w e / C        (Fourier part of the source)
+//   Q  = sum_{hr>0} w tau v v^T e  (xx xy xz yy yz zz)
+template <typename S, int LPC>
+__global__ void k_moments(DMesh m, DPhys p, const S *__restrict__ eps, const double *__restrict__ Tb,
+                          double *__restrict__ Tlat, double *__restrict__ E, double *__restrict__ q,
+                          double *__restrict__ Tband, double *__restrict__ Th, double *__restrict__ Q) {
+    const int nb = p.nb, nc = m.nc;
+    const int lane = threadIdx.x % LPC;
+    const size_t cell = gtid() / LPC;
+    const bool active = cell < (size_t)nc;
+    const int c = active ? (int)cell : 0;
+    double tl = 0, en = 0, qx = 0, qy = 0, qz = 0, th = 0, q6[6] = {0, 0, 0, 0, 0, 0};
+    if (active) {
+        const double tbc = Tb[c];
+        for (int b = lane; b < nb; b += LPC) {
+            const double Cb = p.C[b], lat = p.lat[b], vm = p.vmag[b];
+            const bool hrp = p.hr[b] > 0;
+            const double wtv = p.tau[b] * vm * vm;
+            const double base = Cb * tbc;
+            double tb = 0, tlb = 0, enb = 0, qxb = 0, qyb = 0, qzb = 0;
+            double qq[6] = {0, 0, 0, 0, 0, 0};
+            for (int d = 0; d < p.nd; d++) {
+                const double e = base + (double)eps[((size_t)d * nc + c) * nb + b];
+                const double w = p.w[d];
+                tlb += lat * e * w / Cb;
+                tb += e * w / Cb;
+                enb += e * w / p.capb;
+                const double sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
+                qxb += vm * sx * w * e;
+                qyb += vm * sy * w * e;
+                qzb += vm * sz * w * e;
+                if (hrp) {
+                    const double f = w * wtv * e;
+                    qq[0] += f * sx * sx;
+                    qq[1] += f * sx * sy;
+                    qq[2] += f * sx * sz;
+                    qq[3] += f * sy * sy;
+                    qq[4] += f * sy * sz;
+                    qq[5] += f * sz * sz;
+                }
+            }
+            Tband[(size_t)b * nc + c] = tb;
+            tl += tlb;
+            en += enb;
+            qx += qxb;
+            qy += qyb;
+            qz += qzb;
+            if (hrp) {
+                th += tlb;
+                for (int i = 0; i < 6; i++) q6[i] += qq[i];
+            }
+        }
+    }
+    if (LPC > 1) {
+#pragma unroll
+        for (int off = LPC / 2; off > 0; off >>= 1) {
+            tl += __shfl_down_sync(0xffffffffu, tl, off, LPC);
+            en += __shfl_down_sync(0xffffffffu, en, off, LPC);
+            qx += __shfl_down_sync(0xffffffffu, qx, off, LPC);
+            qy += __shfl_down_sync(0xffffffffu, qy, off, LPC);
+            qz += __shfl_down_sync(0xffffffffu, qz, off, LPC);
+            th += __shfl_down_sync(0xffffffffu, th, off, LPC);
+#pragma unroll
+            for (int i = 0; i < 6; i++) q6[i] += __shfl_down_sync(0xffffffffu, q6[i], off, LPC);
+        }
+    }
+    if (active && lane == 0) {
+        Tlat[c] = tl;
+        E[c] = en;
+        q[3 * c] = qx;
+        q[3 * c + 1] = qy;
+        q[3 * c + 2] = qz;
+        Th[c] = p.kappa * th;
+        for (int i = 0; i < 6; i++) Q[6 * c + i] = q6[i];
+    }
+}
+
+// Th/Q moments of the boundary values (before the incoming gather, as the
+// reference evaluates its face gradients inside the pair loop).
+__global__ void k_side_moments(DMesh m, DPhys p, const double *__restrict__ eb, double *__restrict__ Ths,
+                               double *__restrict__ Qs) {
+    const int s = (int)gtid();
+    if (s >= m.nbs) return;
+    double th = 0, q6[6] = {0, 0, 0, 0, 0, 0};
+    if (m.bs_cell[s] >= 0) {
+        for (int d = 0; d < p.nd; d++) {
+            const double w = p.w[d], sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
+            const double *e = eb + ((size_t)d * m.nbs + s) * p.nb;
+            for (int b = 0; b < p.nb; b++) {
+                if (!(p.hr[b] > 0)) continue;
+                const double x = e[b];
+                th += p.lat[b] * x * w / p.C[b];
+                const double f = w * p.tau[b] * p.vmag[b] * p.vmag[b] * x;
+                q6[0] += f * sx * sx;
+                q6[1] += f * sx * sy;
+                q6[2] += f * sx * sz;
+                q6[3] += f * sy * sy;
+                q6[4] += f * sy * sz;
+                q6[5] += f * sz * sz;
+            }
+        }
+    }
+    Ths[s] = p.kappa * th;
+    for (int i = 0; i < 6; i++) Qs[6 * s + i] = q6[i];
+}
+
+// inverse-distance node values of (Th, Q) with boundary-side override
+__global__ void k_node_interp(DMesh m, const double *__restrict__ Th, const double *__restrict__ Q,
+                              const double *__restrict__ Ths, const double *__restrict__ Qs, double *__restrict__ ThV,
+                              double *__restrict__ QV) {
+    const int i = (int)gtid();
+    if (i >= m.nslot) return;
+    double th = 0, q6[6] = {0, 0, 0, 0, 0, 0};
+    for (int k = m.nv_ptr[i]; k < m.nv_ptr[i + 1]; k++) {
+        const int src = m.nv_src[k];
+        const double w = m.nv_w[k];
+        if (src >= 0) {
+            th += w * Th[src];
+            for (int j = 0; j < 6; j++) q6[j] += w * Q[6 * src + j];
+        } else {
+            const int s = -1 - src;
+            th += w * Ths[s];
+            for (int j = 0; j < 6; j++) q6[j] += w * Qs[6 * s + j];
+        }
+    }
+    ThV[i] = th;
+    for (int j = 0; j < 6; j++) QV[6 * i + j] = q6[j];
+}
+
+__device__ __forceinline__ void symv(const double *q, double x, double y, double z, double &ox, double &oy, double &oz) {
+    ox = q[0] * x + q[1] * y + q[2] * z;
+    oy = q[1] * x + q[3] * y + q[4] * z;
+    oz = q[2] * x + q[4] * y + q[5] * z;
+}
+
+// tangential gradient on face k of cell c of a node field (vals, stride st)
+__device__ __forceinline__ void tangential(const DMesh &m, int c, int k, const double *vals, int stride, int comp,
+                                           bool use_slot, double &tx, double &ty, double &tz) {
+    if (m.dim == 2) {
+        const int v0 = m.cf_v[3 * k], v1 = m.cf_v[3 * k + 1];
+        const double mx = m.node_x[v1] - m.node_x[v0], my = m.node_y[v1] - m.node_y[v0];
+        const double dv = vals[(size_t)v1 * stride + comp] - vals[(size_t)v0 * stride + comp];
+        tx = dv / (mx * mx + my * my) * mx;
+        ty = dv / (mx * mx + my * my) * my;
+        tz = 0;
+    } else {
+        const int f = m.cf_face[k];
+        const int k0 = m.f_cf0[f];
+        const double *W = m.face_w + 9 * (size_t)f;
+        double d1[3] = {0, 0, 0};
+        for (int t = 0; t < 2; t++) {
+            const int a = m.cf_v[3 * k0 + t + 1], b = m.cf_v[3 * k0 + t];
+            d1[t + 1] = m.inv_Lx * (vals[(size_t)a * stride + comp] - vals[(size_t)b * stride + comp]);
+        }
+        tx = W[0] * d1[0] + W[1] * d1[1] + W[2] * d1[2];
+        ty = W[3] * d1[0] + W[4] * d1[1] + W[5] * d1[2];
+        tz = W[6] * d1[0] + W[7] * d1[1] + W[8] * d1[2];
+    }
+}
+
+// Non-Fourier synthetic source from moments:
+//   ReMacro_c = sum_faces A [ -n . (Q-weighted face gradient) + n . (Th face gradient) ]
+// with face gradient G(X) = alpha (X_nb - X_c) n + tangential(X at nodes).
+__global__ void k_remacro(DMesh m, const double *__restrict__ Th, const double *__restrict__ Q,
+                          const double *__restrict__ Ths, const double *__restrict__ Qs, const double *__restrict__ ThV,
+                          const double *__restrict__ QV, double *__restrict__ remacro) {
+    const int c = (int)gtid();
+    if (c >= m.nc) return;
+    double acc = 0;
+    for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+        const double nx = m.cf_nx[k], ny = m.cf_ny[k], nz = m.cf_nz[k], A = m.cf_area[k];
+        double rx, ry, rz, thn, qn[6];
+        const int bnd = m.cf_bound[k];
+        if (bnd < 0) {
+            const int j = m.cf_nbr[k];
+            rx = m.cx[j] - m.cx[c];
+            ry = m.cy[j] - m.cy[c];
+            rz = m.cz[j] - m.cz[c];
+            thn = Th[j];
+            for (int i = 0; i < 6; i++) qn[i] = Q[6 * j + i];
+        } else {
+            if (m.b_type[bnd] == 3) continue;
+            const int s = m.cf_bside[k];
+            rx = m.cf_fx[k] - m.cx[c];
+            ry = m.cf_fy[k] - m.cy[c];
+            rz = m.cf_fz[k] - m.cz[c];
+            thn = Ths[s];
+            for (int i = 0; i < 6; i++) qn[i] = Qs[6 * s + i];
+        }
+        const double alpha = (rx * nx + ry * ny + rz * nz) / (rx * rx + ry * ry + rz * rz);
+        // Fourier part: n . (alpha dTh n + tangential)
+        double tx, ty, tz;
+        tangential(m, c, k, ThV, 1, 0, true, tx, ty, tz);
+        const double nn = nx * nx + ny * ny + nz * nz;
+        double four = alpha * (thn - Th[c]) * nn + (nx * tx + ny * ty + nz * tz);
+        // BTE part: n . [alpha (Q_nb - Q_c) n + (QV_v1 - QV_v0) tangential]
+        double dq[6];
+        for (int i = 0; i < 6; i++) dq[i] = qn[i] - Q[6 * c + i];
+        double gx, gy, gz;
+        symv(dq, nx, ny, nz, gx, gy, gz);
+        double bte = alpha * (nx * gx + ny * gy + nz * gz);
+        // tangential part of the tensor moment: n^T QV t-hat per component
+        double tq[6][3];
+        for (int i = 0; i < 6; i++) tangential(m, c, k, QV, 6, i, true, tq[i][0], tq[i][1], tq[i][2]);
+        // n^T [sum_i comp_i(QV) tangent_i]: the tangential gradient of the
+        // tensor field contracted with n on the left and the gradient index
+        // on the right: sum_{a,b} n_a (dQ_ab/dx_t) ... evaluated as
+        // n_a * T_ab where T_ab = tangential gradient of Q_ab along b.
+        const double tan_q = nx * (tq[0][0] + tq[1][1] + tq[2][2]) + ny * (tq[1][0] + tq[3][1] + tq[4][2]) +
+                             nz * (tq[2][0] + tq[4][1] + tq[5][2]);
+        bte += tan_q;
+        acc += A * (four - bte);
+    }
+    remacro[c] = acc;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// incoming boundary values by wall type; reads only outgoing entries (or a
+// snapshot for chained specular sources), writes only incoming entries
+__global__ void k_gather(DMesh m, DPhys p, const double *__restrict__ dif_w, const int *__restrict__ spec_src,
+                         const double *__restrict__ snap, double *eb) {
+    const int nb = p.nb;
+    const size_t total = (size_t)p.nd * m.nbs * nb;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b = (int)(t % nb);
+        const int s = (int)((t / nb) % m.nbs);
+        const int d = (int)(t / ((size_t)nb * m.nbs));
+        const int c = m.bs_cell[s];
+        if (c < 0 || p.hr[b] == 0) continue;
+        const int k = m.bs_cf[s];
+        const double vm = p.vmag[b];
+        const double vn = vm * p.sx[d] * m.cf_nx[k] + vm * p.sy[d] * m.cf_ny[k] + vm * p.sz[d] * m.cf_nz[k];
+        if (!(vn < 0)) continue;
+        const int ib = s >> 1;
+        const int type = m.b_type[ib];
+        double val;
+        if (type == 1) {
+            val = p.C[b] * m.b_T[ib];
+        } else if (type == 2) {
+            double acc = 0;
+            const double *w = dif_w + (size_t)s * p.nd;
+            for (int q = 0; q < p.nd; q++) {
+                const double wq = w[q];
+                if (wq != 0) acc += wq * eb[((size_t)q * m.nbs + s) * nb + b];
+            }
+            val = acc;
+        } else if (type == 3) {
+            const int src = spec_src[(size_t)s * p.nd + d];
+            const double *from = snap ? snap : eb;
+            val = from[((size_t)src * m.nbs + s) * nb + b];
+        } else if (type < 0) {
+            const int cb = m.b_connect[ib];
+            const int ps = 2 * cb + (s & 1);
+            val = eb[((size_t)d * m.nbs + ps) * nb + b] + p.C[b] * (m.b_T[ib] - m.b_T[cb]);
+        } else {
+            continue;
+        }
+        eb[t] = val;
+    }
+}
+
+// macro boundary temperatures sum lat e w / C with periodic overrides
+__global__ void k_macro_bc(DMesh m, DPhys p, const double *__restrict__ eb, const double *__restrict__ ovr,
+                           double *__restrict__ bTm) {
+    const int s = (int)gtid();
+    if (s >= m.nbs) return;
+    double acc = 0;
+    if (m.bs_cell[s] >= 0) {
+        for (int b = 0; b < p.nb; b++) {
+            const double lc = p.lat[b];
+            const double Cb = p.C[b];
+            for (int d = 0; d < p.nd; d++) acc += lc * eb[((size_t)d * m.nbs + s) * p.nb + b] / Cb * p.w[d];
+        }
+    }
+    const double o = ovr[s];
+    bTm[s] = (o == o) ? o : acc;
+}
+
+// cell-only inverse-distance node temperatures
+__global__ void k_tinterp(DMesh m, const double *__restrict__ T, double *__restrict__ TV) {
+    const int i = (int)gtid();
+    if (i >= m.nslot) return;
+    double acc = 0;
+    for (int k = m.nt_ptr[i]; k < m.nt_ptr[i + 1]; k++) acc += m.nt_w[k] * T[m.nt_src[k]];
+    TV[i] = acc;
+}
+
+// macro right-hand side (negated for the SPD form -K T = -rhs)
+__global__ void k_macro_rhs(DMesh m, double kappa, const double *__restrict__ remacro, const double *__restrict__ bTm,
+                            const double *__restrict__ TV, double *__restrict__ rhs_neg) {
+    const int c = (int)gtid();
+    if (c >= m.nc) return;
+    double r = remacro[c] - m.heat[c] * m.vol[c];
+    for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+        const double nx = m.cf_nx[k], ny = m.cf_ny[k], nz = m.cf_nz[k], A = m.cf_area[k];
+        const int bnd = m.cf_bound[k];
+        double ax, ay, az;
+        if (bnd >= 0) {
+            if (m.b_type[bnd] == 3) continue;
+            ax = m.cf_fx[k] - m.cx[c];
+            ay = m.cf_fy[k] - m.cy[c];
+            az = m.cf_fz[k] - m.cz[c];
+            const double temp = kappa * A / (nx * ax + ny * ay + nz * az);
+            r += -temp * bTm[m.cf_bside[k]];
+        } else {
+            const int j = m.cf_nbr[k];
+            ax = m.cx[j] - m.cx[c];
+            ay = m.cy[j] - m.cy[c];
+            az = m.cz[j] - m.cz[c];
+        }
+        const double an = ax * nx + ay * ny + az * nz;
+        const double a2x = nx - ax / an, a2y = ny - ay / an, a2z = nz - az / an;
+        double gx, gy, gz;
+        if (m.dim == 2) {
+            tangential(m, c, k, TV, 1, 0, true, gx, gy, gz);
+        } else {
+            // the reference accumulates onto the centre-offset vector here
+            // (StaticBTESynthetic.cpp:2368-2370); reproduced as written
+            tangential(m, c, k, TV, 1, 0, true, gx, gy, gz);
+            gx += ax;
+            gy += ay;
+            gz += az;
+        }
+        r -= kappa * A * (a2x * gx + a2y * gy + a2z * gz);
+    }
+    rhs_neg[c] = -r;
+}
+
+__global__ void k_copy(const double *__restrict__ a, double *__restrict__ b, int n) {
+    const int i = (int)gtid();
+    if (i < n) b[i] = a[i];
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(double *addr, double v) {
+    atomicMax(reinterpret_cast<unsigned long long *>(addr), __double_as_longlong(v));
+}
+
+// margins: out = {max|T|, sum|T-Told|, max|q|, sum||q|-|qold||, sum (T1-T)^2}
+__global__ void k_margins(int n, const double *__restrict__ T, const double *__restrict__ Told,
+                          const double *__restrict__ q, const double *__restrict__ qold, double *out) {
+    double tmax = 0, s1 = 0, hmax = 0, s2 = 0;
+    for (size_t i = gtid(); i < (size_t)n; i += gstride()) {
+        tmax = fmax(tmax, fabs(T[i]));
+        s1 += sqrt(pow(T[i] - Told[i], 2));
+        const double h = sqrt(pow(q[3 * i], 2) + pow(q[3 * i + 1], 2) + pow(q[3 * i + 2], 2));
+        const double h1 = sqrt(pow(qold[3 * i], 2) + pow(qold[3 * i + 1], 2) + pow(qold[3 * i + 2], 2));
+        hmax = fmax(hmax, h);
+        s2 += fabs(h - h1);
+    }
+    __shared__ double sh[4][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        tmax = fmax(tmax, __shfl_down_sync(0xffffffffu, tmax, o));
+        hmax = fmax(hmax, __shfl_down_sync(0xffffffffu, hmax, o));
+        s1 += __shfl_down_sync(0xffffffffu, s1, o);
+        s2 += __shfl_down_sync(0xffffffffu, s2, o);
+    }
+    if (lane == 0) {
+        sh[0][wid] = tmax;
+        sh[1][wid] = s1;
+        sh[2][wid] = hmax;
+        sh[3][wid] = s2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
+            tmax = fmax(tmax, sh[0][w]);
+            s1 += sh[1][w];
+            hmax = fmax(hmax, sh[2][w]);
+            s2 += sh[3][w];
+        }
+        atomic_max_nonneg(&out[0], tmax);
+        atomicAdd(&out[1], s1);
+        atomic_max_nonneg(&out[2], hmax);
+        atomicAdd(&out[3], s2);
+    }
+}
+
+__global__ void k_sqdiff(int n, const double *__restrict__ a, const double *__restrict__ b, double *out) {
+    double s = 0;
+    for (size_t i = gtid(); i < (size_t)n; i += gstride()) s += pow(a[i] - b[i], 2);
+    __shared__ double sh[32];
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) s += sh[w];
+        atomicAdd(out, s);
+    }
+}
+
+// Jacobi-preconditioned CG on the negated (SPD) macro matrix, one
+// cooperative launch for the whole solve. Each grid-wide dot product uses a
+// fresh pre-zeroed slot of `scal`, so no slot is reused within a launch.
+__device__ double grid_dot_add(cgrp::grid_group &grid, double v, double *slot) {
+    __shared__ double sh[32];
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += sh[w];
+        atomicAdd(slot, s);
+    }
+    grid.sync();
+    const double r = *(volatile double *)slot;
+    __syncthreads();
+    return r;
+}
+
+__global__ void k_pcg(int n, const int *__restrict__ ptr, const int *__restrict__ idx, const double *__restrict__ val,
+                      const double *__restrict__ dinv, const double *__restrict__ bvec, double *__restrict__ x,
+                      double *__restrict__ r, double *__restrict__ z, double *__restrict__ p, double *__restrict__ Ap,
+                      double *scal, double rtol, int maxit, int nslots) {
+    cgrp::grid_group grid = cgrp::this_grid();
+    const size_t i0 = gtid(), st = gstride();
+    int slot = 0;
+    // r = b - A x, z = D^-1 r, p = z
+    double rz = 0, bb = 0;
+    for (size_t i = i0; i < (size_t)n; i += st) {
+        double ax = 0;
+        for (int k = ptr[i]; k < ptr[i + 1]; k++) ax += val[k] * x[idx[k]];
+        const double ri = bvec[i] - ax;
+        r[i] = ri;
+        const double zi = dinv[i] * ri;
+        z[i] = zi;
+        p[i] = zi;
+        rz += ri * zi;
+        bb += bvec[i] * bvec[i];
+    }
+    rz = grid_dot_add(grid, rz, &scal[slot++]);
+    bb = grid_dot_add(grid, bb, &scal[slot++]);
+    const double thr = rtol * rtol * bb;
+    int it = 0;
+    double rr = rz;
+    // initial residual check
+    {
+        double v = 0;
+        for (size_t i = i0; i < (size_t)n; i += st) v += r[i] * r[i];
+        rr = grid_dot_add(grid, v, &scal[slot++]);
+    }
+    while (it < maxit && rr > thr && slot + 3 < nslots) {
+        double pap = 0;
+        for (size_t i = i0; i < (size_t)n; i += st) {
+            double s = 0;
+            for (int k = ptr[i]; k < ptr[i + 1]; k++) s += val[k] * p[idx[k]];
+            Ap[i] = s;
+            pap += p[i] * s;
+        }
+        pap = grid_dot_add(grid, pap, &scal[slot++]);
+        const double alpha = rz / pap;
+        double rzn = 0, rrn = 0;
+        for (size_t i = i0; i < (size_t)n; i += st) {
+            x[i] += alpha * p[i];
+            const double ri = r[i] - alpha * Ap[i];
+            r[i] = ri;
+            const double zi = dinv[i] * ri;
+            z[i] = zi;
+            rzn += ri * zi;
+            rrn += ri * ri;
+        }
+        rzn = grid_dot_add(grid, rzn, &scal[slot++]);
+        rrn = grid_dot_add(grid, rrn, &scal[slot++]);
+        const double beta = rzn / rz;
+        rz = rzn;
+        rr = rrn;
+        for (size_t i = i0; i < (size_t)n; i += st) p[i] = z[i] + beta * p[i];
+        grid.sync();
+        it++;
+    }
+    if (i0 == 0) scal[nslots - 1] = (double)it;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- host side --
+
+void *Solver::dalloc(size_t bytes) {
+    void *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    allocs_.push_back(p);
+    return p;
+}
+
+Solver::~Solver() {
+    if (cfg.device >= 0) cudaSetDevice(cfg.device);
+    if (cfg.stream) cudaStreamSynchronize(cfg.stream);
+    for (void *p : allocs_) cudaFree(p);
+    if (h_pinned_) cudaFreeHost(h_pinned_);
+    for (auto &e : ev_)
+        if (e) cudaEventDestroy(e);
+    if (cfg.own_stream && cfg.stream) cudaStreamDestroy(cfg.stream);
+}
+
+template <typename T>
+static T *upload(Solver *, std::vector<void *> &allocs, const std::vector<T> &v, cudaStream_t s, bool &ok) {
+    size_t bytes = std::max<size_t>(16, v.size() * sizeof(T));
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        ok = false;
+        return nullptr;
+    }
+    allocs.push_back(p);
+    if (!v.empty() && cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s) != cudaSuccess) ok = false;
+    return (T *)p;
+}
+
+Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std::vector<double> &cell_heat,
+                   const SolverConfig &c) {
+    mesh = m;
+    bands = b;
+    ang = a;
+    cfg = c;
+    if (bands.nmat != 1)
+        return {-8, "more than one material is not supported by this solver (interfaces between materials)"};
+    if (cfg.use_limiter) return {-8, "Order=2limit (gradient limiter) is not supported by this solver"};
+    for (int t : mesh.b_type)
+        if (!(t == 1 || t == 2 || t == 3 || t < 0)) return {-8, "boundary type " + std::to_string(t) + " is not supported"};
+    int ndev = 0;
+    CUDA_TRY(cudaGetDeviceCount(&ndev));
+    if (cfg.device < 0 || cfg.device >= ndev) return {-1, "CUDA device ordinal out of range"};
+    CUDA_TRY(cudaSetDevice(cfg.device));
+    if (!cfg.stream) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&cfg.stream, cudaStreamNonBlocking));
+        cfg.own_stream = true;
+    }
+    for (auto &e : ev_) CUDA_TRY(cudaEventCreate(&e));
+    cudaStream_t s = cfg.stream;
+    build_schedule(mesh, ang, sched, (int)std::max(1u, std::thread::hardware_concurrency()));
+
+    bool ok = true;
+    auto up_d = [&](const std::vector<double> &v) { return upload(this, allocs_, v, s, ok); };
+    auto up_i = [&](const std::vector<int> &v) { return upload(this, allocs_, v, s, ok); };
+    DMesh &d = dm_;
+    d.dim = mesh.dim;
+    d.nc = mesh.nc;
+    d.nn = mesh.nn;
+    d.nbs = mesh.nbs();
+    d.nbd = mesh.nbd();
+    d.nslot = mesh.nn * mesh.nmat;
+    d.ncf = mesh.ncf();
+    d.nf = mesh.nf();
+    d.inv_Lx = 1.0 / mesh.Lx;
+    d.cf_ptr = up_i(mesh.cf_ptr);
+    d.cf_nbr = up_i(mesh.cf_nbr);
+    d.cf_bside = up_i(mesh.cf_bside);
+    d.cf_bound = up_i(mesh.cf_bound);
+    d.cf_v = up_i(mesh.cf_v);
+    d.cf_face = up_i(mesh.cf_face);
+    d.cf_area = up_d(mesh.cf_area);
+    d.cf_nx = up_d(mesh.cf_nx);
+    d.cf_ny = up_d(mesh.cf_ny);
+    d.cf_nz = up_d(mesh.cf_nz);
+    d.cf_fx = up_d(mesh.cf_fx);
+    d.cf_fy = up_d(mesh.cf_fy);
+    d.cf_fz = up_d(mesh.cf_fz);
+    d.vol = up_d(mesh.vol);
+    d.cx = up_d(mesh.cx);
+    d.cy = up_d(mesh.cy);
+    d.cz = up_d(mesh.cz);
+    std::vector<double> heat = cell_heat;
+    heat.resize(mesh.nc, 0.0);
+    d.heat = up_d(heat);
+    d.nbr_ptr = up_i(mesh.nbr_ptr);
+    d.nbr_idx = up_i(mesh.nbr_idx);
+    d.lsq_w = up_d(mesh.lsq_w);
+    d.face_w = up_d(mesh.face_w);
+    d.f_cf0 = up_i(mesh.f_cf0);
+    d.b_type = up_i(mesh.b_type);
+    d.b_connect = up_i(mesh.b_connect);
+    d.b_T = up_d(mesh.b_T);
+    d.bs_cell = up_i(mesh.bs_cell);
+    d.bs_cf = up_i(mesh.bs_cf);
+    d.nv_ptr = up_i(mesh.nv_ptr);
+    d.nv_src = up_i(mesh.nv_src);
+    d.nv_w = up_d(mesh.nv_w);
+    d.nt_ptr = up_i(mesh.nt_ptr);
+    d.nt_src = up_i(mesh.nt_src);
+    d.nt_w = up_d(mesh.nt_w);
+    d.node_x = up_d(mesh.node_x);
+    d.node_y = up_d(mesh.node_y);
+    d.node_z = up_d(mesh.node_z);
+
+    const int nb = bands.nb, nd = ang.nd;
+    DPhys &p = dp_;
+    p.nb = nb;
+    p.nd = nd;
+    p.vmag = up_d(std::vector<double>(bands.v.begin(), bands.v.begin() + nb));
+    p.tau = up_d(std::vector<double>(bands.tau.begin(), bands.tau.begin() + nb));
+    p.C = up_d(std::vector<double>(bands.C.begin(), bands.C.begin() + nb));
+    p.lat = up_d(std::vector<double>(bands.lat.begin(), bands.lat.begin() + nb));
+    p.hr = up_d(std::vector<double>(bands.hr.begin(), bands.hr.begin() + nb));
+    p.kappa = bands.kappa[0];
+    p.capb = bands.capb[0];
+    p.sx = up_d(ang.sx);
+    p.sy = up_d(ang.sy);
+    p.sz = up_d(ang.sz);
+    p.w = up_d(ang.w);
+
+    // schedule
+    lvl_cells_ = up_i(sched.lvl_cells);
+    lvl_ptr_ = up_i(sched.lvl_ptr);
+    dir_lvl_off_ = up_i(sched.dir_lvl_off);
+    if (!sched.lag.empty()) {
+        void *pl = dalloc(sched.lag.size());
+        if (!pl) return {-6, "device allocation failed (lag mask)"};
+        CUDA_TRY(cudaMemcpyAsync(pl, sched.lag.data(), sched.lag.size(), cudaMemcpyHostToDevice, s));
+        lag_ = (unsigned char *)pl;
+    }
+
+    // diffuse weights and specular sources per (side, direction)
+    const int nbs = mesh.nbs();
+    std::vector<double> difw((size_t)nbs * nd, 0.0);
+    std::vector<int> spec((size_t)nbs * nd, 0);
+    need_snapshot_ = false;
+    for (int sd = 0; sd < nbs; sd++) {
+        int cc = mesh.bs_cell[sd];
+        if (cc < 0) continue;
+        int k = mesh.bs_cf[sd];
+        int type = mesh.b_type[sd >> 1];
+        double nx = mesh.cf_nx[k], ny = mesh.cf_ny[k], nz = mesh.cf_nz[k];
+        if (type == 2) {
+            double tot = 0;
+            for (int q = 0; q < nd; q++) {
+                double dn = ang.sx[q] * nx + ang.sy[q] * ny + ang.sz[q] * nz;
+                if (dn >= 0) tot += dn * ang.w[q];
+            }
+            for (int q = 0; q < nd; q++) {
+                double dn = ang.sx[q] * nx + ang.sy[q] * ny + ang.sz[q] * nz;
+                if (dn >= 0) difw[(size_t)sd * nd + q] = dn * ang.w[q] / tot;
+            }
+        } else if (type == 3) {
+            std::vector<int> res(nd, -1);
+            std::vector<char> old_incoming(nd, 0);
+            for (int q = 0; q < nd; q++) {
+                double d1 = ang.sx[q] * nx + ang.sy[q] * ny + ang.sz[q] * nz;
+                double rx = ang.sx[q] - nx * d1 * 2, ry = ang.sy[q] - ny * d1 * 2, rz = ang.sz[q] - nz * d1 * 2;
+                double close = 1;
+                int nf = -1;
+                for (int t = 0; t < nd; t++) {
+                    double l = std::sqrt(std::pow(rx - ang.sx[t], 2) + std::pow(ry - ang.sy[t], 2) + std::pow(rz - ang.sz[t], 2));
+                    if (l < close) {
+                        nf = t;
+                        close = l;
+                    }
+                }
+                if (nf < 0) return {-8, "specular wall: no quadrature direction near the mirror direction"};
+                bool q_in = d1 < 0;
+                if (!q_in) {
+                    res[q] = q;  // outgoing entries are never rewritten
+                    continue;
+                }
+                double dnf = ang.sx[nf] * nx + ang.sy[nf] * ny + ang.sz[nf] * nz;
+                if (dnf >= 0)
+                    res[q] = nf;
+                else if (nf < q) {  // already rewritten earlier in the sequential order
+                    res[q] = res[nf];
+                    old_incoming[q] = old_incoming[nf];
+                } else {
+                    res[q] = nf;
+                    old_incoming[q] = 1;
+                }
+                if (old_incoming[q]) need_snapshot_ = true;
+            }
+            for (int q = 0; q < nd; q++) spec[(size_t)sd * nd + q] = res[q];
+        }
+    }
+    dif_w_ = up_d(difw);
+    spec_src_ = up_i(spec);
+    // periodic macro-temperature overrides (StaticBTESynthetic.cpp:2258-2273)
+    std::vector<double> ovr(nbs, std::numeric_limits<double>::quiet_NaN());
+    for (int ib = 0; ib < mesh.nbd(); ib++)
+        for (int ic = 0; ic < 2; ic++) {
+            if (mesh.bs_cell[2 * ib + ic] < 0) continue;
+            if (mesh.b_type[ib] < 0 && mesh.b_T[ib] > 0) {
+                ovr[2 * ib + ic] = mesh.b_T[ib] / 2;
+                ovr[2 * mesh.b_connect[ib] + ic] = -mesh.b_T[ib] / 2;
+            }
+        }
+    bTovr_ = up_d(ovr);
+    // macro matrix (_get_coefficient_macro, :842-884), stored negated
+    {
+        const double kap = bands.kappa[0];
+        std::vector<int> ptr(mesh.nc + 1, 0), idx;
+        std::vector<double> val, dinv(mesh.nc);
+        for (int c2 = 0; c2 < mesh.nc; c2++) {
+            double diag = 0;
+            std::vector<std::pair<int, double>> row;
+            for (int k = mesh.cf_ptr[c2]; k < mesh.cf_ptr[c2 + 1]; k++) {
+                double temp = kap * mesh.cf_area[k];
+                if (mesh.cf_bound[k] == -1) {
+                    int j = mesh.cf_nbr[k];
+                    double ax = mesh.cx[j] - mesh.cx[c2], ay = mesh.cy[j] - mesh.cy[c2], az = mesh.cz[j] - mesh.cz[c2];
+                    temp = temp / (mesh.cf_nx[k] * ax + mesh.cf_ny[k] * ay + mesh.cf_nz[k] * az);
+                    diag += -temp;
+                    row.push_back({j, temp});
+                } else if (mesh.b_type[mesh.cf_bound[k]] != 3) {
+                    double ax = mesh.cf_fx[k] - mesh.cx[c2], ay = mesh.cf_fy[k] - mesh.cy[c2], az = mesh.cf_fz[k] - mesh.cz[c2];
+                    temp = temp / (mesh.cf_nx[k] * ax + mesh.cf_ny[k] * ay + mesh.cf_nz[k] * az);
+                    diag += -temp;
+                }
+            }
+            row.push_back({c2, diag});
+            std::sort(row.begin(), row.end());
+            // merge duplicates (two faces to the same neighbour)
+            std::vector<std::pair<int, double>> merged;
+            for (auto &e : row) {
+                if (!merged.empty() && merged.back().first == e.first)
+                    merged.back().second += e.second;
+                else
+                    merged.push_back(e);
+            }
+            for (auto &e : merged) {
+                idx.push_back(e.first);
+                val.push_back(-e.second);
+                if (e.first == c2) dinv[c2] = 1.0 / (-e.second);
+            }
+            ptr[c2 + 1] = (int)idx.size();
+        }
+        K_ptr_ = up_i(ptr);
+        K_idx_ = up_i(idx);
+        K_val_ = up_d(val);
+        K_dinv_ = up_d(dinv);
+    }
+    if (!ok) return {-6, "device allocation or upload failed"};
+    Error e = alloc_all();
+    if (e.code) return e;
+    CUDA_TRY(cudaStreamSynchronize(s));
+    initialised = true;
+    return {0, ""};
+}
+
+Error Solver::alloc_all() {
+    const size_t nc = mesh.nc, nb = bands.nb, nd = ang.nd, nbs = mesh.nbs(), nslot = (size_t)mesh.nn * mesh.nmat;
+    const size_t S = cfg.precision == 1 ? sizeof(float) : sizeof(double);
+    const size_t ne = nd * nc * nb;
+    auto A = [&](size_t bytes) { return dalloc(bytes); };
+    eps_ = A(ne * S);
+    grad_ = A(ne * 3 * S);
+    res_ = A(ne * S);
+    Tbase_ = (double *)A(nc * 8);
+    gTb_ = (double *)A(nc * 3 * 8);
+    eb_ = (double *)A(nd * nbs * nb * 8);
+    eb_snap_ = need_snapshot_ ? (double *)A(nd * nbs * nb * 8) : nullptr;
+    T_ = (double *)A(nc * 8);
+    Told_ = (double *)A(nc * 8);
+    Tlat_ = (double *)A(nc * 8);
+    E_ = (double *)A(nc * 8);
+    q_ = (double *)A(nc * 3 * 8);
+    qold_ = (double *)A(nc * 3 * 8);
+    Tband_ = (double *)A(nb * nc * 8);
+    remacro_ = (double *)A(nc * 8);
+    Th_ = (double *)A(nc * 8);
+    Q_ = (double *)A(nc * 6 * 8);
+    Ths_ = (double *)A(nbs * 8);
+    Qs_ = (double *)A(nbs * 6 * 8);
+    ThV_ = (double *)A(nslot * 8);
+    QV_ = (double *)A(nslot * 6 * 8);
+    bTm_ = (double *)A(nbs * 8);
+    TV_ = (double *)A(nslot * 8);
+    rhs_ = (double *)A(nc * 8);
+    T1_ = (double *)A(nc * 8);
+    red_ = (double *)A(8 * 8);
+    cg_r_ = (double *)A(nc * 8);
+    cg_z_ = (double *)A(nc * 8);
+    cg_p_ = (double *)A(nc * 8);
+    cg_Ap_ = (double *)A(nc * 8);
+    cg_scal_ = (double *)A(65536 * 8);
+    for (void *pp : {eps_, grad_, res_, (void *)Tbase_, (void *)eb_, (void *)cg_scal_})
+        if (!pp) return {-6, "device allocation failed (" + std::to_string(ne * S * 5 / 1048576) + " MiB of band state)"};
+    if (cudaMallocHost((void **)&h_pinned_, 16 * sizeof(double)) != cudaSuccess) return {-6, "pinned allocation failed"};
+    cudaStream_t s = cfg.stream;
+    CUDA_TRY(cudaMemsetAsync(eb_, 0, nd * nbs * nb * 8, s));
+    CUDA_TRY(cudaMemsetAsync(Tbase_, 0, nc * 8, s));
+    CUDA_TRY(cudaMemsetAsync(gTb_, 0, nc * 3 * 8, s));
+    CUDA_TRY(cudaMemsetAsync(q_, 0, nc * 3 * 8, s));
+    // cooperative CG grid
+    int per_sm = 0, nsm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg, kThreads, 0));
+    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cfg.device));
+    coop_blocks_ = std::max(1, std::min(per_sm * nsm, (int)((nc + kThreads - 1) / kThreads)));
+    return {0, ""};
+}
+
+Error Solver::set_initial(const double *T0, const double *q0, const double *bth) {
+    if (!initialised) return {-1, "solver not initialised"};
+    if (!T0) return {-1, "T0 is required"};
+    const size_t nc = mesh.nc;
+    cudaStream_t s = cfg.stream;
+    CUDA_TRY(cudaMemcpyAsync(T_, T0, nc * 8, cudaMemcpyHostToDevice, s));
+    if (q0)
+        CUDA_TRY(cudaMemcpyAsync(q_, q0, nc * 3 * 8, cudaMemcpyHostToDevice, s));
+    else
+        CUDA_TRY(cudaMemsetAsync(q_, 0, nc * 3 * 8, s));
+    if (bth) {
+        std::vector<double> bt(bth, bth + mesh.nbd());
+        mesh.b_T = bt;
+        CUDA_TRY(cudaMemcpyAsync((void *)dm_.b_T, bt.data(), bt.size() * 8, cudaMemcpyHostToDevice, s));
+    }
+    // base of the stored deviation: T0 in the FP32 form, 0 in the FP64 form
+    if (cfg.precision == 1) {
+        CUDA_TRY(cudaMemcpyAsync(Tbase_, T0, nc * 8, cudaMemcpyHostToDevice, s));
+        // gradient of the base with the same stencil (host, FP64)
+        std::vector<double> g(nc * 3, 0.0);
+        for (size_t c = 0; c < nc; c++)
+            for (int q = mesh.nbr_ptr[c]; q < mesh.nbr_ptr[c + 1]; q++) {
+                double de = T0[mesh.nbr_idx[q]] - T0[c];
+                for (int r = 0; r < 3; r++) g[3 * c + r] += mesh.lsq_w[3 * (size_t)q + r] * de;
+            }
+        CUDA_TRY(cudaMemcpyAsync(gTb_, g.data(), nc * 3 * 8, cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+    } else {
+        CUDA_TRY(cudaMemsetAsync(Tbase_, 0, nc * 8, s));
+        CUDA_TRY(cudaMemsetAsync(gTb_, 0, nc * 3 * 8, s));
+    }
+    have_initial_ = true;
+    started_ = false;
+    return {0, ""};
+}
+
+Error Solver::fourier_initial() { return {-8, "the Fourier pre-solve is not implemented yet; pass T0 to gbte_set_initial"}; }
+
+Error Solver::macro_solve(double *x, const double *b, long long &iters) {
+    cudaStream_t s = cfg.stream;
+    const int nslots = 65536;
+    CUDA_TRY(cudaMemsetAsync(cg_scal_, 0, nslots * 8, s));
+    int n = mesh.nc;
+    double rtol = cfg.macro_rtol;
+    int maxit = 20000;
+    void *args[] = {&n, &K_ptr_, &K_idx_, &K_val_, &K_dinv_, (void *)&b, &x, &cg_r_, &cg_z_, &cg_p_, &cg_Ap_,
+                    &cg_scal_, &rtol, &maxit, (void *)&nslots};
+    int ns = nslots;
+    args[14] = &ns;
+    CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_pcg, dim3(coop_blocks_), dim3(kThreads), args, 0, s));
+    CUDA_TRY(cudaMemcpyAsync(h_pinned_ + 8, cg_scal_ + nslots - 1, 8, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    iters += (long long)h_pinned_[8];
+    return {0, ""};
+}
+
+template <typename S>
+Error Solver::solve_t(SolveStats &st) {
+    cudaStream_t s = cfg.stream;
+    const int nc = mesh.nc, nb = bands.nb, nd = ang.nd, nbs = mesh.nbs(), nslot = mesh.nn * mesh.nmat;
+    const size_t ne = (size_t)nd * nc * nb;
+    S *eps = (S *)eps_, *g = (S *)grad_, *R = (S *)res_;
+    EView<S> ev{eps, g, Tbase_, gTb_, nb, nc};
+    const int gE = grid_for(ne), gB = grid_for((size_t)nd * nbs * nb);
+    const int gC = (nc + kThreads - 1) / kThreads, gS = (nbs + kThreads - 1) / kThreads,
+              gN = (nslot + kThreads - 1) / kThreads;
+    int lpc = 1;
+    while (lpc < nb && lpc < 32) lpc <<= 1;
+    const int gM = (int)(((size_t)nc * lpc + kThreads - 1) / kThreads);
+    const int nbc = std::min(nb, 8);
+    const int sweep_blocks = nd * ((nb + nbc - 1) / nbc);
+    auto moments = [&]() {
+        switch (lpc) {
+        case 1: k_moments<S, 1><<<gM, kThreads, 0, s>>>(dm_, dp_, eps, Tbase_, Tlat_, E_, q_, Tband_, Th_, Q_); break;
+        case 2: k_moments<S, 2><<<gM, kThreads, 0, s>>>(dm_, dp_, eps, Tbase_, Tlat_, E_, q_, Tband_, Th_, Q_); break;
+        case 4: k_moments<S, 4><<<gM, kThreads, 0, s>>>(dm_, dp_, eps, Tbase_, Tlat_, E_, q_, Tband_, Th_, Q_); break;
+        case 8: k_moments<S, 8><<<gM, kThreads, 0, s>>>(dm_, dp_, eps, Tbase_, Tlat_, E_, q_, Tband_, Th_, Q_); break;
+        case 16: k_moments<S, 16><<<gM, kThreads, 0, s>>>(dm_, dp_, eps, Tbase_, Tlat_, E_, q_, Tband_, Th_, Q_); break;
+        default: k_moments<S, 32><<<gM, kThreads, 0, s>>>(dm_, dp_, eps, Tbase_, Tlat_, E_, q_, Tband_, Th_, Q_); break;
+        }
+    };
+    auto gather = [&]() {
+        if (need_snapshot_) cudaMemcpyAsync(eb_snap_, eb_, (size_t)nd * nbs * nb * 8, cudaMemcpyDeviceToDevice, s);
+        k_gather<<<gB, kThreads, 0, s>>>(dm_, dp_, dif_w_, spec_src_, need_snapshot_ ? eb_snap_ : nullptr, eb_);
+    };
+    if (!started_) {
+        // _set_initial (:765-782) and the initial boundary values (StaticBTESyntheticSolver.cpp:45-62)
+        k_init_eps<S><<<gE, kThreads, 0, s>>>(dm_, dp_, T_, Tbase_, eps);
+        k_gradient<S><<<gE, kThreads, 0, s>>>(dm_, dp_, eps, g);
+        k_bound_out<S><<<gB, kThreads, 0, s>>>(dm_, dp_, ev, eb_);
+        gather();
+        CUDA_TRY(cudaGetLastError());
+        started_ = true;
+    }
+    double errOld = 0, errOldq = 0;
+    int errInc = 0;
+    st = SolveStats();
+    float ms_total = 0, ms_transport = 0, ms_macro = 0;
+    int nt;
+    bool converged = false;
+    for (nt = 0; nt < cfg.max_iter; nt++) {
+        CUDA_TRY(cudaEventRecord(ev_[0], s));
+        // copy() (:2655-2690)
+        CUDA_TRY(cudaMemcpyAsync(Told_, T_, nc * 8, cudaMemcpyDeviceToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(qold_, q_, (size_t)nc * 24, cudaMemcpyDeviceToDevice, s));
+        k_gradient<S><<<gE, kThreads, 0, s>>>(dm_, dp_, eps, g);
+        k_residual<S><<<gE, kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, R);
+        k_sweep<S><<<sweep_blocks, kThreads, 0, s>>>(dm_, dp_, nbc, lvl_cells_, lvl_ptr_, dir_lvl_off_, lag_, R, eps);
+        k_bound_out<S><<<gB, kThreads, 0, s>>>(dm_, dp_, ev, eb_);
+        moments();
+        k_side_moments<<<gS, kThreads, 0, s>>>(dm_, dp_, eb_, Ths_, Qs_);
+        k_node_interp<<<gN, kThreads, 0, s>>>(dm_, Th_, Q_, Ths_, Qs_, ThV_, QV_);
+        k_remacro<<<gC, kThreads, 0, s>>>(dm_, Th_, Q_, Ths_, Qs_, ThV_, QV_, remacro_);
+        gather();
+        k_macro_bc<<<gS, kThreads, 0, s>>>(dm_, dp_, eb_, bTovr_, bTm_);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaEventRecord(ev_[1], s));
+        // _marco_solution: Picard on the non-orthogonal correction
+        k_copy<<<gC, kThreads, 0, s>>>(Tlat_, T_, nc);
+        double internal = 1000, prev_internal = 0;
+        int inner = 0, inner_inc = 0;
+        while (internal > 1e-6) {
+            k_copy<<<gC, kThreads, 0, s>>>(T_, T1_, nc);
+            k_tinterp<<<gN, kThreads, 0, s>>>(dm_, T_, TV_);
+            k_macro_rhs<<<gC, kThreads, 0, s>>>(dm_, dp_.kappa, remacro_, bTm_, TV_, rhs_);
+            CUDA_TRY(cudaGetLastError());
+            Error e = macro_solve(T_, rhs_, st.cg_iterations);
+            if (e.code) return e;
+            CUDA_TRY(cudaMemsetAsync(red_, 0, 8, s));
+            k_sqdiff<<<std::min(gC, 148), kThreads, 0, s>>>(nc, T1_, T_, red_);
+            CUDA_TRY(cudaMemcpyAsync(h_pinned_, red_, 8, cudaMemcpyDeviceToHost, s));
+            CUDA_TRY(cudaStreamSynchronize(s));
+            internal = h_pinned_[0] / nc;
+            inner++;
+            if (inner > 1 && internal > prev_internal) inner_inc++;
+            prev_internal = internal;
+            if (inner_inc >= 10 || !std::isfinite(internal) || inner >= 1000)
+                return {-4, "macro correction does not converge"};
+            if (cfg.verbose) printf("internal residual: %.17g\n", internal);
+        }
+        st.inner_iterations = inner;
+        CUDA_TRY(cudaEventRecord(ev_[2], s));
+        // margins
+        CUDA_TRY(cudaMemsetAsync(red_, 0, 4 * 8, s));
+        k_margins<<<std::min(gC, 148), kThreads, 0, s>>>(nc, T_, Told_, q_, qold_, red_);
+        CUDA_TRY(cudaMemcpyAsync(h_pinned_, red_, 4 * 8, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaEventRecord(ev_[3], s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        float a = 0, b2 = 0, c2 = 0;
+        cudaEventElapsedTime(&a, ev_[0], ev_[1]);
+        cudaEventElapsedTime(&b2, ev_[1], ev_[2]);
+        cudaEventElapsedTime(&c2, ev_[0], ev_[3]);
+        ms_transport += a;
+        ms_macro += b2;
+        ms_total += c2;
+        const double err = h_pinned_[1] / nc / h_pinned_[0];
+        const double errq = h_pinned_[3] / nc / h_pinned_[2];
+        if (cfg.verbose)
+            printf("Iteration #%d\t Margin per band per cell: Temperature:%.6g Heat Flux:%.6g\n", nt, err, errq);
+        if ((err > errOld && errq > errOldq) || std::isnan(err) || std::isnan(errq) || std::isinf(err) || std::isinf(errq))
+            errInc++;
+        else
+            errInc = 0;
+        errOld = err;
+        errOldq = errq;
+        st.err_temp = err;
+        st.err_flux = errq;
+        st.iterations = nt + 1;
+        st.updates += (long long)nd * nc * nb;
+        if (err <= cfg.err_temp && errq <= cfg.err_flux) {
+            converged = true;
+            break;
+        }
+        if (errInc >= 10) {
+            st.solve_ms = ms_total;
+            st.transport_ms = ms_transport;
+            st.macro_ms = ms_macro;
+            return {-4, "margins increased 10 times in a row or became NaN/Inf"};
+        }
+    }
+    st.solve_ms = ms_total;
+    st.transport_ms = ms_transport;
+    st.macro_ms = ms_macro;
+    if (!converged) return {1, "maximum number of iterations reached"};
+    return {0, ""};
+}
+
+Error Solver::solve(SolveStats &st) {
+    if (!initialised) return {-1, "solver not initialised"};
+    if (!have_initial_) return {-1, "call gbte_set_initial (or gbte_fourier_initial) before gbte_solve"};
+    CUDA_TRY(cudaSetDevice(cfg.device));
+    if (cfg.precision == 1) return solve_t<float>(st);
+    return solve_t<double>(st);
+}
+
+Error Solver::get_fields(double *TE, double *TL, double *q, double *TB) {
+    if (!initialised) return {-1, "solver not initialised"};
+    cudaStream_t s = cfg.stream;
+    const size_t nc = mesh.nc;
+    if (TE) CUDA_TRY(cudaMemcpyAsync(TE, E_, nc * 8, cudaMemcpyDeviceToHost, s));
+    if (TL) CUDA_TRY(cudaMemcpyAsync(TL, T_, nc * 8, cudaMemcpyDeviceToHost, s));
+    if (q) CUDA_TRY(cudaMemcpyAsync(q, q_, nc * 24, cudaMemcpyDeviceToHost, s));
+    if (TB) CUDA_TRY(cudaMemcpyAsync(TB, Tband_, nc * bands.nb * 8, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return {0, ""};
+}
+
+}  // namespace gbte

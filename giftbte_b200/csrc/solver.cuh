@@ -1,0 +1,111 @@
+// Device-side solver of the steady synthetic phonon BTE (internal header).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "gbte_internal.h"
+
+namespace gbte {
+
+// Pointers into device memory describing the flattened mesh.
+struct DMesh {
+    int dim, nc, nn, nbs, nbd, nslot, ncf, nf;
+    double inv_Lx;
+    const int *cf_ptr, *cf_nbr, *cf_bside, *cf_bound, *cf_v, *cf_face;
+    const double *cf_area, *cf_nx, *cf_ny, *cf_nz, *cf_fx, *cf_fy, *cf_fz;
+    const double *vol, *cx, *cy, *cz, *heat;
+    const int *nbr_ptr, *nbr_idx;
+    const double *lsq_w;
+    const double *face_w;
+    const int *f_cf0;
+    const int *b_type, *b_connect;
+    const double *b_T;
+    const int *bs_cell, *bs_cf;
+    const int *nv_ptr, *nv_src;
+    const double *nv_w;
+    const int *nt_ptr, *nt_src;
+    const double *nt_w;
+    const double *node_x, *node_y, *node_z;
+};
+
+// Single-material band/direction constants.
+struct DPhys {
+    int nb, nd;
+    const double *vmag, *tau, *C, *lat, *hr;  // [nb]
+    double kappa, capb;
+    const double *sx, *sy, *sz, *w;           // [nd]
+};
+
+struct SolverConfig {
+    int precision = 0;
+    int use_limiter = 0;
+    int max_iter = 10000;
+    double err_temp = 1e-6, err_flux = 1e-4;
+    double macro_rtol = 1e-13;
+    int verbose = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+};
+
+struct SolveStats {
+    int iterations = 0, inner_iterations = 0;
+    double err_temp = 0, err_flux = 0, solve_ms = 0, transport_ms = 0, macro_ms = 0;
+    long long cg_iterations = 0, updates = 0;
+};
+
+class Solver {
+public:
+    ~Solver();
+    Error init(const FlatMesh &m, const Bands &b, const Angles &a, const std::vector<double> &cell_heat,
+               const SolverConfig &cfg);
+    Error set_initial(const double *T0, const double *q0, const double *boundary_thermal_per_bside);
+    Error fourier_initial();
+    Error solve(SolveStats &st);
+    Error get_fields(double *T_energy, double *T_lattice, double *q, double *T_band);
+
+    FlatMesh mesh;
+    Bands bands;
+    Angles ang;
+    Schedule sched;
+    SolverConfig cfg;
+    bool initialised = false;
+    std::string last_error;
+
+private:
+    template <typename S> Error solve_t(SolveStats &st);
+    Error alloc_all();
+    Error macro_solve(double *x_dev, const double *rhs_dev, long long &iters);
+    void *dalloc(size_t bytes);
+    std::vector<void *> allocs_;
+    DMesh dm_{};
+    DPhys dp_{};
+    // state
+    void *eps_ = nullptr, *grad_ = nullptr, *res_ = nullptr;  // storage-type arrays
+    double *Tbase_ = nullptr, *gTb_ = nullptr;
+    double *eb_ = nullptr, *eb_snap_ = nullptr;
+    double *T_ = nullptr, *Told_ = nullptr, *Tlat_ = nullptr, *E_ = nullptr, *q_ = nullptr, *qold_ = nullptr,
+           *Tband_ = nullptr, *remacro_ = nullptr, *Th_ = nullptr, *Q_ = nullptr, *Ths_ = nullptr, *Qs_ = nullptr,
+           *ThV_ = nullptr, *QV_ = nullptr, *bTm_ = nullptr, *bTovr_ = nullptr, *TV_ = nullptr, *rhs_ = nullptr,
+           *T1_ = nullptr, *red_ = nullptr;
+    // diffuse weights / specular map
+    double *dif_w_ = nullptr;
+    int *spec_src_ = nullptr;
+    bool need_snapshot_ = false;
+    // schedule on device
+    int *lvl_cells_ = nullptr, *lvl_ptr_ = nullptr, *dir_lvl_off_ = nullptr;
+    unsigned char *lag_ = nullptr;
+    // macro matrix (negated, SPD), CSR
+    int *K_ptr_ = nullptr, *K_idx_ = nullptr;
+    double *K_val_ = nullptr, *K_dinv_ = nullptr;
+    double *cg_r_ = nullptr, *cg_z_ = nullptr, *cg_p_ = nullptr, *cg_Ap_ = nullptr, *cg_scal_ = nullptr;
+    double *h_pinned_ = nullptr;
+    bool have_initial_ = false;
+    bool started_ = false;
+    int coop_blocks_ = 0;
+    cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+}  // namespace gbte

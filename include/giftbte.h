@@ -1,0 +1,197 @@
+/*
+ * giftbte.h — C ABI of the B200-native steady synthetic phonon-BTE solver.
+ *
+ * This is the drop-in boundary for GiftBTE's StaticBTESynthetic path
+ * (Order=2, IterativeScheme=Synthetic, MatrixSolver=LU). Plain C types only:
+ * pointers and sizes, no C++ or torch types. Every call returns a status code
+ * (GBTE_OK = 0) and never throws or exits; the message of the last failure on
+ * a handle is available from gbte_last_error(). A handle owns one CUDA stream
+ * and its device memory; it is not thread-safe, distinct handles are
+ * independent.
+ *
+ * Reference interfaces replaced (paths inside the GiftBTE project):
+ *   gbte_create          StaticBTESynthetic::StaticBTESynthetic(BTEMesh*,
+ *                        BTEBoundaryCondition*, BTEBand*, BTEAngle*, int, int)
+ *                        includes/StaticBTESynthetic/StaticBTESynthetic.h:177,
+ *                        with the mesh topology of BTEMesh::setMeshParams /
+ *                        setMeshParams1 (src/BTEMesh/BTEMesh.cpp:600-1023)
+ *                        and the quadrature of BTEAngle (src/BTEAngle/
+ *                        BTEAngle.cpp:11-190)
+ *   gbte_create_from_deck  the input stage of main() (src/BTEMain.cpp:87-362):
+ *                        CONTROL / GEOMETRY / PHONON keyword files, BC table,
+ *                        COMSOL or MSH mesh, DATABASE band table
+ *   gbte_set_initial     the writes into solver.temperature[],
+ *                        heatFlux*Global[] and boundaryThermal[] before solve
+ *                        (src/Solution/Solution.cpp:266-285)
+ *   gbte_fourier_initial the Fourier pre-solve that seeds those arrays
+ *                        (src/StaticFourier/StaticFourier.cpp:934-976,
+ *                        src/Solution/Solution.cpp:236-255)
+ *   gbte_solve           StaticBTESynthetic::solve(Use_Backup, Num_Max_Iter,
+ *                        Use_Limiter, error_temp_limit, error_flux_limit)
+ *                        includes/StaticBTESynthetic/StaticBTESynthetic.h:221
+ *   gbte_get_fields      the reads of totalEnergy[], temperature[],
+ *                        heatFlux{X,Y,Z}Global[], temperatureband[] after
+ *                        solve (src/Solution/Solution.cpp:408-413)
+ *   gbte_write_outputs   StaticBTESynthetic::_print_out and
+ *                        SolutionAll::_print_out (StaticBTESynthetic.cpp:
+ *                        2613-2653, Solution.cpp:128-233)
+ *   gbte_destroy         StaticBTESynthetic::~StaticBTESynthetic
+ *                        (StaticBTESynthetic.cpp:52-223)
+ */
+#ifndef GIFTBTE_B200_H
+#define GIFTBTE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GBTE_ABI_VERSION 1
+
+/* status codes */
+#define GBTE_OK 0
+#define GBTE_ERR_ARG -1          /* invalid argument or inconsistent sizes */
+#define GBTE_ERR_IO -2           /* a deck file is missing or malformed */
+#define GBTE_ERR_CUDA -3         /* a CUDA call failed */
+#define GBTE_ERR_DIVERGED -4     /* NaN/Inf or 10 consecutive margin increases */
+#define GBTE_ERR_TIMEOUT -5      /* a bounded device-side wait gave up */
+#define GBTE_ERR_NOMEM -6        /* device allocation failed */
+#define GBTE_ERR_MESH -7         /* mesh topology error (open face, no periodic partner) */
+#define GBTE_ERR_UNSUPPORTED -8  /* input outside the implemented scope */
+#define GBTE_ERR_NOT_CONVERGED 1 /* max_iter reached before the margins (not an error) */
+
+/* precision of the band intensities */
+#define GBTE_FP64 0        /* plain FP64 drop-in form */
+#define GBTE_FP32_MIXED 1  /* FP32 intensities and sweeps, FP64 moments, macro solve and margins */
+
+typedef struct gbte_handle gbte_handle;
+
+/* Unstructured mesh, coordinates already scaled to metres (node * ScaleX..).
+ * 2D: triangles (3 vertices) or quads (4 vertices, COMSOL order
+ * v0 v1 v2 v3 with edges v0-v1, v1-v3, v3-v2, v2-v0); boundary elements are
+ * edges (2 vertices). 3D: tetrahedra; boundary elements are triangles. */
+typedef struct {
+    int dimension;            /* 2 or 3 */
+    int num_nodes;
+    int num_cells;
+    int num_boundary_elements;
+    const double *node_xyz;   /* [num_nodes * 3] */
+    const int *cell_ptr;      /* [num_cells + 1], CSR into cell_verts */
+    const int *cell_verts;
+    const int *cell_region;   /* [num_cells], 0-based geometry region */
+    const int *belem_ptr;     /* [num_boundary_elements + 1] */
+    const int *belem_verts;
+    const int *belem_tag;     /* [num_boundary_elements], tag as in the BC file */
+    double scale_x, scale_y, scale_z;  /* ScaleX/Y/Z (the LSQ stencil is scaled by 1/ScaleX) */
+} gbte_mesh_view;
+
+/* Band table (DATABASE columns), material-major [m * num_bands + b]. */
+typedef struct {
+    int num_materials;
+    int num_bands;
+    const double *group_velocity;
+    const double *relaxation_time;
+    const double *heat_capacity;
+    const double *lattice_ratio;
+    const double *heat_ratio;
+    int num_regions;
+    const int *region_material;  /* [num_regions], 0-based material of each region */
+    int material_dimension;      /* 2 or 3: kappa_bulk = sum C v^2 tau / dim */
+} gbte_band_table;
+
+/* Boundary conditions: type 1 isothermal (value = wall T), 2 diffuse,
+ * 3 specular, < 0 periodic (partner tag = -type, value = temperature jump). */
+typedef struct {
+    int num;
+    const int *tag;
+    const int *type;
+    const double *value;
+} gbte_bc_table;
+
+typedef struct {
+    int method;   /* 1 = CADOM (uniform midpoint), 2 = Gauss-Legendre */
+    int n_theta;
+    int n_phi;
+} gbte_angle_spec;
+
+typedef struct {
+    int precision;            /* GBTE_FP64 or GBTE_FP32_MIXED */
+    int use_limiter;          /* Order=2limit */
+    int max_iter;
+    double err_temp;          /* ResidualTemp */
+    double err_flux;          /* ResidualFlux */
+    const double *cell_heat;  /* [num_cells] W/m^3, may be NULL (no source) */
+    void *stream;             /* cudaStream_t to run on; NULL = the handle creates one */
+    int device;               /* CUDA device ordinal */
+    int verbose;              /* 1: print the per-iteration margins like the reference */
+    double macro_rtol;        /* relative residual of the macro CG solve; 0 = default 1e-13 */
+} gbte_options;
+
+typedef struct {
+    int iterations;
+    double err_temp;          /* last temperature margin */
+    double err_flux;          /* last heat-flux margin */
+    double solve_ms;          /* device time of the outer loop (CUDA events) */
+    double setup_ms;          /* host+device setup inside gbte_create */
+    double transport_ms;      /* gradient + residual + sweep + boundary + moments */
+    double macro_ms;          /* synthetic correction (CG solves) */
+    long long macro_cg_iterations;
+    long long updates;        /* band*direction*cell updates performed */
+    int num_directions;
+    int num_bands;
+    int num_cells;
+    int max_levels;           /* deepest sweep over all directions */
+    int lagged_faces;         /* upwind faces lagged to break cycles (3D) */
+    int inner_iterations;     /* macro Picard steps in the last outer iteration */
+} gbte_stats;
+
+/* Default options (FP64, max_iter 10000, margins 1e-6/1e-4 as the reference). */
+void gbte_default_options(gbte_options *opt);
+
+int gbte_create(const gbte_mesh_view *mesh, const gbte_band_table *bands, const gbte_bc_table *bcs,
+                const gbte_angle_spec *angles, const gbte_options *opt, gbte_handle **out);
+
+/* Reads <dir>/input/{CONTROL,GEOMETRY,PHONON} and the files they name
+ * (relative paths resolved against <dir>, like the reference's CWD).
+ * Options from CONTROL (Order, margins, MaxNumIter) override *opt. */
+int gbte_create_from_deck(const char *dir, const gbte_options *opt, gbte_handle **out);
+
+/* Initial lattice temperature [num_cells] (required before the first solve
+ * unless gbte_fourier_initial is used), optional initial heat flux
+ * [num_cells*3] (the previous-iterate flux of the first margin), optional
+ * boundary temperatures overriding the BC values per boundary element
+ * [num_boundary_elements] (NULL keeps the BC values). */
+int gbte_set_initial(gbte_handle *h, const double *T0, const double *q0, const double *boundary_thermal);
+
+/* Fourier pre-solve with kappa_bulk on the device; sets T0 and q0. */
+int gbte_fourier_initial(gbte_handle *h);
+
+/* Runs the outer source iteration until both margins are below the limits
+ * (GBTE_OK), max_iter is reached (GBTE_ERR_NOT_CONVERGED) or it diverges.
+ * stats may be NULL. */
+int gbte_solve(gbte_handle *h, gbte_stats *stats);
+
+/* Result fields (any pointer may be NULL):
+ * T_energy [Nc]  totalEnergy      -> Temperature.dat
+ * T_lattice[Nc]  macro temperature -> TempLattice.dat
+ * q        [Nc*3] heat flux        -> HeatFlux.dat
+ * T_band   [Nb*Nc] band temperatures -> Tempband.dat */
+int gbte_get_fields(gbte_handle *h, double *T_energy, double *T_lattice, double *q, double *T_band);
+
+/* Writes Temperature.dat, TempLattice.dat, HeatFlux.dat, Tempband.dat and
+ * Result.vtk into <dir> in the reference's formats (17 significant digits). */
+int gbte_write_outputs(gbte_handle *h, const char *dir);
+
+/* Sizes of the problem held by a handle (any pointer may be NULL). */
+int gbte_get_sizes(gbte_handle *h, int *num_cells, int *num_bands, int *num_directions, int *num_boundary_sides);
+
+/* Cell centres [Nc*3] and volumes [Nc] as the solver sees them. */
+int gbte_get_geometry(gbte_handle *h, double *centers, double *volumes);
+
+const char *gbte_last_error(const gbte_handle *h);
+const char *gbte_status_string(int status);
+int gbte_destroy(gbte_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GIFTBTE_B200_H */

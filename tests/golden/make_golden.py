@@ -1,0 +1,116 @@
+"""Generate the golden parity fixtures from the compiled reference.
+
+Each case is a small seeded deck written in the reference's own file formats
+(giftbte_b200.decks), run through the unmodified reference binary
+(oracle/_ref/BTE_CPU, built by ``make -C oracle ref``) to residual 1e-12, and
+stored as ``tests/golden/<case>.npz`` with the mesh, the deck parameters and
+the reference's full-precision fields:
+
+  T      macro-corrected lattice temperature  (TempLattice.dat)
+  E      energy temperature                   (Temperature.dat)
+  q      heat flux, Nc x 3                    (HeatFlux.dat)
+  Tband  band temperatures, Nb x Nc           (Tempband.dat)
+
+Usage (needs the reference tree, so it runs only where that exists):
+    python tests/golden/make_golden.py [case ...]
+"""
+from __future__ import annotations
+
+import json
+import os
+import shutil
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from giftbte_b200 import decks  # noqa: E402
+import oracle  # noqa: E402
+
+
+def cases():
+    out = {}
+    # 1. the gray 2D square (3200 triangles, 32 CADOM directions)
+    out["gray_square_tri"] = decks.config1_deck(40)
+    # 2. quads, isothermal left/right, specular top/bottom, uniform heat,
+    #    2 bands, 3D material quadrature (Gauss, 2x2 -> 32 directions)
+    m = decks.square_quad_mesh(16, 16)
+    b = decks.sine_dispersion_bands(2)
+    out["quad_heat_specular"] = decks.Deck(
+        mesh=m, bands=b, bcs=[decks.BC(1, 1, 300.0), decks.BC(2, 1, 300.0), decks.BC(3, 3, 0.0),
+                              decks.BC(4, 3, 0.0)],
+        scale=(1e-7, 1e-7), material_dim=3, angle_method=2, n_theta=2, n_phi=2, tref=300.0,
+        heat_source=1e16)
+    # 3. jittered triangles, x-periodic with a 1 K jump, y specular, 3 bands
+    m = decks.jitter_interior(decks.square_tri_mesh(16, 16), 0.2 / 16, seed=3)
+    out["periodic_jitter"] = decks.Deck(
+        mesh=m, bands=decks.sine_dispersion_bands(3),
+        bcs=[decks.BC(1, -2, 1.0), decks.BC(2, -1, 0.0), decks.BC(3, 3, 0.0), decks.BC(4, 3, 0.0)],
+        scale=(1e-7, 1e-7), material_dim=2, angle_method=1, n_phi=4, tref=0.0)
+    # 4. nanoporous periodic cell with a diffuse pore (gmsh MSH 4.1 file)
+    m = decks.porous_cell_mesh(0.1, [(0.5, 0.5, 0.25)], seed=4)
+    out["porous_msh"] = decks.Deck(
+        mesh=m, bands=decks.sine_dispersion_bands(4),
+        bcs=[decks.BC(1, -2, 1.0), decks.BC(2, -1, 0.0), decks.BC(3, -4, 0.0), decks.BC(4, -3, 0.0),
+             decks.BC(5, 2, 0.0)],
+        scale=(3e-7, 3e-7), material_dim=2, angle_method=2, n_phi=4, tref=0.0, mesh_format="MSH")
+    for d in out.values():
+        d.residual_temp = 1e-12
+        d.residual_flux = 1e-12
+        d.max_iter = 3000
+    return out
+
+
+def deck_params(d: decks.Deck) -> dict:
+    return {"scale": list(d.scale), "material_dim": d.material_dim, "angle_method": d.angle_method,
+            "n_theta": d.n_theta, "n_phi": d.n_phi, "tref": d.tref, "heat_source": d.heat_source,
+            "mesh_format": d.mesh_format,
+            "bcs": [[b.tag, b.type, b.value] for b in d.bcs]}
+
+
+def make(name: str, d: decks.Deck) -> None:
+    work = tempfile.mkdtemp(prefix=f"golden_{name}_")
+    try:
+        d.write(work)
+        r = oracle.run_reference(work)
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    m = d.mesh
+    B = d.bands
+    np.savez_compressed(
+        os.path.join(HERE, f"{name}.npz"),
+        nodes=m.nodes, cells=np.asarray(m.cells), edges=m.edges, edge_tags=m.edge_tags,
+        cell_region=m.cell_region,
+        band_v=B.v, band_tau=B.tau, band_C=B.C, band_lat=B.lattice_ratio, band_hr=B.heat_ratio,
+        params=json.dumps(deck_params(d)),
+        T=r["T"], E=r["E"], q=r["q"], Tband=r["Tband"], xyz=r["xyz"], iters=r["iters"])
+    print(f"{name}: Nc={m.n_cells} Nb={B.n_bands} iters={r['iters']}")
+
+
+def load(name: str):
+    """Rebuild the Deck and the reference fields of a stored fixture."""
+    z = np.load(os.path.join(HERE, f"{name}.npz"))
+    p = json.loads(str(z["params"]))
+    mesh = decks.Mesh2D(nodes=z["nodes"], cells=z["cells"], edges=z["edges"], edge_tags=z["edge_tags"],
+                        cell_region=z["cell_region"])
+    bands = decks.BandTable(v=z["band_v"], tau=z["band_tau"], C=z["band_C"], lattice_ratio=z["band_lat"],
+                            heat_ratio=z["band_hr"])
+    d = decks.Deck(mesh=mesh, bands=bands, bcs=[decks.BC(int(t), int(ty), float(v)) for t, ty, v in p["bcs"]],
+                   scale=tuple(p["scale"]), material_dim=p["material_dim"], angle_method=p["angle_method"],
+                   n_theta=p["n_theta"], n_phi=p["n_phi"], tref=p["tref"], heat_source=p["heat_source"],
+                   mesh_format=p["mesh_format"], residual_temp=1e-12, residual_flux=1e-12, max_iter=3000)
+    ref = {k: z[k] for k in ("T", "E", "q", "Tband", "xyz")}
+    ref["iters"] = int(z["iters"])
+    return d, ref
+
+
+CASES = ["gray_square_tri", "quad_heat_specular", "periodic_jitter", "porous_msh"]
+
+if __name__ == "__main__":
+    want = sys.argv[1:] or CASES
+    all_cases = cases()
+    for n in want:
+        make(n, all_cases[n])
