@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""Benchmark of the steady synthetic phonon-BTE hot path on B200.
+
+One *step* is one outer source iteration (all bands x directions x cells:
+gradient, residual, upwind sweep, boundary, moments, synthetic correction,
+margins) of the named workload. The default workload is the non-gray 2D
+nanoporous cell: 300 nm periodic square with a centred r = 100 nm diffuse
+pore, Delaunay mesh with mean edge 3 nm (seed 0), 40 sine-dispersion bands,
+64 in-plane CADOM directions, x-periodic 1 K jump.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp32|fp64] [--workload config2|config1]
+
+Prints one JSON line (rank 0). ``value`` is device-resident throughput in
+band*direction*cell updates/s over exactly K timed steps (CUDA events on the
+solver's stream, max over ranks). ``e2e`` is the same metric through the
+public API from host buffers: set the initial field from pinned host memory,
+solve to residual 1e-8, read every result field back. Under torchrun each
+rank solves an independent seeded cell (weak scaling, no collective on the
+data path). ``--impl reference`` times the reference's own CPU solver
+(oracle/_ref/BTE_CPU) on the same deck on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def measured_peak_gbs():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def build_deck(workload: str, seed: int):
+    from giftbte_b200 import decks
+
+    if workload == "config1":
+        d = decks.config1_deck(40)
+        desc = "gray 1 um square, 40x40x2 triangles (3200), 1 band, 32 CADOM directions"
+    else:
+        d = decks.config2_deck(h_nm=3.0, n_bands=40, n_phi=16, seed=seed)
+        desc = (f"2D nanoporous periodic cell 300 nm, r=100 nm diffuse pore, mean edge 3 nm "
+                f"({d.mesh.n_cells} triangles), 40 sine-dispersion bands, 64 CADOM directions, seed {seed}")
+    return d, desc
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def start(self):
+        if shutil.which("nvidia-smi") is None:
+            return
+        self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=self.out, stderr=subprocess.DEVNULL)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.flush()
+        self.out.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.read().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.out.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# algorithmic bytes per band*direction*cell update of each kernel (s = bytes
+# of the stored intensity; the gradient is stored as 3 components)
+def kernel_bytes_per_update(name: str, s: int) -> float:
+    return {
+        "gradient": s + 3 * s,   # read e, write g
+        "residual": s + 3 * s + s,  # read e, read g, write R
+        "sweep": s + 2 * s,      # read R (overwritten by the correction), read+write e
+        "moments": s,            # read e
+    }.get(name, 0.0)
+
+
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import torch
+    import torch.distributed as dist
+
+    import giftbte_b200 as g
+
+    torch.cuda.set_device(local_rank)
+    torch.cuda.init()
+    stream = torch.cuda.current_stream()
+    deck, desc = build_deck(args.workload, seed=rank)
+    nc = deck.mesh.n_cells
+    prec = g.GBTE_FP32_MIXED if args.precision == "fp32" else g.GBTE_FP64
+    s_bytes = 4 if prec == g.GBTE_FP32_MIXED else 8
+
+    solver = g.StaticBTESynthetic.from_deck(deck, precision=prec, device=local_rank, profile=1,
+                                            stream=ctypes_stream(stream))
+    nb, nd = solver.num_bands, solver.num_directions
+    upd_per_step = nb * nd * nc
+    # warm-up (not timed)
+    solver.solve(max_iter=args.warmup, err_temp=0.0, err_flux=0.0)
+    torch.cuda.synchronize()
+    # timed region: exactly K outer iterations (margins 0, so none stops early)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    st = solver.solve(max_iter=args.steps, err_temp=0.0, err_flux=0.0)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = upd_per_step * args.steps * world / (ms * 1e-3)
+
+    # roofline of the dominant kernel (per-launch CUDA events on the solver's stream)
+    kern = st["kernels"]
+    dom = max(kern.items(), key=lambda kv: kv[1]["ms"])
+    dname, dk = dom[0], dom[1]
+    bpu = kernel_bytes_per_update(dname, s_bytes)
+    peak, peak_kind = measured_peak_gbs()
+    per_launch_ms = dk["ms"] / dk["launches"]
+    achieved = (bpu * upd_per_step) / (per_launch_ms * 1e-3) / 1e9 if bpu else None
+    roofline = {"kernel": dname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                "traffic": None, "bytes_per_update": bpu, "launch_ms": per_launch_ms,
+                "kernel_share": dk["ms"] / sum(v["ms"] for v in kern.values())}
+    kernel_table = {k: {"ms_per_launch": v["ms"] / v["launches"], "launches": v["launches"],
+                        "share": v["ms"] / sum(x["ms"] for x in kern.values())} for k, v in kern.items()}
+    solver.close()
+
+    # end to end through the public API: host in, solve to 1e-8, host out
+    e2e, ttr = e2e_solves(args, deck, prec, local_rank, world)
+
+    out = None
+    if rank == 0:
+        fp64 = None
+        if args.compare_fp64 and prec == g.GBTE_FP32_MIXED:
+            fp64 = fp64_reference_run(args, deck, local_rank)
+        cpu = cpu_baseline(args, deck) if world == 1 else None
+        out = {
+            "metric": "band*dir*cell updates/s (time to residual 1e-8 alongside); FP32-mixed vs FP64 on 1 B200",
+            "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if prec == g.GBTE_FP32_MIXED else "f64",
+            "data": "synthetic: seeded mesh and band table generated in-process (no dataset)",
+            "config": {"workload": desc, "cells": nc, "bands": nb, "directions": nd,
+                       "updates_per_step": upd_per_step, "precision": args.precision,
+                       "l2": f"band state {upd_per_step * s_bytes / 1e6:.0f} MB per copy, larger than the 126 MB L2",
+                       "parallelism": f"replicas x{world} (independent seeded cells)" if world > 1 else "1 GPU"},
+            "roofline": roofline, "kernels": kernel_table, "cpu_baseline": cpu, "e2e": e2e,
+            "time_to_residual": ttr, "gpu_launches": int(st["kernel_launches"]), "clocks": clk,
+            "macro": {"ms_per_step": st["macro_ms"] / args.steps, "cg_iterations": st["macro_cg_iterations"]},
+        }
+        if fp64 is not None:
+            out["fp64"] = fp64
+    return out
+
+
+def ctypes_stream(stream) -> int:
+    return int(stream.cuda_stream)
+
+
+def e2e_solves(args, deck, prec, device, world):
+    import torch
+
+    import giftbte_b200 as g
+
+    nc = deck.mesh.n_cells
+    solver = g.StaticBTESynthetic.from_deck(deck, precision=prec, device=device, max_iter=args.max_iter_e2e,
+                                            err_temp=1e-8, err_flux=1e-8)
+    nb = solver.num_bands
+    T0 = torch.full((nc,), float(deck.tref), dtype=torch.float64).pin_memory().numpy()
+    out = {k: np.zeros(n) for k, n in (("E", nc), ("T", nc), ("q", 3 * nc), ("Tb", nb * nc))}
+    nsteps = max(1, min(args.steps, args.e2e_steps))
+    times, iters, ups = [], [], []
+    for _ in range(nsteps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        solver.set_initial(T0)
+        st = solver.solve()
+        f = solver.fields()
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+        iters.append(st["iterations"])
+        ups.append(st["updates"])
+    solver.close()
+    t = max(times)
+    e2e = {"value": sum(ups) / sum(times) * world, "unit": "updates/s",
+           "h2d_bytes_per_step": int(nc * 8), "d2h_bytes_per_step": int(nc * 8 * (2 + 3 + nb)),
+           "steps": nsteps, "step": "set_initial from pinned host + solve to residual 1e-8 + read all fields"}
+    ttr = {"seconds": float(np.median(times)), "iterations": int(np.median(iters)), "residual": 1e-8,
+           "precision": "fp32" if prec == g.GBTE_FP32_MIXED else "fp64"}
+    return e2e, ttr
+
+
+def fp64_reference_run(args, deck, device):
+    """The plain FP64 GPU form on the same workload: time to residual 1e-8
+    and the FP32 form's temperature error against it."""
+    import torch
+
+    import giftbte_b200 as g
+
+    res = {}
+    fields = {}
+    for prec, name in ((g.GBTE_FP64, "fp64"), (g.GBTE_FP32_MIXED, "fp32")):
+        s = g.StaticBTESynthetic.from_deck(deck, precision=prec, device=device, max_iter=args.max_iter_e2e,
+                                           err_temp=1e-8, err_flux=1e-8)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = s.solve()
+        torch.cuda.synchronize()
+        res[name] = {"seconds": time.perf_counter() - t0, "iterations": st["iterations"],
+                     "updates_per_s": st["updates"] / (st["solve_ms"] * 1e-3)}
+        fields[name] = s.fields()
+        s.close()
+    T64, T32 = fields["fp64"]["T"], fields["fp32"]["T"]
+    res["fp32_T_max_rel_err"] = float(np.max(np.abs(T32 - T64)) / np.max(np.abs(T64)))
+    res["fp32_speedup_time_to_residual"] = res["fp64"]["seconds"] / res["fp32"]["seconds"]
+    return res
+
+
+def cpu_baseline(args, deck):
+    """The oracle restatement (multithreaded FP64 CPU port) timed on the
+    host cores on a bounded sample: one outer iteration of the same deck,
+    measured as the difference of a 2-iteration and a 1-iteration run."""
+    import oracle
+
+    if args.skip_cpu:
+        return None
+    try:
+        t = []
+        for n in (1, 2):
+            t0 = time.perf_counter()
+            oracle.solve(deck, max_iter=n, err_T=0.0, err_q=0.0)
+            t.append(time.perf_counter() - t0)
+        per_iter = max(t[1] - t[0], 1e-9)
+        upd = deck.bands.n_bands * (4 * deck.n_phi if deck.material_dim == 2 else 8 * deck.n_theta * deck.n_phi) \
+            * deck.mesh.n_cells
+        return {"value": upd / per_iter, "unit": "updates/s", "cores": os.cpu_count(), "kind": "port",
+                "sample": "one outer iteration of the same deck (difference of 2- and 1-iteration runs)"}
+    except Exception as e:  # the baseline must not take the GPU line down
+        return {"value": None, "unit": "updates/s", "cores": os.cpu_count(), "kind": "port",
+                "sample": f"failed: {e}"}
+
+
+def run_reference(args, rank: int):
+    """The unmodified reference CPU solver on the same deck (1 MPI rank via
+    the single-rank stub build), timed from its own per-iteration
+    'Time taken by inner loop' trace."""
+    if rank != 0:
+        return None
+    import oracle
+
+    deck, desc = build_deck(args.workload, seed=0)
+    nb = deck.bands.n_bands
+    nd = 4 * deck.n_phi if deck.material_dim == 2 else 8 * deck.n_theta * deck.n_phi
+    upd = nb * nd * deck.mesh.n_cells
+    k = max(1, min(args.steps, args.ref_steps))
+    w = min(args.warmup, 1)
+    base = {"impl": "reference", "metric": "band*dir*cell updates/s (time to residual 1e-8 alongside); "
+            "FP32-mixed vs FP64 on 1 B200", "unit": "updates/s", "higher_is_better": True, "n_gpus": 1,
+            "steps": k, "warmup": w, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: the same seeded deck", "config": {"workload": desc}}
+    if not os.path.exists(oracle.REF_BIN):
+        # the restatement stands in when the reference binary was not built
+        cpu = cpu_baseline(args, deck)
+        base.update({"value": cpu["value"], "cpu_baseline": cpu,
+                     "e2e": {"value": cpu["value"], "unit": "updates/s", "h2d_bytes_per_step": 0,
+                             "d2h_bytes_per_step": 0}})
+        return base
+    work = tempfile.mkdtemp(prefix="gbte_ref_")
+    try:
+        deck.max_iter = w + k
+        deck.residual_temp = 0.0
+        deck.residual_flux = 0.0
+        deck.write(work)
+        t0 = time.perf_counter()
+        with open(os.path.join(work, "ref_run.log"), "w") as log:
+            subprocess.run([oracle.REF_BIN], cwd=work, stdout=log, stderr=subprocess.STDOUT, check=True,
+                           timeout=args.ref_timeout)
+        wall = time.perf_counter() - t0
+        with open(os.path.join(work, "ref_run.log")) as f:
+            inner = [float(line.split(":")[1].split()[0]) for line in f if "Time taken by inner loop" in line]
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    timed = inner[w:w + k] if len(inner) >= w + k else inner[-k:]
+    sec = float(np.mean(timed)) * 1e-3
+    value = upd / sec
+    base.update({"value": value, "ms_per_step": sec * 1e3,
+                 "cpu_baseline": {"value": value, "unit": "updates/s", "cores": 1, "kind": "reference",
+                                  "sample": f"{len(timed)} outer iteration(s) of the same deck after "
+                                            f"{w} warm-up; wall {wall:.1f} s incl. the reference's setup"},
+                 "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    return base
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
+    ap.add_argument("--workload", choices=["config2", "config1"], default="config2")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--max-iter-e2e", type=int, default=2000)
+    ap.add_argument("--ref-steps", type=int, default=2)
+    ap.add_argument("--ref-timeout", type=float, default=1500.0)
+    ap.add_argument("--no-fp64", dest="compare_fp64", action="store_false")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, rank)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        out = run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -64,7 +64,7 @@ class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("use_limiter", ctypes.c_int), ("max_iter", ctypes.c_int),
                 ("err_temp", ctypes.c_double), ("err_flux", ctypes.c_double), ("cell_heat", _c_dbl_p),
                 ("stream", ctypes.c_void_p), ("device", ctypes.c_int), ("verbose", ctypes.c_int),
-                ("macro_rtol", ctypes.c_double)]
+                ("macro_rtol", ctypes.c_double), ("profile", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -73,15 +73,40 @@ class Stats(ctypes.Structure):
                 ("macro_ms", ctypes.c_double), ("macro_cg_iterations", ctypes.c_longlong),
                 ("updates", ctypes.c_longlong), ("num_directions", ctypes.c_int), ("num_bands", ctypes.c_int),
                 ("num_cells", ctypes.c_int), ("max_levels", ctypes.c_int), ("lagged_faces", ctypes.c_int),
-                ("inner_iterations", ctypes.c_int)]
+                ("inner_iterations", ctypes.c_int), ("kernel_launches", ctypes.c_longlong),
+                ("kernel_ms", ctypes.c_double * 16), ("kernel_count", ctypes.c_longlong * 16)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("kernel_ms", "kernel_count")}
+        lib = library()
+        d["kernels"] = {}
+        for i in range(16):
+            name = lib.gbte_kernel_name(i)
+            if name is None:
+                break
+            if self.kernel_count[i]:
+                d["kernels"][name.decode()] = {"ms": self.kernel_ms[i], "launches": self.kernel_count[i]}
+        return d
+
+
+class DeckInfo(ctypes.Structure):
+    _fields_ = [("dimension", ctypes.c_int), ("num_nodes", ctypes.c_int), ("num_cells", ctypes.c_int),
+                ("num_faces", ctypes.c_int), ("num_boundaries", ctypes.c_int),
+                ("num_boundary_sides", ctypes.c_int), ("num_bands", ctypes.c_int),
+                ("num_directions", ctypes.c_int), ("num_materials", ctypes.c_int), ("max_levels", ctypes.c_int),
+                ("lagged_faces", ctypes.c_int), ("kappa_bulk", ctypes.c_double),
+                ("capacity_bulk", ctypes.c_double), ("total_volume", ctypes.c_double),
+                ("max_iter_or_zero", ctypes.c_double), ("err_temp", ctypes.c_double),
+                ("err_flux", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
-EXPORTS = ["gbte_default_options", "gbte_create", "gbte_create_from_deck", "gbte_set_initial",
+EXPORTS = ["gbte_inspect_deck", "gbte_inspect_mesh", "gbte_default_options", "gbte_create", "gbte_create_from_deck", "gbte_set_initial",
            "gbte_fourier_initial", "gbte_solve", "gbte_get_fields", "gbte_write_outputs", "gbte_get_sizes",
-           "gbte_get_geometry", "gbte_last_error", "gbte_status_string", "gbte_destroy"]
+           "gbte_get_geometry", "gbte_last_error", "gbte_status_string", "gbte_destroy", "gbte_kernel_name",
+           "gbte_solve_with"]
 
 _lib = None
 
@@ -97,6 +122,7 @@ def library():
         lib.gbte_last_error.restype = ctypes.c_char_p
         lib.gbte_last_error.argtypes = [ctypes.c_void_p]
         lib.gbte_status_string.restype = ctypes.c_char_p
+        lib.gbte_kernel_name.restype = ctypes.c_char_p
         lib.gbte_create.argtypes = [ctypes.POINTER(MeshView), ctypes.POINTER(BandTableC), ctypes.POINTER(BCTable),
                                     ctypes.POINTER(AngleSpec), ctypes.POINTER(Options),
                                     ctypes.POINTER(ctypes.c_void_p)]
@@ -104,12 +130,18 @@ def library():
                                               ctypes.POINTER(ctypes.c_void_p)]
         lib.gbte_set_initial.argtypes = [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, _c_dbl_p]
         lib.gbte_solve.argtypes = [ctypes.c_void_p, ctypes.POINTER(Stats)]
+        lib.gbte_solve_with.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                        ctypes.POINTER(Stats)]
         lib.gbte_get_fields.argtypes = [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, _c_dbl_p, _c_dbl_p]
         lib.gbte_write_outputs.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
         lib.gbte_get_sizes.argtypes = [ctypes.c_void_p] + [_c_int_p] * 4
         lib.gbte_get_geometry.argtypes = [ctypes.c_void_p, _c_dbl_p, _c_dbl_p]
         lib.gbte_destroy.argtypes = [ctypes.c_void_p]
         lib.gbte_fourier_initial.argtypes = [ctypes.c_void_p]
+        lib.gbte_inspect_deck.argtypes = [ctypes.c_char_p, ctypes.POINTER(DeckInfo)]
+        lib.gbte_inspect_mesh.argtypes = [ctypes.POINTER(MeshView), ctypes.POINTER(BandTableC),
+                                          ctypes.POINTER(BCTable), ctypes.POINTER(AngleSpec),
+                                          ctypes.POINTER(DeckInfo)]
         _lib = lib
     return _lib
 
@@ -163,49 +195,18 @@ class StaticBTESynthetic:
                   cell_heat: Optional[np.ndarray] = None, **opt) -> "StaticBTESynthetic":
         """Build from a :class:`giftbte_b200.decks.Deck` held in memory."""
         lib = library()
-        m = deck.mesh
-        nc = m.n_cells
-        nn = len(m.nodes)
-        xyz = np.zeros((nn, 3))
-        xyz[:, 0] = m.nodes[:, 0] * deck.scale[0]
-        xyz[:, 1] = m.nodes[:, 1] * deck.scale[1]
-        if m.nodes.shape[1] > 2:
-            xyz[:, 2] = m.nodes[:, 2] * (deck.scale[2] if len(deck.scale) > 2 else deck.scale[0])
-        cells = [np.asarray(c) for c in m.cells]
-        cptr = np.zeros(nc + 1, dtype=np.int32)
-        cptr[1:] = np.cumsum([len(c) for c in cells])
-        cverts = np.ascontiguousarray(np.concatenate(cells), dtype=np.int32)
-        creg = np.ascontiguousarray(m.cell_region, dtype=np.int32)
-        edges = np.asarray(m.edges)
-        nbe = len(edges)
-        bptr = (np.arange(nbe + 1) * edges.shape[1]).astype(np.int32)
-        bverts = np.ascontiguousarray(edges.ravel(), dtype=np.int32)
-        btag = np.ascontiguousarray(m.edge_tags, dtype=np.int32)
-        dim = 3 if (m.nodes.shape[1] > 2) else 2
-        mv = MeshView(dim, nn, nc, nbe, _ptr(xyz, ctypes.c_double), _ptr(cptr, ctypes.c_int),
-                      _ptr(cverts, ctypes.c_int), _ptr(creg, ctypes.c_int), _ptr(bptr, ctypes.c_int),
-                      _ptr(bverts, ctypes.c_int), _ptr(btag, ctypes.c_int), deck.scale[0], deck.scale[1],
-                      deck.scale[2] if len(deck.scale) > 2 else 1.0)
-        B = deck.bands
-        arrs = [np.ascontiguousarray(getattr(B, k), dtype=np.float64)
-                for k in ("v", "tau", "C", "lattice_ratio", "heat_ratio")]
-        reg = np.zeros(max(1, int(np.max(creg)) + 1), dtype=np.int32)
-        bt = BandTableC(1, B.n_bands, *[_ptr(a, ctypes.c_double) for a in arrs], len(reg),
-                        _ptr(reg, ctypes.c_int), deck.material_dim)
-        tags = np.asarray([b.tag for b in deck.bcs], dtype=np.int32)
-        types = np.asarray([b.type for b in deck.bcs], dtype=np.int32)
-        vals = np.asarray([b.value for b in deck.bcs], dtype=np.float64)
-        bc = BCTable(len(deck.bcs), _ptr(tags, ctypes.c_int), _ptr(types, ctypes.c_int), _ptr(vals, ctypes.c_double))
-        an = AngleSpec(deck.angle_method, deck.n_theta, deck.n_phi)
+        v = _views(deck)
+        nc = deck.mesh.n_cells
         if cell_heat is None and deck.heat_source is not None:
             cell_heat = np.full(nc, float(deck.heat_source))
         heat = np.ascontiguousarray(cell_heat, dtype=np.float64) if cell_heat is not None else None
-        o = default_options(precision, device=device, verbose=verbose, max_iter=deck.max_iter,
-                            err_temp=deck.residual_temp, err_flux=deck.residual_flux, **opt)
+        kw = {"max_iter": deck.max_iter, "err_temp": deck.residual_temp, "err_flux": deck.residual_flux}
+        kw.update(opt)
+        o = default_options(precision, device=device, verbose=verbose, **kw)
         o.cell_heat = _ptr(heat, ctypes.c_double)
         h = ctypes.c_void_p()
-        rc = lib.gbte_create(ctypes.byref(mv), ctypes.byref(bt), ctypes.byref(bc), ctypes.byref(an), ctypes.byref(o),
-                             ctypes.byref(h))
+        rc = lib.gbte_create(ctypes.byref(v["mv"]), ctypes.byref(v["bt"]), ctypes.byref(v["bc"]),
+                             ctypes.byref(v["an"]), ctypes.byref(o), ctypes.byref(h))
         if rc != GBTE_OK:
             raise GBTEError(rc, lib.gbte_last_error(None).decode())
         s = cls(h)
@@ -221,9 +222,18 @@ class StaticBTESynthetic:
         self._check(library().gbte_set_initial(self._h, _ptr(T0, ctypes.c_double), _ptr(q0, ctypes.c_double),
                                                _ptr(bt, ctypes.c_double)))
 
-    def solve(self, allow_not_converged: bool = True) -> dict:
+    def solve(self, max_iter: Optional[int] = None, err_temp: Optional[float] = None,
+              err_flux: Optional[float] = None, allow_not_converged: bool = True) -> dict:
+        """Outer source iteration from the current state (the reference's
+        solve(Use_Backup, Num_Max_Iter, Use_Limiter, error_temp_limit,
+        error_flux_limit)); limits default to the ones given at creation."""
         st = Stats()
-        rc = library().gbte_solve(self._h, ctypes.byref(st))
+        if max_iter is None and err_temp is None and err_flux is None:
+            rc = library().gbte_solve(self._h, ctypes.byref(st))
+        else:
+            rc = library().gbte_solve_with(self._h, int(max_iter if max_iter is not None else 10000),
+                                           float(err_temp if err_temp is not None else 0.0),
+                                           float(err_flux if err_flux is not None else 0.0), ctypes.byref(st))
         self.stats = st.as_dict()
         if rc == GBTE_ERR_NOT_CONVERGED and allow_not_converged:
             return self.stats
@@ -276,6 +286,67 @@ class StaticBTESynthetic:
     def _check(self, rc: int) -> None:
         if rc != GBTE_OK:
             raise GBTEError(rc, library().gbte_last_error(self._h).decode())
+
+
+def _views(deck) -> dict:
+    """C views of an in-memory deck; the returned dict keeps the arrays alive."""
+    m = deck.mesh
+    nc = m.n_cells
+    nn = len(m.nodes)
+    xyz = np.zeros((nn, 3))
+    xyz[:, 0] = m.nodes[:, 0] * deck.scale[0]
+    xyz[:, 1] = m.nodes[:, 1] * deck.scale[1]
+    if m.nodes.shape[1] > 2:
+        xyz[:, 2] = m.nodes[:, 2] * (deck.scale[2] if len(deck.scale) > 2 else deck.scale[0])
+    cells = [np.asarray(c) for c in m.cells]
+    cptr = np.zeros(nc + 1, dtype=np.int32)
+    cptr[1:] = np.cumsum([len(c) for c in cells])
+    cverts = np.ascontiguousarray(np.concatenate(cells), dtype=np.int32)
+    creg = np.ascontiguousarray(m.cell_region, dtype=np.int32)
+    edges = np.asarray(m.edges)
+    nbe = len(edges)
+    bptr = (np.arange(nbe + 1) * edges.shape[1]).astype(np.int32)
+    bverts = np.ascontiguousarray(edges.ravel(), dtype=np.int32)
+    btag = np.ascontiguousarray(m.edge_tags, dtype=np.int32)
+    dim = 3 if (m.nodes.shape[1] > 2) else 2
+    mv = MeshView(dim, nn, nc, nbe, _ptr(xyz, ctypes.c_double), _ptr(cptr, ctypes.c_int),
+                  _ptr(cverts, ctypes.c_int), _ptr(creg, ctypes.c_int), _ptr(bptr, ctypes.c_int),
+                  _ptr(bverts, ctypes.c_int), _ptr(btag, ctypes.c_int), deck.scale[0], deck.scale[1],
+                  deck.scale[2] if len(deck.scale) > 2 else 1.0)
+    B = deck.bands
+    arrs = [np.ascontiguousarray(getattr(B, k), dtype=np.float64)
+            for k in ("v", "tau", "C", "lattice_ratio", "heat_ratio")]
+    reg = np.zeros(max(1, int(np.max(creg)) + 1), dtype=np.int32)
+    bt = BandTableC(1, B.n_bands, *[_ptr(a, ctypes.c_double) for a in arrs], len(reg),
+                    _ptr(reg, ctypes.c_int), deck.material_dim)
+    tags = np.asarray([b.tag for b in deck.bcs], dtype=np.int32)
+    types = np.asarray([b.type for b in deck.bcs], dtype=np.int32)
+    vals = np.asarray([b.value for b in deck.bcs], dtype=np.float64)
+    bc = BCTable(len(deck.bcs), _ptr(tags, ctypes.c_int), _ptr(types, ctypes.c_int), _ptr(vals, ctypes.c_double))
+    an = AngleSpec(deck.angle_method, deck.n_theta, deck.n_phi)
+    return {"mv": mv, "bt": bt, "bc": bc, "an": an,
+            "keep": (xyz, cptr, cverts, creg, bptr, bverts, btag, arrs, reg, tags, types, vals)}
+
+
+def inspect(deck) -> dict:
+    """Host-only summary (no GPU) of what the solver would build for an
+    in-memory deck."""
+    v = _views(deck)
+    info = DeckInfo()
+    rc = library().gbte_inspect_mesh(ctypes.byref(v["mv"]), ctypes.byref(v["bt"]), ctypes.byref(v["bc"]),
+                                     ctypes.byref(v["an"]), ctypes.byref(info))
+    if rc != GBTE_OK:
+        raise GBTEError(rc, library().gbte_last_error(None).decode())
+    return info.as_dict()
+
+
+def inspect_deck(path: str) -> dict:
+    """Host-only summary of a deck directory (reads input/* like the reference)."""
+    info = DeckInfo()
+    rc = library().gbte_inspect_deck(path.encode(), ctypes.byref(info))
+    if rc != GBTE_OK:
+        raise GBTEError(rc, library().gbte_last_error(None).decode())
+    return info.as_dict()
 
 
 def effective_conductivity(q: np.ndarray, volumes: np.ndarray, length: float, delta_T: float, axis: int = 0) -> float:

@@ -11,6 +11,7 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <thread>
 
 #include "../../include/giftbte.h"
 #include "gbte_internal.h"
@@ -53,15 +54,8 @@ double now_ms() {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-int create_common(const gbte::RawMesh &raw, const gbte::Bands &bands_in, const gbte::BCs &bcs, const gbte_angle_spec &as,
-                  const gbte_options &opt, const std::vector<double> &cell_heat, gbte_handle **out) {
-    double t0 = now_ms();
-    std::unique_ptr<gbte_handle> h(new (std::nothrow) gbte_handle());
-    if (!h) {
-        g_create_error = "host allocation failed";
-        return GBTE_ERR_NOMEM;
-    }
-    gbte::Bands bands = bands_in;
+// kappa_bulk / capacity_bulk and the band-table checks of BTEBand.cpp:791-819
+int finish_bands(gbte::Bands &bands) {
     bands.kappa.assign(bands.nmat, 0.0);
     bands.capb.assign(bands.nmat, 0.0);
     for (int m = 0; m < bands.nmat; m++) {  // BTEBand.cpp:791-819
@@ -82,6 +76,20 @@ int create_common(const gbte::RawMesh &raw, const gbte::Bands &bands_in, const g
                 return fail(nullptr, {-1, "band heat capacity, group velocity and relaxation time must be positive"}),
                        GBTE_ERR_ARG;
     }
+    return GBTE_OK;
+}
+
+int create_common(const gbte::RawMesh &raw, const gbte::Bands &bands_in, const gbte::BCs &bcs, const gbte_angle_spec &as,
+                  const gbte_options &opt, const std::vector<double> &cell_heat, gbte_handle **out) {
+    double t0 = now_ms();
+    std::unique_ptr<gbte_handle> h(new (std::nothrow) gbte_handle());
+    if (!h) {
+        g_create_error = "host allocation failed";
+        return GBTE_ERR_NOMEM;
+    }
+    gbte::Bands bands = bands_in;
+    int brc = finish_bands(bands);
+    if (brc != GBTE_OK) return brc;
     gbte::Angles ang;
     gbte::Error e = gbte::make_angles(as.method, as.n_theta, as.n_phi, bands.material_dim, ang);
     if (e.code) return fail(nullptr, e), status_of(e.code);
@@ -96,6 +104,7 @@ int create_common(const gbte::RawMesh &raw, const gbte::Bands &bands_in, const g
     cfg.err_flux = opt.err_flux;
     cfg.macro_rtol = opt.macro_rtol > 0 ? opt.macro_rtol : 1e-13;
     cfg.verbose = opt.verbose;
+    cfg.profile = opt.profile;
     cfg.device = opt.device;
     cfg.stream = (cudaStream_t)opt.stream;
     if (opt.precision != GBTE_FP64 && opt.precision != GBTE_FP32_MIXED)
@@ -122,59 +131,134 @@ void gbte_default_options(gbte_options *o) {
     o->macro_rtol = 1e-13;
 }
 
+static int convert_views(const gbte_mesh_view *mv, const gbte_band_table *bt, const gbte_bc_table *bc,
+                         gbte::RawMesh &raw, gbte::Bands &B, gbte::BCs &bcs) {
+    if (mv->num_nodes <= 0 || mv->num_cells <= 0 || !mv->node_xyz || !mv->cell_ptr || !mv->cell_verts ||
+        !mv->cell_region || (mv->num_boundary_elements > 0 && (!mv->belem_ptr || !mv->belem_verts || !mv->belem_tag)))
+        return fail(nullptr, {-1, "incomplete mesh view"}), GBTE_ERR_ARG;
+    if (bt->num_materials <= 0 || bt->num_bands <= 0 || !bt->group_velocity || !bt->relaxation_time ||
+        !bt->heat_capacity || !bt->lattice_ratio || !bt->heat_ratio || bt->num_regions <= 0 || !bt->region_material)
+        return fail(nullptr, {-1, "incomplete band table"}), GBTE_ERR_ARG;
+    if (bc->num < 0 || (bc->num > 0 && (!bc->tag || !bc->type || !bc->value)))
+        return fail(nullptr, {-1, "incomplete BC table"}), GBTE_ERR_ARG;
+    raw.dim = mv->dimension;
+    raw.xyz.assign(mv->node_xyz, mv->node_xyz + 3 * (size_t)mv->num_nodes);
+    raw.cptr.assign(mv->cell_ptr, mv->cell_ptr + mv->num_cells + 1);
+    if (raw.cptr[0] != 0) return fail(nullptr, {-1, "cell_ptr must start at 0"}), GBTE_ERR_ARG;
+    for (int i = 0; i < mv->num_cells; i++)
+        if (raw.cptr[i + 1] < raw.cptr[i]) return fail(nullptr, {-1, "cell_ptr must be non-decreasing"}), GBTE_ERR_ARG;
+    raw.cverts.assign(mv->cell_verts, mv->cell_verts + raw.cptr.back());
+    raw.creg.assign(mv->cell_region, mv->cell_region + mv->num_cells);
+    raw.bptr.assign(1, 0);
+    if (mv->num_boundary_elements > 0) {
+        raw.bptr.assign(mv->belem_ptr, mv->belem_ptr + mv->num_boundary_elements + 1);
+        if (raw.bptr[0] != 0) return fail(nullptr, {-1, "belem_ptr must start at 0"}), GBTE_ERR_ARG;
+        for (int i = 0; i < mv->num_boundary_elements; i++)
+            if (raw.bptr[i + 1] < raw.bptr[i]) return fail(nullptr, {-1, "belem_ptr must be non-decreasing"}), GBTE_ERR_ARG;
+        raw.bverts.assign(mv->belem_verts, mv->belem_verts + raw.bptr.back());
+        raw.btag.assign(mv->belem_tag, mv->belem_tag + mv->num_boundary_elements);
+    }
+    raw.Lx = mv->scale_x > 0 ? mv->scale_x : 1.0;
+    raw.Ly = mv->scale_y;
+    raw.Lz = mv->scale_z;
+    B.nmat = bt->num_materials;
+    B.nb = bt->num_bands;
+    B.material_dim = bt->material_dimension;
+    size_t n = (size_t)B.nmat * B.nb;
+    B.v.assign(bt->group_velocity, bt->group_velocity + n);
+    B.tau.assign(bt->relaxation_time, bt->relaxation_time + n);
+    B.C.assign(bt->heat_capacity, bt->heat_capacity + n);
+    B.lat.assign(bt->lattice_ratio, bt->lattice_ratio + n);
+    B.hr.assign(bt->heat_ratio, bt->heat_ratio + n);
+    B.region_material.assign(bt->region_material, bt->region_material + bt->num_regions);
+    for (int r : B.region_material)
+        if (r < 0 || r >= B.nmat) return fail(nullptr, {-1, "region_material out of range"}), GBTE_ERR_ARG;
+    for (int i = 0; i < bc->num; i++) {
+        bcs.tag.push_back(bc->tag[i]);
+        bcs.type.push_back(bc->type[i]);
+        bcs.value.push_back(bc->value[i]);
+    }
+    return GBTE_OK;
+}
+
+// host-only build of everything gbte_create would put on the device
+static int inspect_common(const gbte::RawMesh &raw, const gbte::Bands &bands_in, const gbte::BCs &bcs,
+                          const gbte_angle_spec &as, gbte_deck_info *info) {
+    gbte::Bands bands = bands_in;
+    int brc = finish_bands(bands);
+    if (brc != GBTE_OK) return brc;
+    gbte::Angles ang;
+    gbte::Error e = gbte::make_angles(as.method, as.n_theta, as.n_phi, bands.material_dim, ang);
+    if (e.code) return fail(nullptr, e), status_of(e.code);
+    gbte::FlatMesh fm;
+    e = gbte::build_flat_mesh(raw, bcs, bands, fm);
+    if (e.code) return fail(nullptr, e), status_of(e.code);
+    gbte::Schedule sch;
+    gbte::build_schedule(fm, ang, sch, (int)std::max(1u, std::thread::hardware_concurrency()));
+    std::memset(info, 0, sizeof(*info));
+    info->dimension = fm.dim;
+    info->num_nodes = fm.nn;
+    info->num_cells = fm.nc;
+    info->num_faces = fm.nf();
+    info->num_boundaries = fm.nbd();
+    info->num_boundary_sides = fm.nbs();
+    info->num_bands = bands.nb;
+    info->num_directions = ang.nd;
+    info->num_materials = bands.nmat;
+    info->max_levels = sch.max_levels;
+    info->lagged_faces = sch.lagged_faces;
+    info->kappa_bulk = bands.kappa[0];
+    info->capacity_bulk = bands.capb[0];
+    for (double v : fm.vol) info->total_volume += v;
+    return GBTE_OK;
+}
+
+int gbte_inspect_mesh(const gbte_mesh_view *mv, const gbte_band_table *bt, const gbte_bc_table *bc,
+                      const gbte_angle_spec *as, gbte_deck_info *info) {
+    try {
+        if (!mv || !bt || !bc || !as || !info) return fail(nullptr, {-1, "null argument"}), GBTE_ERR_ARG;
+        gbte::RawMesh raw;
+        gbte::Bands B;
+        gbte::BCs bcs;
+        int rc = convert_views(mv, bt, bc, raw, B, bcs);
+        if (rc != GBTE_OK) return rc;
+        return inspect_common(raw, B, bcs, *as, info);
+    } catch (const std::exception &ex) {
+        g_create_error = ex.what();
+        return GBTE_ERR_ARG;
+    }
+}
+
+int gbte_inspect_deck(const char *dir, gbte_deck_info *info) {
+    try {
+        if (!dir || !info) return fail(nullptr, {-1, "null argument"}), GBTE_ERR_ARG;
+        gbte::Deck deck;
+        gbte::Error e = gbte::read_deck(dir, deck);
+        if (e.code) return fail(nullptr, e), status_of(e.code);
+        gbte_angle_spec as{deck.angle_method, deck.n_theta, deck.n_phi};
+        int rc = inspect_common(deck.mesh, deck.bands, deck.bcs, as, info);
+        if (rc == GBTE_OK) {
+            info->max_iter_or_zero = deck.max_iter;
+            info->err_temp = deck.err_temp;
+            info->err_flux = deck.err_flux;
+        }
+        return rc;
+    } catch (const std::exception &ex) {
+        g_create_error = ex.what();
+        return GBTE_ERR_ARG;
+    }
+}
+
 int gbte_create(const gbte_mesh_view *mv, const gbte_band_table *bt, const gbte_bc_table *bc, const gbte_angle_spec *as,
                 const gbte_options *opt, gbte_handle **out) {
     try {
         if (!mv || !bt || !bc || !as || !opt || !out) return fail(nullptr, {-1, "null argument"}), GBTE_ERR_ARG;
         *out = nullptr;
-        if (mv->num_nodes <= 0 || mv->num_cells <= 0 || !mv->node_xyz || !mv->cell_ptr || !mv->cell_verts ||
-            !mv->cell_region || (mv->num_boundary_elements > 0 && (!mv->belem_ptr || !mv->belem_verts || !mv->belem_tag)))
-            return fail(nullptr, {-1, "incomplete mesh view"}), GBTE_ERR_ARG;
-        if (bt->num_materials <= 0 || bt->num_bands <= 0 || !bt->group_velocity || !bt->relaxation_time ||
-            !bt->heat_capacity || !bt->lattice_ratio || !bt->heat_ratio || bt->num_regions <= 0 || !bt->region_material)
-            return fail(nullptr, {-1, "incomplete band table"}), GBTE_ERR_ARG;
-        if (bc->num < 0 || (bc->num > 0 && (!bc->tag || !bc->type || !bc->value)))
-            return fail(nullptr, {-1, "incomplete BC table"}), GBTE_ERR_ARG;
         gbte::RawMesh raw;
-        raw.dim = mv->dimension;
-        raw.xyz.assign(mv->node_xyz, mv->node_xyz + 3 * (size_t)mv->num_nodes);
-        raw.cptr.assign(mv->cell_ptr, mv->cell_ptr + mv->num_cells + 1);
-        if (raw.cptr[0] != 0) return fail(nullptr, {-1, "cell_ptr must start at 0"}), GBTE_ERR_ARG;
-        for (int i = 0; i < mv->num_cells; i++)
-            if (raw.cptr[i + 1] < raw.cptr[i]) return fail(nullptr, {-1, "cell_ptr must be non-decreasing"}), GBTE_ERR_ARG;
-        raw.cverts.assign(mv->cell_verts, mv->cell_verts + raw.cptr.back());
-        raw.creg.assign(mv->cell_region, mv->cell_region + mv->num_cells);
-        raw.bptr.assign(1, 0);
-        if (mv->num_boundary_elements > 0) {
-            raw.bptr.assign(mv->belem_ptr, mv->belem_ptr + mv->num_boundary_elements + 1);
-            if (raw.bptr[0] != 0) return fail(nullptr, {-1, "belem_ptr must start at 0"}), GBTE_ERR_ARG;
-            for (int i = 0; i < mv->num_boundary_elements; i++)
-                if (raw.bptr[i + 1] < raw.bptr[i]) return fail(nullptr, {-1, "belem_ptr must be non-decreasing"}), GBTE_ERR_ARG;
-            raw.bverts.assign(mv->belem_verts, mv->belem_verts + raw.bptr.back());
-            raw.btag.assign(mv->belem_tag, mv->belem_tag + mv->num_boundary_elements);
-        }
-        raw.Lx = mv->scale_x > 0 ? mv->scale_x : 1.0;
-        raw.Ly = mv->scale_y;
-        raw.Lz = mv->scale_z;
         gbte::Bands B;
-        B.nmat = bt->num_materials;
-        B.nb = bt->num_bands;
-        B.material_dim = bt->material_dimension;
-        size_t n = (size_t)B.nmat * B.nb;
-        B.v.assign(bt->group_velocity, bt->group_velocity + n);
-        B.tau.assign(bt->relaxation_time, bt->relaxation_time + n);
-        B.C.assign(bt->heat_capacity, bt->heat_capacity + n);
-        B.lat.assign(bt->lattice_ratio, bt->lattice_ratio + n);
-        B.hr.assign(bt->heat_ratio, bt->heat_ratio + n);
-        B.region_material.assign(bt->region_material, bt->region_material + bt->num_regions);
-        for (int r : B.region_material)
-            if (r < 0 || r >= B.nmat) return fail(nullptr, {-1, "region_material out of range"}), GBTE_ERR_ARG;
         gbte::BCs bcs;
-        for (int i = 0; i < bc->num; i++) {
-            bcs.tag.push_back(bc->tag[i]);
-            bcs.type.push_back(bc->type[i]);
-            bcs.value.push_back(bc->value[i]);
-        }
+        int rc = convert_views(mv, bt, bc, raw, B, bcs);
+        if (rc != GBTE_OK) return rc;
         std::vector<double> heat;
         if (opt->cell_heat) heat.assign(opt->cell_heat, opt->cell_heat + mv->num_cells);
         return create_common(raw, B, bcs, *as, *opt, heat, out);
@@ -271,6 +355,11 @@ int gbte_solve(gbte_handle *h, gbte_stats *st) {
             st->max_levels = h->solver.sched.max_levels;
             st->lagged_faces = h->solver.sched.lagged_faces;
             st->inner_iterations = s.inner_iterations;
+            st->kernel_launches = s.launches;
+            for (int k = 0; k < GBTE_NUM_KERNELS && k < gbte::K_NUM; k++) {
+                st->kernel_ms[k] = s.kernel_ms[k];
+                st->kernel_count[k] = s.kernel_count[k];
+            }
         }
         if (e.code) {
             if (e.code > 0) {
@@ -284,6 +373,20 @@ int gbte_solve(gbte_handle *h, gbte_stats *st) {
         h->err = ex.what();
         return GBTE_ERR_ARG;
     }
+}
+
+int gbte_solve_with(gbte_handle *h, int max_iter, double err_temp, double err_flux, gbte_stats *st) {
+    if (!h) return GBTE_ERR_ARG;
+    if (max_iter < 0 || !(err_temp >= 0) || !(err_flux >= 0)) return fail(h, {-1, "invalid solve limits"}), GBTE_ERR_ARG;
+    gbte::SolverConfig saved = h->solver.cfg;
+    h->solver.cfg.max_iter = max_iter;
+    h->solver.cfg.err_temp = err_temp;
+    h->solver.cfg.err_flux = err_flux;
+    int rc = gbte_solve(h, st);
+    h->solver.cfg.max_iter = saved.max_iter;
+    h->solver.cfg.err_temp = saved.err_temp;
+    h->solver.cfg.err_flux = saved.err_flux;
+    return rc;
 }
 
 int gbte_get_fields(gbte_handle *h, double *TE, double *TL, double *q, double *TB) {
@@ -374,6 +477,8 @@ int gbte_write_outputs(gbte_handle *h, const char *dir) {
     f.close();
     return GBTE_OK;
 }
+
+const char *gbte_kernel_name(int i) { return gbte::kernel_name(i); }
 
 const char *gbte_last_error(const gbte_handle *h) {
     if (!h) return g_create_error.c_str();

@@ -77,6 +77,35 @@ __global__ void k_init_eps(DMesh m, DPhys p, const double *__restrict__ T0, cons
     }
 }
 
+// eps += C_b (Tb_old - Tb_new): moves the base of the stored deviation to a
+// new per-cell temperature without changing e = C_b Tb + eps
+template <typename S>
+__global__ void k_rebase(DMesh m, DPhys p, const double *__restrict__ Tb_old, const double *__restrict__ Tb_new,
+                         S *__restrict__ eps) {
+    const size_t total = (size_t)p.nd * m.nc * p.nb;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b = (int)(t % p.nb);
+        const int c = (int)((t / p.nb) % m.nc);
+        eps[t] = (S)((double)eps[t] + p.C[b] * (Tb_old[c] - Tb_new[c]));
+    }
+}
+
+// least-squares gradient of a cell field with the same stencil
+__global__ void k_cell_lsq_grad(DMesh m, const double *__restrict__ T, double *__restrict__ g) {
+    const int c = (int)gtid();
+    if (c >= m.nc) return;
+    double gx = 0, gy = 0, gz = 0;
+    for (int q = m.nbr_ptr[c]; q < m.nbr_ptr[c + 1]; q++) {
+        const double de = T[m.nbr_idx[q]] - T[c];
+        gx += m.lsq_w[3 * q] * de;
+        gy += m.lsq_w[3 * q + 1] * de;
+        gz += m.lsq_w[3 * q + 2] * de;
+    }
+    g[3 * c] = gx;
+    g[3 * c + 1] = gy;
+    g[3 * c + 2] = gz;
+}
+
 // g[d][c][r][b] = sum_k w_ck (eps_k - eps_c)
 template <typename S>
 __global__ void k_gradient(DMesh m, DPhys p, const S *__restrict__ eps, S *__restrict__ g) {
@@ -706,6 +735,52 @@ __global__ void k_pcg(int n, const int *__restrict__ ptr, const int *__restrict_
 
 // ------------------------------------------------------------- host side --
 
+const char *kernel_name(int k) {
+    static const char *names[K_NUM] = {"gradient", "residual", "sweep", "bound_out", "moments", "side_moments",
+                                       "node_interp", "remacro", "gather", "macro_bc", "tinterp", "macro_rhs",
+                                       "pcg", "reduce", "copy", "init"};
+    return (k >= 0 && k < K_NUM) ? names[k] : nullptr;
+}
+
+void Solver::prof_begin(int id) {
+    launches_++;
+    if (!cfg.profile) return;
+    if ((int)pev_.size() < 2 * (pused_ + 1)) {
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        pev_.push_back(a);
+        pev_.push_back(b);
+        pid_.push_back(0);
+    }
+    pid_[pused_] = id;
+    cudaEventRecord(pev_[2 * pused_], cfg.stream);
+}
+
+void Solver::prof_end() {
+    if (!cfg.profile) return;
+    cudaEventRecord(pev_[2 * pused_ + 1], cfg.stream);
+    pused_++;
+}
+
+// call only after the stream has been synchronised
+void Solver::prof_collect(SolveStats &st) {
+    for (int i = 0; i < pused_; i++) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, pev_[2 * i], pev_[2 * i + 1]);
+        st.kernel_ms[pid_[i]] += ms;
+        st.kernel_count[pid_[i]]++;
+    }
+    pused_ = 0;
+}
+
+#define GL(id, ...)      \
+    do {                 \
+        prof_begin(id);  \
+        __VA_ARGS__;     \
+        prof_end();      \
+    } while (0)
+
 void *Solver::dalloc(size_t bytes) {
     void *p = nullptr;
     if (bytes == 0) bytes = 16;
@@ -1063,7 +1138,9 @@ Error Solver::macro_solve(double *x, const double *b, long long &iters) {
                     &cg_scal_, &rtol, &maxit, (void *)&nslots};
     int ns = nslots;
     args[14] = &ns;
-    CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_pcg, dim3(coop_blocks_), dim3(kThreads), args, 0, s));
+    cudaError_t lerr = cudaSuccess;
+    GL(K_PCG, lerr = cudaLaunchCooperativeKernel((void *)k_pcg, dim3(coop_blocks_), dim3(kThreads), args, 0, s));
+    CUDA_TRY(lerr);
     CUDA_TRY(cudaMemcpyAsync(h_pinned_ + 8, cg_scal_ + nslots - 1, 8, cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
     iters += (long long)h_pinned_[8];
@@ -1086,6 +1163,7 @@ Error Solver::solve_t(SolveStats &st) {
     const int nbc = std::min(nb, 8);
     const int sweep_blocks = nd * ((nb + nbc - 1) / nbc);
     auto moments = [&]() {
+        prof_begin(K_MOMENTS);
         switch (lpc) {
         case 1: k_moments<S, 1><<<gM, kThreads, 0, s>>>(dm_, dp_, eps, Tbase_, Tlat_, E_, q_, Tband_, Th_, Q_); break;
         case 2: k_moments<S, 2><<<gM, kThreads, 0, s>>>(dm_, dp_, eps, Tbase_, Tlat_, E_, q_, Tband_, Th_, Q_); break;
@@ -1094,16 +1172,17 @@ Error Solver::solve_t(SolveStats &st) {
         case 16: k_moments<S, 16><<<gM, kThreads, 0, s>>>(dm_, dp_, eps, Tbase_, Tlat_, E_, q_, Tband_, Th_, Q_); break;
         default: k_moments<S, 32><<<gM, kThreads, 0, s>>>(dm_, dp_, eps, Tbase_, Tlat_, E_, q_, Tband_, Th_, Q_); break;
         }
+        prof_end();
     };
     auto gather = [&]() {
         if (need_snapshot_) cudaMemcpyAsync(eb_snap_, eb_, (size_t)nd * nbs * nb * 8, cudaMemcpyDeviceToDevice, s);
-        k_gather<<<gB, kThreads, 0, s>>>(dm_, dp_, dif_w_, spec_src_, need_snapshot_ ? eb_snap_ : nullptr, eb_);
+        GL(K_GATHER, k_gather<<<gB, kThreads, 0, s>>>(dm_, dp_, dif_w_, spec_src_, need_snapshot_ ? eb_snap_ : nullptr, eb_));
     };
     if (!started_) {
         // _set_initial (:765-782) and the initial boundary values (StaticBTESyntheticSolver.cpp:45-62)
-        k_init_eps<S><<<gE, kThreads, 0, s>>>(dm_, dp_, T_, Tbase_, eps);
-        k_gradient<S><<<gE, kThreads, 0, s>>>(dm_, dp_, eps, g);
-        k_bound_out<S><<<gB, kThreads, 0, s>>>(dm_, dp_, ev, eb_);
+        GL(K_INIT, k_init_eps<S><<<gE, kThreads, 0, s>>>(dm_, dp_, T_, Tbase_, eps));
+        GL(K_GRADIENT, k_gradient<S><<<gE, kThreads, 0, s>>>(dm_, dp_, eps, g));
+        GL(K_BOUND_OUT, k_bound_out<S><<<gB, kThreads, 0, s>>>(dm_, dp_, ev, eb_));
         gather();
         CUDA_TRY(cudaGetLastError());
         started_ = true;
@@ -1111,6 +1190,8 @@ Error Solver::solve_t(SolveStats &st) {
     double errOld = 0, errOldq = 0;
     int errInc = 0;
     st = SolveStats();
+    launches_ = 0;
+    pused_ = 0;
     float ms_total = 0, ms_transport = 0, ms_macro = 0;
     int nt;
     bool converged = false;
@@ -1119,33 +1200,35 @@ Error Solver::solve_t(SolveStats &st) {
         // copy() (:2655-2690)
         CUDA_TRY(cudaMemcpyAsync(Told_, T_, nc * 8, cudaMemcpyDeviceToDevice, s));
         CUDA_TRY(cudaMemcpyAsync(qold_, q_, (size_t)nc * 24, cudaMemcpyDeviceToDevice, s));
-        k_gradient<S><<<gE, kThreads, 0, s>>>(dm_, dp_, eps, g);
-        k_residual<S><<<gE, kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, R);
-        k_sweep<S><<<sweep_blocks, kThreads, 0, s>>>(dm_, dp_, nbc, lvl_cells_, lvl_ptr_, dir_lvl_off_, lag_, R, eps);
-        k_bound_out<S><<<gB, kThreads, 0, s>>>(dm_, dp_, ev, eb_);
+        GL(K_GRADIENT, k_gradient<S><<<gE, kThreads, 0, s>>>(dm_, dp_, eps, g));
+        GL(K_RESIDUAL, k_residual<S><<<gE, kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, R));
+        GL(K_SWEEP, k_sweep<S><<<sweep_blocks, kThreads, 0, s>>>(dm_, dp_, nbc, lvl_cells_, lvl_ptr_, dir_lvl_off_, lag_, R, eps));
+        GL(K_BOUND_OUT, k_bound_out<S><<<gB, kThreads, 0, s>>>(dm_, dp_, ev, eb_));
         moments();
-        k_side_moments<<<gS, kThreads, 0, s>>>(dm_, dp_, eb_, Ths_, Qs_);
-        k_node_interp<<<gN, kThreads, 0, s>>>(dm_, Th_, Q_, Ths_, Qs_, ThV_, QV_);
-        k_remacro<<<gC, kThreads, 0, s>>>(dm_, Th_, Q_, Ths_, Qs_, ThV_, QV_, remacro_);
+        GL(K_SIDE_MOMENTS, k_side_moments<<<gS, kThreads, 0, s>>>(dm_, dp_, eb_, Ths_, Qs_));
+        GL(K_NODE_INTERP, k_node_interp<<<gN, kThreads, 0, s>>>(dm_, Th_, Q_, Ths_, Qs_, ThV_, QV_));
+        GL(K_REMACRO, k_remacro<<<gC, kThreads, 0, s>>>(dm_, Th_, Q_, Ths_, Qs_, ThV_, QV_, remacro_));
         gather();
-        k_macro_bc<<<gS, kThreads, 0, s>>>(dm_, dp_, eb_, bTovr_, bTm_);
+        GL(K_MACRO_BC, k_macro_bc<<<gS, kThreads, 0, s>>>(dm_, dp_, eb_, bTovr_, bTm_));
         CUDA_TRY(cudaGetLastError());
         CUDA_TRY(cudaEventRecord(ev_[1], s));
         // _marco_solution: Picard on the non-orthogonal correction
-        k_copy<<<gC, kThreads, 0, s>>>(Tlat_, T_, nc);
+        GL(K_COPY, k_copy<<<gC, kThreads, 0, s>>>(Tlat_, T_, nc));
         double internal = 1000, prev_internal = 0;
         int inner = 0, inner_inc = 0;
         while (internal > 1e-6) {
-            k_copy<<<gC, kThreads, 0, s>>>(T_, T1_, nc);
-            k_tinterp<<<gN, kThreads, 0, s>>>(dm_, T_, TV_);
-            k_macro_rhs<<<gC, kThreads, 0, s>>>(dm_, dp_.kappa, remacro_, bTm_, TV_, rhs_);
+            GL(K_COPY, k_copy<<<gC, kThreads, 0, s>>>(T_, T1_, nc));
+            GL(K_TINTERP, k_tinterp<<<gN, kThreads, 0, s>>>(dm_, T_, TV_));
+            GL(K_MACRO_RHS, k_macro_rhs<<<gC, kThreads, 0, s>>>(dm_, dp_.kappa, remacro_, bTm_, TV_, rhs_));
             CUDA_TRY(cudaGetLastError());
             Error e = macro_solve(T_, rhs_, st.cg_iterations);
+            prof_collect(st);
             if (e.code) return e;
             CUDA_TRY(cudaMemsetAsync(red_, 0, 8, s));
-            k_sqdiff<<<std::min(gC, 148), kThreads, 0, s>>>(nc, T1_, T_, red_);
+            GL(K_REDUCE, k_sqdiff<<<std::min(gC, 148), kThreads, 0, s>>>(nc, T1_, T_, red_));
             CUDA_TRY(cudaMemcpyAsync(h_pinned_, red_, 8, cudaMemcpyDeviceToHost, s));
             CUDA_TRY(cudaStreamSynchronize(s));
+            prof_collect(st);
             internal = h_pinned_[0] / nc;
             inner++;
             if (inner > 1 && internal > prev_internal) inner_inc++;
@@ -1158,10 +1241,11 @@ Error Solver::solve_t(SolveStats &st) {
         CUDA_TRY(cudaEventRecord(ev_[2], s));
         // margins
         CUDA_TRY(cudaMemsetAsync(red_, 0, 4 * 8, s));
-        k_margins<<<std::min(gC, 148), kThreads, 0, s>>>(nc, T_, Told_, q_, qold_, red_);
+        GL(K_REDUCE, k_margins<<<std::min(gC, 148), kThreads, 0, s>>>(nc, T_, Told_, q_, qold_, red_));
         CUDA_TRY(cudaMemcpyAsync(h_pinned_, red_, 4 * 8, cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaEventRecord(ev_[3], s));
         CUDA_TRY(cudaStreamSynchronize(s));
+            prof_collect(st);
         float a = 0, b2 = 0, c2 = 0;
         cudaEventElapsedTime(&a, ev_[0], ev_[1]);
         cudaEventElapsedTime(&b2, ev_[1], ev_[2]);
@@ -1187,16 +1271,29 @@ Error Solver::solve_t(SolveStats &st) {
             converged = true;
             break;
         }
+        // FP32 form: re-base the stored deviation on the current macro
+        // temperature after iterations 1, 2, 4, 8, 16 and every 16th after
+        if (sizeof(S) == 4) {
+            const int it1 = nt + 1;
+            if ((it1 & (it1 - 1)) == 0 || it1 % 16 == 0) {
+                GL(K_INIT, k_copy<<<gC, kThreads, 0, s>>>(Tbase_, T1_, nc));
+                GL(K_INIT, k_copy<<<gC, kThreads, 0, s>>>(T_, Tbase_, nc));
+                GL(K_INIT, k_rebase<S><<<gE, kThreads, 0, s>>>(dm_, dp_, T1_, Tbase_, eps));
+                GL(K_INIT, k_cell_lsq_grad<<<gC, kThreads, 0, s>>>(dm_, Tbase_, gTb_));
+            }
+        }
         if (errInc >= 10) {
             st.solve_ms = ms_total;
             st.transport_ms = ms_transport;
             st.macro_ms = ms_macro;
+            st.launches = launches_;
             return {-4, "margins increased 10 times in a row or became NaN/Inf"};
         }
     }
     st.solve_ms = ms_total;
     st.transport_ms = ms_transport;
     st.macro_ms = ms_macro;
+    st.launches = launches_;
     if (!converged) return {1, "maximum number of iterations reached"};
     return {0, ""};
 }

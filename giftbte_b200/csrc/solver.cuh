@@ -45,15 +45,24 @@ struct SolverConfig {
     double err_temp = 1e-6, err_flux = 1e-4;
     double macro_rtol = 1e-13;
     int verbose = 0;
+    int profile = 0;
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
 };
 
+enum KernelId {
+    K_GRADIENT = 0, K_RESIDUAL, K_SWEEP, K_BOUND_OUT, K_MOMENTS, K_SIDE_MOMENTS, K_NODE_INTERP, K_REMACRO,
+    K_GATHER, K_MACRO_BC, K_TINTERP, K_MACRO_RHS, K_PCG, K_REDUCE, K_COPY, K_INIT, K_NUM
+};
+const char *kernel_name(int k);
+
 struct SolveStats {
     int iterations = 0, inner_iterations = 0;
     double err_temp = 0, err_flux = 0, solve_ms = 0, transport_ms = 0, macro_ms = 0;
-    long long cg_iterations = 0, updates = 0;
+    long long cg_iterations = 0, updates = 0, launches = 0;
+    double kernel_ms[K_NUM] = {0};
+    long long kernel_count[K_NUM] = {0};
 };
 
 class Solver {
@@ -106,6 +115,14 @@ private:
     bool started_ = false;
     int coop_blocks_ = 0;
     cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+    // per-launch profiling (options.profile)
+    std::vector<cudaEvent_t> pev_;
+    std::vector<int> pid_;
+    int pused_ = 0;
+    void prof_begin(int id);
+    void prof_end();
+    void prof_collect(SolveStats &st);
+    long long launches_ = 0;
 };
 
 }  // namespace gbte

@@ -166,7 +166,10 @@ def porous_cell_mesh(h: float, pores: Sequence[Tuple[float, float, float]], seed
                      side: float = 1.0) -> Mesh2D:
     """Periodic square cell [0,side]^2 with circular pores (cx, cy, r), all
     in unit coordinates, meshed as a Delaunay triangulation of Poisson-disk
-    interior points plus evenly spaced boundary points.
+    interior points plus evenly spaced boundary points. ``h`` is the target
+    mean edge length: boundary points are h apart and the Poisson-disk
+    minimum distance is h / 1.5 (the mean Delaunay edge of a maximal
+    Poisson-disk sample is about 1.5 times its minimum distance).
 
     The x- and y-faces carry identical node positions (translation-matched),
     which the reference's nearest-face-centre periodic pairing needs
@@ -187,7 +190,7 @@ def porous_cell_mesh(h: float, pores: Sequence[Tuple[float, float, float]], seed
         t = np.arange(m) * 2 * np.pi / m
         pore_pts.append(np.stack([cx + r * np.cos(t), cy + r * np.sin(t)], axis=1))
 
-    margin = 0.6 * h
+    margin = 0.5 * h
 
     def inside(p):
         if p[0] < margin or p[0] > side - margin or p[1] < margin or p[1] > side - margin:
@@ -197,7 +200,7 @@ def porous_cell_mesh(h: float, pores: Sequence[Tuple[float, float, float]], seed
                 return False
         return True
 
-    ipts = _poisson_disk(rng, h, inside, ((0.0, 0.0), (side, side)))
+    ipts = _poisson_disk(rng, h / 1.5, inside, ((0.0, 0.0), (side, side)))
     pts = np.concatenate([np.asarray(bpts)] + pore_pts + [ipts], axis=0)
     tri = Delaunay(pts)
     simp = tri.simplices

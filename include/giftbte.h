@@ -124,7 +124,10 @@ typedef struct {
     int device;               /* CUDA device ordinal */
     int verbose;              /* 1: print the per-iteration margins like the reference */
     double macro_rtol;        /* relative residual of the macro CG solve; 0 = default 1e-13 */
+    int profile;              /* 1: time every kernel launch with CUDA events (gbte_stats.kernel_ms) */
 } gbte_options;
+
+#define GBTE_NUM_KERNELS 16
 
 typedef struct {
     int iterations;
@@ -142,7 +145,38 @@ typedef struct {
     int max_levels;           /* deepest sweep over all directions */
     int lagged_faces;         /* upwind faces lagged to break cycles (3D) */
     int inner_iterations;     /* macro Picard steps in the last outer iteration */
+    long long kernel_launches;            /* kernels launched by this solve */
+    double kernel_ms[GBTE_NUM_KERNELS];   /* per-kernel device time when options.profile = 1 */
+    long long kernel_count[GBTE_NUM_KERNELS];
 } gbte_stats;
+
+/* Name of kernel slot i of gbte_stats.kernel_ms (NULL past the last one). */
+const char *gbte_kernel_name(int i);
+
+/* Host-only summary of a deck or mesh (no CUDA needed): what gbte_create
+ * would build. Replaces the reference's stdout trace of the input stage. */
+typedef struct {
+    int dimension;
+    int num_nodes;
+    int num_cells;
+    int num_faces;             /* global face list (Element_Faces) */
+    int num_boundaries;        /* boundary elements matched to the BC table */
+    int num_boundary_sides;    /* 2 * num_boundaries */
+    int num_bands;
+    int num_directions;
+    int num_materials;
+    int max_levels;            /* deepest upwind sweep over all directions */
+    int lagged_faces;          /* upwind faces lagged to break cycles */
+    double kappa_bulk;         /* material 0 */
+    double capacity_bulk;      /* material 0 */
+    double total_volume;
+    double max_iter_or_zero;   /* MaxNumIter from CONTROL (decks only) */
+    double err_temp, err_flux; /* ResidualTemp / ResidualFlux from CONTROL (decks only) */
+} gbte_deck_info;
+
+int gbte_inspect_deck(const char *dir, gbte_deck_info *info);
+int gbte_inspect_mesh(const gbte_mesh_view *mesh, const gbte_band_table *bands, const gbte_bc_table *bcs,
+                      const gbte_angle_spec *angles, gbte_deck_info *info);
 
 /* Default options (FP64, max_iter 10000, margins 1e-6/1e-4 as the reference). */
 void gbte_default_options(gbte_options *opt);
@@ -169,6 +203,13 @@ int gbte_fourier_initial(gbte_handle *h);
  * (GBTE_OK), max_iter is reached (GBTE_ERR_NOT_CONVERGED) or it diverges.
  * stats may be NULL. */
 int gbte_solve(gbte_handle *h, gbte_stats *stats);
+
+/* gbte_solve with the per-call limits of the reference's
+ * solve(Use_Backup, Num_Max_Iter, Use_Limiter, error_temp_limit,
+ * error_flux_limit): runs at most max_iter further outer iterations from the
+ * current state and stops when both margins are at or below the limits
+ * (limits of 0 run exactly max_iter iterations). */
+int gbte_solve_with(gbte_handle *h, int max_iter, double err_temp, double err_flux, gbte_stats *stats);
 
 /* Result fields (any pointer may be NULL):
  * T_energy [Nc]  totalEnergy      -> Temperature.dat

@@ -1,0 +1,107 @@
+"""The C ABI: symbols, host-only inspection and error behaviour (no GPU)."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import giftbte_b200 as g
+from giftbte_b200 import decks
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    with open(os.path.join(ROOT, "include", "giftbte.h")) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"\b(gbte_[a-z_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = g.library()
+    names = declared_symbols()
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert sorted(g.EXPORTS) == names
+
+
+def test_status_strings():
+    lib = g.library()
+    for code in (0, -1, -2, -3, -4, -5, -6, -7, -8, 1):
+        assert lib.gbte_status_string(code).decode() != "unknown status"
+
+
+def test_inspect_gray_square():
+    info = g.inspect(decks.config1_deck(40))
+    assert info["num_cells"] == 3200 and info["num_nodes"] == 1681
+    assert info["num_faces"] == 3 * 3200 // 2 + 160 // 2
+    assert info["num_boundaries"] == 160 and info["num_boundary_sides"] == 320
+    assert info["num_directions"] == 32 and info["num_bands"] == 1
+    assert info["lagged_faces"] == 0 and info["max_levels"] > 40
+    assert info["kappa_bulk"] == pytest.approx(1.66e6 * 6400.0 ** 2 * (1e-7 / 6400.0) / 2, rel=1e-14)
+    assert info["total_volume"] == pytest.approx(1e-12, rel=1e-12)
+
+
+@pytest.mark.parametrize("fmt", ["COMSOL", "MSH"])
+def test_deck_files_round_trip(tmp_path, fmt):
+    d = decks.config2_deck(h_nm=15.0, n_bands=5, n_phi=4, mesh_format=fmt)
+    d.write(str(tmp_path))
+    a = g.inspect(d)
+    b = g.inspect_deck(str(tmp_path))
+    for k in ("num_cells", "num_nodes", "num_faces", "num_boundaries", "num_bands", "num_directions", "max_levels"):
+        assert a[k] == b[k], k
+    assert b["kappa_bulk"] == pytest.approx(a["kappa_bulk"], rel=1e-15)
+    assert b["total_volume"] == pytest.approx(a["total_volume"], rel=1e-12)
+    # annulus area: 300 nm square minus a polygonal r = 100 nm pore
+    assert b["total_volume"] == pytest.approx((300e-9) ** 2 - np.pi * (100e-9) ** 2, rel=2e-3)
+    assert b["err_temp"] == d.residual_temp
+
+
+@pytest.mark.parametrize("method,dim,nt,nphi,nd", [(1, 2, 4, 8, 32), (2, 2, 4, 16, 64), (1, 3, 2, 2, 32),
+                                                   (2, 3, 4, 4, 128)])
+def test_quadrature_sizes(method, dim, nt, nphi, nd):
+    d = decks.config1_deck(4, angle_method=method, material_dim=dim, n_theta=nt, n_phi=nphi)
+    assert g.inspect(d)["num_directions"] == nd
+
+
+def test_missing_deck_is_io_error(tmp_path):
+    with pytest.raises(g.GBTEError) as e:
+        g.inspect_deck(str(tmp_path / "nope"))
+    assert e.value.status == -2
+
+
+def test_periodic_without_partner_is_mesh_error():
+    d = decks.config1_deck(6)
+    d.bcs = [decks.BC(1, -7, 1.0), decks.BC(2, 1, 0.0), decks.BC(3, 2, 0.0), decks.BC(4, 2, 0.0)]
+    with pytest.raises(g.GBTEError) as e:
+        g.inspect(d)
+    assert e.value.status == -7
+
+
+def test_bad_lattice_ratio_is_argument_error():
+    d = decks.config1_deck(6)
+    d.bands.lattice_ratio = d.bands.lattice_ratio * 0.5
+    with pytest.raises(g.GBTEError) as e:
+        g.inspect(d)
+    assert e.value.status == -1
+
+
+def test_interface_boundary_is_unsupported(tmp_path):
+    d = decks.config1_deck(6)
+    d.write(str(tmp_path))
+    with open(tmp_path / "input" / "bc.dat", "w") as f:
+        f.write("1 #n\n\nheader\n1 5 0 input/trans.dat\n")
+    with pytest.raises(g.GBTEError) as e:
+        g.inspect_deck(str(tmp_path))
+    assert e.value.status == -8
+
+
+def test_create_without_device_fails_cleanly():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(g.GBTEError) as e:
+        g.StaticBTESynthetic.from_deck(decks.config1_deck(4))
+    assert e.value.status == -3
