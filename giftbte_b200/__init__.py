@@ -222,6 +222,11 @@ class StaticBTESynthetic:
         self._check(library().gbte_set_initial(self._h, _ptr(T0, ctypes.c_double), _ptr(q0, ctypes.c_double),
                                                _ptr(bt, ctypes.c_double)))
 
+    def fourier_initial(self) -> None:
+        """Replace the initial field by the Fourier pre-solve (kappa_bulk) the
+        reference runs before the BTE (StaticFourier::_solve)."""
+        self._check(library().gbte_fourier_initial(self._h))
+
     def solve(self, max_iter: Optional[int] = None, err_temp: Optional[float] = None,
               err_flux: Optional[float] = None, allow_not_converged: bool = True) -> dict:
         """Outer source iteration from the current state (the reference's

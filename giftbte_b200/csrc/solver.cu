@@ -39,6 +39,7 @@
 #include <cstring>
 #include <limits>
 #include <thread>
+#include <type_traits>
 
 #include "solver.cuh"
 
@@ -55,8 +56,15 @@ namespace gbte {
 namespace {
 
 constexpr int kThreads = 256;
+// residual reduction required of a macro CG solve that starts from the
+// previous outer iteration's solution of the same Picard step
+constexpr double kWarmEta = 1e-6;
 
 __device__ __forceinline__ size_t gtid() { return blockIdx.x * (size_t)blockDim.x + threadIdx.x; }
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
 __device__ __forceinline__ size_t gstride() { return (size_t)gridDim.x * blockDim.x; }
 
 int grid_for(size_t total, int threads = kThreads) {
@@ -106,33 +114,36 @@ __global__ void k_cell_lsq_grad(DMesh m, const double *__restrict__ T, double *_
     g[3 * c + 2] = gz;
 }
 
-// g[d][c][r][b] = sum_k w_ck (eps_k - eps_c)
-template <typename S>
-__global__ void k_gradient(DMesh m, DPhys p, const S *__restrict__ eps, S *__restrict__ g) {
+// g[d][c][r][b] = sum_k w_ck (eps_k - eps_c), r < DIM (weights in the
+// storage precision; lanes of a warp share the cell, so the stencil loads
+// are broadcasts and the neighbour loads are coalesced over bands)
+template <typename S, int DIM>
+__global__ void __launch_bounds__(256) k_gradient(DMesh m, DPhys p, const S *__restrict__ w, const S *__restrict__ eps,
+                                                  S *__restrict__ g) {
     const int nb = p.nb, nc = m.nc;
     const size_t total = (size_t)p.nd * nc * nb;
     for (size_t t = gtid(); t < total; t += gstride()) {
         const int b = (int)(t % nb);
         const size_t dc = t / nb;
         const int c = (int)(dc % nc);
-        const S *ed = eps + (dc - c) * nb;
-        const S ec = ed[(size_t)c * nb + b];
+        const S *ed = eps + (dc - c) * nb + b;
+        const S ec = ed[(size_t)c * nb];
         S gx = 0, gy = 0, gz = 0;
         const int q1 = m.nbr_ptr[c + 1];
         for (int q = m.nbr_ptr[c]; q < q1; q++) {
-            const S de = ed[(size_t)m.nbr_idx[q] * nb + b] - ec;
-            gx += (S)m.lsq_w[3 * q] * de;
-            gy += (S)m.lsq_w[3 * q + 1] * de;
-            gz += (S)m.lsq_w[3 * q + 2] * de;
+            const S de = ed[(size_t)m.nbr_idx[q] * nb] - ec;
+            gx += w[3 * q] * de;
+            gy += w[3 * q + 1] * de;
+            if (DIM == 3) gz += w[3 * q + 2] * de;
         }
-        S *gp = g + dc * 3 * nb + b;
+        S *gp = g + dc * DIM * nb + b;
         gp[0] = gx;
         gp[nb] = gy;
-        gp[2 * nb] = gz;
+        if (DIM == 3) gp[2 * nb] = gz;
     }
 }
 
-template <typename S>
+template <typename S, int DIM>
 struct EView {
     const S *eps, *g;
     const double *Tb, *gTb;
@@ -141,16 +152,20 @@ struct EView {
         return Cb * Tb[c] + (double)eps[(d * nc + c) * nb + b];
     }
     __device__ __forceinline__ double gdot(size_t d, int c, int b, double Cb, double rx, double ry, double rz) const {
-        const S *gp = g + (d * nc + c) * 3 * nb + b;
-        return ((double)gp[0] + Cb * gTb[3 * c]) * rx + ((double)gp[nb] + Cb * gTb[3 * c + 1]) * ry +
-               ((double)gp[2 * nb] + Cb * gTb[3 * c + 2]) * rz;
+        const S *gp = g + (d * nc + c) * DIM * nb + b;
+        double v = ((double)gp[0] + Cb * gTb[3 * c]) * rx + ((double)gp[nb] + Cb * gTb[3 * c + 1]) * ry;
+        if (DIM == 3) v += ((double)gp[2 * nb] + Cb * gTb[3 * c + 2]) * rz;
+        return v;
     }
 };
 
-// R = C_b T_old + Q hr tau - e - sum_f tau (v.n) A/V x_f  (second-order upwind x_f)
-template <typename S>
-__global__ void k_residual(DMesh m, DPhys p, EView<S> ev, const double *__restrict__ Told, const double *__restrict__ eb,
-                           S *__restrict__ R) {
+// R = C_b T_old + Q hr tau - e - sum_f tau (v.n) A/V x_f  (second-order upwind
+// x_f), written in the direction's level order Rlo[d][pos][b] so that the
+// sweep reads each level as one contiguous block
+template <typename S, int DIM>
+__global__ void __launch_bounds__(256) k_residual(DMesh m, DPhys p, EView<S, DIM> ev, const double *__restrict__ Told,
+                                                  const double *__restrict__ eb, const int *__restrict__ pos_of,
+                                                  S *__restrict__ Rlo) {
     const int nb = p.nb, nc = m.nc;
     const size_t total = (size_t)p.nd * nc * nb;
     for (size_t t = gtid(); t < total; t += gstride()) {
@@ -161,11 +176,10 @@ __global__ void k_residual(DMesh m, DPhys p, EView<S> ev, const double *__restri
         const double Cb = p.C[b], tau = p.tau[b], vm = p.vmag[b];
         const double vx = vm * p.sx[d], vy = vm * p.sy[d], vz = vm * p.sz[d];
         const double ec = ev.e(d, c, b, Cb);
-        const double cx = m.cx[c], cy = m.cy[c], cz = m.cz[c], vol = m.vol[c];
+        const double cx = m.cx[c], cy = m.cy[c], cz = m.cz[c], tv = tau / m.vol[c];
         double acc = 0;
         for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
-            const double vn = vx * m.cf_nx[k] + vy * m.cf_ny[k] + vz * m.cf_nz[k];
-            const double temp = tau * m.cf_area[k] / vol * vn;
+            const double vn = vx * m.cf_nx[k] + vy * m.cf_ny[k] + (DIM == 3 ? vz * m.cf_nz[k] : vz * 0.0);
             double x;
             if (vn >= 0) {
                 x = ec + ev.gdot(d, c, b, Cb, m.cf_fx[k] - cx, m.cf_fy[k] - cy, m.cf_fz[k] - cz);
@@ -175,61 +189,330 @@ __global__ void k_residual(DMesh m, DPhys p, EView<S> ev, const double *__restri
             } else {
                 x = eb[(d * m.nbs + m.cf_bside[k]) * nb + b];
             }
-            acc += temp * x;
+            acc += tv * m.cf_area[k] * vn * x;
         }
         const double r = Cb * Told[c] + m.heat[c] * p.hr[b] * tau - ec - acc;
-        R[t] = (S)r;
+        Rlo[(d * nc + pos_of[dc]) * nb + b] = (S)r;
     }
 }
 
-// Level-scheduled upwind sweep: one CTA per (direction, band chunk). Cells
-// of a level depend only on cells of earlier levels of the same direction,
-// so a __syncthreads between levels orders the whole sweep. R is
-// overwritten in place by the correction d, and eps += d.
-template <typename S>
-__global__ void __launch_bounds__(256) k_sweep(DMesh m, DPhys p, int nbc, const int *__restrict__ lvl_cells,
-                                               const int *__restrict__ lvl_ptr, const int *__restrict__ dir_lvl_off,
-                                               const unsigned char *__restrict__ lag, S *R, S *eps) {
-    const int nb = p.nb, nc = m.nc;
-    const int nchunks = (nb + nbc - 1) / nbc;
+// ---- band-vector forms (band count a multiple of BC = 4) ----
+// One thread per (direction, cell, BC consecutive bands): the cell's geometry
+// and stencil are loaded once for BC bands and the band values move as
+// 16-byte vectors.
+template <typename S, int BC>
+__device__ __forceinline__ void ld8(const S *p, S (&v)[BC]) {
+    if (sizeof(S) == 4) {
+#pragma unroll
+        for (int h = 0; h < BC / 4; h++) {
+            const float4 a = reinterpret_cast<const float4 *>(p)[h];
+            v[4 * h] = a.x, v[4 * h + 1] = a.y, v[4 * h + 2] = a.z, v[4 * h + 3] = a.w;
+        }
+    } else {
+        const double2 *q = reinterpret_cast<const double2 *>(p);
+#pragma unroll
+        for (int i = 0; i < BC / 2; i++) {
+            const double2 t = q[i];
+            v[2 * i] = t.x;
+            v[2 * i + 1] = t.y;
+        }
+    }
+}
+template <typename S, int BC>
+__device__ __forceinline__ void st8(S *p, const S (&v)[BC]) {
+    if (sizeof(S) == 4) {
+#pragma unroll
+        for (int h = 0; h < BC / 4; h++)
+            reinterpret_cast<float4 *>(p)[h] = make_float4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
+    } else {
+        double2 *q = reinterpret_cast<double2 *>(p);
+#pragma unroll
+        for (int i = 0; i < BC / 2; i++) q[i] = make_double2(v[2 * i], v[2 * i + 1]);
+    }
+}
+
+template <typename S, int DIM, int BC>
+__global__ void __launch_bounds__(256) k_gradient8(DMesh m, DPhys p, const S *__restrict__ w, const S *__restrict__ eps,
+                                                   S *__restrict__ g) {
+    const int nb = p.nb, nc = m.nc, nbc = nb / BC;
+    const size_t total = (size_t)p.nd * nc * nbc;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int bc = (int)(t % nbc);
+        const size_t dc = t / nbc;
+        const int c = (int)(dc % nc);
+        const S *ed = eps + (dc - c) * nb + BC * bc;
+        S ec[BC], ek[BC], gx[BC], gy[BC], gz[BC];
+        ld8(ed + (size_t)c * nb, ec);
+#pragma unroll
+        for (int i = 0; i < BC; i++) gx[i] = gy[i] = gz[i] = 0;
+        const int q1 = m.nbr_ptr[c + 1];
+        for (int q = m.nbr_ptr[c]; q < q1; q++) {
+            ld8(ed + (size_t)m.nbr_idx[q] * nb, ek);
+            const S wx = w[3 * q], wy = w[3 * q + 1], wz = DIM == 3 ? w[3 * q + 2] : S(0);
+#pragma unroll
+            for (int i = 0; i < BC; i++) {
+                const S de = ek[i] - ec[i];
+                gx[i] += wx * de;
+                gy[i] += wy * de;
+                if (DIM == 3) gz[i] += wz * de;
+            }
+        }
+        S *gp = g + dc * DIM * nb + BC * bc;
+        st8(gp, gx);
+        st8(gp + nb, gy);
+        if (DIM == 3) st8(gp + 2 * nb, gz);
+    }
+}
+
+// Residual, BC bands per thread. The upwind side of a face is chosen by the
+// sign of s.n (shared by all bands; the reference's (|v| s).n differs from it
+// only by rounding when the face is tangent to the direction, where the
+// flux coefficient is zero).
+template <typename S, int DIM, int BC>
+__global__ void __launch_bounds__(256) k_residual8(DMesh m, DPhys p, EView<S, DIM> ev, const double *__restrict__ Told,
+                                                   const double *__restrict__ eb, const int *__restrict__ pos_of,
+                                                   S *__restrict__ Rlo) {
+    const int nb = p.nb, nc = m.nc, nbc = nb / BC;
+    const size_t total = (size_t)p.nd * nc * nbc;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int bc = (int)(t % nbc), b0 = BC * bc;
+        const size_t dc = t / nbc;
+        const int c = (int)(dc % nc);
+        const size_t d = dc / nc;
+        const double sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
+        const size_t dbase = d * nc;
+        double Cb[BC], tv[BC], acc[BC], ec[BC];
+        S v[BC], gxv[BC], gyv[BC], gzv[BC];
+        const double invV = 1.0 / m.vol[c];
+        {
+            ld8(ev.eps + (dbase + c) * nb + b0, v);
+            const double tb = ev.Tb[c];
+#pragma unroll
+            for (int i = 0; i < BC; i++) {
+                Cb[i] = p.C[b0 + i];
+                tv[i] = p.tau[b0 + i] * p.vmag[b0 + i];
+                ec[i] = Cb[i] * tb + (double)v[i];
+                acc[i] = 0;
+            }
+        }
+        const double gbx = ev.gTb[3 * c], gby = ev.gTb[3 * c + 1], gbz = ev.gTb[3 * c + 2];
+        bool have_gc = false;
+        for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+            const double sn = sx * m.cf_nx[k] + sy * m.cf_ny[k] + (DIM == 3 ? sz * m.cf_nz[k] : 0.0);
+            const double a = m.cf_area[k] * invV * sn;
+            if (sn >= 0) {
+                if (!have_gc) {
+                    const S *gp = ev.g + (dbase + c) * DIM * nb + b0;
+                    ld8(gp, gxv);
+                    ld8(gp + nb, gyv);
+                    if (DIM == 3) ld8(gp + 2 * nb, gzv);
+                    have_gc = true;
+                }
+                const double rx = m.cf_fx[k] - m.cx[c], ry = m.cf_fy[k] - m.cy[c], rz = m.cf_fz[k] - m.cz[c];
+#pragma unroll
+                for (int i = 0; i < BC; i++) {
+                    double x = ec[i] + ((double)gxv[i] + Cb[i] * gbx) * rx + ((double)gyv[i] + Cb[i] * gby) * ry;
+                    if (DIM == 3) x += ((double)gzv[i] + Cb[i] * gbz) * rz;
+                    acc[i] += tv[i] * a * x;
+                }
+            } else if (m.cf_bound[k] < 0) {
+                const int j = m.cf_nbr[k];
+                S ej[BC], hx[BC], hy[BC], hz[BC];
+                ld8(ev.eps + (dbase + j) * nb + b0, ej);
+                const S *gp = ev.g + (dbase + j) * DIM * nb + b0;
+                ld8(gp, hx);
+                ld8(gp + nb, hy);
+                if (DIM == 3) ld8(gp + 2 * nb, hz);
+                const double tj = ev.Tb[j], jx = ev.gTb[3 * j], jy = ev.gTb[3 * j + 1], jz = ev.gTb[3 * j + 2];
+                const double rx = m.cf_fx[k] - m.cx[j], ry = m.cf_fy[k] - m.cy[j], rz = m.cf_fz[k] - m.cz[j];
+#pragma unroll
+                for (int i = 0; i < BC; i++) {
+                    double x = Cb[i] * tj + (double)ej[i] + ((double)hx[i] + Cb[i] * jx) * rx + ((double)hy[i] + Cb[i] * jy) * ry;
+                    if (DIM == 3) x += ((double)hz[i] + Cb[i] * jz) * rz;
+                    acc[i] += tv[i] * a * x;
+                }
+            } else {
+                const double *e = eb + (d * m.nbs + m.cf_bside[k]) * nb + b0;
+#pragma unroll
+                for (int i = 0; i < BC; i++) acc[i] += tv[i] * a * e[i];
+            }
+        }
+        const double To = Told[c], hc = m.heat[c];
+        S out[BC];
+#pragma unroll
+        for (int i = 0; i < BC; i++)
+            out[i] = (S)(Cb[i] * To + hc * p.hr[b0 + i] * p.tau[b0 + i] - ec[i] - acc[i]);
+        st8(Rlo + (dbase + pos_of[dc]) * nb + b0, out);
+    }
+}
+
+// Level-synchronous upwind sweep, one CTA per (direction, NBC bands).
+// Records and residuals are in level order, so the next level's operands
+// are contiguous and are prefetched into registers before the barrier; the
+// corrections of the last RING positions live in a shared-memory ring, older
+// ones are read back from global memory (where every correction is also
+// stored, in place of its residual).
+template <typename S, int NBC, int RING, int PF>
+__global__ void __launch_bounds__(64) k_sweep(int nb, int nc, const int *__restrict__ lvl_ptr,
+                                              const int *__restrict__ dir_lvl_off, const unsigned char *__restrict__ rec_nin,
+                                              const int *__restrict__ rec_np, const double *__restrict__ rec_a,
+                                              const double *__restrict__ rec_sig, const double *__restrict__ kbv, S *Rlo) {
+    __shared__ S ring[RING * NBC];
+    const int nchunks = (nb + NBC - 1) / NBC;
     const int d = blockIdx.x / nchunks, chunk = blockIdx.x % nchunks;
-    const int b0 = chunk * nbc, nbl = min(nbc, nb - b0);
-    const double sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
-    const int *cells = lvl_cells + (size_t)d * nc;
+    const int b0 = chunk * NBC, nbl = min(NBC, nb - b0);
     const int *lp = lvl_ptr + dir_lvl_off[d];
     const int nlev = dir_lvl_off[d + 1] - dir_lvl_off[d] - 1;
-    S *Rd = R + (size_t)d * nc * nb;
-    S *ed = eps + (size_t)d * nc * nb;
+    const size_t base = (size_t)d * nc;
+    const int bd = blockDim.x;
+    // prefetch registers for up to PF items of the next level
+    S pR[PF];
+    int pN[PF];
+    double pS[PF];
+    int c0 = lp[0], c1 = nlev > 0 ? lp[1] : 0;
+    auto load = [&](int cc0, int cc1) {
+#pragma unroll
+        for (int i = 0; i < PF; i++) {
+            const int t = threadIdx.x + i * bd;
+            pN[i] = -1;
+            if (t < (cc1 - cc0) * nbl) {
+                const size_t P = base + cc0 + t / nbl;
+                const int b = b0 + t % nbl;
+                pR[i] = Rlo[P * nb + b];
+                pN[i] = rec_nin[P];
+                pS[i] = rec_sig[P];
+            }
+        }
+    };
+    load(c0, c1);
     for (int l = 0; l < nlev; l++) {
-        const int c0 = lp[l], items = (lp[l + 1] - c0) * nbl;
-        for (int t = threadIdx.x; t < items; t += blockDim.x) {
-            const int c = cells[c0 + t / nbl];
-            const int b = b0 + t % nbl;
-            const double kb = p.tau[b] * p.vmag[b];
-            const double vol = m.vol[c];
-            const unsigned lm = lag ? lag[(size_t)d * nc + c] : 0u;
-            S acc = Rd[(size_t)c * nb + b];
-            double sig = 0;
-            int j = 0;
-            for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++, j++) {
-                const double dpn = sx * m.cf_nx[k] + sy * m.cf_ny[k] + sz * m.cf_nz[k];
-                const double a = m.cf_area[k] / vol * dpn;
-                if (dpn >= 0)
-                    sig += a;
-                else if (m.cf_bound[k] < 0 && !((lm >> j) & 1u))
-                    acc -= (S)(kb * a) * Rd[(size_t)m.cf_nbr[k] * nb + b];
+        const int n0 = c1, n1 = (l + 1 < nlev) ? lp[l + 2] : c1;
+        const int items = (c1 - c0) * nbl;
+        for (int t = threadIdx.x; t < items; t += bd) {
+            const int i = t / bd;
+            const size_t P = base + c0 + t / nbl;
+            const int lb = t % nbl, b = b0 + lb;
+            const double kb = kbv[b];
+            S acc;
+            int nin;
+            double sig;
+            if (i < PF) {
+                acc = pR[0];
+#pragma unroll
+                for (int u = 1; u < PF; u++)
+                    if (i == u) acc = pR[u];
+                nin = pN[0];
+                sig = pS[0];
+#pragma unroll
+                for (int u = 1; u < PF; u++)
+                    if (i == u) {
+                        nin = pN[u];
+                        sig = pS[u];
+                    }
+            } else {
+                acc = Rlo[P * nb + b];
+                nin = rec_nin[P];
+                sig = rec_sig[P];
+            }
+            for (int j = 0; j < nin; j++) {
+                const int np = rec_np[4 * P + j];
+                const S dj = (np >= c1 - RING) ? ring[(np % RING) * NBC + lb] : Rlo[(base + np) * nb + b];
+                acc -= (S)(kb * rec_a[4 * P + j]) * dj;
             }
             const S dl = acc / (S)(1.0 + kb * sig);
-            Rd[(size_t)c * nb + b] = dl;
-            ed[(size_t)c * nb + b] += dl;
+            Rlo[P * nb + b] = dl;
+            ring[((c0 + t / nbl) % RING) * NBC + lb] = dl;
         }
+        load(n0, n1);
         __syncthreads();
+        c0 = n0;
+        c1 = n1;
+    }
+}
+
+// e += d (corrections gathered from level order) fused with the moments,
+// one thread per (cell, band) looping over directions with the angular
+// weights of every moment tabulated in shared memory:
+//   S0 = sum_d w e, S1 = sum_d w s e, S2 = sum_d w s s^T e
+//   Tlat = sum_b lat S0 / C     (temperature, StaticBTESynthetic.cpp:2493)
+//   Tband[b] = S0 / C           (:2494)
+//   E = sum_b S0 / C_bulk        (:2504)
+//   q = sum_b |v| S1             (:2515-2517)
+//   Th = kappa sum_{hr>0} lat S0 / C,  Q = sum_{hr>0} tau |v|^2 S2
+// (the two moments of the synthetic source). blockDim = cpb * nb.
+constexpr int kMomSlots = 12;
+constexpr int kWTab = 10;
+
+template <typename S>
+__global__ void k_moments(DMesh m, DPhys p, int cpb, S *__restrict__ eps, const S *__restrict__ Rlo,
+                          const int *__restrict__ pos_of, const double *__restrict__ Tb,
+                          const double *__restrict__ wtab, double *__restrict__ Tlat, double *__restrict__ E,
+                          double *__restrict__ q, double *__restrict__ Tband, double *__restrict__ Th,
+                          double *__restrict__ Q, int apply) {
+    extern __shared__ double sm_dyn[];
+    double *wt = sm_dyn;                         // [nd][kWTab]
+    double *smom = sm_dyn + (size_t)p.nd * kWTab;  // [cpb][kMomSlots]
+    const int nb = p.nb, nc = m.nc;
+    for (int i = threadIdx.x; i < p.nd * kWTab; i += blockDim.x) wt[i] = wtab[i];
+    for (int i = threadIdx.x; i < cpb * kMomSlots; i += blockDim.x) smom[i] = 0;
+    __syncthreads();
+    const int lc = threadIdx.x / nb, b = threadIdx.x % nb;
+    const int c = blockIdx.x * cpb + lc;
+    if (lc < cpb && c < nc) {
+        const double Cb = p.C[b];
+        const double base = Cb * Tb[c];
+        double a[kWTab];
+#pragma unroll
+        for (int i = 0; i < kWTab; i++) a[i] = 0;
+        const size_t stride = (size_t)nc * nb;
+        S *e0 = eps + (size_t)c * nb + b;
+        const int *po = pos_of + c;
+#pragma unroll 4
+        for (int d = 0; d < p.nd; d++) {
+            S ev = e0[d * stride];
+            if (apply) {
+                ev += Rlo[((size_t)d * nc + po[(size_t)d * nc]) * nb + b];
+                e0[d * stride] = ev;
+            }
+            const double e = base + (double)ev;
+            const double *w = wt + kWTab * d;
+#pragma unroll
+            for (int i = 0; i < kWTab; i++) a[i] += w[i] * e;
+        }
+        Tband[(size_t)b * nc + c] = a[0] / Cb;
+        const double vm = p.vmag[b], lat = p.lat[b];
+        const double tl = lat * a[0] / Cb;
+        double *smc = smom + kMomSlots * lc;
+        atomicAdd(&smc[0], tl);
+        atomicAdd(&smc[1], a[0] / p.capb);
+        atomicAdd(&smc[2], vm * a[1]);
+        atomicAdd(&smc[3], vm * a[2]);
+        atomicAdd(&smc[4], vm * a[3]);
+        if (p.hr[b] > 0) {
+            const double f = p.tau[b] * vm * vm;
+            atomicAdd(&smc[5], tl);
+#pragma unroll
+            for (int i = 0; i < 6; i++) atomicAdd(&smc[6 + i], f * a[4 + i]);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < cpb; i += blockDim.x) {
+        const int cc = blockIdx.x * cpb + i;
+        if (cc >= nc) continue;
+        const double *smc = smom + kMomSlots * i;
+        Tlat[cc] = smc[0];
+        E[cc] = smc[1];
+        q[3 * cc] = smc[2];
+        q[3 * cc + 1] = smc[3];
+        q[3 * cc + 2] = smc[4];
+        Th[cc] = p.kappa * smc[5];
+        for (int j = 0; j < 6; j++) Q[6 * cc + j] = smc[6 + j];
     }
 }
 
 // outgoing boundary values: e_c(new) + g_c(pre-sweep) . (x_f - x_c)
-template <typename S>
-__global__ void k_bound_out(DMesh m, DPhys p, EView<S> ev, double *__restrict__ eb) {
+template <typename S, int DIM>
+__global__ void k_bound_out(DMesh m, DPhys p, EView<S, DIM> ev, double *__restrict__ eb) {
     const int nb = p.nb;
     const size_t total = (size_t)p.nd * m.nbs * nb;
     for (size_t t = gtid(); t < total; t += gstride()) {
@@ -249,115 +532,37 @@ __global__ void k_bound_out(DMesh m, DPhys p, EView<S> ev, double *__restrict__ 
     }
 }
 
-// Per-cell moments over all (b, d). LPC lanes cooperate on one cell.
-//   Tlat = sum lat w e / C          (temperature, :2493)
-//   Tband[b] = sum_d w e / C        (:2494)
-//   E = sum w e / C_bulk             (:2504)
-//   q = sum v w e                    (:2515-2517)
-//   Th = kappa sum_{hr>0} lat w e / C        (Fourier part of the source)
-//   Q  = sum_{hr>0} w tau v v^T e  (xx xy xz yy yz zz)
-template <typename S, int LPC>
-__global__ void k_moments(DMesh m, DPhys p, const S *__restrict__ eps, const double *__restrict__ Tb,
-                          double *__restrict__ Tlat, double *__restrict__ E, double *__restrict__ q,
-                          double *__restrict__ Tband, double *__restrict__ Th, double *__restrict__ Q) {
-    const int nb = p.nb, nc = m.nc;
-    const int lane = threadIdx.x % LPC;
-    const size_t cell = gtid() / LPC;
-    const bool active = cell < (size_t)nc;
-    const int c = active ? (int)cell : 0;
-    double tl = 0, en = 0, qx = 0, qy = 0, qz = 0, th = 0, q6[6] = {0, 0, 0, 0, 0, 0};
-    if (active) {
-        const double tbc = Tb[c];
-        for (int b = lane; b < nb; b += LPC) {
-            const double Cb = p.C[b], lat = p.lat[b], vm = p.vmag[b];
-            const bool hrp = p.hr[b] > 0;
-            const double wtv = p.tau[b] * vm * vm;
-            const double base = Cb * tbc;
-            double tb = 0, tlb = 0, enb = 0, qxb = 0, qyb = 0, qzb = 0;
-            double qq[6] = {0, 0, 0, 0, 0, 0};
-            for (int d = 0; d < p.nd; d++) {
-                const double e = base + (double)eps[((size_t)d * nc + c) * nb + b];
-                const double w = p.w[d];
-                tlb += lat * e * w / Cb;
-                tb += e * w / Cb;
-                enb += e * w / p.capb;
-                const double sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
-                qxb += vm * sx * w * e;
-                qyb += vm * sy * w * e;
-                qzb += vm * sz * w * e;
-                if (hrp) {
-                    const double f = w * wtv * e;
-                    qq[0] += f * sx * sx;
-                    qq[1] += f * sx * sy;
-                    qq[2] += f * sx * sz;
-                    qq[3] += f * sy * sy;
-                    qq[4] += f * sy * sz;
-                    qq[5] += f * sz * sz;
-                }
-            }
-            Tband[(size_t)b * nc + c] = tb;
-            tl += tlb;
-            en += enb;
-            qx += qxb;
-            qy += qyb;
-            qz += qzb;
-            if (hrp) {
-                th += tlb;
-                for (int i = 0; i < 6; i++) q6[i] += qq[i];
-            }
-        }
-    }
-    if (LPC > 1) {
-#pragma unroll
-        for (int off = LPC / 2; off > 0; off >>= 1) {
-            tl += __shfl_down_sync(0xffffffffu, tl, off, LPC);
-            en += __shfl_down_sync(0xffffffffu, en, off, LPC);
-            qx += __shfl_down_sync(0xffffffffu, qx, off, LPC);
-            qy += __shfl_down_sync(0xffffffffu, qy, off, LPC);
-            qz += __shfl_down_sync(0xffffffffu, qz, off, LPC);
-            th += __shfl_down_sync(0xffffffffu, th, off, LPC);
-#pragma unroll
-            for (int i = 0; i < 6; i++) q6[i] += __shfl_down_sync(0xffffffffu, q6[i], off, LPC);
-        }
-    }
-    if (active && lane == 0) {
-        Tlat[c] = tl;
-        E[c] = en;
-        q[3 * c] = qx;
-        q[3 * c + 1] = qy;
-        q[3 * c + 2] = qz;
-        Th[c] = p.kappa * th;
-        for (int i = 0; i < 6; i++) Q[6 * c + i] = q6[i];
-    }
-}
-
 // Th/Q moments of the boundary values (before the incoming gather, as the
 // reference evaluates its face gradients inside the pair loop).
+// one warp per boundary side, lanes over (direction, band)
 __global__ void k_side_moments(DMesh m, DPhys p, const double *__restrict__ eb, double *__restrict__ Ths,
                                double *__restrict__ Qs) {
-    const int s = (int)gtid();
+    const int s = (int)(gtid() >> 5), lane = threadIdx.x & 31;
     if (s >= m.nbs) return;
     double th = 0, q6[6] = {0, 0, 0, 0, 0, 0};
     if (m.bs_cell[s] >= 0) {
-        for (int d = 0; d < p.nd; d++) {
+        const int n = p.nd * p.nb;
+        for (int i = lane; i < n; i += 32) {
+            const int d = i / p.nb, b = i % p.nb;
+            if (!(p.hr[b] > 0)) continue;
             const double w = p.w[d], sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
-            const double *e = eb + ((size_t)d * m.nbs + s) * p.nb;
-            for (int b = 0; b < p.nb; b++) {
-                if (!(p.hr[b] > 0)) continue;
-                const double x = e[b];
-                th += p.lat[b] * x * w / p.C[b];
-                const double f = w * p.tau[b] * p.vmag[b] * p.vmag[b] * x;
-                q6[0] += f * sx * sx;
-                q6[1] += f * sx * sy;
-                q6[2] += f * sx * sz;
-                q6[3] += f * sy * sy;
-                q6[4] += f * sy * sz;
-                q6[5] += f * sz * sz;
-            }
+            const double x = eb[((size_t)d * m.nbs + s) * p.nb + b];
+            th += p.lat[b] * x * w / p.C[b];
+            const double f = w * p.tau[b] * p.vmag[b] * p.vmag[b] * x;
+            q6[0] += f * sx * sx;
+            q6[1] += f * sx * sy;
+            q6[2] += f * sx * sz;
+            q6[3] += f * sy * sy;
+            q6[4] += f * sy * sz;
+            q6[5] += f * sz * sz;
         }
     }
-    Ths[s] = p.kappa * th;
-    for (int i = 0; i < 6; i++) Qs[6 * s + i] = q6[i];
+    th = warp_sum(th);
+    for (int i = 0; i < 6; i++) q6[i] = warp_sum(q6[i]);
+    if (lane == 0) {
+        Ths[s] = p.kappa * th;
+        for (int i = 0; i < 6; i++) Qs[6 * s + i] = q6[i];
+    }
 }
 
 // inverse-distance node values of (Th, Q) with boundary-side override
@@ -470,10 +675,6 @@ __global__ void k_remacro(DMesh m, const double *__restrict__ Th, const double *
     remacro[c] = acc;
 }
 
-__device__ __forceinline__ double warp_sum(double v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return v;
-}
 
 // incoming boundary values by wall type; reads only outgoing entries (or a
 // snapshot for chained specular sources), writes only incoming entries
@@ -522,18 +723,21 @@ __global__ void k_gather(DMesh m, DPhys p, const double *__restrict__ dif_w, con
 // macro boundary temperatures sum lat e w / C with periodic overrides
 __global__ void k_macro_bc(DMesh m, DPhys p, const double *__restrict__ eb, const double *__restrict__ ovr,
                            double *__restrict__ bTm) {
-    const int s = (int)gtid();
+    const int s = (int)(gtid() >> 5), lane = threadIdx.x & 31;
     if (s >= m.nbs) return;
     double acc = 0;
     if (m.bs_cell[s] >= 0) {
-        for (int b = 0; b < p.nb; b++) {
-            const double lc = p.lat[b];
-            const double Cb = p.C[b];
-            for (int d = 0; d < p.nd; d++) acc += lc * eb[((size_t)d * m.nbs + s) * p.nb + b] / Cb * p.w[d];
+        const int n = p.nd * p.nb;
+        for (int i = lane; i < n; i += 32) {
+            const int d = i / p.nb, b = i % p.nb;
+            acc += p.lat[b] * eb[((size_t)d * m.nbs + s) * p.nb + b] / p.C[b] * p.w[d];
         }
     }
-    const double o = ovr[s];
-    bTm[s] = (o == o) ? o : acc;
+    acc = warp_sum(acc);
+    if (lane == 0) {
+        const double o = ovr[s];
+        bTm[s] = (o == o) ? o : acc;
+    }
 }
 
 // cell-only inverse-distance node temperatures
@@ -584,6 +788,60 @@ __global__ void k_macro_rhs(DMesh m, double kappa, const double *__restrict__ re
         r -= kappa * A * (a2x * gx + a2y * gy + a2z * gz);
     }
     rhs_neg[c] = -r;
+}
+
+// Fourier pre-solve right-hand side (StaticFourier::_get_Re, StaticFourier.cpp:520-613),
+// negated for the SPD form; dirichlet[ib] marks isothermal walls and periodic
+// pairs that carry a temperature jump
+__global__ void k_fourier_rhs(DMesh m, double kappa, const int *__restrict__ dirichlet, const double *__restrict__ bT,
+                              const double *__restrict__ TV, double *__restrict__ rhs_neg) {
+    const int c = (int)gtid();
+    if (c >= m.nc) return;
+    double r = -m.heat[c] * m.vol[c];
+    for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+        const double nx = m.cf_nx[k], ny = m.cf_ny[k], nz = m.cf_nz[k], A = m.cf_area[k];
+        const int bnd = m.cf_bound[k];
+        double ax, ay, az;
+        if (bnd >= 0) {
+            if (!dirichlet[bnd]) continue;
+            ax = m.cf_fx[k] - m.cx[c];
+            ay = m.cf_fy[k] - m.cy[c];
+            az = m.cf_fz[k] - m.cz[c];
+            r += -(kappa * A / (nx * ax + ny * ay + nz * az)) * bT[bnd];
+        } else {
+            const int j = m.cf_nbr[k];
+            ax = m.cx[j] - m.cx[c];
+            ay = m.cy[j] - m.cy[c];
+            az = m.cz[j] - m.cz[c];
+        }
+        const double an = ax * nx + ay * ny + az * nz;
+        const double a2x = nx - ax / an, a2y = ny - ay / an, a2z = nz - az / an;
+        double gx, gy, gz;
+        tangential(m, c, k, TV, 1, 0, true, gx, gy, gz);
+        r -= kappa * A * (a2x * gx + a2y * gy + a2z * gz);
+    }
+    rhs_neg[c] = -r;
+}
+
+// Fourier heat flux -kappa grad T from the least-squares stencil
+// (StaticFourier::_get_heat_flux, StaticFourier.cpp:615-711)
+__global__ void k_fourier_flux(DMesh m, double kappa, const double *__restrict__ T, double *__restrict__ q) {
+    const int c = (int)gtid();
+    if (c >= m.nc) return;
+    int interior = 0;
+    for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) interior += (m.cf_bound[k] < 0);
+    double gx = 0, gy = 0, gz = 0;
+    if (m.dim == 3 || interior >= 2) {
+        for (int q2 = m.nbr_ptr[c]; q2 < m.nbr_ptr[c + 1]; q2++) {
+            const double de = T[m.nbr_idx[q2]] - T[c];
+            gx += m.lsq_w[3 * q2] * de;
+            gy += m.lsq_w[3 * q2 + 1] * de;
+            gz += m.lsq_w[3 * q2 + 2] * de;
+        }
+    }
+    q[3 * c] = -kappa * gx;
+    q[3 * c + 1] = -kappa * gy;
+    q[3 * c + 2] = -kappa * gz;
 }
 
 __global__ void k_copy(const double *__restrict__ a, double *__restrict__ b, int n) {
@@ -668,10 +926,36 @@ __device__ double grid_dot_add(cgrp::grid_group &grid, double v, double *slot) {
     return r;
 }
 
+__device__ void grid_dot_add2(cgrp::grid_group &grid, double &v1, double &v2, double *slot) {
+    __shared__ double sh1[32], sh2[32];
+    v1 = warp_sum(v1);
+    v2 = warp_sum(v2);
+    if ((threadIdx.x & 31) == 0) {
+        sh1[threadIdx.x >> 5] = v1;
+        sh2[threadIdx.x >> 5] = v2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, b = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            a += sh1[w];
+            b += sh2[w];
+        }
+        atomicAdd(slot, a);
+        atomicAdd(slot + 1, b);
+    }
+    grid.sync();
+    v1 = *(volatile double *)slot;
+    v2 = *(volatile double *)(slot + 1);
+    __syncthreads();
+}
+
+// Stops when |r| <= max(rtol |b|, eta |r0|): rtol is the absolute floor,
+// eta bounds the reduction needed from a warm start.
 __global__ void k_pcg(int n, const int *__restrict__ ptr, const int *__restrict__ idx, const double *__restrict__ val,
                       const double *__restrict__ dinv, const double *__restrict__ bvec, double *__restrict__ x,
                       double *__restrict__ r, double *__restrict__ z, double *__restrict__ p, double *__restrict__ Ap,
-                      double *scal, double rtol, int maxit, int nslots) {
+                      double *scal, double rtol, double eta, int maxit, int nslots) {
     cgrp::grid_group grid = cgrp::this_grid();
     const size_t i0 = gtid(), st = gstride();
     int slot = 0;
@@ -690,7 +974,6 @@ __global__ void k_pcg(int n, const int *__restrict__ ptr, const int *__restrict_
     }
     rz = grid_dot_add(grid, rz, &scal[slot++]);
     bb = grid_dot_add(grid, bb, &scal[slot++]);
-    const double thr = rtol * rtol * bb;
     int it = 0;
     double rr = rz;
     // initial residual check
@@ -699,6 +982,7 @@ __global__ void k_pcg(int n, const int *__restrict__ ptr, const int *__restrict_
         for (size_t i = i0; i < (size_t)n; i += st) v += r[i] * r[i];
         rr = grid_dot_add(grid, v, &scal[slot++]);
     }
+    const double thr = fmax(rtol * rtol * bb, eta * eta * rr);
     while (it < maxit && rr > thr && slot + 3 < nslots) {
         double pap = 0;
         for (size_t i = i0; i < (size_t)n; i += st) {
@@ -719,8 +1003,8 @@ __global__ void k_pcg(int n, const int *__restrict__ ptr, const int *__restrict_
             rzn += ri * zi;
             rrn += ri * ri;
         }
-        rzn = grid_dot_add(grid, rzn, &scal[slot++]);
-        rrn = grid_dot_add(grid, rrn, &scal[slot++]);
+        grid_dot_add2(grid, rzn, rrn, &scal[slot]);
+        slot += 2;
         const double beta = rzn / rz;
         rz = rzn;
         rr = rrn;
@@ -871,6 +1155,10 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
     d.nbr_ptr = up_i(mesh.nbr_ptr);
     d.nbr_idx = up_i(mesh.nbr_idx);
     d.lsq_w = up_d(mesh.lsq_w);
+    {
+        std::vector<float> wf(mesh.lsq_w.begin(), mesh.lsq_w.end());
+        d.lsq_wf = upload(this, allocs_, wf, s, ok);
+    }
     d.face_w = up_d(mesh.face_w);
     d.f_cf0 = up_i(mesh.f_cf0);
     d.b_type = up_i(mesh.b_type);
@@ -915,6 +1203,69 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
         lag_ = (unsigned char *)pl;
     }
 
+    // level-ordered sweep records (neighbours as positions in the same
+    // direction's level order) and the cell -> position map
+    {
+        const int nc2 = mesh.nc;
+        std::vector<int> po((size_t)nd * nc2);
+        for (int dd = 0; dd < nd; dd++)
+            for (int pos = 0; pos < nc2; pos++) po[(size_t)dd * nc2 + sched.lvl_cells[(size_t)dd * nc2 + pos]] = pos;
+        pos_of_ = up_i(po);
+        std::vector<int> rc((size_t)nd * nc2), rn((size_t)nd * nc2 * 4, 0);
+        std::vector<unsigned char> rnin((size_t)nd * nc2, 0);
+        std::vector<double> rsig((size_t)nd * nc2, 0.0), ra((size_t)nd * nc2 * 4, 0.0);
+        for (int dd = 0; dd < nd; dd++)
+            for (int pos = 0; pos < nc2; pos++) {
+                size_t P = (size_t)dd * nc2 + pos;
+                int c = sched.lvl_cells[P];
+                rc[P] = c;
+                unsigned lm = sched.lag.empty() ? 0u : sched.lag[(size_t)dd * nc2 + c];
+                double sig = 0;
+                int j = 0, nin = 0;
+                for (int k = mesh.cf_ptr[c]; k < mesh.cf_ptr[c + 1]; k++, j++) {
+                    double dpn = ang.sx[dd] * mesh.cf_nx[k] + ang.sy[dd] * mesh.cf_ny[k] + ang.sz[dd] * mesh.cf_nz[k];
+                    double a = mesh.cf_area[k] / mesh.vol[c] * dpn;
+                    if (dpn >= 0)
+                        sig += a;
+                    else if (mesh.cf_bound[k] < 0 && !((lm >> j) & 1u)) {
+                        if (nin >= 4) return {-8, "a cell has more than four upwind neighbours"};
+                        rn[4 * P + nin] = po[(size_t)dd * nc2 + mesh.cf_nbr[k]];
+                        ra[4 * P + nin] = a;
+                        nin++;
+                    }
+                }
+                rsig[P] = sig;
+                rnin[P] = (unsigned char)nin;
+            }
+        rec_cell_ = up_i(rc);
+        rec_nbr_ = up_i(rn);
+        rec_sig_ = up_d(rsig);
+        rec_a_ = up_d(ra);
+        void *pn = dalloc(rnin.size());
+        if (!pn) return {-6, "device allocation failed (sweep records)"};
+        CUDA_TRY(cudaMemcpyAsync(pn, rnin.data(), rnin.size(), cudaMemcpyHostToDevice, s));
+        rec_nin_ = (unsigned char *)pn;
+        std::vector<double> kb(nb);
+        for (int b2 = 0; b2 < nb; b2++) kb[b2] = bands.tau[b2] * bands.v[b2];
+        kb_ = up_d(kb);
+        // angular weights of the moments: w, w s, w s s^T (xx xy xz yy yz zz)
+        std::vector<double> wt((size_t)nd * 10);
+        for (int dd = 0; dd < nd; dd++) {
+            double w = ang.w[dd], x = ang.sx[dd], y = ang.sy[dd], z = ang.sz[dd];
+            double *r = &wt[(size_t)dd * 10];
+            r[0] = w;
+            r[1] = w * x;
+            r[2] = w * y;
+            r[3] = w * z;
+            r[4] = w * x * x;
+            r[5] = w * x * y;
+            r[6] = w * x * z;
+            r[7] = w * y * y;
+            r[8] = w * y * z;
+            r[9] = w * z * z;
+        }
+        wtab_ = up_d(wt);
+    }
     // diffuse weights and specular sources per (side, direction)
     const int nbs = mesh.nbs();
     std::vector<double> difw((size_t)nbs * nd, 0.0);
@@ -1029,6 +1380,75 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
         K_val_ = up_d(val);
         K_dinv_ = up_d(dinv);
     }
+    // Fourier pre-solve matrix (StaticFourier::_get_coefficient_macro, StaticFourier.cpp:449-518):
+    // isothermal walls and periodic pairs with a temperature jump are Dirichlet-like,
+    // every other wall is adiabatic
+    {
+        const double kap = bands.kappa[0];
+        const int nbd = mesh.nbd();
+        std::vector<int> dir(nbd, 0);
+        std::vector<double> bT(nbd, 0.0);
+        for (int ib = 0; ib < nbd; ib++) {
+            int t = mesh.b_type[ib];
+            if (t == 1) dir[ib] = 1;
+            if (t < 0 && (mesh.b_T[ib] != 0 || mesh.b_T[mesh.b_connect[ib]] != 0)) dir[ib] = 1;
+        }
+        // boundary temperatures (SolutionAll::_set_initial, Solution.cpp:100-118)
+        for (int ib = 0; ib < nbd; ib++) {
+            int t = mesh.b_type[ib];
+            if (t == 1)
+                bT[ib] = mesh.b_T[ib];
+            else if (t < 0 && mesh.b_T[ib] != 0) {
+                bT[ib] = mesh.b_T[ib] / 2;
+                bT[mesh.b_connect[ib]] = -mesh.b_T[ib] / 2;
+            }
+        }
+        std::vector<int> ptr(mesh.nc + 1, 0), idx;
+        std::vector<double> val, dinv(mesh.nc, 0.0);
+        bool singular = true;
+        for (int c2 = 0; c2 < mesh.nc; c2++) {
+            double diag = 0;
+            std::vector<std::pair<int, double>> row;
+            for (int k = mesh.cf_ptr[c2]; k < mesh.cf_ptr[c2 + 1]; k++) {
+                double temp = kap * mesh.cf_area[k];
+                int bnd = mesh.cf_bound[k];
+                if (bnd == -1) {
+                    int j = mesh.cf_nbr[k];
+                    double ax = mesh.cx[j] - mesh.cx[c2], ay = mesh.cy[j] - mesh.cy[c2], az = mesh.cz[j] - mesh.cz[c2];
+                    temp = temp / (mesh.cf_nx[k] * ax + mesh.cf_ny[k] * ay + mesh.cf_nz[k] * az);
+                    diag += -temp;
+                    row.push_back({j, temp});
+                } else if (dir[bnd]) {
+                    double ax = mesh.cf_fx[k] - mesh.cx[c2], ay = mesh.cf_fy[k] - mesh.cy[c2], az = mesh.cf_fz[k] - mesh.cz[c2];
+                    temp = temp / (mesh.cf_nx[k] * ax + mesh.cf_ny[k] * ay + mesh.cf_nz[k] * az);
+                    diag += -temp;
+                    singular = false;
+                }
+            }
+            row.push_back({c2, diag});
+            std::sort(row.begin(), row.end());
+            std::vector<std::pair<int, double>> merged;
+            for (auto &e : row) {
+                if (!merged.empty() && merged.back().first == e.first)
+                    merged.back().second += e.second;
+                else
+                    merged.push_back(e);
+            }
+            for (auto &e : merged) {
+                idx.push_back(e.first);
+                val.push_back(-e.second);
+                if (e.first == c2) dinv[c2] = 1.0 / (-e.second);
+            }
+            ptr[mesh.nc == 0 ? 0 : c2 + 1] = (int)idx.size();
+        }
+        fourier_singular_ = singular;
+        KF_ptr_ = up_i(ptr);
+        KF_idx_ = up_i(idx);
+        KF_val_ = up_d(val);
+        KF_dinv_ = up_d(dinv);
+        bTF_ = up_d(bT);
+        bF_dir_ = up_i(dir);
+    }
     if (!ok) return {-6, "device allocation or upload failed"};
     Error e = alloc_all();
     if (e.code) return e;
@@ -1043,7 +1463,7 @@ Error Solver::alloc_all() {
     const size_t ne = nd * nc * nb;
     auto A = [&](size_t bytes) { return dalloc(bytes); };
     eps_ = A(ne * S);
-    grad_ = A(ne * 3 * S);
+    grad_ = A(ne * mesh.dim * S);
     res_ = A(ne * S);
     Tbase_ = (double *)A(nc * 8);
     gTb_ = (double *)A(nc * 3 * 8);
@@ -1122,58 +1542,96 @@ Error Solver::set_initial(const double *T0, const double *q0, const double *bth)
     }
     have_initial_ = true;
     started_ = false;
+    last_margin_ = 1.0;
+    std::fill(warm_ok_.begin(), warm_ok_.end(), 0);
     return {0, ""};
 }
 
-Error Solver::fourier_initial() { return {-8, "the Fourier pre-solve is not implemented yet; pass T0 to gbte_set_initial"}; }
+// Fourier pre-solve seeding the BTE (StaticFourier::_solve, StaticFourier.cpp:934-976,
+// called from SolutionAll::_Fourier_Solver, Solution.cpp:236-255): Picard on
+// the non-orthogonal correction until the mean squared change is <= 1e-5,
+// starting from the current initial temperature (Tref for a deck).
+Error Solver::fourier_initial() {
+    if (!initialised) return {-1, "solver not initialised"};
+    if (fourier_singular_) return {-8, "Fourier pre-solve: no isothermal or temperature-jump boundary (singular system)"};
+    if (!have_initial_) return {-1, "set an initial temperature first"};
+    cudaStream_t s = cfg.stream;
+    const int nc = mesh.nc, nslot = mesh.nn * mesh.nmat;
+    const int gC = (nc + kThreads - 1) / kThreads, gN = (nslot + kThreads - 1) / kThreads;
+    double internal = 1000;
+    long long it = 0;
+    int steps = 0;
+    while (internal > 1e-5) {
+        GL(K_COPY, k_copy<<<gC, kThreads, 0, s>>>(T_, T1_, nc));
+        GL(K_TINTERP, k_tinterp<<<gN, kThreads, 0, s>>>(dm_, T_, TV_));
+        GL(K_MACRO_RHS, k_fourier_rhs<<<gC, kThreads, 0, s>>>(dm_, dp_.kappa, bF_dir_, bTF_, TV_, rhs_));
+        CUDA_TRY(cudaGetLastError());
+        Error e = cg_solve(KF_ptr_, KF_idx_, KF_val_, KF_dinv_, T_, rhs_, cfg.macro_rtol, 0.0, it, cg_scal_, cg_r_,
+                           cg_z_, cg_p_, cg_Ap_);
+        if (e.code) return e;
+        CUDA_TRY(cudaMemsetAsync(red_, 0, 8, s));
+        GL(K_REDUCE, k_sqdiff<<<std::min(gC, 148), kThreads, 0, s>>>(nc, T1_, T_, red_));
+        CUDA_TRY(cudaMemcpyAsync(h_pinned_, red_, 8, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        internal = h_pinned_[0] / nc;
+        if (cfg.verbose) printf("iterations residual: %.17g\n", internal);
+        if (!std::isfinite(internal) || ++steps >= 1000) return {-4, "Fourier pre-solve does not converge"};
+    }
+    GL(K_INIT, k_fourier_flux<<<gC, kThreads, 0, s>>>(dm_, dp_.kappa, T_, q_));
+    CUDA_TRY(cudaGetLastError());
+    fourier_iterations = steps;
+    std::vector<double> T0(nc), q0(3 * (size_t)nc);
+    CUDA_TRY(cudaMemcpyAsync(T0.data(), T_, nc * 8, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(q0.data(), q_, (size_t)nc * 24, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return set_initial(T0.data(), q0.data(), nullptr);
+}
 
 Error Solver::macro_solve(double *x, const double *b, long long &iters) {
+    return cg_solve(K_ptr_, K_idx_, K_val_, K_dinv_, x, b, cfg.macro_rtol, 0.0, iters, cg_scal_, cg_r_, cg_z_, cg_p_, cg_Ap_);
+}
+
+// Jacobi-PCG on a negated (SPD) CSR system; scratch vectors and the 65536
+// reduction slots are passed in by the caller
+Error Solver::cg_solve(const int *ptr, const int *idx, const double *val, const double *dinv, double *x, const double *b,
+                       double rtol, double eta, long long &iters, double *scal, double *r, double *z, double *p,
+                       double *Ap) {
     cudaStream_t s = cfg.stream;
-    const int nslots = 65536;
-    CUDA_TRY(cudaMemsetAsync(cg_scal_, 0, nslots * 8, s));
+    int nslots = 65536;
+    CUDA_TRY(cudaMemsetAsync(scal, 0, nslots * 8, s));
     int n = mesh.nc;
-    double rtol = cfg.macro_rtol;
     int maxit = 20000;
-    void *args[] = {&n, &K_ptr_, &K_idx_, &K_val_, &K_dinv_, (void *)&b, &x, &cg_r_, &cg_z_, &cg_p_, &cg_Ap_,
-                    &cg_scal_, &rtol, &maxit, (void *)&nslots};
-    int ns = nslots;
-    args[14] = &ns;
+    void *args[] = {&n, (void *)&ptr, (void *)&idx, (void *)&val, (void *)&dinv, (void *)&b, &x, &r, &z, &p, &Ap,
+                    &scal, &rtol, &eta, &maxit, &nslots};
     cudaError_t lerr = cudaSuccess;
     GL(K_PCG, lerr = cudaLaunchCooperativeKernel((void *)k_pcg, dim3(coop_blocks_), dim3(kThreads), args, 0, s));
     CUDA_TRY(lerr);
-    CUDA_TRY(cudaMemcpyAsync(h_pinned_ + 8, cg_scal_ + nslots - 1, 8, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(h_pinned_ + 8, scal + nslots - 1, 8, cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
     iters += (long long)h_pinned_[8];
     return {0, ""};
 }
 
-template <typename S>
+template <typename S, int DIM>
 Error Solver::solve_t(SolveStats &st) {
     cudaStream_t s = cfg.stream;
     const int nc = mesh.nc, nb = bands.nb, nd = ang.nd, nbs = mesh.nbs(), nslot = mesh.nn * mesh.nmat;
     const size_t ne = (size_t)nd * nc * nb;
     S *eps = (S *)eps_, *g = (S *)grad_, *R = (S *)res_;
-    EView<S> ev{eps, g, Tbase_, gTb_, nb, nc};
-    const int gE = grid_for(ne), gB = grid_for((size_t)nd * nbs * nb);
-    const int gC = (nc + kThreads - 1) / kThreads, gS = (nbs + kThreads - 1) / kThreads,
-              gN = (nslot + kThreads - 1) / kThreads;
-    int lpc = 1;
-    while (lpc < nb && lpc < 32) lpc <<= 1;
-    const int gM = (int)(((size_t)nc * lpc + kThreads - 1) / kThreads);
-    const int nbc = std::min(nb, 8);
-    const int sweep_blocks = nd * ((nb + nbc - 1) / nbc);
-    auto moments = [&]() {
-        prof_begin(K_MOMENTS);
-        switch (lpc) {
-        case 1: k_moments<S, 1><<<gM, kThreads, 0, s>>>(dm_, dp_, eps, Tbase_, Tlat_, E_, q_, Tband_, Th_, Q_); break;
-        case 2: k_moments<S, 2><<<gM, kThreads, 0, s>>>(dm_, dp_, eps, Tbase_, Tlat_, E_, q_, Tband_, Th_, Q_); break;
-        case 4: k_moments<S, 4><<<gM, kThreads, 0, s>>>(dm_, dp_, eps, Tbase_, Tlat_, E_, q_, Tband_, Th_, Q_); break;
-        case 8: k_moments<S, 8><<<gM, kThreads, 0, s>>>(dm_, dp_, eps, Tbase_, Tlat_, E_, q_, Tband_, Th_, Q_); break;
-        case 16: k_moments<S, 16><<<gM, kThreads, 0, s>>>(dm_, dp_, eps, Tbase_, Tlat_, E_, q_, Tband_, Th_, Q_); break;
-        default: k_moments<S, 32><<<gM, kThreads, 0, s>>>(dm_, dp_, eps, Tbase_, Tlat_, E_, q_, Tband_, Th_, Q_); break;
-        }
-        prof_end();
-    };
+    const S *w = std::is_same<S, float>::value ? (const S *)dm_.lsq_wf : (const S *)dm_.lsq_w;
+    EView<S, DIM> ev{eps, g, Tbase_, gTb_, nb, nc};
+    const int gE = grid_for(ne), gB = grid_for((size_t)nd * nbs * nb), gE8 = grid_for(ne / 4);
+    const int gC = (nc + kThreads - 1) / kThreads, gN = (nslot + kThreads - 1) / kThreads;
+    constexpr int NBC = 2, RING = 2048, PF = 2;
+    const int sweep_blocks = nd * ((nb + NBC - 1) / NBC);
+    const int cpb = std::max(1, 256 / nb);
+    const int gM = (nc + cpb - 1) / cpb;
+    const size_t msmem = ((size_t)nd * kWTab + (size_t)cpb * kMomSlots) * sizeof(double);
+    const int gW = (int)(((size_t)nbs * 32 + kThreads - 1) / kThreads);
+    if (msmem > 200 * 1024) return {-8, "too many directions for the moments kernel's shared-memory weight table"};
+    if (nb > 256) return {-8, "more than 256 bands are not supported"};
+    if (msmem > 48 * 1024)
+        CUDA_TRY(cudaFuncSetAttribute(k_moments<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem));
     auto gather = [&]() {
         if (need_snapshot_) cudaMemcpyAsync(eb_snap_, eb_, (size_t)nd * nbs * nb * 8, cudaMemcpyDeviceToDevice, s);
         GL(K_GATHER, k_gather<<<gB, kThreads, 0, s>>>(dm_, dp_, dif_w_, spec_src_, need_snapshot_ ? eb_snap_ : nullptr, eb_));
@@ -1181,8 +1639,8 @@ Error Solver::solve_t(SolveStats &st) {
     if (!started_) {
         // _set_initial (:765-782) and the initial boundary values (StaticBTESyntheticSolver.cpp:45-62)
         GL(K_INIT, k_init_eps<S><<<gE, kThreads, 0, s>>>(dm_, dp_, T_, Tbase_, eps));
-        GL(K_GRADIENT, k_gradient<S><<<gE, kThreads, 0, s>>>(dm_, dp_, eps, g));
-        GL(K_BOUND_OUT, k_bound_out<S><<<gB, kThreads, 0, s>>>(dm_, dp_, ev, eb_));
+        GL(K_GRADIENT, (k_gradient<S, DIM><<<gE, kThreads, 0, s>>>(dm_, dp_, w, eps, g)));
+        GL(K_BOUND_OUT, (k_bound_out<S, DIM><<<gB, kThreads, 0, s>>>(dm_, dp_, ev, eb_)));
         gather();
         CUDA_TRY(cudaGetLastError());
         started_ = true;
@@ -1200,16 +1658,23 @@ Error Solver::solve_t(SolveStats &st) {
         // copy() (:2655-2690)
         CUDA_TRY(cudaMemcpyAsync(Told_, T_, nc * 8, cudaMemcpyDeviceToDevice, s));
         CUDA_TRY(cudaMemcpyAsync(qold_, q_, (size_t)nc * 24, cudaMemcpyDeviceToDevice, s));
-        GL(K_GRADIENT, k_gradient<S><<<gE, kThreads, 0, s>>>(dm_, dp_, eps, g));
-        GL(K_RESIDUAL, k_residual<S><<<gE, kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, R));
-        GL(K_SWEEP, k_sweep<S><<<sweep_blocks, kThreads, 0, s>>>(dm_, dp_, nbc, lvl_cells_, lvl_ptr_, dir_lvl_off_, lag_, R, eps));
-        GL(K_BOUND_OUT, k_bound_out<S><<<gB, kThreads, 0, s>>>(dm_, dp_, ev, eb_));
-        moments();
-        GL(K_SIDE_MOMENTS, k_side_moments<<<gS, kThreads, 0, s>>>(dm_, dp_, eb_, Ths_, Qs_));
+        if (nb % 4 == 0) {
+            GL(K_GRADIENT, (k_gradient8<S, DIM, 4><<<gE8, kThreads, 0, s>>>(dm_, dp_, w, eps, g)));
+            GL(K_RESIDUAL, (k_residual8<S, DIM, 4><<<gE8, kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, pos_of_, R)));
+        } else {
+            GL(K_GRADIENT, (k_gradient<S, DIM><<<gE, kThreads, 0, s>>>(dm_, dp_, w, eps, g)));
+            GL(K_RESIDUAL, (k_residual<S, DIM><<<gE, kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, pos_of_, R)));
+        }
+        GL(K_SWEEP, (k_sweep<S, NBC, RING, PF><<<sweep_blocks, 64, 0, s>>>(nb, nc, lvl_ptr_, dir_lvl_off_, rec_nin_, rec_nbr_,
+                                                                           rec_a_, rec_sig_, kb_, R)));
+        GL(K_MOMENTS, (k_moments<S><<<gM, cpb * nb, msmem, s>>>(dm_, dp_, cpb, eps, R, pos_of_, Tbase_, wtab_, Tlat_, E_,
+                                                                q_, Tband_, Th_, Q_, 1)));
+        GL(K_BOUND_OUT, (k_bound_out<S, DIM><<<gB, kThreads, 0, s>>>(dm_, dp_, ev, eb_)));
+        GL(K_SIDE_MOMENTS, k_side_moments<<<gW, kThreads, 0, s>>>(dm_, dp_, eb_, Ths_, Qs_));
         GL(K_NODE_INTERP, k_node_interp<<<gN, kThreads, 0, s>>>(dm_, Th_, Q_, Ths_, Qs_, ThV_, QV_));
         GL(K_REMACRO, k_remacro<<<gC, kThreads, 0, s>>>(dm_, Th_, Q_, Ths_, Qs_, ThV_, QV_, remacro_));
         gather();
-        GL(K_MACRO_BC, k_macro_bc<<<gS, kThreads, 0, s>>>(dm_, dp_, eb_, bTovr_, bTm_));
+        GL(K_MACRO_BC, k_macro_bc<<<gW, kThreads, 0, s>>>(dm_, dp_, eb_, bTovr_, bTm_));
         CUDA_TRY(cudaGetLastError());
         CUDA_TRY(cudaEventRecord(ev_[1], s));
         // _marco_solution: Picard on the non-orthogonal correction
@@ -1221,8 +1686,28 @@ Error Solver::solve_t(SolveStats &st) {
             GL(K_TINTERP, k_tinterp<<<gN, kThreads, 0, s>>>(dm_, T_, TV_));
             GL(K_MACRO_RHS, k_macro_rhs<<<gC, kThreads, 0, s>>>(dm_, dp_.kappa, remacro_, bTm_, TV_, rhs_));
             CUDA_TRY(cudaGetLastError());
-            Error e = macro_solve(T_, rhs_, st.cg_iterations);
+            // warm start from this Picard step's solution of the previous
+            // outer iteration; tolerance tightens with the outer margin
+            const int step = inner;
+            if (step < (int)warm_.size() && warm_[step] && warm_ok_[step])
+                CUDA_TRY(cudaMemcpyAsync(T_, warm_[step], (size_t)nc * 8, cudaMemcpyDeviceToDevice, s));
+            // from a warm start the residual must drop by kWarmEta; the
+            // absolute floor macro_rtol * |b| still bounds the final error
+            const bool warm = step < (int)warm_.size() && warm_[step] && warm_ok_[step];
+            Error e = cg_solve(K_ptr_, K_idx_, K_val_, K_dinv_, T_, rhs_, cfg.macro_rtol, warm ? kWarmEta : 0.0,
+                               st.cg_iterations, cg_scal_, cg_r_, cg_z_, cg_p_, cg_Ap_);
             prof_collect(st);
+            if (!e.code) {
+                if (step >= (int)warm_.size()) {
+                    warm_.resize(step + 1, nullptr);
+                    warm_ok_.resize(step + 1, 0);
+                }
+                if (!warm_[step]) warm_[step] = (double *)dalloc((size_t)nc * 8);
+                if (warm_[step]) {
+                    CUDA_TRY(cudaMemcpyAsync(warm_[step], T_, (size_t)nc * 8, cudaMemcpyDeviceToDevice, s));
+                    warm_ok_[step] = 1;
+                }
+            }
             if (e.code) return e;
             CUDA_TRY(cudaMemsetAsync(red_, 0, 8, s));
             GL(K_REDUCE, k_sqdiff<<<std::min(gC, 148), kThreads, 0, s>>>(nc, T1_, T_, red_));
@@ -1263,6 +1748,7 @@ Error Solver::solve_t(SolveStats &st) {
             errInc = 0;
         errOld = err;
         errOldq = errq;
+        last_margin_ = std::isfinite(err) && std::isfinite(errq) ? std::max(err, errq) : 1.0;
         st.err_temp = err;
         st.err_flux = errq;
         st.iterations = nt + 1;
@@ -1302,8 +1788,12 @@ Error Solver::solve(SolveStats &st) {
     if (!initialised) return {-1, "solver not initialised"};
     if (!have_initial_) return {-1, "call gbte_set_initial (or gbte_fourier_initial) before gbte_solve"};
     CUDA_TRY(cudaSetDevice(cfg.device));
-    if (cfg.precision == 1) return solve_t<float>(st);
-    return solve_t<double>(st);
+    if (mesh.dim == 2) {
+        if (cfg.precision == 1) return solve_t<float, 2>(st);
+        return solve_t<double, 2>(st);
+    }
+    if (cfg.precision == 1) return solve_t<float, 3>(st);
+    return solve_t<double, 3>(st);
 }
 
 Error Solver::get_fields(double *TE, double *TL, double *q, double *TB) {

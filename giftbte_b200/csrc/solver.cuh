@@ -18,6 +18,7 @@ struct DMesh {
     const double *vol, *cx, *cy, *cz, *heat;
     const int *nbr_ptr, *nbr_idx;
     const double *lsq_w;
+    const float *lsq_wf;
     const double *face_w;
     const int *f_cf0;
     const int *b_type, *b_connect;
@@ -72,6 +73,7 @@ public:
                const SolverConfig &cfg);
     Error set_initial(const double *T0, const double *q0, const double *boundary_thermal_per_bside);
     Error fourier_initial();
+    int fourier_iterations = 0;
     Error solve(SolveStats &st);
     Error get_fields(double *T_energy, double *T_lattice, double *q, double *T_band);
 
@@ -84,9 +86,11 @@ public:
     std::string last_error;
 
 private:
-    template <typename S> Error solve_t(SolveStats &st);
+    template <typename S, int DIM> Error solve_t(SolveStats &st);
     Error alloc_all();
     Error macro_solve(double *x_dev, const double *rhs_dev, long long &iters);
+    Error cg_solve(const int *ptr, const int *idx, const double *val, const double *dinv, double *x, const double *b,
+                   double rtol, double eta, long long &iters, double *scal, double *r, double *z, double *p, double *Ap);
     void *dalloc(size_t bytes);
     std::vector<void *> allocs_;
     DMesh dm_{};
@@ -105,7 +109,23 @@ private:
     bool need_snapshot_ = false;
     // schedule on device
     int *lvl_cells_ = nullptr, *lvl_ptr_ = nullptr, *dir_lvl_off_ = nullptr;
+    // level-ordered sweep records per direction: cell, sum of outgoing
+    // A/V (s.n), and up to 4 incoming (neighbour, A/V (s.n)) pairs
+    int *rec_cell_ = nullptr, *rec_nbr_ = nullptr, *pos_of_ = nullptr;
+    double *wtab_ = nullptr;
+    unsigned char *rec_nin_ = nullptr;
+    double *rec_sig_ = nullptr, *rec_a_ = nullptr, *kb_ = nullptr;
+    // warm starts of the macro solves: solution of each Picard step of the
+    // previous outer iteration
+    std::vector<double *> warm_;
+    std::vector<char> warm_ok_;
+    double last_margin_ = 1.0;
     unsigned char *lag_ = nullptr;
+    // Fourier pre-solve system (StaticFourier._get_coefficient_macro), negated, CSR
+    int *KF_ptr_ = nullptr, *KF_idx_ = nullptr;
+    double *KF_val_ = nullptr, *KF_dinv_ = nullptr, *bTF_ = nullptr;
+    int *bF_dir_ = nullptr;
+    bool fourier_singular_ = true;
     // macro matrix (negated, SPD), CSR
     int *K_ptr_ = nullptr, *K_idx_ = nullptr;
     double *K_val_ = nullptr, *K_dinv_ = nullptr;

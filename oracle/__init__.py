@@ -126,10 +126,21 @@ def read_reference_outputs(deck_root: str) -> Dict[str, np.ndarray]:
     nb = int(tb[:, 0].max())
     out = {"xyz": T[:, :3], "T": T[:, 3], "E": E[:, 3], "q": q[:, 3:6],
            "Tband": tb[:, 4].reshape(nb, -1)}
+    fm = os.path.join(deck_root, "Temperature_macro.dat")
+    if os.path.exists(fm):
+        out["Tf"] = np.loadtxt(fm)[:, 3]
+        out["qf"] = np.loadtxt(os.path.join(deck_root, "HeatFlux_macro.dat"))[:, 3:6]
     iters = 0
+    margins = []
     logp = os.path.join(deck_root, "ref_run.log")
     if os.path.exists(logp):
         with open(logp) as f:
-            iters = sum(1 for line in f if line.startswith("Iteration #"))
+            for line in f:
+                if line.startswith("Iteration #"):
+                    iters += 1
+                    t = line.split("Temperature:")[1].split()[0]
+                    q = line.split("Heat Flux:")[1].split()[0]
+                    margins.append((float(t), float(q)))
     out["iters"] = iters
+    out["margins"] = np.asarray(margins).reshape(-1, 2)
     return out

@@ -10,6 +10,9 @@ the reference's full-precision fields:
   E      energy temperature                   (Temperature.dat)
   q      heat flux, Nc x 3                    (HeatFlux.dat)
   Tband  band temperatures, Nb x Nc           (Tempband.dat)
+  Tf, qf the Fourier pre-solve that seeds the BTE (Temperature_macro.dat,
+         HeatFlux_macro.dat)
+  margins per-iteration (temperature, heat-flux) margins from the log
 
 Usage (needs the reference tree, so it runs only where that exists):
     python tests/golden/make_golden.py [case ...]
@@ -86,7 +89,8 @@ def make(name: str, d: decks.Deck) -> None:
         cell_region=m.cell_region,
         band_v=B.v, band_tau=B.tau, band_C=B.C, band_lat=B.lattice_ratio, band_hr=B.heat_ratio,
         params=json.dumps(deck_params(d)),
-        T=r["T"], E=r["E"], q=r["q"], Tband=r["Tband"], xyz=r["xyz"], iters=r["iters"])
+        T=r["T"], E=r["E"], q=r["q"], Tband=r["Tband"], xyz=r["xyz"], iters=r["iters"],
+        Tf=r["Tf"], qf=r["qf"], margins=r["margins"])
     print(f"{name}: Nc={m.n_cells} Nb={B.n_bands} iters={r['iters']}")
 
 
@@ -102,7 +106,7 @@ def load(name: str):
                    scale=tuple(p["scale"]), material_dim=p["material_dim"], angle_method=p["angle_method"],
                    n_theta=p["n_theta"], n_phi=p["n_phi"], tref=p["tref"], heat_source=p["heat_source"],
                    mesh_format=p["mesh_format"], residual_temp=1e-12, residual_flux=1e-12, max_iter=3000)
-    ref = {k: z[k] for k in ("T", "E", "q", "Tband", "xyz")}
+    ref = {k: z[k] for k in ("T", "E", "q", "Tband", "xyz", "Tf", "qf", "margins") if k in z}
     ref["iters"] = int(z["iters"])
     return d, ref
 
