@@ -106,7 +106,7 @@ class DeckInfo(ctypes.Structure):
 EXPORTS = ["gbte_inspect_deck", "gbte_inspect_mesh", "gbte_default_options", "gbte_create", "gbte_create_from_deck", "gbte_set_initial",
            "gbte_fourier_initial", "gbte_solve", "gbte_get_fields", "gbte_write_outputs", "gbte_get_sizes",
            "gbte_get_geometry", "gbte_last_error", "gbte_status_string", "gbte_destroy", "gbte_kernel_name",
-           "gbte_solve_with"]
+           "gbte_solve_with", "gbte_fourier_initial_noalloc"]
 
 _lib = None
 
@@ -138,6 +138,7 @@ def library():
         lib.gbte_get_geometry.argtypes = [ctypes.c_void_p, _c_dbl_p, _c_dbl_p]
         lib.gbte_destroy.argtypes = [ctypes.c_void_p]
         lib.gbte_fourier_initial.argtypes = [ctypes.c_void_p]
+        lib.gbte_fourier_initial_noalloc.argtypes = [ctypes.c_void_p]
         lib.gbte_inspect_deck.argtypes = [ctypes.c_char_p, ctypes.POINTER(DeckInfo)]
         lib.gbte_inspect_mesh.argtypes = [ctypes.POINTER(MeshView), ctypes.POINTER(BandTableC),
                                           ctypes.POINTER(BCTable), ctypes.POINTER(AngleSpec),
@@ -226,6 +227,12 @@ class StaticBTESynthetic:
         """Replace the initial field by the Fourier pre-solve (kappa_bulk) the
         reference runs before the BTE (StaticFourier::_solve)."""
         self._check(library().gbte_fourier_initial(self._h))
+
+    def fourier_initial_noalloc(self) -> None:
+        """The Fourier pre-solve without any device allocation (its scratch
+        lives in a static device array of the library; see
+        gbte_fourier_initial_noalloc in include/giftbte.h for the limits)."""
+        self._check(library().gbte_fourier_initial_noalloc(self._h))
 
     def solve(self, max_iter: Optional[int] = None, err_temp: Optional[float] = None,
               err_flux: Optional[float] = None, allow_not_converged: bool = True) -> dict:

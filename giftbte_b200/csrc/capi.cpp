@@ -333,6 +333,13 @@ int gbte_fourier_initial(gbte_handle *h) {
     return GBTE_OK;
 }
 
+int gbte_fourier_initial_noalloc(gbte_handle *h) {
+    if (!h) return GBTE_ERR_ARG;
+    gbte::Error e = h->solver.fourier_initial_noalloc();
+    if (e.code) return fail(h, e), status_of(e.code);
+    return GBTE_OK;
+}
+
 int gbte_solve(gbte_handle *h, gbte_stats *st) {
     if (!h) return GBTE_ERR_ARG;
     try {

@@ -38,6 +38,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <mutex>
 #include <thread>
 #include <type_traits>
 
@@ -1805,6 +1806,107 @@ Error Solver::get_fields(double *TE, double *TL, double *q, double *TB) {
     if (q) CUDA_TRY(cudaMemcpyAsync(q, q_, nc * 24, cudaMemcpyDeviceToHost, s));
     if (TB) CUDA_TRY(cudaMemcpyAsync(TB, Tband_, nc * bands.nb * 8, cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
+    return {0, ""};
+}
+
+// ------------------------------------------------ allocation-free variant --
+//
+// Scratch of gbte_fourier_initial_noalloc: one file-scope device array that
+// every GPU loading this library holds until the process exits. Layout for a
+// problem of nc cells and ns node slots (both <= kNoAllocMaxCells): previous
+// iterate, node temperatures, right-hand side, the four CG vectors, then the
+// CG reduction slots and a small reduction output.
+constexpr int kNoAllocMaxCells = 131072;
+constexpr int kNoAllocSlots = 65536;
+constexpr size_t kNoAllocDoubles = 7 * (size_t)kNoAllocMaxCells + kNoAllocSlots + 8;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+namespace {
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[64] = {nullptr};
+
+// Device address of the scratch array for the current device, looked up
+// once per device (the host-side symbol is only a stand-in, never a device
+// address).
+Error noalloc_scratch(int device, double **out) {
+    if (device < 0 || device >= 64) return {-1, "device ordinal out of range for the allocation-free scratch"};
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess) return {-3, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e)};
+        g_noalloc_ptr[device] = (double *)ptr;
+    }
+    *out = g_noalloc_ptr[device];
+    return {0, ""};
+}
+}  // namespace
+
+// Same computation as fourier_initial(), with every scratch buffer taken from
+// g_noalloc_scratch and no device or pinned allocation: the results land in
+// the handle's own state (initial temperature, flux and the FP32 base).
+Error Solver::fourier_initial_noalloc() {
+    if (!initialised) return {-1, "solver not initialised"};
+    if (!have_initial_) return {-1, "set an initial temperature first"};
+    if (fourier_singular_) return {-8, "Fourier pre-solve: no isothermal or temperature-jump boundary (singular system)"};
+    const int nc = mesh.nc, nslot = mesh.nn * mesh.nmat;
+    if (nc > kNoAllocMaxCells || nslot > kNoAllocMaxCells)
+        return {-1, "the allocation-free Fourier pre-solve holds at most " + std::to_string(kNoAllocMaxCells) +
+                        " cells and node slots (this mesh has " + std::to_string(nc) + " cells, " +
+                        std::to_string(nslot) + " node slots)"};
+    CUDA_TRY(cudaSetDevice(cfg.device));
+    double *base = nullptr;
+    Error e0 = noalloc_scratch(cfg.device, &base);
+    if (e0.code) return e0;
+    const size_t N = kNoAllocMaxCells;
+    double *T1 = base, *TV = base + N, *rhs = base + 2 * N, *r = base + 3 * N, *z = base + 4 * N, *pv = base + 5 * N,
+           *Ap = base + 6 * N, *scal = base + 7 * N, *red = scal + kNoAllocSlots;
+    cudaStream_t s = cfg.stream;
+    const int gC = (nc + kThreads - 1) / kThreads, gN = (nslot + kThreads - 1) / kThreads;
+    double internal = 1000, h = 0;
+    long long it = 0;
+    int steps = 0;
+    while (internal > 1e-5) {
+        GL(K_COPY, k_copy<<<gC, kThreads, 0, s>>>(T_, T1, nc));
+        GL(K_TINTERP, k_tinterp<<<gN, kThreads, 0, s>>>(dm_, T_, TV));
+        GL(K_MACRO_RHS, k_fourier_rhs<<<gC, kThreads, 0, s>>>(dm_, dp_.kappa, bF_dir_, bTF_, TV, rhs));
+        CUDA_TRY(cudaGetLastError());
+        // the reduction slots must start at zero on every solve
+        CUDA_TRY(cudaMemsetAsync(scal, 0, kNoAllocSlots * sizeof(double), s));
+        int n = nc, maxit = 20000, nslots = kNoAllocSlots;
+        double rtol = cfg.macro_rtol, eta = 0.0;
+        void *args[] = {&n, (void *)&KF_ptr_, (void *)&KF_idx_, (void *)&KF_val_, (void *)&KF_dinv_, (void *)&rhs,
+                        (void *)&T_, (void *)&r, (void *)&z, (void *)&pv, (void *)&Ap, (void *)&scal, &rtol, &eta, &maxit,
+                        &nslots};
+        cudaError_t lerr = cudaSuccess;
+        GL(K_PCG, lerr = cudaLaunchCooperativeKernel((void *)k_pcg, dim3(coop_blocks_), dim3(kThreads), args, 0, s));
+        CUDA_TRY(lerr);
+        CUDA_TRY(cudaMemsetAsync(red, 0, sizeof(double), s));
+        GL(K_REDUCE, k_sqdiff<<<std::min(gC, 148), kThreads, 0, s>>>(nc, T1, T_, red));
+        CUDA_TRY(cudaMemcpyAsync(&h, red, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        internal = h / nc;
+        it++;
+        if (cfg.verbose) printf("iterations residual: %.17g\n", internal);
+        if (!std::isfinite(internal) || ++steps >= 1000) return {-4, "Fourier pre-solve does not converge"};
+    }
+    GL(K_INIT, k_fourier_flux<<<gC, kThreads, 0, s>>>(dm_, dp_.kappa, T_, q_));
+    // the new initial field: T_ and q_ hold it; the FP32 form stores its
+    // deviation from this temperature
+    if (cfg.precision == 1) {
+        CUDA_TRY(cudaMemcpyAsync(Tbase_, T_, (size_t)nc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        GL(K_INIT, k_cell_lsq_grad<<<gC, kThreads, 0, s>>>(dm_, Tbase_, gTb_));
+    } else {
+        CUDA_TRY(cudaMemsetAsync(Tbase_, 0, (size_t)nc * sizeof(double), s));
+        CUDA_TRY(cudaMemsetAsync(gTb_, 0, (size_t)nc * 3 * sizeof(double), s));
+    }
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(s));
+    fourier_iterations = steps;
+    have_initial_ = true;
+    started_ = false;
+    last_margin_ = 1.0;
+    std::fill(warm_ok_.begin(), warm_ok_.end(), 0);
     return {0, ""};
 }
 

@@ -73,6 +73,7 @@ public:
                const SolverConfig &cfg);
     Error set_initial(const double *T0, const double *q0, const double *boundary_thermal_per_bside);
     Error fourier_initial();
+    Error fourier_initial_noalloc();
     int fourier_iterations = 0;
     Error solve(SolveStats &st);
     Error get_fields(double *T_energy, double *T_lattice, double *q, double *T_band);

@@ -199,6 +199,26 @@ int gbte_set_initial(gbte_handle *h, const double *T0, const double *q0, const d
 /* Fourier pre-solve with kappa_bulk on the device; sets T0 and q0. */
 int gbte_fourier_initial(gbte_handle *h);
 
+/* Allocation-free variant of gbte_fourier_initial (no counterpart in the
+ * reference): the same Fourier pre-solve, with all of its scratch vectors
+ * taken from one static device array inside this library instead of memory
+ * allocated on the device. It is for callers that must not allocate device
+ * memory once their run has started, typically because they hand out all
+ * device memory from their own pool reserved at start-up, or run under a
+ * fixed device-memory limit, where an allocation mid-run can fail, stall or
+ * fragment that pool. Such a caller creates the handle during start-up and
+ * re-seeds it here later. The call allocates nothing on the device or in
+ * pinned memory. Limits: at most 131072 cells and 131072 node slots (nodes x
+ * materials); larger meshes get GBTE_ERR_ARG. The static array (about 7.9 MB)
+ * is held by every GPU that loads the library until the process exits. The
+ * first call on each device looks up the array's device address; make that
+ * first call before any stream capture. All calls share the one array, so
+ * calls that overlap on the GPU (other threads or streams) race; the CG
+ * reduction slots are cleared on every solve, everything else is written
+ * before it is read. Results go to the handle exactly as with
+ * gbte_fourier_initial. */
+int gbte_fourier_initial_noalloc(gbte_handle *h);
+
 /* Runs the outer source iteration until both margins are below the limits
  * (GBTE_OK), max_iter is reached (GBTE_ERR_NOT_CONVERGED) or it diverges.
  * stats may be NULL. */
