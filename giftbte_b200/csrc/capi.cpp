@@ -105,6 +105,7 @@ int create_common(const gbte::RawMesh &raw, const gbte::Bands &bands_in, const g
     cfg.macro_rtol = opt.macro_rtol > 0 ? opt.macro_rtol : 1e-13;
     cfg.verbose = opt.verbose;
     cfg.profile = opt.profile;
+    cfg.sweep_bands = opt.sweep_bands;
     cfg.device = opt.device;
     cfg.stream = (cudaStream_t)opt.stream;
     if (opt.precision != GBTE_FP64 && opt.precision != GBTE_FP32_MIXED)

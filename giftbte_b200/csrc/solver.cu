@@ -59,7 +59,7 @@ namespace {
 constexpr int kThreads = 256;
 // residual reduction required of a macro CG solve that starts from the
 // previous outer iteration's solution of the same Picard step
-constexpr double kWarmEta = 1e-6;
+constexpr double kWarmEta = 1e-4;
 
 __device__ __forceinline__ size_t gtid() { return blockIdx.x * (size_t)blockDim.x + threadIdx.x; }
 __device__ __forceinline__ double warp_sum(double v) {
@@ -347,88 +347,132 @@ __global__ void __launch_bounds__(256) k_residual8(DMesh m, DPhys p, EView<S, DI
     }
 }
 
-// Level-synchronous upwind sweep, one CTA per (direction, NBC bands).
-// Records and residuals are in level order, so the next level's operands
-// are contiguous and are prefetched into registers before the barrier; the
-// corrections of the last RING positions live in a shared-memory ring, older
-// ones are read back from global memory (where every correction is also
-// stored, in place of its residual).
-template <typename S, int NBC, int RING, int PF>
-__global__ void __launch_bounds__(64) k_sweep(int nb, int nc, const int *__restrict__ lvl_ptr,
-                                              const int *__restrict__ dir_lvl_off, const unsigned char *__restrict__ rec_nin,
-                                              const int *__restrict__ rec_np, const double *__restrict__ rec_a,
-                                              const double *__restrict__ rec_sig, const double *__restrict__ kbv, S *Rlo) {
-    __shared__ S ring[RING * NBC];
-    const int nchunks = (nb + NBC - 1) / NBC;
+__device__ __forceinline__ void cp_async(void *smem, const void *gmem, int bytes) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    if (bytes == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+    else if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// One cell of a direction's level order, as the sweep reads it: up to four
+// upwind neighbours (their positions in the same level order) with their
+// coefficients a_j = A_f/V (s.n_f) < 0, sig = sum of the outgoing A_f/V (s.n_f),
+// and the neighbour count. 48 bytes in FP32 storage, 64 in FP64, so that a
+// level's records are one contiguous range copied in 16-byte pieces.
+template <typename S>
+struct alignas(16) SweepRec {
+    int np[4];
+    S a[4];
+    S sig;
+    int nin;
+};
+
+static_assert(sizeof(SweepRec<float>) == 48 && sizeof(SweepRec<double>) == 64, "sweep record layout");
+
+__device__ __forceinline__ float sweep_div(float x, float y) { return __fdividef(x, y); }
+__device__ __forceinline__ double sweep_div(double x, double y) { return x / y; }
+
+// Level-synchronous upwind sweep: A^-1 R for one direction and a chunk of
+// nbc <= 32 bands per CTA (blockDim = nbc * cells_per_pass). Each thread owns
+// one band (tid % nbc) for the whole sweep, so the per-level overhead (level
+// bounds, record staging, barrier) is shared by nbc bands of every cell.
+// d_c = (R_c - kb sum_j a_j d_j) / (1 + kb sig_c), kb = tau |v| of the band.
+// Records and residuals are in level order, so a level's operands are
+// contiguous: they are staged into shared memory LOOK-1 levels ahead with
+// cp.async. The corrections of the last ring_n positions live in a shared
+// ring (ring_n a power of two >= widest level, so one level's writes never
+// collide); older ones are read back from global memory, where every
+// correction is also stored in place of its residual. Shared memory:
+//   LOOK slots of { SweepRec[LCAP], R[LCAP][nbc] S }, the ring
+//   [ring_n][nbc] S, and the direction's level bounds [max_lev + 1] i32.
+// Levels longer than LCAP read their overflow records from global memory.
+// rvec: the band chunk of a residual row is copied in 16-byte pieces (its
+// byte size, offset and the row pitch are multiples of 16).
+template <typename S, int LOOK, int LCAP>
+__global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int nbc, int ring_n, int rvec,
+                                               const int *__restrict__ lvl_ptr, const int *__restrict__ dir_lvl_off,
+                                               const SweepRec<S> *__restrict__ rec, const double *__restrict__ kbv,
+                                               S *Rlo) {
+    extern __shared__ __align__(16) unsigned char wsm[];
+    const size_t rbytes = ((size_t)LCAP * nbc * sizeof(S) + 15) & ~(size_t)15;
+    const size_t slot_bytes = (size_t)LCAP * sizeof(SweepRec<S>) + rbytes;
+    S *ring = reinterpret_cast<S *>(wsm + LOOK * slot_bytes);
+    int *lp = reinterpret_cast<int *>(wsm + LOOK * slot_bytes + (((size_t)ring_n * nbc * sizeof(S) + 15) & ~(size_t)15));
+    const int nchunks = (nb + nbc - 1) / nbc;
     const int d = blockIdx.x / nchunks, chunk = blockIdx.x % nchunks;
-    const int b0 = chunk * NBC, nbl = min(NBC, nb - b0);
-    const int *lp = lvl_ptr + dir_lvl_off[d];
+    const int b0 = chunk * nbc, nbl = min(nbc, nb - b0);
     const int nlev = dir_lvl_off[d + 1] - dir_lvl_off[d] - 1;
     const size_t base = (size_t)d * nc;
-    const int bd = blockDim.x;
-    // prefetch registers for up to PF items of the next level
-    S pR[PF];
-    int pN[PF];
-    double pS[PF];
-    int c0 = lp[0], c1 = nlev > 0 ? lp[1] : 0;
-    auto load = [&](int cc0, int cc1) {
-#pragma unroll
-        for (int i = 0; i < PF; i++) {
-            const int t = threadIdx.x + i * bd;
-            pN[i] = -1;
-            if (t < (cc1 - cc0) * nbl) {
-                const size_t P = base + cc0 + t / nbl;
-                const int b = b0 + t % nbl;
-                pR[i] = Rlo[P * nb + b];
-                pN[i] = rec_nin[P];
-                pS[i] = rec_sig[P];
-            }
-        }
+    const int tid = threadIdx.x, bd = blockDim.x;
+    const int lb = tid % nbc, lc0 = tid / nbc, cpp = bd / nbc;  // band of this thread, cell offset, cells per pass
+    const bool band_ok = lb < nbl;
+    const S kb = band_ok ? (S)kbv[b0 + lb] : (S)0;
+    const int mask = ring_n - 1;
+    // residual staging: each cell's band chunk is K pieces of `unit` bytes;
+    // thread tid copies piece rk of cells rc0, rc0 + rstep, ...
+    const int unit = rvec ? 16 : (int)sizeof(S);
+    const int K = nbl * (int)sizeof(S) / unit;
+    const int rk = tid % K, rc0 = tid / K, rstep = bd / K;
+    for (int i = tid; i <= nlev; i += bd) lp[i] = lvl_ptr[dir_lvl_off[d] + i];
+    __syncthreads();
+    auto issue = [&](int l) {
+        if (l >= nlev) return;
+        unsigned char *slot = wsm + (l % LOOK) * slot_bytes;
+        const int c0 = lp[l], n = min(lp[l + 1] - c0, LCAP);
+        const size_t P0 = base + c0;
+        const unsigned char *src = reinterpret_cast<const unsigned char *>(rec + P0);
+        const int npieces = n * (int)(sizeof(SweepRec<S>) / 16);
+        for (int i = tid; i < npieces; i += bd) cp_async(slot + 16 * i, src + 16 * i, 16);
+        unsigned char *sR = slot + (size_t)LCAP * sizeof(SweepRec<S>);
+        if (rc0 < rstep)
+            for (int ci = rc0; ci < n; ci += rstep)
+                cp_async(sR + (size_t)ci * nbc * sizeof(S) + rk * unit,
+                         reinterpret_cast<const unsigned char *>(Rlo + (P0 + ci) * nb + b0) + rk * unit, unit);
     };
-    load(c0, c1);
-    for (int l = 0; l < nlev; l++) {
-        const int n0 = c1, n1 = (l + 1 < nlev) ? lp[l + 2] : c1;
-        const int items = (c1 - c0) * nbl;
-        for (int t = threadIdx.x; t < items; t += bd) {
-            const int i = t / bd;
-            const size_t P = base + c0 + t / nbl;
-            const int lb = t % nbl, b = b0 + lb;
-            const double kb = kbv[b];
-            S acc;
-            int nin;
-            double sig;
-            if (i < PF) {
-                acc = pR[0];
 #pragma unroll
-                for (int u = 1; u < PF; u++)
-                    if (i == u) acc = pR[u];
-                nin = pN[0];
-                sig = pS[0];
-#pragma unroll
-                for (int u = 1; u < PF; u++)
-                    if (i == u) {
-                        nin = pN[u];
-                        sig = pS[u];
-                    }
-            } else {
-                acc = Rlo[P * nb + b];
-                nin = rec_nin[P];
-                sig = rec_sig[P];
-            }
-            for (int j = 0; j < nin; j++) {
-                const int np = rec_np[4 * P + j];
-                const S dj = (np >= c1 - RING) ? ring[(np % RING) * NBC + lb] : Rlo[(base + np) * nb + b];
-                acc -= (S)(kb * rec_a[4 * P + j]) * dj;
-            }
-            const S dl = acc / (S)(1.0 + kb * sig);
-            Rlo[P * nb + b] = dl;
-            ring[((c0 + t / nbl) % RING) * NBC + lb] = dl;
-        }
-        load(n0, n1);
-        __syncthreads();
-        c0 = n0;
-        c1 = n1;
+    for (int k = 0; k < LOOK - 1; k++) {
+        issue(k);
+        cp_async_commit();
     }
+    for (int l = 0; l < nlev; l++) {
+        cp_async_wait<LOOK - 2>();
+        __syncthreads();
+        issue(l + LOOK - 1);
+        cp_async_commit();
+        if (!band_ok) continue;
+        const unsigned char *slot = wsm + (l % LOOK) * slot_bytes;
+        const SweepRec<S> *srec = reinterpret_cast<const SweepRec<S> *>(slot);
+        const S *sR = reinterpret_cast<const S *>(slot + (size_t)LCAP * sizeof(SweepRec<S>));
+        const int c0 = lp[l], c1 = lp[l + 1], n = c1 - c0;
+        const int lo = c1 - ring_n;
+        for (int li = lc0; li < n; li += cpp) {
+            const size_t P = base + c0 + li;
+            const bool st = li < LCAP;
+            const SweepRec<S> r = st ? srec[li] : rec[P];
+            const S r0 = st ? sR[li * nbc + lb] : Rlo[P * nb + b0 + lb];
+            S sum = (S)0;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int q = r.np[j];
+                if (j < r.nin) {
+                    const S dj = (q >= lo) ? ring[(q & mask) * nbc + lb] : Rlo[(base + q) * nb + b0 + lb];
+                    sum += r.a[j] * dj;
+                }
+            }
+            const S dl = sweep_div(r0 - kb * sum, (S)1 + kb * r.sig);
+            Rlo[P * nb + b0 + lb] = dl;
+            ring[((c0 + li) & mask) * nbc + lb] = dl;
+        }
+    }
+    cp_async_wait<0>();
 }
 
 // e += d (corrections gathered from level order) fused with the moments,
@@ -1197,6 +1241,10 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
     lvl_cells_ = up_i(sched.lvl_cells);
     lvl_ptr_ = up_i(sched.lvl_ptr);
     dir_lvl_off_ = up_i(sched.dir_lvl_off);
+    max_lvl_width_ = 0;
+    for (int d = 0; d + 1 < (int)sched.dir_lvl_off.size(); d++)
+        for (int k = sched.dir_lvl_off[d]; k + 1 < sched.dir_lvl_off[d + 1]; k++)
+            max_lvl_width_ = std::max(max_lvl_width_, sched.lvl_ptr[k + 1] - sched.lvl_ptr[k]);
     if (!sched.lag.empty()) {
         void *pl = dalloc(sched.lag.size());
         if (!pl) return {-6, "device allocation failed (lag mask)"};
@@ -1212,16 +1260,21 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
         for (int dd = 0; dd < nd; dd++)
             for (int pos = 0; pos < nc2; pos++) po[(size_t)dd * nc2 + sched.lvl_cells[(size_t)dd * nc2 + pos]] = pos;
         pos_of_ = up_i(po);
-        std::vector<int> rc((size_t)nd * nc2), rn((size_t)nd * nc2 * 4, 0);
-        std::vector<unsigned char> rnin((size_t)nd * nc2, 0);
-        std::vector<double> rsig((size_t)nd * nc2, 0.0), ra((size_t)nd * nc2 * 4, 0.0);
+        // packed sweep records in the storage precision
+        std::vector<SweepRec<double>> recd;
+        std::vector<SweepRec<float>> recf;
+        const bool f32 = cfg.precision == 1;
+        if (f32)
+            recf.assign((size_t)nd * nc2, SweepRec<float>{});
+        else
+            recd.assign((size_t)nd * nc2, SweepRec<double>{});
         for (int dd = 0; dd < nd; dd++)
             for (int pos = 0; pos < nc2; pos++) {
                 size_t P = (size_t)dd * nc2 + pos;
                 int c = sched.lvl_cells[P];
-                rc[P] = c;
                 unsigned lm = sched.lag.empty() ? 0u : sched.lag[(size_t)dd * nc2 + c];
-                double sig = 0;
+                double sig = 0, av[4] = {0, 0, 0, 0};
+                int npos[4] = {0, 0, 0, 0};
                 int j = 0, nin = 0;
                 for (int k = mesh.cf_ptr[c]; k < mesh.cf_ptr[c + 1]; k++, j++) {
                     double dpn = ang.sx[dd] * mesh.cf_nx[k] + ang.sy[dd] * mesh.cf_ny[k] + ang.sz[dd] * mesh.cf_nz[k];
@@ -1230,22 +1283,29 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
                         sig += a;
                     else if (mesh.cf_bound[k] < 0 && !((lm >> j) & 1u)) {
                         if (nin >= 4) return {-8, "a cell has more than four upwind neighbours"};
-                        rn[4 * P + nin] = po[(size_t)dd * nc2 + mesh.cf_nbr[k]];
-                        ra[4 * P + nin] = a;
+                        npos[nin] = po[(size_t)dd * nc2 + mesh.cf_nbr[k]];
+                        av[nin] = a;
                         nin++;
                     }
                 }
-                rsig[P] = sig;
-                rnin[P] = (unsigned char)nin;
+                if (f32) {
+                    SweepRec<float> &r = recf[P];
+                    for (int q = 0; q < 4; q++) r.np[q] = npos[q], r.a[q] = (float)av[q];
+                    r.sig = (float)sig;
+                    r.nin = nin;
+                } else {
+                    SweepRec<double> &r = recd[P];
+                    for (int q = 0; q < 4; q++) r.np[q] = npos[q], r.a[q] = av[q];
+                    r.sig = sig;
+                    r.nin = nin;
+                }
             }
-        rec_cell_ = up_i(rc);
-        rec_nbr_ = up_i(rn);
-        rec_sig_ = up_d(rsig);
-        rec_a_ = up_d(ra);
-        void *pn = dalloc(rnin.size());
-        if (!pn) return {-6, "device allocation failed (sweep records)"};
-        CUDA_TRY(cudaMemcpyAsync(pn, rnin.data(), rnin.size(), cudaMemcpyHostToDevice, s));
-        rec_nin_ = (unsigned char *)pn;
+        const size_t rec_bytes = f32 ? recf.size() * sizeof(SweepRec<float>) : recd.size() * sizeof(SweepRec<double>);
+        rec_ = dalloc(rec_bytes);
+        if (!rec_) return {-6, "device allocation failed (sweep records)"};
+        CUDA_TRY(cudaMemcpyAsync(rec_, f32 ? (const void *)recf.data() : (const void *)recd.data(), rec_bytes,
+                                 cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
         std::vector<double> kb(nb);
         for (int b2 = 0; b2 < nb; b2++) kb[b2] = bands.tau[b2] * bands.v[b2];
         kb_ = up_d(kb);
@@ -1623,8 +1683,30 @@ Error Solver::solve_t(SolveStats &st) {
     EView<S, DIM> ev{eps, g, Tbase_, gTb_, nb, nc};
     const int gE = grid_for(ne), gB = grid_for((size_t)nd * nbs * nb), gE8 = grid_for(ne / 4);
     const int gC = (nc + kThreads - 1) / kThreads, gN = (nslot + kThreads - 1) / kThreads;
-    constexpr int NBC = 2, RING = 2048, PF = 2;
-    const int sweep_blocks = nd * ((nb + NBC - 1) / NBC);
+    constexpr int LOOK = 4, LCAP = 128;
+    // sweep: nb split into equal chunks of at most sweep_bands bands
+    // (default 8 in FP32, 4 in FP64: the fastest on the 17,939-cell 40-band
+    // cell); the ring holds at least one whole level (distinct slots for the
+    // cells written in one level) and 512 positions or more; more chunks
+    // when that does not fit in shared memory
+    int wring = 512;
+    while (wring < max_lvl_width_) wring *= 2;
+    const int wcap = (cfg.sweep_bands >= 1 && cfg.sweep_bands <= 32) ? cfg.sweep_bands : (sizeof(S) == 4 ? 8 : 4);
+    const size_t wlp = ((size_t)(sched.max_levels + 1) * sizeof(int) + 15) & ~(size_t)15;
+    int wchunks = 0, wnbc = 0;
+    size_t wslot = 0, wsmem = 0;
+    for (int cap = wcap; cap >= 1; cap--) {
+        wnbc = (nb + (nb + cap - 1) / cap - 1) / ((nb + cap - 1) / cap);  // equal chunks of <= cap bands
+        wchunks = (nb + wnbc - 1) / wnbc;                                // every chunk non-empty
+        wslot = (size_t)LCAP * sizeof(SweepRec<S>) + (((size_t)LCAP * wnbc * sizeof(S) + 15) & ~(size_t)15);
+        wsmem = LOOK * wslot + (((size_t)wring * wnbc * sizeof(S) + 15) & ~(size_t)15) + wlp;
+        if (wsmem <= 220 * 1024 || wnbc == 1) break;
+    }
+    if (wsmem > 220 * 1024) return {-8, "sweep level too wide for the shared-memory correction ring"};
+    const int wide_threads = std::max(wnbc, (256 / wnbc) * wnbc), wide_blocks = nd * wchunks;
+    const int wlast = nb - (wchunks - 1) * wnbc;  // bands of the last chunk
+    const int wrvec = ((wnbc * sizeof(S)) % 16 == 0 && (nb * sizeof(S)) % 16 == 0 && (wlast * sizeof(S)) % 16 == 0) ? 1 : 0;
+    CUDA_TRY(cudaFuncSetAttribute(k_sweep<S, LOOK, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsmem));
     const int cpb = std::max(1, 256 / nb);
     const int gM = (nc + cpb - 1) / cpb;
     const size_t msmem = ((size_t)nd * kWTab + (size_t)cpb * kMomSlots) * sizeof(double);
@@ -1666,8 +1748,8 @@ Error Solver::solve_t(SolveStats &st) {
             GL(K_GRADIENT, (k_gradient<S, DIM><<<gE, kThreads, 0, s>>>(dm_, dp_, w, eps, g)));
             GL(K_RESIDUAL, (k_residual<S, DIM><<<gE, kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, pos_of_, R)));
         }
-        GL(K_SWEEP, (k_sweep<S, NBC, RING, PF><<<sweep_blocks, 64, 0, s>>>(nb, nc, lvl_ptr_, dir_lvl_off_, rec_nin_, rec_nbr_,
-                                                                           rec_a_, rec_sig_, kb_, R)));
+        GL(K_SWEEP, (k_sweep<S, LOOK, LCAP><<<wide_blocks, wide_threads, wsmem, s>>>(
+                        nb, nc, wnbc, wring, wrvec, lvl_ptr_, dir_lvl_off_, (const SweepRec<S> *)rec_, kb_, R)));
         GL(K_MOMENTS, (k_moments<S><<<gM, cpb * nb, msmem, s>>>(dm_, dp_, cpb, eps, R, pos_of_, Tbase_, wtab_, Tlat_, E_,
                                                                 q_, Tband_, Th_, Q_, 1)));
         GL(K_BOUND_OUT, (k_bound_out<S, DIM><<<gB, kThreads, 0, s>>>(dm_, dp_, ev, eb_)));

@@ -47,6 +47,7 @@ struct SolverConfig {
     double macro_rtol = 1e-13;
     int verbose = 0;
     int profile = 0;
+    int sweep_bands = 0;  // bands per sweep CTA, 0 = automatic
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -110,12 +111,13 @@ private:
     bool need_snapshot_ = false;
     // schedule on device
     int *lvl_cells_ = nullptr, *lvl_ptr_ = nullptr, *dir_lvl_off_ = nullptr;
-    // level-ordered sweep records per direction: cell, sum of outgoing
-    // A/V (s.n), and up to 4 incoming (neighbour, A/V (s.n)) pairs
-    int *rec_cell_ = nullptr, *rec_nbr_ = nullptr, *pos_of_ = nullptr;
+    int max_lvl_width_ = 0;  // widest level of any direction (cells)
+    // level-ordered sweep records per direction: sum of outgoing A/V (s.n)
+    // and up to 4 incoming (neighbour position, A/V (s.n)) pairs
+    void *rec_ = nullptr;  // SweepRec<storage type>[nd][nc] in level order
+    int *pos_of_ = nullptr;
     double *wtab_ = nullptr;
-    unsigned char *rec_nin_ = nullptr;
-    double *rec_sig_ = nullptr, *rec_a_ = nullptr, *kb_ = nullptr;
+    double *kb_ = nullptr;
     // warm starts of the macro solves: solution of each Picard step of the
     // previous outer iteration
     std::vector<double *> warm_;

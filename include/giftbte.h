@@ -125,6 +125,7 @@ typedef struct {
     int verbose;              /* 1: print the per-iteration margins like the reference */
     double macro_rtol;        /* relative residual of the macro CG solve; 0 = default 1e-13 */
     int profile;              /* 1: time every kernel launch with CUDA events (gbte_stats.kernel_ms) */
+    int sweep_bands;          /* bands per CTA of the upwind sweep (1..32); 0 = automatic */
 } gbte_options;
 
 #define GBTE_NUM_KERNELS 16
