@@ -33,6 +33,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <unordered_map>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -1060,6 +1061,171 @@ __global__ void k_pcg(int n, const int *__restrict__ ptr, const int *__restrict_
     if (i0 == 0) scal[nslots - 1] = (double)it;
 }
 
+// Sum over a warp by an xor butterfly: every lane ends with the same,
+// bitwise identical value (each pairwise add is commutative).
+__device__ __forceinline__ double warp_allsum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Jacobi-preconditioned CG in the Chronopoulos-Gear form on one
+// thread-block cluster, the whole system resident in shared memory.
+// The rows are split into C compact parts (recursive coordinate bisection on
+// the cell centres); CTA k owns part k: rows part_ptr[k] .. part_ptr[k+1] of
+// the permuted order (perm maps them to the caller's rows). Its matrix is
+// stored as the diagonal plus K off-diagonal columns in ELL form, column
+// indices local (< nr) or into a halo that follows the local entries. After
+// each update of u = D^-1 r, every CTA stores the u values its neighbours
+// need straight into their halos (distributed shared memory), so the
+// product w = A u reads only local shared memory. The three dot products
+// of an iteration, (r,u), (w,u) and (r,r), are reduced together: warp ->
+// CTA -> one partial per CTA pushed into every CTA, summed there in rank
+// order, so all CTAs hold bitwise identical scalars and take the same
+// branch at the stopping test |r| <= max(rtol |b|, eta |r0|). Two cluster
+// barriers per iteration: after the halo exchange and after the partials.
+// When t1 is given, sum (x - t1)^2 of the solution is reduced too.
+// out[0] = iterations, out[1] = that sum, out[2] = |r|^2 at exit.
+__global__ void __launch_bounds__(256, 1)
+    k_cg_cluster(int K, int nrmax, int hmax, int smax, const int *__restrict__ part_ptr, const int *__restrict__ perm,
+                 const double *__restrict__ ell_val, const int *__restrict__ ell_col, const double *__restrict__ diag,
+                 const int *__restrict__ nhalo, const int *__restrict__ nsend, const int *__restrict__ snd_src,
+                 const int *__restrict__ snd_dst, const double *__restrict__ bvec, double *__restrict__ x, double rtol,
+                 double eta, int maxit, const double *__restrict__ t1, double *__restrict__ out) {
+    cgrp::cluster_group cl = cgrp::this_cluster();
+    const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    extern __shared__ __align__(16) unsigned char pcs[];
+    double *xs = reinterpret_cast<double *>(pcs), *rs = xs + nrmax, *ps = rs + nrmax, *ss = ps + nrmax,
+           *ws = ss + nrmax, *dg = ws + nrmax, *di = dg + nrmax, *us = di + nrmax;  // us: [nrmax + hmax]
+    double *part = us + nrmax + hmax;  // [32][4] partial sums pushed by every CTA
+    double *wsum = part + 128;         // [32][4] warp partial sums
+    double *ev = wsum + 128;           // [K][nrmax]
+    double **raddr = reinterpret_cast<double **>(ev + (size_t)K * nrmax);  // [smax] halo slots in other CTAs
+    int *ec = reinterpret_cast<int *>(raddr + smax);                       // [K][nrmax]
+    int *ssrc = ec + (size_t)K * nrmax;                                    // [smax]
+    const int tid = threadIdx.x, bd = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = bd >> 5;
+    const int base = part_ptr[rank], nr = part_ptr[rank + 1] - base, ns = nsend[rank];
+    (void)nhalo;
+    for (int i = tid; i < nr; i += bd) {
+        const int o = perm[base + i];
+        xs[i] = x[o];
+        us[i] = xs[i];
+        rs[i] = bvec[o];
+        dg[i] = diag[base + i];
+        di[i] = 1.0 / dg[i];
+        ps[i] = 0.0;
+        ss[i] = 0.0;
+    }
+    for (int e = tid; e < K * nrmax; e += bd) {
+        ev[e] = ell_val[(size_t)rank * K * nrmax + e];
+        ec[e] = ell_col[(size_t)rank * K * nrmax + e];
+    }
+    for (int e = tid; e < ns; e += bd) {
+        ssrc[e] = snd_src[(size_t)rank * smax + e];
+        const int d = snd_dst[(size_t)rank * smax + e];
+        raddr[e] = cl.map_shared_rank(us, d >> 20) + (d & 0xFFFFF);
+    }
+    cl.sync();
+    auto push_halo = [&]() {
+        for (int e = tid; e < ns; e += bd) *raddr[e] = us[ssrc[e]];
+    };
+    auto matvec = [&](int i) {
+        double s = dg[i] * us[i];
+        for (int k = 0; k < K; k++) s += ev[k * nrmax + i] * us[ec[k * nrmax + i]];
+        return s;
+    };
+    // sums of nv <= 4 values over the cluster, identical in every thread
+    auto csum = [&](double *v, int nv) {
+        for (int j = 0; j < nv; j++) v[j] = warp_allsum(v[j]);
+        if (lane == 0)
+            for (int j = 0; j < nv; j++) wsum[warp * 4 + j] = v[j];
+        __syncthreads();
+        if (warp == 0) {
+            double t[4];
+            for (int j = 0; j < nv; j++) t[j] = warp_allsum(lane < nw ? wsum[lane * 4 + j] : 0.0);
+            if (lane < C) {
+                double *dst = cl.map_shared_rank(part, lane) + rank * 4;
+                for (int j = 0; j < nv; j++) dst[j] = t[j];
+            }
+        }
+        cl.sync();
+        for (int j = 0; j < nv; j++) v[j] = warp_allsum(lane < C ? part[lane * 4 + j] : 0.0);
+    };
+    // r = b - A x (x's halo first), u = D^-1 r, w = A u
+    push_halo();
+    cl.sync();
+    double bb = 0;
+    for (int i = tid; i < nr; i += bd) {
+        const double bi = rs[i];
+        bb += bi * bi;
+        rs[i] = bi - matvec(i);
+    }
+    cl.sync();  // every CTA has read x's halo before u's arrives
+    for (int i = tid; i < nr; i += bd) us[i] = di[i] * rs[i];
+    __syncthreads();
+    push_halo();
+    cl.sync();
+    double v[4] = {0, 0, 0, bb};
+    for (int i = tid; i < nr; i += bd) {
+        const double w = matvec(i);
+        ws[i] = w;
+        v[0] += rs[i] * us[i];
+        v[1] += w * us[i];
+        v[2] += rs[i] * rs[i];
+    }
+    csum(v, 4);
+    double gam = v[0], rr = v[2];
+    const double thr = fmax(rtol * rtol * v[3], eta * eta * rr);
+    double alpha = gam / v[1], beta = 0.0;
+    int it = 0;
+    while (it < maxit && rr > thr) {
+        for (int i = tid; i < nr; i += bd) {
+            const double p = us[i] + beta * ps[i], s = ws[i] + beta * ss[i];
+            ps[i] = p;
+            ss[i] = s;
+            xs[i] += alpha * p;
+            const double r = rs[i] - alpha * s;
+            rs[i] = r;
+            us[i] = di[i] * r;
+        }
+        __syncthreads();
+        push_halo();
+        cl.sync();
+        double t[3] = {0, 0, 0};
+        for (int i = tid; i < nr; i += bd) {
+            const double w = matvec(i);
+            ws[i] = w;
+            t[0] += rs[i] * us[i];
+            t[1] += w * us[i];
+            t[2] += rs[i] * rs[i];
+        }
+        csum(t, 3);
+        beta = t[0] / gam;
+        alpha = t[0] / (t[1] - beta * t[0] / alpha);
+        gam = t[0];
+        rr = t[2];
+        it++;
+    }
+    double sq = 0;
+    for (int i = tid; i < nr; i += bd) {
+        const int o = perm[base + i];
+        x[o] = xs[i];
+        if (t1) {
+            const double dd = xs[i] - t1[o];
+            sq += dd * dd;
+        }
+    }
+    if (t1) {
+        cl.sync();  // every CTA has read the last partials before new ones arrive
+        csum(&sq, 1);
+    }
+    if (rank == 0 && tid == 0) {
+        out[0] = (double)it;
+        out[1] = sq;
+        out[2] = rr;
+    }
+    cl.sync();  // no CTA leaves while another may still write its shared memory
+}
+
 }  // namespace
 
 // ------------------------------------------------------------- host side --
@@ -1440,6 +1606,8 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
         K_idx_ = up_i(idx);
         K_val_ = up_d(val);
         K_dinv_ = up_d(dinv);
+        Error pe = cg_plan(ptr, idx, val, kplan_);
+        if (pe.code) return pe;
     }
     // Fourier pre-solve matrix (StaticFourier::_get_coefficient_macro, StaticFourier.cpp:449-518):
     // isothermal walls and periodic pairs with a temperature jump are Dirichlet-like,
@@ -1507,6 +1675,8 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
         KF_idx_ = up_i(idx);
         KF_val_ = up_d(val);
         KF_dinv_ = up_d(dinv);
+        Error pe = cg_plan(ptr, idx, val, kfplan_);
+        if (pe.code) return pe;
         bTF_ = up_d(bT);
         bF_dir_ = up_i(dir);
     }
@@ -1627,14 +1797,11 @@ Error Solver::fourier_initial() {
         GL(K_TINTERP, k_tinterp<<<gN, kThreads, 0, s>>>(dm_, T_, TV_));
         GL(K_MACRO_RHS, k_fourier_rhs<<<gC, kThreads, 0, s>>>(dm_, dp_.kappa, bF_dir_, bTF_, TV_, rhs_));
         CUDA_TRY(cudaGetLastError());
-        Error e = cg_solve(KF_ptr_, KF_idx_, KF_val_, KF_dinv_, T_, rhs_, cfg.macro_rtol, 0.0, it, cg_scal_, cg_r_,
-                           cg_z_, cg_p_, cg_Ap_);
+        double sq = 0;
+        Error e = cg_solve(kfplan_, KF_ptr_, KF_idx_, KF_val_, KF_dinv_, T_, rhs_, cfg.macro_rtol, 0.0, it, cg_scal_,
+                           cg_r_, cg_z_, cg_p_, cg_Ap_, T1_, &sq);
         if (e.code) return e;
-        CUDA_TRY(cudaMemsetAsync(red_, 0, 8, s));
-        GL(K_REDUCE, k_sqdiff<<<std::min(gC, 148), kThreads, 0, s>>>(nc, T1_, T_, red_));
-        CUDA_TRY(cudaMemcpyAsync(h_pinned_, red_, 8, cudaMemcpyDeviceToHost, s));
-        CUDA_TRY(cudaStreamSynchronize(s));
-        internal = h_pinned_[0] / nc;
+        internal = sq / nc;
         if (cfg.verbose) printf("iterations residual: %.17g\n", internal);
         if (!std::isfinite(internal) || ++steps >= 1000) return {-4, "Fourier pre-solve does not converge"};
     }
@@ -1648,28 +1815,231 @@ Error Solver::fourier_initial() {
     return set_initial(T0.data(), q0.data(), nullptr);
 }
 
-Error Solver::macro_solve(double *x, const double *b, long long &iters) {
-    return cg_solve(K_ptr_, K_idx_, K_val_, K_dinv_, x, b, cfg.macro_rtol, 0.0, iters, cg_scal_, cg_r_, cg_z_, cg_p_, cg_Ap_);
+constexpr int kCgThreads = 256;  // threads per CTA of the cluster-resident CG
+
+// Recursive coordinate bisection of cells [first, last) of ids into nparts
+// parts of near-equal size, split at the median of the axis of largest
+// extent; part boundaries are appended to bounds.
+static void rcb_split(std::vector<int> &ids, int first, int last, int nparts, const FlatMesh &m,
+                      std::vector<int> &bounds) {
+    if (nparts == 1 || last - first <= 1) {
+        for (int k = 0; k < nparts - 1; k++) bounds.push_back(last);
+        bounds.push_back(last);
+        return;
+    }
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    const double *cs[3] = {m.cx.data(), m.cy.data(), m.cz.data()};
+    for (int i = first; i < last; i++)
+        for (int a = 0; a < 3; a++) {
+            lo[a] = std::min(lo[a], cs[a][ids[i]]);
+            hi[a] = std::max(hi[a], cs[a][ids[i]]);
+        }
+    int ax = 0;
+    for (int a = 1; a < 3; a++)
+        if (hi[a] - lo[a] > hi[ax] - lo[ax]) ax = a;
+    const int nl = nparts / 2;
+    const int mid = first + (int)((long long)(last - first) * nl / nparts);
+    const double *c = cs[ax];
+    std::nth_element(ids.begin() + first, ids.begin() + mid, ids.begin() + last,
+                     [&](int u, int v) { return c[u] < c[v] || (c[u] == c[v] && u < v); });
+    rcb_split(ids, first, mid, nl, m, bounds);
+    rcb_split(ids, mid, last, nparts - nl, m, bounds);
 }
 
-// Jacobi-PCG on a negated (SPD) CSR system; scratch vectors and the 65536
-// reduction slots are passed in by the caller
-Error Solver::cg_solve(const int *ptr, const int *idx, const double *val, const double *dinv, double *x, const double *b,
-                       double rtol, double eta, long long &iters, double *scal, double *r, double *z, double *p,
-                       double *Ap) {
+// Cluster-resident CG plan for a CSR system (negated, SPD, one diagonal
+// entry per row) of mesh.nc rows: C = 16 parts by coordinate bisection,
+// then per part the ELL block, the halo (columns owned by other parts) and
+// the list of values this part sends into other parts' halos. C = 0 when
+// the parts do not fit in one CTA's shared memory or the device cannot
+// schedule the cluster.
+Error Solver::cg_plan(const std::vector<int> &ptr, const std::vector<int> &idx, const std::vector<double> &val,
+                      CgPlan &pl) {
+    pl = CgPlan{};
+    const int n = mesh.nc, C = 16;
+    if (n < C) return {0, ""};
+    int max_smem = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, cfg.device));
+    std::vector<int> perm(n), bounds{0};
+    for (int i = 0; i < n; i++) perm[i] = i;
+    rcb_split(perm, 0, n, C, mesh, bounds);
+    std::vector<int> newidx(n), owner(n);
+    for (int k = 0; k < C; k++)
+        for (int q = bounds[k]; q < bounds[k + 1]; q++) {
+            newidx[perm[q]] = q;
+            owner[q] = k;
+        }
+    int nrmax = 0, K = 0;
+    for (int k = 0; k < C; k++) nrmax = std::max(nrmax, bounds[k + 1] - bounds[k]);
+    for (int r = 0; r < n; r++) K = std::max(K, ptr[r + 1] - ptr[r] - 1);
+    // halos: per part, the (owner part, owner-local row) of each foreign column
+    std::vector<std::vector<std::pair<int, int>>> halo(C);
+    std::vector<std::unordered_map<int, int>> hslot(C);
+    std::vector<double> diag(n, 0.0);
+    std::vector<std::vector<std::pair<int, double>>> offd(n);  // new row -> (local column code, value)
+    for (int q = 0; q < n; q++) {
+        const int k = owner[q], old = perm[q], nrk = bounds[k + 1] - bounds[k];
+        bool has_diag = false;
+        for (int e = ptr[old]; e < ptr[old + 1]; e++) {
+            const int jn = newidx[idx[e]];
+            if (idx[e] == old) {
+                diag[q] = val[e];
+                has_diag = true;
+                continue;
+            }
+            int col;
+            if (owner[jn] == k) {
+                col = jn - bounds[k];
+            } else {
+                auto it = hslot[k].find(jn);
+                int h;
+                if (it == hslot[k].end()) {
+                    h = (int)halo[k].size();
+                    hslot[k][jn] = h;
+                    halo[k].push_back({owner[jn], jn - bounds[owner[jn]]});
+                } else {
+                    h = it->second;
+                }
+                col = -1 - h;  // resolved once nrk is known: nrk + h
+            }
+            offd[q].push_back({col < 0 ? nrk + (-1 - col) : col, val[e]});
+        }
+        if (!has_diag || !(diag[q] > 0)) return {0, ""};  // not the expected SPD form: grid-wide kernel
+    }
+    int hmax = 0;
+    for (int k = 0; k < C; k++) hmax = std::max(hmax, (int)halo[k].size());
+    // sends: part o stores its row l into part k's halo slot nr_k + h
+    std::vector<std::vector<std::pair<int, int>>> sends(C);
+    for (int k = 0; k < C; k++) {
+        const int nrk = bounds[k + 1] - bounds[k];
+        for (int h = 0; h < (int)halo[k].size(); h++)
+            sends[halo[k][h].first].push_back({halo[k][h].second, (k << 20) | (nrk + h)});
+    }
+    int smax = 0;
+    for (int k = 0; k < C; k++) smax = std::max(smax, (int)sends[k].size());
+    if (nrmax + hmax >= (1 << 20)) return {0, ""};
+    const size_t smem = 8 * ((size_t)8 * nrmax + hmax + 256 + (size_t)K * nrmax + smax) + 4 * ((size_t)K * nrmax + smax);
+    if (smem > (size_t)max_smem) return {0, ""};
+    CUDA_TRY(cudaFuncSetAttribute(k_cg_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_TRY(cudaFuncSetAttribute(k_cg_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(C);
+    lc.blockDim = dim3(kCgThreads);
+    lc.dynamicSmemBytes = smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, k_cg_cluster, &lc) != cudaSuccess || nclusters < 1) {
+        cudaGetLastError();
+        return {0, ""};
+    }
+    // device arrays; ELL padding: value 0 on the row's own (local) entry
+    const size_t ell = (size_t)C * K * nrmax;
+    std::vector<double> ev(std::max<size_t>(ell, 1), 0.0);
+    std::vector<int> ec(std::max<size_t>(ell, 1), 0), nh(C), ns(C), ssrc((size_t)C * std::max(smax, 1), 0),
+        sdst((size_t)C * std::max(smax, 1), 0);
+    for (int q = 0; q < n; q++) {
+        const int k = owner[q], i = q - bounds[k];
+        for (int kk = 0; kk < K; kk++) {
+            const size_t e = ((size_t)k * K + kk) * nrmax + i;
+            if (kk < (int)offd[q].size()) {
+                ec[e] = offd[q][kk].first;
+                ev[e] = offd[q][kk].second;
+            } else {
+                ec[e] = i;
+                ev[e] = 0.0;
+            }
+        }
+    }
+    for (int k = 0; k < C; k++) {
+        nh[k] = (int)halo[k].size();
+        ns[k] = (int)sends[k].size();
+        for (int e = 0; e < ns[k]; e++) {
+            ssrc[(size_t)k * smax + e] = sends[k][e].first;
+            sdst[(size_t)k * smax + e] = sends[k][e].second;
+        }
+    }
+    bool ok = true;
     cudaStream_t s = cfg.stream;
-    int nslots = 65536;
-    CUDA_TRY(cudaMemsetAsync(scal, 0, nslots * 8, s));
+    pl.part_ptr = upload(this, allocs_, bounds, s, ok);
+    pl.perm = upload(this, allocs_, perm, s, ok);
+    pl.ell_val = upload(this, allocs_, ev, s, ok);
+    pl.ell_col = upload(this, allocs_, ec, s, ok);
+    pl.diag = upload(this, allocs_, diag, s, ok);
+    pl.nhalo = upload(this, allocs_, nh, s, ok);
+    pl.nsend = upload(this, allocs_, ns, s, ok);
+    pl.snd_src = upload(this, allocs_, ssrc, s, ok);
+    pl.snd_dst = upload(this, allocs_, sdst, s, ok);
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (!ok) return {-6, "device allocation failed (cluster CG plan)"};
+    pl.C = C;
+    pl.K = K;
+    pl.nrmax = nrmax;
+    pl.hmax = hmax;
+    pl.smax = smax;
+    pl.smem = smem;
+    return {0, ""};
+}
+
+// Jacobi-preconditioned CG on a negated (SPD) CSR system, from the initial
+// guess in x. With a cluster plan the whole solve runs in one
+// cluster-resident kernel;
+// otherwise in the grid-wide cooperative kernel, with scratch vectors and
+// 65536 reduction slots passed in by the caller. When t1 is given, *sq
+// receives sum (x - t1)^2 of the solution. Waits for the stream.
+Error Solver::cg_solve(const CgPlan &pl, const int *ptr, const int *idx, const double *val, const double *dinv,
+                       double *x, const double *b, double rtol, double eta, long long &iters, double *scal, double *r,
+                       double *z, double *p, double *Ap, const double *t1, double *sq) {
+    cudaStream_t s = cfg.stream;
     int n = mesh.nc;
     int maxit = 20000;
+    cudaError_t lerr = cudaSuccess;
+    if (pl.C) {
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(pl.C);
+        lc.blockDim = dim3(kCgThreads);
+        lc.dynamicSmemBytes = pl.smem;
+        lc.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = pl.C;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        lc.attrs = at;
+        lc.numAttrs = 1;
+        GL(K_PCG, lerr = cudaLaunchKernelEx(&lc, k_cg_cluster, pl.K, pl.nrmax, pl.hmax, pl.smax,
+                                            (const int *)pl.part_ptr, (const int *)pl.perm, (const double *)pl.ell_val,
+                                            (const int *)pl.ell_col, (const double *)pl.diag, (const int *)pl.nhalo,
+                                            (const int *)pl.nsend, (const int *)pl.snd_src, (const int *)pl.snd_dst, b,
+                                            x, rtol, eta, maxit, t1, scal));
+        CUDA_TRY(lerr);
+        CUDA_TRY(cudaMemcpyAsync(h_pinned_ + 8, scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        iters += (long long)h_pinned_[8];
+        if (sq) *sq = t1 ? h_pinned_[9] : 0.0;
+        return {0, ""};
+    }
+    int nslots = 65536;
+    CUDA_TRY(cudaMemsetAsync(scal, 0, nslots * 8, s));
     void *args[] = {&n, (void *)&ptr, (void *)&idx, (void *)&val, (void *)&dinv, (void *)&b, &x, &r, &z, &p, &Ap,
                     &scal, &rtol, &eta, &maxit, &nslots};
-    cudaError_t lerr = cudaSuccess;
     GL(K_PCG, lerr = cudaLaunchCooperativeKernel((void *)k_pcg, dim3(coop_blocks_), dim3(kThreads), args, 0, s));
     CUDA_TRY(lerr);
-    CUDA_TRY(cudaMemcpyAsync(h_pinned_ + 8, scal + nslots - 1, 8, cudaMemcpyDeviceToHost, s));
+    // the CG uses slots below nslots - 1 only while slot + 3 < nslots, so
+    // nslots - 2 is free again after it
+    if (t1) {
+        CUDA_TRY(cudaMemsetAsync(scal + nslots - 2, 0, sizeof(double), s));
+        GL(K_REDUCE, k_sqdiff<<<std::min((n + kThreads - 1) / kThreads, 148), kThreads, 0, s>>>(n, t1, x,
+                                                                                                 scal + nslots - 2));
+    }
+    CUDA_TRY(cudaMemcpyAsync(h_pinned_ + 8, scal + nslots - 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
-    iters += (long long)h_pinned_[8];
+    iters += (long long)h_pinned_[9];
+    if (sq) *sq = t1 ? h_pinned_[8] : 0.0;
     return {0, ""};
 }
 
@@ -1777,8 +2147,9 @@ Error Solver::solve_t(SolveStats &st) {
             // from a warm start the residual must drop by kWarmEta; the
             // absolute floor macro_rtol * |b| still bounds the final error
             const bool warm = step < (int)warm_.size() && warm_[step] && warm_ok_[step];
-            Error e = cg_solve(K_ptr_, K_idx_, K_val_, K_dinv_, T_, rhs_, cfg.macro_rtol, warm ? kWarmEta : 0.0,
-                               st.cg_iterations, cg_scal_, cg_r_, cg_z_, cg_p_, cg_Ap_);
+            double sq = 0;
+            Error e = cg_solve(kplan_, K_ptr_, K_idx_, K_val_, K_dinv_, T_, rhs_, cfg.macro_rtol,
+                               warm ? kWarmEta : 0.0, st.cg_iterations, cg_scal_, cg_r_, cg_z_, cg_p_, cg_Ap_, T1_, &sq);
             prof_collect(st);
             if (!e.code) {
                 if (step >= (int)warm_.size()) {
@@ -1792,12 +2163,7 @@ Error Solver::solve_t(SolveStats &st) {
                 }
             }
             if (e.code) return e;
-            CUDA_TRY(cudaMemsetAsync(red_, 0, 8, s));
-            GL(K_REDUCE, k_sqdiff<<<std::min(gC, 148), kThreads, 0, s>>>(nc, T1_, T_, red_));
-            CUDA_TRY(cudaMemcpyAsync(h_pinned_, red_, 8, cudaMemcpyDeviceToHost, s));
-            CUDA_TRY(cudaStreamSynchronize(s));
-            prof_collect(st);
-            internal = h_pinned_[0] / nc;
+            internal = sq / nc;
             inner++;
             if (inner > 1 && internal > prev_internal) inner_inc++;
             prev_internal = internal;
@@ -1897,10 +2263,10 @@ Error Solver::get_fields(double *TE, double *TL, double *q, double *TB) {
 // every GPU loading this library holds until the process exits. Layout for a
 // problem of nc cells and ns node slots (both <= kNoAllocMaxCells): previous
 // iterate, node temperatures, right-hand side, the four CG vectors, then the
-// CG reduction slots and a small reduction output.
+// CG reduction slots.
 constexpr int kNoAllocMaxCells = 131072;
 constexpr int kNoAllocSlots = 65536;
-constexpr size_t kNoAllocDoubles = 7 * (size_t)kNoAllocMaxCells + kNoAllocSlots + 8;
+constexpr size_t kNoAllocDoubles = 7 * (size_t)kNoAllocMaxCells + kNoAllocSlots;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
 namespace {
@@ -1942,7 +2308,7 @@ Error Solver::fourier_initial_noalloc() {
     if (e0.code) return e0;
     const size_t N = kNoAllocMaxCells;
     double *T1 = base, *TV = base + N, *rhs = base + 2 * N, *r = base + 3 * N, *z = base + 4 * N, *pv = base + 5 * N,
-           *Ap = base + 6 * N, *scal = base + 7 * N, *red = scal + kNoAllocSlots;
+           *Ap = base + 6 * N, *scal = base + 7 * N;
     cudaStream_t s = cfg.stream;
     const int gC = (nc + kThreads - 1) / kThreads, gN = (nslot + kThreads - 1) / kThreads;
     double internal = 1000, h = 0;
@@ -1953,22 +2319,12 @@ Error Solver::fourier_initial_noalloc() {
         GL(K_TINTERP, k_tinterp<<<gN, kThreads, 0, s>>>(dm_, T_, TV));
         GL(K_MACRO_RHS, k_fourier_rhs<<<gC, kThreads, 0, s>>>(dm_, dp_.kappa, bF_dir_, bTF_, TV, rhs));
         CUDA_TRY(cudaGetLastError());
-        // the reduction slots must start at zero on every solve
-        CUDA_TRY(cudaMemsetAsync(scal, 0, kNoAllocSlots * sizeof(double), s));
-        int n = nc, maxit = 20000, nslots = kNoAllocSlots;
-        double rtol = cfg.macro_rtol, eta = 0.0;
-        void *args[] = {&n, (void *)&KF_ptr_, (void *)&KF_idx_, (void *)&KF_val_, (void *)&KF_dinv_, (void *)&rhs,
-                        (void *)&T_, (void *)&r, (void *)&z, (void *)&pv, (void *)&Ap, (void *)&scal, &rtol, &eta, &maxit,
-                        &nslots};
-        cudaError_t lerr = cudaSuccess;
-        GL(K_PCG, lerr = cudaLaunchCooperativeKernel((void *)k_pcg, dim3(coop_blocks_), dim3(kThreads), args, 0, s));
-        CUDA_TRY(lerr);
-        CUDA_TRY(cudaMemsetAsync(red, 0, sizeof(double), s));
-        GL(K_REDUCE, k_sqdiff<<<std::min(gC, 148), kThreads, 0, s>>>(nc, T1, T_, red));
-        CUDA_TRY(cudaMemcpyAsync(&h, red, sizeof(double), cudaMemcpyDeviceToHost, s));
-        CUDA_TRY(cudaStreamSynchronize(s));
+        // cg_solve zeroes the kNoAllocSlots reduction slots (65536) itself
+        // when it takes the grid-wide kernel
+        Error e = cg_solve(kfplan_, KF_ptr_, KF_idx_, KF_val_, KF_dinv_, T_, rhs, cfg.macro_rtol, 0.0, it, scal, r, z,
+                           pv, Ap, T1, &h);
+        if (e.code) return e;
         internal = h / nc;
-        it++;
         if (cfg.verbose) printf("iterations residual: %.17g\n", internal);
         if (!std::isfinite(internal) || ++steps >= 1000) return {-4, "Fourier pre-solve does not converge"};
     }

@@ -67,6 +67,18 @@ struct SolveStats {
     long long kernel_count[K_NUM] = {0};
 };
 
+// Launch plan of the cluster-resident CG for one CSR system: cluster size
+// (0 = the system does not fit, use the grid-wide kernel), the per-CTA
+// layout bounds (off-diagonals per row K, rows, halo entries, sends), the
+// dynamic shared memory and the partitioned system in device memory.
+struct CgPlan {
+    int C = 0, K = 0, nrmax = 0, hmax = 0, smax = 0;
+    size_t smem = 0;
+    int *part_ptr = nullptr, *perm = nullptr, *ell_col = nullptr, *nhalo = nullptr, *nsend = nullptr,
+        *snd_src = nullptr, *snd_dst = nullptr;
+    double *ell_val = nullptr, *diag = nullptr;
+};
+
 class Solver {
 public:
     ~Solver();
@@ -90,9 +102,12 @@ public:
 private:
     template <typename S, int DIM> Error solve_t(SolveStats &st);
     Error alloc_all();
-    Error macro_solve(double *x_dev, const double *rhs_dev, long long &iters);
-    Error cg_solve(const int *ptr, const int *idx, const double *val, const double *dinv, double *x, const double *b,
-                   double rtol, double eta, long long &iters, double *scal, double *r, double *z, double *p, double *Ap);
+    Error cg_solve(const CgPlan &pl, const int *ptr, const int *idx, const double *val, const double *dinv, double *x,
+                   const double *b, double rtol, double eta, long long &iters, double *scal, double *r, double *z,
+                   double *p, double *Ap, const double *t1, double *sq);
+    Error cg_plan(const std::vector<int> &ptr, const std::vector<int> &idx, const std::vector<double> &val,
+                  CgPlan &pl);
+    CgPlan kplan_, kfplan_;  // macro and Fourier systems
     void *dalloc(size_t bytes);
     std::vector<void *> allocs_;
     DMesh dm_{};
