@@ -266,14 +266,57 @@ __global__ void __launch_bounds__(256) k_gradient8(DMesh m, DPhys p, const S *__
     }
 }
 
-// Residual, BC bands per thread. The upwind side of a face is chosen by the
-// sign of s.n (shared by all bands; the reference's (|v| s).n differs from it
-// only by rounding when the face is tangent to the direction, where the
-// flux coefficient is zero).
+// Band-independent part of the face fluxes of the FP32 form's base field:
+// B[d][c] = sum_f A_f/V (s.n_f) beta_f, beta_f the second-order upwind face
+// value of T_base (T_base + grad T_base . r from the upwind cell; T_base of
+// the cell itself on boundary inflow faces). With it the residual's band
+// loop only handles the stored deviations. Zero in the FP64 form, whose
+// base is zero.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_base_flux(DMesh m, DPhys p, const double *__restrict__ Tb,
+                                                   const double *__restrict__ gTb, double *__restrict__ B) {
+    const int nc = m.nc;
+    const size_t total = (size_t)p.nd * nc;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int c = (int)(t % nc);
+        const size_t d = t / nc;
+        const double sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
+        const double invV = 1.0 / m.vol[c];
+        double acc = 0;
+        for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+            const double sn = sx * m.cf_nx[k] + sy * m.cf_ny[k] + (DIM == 3 ? sz * m.cf_nz[k] : 0.0);
+            const double a = m.cf_area[k] * invV * sn;
+            double beta;
+            if (sn >= 0) {
+                beta = Tb[c] + gTb[3 * c] * (m.cf_fx[k] - m.cx[c]) + gTb[3 * c + 1] * (m.cf_fy[k] - m.cy[c]);
+                if (DIM == 3) beta += gTb[3 * c + 2] * (m.cf_fz[k] - m.cz[c]);
+            } else if (m.cf_bound[k] < 0) {
+                const int j = m.cf_nbr[k];
+                beta = Tb[j] + gTb[3 * j] * (m.cf_fx[k] - m.cx[j]) + gTb[3 * j + 1] * (m.cf_fy[k] - m.cy[j]);
+                if (DIM == 3) beta += gTb[3 * j + 2] * (m.cf_fz[k] - m.cz[j]);
+            } else {
+                beta = Tb[c];
+            }
+            acc += a * beta;
+        }
+        B[t] = acc;
+    }
+}
+
+// Residual, BC bands per thread, in the storage precision S on the stored
+// deviations eps = e - C_b T_base (the base part enters through B):
+//   R = C_b (T_old - T_base - tau|v| B) + Q hr tau
+//       - eps_c - tau|v| sum_f A_f/V (s.n_f) y_f
+// with y_f the deviation of the second-order upwind face value
+// (eps + g . r of the upwind cell; e_wall - C_b T_base on boundary inflow
+// faces). The first two terms are formed in FP64 and rounded once. The
+// upwind side of a face is chosen by the sign of s.n (shared by all bands;
+// the reference's (|v| s).n differs from it only by rounding when the face
+// is tangent to the direction, where the flux coefficient is zero).
 template <typename S, int DIM, int BC>
-__global__ void __launch_bounds__(256) k_residual8(DMesh m, DPhys p, EView<S, DIM> ev, const double *__restrict__ Told,
-                                                   const double *__restrict__ eb, const int *__restrict__ pos_of,
-                                                   S *__restrict__ Rlo) {
+__global__ void __launch_bounds__(256, sizeof(S) == 4 ? 4 : 2) k_residual8(DMesh m, DPhys p, EView<S, DIM> ev, const double *__restrict__ Bf,
+                                                   const double *__restrict__ Told, const double *__restrict__ eb,
+                                                   const int *__restrict__ pos_of, S *__restrict__ Rlo) {
     const int nb = p.nb, nc = m.nc, nbc = nb / BC;
     const size_t total = (size_t)p.nd * nc * nbc;
     for (size_t t = gtid(); t < total; t += gstride()) {
@@ -283,25 +326,15 @@ __global__ void __launch_bounds__(256) k_residual8(DMesh m, DPhys p, EView<S, DI
         const size_t d = dc / nc;
         const double sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
         const size_t dbase = d * nc;
-        double Cb[BC], tv[BC], acc[BC], ec[BC];
-        S v[BC], gxv[BC], gyv[BC], gzv[BC];
-        const double invV = 1.0 / m.vol[c];
-        {
-            ld8(ev.eps + (dbase + c) * nb + b0, v);
-            const double tb = ev.Tb[c];
+        S ec[BC], acc[BC], gxv[BC], gyv[BC], gzv[BC];
+        const double invV = 1.0 / m.vol[c], tb = ev.Tb[c];
+        ld8(ev.eps + (dbase + c) * nb + b0, ec);
 #pragma unroll
-            for (int i = 0; i < BC; i++) {
-                Cb[i] = p.C[b0 + i];
-                tv[i] = p.tau[b0 + i] * p.vmag[b0 + i];
-                ec[i] = Cb[i] * tb + (double)v[i];
-                acc[i] = 0;
-            }
-        }
-        const double gbx = ev.gTb[3 * c], gby = ev.gTb[3 * c + 1], gbz = ev.gTb[3 * c + 2];
+        for (int i = 0; i < BC; i++) acc[i] = (S)0;
         bool have_gc = false;
         for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
             const double sn = sx * m.cf_nx[k] + sy * m.cf_ny[k] + (DIM == 3 ? sz * m.cf_nz[k] : 0.0);
-            const double a = m.cf_area[k] * invV * sn;
+            const S a = (S)(m.cf_area[k] * invV * sn);
             if (sn >= 0) {
                 if (!have_gc) {
                     const S *gp = ev.g + (dbase + c) * DIM * nb + b0;
@@ -310,12 +343,13 @@ __global__ void __launch_bounds__(256) k_residual8(DMesh m, DPhys p, EView<S, DI
                     if (DIM == 3) ld8(gp + 2 * nb, gzv);
                     have_gc = true;
                 }
-                const double rx = m.cf_fx[k] - m.cx[c], ry = m.cf_fy[k] - m.cy[c], rz = m.cf_fz[k] - m.cz[c];
+                const S rx = (S)(m.cf_fx[k] - m.cx[c]), ry = (S)(m.cf_fy[k] - m.cy[c]);
+                const S rz = DIM == 3 ? (S)(m.cf_fz[k] - m.cz[c]) : (S)0;
 #pragma unroll
                 for (int i = 0; i < BC; i++) {
-                    double x = ec[i] + ((double)gxv[i] + Cb[i] * gbx) * rx + ((double)gyv[i] + Cb[i] * gby) * ry;
-                    if (DIM == 3) x += ((double)gzv[i] + Cb[i] * gbz) * rz;
-                    acc[i] += tv[i] * a * x;
+                    S y = ec[i] + gxv[i] * rx + gyv[i] * ry;
+                    if (DIM == 3) y += gzv[i] * rz;
+                    acc[i] += a * y;
                 }
             } else if (m.cf_bound[k] < 0) {
                 const int j = m.cf_nbr[k];
@@ -325,25 +359,28 @@ __global__ void __launch_bounds__(256) k_residual8(DMesh m, DPhys p, EView<S, DI
                 ld8(gp, hx);
                 ld8(gp + nb, hy);
                 if (DIM == 3) ld8(gp + 2 * nb, hz);
-                const double tj = ev.Tb[j], jx = ev.gTb[3 * j], jy = ev.gTb[3 * j + 1], jz = ev.gTb[3 * j + 2];
-                const double rx = m.cf_fx[k] - m.cx[j], ry = m.cf_fy[k] - m.cy[j], rz = m.cf_fz[k] - m.cz[j];
+                const S rx = (S)(m.cf_fx[k] - m.cx[j]), ry = (S)(m.cf_fy[k] - m.cy[j]);
+                const S rz = DIM == 3 ? (S)(m.cf_fz[k] - m.cz[j]) : (S)0;
 #pragma unroll
                 for (int i = 0; i < BC; i++) {
-                    double x = Cb[i] * tj + (double)ej[i] + ((double)hx[i] + Cb[i] * jx) * rx + ((double)hy[i] + Cb[i] * jy) * ry;
-                    if (DIM == 3) x += ((double)hz[i] + Cb[i] * jz) * rz;
-                    acc[i] += tv[i] * a * x;
+                    S y = ej[i] + hx[i] * rx + hy[i] * ry;
+                    if (DIM == 3) y += hz[i] * rz;
+                    acc[i] += a * y;
                 }
             } else {
                 const double *e = eb + (d * m.nbs + m.cf_bside[k]) * nb + b0;
 #pragma unroll
-                for (int i = 0; i < BC; i++) acc[i] += tv[i] * a * e[i];
+                for (int i = 0; i < BC; i++) acc[i] += a * (S)(e[i] - p.C[b0 + i] * tb);
             }
         }
-        const double To = Told[c], hc = m.heat[c];
+        const double dT = Told[c] - tb, B = Bf[dc], hc = m.heat[c];
         S out[BC];
 #pragma unroll
-        for (int i = 0; i < BC; i++)
-            out[i] = (S)(Cb[i] * To + hc * p.hr[b0 + i] * p.tau[b0 + i] - ec[i] - acc[i]);
+        for (int i = 0; i < BC; i++) {
+            const double tv = p.tau[b0 + i] * p.vmag[b0 + i];
+            const S fixed = (S)(p.C[b0 + i] * (dT - tv * B) + hc * p.hr[b0 + i] * p.tau[b0 + i]);
+            out[i] = fixed - ec[i] - (S)tv * acc[i];
+        }
         st8(Rlo + (dbase + pos_of[dc]) * nb + b0, out);
     }
 }
@@ -1697,6 +1734,7 @@ Error Solver::alloc_all() {
     grad_ = A(ne * mesh.dim * S);
     res_ = A(ne * S);
     Tbase_ = (double *)A(nc * 8);
+    Bflux_ = (double *)A((size_t)nd * nc * 8);
     gTb_ = (double *)A(nc * 3 * 8);
     eb_ = (double *)A(nd * nbs * nb * 8);
     eb_snap_ = need_snapshot_ ? (double *)A(nd * nbs * nb * 8) : nullptr;
@@ -1724,7 +1762,7 @@ Error Solver::alloc_all() {
     cg_p_ = (double *)A(nc * 8);
     cg_Ap_ = (double *)A(nc * 8);
     cg_scal_ = (double *)A(65536 * 8);
-    for (void *pp : {eps_, grad_, res_, (void *)Tbase_, (void *)eb_, (void *)cg_scal_})
+    for (void *pp : {eps_, grad_, res_, (void *)Tbase_, (void *)Bflux_, (void *)eb_, (void *)cg_scal_})
         if (!pp) return {-6, "device allocation failed (" + std::to_string(ne * S * 5 / 1048576) + " MiB of band state)"};
     if (cudaMallocHost((void **)&h_pinned_, 16 * sizeof(double)) != cudaSuccess) return {-6, "pinned allocation failed"};
     cudaStream_t s = cfg.stream;
@@ -2098,6 +2136,8 @@ Error Solver::solve_t(SolveStats &st) {
         CUDA_TRY(cudaGetLastError());
         started_ = true;
     }
+    // base-field face fluxes for the current T_base (zero base in FP64)
+    GL(K_INIT, (k_base_flux<DIM><<<grid_for((size_t)nd * nc), kThreads, 0, s>>>(dm_, dp_, Tbase_, gTb_, Bflux_)));
     double errOld = 0, errOldq = 0;
     int errInc = 0;
     st = SolveStats();
@@ -2113,7 +2153,7 @@ Error Solver::solve_t(SolveStats &st) {
         CUDA_TRY(cudaMemcpyAsync(qold_, q_, (size_t)nc * 24, cudaMemcpyDeviceToDevice, s));
         if (nb % 4 == 0) {
             GL(K_GRADIENT, (k_gradient8<S, DIM, 4><<<gE8, kThreads, 0, s>>>(dm_, dp_, w, eps, g)));
-            GL(K_RESIDUAL, (k_residual8<S, DIM, 4><<<gE8, kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, pos_of_, R)));
+            GL(K_RESIDUAL, (k_residual8<S, DIM, 4><<<gE8, kThreads, 0, s>>>(dm_, dp_, ev, Bflux_, Told_, eb_, pos_of_, R)));
         } else {
             GL(K_GRADIENT, (k_gradient<S, DIM><<<gE, kThreads, 0, s>>>(dm_, dp_, w, eps, g)));
             GL(K_RESIDUAL, (k_residual<S, DIM><<<gE, kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, pos_of_, R)));
@@ -2215,6 +2255,8 @@ Error Solver::solve_t(SolveStats &st) {
                 GL(K_INIT, k_copy<<<gC, kThreads, 0, s>>>(T_, Tbase_, nc));
                 GL(K_INIT, k_rebase<S><<<gE, kThreads, 0, s>>>(dm_, dp_, T1_, Tbase_, eps));
                 GL(K_INIT, k_cell_lsq_grad<<<gC, kThreads, 0, s>>>(dm_, Tbase_, gTb_));
+                GL(K_INIT, (k_base_flux<DIM><<<grid_for((size_t)nd * nc), kThreads, 0, s>>>(dm_, dp_, Tbase_, gTb_,
+                                                                                            Bflux_)));
             }
         }
         if (errInc >= 10) {

@@ -115,6 +115,7 @@ private:
     // state
     void *eps_ = nullptr, *grad_ = nullptr, *res_ = nullptr;  // storage-type arrays
     double *Tbase_ = nullptr, *gTb_ = nullptr;
+    double *Bflux_ = nullptr;  // [nd][nc] base-field face flux sums of the residual
     double *eb_ = nullptr, *eb_snap_ = nullptr;
     double *T_ = nullptr, *Told_ = nullptr, *Tlat_ = nullptr, *E_ = nullptr, *q_ = nullptr, *qold_ = nullptr,
            *Tband_ = nullptr, *remacro_ = nullptr, *Th_ = nullptr, *Q_ = nullptr, *Ths_ = nullptr, *Qs_ = nullptr,
