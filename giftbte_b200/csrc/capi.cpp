@@ -211,6 +211,13 @@ static int inspect_common(const gbte::RawMesh &raw, const gbte::Bands &bands_in,
     info->kappa_bulk = bands.kappa[0];
     info->capacity_bulk = bands.capb[0];
     for (double v : fm.vol) info->total_volume += v;
+    gbte::SweepPlan sp;
+    e = gbte::build_sweep_plan(fm, ang, sch, gbte::kSweepMinRing, gbte::kSweepFarCap, sp);
+    if (e.code) return fail(nullptr, e), status_of(e.code);
+    info->max_level_width = sp.max_width;
+    info->sweep_ring = sp.ring;
+    info->far_slots = sp.far_slots;
+    info->far_refs = sp.far_refs;
     return GBTE_OK;
 }
 

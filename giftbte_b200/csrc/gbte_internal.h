@@ -109,8 +109,37 @@ struct Deck {
 };
 Error read_deck(const std::string &dir, Deck &deck);
 
+// Level-order records of the upwind sweep of every direction, position P =
+// d*nc + (index in the direction's level order). The sweep keeps the
+// corrections of the last `ring` positions (a power of two, at least the
+// widest level) on chip; an upwind reference further back is a far
+// reference. With far slots enabled (far_cap > 0), the cell read that way
+// also stores its correction into an on-chip far slot, allocated per
+// direction over the interval from its own level to its last far reader's
+// level; np then holds -(1 + slot) for that neighbour. Without far slots,
+// np always holds the neighbour's position and far references are read
+// from global memory.
+struct SweepPlan {
+    int ring = 0, max_width = 0, far_slots = 0;
+    long long far_refs = 0;  // upwind references outside the ring (all directions)
+    bool far_enabled = false;
+    std::vector<int> np;      // [nd*nc*4] position (>= 0) or -(1 + far slot)
+    std::vector<double> a;    // [nd*nc*4] A_f/V (s.n_f) of the upwind faces (< 0)
+    std::vector<double> sig;  // [nd*nc] sum of the outgoing A_f/V (s.n_f)
+    std::vector<int> nin;     // [nd*nc] upwind neighbours (<= 4)
+    std::vector<int> cell;    // [nd*nc] the cell at this position
+    std::vector<int> far_w;   // [nd*nc] far slot this cell stores into, -1 none
+};
+
 Error make_angles(int method, int ntheta, int nphi, int material_dim, Angles &out);
 Error build_flat_mesh(const RawMesh &raw, const BCs &bcs, const Bands &bands, FlatMesh &out);
 void build_schedule(const FlatMesh &m, const Angles &a, Schedule &out, int nthreads);
+// min_ring: the smallest ring (rounded up to a power of two and to the
+// widest level); far_cap: most far slots allowed, 0 disables them. The
+// solver uses kSweepMinRing and kSweepFarCap.
+constexpr int kSweepMinRing = 512;
+constexpr int kSweepFarCap = 2048;
+Error build_sweep_plan(const FlatMesh &m, const Angles &a, const Schedule &s, int min_ring, int far_cap,
+                       SweepPlan &out);
 
 }  // namespace gbte

@@ -19,6 +19,7 @@
 #include <cmath>
 #include <numeric>
 #include <queue>
+#include <string>
 #include <thread>
 
 #include "gbte_internal.h"
@@ -580,6 +581,119 @@ void build_schedule(const FlatMesh &m, const Angles &a, Schedule &s, int nthread
         for (int d = 0; d < nd; d++) std::copy(dir_lag[d].begin(), dir_lag[d].end(), s.lag.begin() + (size_t)d * nc);
     } else
         s.lag.clear();
+}
+
+Error build_sweep_plan(const FlatMesh &m, const Angles &a, const Schedule &s, int min_ring, int far_cap,
+                       SweepPlan &out) {
+    const int nc = m.nc, nd = a.nd;
+    out = SweepPlan{};
+    for (int d = 0; d < nd; d++)
+        for (int k = s.dir_lvl_off[d]; k + 1 < s.dir_lvl_off[d + 1]; k++)
+            out.max_width = std::max(out.max_width, s.lvl_ptr[k + 1] - s.lvl_ptr[k]);
+    int ring = 1;
+    while (ring < std::max(min_ring, out.max_width)) ring *= 2;
+    out.ring = ring;
+    const size_t N = (size_t)nd * nc;
+    out.np.assign(4 * N, 0);
+    out.a.assign(4 * N, 0.0);
+    out.sig.assign(N, 0.0);
+    out.nin.assign(N, 0);
+    out.cell.assign(N, 0);
+    out.far_w.assign(N, -1);
+    std::vector<int> np_far(4 * N, 0);  // np with far references encoded as slots
+    std::vector<int> dir_slots(nd, 0);
+    std::vector<long long> dir_refs(nd, 0);
+    std::vector<std::string> dir_err(nd);
+    auto work = [&](int d) {
+        const int *lc = &s.lvl_cells[(size_t)d * nc];
+        const int *lp = &s.lvl_ptr[s.dir_lvl_off[d]];
+        const int nl = s.dir_lvl_off[d + 1] - s.dir_lvl_off[d] - 1;
+        std::vector<int> po(nc), lev(nc), last_read(nc, -1);
+        for (int l = 0; l < nl; l++)
+            for (int pos = lp[l]; pos < lp[l + 1]; pos++) {
+                po[lc[pos]] = pos;
+                lev[pos] = l;
+            }
+        const size_t P0 = (size_t)d * nc;
+        for (int pos = 0; pos < nc; pos++) {
+            const size_t P = P0 + pos;
+            const int c = lc[pos];
+            out.cell[P] = c;
+            const unsigned lm = s.lag.empty() ? 0u : s.lag[P0 + c];
+            double sig = 0;
+            int j = 0, nin = 0;
+            for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++, j++) {
+                const double dpn = a.sx[d] * m.cf_nx[k] + a.sy[d] * m.cf_ny[k] + a.sz[d] * m.cf_nz[k];
+                const double av = m.cf_area[k] / m.vol[c] * dpn;
+                if (dpn >= 0)
+                    sig += av;
+                else if (m.cf_bound[k] < 0 && !((lm >> j) & 1u)) {
+                    if (nin >= 4) {
+                        dir_err[d] = "a cell has more than four upwind neighbours";
+                        return;
+                    }
+                    const int q = po[m.cf_nbr[k]];
+                    out.np[4 * P + nin] = q;
+                    out.a[4 * P + nin] = av;
+                    if (q < lp[lev[pos] + 1] - ring) {
+                        last_read[q] = std::max(last_read[q], lev[pos]);
+                        dir_refs[d]++;
+                    }
+                    nin++;
+                }
+            }
+            out.sig[P] = sig;
+            out.nin[P] = nin;
+        }
+        // far slots: a slot is taken at its writer's level and free again
+        // from the level after its last reader's
+        std::vector<int> slot(nc, -1), freel;
+        std::vector<std::vector<int>> release(nl + 1);
+        int nslots = 0;
+        for (int l = 0; l < nl; l++) {
+            for (int sl : release[l]) freel.push_back(sl);
+            for (int pos = lp[l]; pos < lp[l + 1]; pos++) {
+                if (last_read[pos] < 0) continue;
+                int sl;
+                if (!freel.empty()) {
+                    sl = freel.back();
+                    freel.pop_back();
+                } else {
+                    sl = nslots++;
+                }
+                slot[pos] = sl;
+                release[last_read[pos] + 1].push_back(sl);
+            }
+        }
+        dir_slots[d] = nslots;
+        for (int pos = 0; pos < nc; pos++) {
+            const size_t P = P0 + pos;
+            for (int jj = 0; jj < 4; jj++) {
+                const int q = out.np[4 * P + jj];
+                np_far[4 * P + jj] = (jj < out.nin[P] && q < lp[lev[pos] + 1] - ring) ? -(1 + slot[q]) : q;
+            }
+        }
+        for (int pos = 0; pos < nc; pos++) out.far_w[P0 + pos] = slot[pos];
+    };
+    const int nthreads = std::max(1, std::min((int)std::max(1u, std::thread::hardware_concurrency()), nd));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthreads; t++)
+        pool.emplace_back([&, t]() {
+            for (int d = t; d < nd; d += nthreads) work(d);
+        });
+    for (auto &th : pool) th.join();
+    for (int d = 0; d < nd; d++)
+        if (!dir_err[d].empty()) return {-8, dir_err[d]};
+    for (int d = 0; d < nd; d++) {
+        out.far_slots = std::max(out.far_slots, dir_slots[d]);
+        out.far_refs += dir_refs[d];
+    }
+    out.far_enabled = far_cap > 0 && out.far_slots <= far_cap;
+    if (out.far_enabled)
+        out.np.swap(np_far);
+    else
+        std::fill(out.far_w.begin(), out.far_w.end(), -1);
+    return {0, ""};
 }
 
 }  // namespace gbte

@@ -243,20 +243,31 @@ __global__ void __launch_bounds__(256) k_gradient8(DMesh m, DPhys p, const S *__
         const size_t dc = t / nbc;
         const int c = (int)(dc % nc);
         const S *ed = eps + (dc - c) * nb + BC * bc;
-        S ec[BC], ek[BC], gx[BC], gy[BC], gz[BC];
+        S ec[BC], gx[BC], gy[BC], gz[BC];
         ld8(ed + (size_t)c * nb, ec);
 #pragma unroll
         for (int i = 0; i < BC; i++) gx[i] = gy[i] = gz[i] = 0;
+        // neighbours in groups of four: the four rows are requested before
+        // any is used, so four loads per thread are in flight
         const int q1 = m.nbr_ptr[c + 1];
-        for (int q = m.nbr_ptr[c]; q < q1; q++) {
-            ld8(ed + (size_t)m.nbr_idx[q] * nb, ek);
-            const S wx = w[3 * q], wy = w[3 * q + 1], wz = DIM == 3 ? w[3 * q + 2] : S(0);
+        for (int q = m.nbr_ptr[c]; q < q1; q += 4) {
+            S e4[4][BC];
+            int jn[4];
 #pragma unroll
-            for (int i = 0; i < BC; i++) {
-                const S de = ek[i] - ec[i];
-                gx[i] += wx * de;
-                gy[i] += wy * de;
-                if (DIM == 3) gz[i] += wz * de;
+            for (int u = 0; u < 4; u++) jn[u] = q + u < q1 ? m.nbr_idx[q + u] : c;
+#pragma unroll
+            for (int u = 0; u < 4; u++) ld8(ed + (size_t)jn[u] * nb, e4[u]);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                if (q + u >= q1) break;
+                const S wx = w[3 * (q + u)], wy = w[3 * (q + u) + 1], wz = DIM == 3 ? w[3 * (q + u) + 2] : S(0);
+#pragma unroll
+                for (int i = 0; i < BC; i++) {
+                    const S de = e4[u][i] - ec[i];
+                    gx[i] += wx * de;
+                    gy[i] += wy * de;
+                    if (DIM == 3) gz[i] += wz * de;
+                }
             }
         }
         S *gp = g + dc * DIM * nb + BC * bc;
@@ -401,17 +412,21 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // One cell of a direction's level order, as the sweep reads it: up to four
-// upwind neighbours (their positions in the same level order) with their
-// coefficients a_j = A_f/V (s.n_f) < 0, sig = sum of the outgoing A_f/V (s.n_f),
-// and the neighbour count. 48 bytes in FP32 storage, 64 in FP64, so that a
-// level's records are one contiguous range copied in 16-byte pieces.
+// upwind neighbours (their positions in the same level order, or -(1 +
+// far slot)) with their coefficients a_j = A_f/V (s.n_f) < 0, sig = sum of
+// the outgoing A_f/V (s.n_f), meta = neighbour count | (1 + the far slot
+// this cell stores into, 0 for none) << 3, and the cell itself. 48 bytes in
+// FP32 storage, 64 in FP64, so that a level's records are one contiguous
+// range copied in 16-byte pieces.
 template <typename S>
 struct alignas(16) SweepRec {
     int np[4];
     S a[4];
     S sig;
-    int nin;
+    int meta;
+    int cell;
 };
+
 
 static_assert(sizeof(SweepRec<float>) == 48 && sizeof(SweepRec<double>) == 64, "sweep record layout");
 
@@ -425,25 +440,32 @@ __device__ __forceinline__ double sweep_div(double x, double y) { return x / y; 
 // d_c = (R_c - kb sum_j a_j d_j) / (1 + kb sig_c), kb = tau |v| of the band.
 // Records and residuals are in level order, so a level's operands are
 // contiguous: they are staged into shared memory LOOK-1 levels ahead with
-// cp.async. The corrections of the last ring_n positions live in a shared
-// ring (ring_n a power of two >= widest level, so one level's writes never
-// collide); older ones are read back from global memory, where every
-// correction is also stored in place of its residual. Shared memory:
+// cp.async. Every correction is stored in cell order, Dc[d][cell][b], for
+// the update that follows; the corrections of the last ring_n positions
+// also live in a shared ring (ring_n a power of two >= widest level, so one
+// level's writes never collide). A cell read after it has left the ring
+// also stores its correction into a shared far slot named by its record
+// (nfar > 0); without far slots such reads go back to Dc through the level
+// order's cell list. Shared memory:
 //   LOOK slots of { SweepRec[LCAP], R[LCAP][nbc] S }, the ring
-//   [ring_n][nbc] S, and the direction's level bounds [max_lev + 1] i32.
+//   [ring_n][nbc] S, the far slots [nfar][nbc] S, and the direction's level
+//   bounds [max_lev + 1] i32.
 // Levels longer than LCAP read their overflow records from global memory.
 // rvec: the band chunk of a residual row is copied in 16-byte pieces (its
 // byte size, offset and the row pitch are multiples of 16).
 template <typename S, int LOOK, int LCAP>
-__global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int nbc, int ring_n, int rvec,
+__global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int nbc, int ring_n, int nfar, int rvec,
                                                const int *__restrict__ lvl_ptr, const int *__restrict__ dir_lvl_off,
-                                               const SweepRec<S> *__restrict__ rec, const double *__restrict__ kbv,
-                                               S *Rlo) {
+                                               const SweepRec<S> *__restrict__ rec, const int *__restrict__ lvl_cells,
+                                               const double *__restrict__ kbv, const S *__restrict__ Rlo,
+                                               S *__restrict__ Dc) {
     extern __shared__ __align__(16) unsigned char wsm[];
     const size_t rbytes = ((size_t)LCAP * nbc * sizeof(S) + 15) & ~(size_t)15;
     const size_t slot_bytes = (size_t)LCAP * sizeof(SweepRec<S>) + rbytes;
     S *ring = reinterpret_cast<S *>(wsm + LOOK * slot_bytes);
-    int *lp = reinterpret_cast<int *>(wsm + LOOK * slot_bytes + (((size_t)ring_n * nbc * sizeof(S) + 15) & ~(size_t)15));
+    S *far = reinterpret_cast<S *>(wsm + LOOK * slot_bytes + (((size_t)ring_n * nbc * sizeof(S) + 15) & ~(size_t)15));
+    int *lp = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(far) +
+                                      (((size_t)nfar * nbc * sizeof(S) + 15) & ~(size_t)15));
     const int nchunks = (nb + nbc - 1) / nbc;
     const int d = blockIdx.x / nchunks, chunk = blockIdx.x % nchunks;
     const int b0 = chunk * nbc, nbl = min(nbc, nb - b0);
@@ -496,51 +518,59 @@ __global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int nbc, int ring
             const bool st = li < LCAP;
             const SweepRec<S> r = st ? srec[li] : rec[P];
             const S r0 = st ? sR[li * nbc + lb] : Rlo[P * nb + b0 + lb];
+            const int nin = r.meta & 7, fw = (r.meta >> 3) - 1;
             S sum = (S)0;
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const int q = r.np[j];
-                if (j < r.nin) {
-                    const S dj = (q >= lo) ? ring[(q & mask) * nbc + lb] : Rlo[(base + q) * nb + b0 + lb];
+                if (j < nin) {
+                    const S dj = q >= lo  ? ring[(q & mask) * nbc + lb]
+                                 : q < 0 ? far[(-1 - q) * nbc + lb]
+                                         : Dc[(base + lvl_cells[base + q]) * nb + b0 + lb];
                     sum += r.a[j] * dj;
                 }
             }
             const S dl = sweep_div(r0 - kb * sum, (S)1 + kb * r.sig);
-            Rlo[P * nb + b0 + lb] = dl;
+            Dc[(base + r.cell) * nb + b0 + lb] = dl;
+            if (fw >= 0) far[fw * nbc + lb] = dl;
             ring[((c0 + li) & mask) * nbc + lb] = dl;
         }
     }
     cp_async_wait<0>();
 }
 
-// e += d (corrections gathered from level order) fused with the moments,
-// one thread per (cell, band) looping over directions with the angular
-// weights of every moment tabulated in shared memory:
+// e += d (the sweep's corrections, cell order) fused with the moments, one
+// thread per (cell, band) looping over directions with the angular weights
+// of every moment tabulated in shared memory:
 //   S0 = sum_d w e, S1 = sum_d w s e, S2 = sum_d w s s^T e
 //   Tlat = sum_b lat S0 / C     (temperature, StaticBTESynthetic.cpp:2493)
 //   Tband[b] = S0 / C           (:2494)
 //   E = sum_b S0 / C_bulk        (:2504)
 //   q = sum_b |v| S1             (:2515-2517)
 //   Th = kappa sum_{hr>0} lat S0 / C,  Q = sum_{hr>0} tau |v|^2 S2
-// (the two moments of the synthetic source). blockDim = cpb * nb.
+// (the two moments of the synthetic source). blockDim = cpb * nb. The band
+// sums of each cell are formed in shared memory in band order (no atomics),
+// so the moments are reproducible bit for bit.
 constexpr int kMomSlots = 12;
 constexpr int kWTab = 10;
+constexpr int kMomUnroll = 8;
 
 template <typename S>
-__global__ void k_moments(DMesh m, DPhys p, int cpb, S *__restrict__ eps, const S *__restrict__ Rlo,
-                          const int *__restrict__ pos_of, const double *__restrict__ Tb,
-                          const double *__restrict__ wtab, double *__restrict__ Tlat, double *__restrict__ E,
-                          double *__restrict__ q, double *__restrict__ Tband, double *__restrict__ Th,
-                          double *__restrict__ Q, int apply) {
+__global__ void __launch_bounds__(256) k_moments(DMesh m, DPhys p, int cpb, S *__restrict__ eps,
+                                                 const S *__restrict__ Dc, const double *__restrict__ Tb,
+                                                 const double *__restrict__ wtab, double *__restrict__ Tlat,
+                                                 double *__restrict__ E, double *__restrict__ q,
+                                                 double *__restrict__ Tband, double *__restrict__ Th,
+                                                 double *__restrict__ Q, int apply) {
     extern __shared__ double sm_dyn[];
-    double *wt = sm_dyn;                         // [nd][kWTab]
-    double *smom = sm_dyn + (size_t)p.nd * kWTab;  // [cpb][kMomSlots]
-    const int nb = p.nb, nc = m.nc;
-    for (int i = threadIdx.x; i < p.nd * kWTab; i += blockDim.x) wt[i] = wtab[i];
-    for (int i = threadIdx.x; i < cpb * kMomSlots; i += blockDim.x) smom[i] = 0;
+    double *wt = sm_dyn;                           // [nd][kWTab]
+    double *part = sm_dyn + (size_t)p.nd * kWTab;  // [blockDim][kMomSlots]
+    const int nb = p.nb, nc = m.nc, nd = p.nd;
+    for (int i = threadIdx.x; i < nd * kWTab; i += blockDim.x) wt[i] = wtab[i];
     __syncthreads();
     const int lc = threadIdx.x / nb, b = threadIdx.x % nb;
     const int c = blockIdx.x * cpb + lc;
+    double *mine = part + (size_t)threadIdx.x * kMomSlots;
     if (lc < cpb && c < nc) {
         const double Cb = p.C[b];
         const double base = Cb * Tb[c];
@@ -549,47 +579,60 @@ __global__ void k_moments(DMesh m, DPhys p, int cpb, S *__restrict__ eps, const 
         for (int i = 0; i < kWTab; i++) a[i] = 0;
         const size_t stride = (size_t)nc * nb;
         S *e0 = eps + (size_t)c * nb + b;
-        const int *po = pos_of + c;
-#pragma unroll 4
-        for (int d = 0; d < p.nd; d++) {
-            S ev = e0[d * stride];
-            if (apply) {
-                ev += Rlo[((size_t)d * nc + po[(size_t)d * nc]) * nb + b];
-                e0[d * stride] = ev;
-            }
-            const double e = base + (double)ev;
-            const double *w = wt + kWTab * d;
+        const S *d0 = Dc + (size_t)c * nb + b;
+        for (int d = 0; d < nd; d += kMomUnroll) {
+            S ev[kMomUnroll], dv[kMomUnroll];
 #pragma unroll
-            for (int i = 0; i < kWTab; i++) a[i] += w[i] * e;
+            for (int u = 0; u < kMomUnroll; u++) {
+                ev[u] = (S)0;
+                dv[u] = (S)0;
+                if (d + u < nd) {
+                    ev[u] = e0[(size_t)(d + u) * stride];
+                    if (apply) dv[u] = d0[(size_t)(d + u) * stride];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kMomUnroll; u++) {
+                if (d + u >= nd) break;
+                const S en = ev[u] + dv[u];
+                if (apply) e0[(size_t)(d + u) * stride] = en;
+                const double e = base + (double)en;
+                const double *w = wt + kWTab * (d + u);
+#pragma unroll
+                for (int i = 0; i < kWTab; i++) a[i] += w[i] * e;
+            }
         }
         Tband[(size_t)b * nc + c] = a[0] / Cb;
         const double vm = p.vmag[b], lat = p.lat[b];
         const double tl = lat * a[0] / Cb;
-        double *smc = smom + kMomSlots * lc;
-        atomicAdd(&smc[0], tl);
-        atomicAdd(&smc[1], a[0] / p.capb);
-        atomicAdd(&smc[2], vm * a[1]);
-        atomicAdd(&smc[3], vm * a[2]);
-        atomicAdd(&smc[4], vm * a[3]);
-        if (p.hr[b] > 0) {
-            const double f = p.tau[b] * vm * vm;
-            atomicAdd(&smc[5], tl);
+        const bool syn = p.hr[b] > 0;
+        const double f = p.tau[b] * vm * vm;
+        mine[0] = tl;
+        mine[1] = a[0] / p.capb;
+        mine[2] = vm * a[1];
+        mine[3] = vm * a[2];
+        mine[4] = vm * a[3];
+        mine[5] = syn ? tl : 0.0;
 #pragma unroll
-            for (int i = 0; i < 6; i++) atomicAdd(&smc[6 + i], f * a[4 + i]);
-        }
+        for (int i = 0; i < 6; i++) mine[6 + i] = syn ? f * a[4 + i] : 0.0;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < cpb; i += blockDim.x) {
+    for (int t = threadIdx.x; t < cpb * kMomSlots; t += blockDim.x) {
+        const int i = t / kMomSlots, j = t % kMomSlots;
         const int cc = blockIdx.x * cpb + i;
         if (cc >= nc) continue;
-        const double *smc = smom + kMomSlots * i;
-        Tlat[cc] = smc[0];
-        E[cc] = smc[1];
-        q[3 * cc] = smc[2];
-        q[3 * cc + 1] = smc[3];
-        q[3 * cc + 2] = smc[4];
-        Th[cc] = p.kappa * smc[5];
-        for (int j = 0; j < 6; j++) Q[6 * cc + j] = smc[6 + j];
+        double sum = 0;
+        for (int bb = 0; bb < nb; bb++) sum += part[((size_t)i * nb + bb) * kMomSlots + j];
+        if (j == 0)
+            Tlat[cc] = sum;
+        else if (j == 1)
+            E[cc] = sum;
+        else if (j < 5)
+            q[3 * cc + j - 2] = sum;
+        else if (j == 5)
+            Th[cc] = p.kappa * sum;
+        else
+            Q[6 * cc + j - 6] = sum;
     }
 }
 
@@ -1463,7 +1506,13 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
         for (int dd = 0; dd < nd; dd++)
             for (int pos = 0; pos < nc2; pos++) po[(size_t)dd * nc2 + sched.lvl_cells[(size_t)dd * nc2 + pos]] = pos;
         pos_of_ = up_i(po);
-        // packed sweep records in the storage precision
+        // packed sweep records in the storage precision (host plan with
+        // the on-chip ring and far slots)
+        SweepPlan sp;
+        Error pe = build_sweep_plan(mesh, ang, sched, kSweepMinRing, kSweepFarCap, sp);
+        if (pe.code) return pe;
+        ring_ = sp.ring;
+        far_slots_ = sp.far_enabled ? sp.far_slots : 0;
         std::vector<SweepRec<double>> recd;
         std::vector<SweepRec<float>> recf;
         const bool f32 = cfg.precision == 1;
@@ -1471,38 +1520,22 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
             recf.assign((size_t)nd * nc2, SweepRec<float>{});
         else
             recd.assign((size_t)nd * nc2, SweepRec<double>{});
-        for (int dd = 0; dd < nd; dd++)
-            for (int pos = 0; pos < nc2; pos++) {
-                size_t P = (size_t)dd * nc2 + pos;
-                int c = sched.lvl_cells[P];
-                unsigned lm = sched.lag.empty() ? 0u : sched.lag[(size_t)dd * nc2 + c];
-                double sig = 0, av[4] = {0, 0, 0, 0};
-                int npos[4] = {0, 0, 0, 0};
-                int j = 0, nin = 0;
-                for (int k = mesh.cf_ptr[c]; k < mesh.cf_ptr[c + 1]; k++, j++) {
-                    double dpn = ang.sx[dd] * mesh.cf_nx[k] + ang.sy[dd] * mesh.cf_ny[k] + ang.sz[dd] * mesh.cf_nz[k];
-                    double a = mesh.cf_area[k] / mesh.vol[c] * dpn;
-                    if (dpn >= 0)
-                        sig += a;
-                    else if (mesh.cf_bound[k] < 0 && !((lm >> j) & 1u)) {
-                        if (nin >= 4) return {-8, "a cell has more than four upwind neighbours"};
-                        npos[nin] = po[(size_t)dd * nc2 + mesh.cf_nbr[k]];
-                        av[nin] = a;
-                        nin++;
-                    }
-                }
-                if (f32) {
-                    SweepRec<float> &r = recf[P];
-                    for (int q = 0; q < 4; q++) r.np[q] = npos[q], r.a[q] = (float)av[q];
-                    r.sig = (float)sig;
-                    r.nin = nin;
-                } else {
-                    SweepRec<double> &r = recd[P];
-                    for (int q = 0; q < 4; q++) r.np[q] = npos[q], r.a[q] = av[q];
-                    r.sig = sig;
-                    r.nin = nin;
-                }
+        for (size_t P = 0; P < (size_t)nd * nc2; P++) {
+            const int meta = sp.nin[P] | ((sp.far_w[P] + 1) << 3);
+            if (f32) {
+                SweepRec<float> &r = recf[P];
+                for (int q = 0; q < 4; q++) r.np[q] = sp.np[4 * P + q], r.a[q] = (float)sp.a[4 * P + q];
+                r.sig = (float)sp.sig[P];
+                r.meta = meta;
+                r.cell = sp.cell[P];
+            } else {
+                SweepRec<double> &r = recd[P];
+                for (int q = 0; q < 4; q++) r.np[q] = sp.np[4 * P + q], r.a[q] = sp.a[4 * P + q];
+                r.sig = sp.sig[P];
+                r.meta = meta;
+                r.cell = sp.cell[P];
             }
+        }
         const size_t rec_bytes = f32 ? recf.size() * sizeof(SweepRec<float>) : recd.size() * sizeof(SweepRec<double>);
         rec_ = dalloc(rec_bytes);
         if (!rec_) return {-6, "device allocation failed (sweep records)"};
@@ -1733,6 +1766,7 @@ Error Solver::alloc_all() {
     eps_ = A(ne * S);
     grad_ = A(ne * mesh.dim * S);
     res_ = A(ne * S);
+    corr_ = A(ne * S);
     Tbase_ = (double *)A(nc * 8);
     Bflux_ = (double *)A((size_t)nd * nc * 8);
     gTb_ = (double *)A(nc * 3 * 8);
@@ -1762,8 +1796,10 @@ Error Solver::alloc_all() {
     cg_p_ = (double *)A(nc * 8);
     cg_Ap_ = (double *)A(nc * 8);
     cg_scal_ = (double *)A(65536 * 8);
-    for (void *pp : {eps_, grad_, res_, (void *)Tbase_, (void *)Bflux_, (void *)eb_, (void *)cg_scal_})
-        if (!pp) return {-6, "device allocation failed (" + std::to_string(ne * S * 5 / 1048576) + " MiB of band state)"};
+    for (void *pp : {eps_, grad_, res_, corr_, (void *)Tbase_, (void *)Bflux_, (void *)eb_, (void *)cg_scal_})
+        if (!pp)
+            return {-6, "device allocation failed (" + std::to_string(ne * S * (3 + mesh.dim) / 1048576) +
+                            " MiB of band state)"};
     if (cudaMallocHost((void **)&h_pinned_, 16 * sizeof(double)) != cudaSuccess) return {-6, "pinned allocation failed"};
     cudaStream_t s = cfg.stream;
     CUDA_TRY(cudaMemsetAsync(eb_, 0, nd * nbs * nb * 8, s));
@@ -2097,8 +2133,7 @@ Error Solver::solve_t(SolveStats &st) {
     // cell); the ring holds at least one whole level (distinct slots for the
     // cells written in one level) and 512 positions or more; more chunks
     // when that does not fit in shared memory
-    int wring = 512;
-    while (wring < max_lvl_width_) wring *= 2;
+    const int wring = ring_;
     const int wcap = (cfg.sweep_bands >= 1 && cfg.sweep_bands <= 32) ? cfg.sweep_bands : (sizeof(S) == 4 ? 8 : 4);
     const size_t wlp = ((size_t)(sched.max_levels + 1) * sizeof(int) + 15) & ~(size_t)15;
     int wchunks = 0, wnbc = 0;
@@ -2107,7 +2142,8 @@ Error Solver::solve_t(SolveStats &st) {
         wnbc = (nb + (nb + cap - 1) / cap - 1) / ((nb + cap - 1) / cap);  // equal chunks of <= cap bands
         wchunks = (nb + wnbc - 1) / wnbc;                                // every chunk non-empty
         wslot = (size_t)LCAP * sizeof(SweepRec<S>) + (((size_t)LCAP * wnbc * sizeof(S) + 15) & ~(size_t)15);
-        wsmem = LOOK * wslot + (((size_t)wring * wnbc * sizeof(S) + 15) & ~(size_t)15) + wlp;
+        wsmem = LOOK * wslot + (((size_t)wring * wnbc * sizeof(S) + 15) & ~(size_t)15) +
+                (((size_t)far_slots_ * wnbc * sizeof(S) + 15) & ~(size_t)15) + wlp;
         if (wsmem <= 220 * 1024 || wnbc == 1) break;
     }
     if (wsmem > 220 * 1024) return {-8, "sweep level too wide for the shared-memory correction ring"};
@@ -2117,7 +2153,7 @@ Error Solver::solve_t(SolveStats &st) {
     CUDA_TRY(cudaFuncSetAttribute(k_sweep<S, LOOK, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsmem));
     const int cpb = std::max(1, 256 / nb);
     const int gM = (nc + cpb - 1) / cpb;
-    const size_t msmem = ((size_t)nd * kWTab + (size_t)cpb * kMomSlots) * sizeof(double);
+    const size_t msmem = ((size_t)nd * kWTab + (size_t)cpb * nb * kMomSlots) * sizeof(double);
     const int gW = (int)(((size_t)nbs * 32 + kThreads - 1) / kThreads);
     if (msmem > 200 * 1024) return {-8, "too many directions for the moments kernel's shared-memory weight table"};
     if (nb > 256) return {-8, "more than 256 bands are not supported"};
@@ -2159,8 +2195,9 @@ Error Solver::solve_t(SolveStats &st) {
             GL(K_RESIDUAL, (k_residual<S, DIM><<<gE, kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, pos_of_, R)));
         }
         GL(K_SWEEP, (k_sweep<S, LOOK, LCAP><<<wide_blocks, wide_threads, wsmem, s>>>(
-                        nb, nc, wnbc, wring, wrvec, lvl_ptr_, dir_lvl_off_, (const SweepRec<S> *)rec_, kb_, R)));
-        GL(K_MOMENTS, (k_moments<S><<<gM, cpb * nb, msmem, s>>>(dm_, dp_, cpb, eps, R, pos_of_, Tbase_, wtab_, Tlat_, E_,
+                        nb, nc, wnbc, wring, far_slots_, wrvec, lvl_ptr_, dir_lvl_off_, (const SweepRec<S> *)rec_, lvl_cells_, kb_,
+                        R, (S *)corr_)));
+        GL(K_MOMENTS, (k_moments<S><<<gM, cpb * nb, msmem, s>>>(dm_, dp_, cpb, eps, (const S *)corr_, Tbase_, wtab_, Tlat_, E_,
                                                                 q_, Tband_, Th_, Q_, 1)));
         GL(K_BOUND_OUT, (k_bound_out<S, DIM><<<gB, kThreads, 0, s>>>(dm_, dp_, ev, eb_)));
         GL(K_SIDE_MOMENTS, k_side_moments<<<gW, kThreads, 0, s>>>(dm_, dp_, eb_, Ths_, Qs_));

@@ -113,7 +113,9 @@ private:
     DMesh dm_{};
     DPhys dp_{};
     // state
-    void *eps_ = nullptr, *grad_ = nullptr, *res_ = nullptr;  // storage-type arrays
+    // storage-type arrays [nd][nc][nb]: deviations, gradients (x DIM),
+    // residuals (level order) and sweep corrections (cell order)
+    void *eps_ = nullptr, *grad_ = nullptr, *res_ = nullptr, *corr_ = nullptr;
     double *Tbase_ = nullptr, *gTb_ = nullptr;
     double *Bflux_ = nullptr;  // [nd][nc] base-field face flux sums of the residual
     double *eb_ = nullptr, *eb_snap_ = nullptr;
@@ -128,6 +130,8 @@ private:
     // schedule on device
     int *lvl_cells_ = nullptr, *lvl_ptr_ = nullptr, *dir_lvl_off_ = nullptr;
     int max_lvl_width_ = 0;  // widest level of any direction (cells)
+    int ring_ = 0;           // on-chip ring of the sweep (positions, power of two)
+    int far_slots_ = 0;      // on-chip far slots of the sweep (0: far reads go to memory)
     // level-ordered sweep records per direction: sum of outgoing A/V (s.n)
     // and up to 4 incoming (neighbour position, A/V (s.n)) pairs
     void *rec_ = nullptr;  // SweepRec<storage type>[nd][nc] in level order

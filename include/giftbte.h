@@ -173,6 +173,10 @@ typedef struct {
     double total_volume;
     double max_iter_or_zero;   /* MaxNumIter from CONTROL (decks only) */
     double err_temp, err_flux; /* ResidualTemp / ResidualFlux from CONTROL (decks only) */
+    int max_level_width;       /* widest sweep level (cells) */
+    int sweep_ring;            /* on-chip correction ring of the sweep (positions) */
+    int far_slots;             /* on-chip slots for upwind reads older than the ring */
+    long long far_refs;        /* upwind reads older than the ring, all directions */
 } gbte_deck_info;
 
 int gbte_inspect_deck(const char *dir, gbte_deck_info *info);
