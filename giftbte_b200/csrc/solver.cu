@@ -1148,14 +1148,14 @@ __device__ __forceinline__ double warp_allsum(double v) {
     return v;
 }
 
-// Jacobi-preconditioned CG in the Chronopoulos-Gear form on one
-// thread-block cluster, the whole system resident in shared memory.
+// Preconditioned CG in the Chronopoulos-Gear form on one thread-block
+// cluster, the whole system resident in shared memory.
 // The rows are split into C compact parts (recursive coordinate bisection on
 // the cell centres); CTA k owns part k: rows part_ptr[k] .. part_ptr[k+1] of
 // the permuted order (perm maps them to the caller's rows). Its matrix is
 // stored as the diagonal plus K off-diagonal columns in ELL form, column
 // indices local (< nr) or into a halo that follows the local entries. After
-// each update of u = D^-1 r, every CTA stores the u values its neighbours
+// each update of u = M^-1 r, every CTA stores the u values its neighbours
 // need straight into their halos (distributed shared memory), so the
 // product w = A u reads only local shared memory. The three dot products
 // of an iteration, (r,u), (w,u) and (r,r), are reduced together: warp ->
@@ -1163,28 +1163,46 @@ __device__ __forceinline__ double warp_allsum(double v) {
 // order, so all CTAs hold bitwise identical scalars and take the same
 // branch at the stopping test |r| <= max(rtol |b|, eta |r0|). Two cluster
 // barriers per iteration: after the halo exchange and after the partials.
+//
+// Preconditioner: M^-1 = D^-1 (Jacobi), plus with `coarse` a two-level
+// additive correction R^T Ac^-1 R on kCgAgg aggregates per part (compact
+// sub-parts, rows sorted by aggregate, local ranges agg_ptr), R the
+// aggregate sums and Ac = R A R^T. CTA k keeps rows [kCgAgg k, kCgAgg (k+1))
+// of Ac^-1 (ainv). Every CTA needs all aggregate sums of r: they follow
+// from R r_new = R r - alpha (R w + beta R s), the exact sums of r, s and w
+// being pushed into every CTA together with the dot-product partials, so
+// the coarse level adds no barrier.
 // When t1 is given, sum (x - t1)^2 of the solution is reduced too.
 // out[0] = iterations, out[1] = that sum, out[2] = |r|^2 at exit.
-__global__ void __launch_bounds__(256, 1)
-    k_cg_cluster(int K, int nrmax, int hmax, int smax, const int *__restrict__ part_ptr, const int *__restrict__ perm,
-                 const double *__restrict__ ell_val, const int *__restrict__ ell_col, const double *__restrict__ diag,
-                 const int *__restrict__ nhalo, const int *__restrict__ nsend, const int *__restrict__ snd_src,
-                 const int *__restrict__ snd_dst, const double *__restrict__ bvec, double *__restrict__ x, double rtol,
-                 double eta, int maxit, const double *__restrict__ t1, double *__restrict__ out) {
+constexpr int kCgAgg = 16;      // aggregates per CTA of the coarse level
+constexpr int kCgThreads = 256;  // threads per CTA (= kCgAgg * kCgAgg: one coarse product term each)
+
+__global__ void __launch_bounds__(kCgThreads, 1)
+    k_cg_cluster(int K, int nrmax, int hmax, int smax, int coarse, const int *__restrict__ part_ptr,
+                 const int *__restrict__ perm, const double *__restrict__ ell_val, const int *__restrict__ ell_col,
+                 const double *__restrict__ diag, const int *__restrict__ agg_ptr, const double *__restrict__ ainv,
+                 const int *__restrict__ nsend, const int *__restrict__ snd_src, const int *__restrict__ snd_dst,
+                 const double *__restrict__ bvec, double *__restrict__ x, double rtol, double eta, int maxit,
+                 const double *__restrict__ t1, double *__restrict__ out) {
     cgrp::cluster_group cl = cgrp::this_cluster();
     const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    const int NA = C * kCgAgg;  // aggregates in all
     extern __shared__ __align__(16) unsigned char pcs[];
     double *xs = reinterpret_cast<double *>(pcs), *rs = xs + nrmax, *ps = rs + nrmax, *ss = ps + nrmax,
            *ws = ss + nrmax, *dg = ws + nrmax, *di = dg + nrmax, *us = di + nrmax;  // us: [nrmax + hmax]
     double *part = us + nrmax + hmax;  // [32][4] partial sums pushed by every CTA
     double *wsum = part + 128;         // [32][4] warp partial sums
-    double *ev = wsum + 128;           // [K][nrmax]
+    double *ai = wsum + 128;           // [kCgAgg][NA] this CTA's rows of Ac^-1
+    double *pr = ai + kCgAgg * NA;     // [3][NA] aggregate sums of r, s, w pushed by every CTA
+    double *cc = pr + 3 * NA;          // [kCgAgg] coarse correction of this CTA's aggregates
+    double *ev = cc + kCgAgg;          // [K][nrmax]
     double **raddr = reinterpret_cast<double **>(ev + (size_t)K * nrmax);  // [smax] halo slots in other CTAs
     int *ec = reinterpret_cast<int *>(raddr + smax);                       // [K][nrmax]
     int *ssrc = ec + (size_t)K * nrmax;                                    // [smax]
+    int *aptr = ssrc + smax;                                               // [kCgAgg + 1]
+    int *aggl = aptr + kCgAgg + 1;                                         // [nrmax] aggregate of each row
     const int tid = threadIdx.x, bd = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = bd >> 5;
     const int base = part_ptr[rank], nr = part_ptr[rank + 1] - base, ns = nsend[rank];
-    (void)nhalo;
     for (int i = tid; i < nr; i += bd) {
         const int o = perm[base + i];
         xs[i] = x[o];
@@ -1203,6 +1221,17 @@ __global__ void __launch_bounds__(256, 1)
         ssrc[e] = snd_src[(size_t)rank * smax + e];
         const int d = snd_dst[(size_t)rank * smax + e];
         raddr[e] = cl.map_shared_rank(us, d >> 20) + (d & 0xFFFFF);
+    }
+    if (tid < kCgAgg) cc[tid] = 0.0;
+    for (int e = tid; e < 3 * NA; e += bd) pr[e] = 0.0;  // before any CTA pushes (first cluster barrier)
+    if (coarse) {
+        for (int e = tid; e < kCgAgg * NA; e += bd) ai[e] = ainv[(size_t)rank * kCgAgg * NA + e];
+        for (int e = tid; e <= kCgAgg; e += bd) aptr[e] = agg_ptr[rank * (kCgAgg + 1) + e];
+        __syncthreads();
+        for (int a = 0; a < kCgAgg; a++)
+            for (int i = aptr[a] + tid; i < aptr[a + 1]; i += bd) aggl[i] = a;
+    } else {
+        for (int i = tid; i < nr; i += bd) aggl[i] = 0;
     }
     cl.sync();
     auto push_halo = [&]() {
@@ -1230,7 +1259,34 @@ __global__ void __launch_bounds__(256, 1)
         cl.sync();
         for (int j = 0; j < nv; j++) v[j] = warp_allsum(lane < C ? part[lane * 4 + j] : 0.0);
     };
-    // r = b - A x (x's halo first), u = D^-1 r, w = A u
+    // this CTA's aggregate sums of nv of the vectors (r, s, w) stored into
+    // pr of every CTA (rows already written by all threads: call after a
+    // barrier); each warp sums its aggregates in a fixed order
+    auto push_agg = [&](int nv) {
+        const double *vec[3] = {rs, ss, ws};
+        for (int a = warp; a < kCgAgg; a += nw) {
+            double t[3] = {0, 0, 0};
+            for (int i = aptr[a] + lane; i < aptr[a + 1]; i += 32)
+                for (int v = 0; v < nv; v++) t[v] += vec[v][i];
+            for (int v = 0; v < nv; v++) t[v] = warp_allsum(t[v]);
+            if (lane < C) {
+                double *dst = cl.map_shared_rank(pr, lane) + rank * kCgAgg + a;
+                for (int v = 0; v < nv; v++) dst[v * NA] = t[v];
+            }
+        }
+    };
+    // cc = this CTA's rows of Ac^-1 times the aggregate sums of the new r,
+    // R r - al (R w + be R s) from the pushed sums (al = 0: R r itself);
+    // blockDim = kCgAgg^2: thread (a, j) takes the columns j, j + 16, ...
+    auto coarse_corr = [&](double al, double be) {
+        const int a = tid >> 4, j = tid & 15;
+        double t = 0;
+        for (int J = j; J < NA; J += 16) t += ai[a * NA + J] * (pr[J] - al * (pr[2 * NA + J] + be * pr[NA + J]));
+        for (int o = 8; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if (j == 0) cc[a] = t;
+        __syncthreads();
+    };
+    // r = b - A x (x's halo first), u = M^-1 r, w = A u
     push_halo();
     cl.sync();
     double bb = 0;
@@ -1239,8 +1295,13 @@ __global__ void __launch_bounds__(256, 1)
         bb += bi * bi;
         rs[i] = bi - matvec(i);
     }
-    cl.sync();  // every CTA has read x's halo before u's arrives
-    for (int i = tid; i < nr; i += bd) us[i] = di[i] * rs[i];
+    if (coarse) {
+        __syncthreads();
+        push_agg(1);
+    }
+    cl.sync();  // every CTA has read x's halo before u's arrives; sums of r0 in place
+    if (coarse) coarse_corr(0.0, 0.0);
+    for (int i = tid; i < nr; i += bd) us[i] = di[i] * rs[i] + (coarse ? cc[aggl[i]] : 0.0);
     __syncthreads();
     push_halo();
     cl.sync();
@@ -1252,12 +1313,17 @@ __global__ void __launch_bounds__(256, 1)
         v[1] += w * us[i];
         v[2] += rs[i] * rs[i];
     }
+    if (coarse) {
+        __syncthreads();
+        push_agg(3);
+    }
     csum(v, 4);
     double gam = v[0], rr = v[2];
     const double thr = fmax(rtol * rtol * v[3], eta * eta * rr);
     double alpha = gam / v[1], beta = 0.0;
     int it = 0;
     while (it < maxit && rr > thr) {
+        if (coarse) coarse_corr(alpha, beta);
         for (int i = tid; i < nr; i += bd) {
             const double p = us[i] + beta * ps[i], s = ws[i] + beta * ss[i];
             ps[i] = p;
@@ -1265,7 +1331,7 @@ __global__ void __launch_bounds__(256, 1)
             xs[i] += alpha * p;
             const double r = rs[i] - alpha * s;
             rs[i] = r;
-            us[i] = di[i] * r;
+            us[i] = di[i] * r + (coarse ? cc[aggl[i]] : 0.0);
         }
         __syncthreads();
         push_halo();
@@ -1277,6 +1343,10 @@ __global__ void __launch_bounds__(256, 1)
             t[0] += rs[i] * us[i];
             t[1] += w * us[i];
             t[2] += rs[i] * rs[i];
+        }
+        if (coarse) {
+            __syncthreads();
+            push_agg(3);
         }
         csum(t, 3);
         beta = t[0] / gam;
@@ -1889,8 +1959,6 @@ Error Solver::fourier_initial() {
     return set_initial(T0.data(), q0.data(), nullptr);
 }
 
-constexpr int kCgThreads = 256;  // threads per CTA of the cluster-resident CG
-
 // Recursive coordinate bisection of cells [first, last) of ids into nparts
 // parts of near-equal size, split at the median of the axis of largest
 // extent; part boundaries are appended to bounds.
@@ -1920,12 +1988,46 @@ static void rcb_split(std::vector<int> &ids, int first, int last, int nparts, co
     rcb_split(ids, mid, last, nparts - nl, m, bounds);
 }
 
+// Inverse of a dense SPD matrix (n x n, row-major) by Cholesky; false when
+// it is not numerically positive definite.
+static bool spd_inverse(std::vector<double> A, int n, std::vector<double> &inv) {
+    for (int j = 0; j < n; j++) {
+        double d = A[(size_t)j * n + j];
+        for (int k = 0; k < j; k++) d -= A[(size_t)j * n + k] * A[(size_t)j * n + k];
+        if (!(d > 0)) return false;
+        d = std::sqrt(d);
+        A[(size_t)j * n + j] = d;
+        for (int i = j + 1; i < n; i++) {
+            double v = A[(size_t)i * n + j];
+            for (int k = 0; k < j; k++) v -= A[(size_t)i * n + k] * A[(size_t)j * n + k];
+            A[(size_t)i * n + j] = v / d;
+        }
+    }
+    inv.assign((size_t)n * n, 0.0);
+    std::vector<double> y(n);
+    for (int c = 0; c < n; c++) {
+        for (int i = 0; i < n; i++) {  // L y = e_c
+            double v = (i == c) ? 1.0 : 0.0;
+            for (int k = 0; k < i; k++) v -= A[(size_t)i * n + k] * y[k];
+            y[i] = v / A[(size_t)i * n + i];
+        }
+        for (int i = n - 1; i >= 0; i--) {  // L^T z = y
+            double v = y[i];
+            for (int k = i + 1; k < n; k++) v -= A[(size_t)k * n + i] * inv[(size_t)k * n + c];
+            inv[(size_t)i * n + c] = v / A[(size_t)i * n + i];
+        }
+    }
+    return true;
+}
+
 // Cluster-resident CG plan for a CSR system (negated, SPD, one diagonal
-// entry per row) of mesh.nc rows: C = 16 parts by coordinate bisection,
-// then per part the ELL block, the halo (columns owned by other parts) and
-// the list of values this part sends into other parts' halos. C = 0 when
-// the parts do not fit in one CTA's shared memory or the device cannot
-// schedule the cluster.
+// entry per row) of mesh.nc rows: C * kCgAgg aggregates by coordinate
+// bisection, kCgAgg consecutive ones forming the part of a CTA; per part the
+// ELL block, the halo (columns owned by other parts), the list of values
+// this part sends into other parts' halos, and the coarse level (rows of
+// the inverse of R A R^T; none when an aggregate is empty or R A R^T is not
+// positive definite). C = 0 when the parts do not fit in one CTA's shared
+// memory or the device cannot schedule the cluster.
 Error Solver::cg_plan(const std::vector<int> &ptr, const std::vector<int> &idx, const std::vector<double> &val,
                       CgPlan &pl) {
     pl = CgPlan{};
@@ -1933,10 +2035,14 @@ Error Solver::cg_plan(const std::vector<int> &ptr, const std::vector<int> &idx, 
     if (n < C) return {0, ""};
     int max_smem = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, cfg.device));
-    std::vector<int> perm(n), bounds{0};
+    const int NA = C * kCgAgg;
+    std::vector<int> perm(n), abounds{0}, bounds(C + 1);
     for (int i = 0; i < n; i++) perm[i] = i;
-    rcb_split(perm, 0, n, C, mesh, bounds);
-    std::vector<int> newidx(n), owner(n);
+    rcb_split(perm, 0, n, NA, mesh, abounds);
+    for (int k = 0; k <= C; k++) bounds[k] = abounds[k * kCgAgg];
+    std::vector<int> newidx(n), owner(n), agg(n);
+    for (int g = 0; g < NA; g++)
+        for (int q = abounds[g]; q < abounds[g + 1]; q++) agg[q] = g;
     for (int k = 0; k < C; k++)
         for (int q = bounds[k]; q < bounds[k + 1]; q++) {
             newidx[perm[q]] = q;
@@ -1991,7 +2097,8 @@ Error Solver::cg_plan(const std::vector<int> &ptr, const std::vector<int> &idx, 
     int smax = 0;
     for (int k = 0; k < C; k++) smax = std::max(smax, (int)sends[k].size());
     if (nrmax + hmax >= (1 << 20)) return {0, ""};
-    const size_t smem = 8 * ((size_t)8 * nrmax + hmax + 256 + (size_t)K * nrmax + smax) + 4 * ((size_t)K * nrmax + smax);
+    const size_t smem = 8 * ((size_t)8 * nrmax + hmax + 256 + (size_t)(kCgAgg + 3) * NA + kCgAgg + (size_t)K * nrmax + smax) +
+                        4 * ((size_t)K * nrmax + smax + kCgAgg + 1 + nrmax);
     if (smem > (size_t)max_smem) return {0, ""};
     CUDA_TRY(cudaFuncSetAttribute(k_cg_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     CUDA_TRY(cudaFuncSetAttribute(k_cg_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -2014,7 +2121,7 @@ Error Solver::cg_plan(const std::vector<int> &ptr, const std::vector<int> &idx, 
     // device arrays; ELL padding: value 0 on the row's own (local) entry
     const size_t ell = (size_t)C * K * nrmax;
     std::vector<double> ev(std::max<size_t>(ell, 1), 0.0);
-    std::vector<int> ec(std::max<size_t>(ell, 1), 0), nh(C), ns(C), ssrc((size_t)C * std::max(smax, 1), 0),
+    std::vector<int> ec(std::max<size_t>(ell, 1), 0), ns(C), ssrc((size_t)C * std::max(smax, 1), 0),
         sdst((size_t)C * std::max(smax, 1), 0);
     for (int q = 0; q < n; q++) {
         const int k = owner[q], i = q - bounds[k];
@@ -2030,21 +2137,38 @@ Error Solver::cg_plan(const std::vector<int> &ptr, const std::vector<int> &idx, 
         }
     }
     for (int k = 0; k < C; k++) {
-        nh[k] = (int)halo[k].size();
         ns[k] = (int)sends[k].size();
         for (int e = 0; e < ns[k]; e++) {
             ssrc[(size_t)k * smax + e] = sends[k][e].first;
             sdst[(size_t)k * smax + e] = sends[k][e].second;
         }
     }
+    // coarse level: Ac = R A R^T over the aggregates, inverted on the host
+    bool coarse = true;
+    for (int g = 0; g < NA && coarse; g++) coarse = abounds[g + 1] - abounds[g] >= 4;
+    std::vector<double> ainv;
+    if (coarse) {
+        std::vector<double> Ac((size_t)NA * NA, 0.0);
+        for (int q = 0; q < n; q++) {
+            const int old = perm[q];
+            for (int e = ptr[old]; e < ptr[old + 1]; e++) Ac[(size_t)agg[q] * NA + agg[newidx[idx[e]]]] += val[e];
+        }
+        coarse = spd_inverse(Ac, NA, ainv);
+    }
+    if (!coarse) ainv.assign(1, 0.0);
+    std::vector<int> aptr((size_t)C * (kCgAgg + 1));
+    for (int k = 0; k < C; k++)
+        for (int a = 0; a <= kCgAgg; a++) aptr[(size_t)k * (kCgAgg + 1) + a] = abounds[k * kCgAgg + a] - bounds[k];
     bool ok = true;
     cudaStream_t s = cfg.stream;
+    pl.coarse = coarse ? 1 : 0;
+    pl.agg_ptr = upload(this, allocs_, aptr, s, ok);
+    pl.ainv = upload(this, allocs_, ainv, s, ok);
     pl.part_ptr = upload(this, allocs_, bounds, s, ok);
     pl.perm = upload(this, allocs_, perm, s, ok);
     pl.ell_val = upload(this, allocs_, ev, s, ok);
     pl.ell_col = upload(this, allocs_, ec, s, ok);
     pl.diag = upload(this, allocs_, diag, s, ok);
-    pl.nhalo = upload(this, allocs_, nh, s, ok);
     pl.nsend = upload(this, allocs_, ns, s, ok);
     pl.snd_src = upload(this, allocs_, ssrc, s, ok);
     pl.snd_dst = upload(this, allocs_, sdst, s, ok);
@@ -2085,11 +2209,11 @@ Error Solver::cg_solve(const CgPlan &pl, const int *ptr, const int *idx, const d
         at[0].val.clusterDim.z = 1;
         lc.attrs = at;
         lc.numAttrs = 1;
-        GL(K_PCG, lerr = cudaLaunchKernelEx(&lc, k_cg_cluster, pl.K, pl.nrmax, pl.hmax, pl.smax,
+        GL(K_PCG, lerr = cudaLaunchKernelEx(&lc, k_cg_cluster, pl.K, pl.nrmax, pl.hmax, pl.smax, pl.coarse,
                                             (const int *)pl.part_ptr, (const int *)pl.perm, (const double *)pl.ell_val,
-                                            (const int *)pl.ell_col, (const double *)pl.diag, (const int *)pl.nhalo,
-                                            (const int *)pl.nsend, (const int *)pl.snd_src, (const int *)pl.snd_dst, b,
-                                            x, rtol, eta, maxit, t1, scal));
+                                            (const int *)pl.ell_col, (const double *)pl.diag, (const int *)pl.agg_ptr,
+                                            (const double *)pl.ainv, (const int *)pl.nsend, (const int *)pl.snd_src,
+                                            (const int *)pl.snd_dst, b, x, rtol, eta, maxit, t1, scal));
         CUDA_TRY(lerr);
         CUDA_TRY(cudaMemcpyAsync(h_pinned_ + 8, scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaStreamSynchronize(s));

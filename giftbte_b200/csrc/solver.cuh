@@ -69,14 +69,15 @@ struct SolveStats {
 
 // Launch plan of the cluster-resident CG for one CSR system: cluster size
 // (0 = the system does not fit, use the grid-wide kernel), the per-CTA
-// layout bounds (off-diagonals per row K, rows, halo entries, sends), the
-// dynamic shared memory and the partitioned system in device memory.
+// layout bounds (off-diagonals per row K, rows, halo entries, sends),
+// whether the two-level preconditioner is on, the dynamic shared memory and
+// the partitioned system in device memory.
 struct CgPlan {
-    int C = 0, K = 0, nrmax = 0, hmax = 0, smax = 0;
+    int C = 0, K = 0, nrmax = 0, hmax = 0, smax = 0, coarse = 0;
     size_t smem = 0;
-    int *part_ptr = nullptr, *perm = nullptr, *ell_col = nullptr, *nhalo = nullptr, *nsend = nullptr,
-        *snd_src = nullptr, *snd_dst = nullptr;
-    double *ell_val = nullptr, *diag = nullptr;
+    int *part_ptr = nullptr, *perm = nullptr, *ell_col = nullptr, *nsend = nullptr, *snd_src = nullptr,
+        *snd_dst = nullptr, *agg_ptr = nullptr;
+    double *ell_val = nullptr, *diag = nullptr, *ainv = nullptr;
 };
 
 class Solver {
