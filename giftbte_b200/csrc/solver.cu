@@ -1168,14 +1168,19 @@ __device__ __forceinline__ double warp_allsum(double v) {
 // additive correction R^T Ac^-1 R on kCgAgg aggregates per part (compact
 // sub-parts, rows sorted by aggregate, local ranges agg_ptr), R the
 // aggregate sums and Ac = R A R^T. CTA k keeps rows [kCgAgg k, kCgAgg (k+1))
-// of Ac^-1 (ainv). Every CTA needs all aggregate sums of r: they follow
-// from R r_new = R r - alpha (R w + beta R s), the exact sums of r, s and w
-// being pushed into every CTA together with the dot-product partials, so
-// the coarse level adds no barrier.
+// of Ac^-1 (ainv) in registers, 8 per thread. Every CTA needs all
+// aggregate sums of r: they follow from R r_new = R r - alpha (R w + beta
+// R s), the exact sums of r, s and w being pushed into every CTA together
+// with the dot-product partials, so the coarse level adds no cluster
+// barrier. Warp w owns aggregate w (its rows in every row loop), so these
+// sums accumulate in registers.
 // When t1 is given, sum (x - t1)^2 of the solution is reduced too.
 // out[0] = iterations, out[1] = that sum, out[2] = |r|^2 at exit.
-constexpr int kCgAgg = 16;      // aggregates per CTA of the coarse level
-constexpr int kCgThreads = 256;  // threads per CTA (= kCgAgg * kCgAgg: one coarse product term each)
+constexpr int kCgAgg = 16;       // aggregates per CTA of the coarse level
+constexpr int kCgThreads = 512;  // threads per CTA: one warp per aggregate
+constexpr int kCgMaxC = 16;      // largest cluster (NA = C kCgAgg)
+constexpr int kCgTerms = kCgMaxC * kCgAgg / 32;  // coarse terms per thread
+static_assert(kCgAgg == kCgThreads / 32 && kCgMaxC * kCgAgg <= kCgThreads, "CG thread layout");
 
 __global__ void __launch_bounds__(kCgThreads, 1)
     k_cg_cluster(int K, int nrmax, int hmax, int smax, int coarse, const int *__restrict__ part_ptr,
@@ -1186,21 +1191,20 @@ __global__ void __launch_bounds__(kCgThreads, 1)
                  const double *__restrict__ t1, double *__restrict__ out) {
     cgrp::cluster_group cl = cgrp::this_cluster();
     const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
-    const int NA = C * kCgAgg;  // aggregates in all
+    const int NA = C * kCgAgg;  // aggregates in all (<= kCgThreads)
     extern __shared__ __align__(16) unsigned char pcs[];
     double *xs = reinterpret_cast<double *>(pcs), *rs = xs + nrmax, *ps = rs + nrmax, *ss = ps + nrmax,
            *ws = ss + nrmax, *dg = ws + nrmax, *di = dg + nrmax, *us = di + nrmax;  // us: [nrmax + hmax]
     double *part = us + nrmax + hmax;  // [32][4] partial sums pushed by every CTA
     double *wsum = part + 128;         // [32][4] warp partial sums
-    double *ai = wsum + 128;           // [kCgAgg][NA] this CTA's rows of Ac^-1
-    double *pr = ai + kCgAgg * NA;     // [3][NA] aggregate sums of r, s, w pushed by every CTA
-    double *cc = pr + 3 * NA;          // [kCgAgg] coarse correction of this CTA's aggregates
+    double *pr = wsum + 128;           // [3][NA] aggregate sums of r, s, w pushed by every CTA
+    double *rn = pr + 3 * NA;          // [NA] aggregate sums of the new r
+    double *cc = rn + NA;              // [kCgAgg] coarse correction of this CTA's aggregates
     double *ev = cc + kCgAgg;          // [K][nrmax]
     double **raddr = reinterpret_cast<double **>(ev + (size_t)K * nrmax);  // [smax] halo slots in other CTAs
     int *ec = reinterpret_cast<int *>(raddr + smax);                       // [K][nrmax]
     int *ssrc = ec + (size_t)K * nrmax;                                    // [smax]
     int *aptr = ssrc + smax;                                               // [kCgAgg + 1]
-    int *aggl = aptr + kCgAgg + 1;                                         // [nrmax] aggregate of each row
     const int tid = threadIdx.x, bd = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = bd >> 5;
     const int base = part_ptr[rank], nr = part_ptr[rank + 1] - base, ns = nsend[rank];
     for (int i = tid; i < nr; i += bd) {
@@ -1224,16 +1228,18 @@ __global__ void __launch_bounds__(kCgThreads, 1)
     }
     if (tid < kCgAgg) cc[tid] = 0.0;
     for (int e = tid; e < 3 * NA; e += bd) pr[e] = 0.0;  // before any CTA pushes (first cluster barrier)
-    if (coarse) {
-        for (int e = tid; e < kCgAgg * NA; e += bd) ai[e] = ainv[(size_t)rank * kCgAgg * NA + e];
-        for (int e = tid; e <= kCgAgg; e += bd) aptr[e] = agg_ptr[rank * (kCgAgg + 1) + e];
-        __syncthreads();
-        for (int a = 0; a < kCgAgg; a++)
-            for (int i = aptr[a] + tid; i < aptr[a + 1]; i += bd) aggl[i] = a;
-    } else {
-        for (int i = tid; i < nr; i += bd) aggl[i] = 0;
-    }
+    for (int e = tid; e <= kCgAgg; e += bd) aptr[e] = agg_ptr[rank * (kCgAgg + 1) + e];
+    // this thread's coarse terms: row `warp` of this CTA's block of Ac^-1,
+    // columns lane, lane + 32, ...
+    double air[kCgTerms];
+#pragma unroll
+    for (int k = 0; k < kCgTerms; k++)
+        air[k] = (coarse && lane + 32 * k < NA) ? ainv[((size_t)rank * kCgAgg + warp) * NA + lane + 32 * k] : 0.0;
     cl.sync();
+    // the rows of this warp's aggregate
+    auto rows = [&](auto &&f) {
+        for (int i = aptr[warp] + lane; i < aptr[warp + 1]; i += 32) f(i);
+    };
     auto push_halo = [&]() {
         for (int e = tid; e < ns; e += bd) *raddr[e] = us[ssrc[e]];
     };
@@ -1259,64 +1265,58 @@ __global__ void __launch_bounds__(kCgThreads, 1)
         cl.sync();
         for (int j = 0; j < nv; j++) v[j] = warp_allsum(lane < C ? part[lane * 4 + j] : 0.0);
     };
-    // this CTA's aggregate sums of nv of the vectors (r, s, w) stored into
-    // pr of every CTA (rows already written by all threads: call after a
-    // barrier); each warp sums its aggregates in a fixed order
-    auto push_agg = [&](int nv) {
-        const double *vec[3] = {rs, ss, ws};
-        for (int a = warp; a < kCgAgg; a += nw) {
-            double t[3] = {0, 0, 0};
-            for (int i = aptr[a] + lane; i < aptr[a + 1]; i += 32)
-                for (int v = 0; v < nv; v++) t[v] += vec[v][i];
-            for (int v = 0; v < nv; v++) t[v] = warp_allsum(t[v]);
-            if (lane < C) {
-                double *dst = cl.map_shared_rank(pr, lane) + rank * kCgAgg + a;
-                for (int v = 0; v < nv; v++) dst[v * NA] = t[v];
-            }
+    // this warp's aggregate sums (v[0..nv): r, s, w) stored into pr of
+    // every CTA
+    auto push_agg = [&](double *v, int nv) {
+        for (int j = 0; j < nv; j++) v[j] = warp_allsum(v[j]);
+        if (lane < C) {
+            double *dst = cl.map_shared_rank(pr, lane) + rank * kCgAgg + warp;
+            for (int j = 0; j < nv; j++) dst[j * NA] = v[j];
         }
     };
     // cc = this CTA's rows of Ac^-1 times the aggregate sums of the new r,
     // R r - al (R w + be R s) from the pushed sums (al = 0: R r itself);
-    // blockDim = kCgAgg^2: thread (a, j) takes the columns j, j + 16, ...
+    // warp a forms cc[a]
     auto coarse_corr = [&](double al, double be) {
-        const int a = tid >> 4, j = tid & 15;
+        if (tid < NA) rn[tid] = pr[tid] - al * (pr[2 * NA + tid] + be * pr[NA + tid]);
+        __syncthreads();
         double t = 0;
-        for (int J = j; J < NA; J += 16) t += ai[a * NA + J] * (pr[J] - al * (pr[2 * NA + J] + be * pr[NA + J]));
-        for (int o = 8; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-        if (j == 0) cc[a] = t;
+#pragma unroll
+        for (int k = 0; k < kCgTerms; k++)
+            if (lane + 32 * k < NA) t += air[k] * rn[lane + 32 * k];
+        t = warp_allsum(t);
+        if (lane == 0) cc[warp] = t;
         __syncthreads();
     };
     // r = b - A x (x's halo first), u = M^-1 r, w = A u
     push_halo();
     cl.sync();
-    double bb = 0;
-    for (int i = tid; i < nr; i += bd) {
-        const double bi = rs[i];
+    double bb = 0, ag[3] = {0, 0, 0};
+    rows([&](int i) {
+        const double bi = rs[i], r = bi - matvec(i);
         bb += bi * bi;
-        rs[i] = bi - matvec(i);
-    }
-    if (coarse) {
-        __syncthreads();
-        push_agg(1);
-    }
+        rs[i] = r;
+        ag[0] += r;
+    });
+    if (coarse) push_agg(ag, 1);
     cl.sync();  // every CTA has read x's halo before u's arrives; sums of r0 in place
     if (coarse) coarse_corr(0.0, 0.0);
-    for (int i = tid; i < nr; i += bd) us[i] = di[i] * rs[i] + (coarse ? cc[aggl[i]] : 0.0);
+    rows([&](int i) { us[i] = di[i] * rs[i] + cc[warp]; });
     __syncthreads();
     push_halo();
     cl.sync();
     double v[4] = {0, 0, 0, bb};
-    for (int i = tid; i < nr; i += bd) {
+    ag[0] = ag[1] = ag[2] = 0;
+    rows([&](int i) {
         const double w = matvec(i);
         ws[i] = w;
         v[0] += rs[i] * us[i];
         v[1] += w * us[i];
         v[2] += rs[i] * rs[i];
-    }
-    if (coarse) {
-        __syncthreads();
-        push_agg(3);
-    }
+        ag[0] += rs[i];
+        ag[2] += w;
+    });
+    if (coarse) push_agg(ag, 3);
     csum(v, 4);
     double gam = v[0], rr = v[2];
     const double thr = fmax(rtol * rtol * v[3], eta * eta * rr);
@@ -1324,30 +1324,32 @@ __global__ void __launch_bounds__(kCgThreads, 1)
     int it = 0;
     while (it < maxit && rr > thr) {
         if (coarse) coarse_corr(alpha, beta);
-        for (int i = tid; i < nr; i += bd) {
+        ag[0] = ag[1] = ag[2] = 0;
+        const double cw = cc[warp];
+        rows([&](int i) {
             const double p = us[i] + beta * ps[i], s = ws[i] + beta * ss[i];
             ps[i] = p;
             ss[i] = s;
             xs[i] += alpha * p;
             const double r = rs[i] - alpha * s;
             rs[i] = r;
-            us[i] = di[i] * r + (coarse ? cc[aggl[i]] : 0.0);
-        }
+            us[i] = di[i] * r + cw;
+            ag[0] += r;
+            ag[1] += s;
+        });
         __syncthreads();
         push_halo();
         cl.sync();
         double t[3] = {0, 0, 0};
-        for (int i = tid; i < nr; i += bd) {
+        rows([&](int i) {
             const double w = matvec(i);
             ws[i] = w;
             t[0] += rs[i] * us[i];
             t[1] += w * us[i];
             t[2] += rs[i] * rs[i];
-        }
-        if (coarse) {
-            __syncthreads();
-            push_agg(3);
-        }
+            ag[2] += w;
+        });
+        if (coarse) push_agg(ag, 3);
         csum(t, 3);
         beta = t[0] / gam;
         alpha = t[0] / (t[1] - beta * t[0] / alpha);
@@ -2031,7 +2033,7 @@ static bool spd_inverse(std::vector<double> A, int n, std::vector<double> &inv) 
 Error Solver::cg_plan(const std::vector<int> &ptr, const std::vector<int> &idx, const std::vector<double> &val,
                       CgPlan &pl) {
     pl = CgPlan{};
-    const int n = mesh.nc, C = 16;
+    const int n = mesh.nc, C = kCgMaxC;
     if (n < C) return {0, ""};
     int max_smem = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, cfg.device));
@@ -2097,8 +2099,8 @@ Error Solver::cg_plan(const std::vector<int> &ptr, const std::vector<int> &idx, 
     int smax = 0;
     for (int k = 0; k < C; k++) smax = std::max(smax, (int)sends[k].size());
     if (nrmax + hmax >= (1 << 20)) return {0, ""};
-    const size_t smem = 8 * ((size_t)8 * nrmax + hmax + 256 + (size_t)(kCgAgg + 3) * NA + kCgAgg + (size_t)K * nrmax + smax) +
-                        4 * ((size_t)K * nrmax + smax + kCgAgg + 1 + nrmax);
+    const size_t smem = 8 * ((size_t)8 * nrmax + hmax + 256 + (size_t)4 * NA + kCgAgg + (size_t)K * nrmax + smax) +
+                        4 * ((size_t)K * nrmax + smax + kCgAgg + 1);
     if (smem > (size_t)max_smem) return {0, ""};
     CUDA_TRY(cudaFuncSetAttribute(k_cg_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     CUDA_TRY(cudaFuncSetAttribute(k_cg_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
