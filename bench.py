@@ -111,15 +111,41 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-# algorithmic bytes per band*direction*cell update of each kernel (s = bytes
-# of the stored intensity; the gradient is stored as 3 components)
-def kernel_bytes_per_update(name: str, s: int) -> float:
-    return {
-        "gradient": s + 3 * s,   # read e, write g
-        "residual": s + 3 * s + s,  # read e, read g, write R
-        "sweep": s + 2 * s,      # read R (overwritten by the correction), read+write e
-        "moments": s,            # read e
-    }.get(name, 0.0)
+# Algorithmic bytes of one launch of each kernel: the least DRAM traffic its
+# work needs. s = bytes of a stored intensity (4 in the FP32 form, 8 in
+# FP64), dim = stored gradient components, rec = bytes of one sweep record
+# (per direction and cell). Per band*direction*cell update unless noted:
+#   gradient  read e, write g                         (1 + dim) s
+#   residual  read e and g, write R                   (2 + dim) s
+#   sweep     read R, write the corrections, read the
+#             level records once per band             2 s + rec / nb
+#   moments   read e and the corrections, write e     3 s
+#   pcg       (per launch) the macro system and three vectors, read once:
+#             nnz (8 B value + 4 B column) + nc (b, x in, x out, diagonal: 32 B; order: 4 B)
+def kernel_algorithmic_bytes(name: str, s: int, dim: int, nb: int, nd: int, nc: int, nnz: int):
+    rec = 48 if s == 4 else 64
+    per_update = {"gradient": (1 + dim) * s, "residual": (2 + dim) * s, "sweep": 2 * s + rec / nb,
+                  "moments": 3 * s}
+    if name in per_update:
+        return per_update[name] * nb * nd * nc
+    if name == "pcg":
+        return nnz * 12 + nc * 36
+    return None
+
+
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
+# one ncu capture of each kernel on the 17,939-cell 40-band cell, FP32 form;
+# see profiles/transport_kernels_config2_fp32.md for the command.
+NCU_TRAFFIC_CONFIG2_FP32 = {"residual": 757.636864e6, "sweep": 391.150336e6, "gradient": 518.09664e6,
+                            "moments": 516.764928e6, "pcg": 1.895424e6}
+
+
+def macro_nnz(deck) -> int:
+    """Nonzeros of the macro two-point-flux system: one diagonal entry per cell and
+    one per interior face side (boundary and periodic faces enter the
+    right-hand side)."""
+    m = deck.mesh
+    return m.n_cells + sum(len(c) for c in m.cells) - len(m.edges)
 
 
 def run_ours(args, rank: int, world: int, local_rank: int):
@@ -163,18 +189,34 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         ms = float(t.item())
     value = upd_per_step * args.steps * world / (ms * 1e-3)
 
-    # roofline of the dominant kernel (per-launch CUDA events on the solver's stream)
+    # roofline of the dominant kernel (per-launch CUDA events on the solver's
+    # stream), and of every streaming kernel
     kern = st["kernels"]
-    dom = max(kern.items(), key=lambda kv: kv[1]["ms"])
-    dname, dk = dom[0], dom[1]
-    bpu = kernel_bytes_per_update(dname, s_bytes)
     peak, peak_kind = measured_peak_gbs()
-    per_launch_ms = dk["ms"] / dk["launches"]
-    achieved = (bpu * upd_per_step) / (per_launch_ms * 1e-3) / 1e9 if bpu else None
-    roofline = {"kernel": dname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+    total_ms = sum(v["ms"] for v in kern.values())
+    dim = 2 if deck.mesh.nodes.shape[1] == 2 else 3
+    nnz = macro_nnz(deck)
+
+    def kernel_roofline(name):
+        k = kern[name]
+        per_launch_ms = k["ms"] / k["launches"]
+        alg = kernel_algorithmic_bytes(name, s_bytes, dim, nb, nd, nc, nnz)
+        achieved = alg / (per_launch_ms * 1e-3) / 1e9 if alg else None
+        traffic = None
+        if args.workload == "config2" and prec == g.GBTE_FP32_MIXED:
+            traffic = NCU_TRAFFIC_CONFIG2_FP32.get(name)
+        return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                "traffic": None, "bytes_per_update": bpu, "launch_ms": per_launch_ms,
-                "kernel_share": dk["ms"] / sum(v["ms"] for v in kern.values())}
+                "traffic": traffic, "algorithmic_bytes": alg, "launch_ms": per_launch_ms,
+                "kernel_share": k["ms"] / total_ms}
+
+    dname = max(kern.items(), key=lambda kv: kv[1]["ms"])[0]
+    roofline = kernel_roofline(dname)
+    if dname == "pcg":
+        roofline["note"] = ("the macro CG is latency-bound (two cluster barriers per CG iteration on a "
+                            "shared-memory-resident system), not bandwidth-bound: its HBM fraction is "
+                            "near zero by construction; see hbm_kernels for the streaming kernels")
+    hbm_kernels = {n: kernel_roofline(n) for n in ("residual", "sweep", "gradient", "moments") if n in kern}
     kernel_table = {k: {"ms_per_launch": v["ms"] / v["launches"], "launches": v["launches"],
                         "share": v["ms"] / sum(x["ms"] for x in kern.values())} for k, v in kern.items()}
     solver.close()
@@ -198,7 +240,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                        "updates_per_step": upd_per_step, "precision": args.precision,
                        "l2": f"band state {upd_per_step * s_bytes / 1e6:.0f} MB per copy, larger than the 126 MB L2",
                        "parallelism": f"replicas x{world} (independent seeded cells)" if world > 1 else "1 GPU"},
-            "roofline": roofline, "kernels": kernel_table, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roofline, "hbm_kernels": hbm_kernels, "kernels": kernel_table, "cpu_baseline": cpu,
+            "e2e": e2e,
             "time_to_residual": ttr, "gpu_launches": int(st["kernel_launches"]), "clocks": clk,
             "macro": {"ms_per_step": st["macro_ms"] / args.steps, "cg_iterations": st["macro_cg_iterations"]},
         }
