@@ -199,8 +199,8 @@ class StaticBTESynthetic:
         lib = library()
         v = _views(deck)
         nc = deck.mesh.n_cells
-        if cell_heat is None and deck.heat_source is not None:
-            cell_heat = np.full(nc, float(deck.heat_source))
+        if cell_heat is None:
+            cell_heat = deck.cell_heat()
         heat = np.ascontiguousarray(cell_heat, dtype=np.float64) if cell_heat is not None else None
         kw = {"max_iter": deck.max_iter, "err_temp": deck.residual_temp, "err_flux": deck.residual_flux}
         kw.update(opt)

@@ -54,6 +54,84 @@ class Mesh2D:
         return int(self.cells.shape[0])
 
 
+@dataclasses.dataclass
+class Mesh3D:
+    """A 3D tetrahedral mesh in unit coordinates (multiplied by ScaleX/Y/Z on
+    read). Same field names as :class:`Mesh2D`, with triangles as boundary
+    elements:
+
+    nodes:      (Nn, 3) float64
+    cells:      (Nc, 4) int tetrahedra
+    edges:      (Nb, 3) int boundary triangles
+    edge_tags:  (Nb,) int boundary tags (1-based, as the BC file names them)
+    cell_region:(Nc,) int region index (0-based, GeometryMaterialType row - 1)
+    """
+
+    nodes: np.ndarray
+    cells: np.ndarray
+    edges: np.ndarray
+    edge_tags: np.ndarray
+    cell_region: np.ndarray
+
+    @property
+    def n_cells(self) -> int:
+        return int(self.cells.shape[0])
+
+
+def hex_tet_block_mesh(nx: int, ny: int, nz: int, h: float, jitter: float = 0.0, seed: int = 0,
+                       region_z: Optional[float] = None) -> Mesh3D:
+    """Structured nx x ny x nz grid of cubes of edge h on [0, nx h] x [0, ny h]
+    x [0, nz h], each cube split into the 6 tetrahedra around its
+    (0,0,0)-(1,1,1) diagonal (the same split in every cube, so faces match).
+    Vertices are moved by a uniform random offset of up to jitter * h per
+    coordinate (seeded), except along the coordinates in which they lie on
+    the outer boundary. Boundary tags: 1 bottom (z = 0), 2 top, 3 x = 0,
+    4 x = max, 5 y = 0, 6 y = max. Cells whose centre has z >= region_z are
+    region 1, the rest region 0."""
+    ix, iy, iz = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
+    grid = np.stack([ix.ravel(), iy.ravel(), iz.ravel()], axis=1)  # node id = (i * (ny+1) + j) * (nz+1) + k
+
+    def nid(i, j, k):
+        return (i * (ny + 1) + j) * (nz + 1) + k
+
+    nodes = grid.astype(np.float64) * h
+    if jitter > 0:
+        rng = np.random.default_rng(seed)
+        off = rng.uniform(-jitter * h, jitter * h, size=nodes.shape)
+        lim = np.array([nx, ny, nz])
+        off[(grid == 0) | (grid == lim)] = 0.0
+        nodes += off
+    ci, cj, ck = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    ci, cj, ck = ci.ravel(), cj.ravel(), ck.ravel()
+    e = np.eye(3, dtype=int)
+    tets = []
+    for perm in ((0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)):
+        a = np.zeros(3, dtype=int)
+        b = e[perm[0]]
+        c = b + e[perm[1]]
+        d = np.ones(3, dtype=int)
+        tets.append(np.stack([nid(ci + p[0], cj + p[1], ck + p[2]) for p in (a, b, c, d)], axis=1))
+    cells = np.stack(tets, axis=1).reshape(-1, 4)
+    # boundary triangles: tet faces that occur once
+    faces = np.concatenate([cells[:, [0, 1, 2]], cells[:, [0, 1, 3]], cells[:, [0, 2, 3]], cells[:, [1, 2, 3]]])
+    key = np.sort(faces, axis=1)
+    _, inv, cnt = np.unique(key, axis=0, return_inverse=True, return_counts=True)
+    bfaces = faces[cnt[inv.ravel()] == 1]
+    g = grid[bfaces]  # integer coordinates of the three vertices
+    tags = np.zeros(len(bfaces), dtype=np.int64)
+    for t, (axis, val) in enumerate(((2, 0), (2, nz), (0, 0), (0, nx), (1, 0), (1, ny)), start=1):
+        on = np.all(g[:, :, axis] == val, axis=1)
+        tags[(tags == 0) & on] = t
+    assert np.all(tags > 0)
+    cz = nodes[cells][:, :, 2].mean(axis=1)
+    region = np.zeros(len(cells), dtype=np.int64)
+    if region_z is not None:
+        region[cz >= region_z] = 1
+    # cells grouped by region, the order in which the MSH file lists them
+    order = np.argsort(region, kind="stable")
+    return Mesh3D(nodes=nodes, cells=cells[order], edges=bfaces, edge_tags=tags, cell_region=region[order])
+
+
 def square_tri_mesh(nx: int, ny: int) -> Mesh2D:
     """Structured nx x ny grid on [0,1]^2, each square split into 2 triangles
     along its (0,0)-(1,1) diagonal. Boundary tags: 1 left, 2 right,
@@ -369,6 +447,33 @@ def write_msh41(path: str, mesh: Mesh2D) -> None:
         f.write("\n".join(lines) + "\n")
 
 
+def write_msh41_3d(path: str, mesh: Mesh3D) -> None:
+    """gmsh MSH 4.1 ASCII, 3D: one node block, boundary triangles tagged by
+    their boundary tag (entity tag), tetrahedra in entity (region + 1)."""
+    nn = len(mesh.nodes)
+    lines = ["$MeshFormat", "4.1 0 8", "$EndMeshFormat", "$Nodes",
+             f"1 {nn} 1 {nn}", f"3 1 0 {nn}"]
+    lines += [str(i + 1) for i in range(nn)]
+    lines += [f"{x:.17g} {y:.17g} {z:.17g}" for x, y, z in mesh.nodes]
+    lines += ["$EndNodes", "$Elements"]
+    blocks = []
+    for t in np.unique(mesh.edge_tags):
+        blocks.append((2, int(t), 2, mesh.edges[mesh.edge_tags == t]))
+    for reg in np.unique(mesh.cell_region):
+        blocks.append((3, int(reg) + 1, 4, mesh.cells[mesh.cell_region == reg]))
+    total = sum(len(b[3]) for b in blocks)
+    lines.append(f"{len(blocks)} {total} 1 {total}")
+    eid = 1
+    for dim, tag, typ, els in blocks:
+        lines.append(f"{dim} {tag} {typ} {len(els)}")
+        for el in els:
+            lines.append(f"{eid} " + " ".join(str(int(v) + 1) for v in el))
+            eid += 1
+    lines.append("$EndElements")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
 def write_band_database(path: str, bands: BandTable) -> None:
     with open(path, "w") as f:
         for i in range(bands.n_bands):
@@ -401,14 +506,35 @@ class Deck:
     max_iter: int = 10000
     order: str = "2"
     heat_source: Optional[float] = None   # uniform volumetric heat (W/m^3)
-    mesh_format: str = "COMSOL"           # COMSOL or MSH
+    mesh_format: str = "COMSOL"           # COMSOL or MSH (3D meshes: MSH)
+    region_heat: Optional[List[float]] = None  # heat per region (W/m^3), HeatType REGION
+
+    @property
+    def dimension(self) -> int:
+        return int(self.mesh.nodes.shape[1])
+
+    @property
+    def n_regions(self) -> int:
+        return int(np.max(self.mesh.cell_region)) + 1
+
+    def cell_heat(self) -> Optional[np.ndarray]:
+        """Volumetric heat per cell, or None when there is none."""
+        if self.region_heat is not None:
+            return np.asarray(self.region_heat, dtype=np.float64)[np.asarray(self.mesh.cell_region)]
+        if self.heat_source is not None:
+            return np.full(self.mesh.n_cells, float(self.heat_source))
+        return None
 
     def write(self, root: str) -> str:
         """Write ``root/input/*``; returns the input directory."""
         d = os.path.join(root, "input")
         os.makedirs(d, exist_ok=True)
         mesh_name = "mesh.mphtxt" if self.mesh_format == "COMSOL" else "mesh.msh"
-        if self.mesh_format == "COMSOL":
+        if self.dimension == 3:
+            if self.mesh_format != "MSH":
+                raise ValueError("3D meshes are written as MSH")
+            write_msh41_3d(os.path.join(d, mesh_name), self.mesh)
+        elif self.mesh_format == "COMSOL":
             write_mphtxt(os.path.join(d, mesh_name), self.mesh)
         else:
             write_msh41(os.path.join(d, mesh_name), self.mesh)
@@ -423,17 +549,27 @@ class Deck:
                     "Tref=\n%.17g\nMaxNumIter=\n%d\nResidualTemp=\n%.17g\nResidualFlux=\n%.17g\n"
                     % (self.order, self.tref, self.max_iter, self.residual_temp, self.residual_flux))
         with open(os.path.join(d, "GEOMETRY"), "w") as f:
-            f.write("GeometryDimension=\n2\nScaleX=\n%.17g\nScaleY=\n%.17g\nBCFile=\ninput/bc.dat\n"
-                    "MeshType=\n%s\nMeshFile=\ninput/%s\n"
-                    % (self.scale[0], self.scale[1], self.mesh_format, mesh_name))
+            f.write("GeometryDimension=\n%d\nScaleX=\n%.17g\nScaleY=\n%.17g\n"
+                    % (self.dimension, self.scale[0], self.scale[1]))
+            if self.dimension == 3:
+                f.write("ScaleZ=\n%.17g\n" % self.scale[2])
+            f.write("BCFile=\ninput/bc.dat\nMeshType=\n%s\nMeshFile=\ninput/%s\n"
+                    % (self.mesh_format, mesh_name))
             if self.heat_source is not None:
                 f.write("UniformHeat=\n%.17g\n" % self.heat_source)
+            if self.region_heat is not None:
+                f.write("HeatType=\nREGION\nHeatFile=\ninput/heat.dat\n")
+        if self.region_heat is not None:
+            with open(os.path.join(d, "heat.dat"), "w") as f:
+                f.write(f"{len(self.region_heat)}\n")
+                for i, q in enumerate(self.region_heat):
+                    f.write(f"{i + 1} {q:.17g}\n")
         with open(os.path.join(d, "PHONON"), "w") as f:
             f.write("MaterialNumber=\n1\nBandNumber=\n%d\n\nMaterialFile 1= DATABASE\ninput/bands.dat\n\n"
-                    "GeometryMaterialType=\n1 1\n\nMaterialDimension=\n%d\nAngle_method=\n%d\n"
+                    "GeometryMaterialType=\n%s\n\nMaterialDimension=\n%d\nAngle_method=\n%d\n"
                     "Ntheta=\n%d\nNphi=\n%d\n"
-                    % (self.bands.n_bands, self.material_dim, self.angle_method,
-                       self.n_theta, self.n_phi))
+                    % (self.bands.n_bands, "\n".join(f"{r + 1} 1" for r in range(self.n_regions)),
+                       self.material_dim, self.angle_method, self.n_theta, self.n_phi))
         return d
 
 
@@ -466,3 +602,25 @@ def config2_deck(h_nm: float = 3.0, n_bands: int = 40, n_phi: int = 16, seed: in
     kw.setdefault("angle_method", 1)
     kw.setdefault("tref", 0.0)
     return Deck(mesh=mesh, bands=bands, bcs=bcs, scale=(L, L), **kw)
+
+
+def config3_deck(h_nm: float = 2.5, n_bands: int = 40, n_theta: int = 4, n_phi: int = 4, seed: int = 1,
+                 size_nm: Tuple[float, float, float] = (100.0, 100.0, 500.0), **kw) -> Deck:
+    """3D hotspot block: size_nm box (100 x 100 x 500 nm by default) of cubes
+    of edge h split into 6 tetrahedra each, vertices jittered by up to 20% of
+    h (seeded), the config-2 sine-dispersion bands, Gauss-Legendre angles
+    (8 * n_theta * n_phi directions: 128 by default), 1e18 W/m^3 generated
+    in the top 20 nm (region 2, HeatType REGION), bottom isothermal at
+    300 K, sides and top diffuse. Coordinates are in nm (Scale 1e-9)."""
+    nx, ny, nz = (int(round(x / h_nm)) for x in size_nm)
+    mesh = hex_tet_block_mesh(nx, ny, nz, h_nm, jitter=0.2, seed=seed, region_z=size_nm[2] - 20.0)
+    bands = sine_dispersion_bands(n_bands)
+    bcs = [BC(1, 1, 300.0), BC(2, 2, 0.0), BC(3, 2, 0.0), BC(4, 2, 0.0), BC(5, 2, 0.0), BC(6, 2, 0.0)]
+    kw.setdefault("angle_method", 2)
+    kw.setdefault("n_theta", n_theta)
+    kw.setdefault("n_phi", n_phi)
+    kw.setdefault("material_dim", 3)
+    kw.setdefault("tref", 300.0)
+    kw.setdefault("mesh_format", "MSH")
+    kw.setdefault("region_heat", [0.0, 1e18])
+    return Deck(mesh=mesh, bands=bands, bcs=bcs, scale=(1e-9, 1e-9, 1e-9), **kw)

@@ -55,19 +55,21 @@ def solve(deck, T0: Optional[np.ndarray] = None, max_iter: Optional[int] = None,
     temperatures ``Tband`` (Nb x Nc), iteration count and final margins.
     """
     m = deck.mesh
+    dim = deck.dimension
     nc = m.n_cells
     nn = len(m.nodes)
     xyz = np.zeros((nn, 3))
-    xyz[:, 0] = m.nodes[:, 0] * deck.scale[0]
-    xyz[:, 1] = m.nodes[:, 1] * deck.scale[1]
+    for a in range(dim):
+        xyz[:, a] = m.nodes[:, a] * deck.scale[a]
     cells = [np.asarray(c) for c in m.cells]
     cptr = np.zeros(nc + 1, dtype=np.int32)
     cptr[1:] = np.cumsum([len(c) for c in cells])
     cverts = np.concatenate(cells).astype(np.int32)
     creg = np.asarray(m.cell_region, dtype=np.int32)
-    nbe = len(m.edges)
-    bptr = (np.arange(nbe + 1) * 2).astype(np.int32)
-    bverts = np.asarray(m.edges, dtype=np.int32).ravel()
+    belems = np.asarray(m.edges, dtype=np.int32)
+    nbe = len(belems)
+    bptr = (np.arange(nbe + 1) * belems.shape[1]).astype(np.int32)
+    bverts = np.ascontiguousarray(belems.ravel())
     btag = np.asarray(m.edge_tags, dtype=np.int32)
     bc_tag = np.asarray([b.tag for b in deck.bcs], dtype=np.int32)
     bc_type = np.asarray([b.type for b in deck.bcs], dtype=np.int32)
@@ -76,24 +78,24 @@ def solve(deck, T0: Optional[np.ndarray] = None, max_iter: Optional[int] = None,
     nb = B.n_bands
     arr = {k: np.ascontiguousarray(getattr(B, k), dtype=np.float64)
            for k in ("v", "tau", "C", "lattice_ratio", "heat_ratio")}
-    reg_mat = np.zeros(1, dtype=np.int32)
+    reg_mat = np.zeros(deck.n_regions, dtype=np.int32)
     if T0 is None:
         T0 = np.full(nc, deck.tref)
     T0 = np.ascontiguousarray(T0, dtype=np.float64)
-    if cell_heat is None and deck.heat_source is not None:
-        cell_heat = np.full(nc, float(deck.heat_source))
+    if cell_heat is None:
+        cell_heat = deck.cell_heat()
     if cell_heat is not None:
         cell_heat = np.ascontiguousarray(cell_heat, dtype=np.float64)
     out_T = np.zeros(nc); out_E = np.zeros(nc); out_q = np.zeros(3 * nc); out_Tb = np.zeros(nb * nc)
     iters = ctypes.c_int(0)
     err = np.zeros(2)
     rc = lib().oracle_solve(
-        2, nn, _p(xyz, ctypes.c_double), nc, _p(cptr, ctypes.c_int), _p(cverts, ctypes.c_int),
+        dim, nn, _p(xyz, ctypes.c_double), nc, _p(cptr, ctypes.c_int), _p(cverts, ctypes.c_int),
         _p(creg, ctypes.c_int), nbe, _p(bptr, ctypes.c_int), _p(bverts, ctypes.c_int), _p(btag, ctypes.c_int),
         len(deck.bcs), _p(bc_tag, ctypes.c_int), _p(bc_type, ctypes.c_int), _p(bc_val, ctypes.c_double),
         1, nb, _p(arr["v"], ctypes.c_double), _p(arr["tau"], ctypes.c_double), _p(arr["C"], ctypes.c_double),
         _p(arr["lattice_ratio"], ctypes.c_double), _p(arr["heat_ratio"], ctypes.c_double),
-        _p(reg_mat, ctypes.c_int), 1, deck.material_dim, deck.angle_method, deck.n_theta, deck.n_phi,
+        _p(reg_mat, ctypes.c_int), len(reg_mat), deck.material_dim, deck.angle_method, deck.n_theta, deck.n_phi,
         ctypes.c_double(deck.scale[0]), _p(cell_heat, ctypes.c_double), _p(T0, ctypes.c_double), None,
         int(max_iter if max_iter is not None else deck.max_iter),
         ctypes.c_double(err_T if err_T is not None else deck.residual_temp),
