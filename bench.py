@@ -50,12 +50,18 @@ def measured_peak_gbs():
         return HBM_FALLBACK_GBS, "fallback"
 
 
-def build_deck(workload: str, seed: int):
+def build_deck(workload: str, seed: int, h_nm: float = 0.0):
     from giftbte_b200 import decks
 
     if workload == "config1":
         d = decks.config1_deck(40)
         desc = "gray 1 um square, 40x40x2 triangles (3200), 1 band, 32 CADOM directions"
+    elif workload == "config3":
+        h = h_nm or 2.5
+        d = decks.config3_deck(h_nm=h, seed=1 + seed)
+        desc = (f"3D hotspot block 100x100x500 nm, cubes of {h} nm split into 6 jittered tets "
+                f"({d.mesh.n_cells} tets), 40 sine-dispersion bands, 128 Gauss directions, "
+                f"1e18 W/m^3 in the top 20 nm, seed {1 + seed}")
     else:
         d = decks.config2_deck(h_nm=3.0, n_bands=40, n_phi=16, seed=seed)
         desc = (f"2D nanoporous periodic cell 300 nm, r=100 nm diffuse pore, mean edge 3 nm "
@@ -157,7 +163,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     torch.cuda.set_device(local_rank)
     torch.cuda.init()
     stream = torch.cuda.current_stream()
-    deck, desc = build_deck(args.workload, seed=rank)
+    deck, desc = build_deck(args.workload, seed=rank, h_nm=args.h_nm)
     nc = deck.mesh.n_cells
     prec = g.GBTE_FP32_MIXED if args.precision == "fp32" else g.GBTE_FP64
     s_bytes = 4 if prec == g.GBTE_FP32_MIXED else 8
@@ -345,7 +351,10 @@ def run_reference(args, rank: int):
         return None
     import oracle
 
-    deck, desc = build_deck(args.workload, seed=0)
+    if args.workload == "config3":
+        return {"impl": "reference", "unavailable": "the reference's public release has no 3D mesh code "
+                                                    "(3D decks cannot be read by it)"}
+    deck, desc = build_deck(args.workload, seed=0, h_nm=args.h_nm)
     nb = deck.bands.n_bands
     nd = 4 * deck.n_phi if deck.material_dim == 2 else 8 * deck.n_theta * deck.n_phi
     upd = nb * nd * deck.mesh.n_cells
@@ -395,7 +404,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
-    ap.add_argument("--workload", choices=["config2", "config1"], default="config2")
+    ap.add_argument("--workload", choices=["config2", "config1", "config3"], default="config2")
+    ap.add_argument("--h-nm", type=float, default=0.0, help="config3 mesh spacing (default 2.5 nm)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--max-iter-e2e", type=int, default=2000)
     ap.add_argument("--ref-steps", type=int, default=2)

@@ -64,7 +64,8 @@ class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("use_limiter", ctypes.c_int), ("max_iter", ctypes.c_int),
                 ("err_temp", ctypes.c_double), ("err_flux", ctypes.c_double), ("cell_heat", _c_dbl_p),
                 ("stream", ctypes.c_void_p), ("device", ctypes.c_int), ("verbose", ctypes.c_int),
-                ("macro_rtol", ctypes.c_double), ("profile", ctypes.c_int), ("sweep_bands", ctypes.c_int)]
+                ("macro_rtol", ctypes.c_double), ("profile", ctypes.c_int), ("sweep_bands", ctypes.c_int),
+                ("sweep_far_slots", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):

@@ -106,6 +106,7 @@ int create_common(const gbte::RawMesh &raw, const gbte::Bands &bands_in, const g
     cfg.verbose = opt.verbose;
     cfg.profile = opt.profile;
     cfg.sweep_bands = opt.sweep_bands;
+    cfg.sweep_far_slots = opt.sweep_far_slots;
     cfg.device = opt.device;
     cfg.stream = (cudaStream_t)opt.stream;
     if (opt.precision != GBTE_FP64 && opt.precision != GBTE_FP32_MIXED)

@@ -804,7 +804,26 @@ __global__ void k_remacro(DMesh m, const double *__restrict__ Th, const double *
 
 // incoming boundary values by wall type; reads only outgoing entries (or a
 // snapshot for chained specular sources), writes only incoming entries
-__global__ void k_gather(DMesh m, DPhys p, const double *__restrict__ dif_w, const int *__restrict__ spec_src,
+// Diffuse walls re-emit the same value into every incoming direction: the
+// weighted sum of the outgoing values, formed once per (wall side, band).
+__global__ void k_diffuse_sum(DMesh m, DPhys p, const double *__restrict__ dif_w, const double *__restrict__ eb,
+                              double *__restrict__ dsum) {
+    const int nb = p.nb;
+    const size_t total = (size_t)m.nbs * nb;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b = (int)(t % nb), s = (int)(t / nb);
+        if (m.bs_cell[s] < 0 || m.b_type[s >> 1] != 2) continue;
+        double acc = 0;
+        const double *w = dif_w + (size_t)s * p.nd;
+        for (int q = 0; q < p.nd; q++) {
+            const double wq = w[q];
+            if (wq != 0) acc += wq * eb[((size_t)q * m.nbs + s) * nb + b];
+        }
+        dsum[t] = acc;
+    }
+}
+
+__global__ void k_gather(DMesh m, DPhys p, const double *__restrict__ dsum, const int *__restrict__ spec_src,
                          const double *__restrict__ snap, double *eb) {
     const int nb = p.nb;
     const size_t total = (size_t)p.nd * m.nbs * nb;
@@ -824,13 +843,7 @@ __global__ void k_gather(DMesh m, DPhys p, const double *__restrict__ dif_w, con
         if (type == 1) {
             val = p.C[b] * m.b_T[ib];
         } else if (type == 2) {
-            double acc = 0;
-            const double *w = dif_w + (size_t)s * p.nd;
-            for (int q = 0; q < p.nd; q++) {
-                const double wq = w[q];
-                if (wq != 0) acc += wq * eb[((size_t)q * m.nbs + s) * nb + b];
-            }
-            val = acc;
+            val = dsum[(size_t)s * nb + b];
         } else if (type == 3) {
             const int src = spec_src[(size_t)s * p.nd + d];
             const double *from = snap ? snap : eb;
@@ -1581,7 +1594,8 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
         // packed sweep records in the storage precision (host plan with
         // the on-chip ring and far slots)
         SweepPlan sp;
-        Error pe = build_sweep_plan(mesh, ang, sched, kSweepMinRing, kSweepFarCap, sp);
+        Error pe = build_sweep_plan(mesh, ang, sched, kSweepMinRing,
+                                    cfg.sweep_far_slots == 0 ? kSweepFarCap : std::max(0, cfg.sweep_far_slots), sp);
         if (pe.code) return pe;
         ring_ = sp.ring;
         far_slots_ = sp.far_enabled ? sp.far_slots : 0;
@@ -1841,6 +1855,7 @@ Error Solver::alloc_all() {
     corr_ = A(ne * S);
     Tbase_ = (double *)A(nc * 8);
     Bflux_ = (double *)A((size_t)nd * nc * 8);
+    dsum_ = (double *)A(std::max<size_t>(1, nbs) * nb * 8);
     gTb_ = (double *)A(nc * 3 * 8);
     eb_ = (double *)A(nd * nbs * nb * 8);
     eb_snap_ = need_snapshot_ ? (double *)A(nd * nbs * nb * 8) : nullptr;
@@ -2287,7 +2302,8 @@ Error Solver::solve_t(SolveStats &st) {
         CUDA_TRY(cudaFuncSetAttribute(k_moments<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem));
     auto gather = [&]() {
         if (need_snapshot_) cudaMemcpyAsync(eb_snap_, eb_, (size_t)nd * nbs * nb * 8, cudaMemcpyDeviceToDevice, s);
-        GL(K_GATHER, k_gather<<<gB, kThreads, 0, s>>>(dm_, dp_, dif_w_, spec_src_, need_snapshot_ ? eb_snap_ : nullptr, eb_));
+        GL(K_GATHER, k_diffuse_sum<<<grid_for((size_t)nbs * nb), kThreads, 0, s>>>(dm_, dp_, dif_w_, eb_, dsum_));
+        GL(K_GATHER, k_gather<<<gB, kThreads, 0, s>>>(dm_, dp_, dsum_, spec_src_, need_snapshot_ ? eb_snap_ : nullptr, eb_));
     };
     if (!started_) {
         // _set_initial (:765-782) and the initial boundary values (StaticBTESyntheticSolver.cpp:45-62)

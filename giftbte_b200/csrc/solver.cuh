@@ -47,7 +47,8 @@ struct SolverConfig {
     double macro_rtol = 1e-13;
     int verbose = 0;
     int profile = 0;
-    int sweep_bands = 0;  // bands per sweep CTA, 0 = automatic
+    int sweep_bands = 0;      // bands per sweep CTA, 0 = automatic
+    int sweep_far_slots = 0;  // far-slot cap of the sweep plan: 0 = automatic, < 0 = none
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -126,6 +127,7 @@ private:
            *T1_ = nullptr, *red_ = nullptr;
     // diffuse weights / specular map
     double *dif_w_ = nullptr;
+    double *dsum_ = nullptr;  // [wall side][band] diffuse re-emission sums
     int *spec_src_ = nullptr;
     bool need_snapshot_ = false;
     // schedule on device

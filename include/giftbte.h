@@ -126,6 +126,8 @@ typedef struct {
     double macro_rtol;        /* relative residual of the macro CG solve; 0 = default 1e-13 */
     int profile;              /* 1: time every kernel launch with CUDA events (gbte_stats.kernel_ms) */
     int sweep_bands;          /* bands per CTA of the upwind sweep (1..32); 0 = automatic */
+    int sweep_far_slots;      /* on-chip slots per direction for upwind reads older than the sweep's
+                                 ring: 0 = automatic (2048), < 0 = none (such reads go to memory) */
 } gbte_options;
 
 #define GBTE_NUM_KERNELS 16
