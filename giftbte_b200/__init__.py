@@ -108,7 +108,7 @@ class DeckInfo(ctypes.Structure):
 EXPORTS = ["gbte_inspect_deck", "gbte_inspect_mesh", "gbte_default_options", "gbte_create", "gbte_create_from_deck", "gbte_set_initial",
            "gbte_fourier_initial", "gbte_solve", "gbte_get_fields", "gbte_write_outputs", "gbte_get_sizes",
            "gbte_get_geometry", "gbte_last_error", "gbte_status_string", "gbte_destroy", "gbte_kernel_name",
-           "gbte_solve_with", "gbte_fourier_initial_noalloc"]
+           "gbte_solve_with", "gbte_fourier_initial_noalloc", "gbte_batch_create", "gbte_batch_geometries"]
 
 _lib = None
 
@@ -141,6 +141,10 @@ def library():
         lib.gbte_destroy.argtypes = [ctypes.c_void_p]
         lib.gbte_fourier_initial.argtypes = [ctypes.c_void_p]
         lib.gbte_fourier_initial_noalloc.argtypes = [ctypes.c_void_p]
+        lib.gbte_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(MeshView), ctypes.POINTER(BandTableC),
+                                          ctypes.POINTER(BCTable), ctypes.POINTER(AngleSpec),
+                                          ctypes.POINTER(Options), ctypes.POINTER(ctypes.c_void_p)]
+        lib.gbte_batch_geometries.argtypes = [ctypes.c_void_p, _c_int_p, _c_int_p]
         lib.gbte_inspect_deck.argtypes = [ctypes.c_char_p, ctypes.POINTER(DeckInfo)]
         lib.gbte_inspect_mesh.argtypes = [ctypes.POINTER(MeshView), ctypes.POINTER(BandTableC),
                                           ctypes.POINTER(BCTable), ctypes.POINTER(AngleSpec),
@@ -215,6 +219,61 @@ class StaticBTESynthetic:
         s = cls(h)
         s.set_initial(np.full(nc, deck.tref))
         return s
+
+    @classmethod
+    def from_decks(cls, decks, precision: int = GBTE_FP64, device: int = 0, verbose: int = 0,
+                   **opt) -> "StaticBTESynthetic":
+        """One batched solve of several independent in-memory decks
+        (gbte_batch_create): the band table, quadrature, ScaleX and the
+        iteration limits come from the first deck; fields are the decks'
+        cell arrays concatenated (see :meth:`geometry_offsets`)."""
+        lib = library()
+        views = [_views(d) for d in decks]
+        n = len(decks)
+        meshes = (MeshView * n)(*[v["mv"] for v in views])
+        bcs = (BCTable * n)(*[v["bc"] for v in views])
+        nreg = max(int(np.max(d.mesh.cell_region)) + 1 for d in decks)
+        B = decks[0].bands
+        arrs = [np.ascontiguousarray(getattr(B, k), dtype=np.float64)
+                for k in ("v", "tau", "C", "lattice_ratio", "heat_ratio")]
+        reg = np.zeros(nreg, dtype=np.int32)
+        bt = BandTableC(1, B.n_bands, *[_ptr(a, ctypes.c_double) for a in arrs], nreg, _ptr(reg, ctypes.c_int),
+                        decks[0].material_dim)
+        heats = [d.cell_heat() for d in decks]
+        heat = None
+        if any(h is not None for h in heats):
+            heat = np.ascontiguousarray(np.concatenate([h if h is not None else np.zeros(d.mesh.n_cells)
+                                                        for h, d in zip(heats, decks)]), dtype=np.float64)
+        d0 = decks[0]
+        kw = {"max_iter": d0.max_iter, "err_temp": d0.residual_temp, "err_flux": d0.residual_flux}
+        kw.update(opt)
+        o = default_options(precision, device=device, verbose=verbose, **kw)
+        o.cell_heat = _ptr(heat, ctypes.c_double)
+        h = ctypes.c_void_p()
+        rc = lib.gbte_batch_create(n, meshes, ctypes.byref(bt), bcs, ctypes.byref(views[0]["an"]), ctypes.byref(o),
+                                   ctypes.byref(h))
+        if rc != GBTE_OK:
+            raise GBTEError(rc, lib.gbte_last_error(None).decode())
+        s = cls(h)
+        s.set_initial(np.concatenate([np.full(d.mesh.n_cells, d.tref) for d in decks]))
+        return s
+
+    def geometry_offsets(self) -> np.ndarray:
+        """Cell ranges of the geometries of this handle ([num + 1])."""
+        lib = library()
+        n = ctypes.c_int()
+        self._check(lib.gbte_batch_geometries(self._h, ctypes.byref(n), None))
+        off = np.zeros(n.value + 1, dtype=np.int32)
+        self._check(lib.gbte_batch_geometries(self._h, ctypes.byref(n), _ptr(off, ctypes.c_int)))
+        return off
+
+    def split(self, field: np.ndarray) -> list:
+        """A concatenated cell field (cells on the last axis for band fields)
+        cut into the geometries' pieces."""
+        off = self.geometry_offsets()
+        if field.ndim == 2 and field.shape[0] == self.num_bands and field.shape[1] == self.num_cells:
+            return [field[:, off[k]:off[k + 1]] for k in range(len(off) - 1)]
+        return [field[off[k]:off[k + 1]] for k in range(len(off) - 1)]
 
     # --- the reference's solve interface ----------------------------------
     def set_initial(self, T0: np.ndarray, q0: Optional[np.ndarray] = None,

@@ -280,6 +280,55 @@ int gbte_create(const gbte_mesh_view *mv, const gbte_band_table *bt, const gbte_
     }
 }
 
+int gbte_batch_create(int num, const gbte_mesh_view *meshes, const gbte_band_table *bt, const gbte_bc_table *bcs,
+                      const gbte_angle_spec *as, const gbte_options *opt, gbte_handle **out) {
+    try {
+        if (num <= 0 || !meshes || !bt || !bcs || !as || !opt || !out)
+            return fail(nullptr, {-1, "null argument or empty batch"}), GBTE_ERR_ARG;
+        *out = nullptr;
+        std::vector<gbte::RawMesh> raws(num);
+        std::vector<gbte::BCs> tables(num);
+        gbte::Bands B;
+        long long total = 0;
+        for (int k = 0; k < num; k++) {
+            gbte::Bands Bk;
+            int rc = convert_views(&meshes[k], bt, &bcs[k], raws[k], Bk, tables[k]);
+            if (rc != GBTE_OK) return rc;
+            if (k == 0) B = Bk;
+            total += meshes[k].num_cells;
+        }
+        gbte::RawMesh raw;
+        gbte::BCs all;
+        gbte::Error e = gbte::make_union(raws, tables, raw, all);
+        if (e.code) return fail(nullptr, e), status_of(e.code);
+        std::vector<double> heat;
+        if (opt->cell_heat) heat.assign(opt->cell_heat, opt->cell_heat + total);
+        return create_common(raw, B, all, *as, *opt, heat, out);
+    } catch (const std::bad_alloc &) {
+        g_create_error = "host allocation failed";
+        return GBTE_ERR_NOMEM;
+    } catch (const std::exception &ex) {
+        g_create_error = ex.what();
+        return GBTE_ERR_ARG;
+    }
+}
+
+int gbte_batch_geometries(gbte_handle *h, int *num, int *cell_offsets) {
+    if (!h) return GBTE_ERR_ARG;
+    const std::vector<int> &cp = h->solver.mesh.comp_ptr;
+    const int n = cp.empty() ? 1 : (int)cp.size() - 1;
+    if (num) *num = n;
+    if (cell_offsets) {
+        if (cp.empty()) {
+            cell_offsets[0] = 0;
+            cell_offsets[1] = h->solver.mesh.nc;
+        } else {
+            for (int k = 0; k <= n; k++) cell_offsets[k] = cp[k];
+        }
+    }
+    return GBTE_OK;
+}
+
 int gbte_create_from_deck(const char *dir, const gbte_options *opt_in, gbte_handle **out) {
     try {
         if (!dir || !out) return fail(nullptr, {-1, "null argument"}), GBTE_ERR_ARG;

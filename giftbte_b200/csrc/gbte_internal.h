@@ -18,6 +18,9 @@ struct RawMesh {
     std::vector<int> cptr, cverts, creg;   // cells
     std::vector<int> bptr, bverts, btag;   // boundary elements
     double Lx = 1, Ly = 1, Lz = 1;
+    // independent geometries of a batched solve: cells comp_ptr[k] ..
+    // comp_ptr[k+1] (no face or node shared between them); empty = one
+    std::vector<int> comp_ptr;
     int nn() const { return (int)(xyz.size() / 3); }
     int nc() const { return (int)cptr.size() - 1; }
     int nbe() const { return (int)bptr.size() - 1; }
@@ -79,6 +82,9 @@ struct FlatMesh {
     std::vector<double> node_x, node_y, node_z;
     // raw cell vertex lists (for output)
     std::vector<int> cptr, cverts;
+    // independent geometries (batched solve): cells comp_ptr[k] .. comp_ptr[k+1]
+    std::vector<int> comp_ptr;
+    int ncomp() const { return (int)comp_ptr.size() - 1; }
 
     int ncf() const { return (int)cf_area.size(); }
     int nbd() const { return (int)b_type.size(); }
@@ -86,11 +92,16 @@ struct FlatMesh {
     int nf() const { return (int)f_cell0.size(); }
 };
 
-// Per-direction upwind schedule: cells in level order.
+// Per-direction upwind schedule: cells in level order. With several
+// independent geometries (components), each component's cells keep their
+// own position range (its cell range) and their own levels, so that one
+// sweep CTA can walk one component of one direction.
 struct Schedule {
+    int ncomp = 1;
     std::vector<int> lvl_cells;   // [nd*nc]
-    std::vector<int> lvl_ptr;     // concatenated level offsets
-    std::vector<int> dir_lvl_off; // [nd+1] offsets into lvl_ptr (levels of d: lvl_ptr[dir_lvl_off[d] .. +1])
+    std::vector<int> lvl_ptr;     // concatenated level offsets (positions within the direction)
+    std::vector<int> dir_lvl_off; // [nd*ncomp+1] offsets into lvl_ptr: levels of (d, comp) are
+                                  // lvl_ptr[dir_lvl_off[d*ncomp+comp] .. dir_lvl_off[d*ncomp+comp+1]-1]
     std::vector<uint8_t> lag;     // [nd*nc] bit j set: face j of the cell is lagged (empty if none)
     int max_levels = 0;
     int lagged_faces = 0;
@@ -130,6 +141,12 @@ struct SweepPlan {
     std::vector<int> cell;    // [nd*nc] the cell at this position
     std::vector<int> far_w;   // [nd*nc] far slot this cell stores into, -1 none
 };
+
+// Disjoint union of independent geometries for one batched solve: nodes,
+// cells and boundary elements concatenated, the boundary tags of geometry k
+// (and the tags its periodic types name) shifted by k * (largest tag + 1),
+// comp_ptr set to the geometries' cell ranges. All share ScaleX.
+Error make_union(const std::vector<RawMesh> &meshes, const std::vector<BCs> &bcs, RawMesh &out, BCs &out_bcs);
 
 Error make_angles(int method, int ntheta, int nphi, int material_dim, Angles &out);
 Error build_flat_mesh(const RawMesh &raw, const BCs &bcs, const Bands &bands, FlatMesh &out);

@@ -21,6 +21,7 @@
 #include <queue>
 #include <string>
 #include <thread>
+#include <unordered_map>
 
 #include "gbte_internal.h"
 
@@ -100,6 +101,14 @@ Error build_flat_mesh(const RawMesh &raw, const BCs &bcs, const Bands &bands, Fl
     };
     m.cptr = raw.cptr;
     m.cverts = raw.cverts;
+    if (raw.comp_ptr.empty()) {
+        m.comp_ptr = {0, nc};
+    } else {
+        m.comp_ptr = raw.comp_ptr;
+        if (m.comp_ptr.front() != 0 || m.comp_ptr.back() != nc) return {-1, "component ranges must cover the cells"};
+        for (size_t k = 0; k + 1 < m.comp_ptr.size(); k++)
+            if (m.comp_ptr[k + 1] <= m.comp_ptr[k]) return {-1, "component ranges must be non-empty and increasing"};
+    }
     m.matter.resize(nc);
     m.vol.resize(nc);
     m.cx.resize(nc);
@@ -315,14 +324,19 @@ Error build_flat_mesh(const RawMesh &raw, const BCs &bcs, const Bands &bands, Fl
         if (m.cf_bound[k] < 0 && m.cf_nbr[k] < 0) return {-7, "a face is neither an interior face nor on a boundary in the BC table"};
     for (int k = 0; k < ncf; k++)
         if (m.cf_bound[k] >= 0) m.cf_nbr[k] = m.cf_nbr[k];  // boundary faces keep their neighbour for the face list
-    // periodic partners
+    // periodic partners: candidates are the boundaries whose type names this
+    // tag, in boundary order (the first nearest one wins)
+    std::unordered_map<int, std::vector<int>> naming;
+    for (int j = 0; j < nbd; j++)
+        if (types[b_row[j]] < 0) naming[-types[b_row[j]]].push_back(j);
     for (int ib = 0; ib < nbd; ib++) {
         if (types[b_row[ib]] >= 0) continue;
         double best = 1000;
         int k0 = m.bs_cf[2 * ib];
         if (k0 < 0) return {-7, "periodic boundary without a cell"};
-        for (int j = 0; j < nbd; j++) {
-            if (tags[b_row[ib]] != -types[b_row[j]]) continue;
+        auto cand = naming.find(tags[b_row[ib]]);
+        if (cand == naming.end()) return {-7, "periodic boundary tag " + std::to_string(tags[b_row[ib]]) + " has no partner"};
+        for (int j : cand->second) {
             int k1 = m.bs_cf[2 * j];
             if (k1 < 0) continue;
             double d1 = dist3(m.cf_fx[k0], m.cf_fy[k0], m.cf_fz[k0], m.cf_fx[k1], m.cf_fy[k1], m.cf_fz[k1]);
@@ -474,9 +488,10 @@ Error build_flat_mesh(const RawMesh &raw, const BCs &bcs, const Bands &bands, Fl
 // the neighbour's correction as zero, which changes only the convergence
 // rate of the defect correction, not its fixed point.
 void build_schedule(const FlatMesh &m, const Angles &a, Schedule &s, int nthreads) {
-    const int nc = m.nc, nd = a.nd;
+    const int nc = m.nc, nd = a.nd, ncomp = std::max(1, m.ncomp());
+    s.ncomp = ncomp;
     s.lvl_cells.assign((size_t)nd * nc, 0);
-    std::vector<std::vector<int>> dir_ptr(nd);
+    std::vector<std::vector<int>> dir_ptr((size_t)nd * ncomp);
     std::vector<std::vector<uint8_t>> dir_lag(nd);
     std::vector<int> dir_lagged(nd, 0);
     auto work = [&](int d) {
@@ -545,16 +560,24 @@ void build_schedule(const FlatMesh &m, const Angles &a, Schedule &s, int nthread
             }
             frontier.swap(nxt);
         }
-        // group by level (stable within a level)
-        int nl = 0;
-        for (int c = 0; c < nc; c++) nl = std::max(nl, level[c] + 1);
-        std::vector<int> cnt(nl + 1, 0);
-        for (int c = 0; c < nc; c++) cnt[level[c] + 1]++;
-        for (int l = 0; l < nl; l++) cnt[l + 1] += cnt[l];
-        std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+        // group by component, then by level (stable within a level): the
+        // cells of component k take positions comp_ptr[k] .. comp_ptr[k+1]
         int *dst = &s.lvl_cells[(size_t)d * nc];
-        for (int c : order) dst[fill[level[c]]++] = c;
-        dir_ptr[d] = cnt;
+        std::vector<int> comp_of(nc);
+        for (int k = 0; k < ncomp; k++)
+            for (int c = m.comp_ptr[k]; c < m.comp_ptr[k + 1]; c++) comp_of[c] = k;
+        std::vector<std::vector<int>> fills(ncomp);
+        for (int k = 0; k < ncomp; k++) {
+            int nl = 0;
+            for (int c = m.comp_ptr[k]; c < m.comp_ptr[k + 1]; c++) nl = std::max(nl, level[c] + 1);
+            std::vector<int> cnt(nl + 1, 0);
+            for (int c = m.comp_ptr[k]; c < m.comp_ptr[k + 1]; c++) cnt[level[c] + 1]++;
+            cnt[0] = m.comp_ptr[k];
+            for (int l = 0; l < nl; l++) cnt[l + 1] += cnt[l];
+            fills[k].assign(cnt.begin(), cnt.end() - 1);
+            dir_ptr[(size_t)d * ncomp + k] = cnt;
+        }
+        for (int c : order) dst[fills[comp_of[c]][level[c]]++] = c;
         dir_lag[d] = lag;
         dir_lagged[d] = lagged;
     };
@@ -565,17 +588,17 @@ void build_schedule(const FlatMesh &m, const Angles &a, Schedule &s, int nthread
             for (int d = t; d < nd; d += nthreads) work(d);
         });
     for (auto &th : pool) th.join();
-    s.dir_lvl_off.assign(nd + 1, 0);
+    s.dir_lvl_off.assign((size_t)nd * ncomp + 1, 0);
     s.lvl_ptr.clear();
     s.max_levels = 0;
     s.lagged_faces = 0;
-    for (int d = 0; d < nd; d++) {
-        s.dir_lvl_off[d] = (int)s.lvl_ptr.size();
-        s.lvl_ptr.insert(s.lvl_ptr.end(), dir_ptr[d].begin(), dir_ptr[d].end());
-        s.max_levels = std::max(s.max_levels, (int)dir_ptr[d].size() - 1);
-        s.lagged_faces += dir_lagged[d];
+    for (size_t e = 0; e < (size_t)nd * ncomp; e++) {
+        s.dir_lvl_off[e] = (int)s.lvl_ptr.size();
+        s.lvl_ptr.insert(s.lvl_ptr.end(), dir_ptr[e].begin(), dir_ptr[e].end());
+        s.max_levels = std::max(s.max_levels, (int)dir_ptr[e].size() - 1);
     }
-    s.dir_lvl_off[nd] = (int)s.lvl_ptr.size();
+    for (int d = 0; d < nd; d++) s.lagged_faces += dir_lagged[d];
+    s.dir_lvl_off[(size_t)nd * ncomp] = (int)s.lvl_ptr.size();
     if (s.lagged_faces > 0) {
         s.lag.assign((size_t)nd * nc, 0);
         for (int d = 0; d < nd; d++) std::copy(dir_lag[d].begin(), dir_lag[d].end(), s.lag.begin() + (size_t)d * nc);
@@ -585,10 +608,10 @@ void build_schedule(const FlatMesh &m, const Angles &a, Schedule &s, int nthread
 
 Error build_sweep_plan(const FlatMesh &m, const Angles &a, const Schedule &s, int min_ring, int far_cap,
                        SweepPlan &out) {
-    const int nc = m.nc, nd = a.nd;
+    const int nc = m.nc, nd = a.nd, ncomp = s.ncomp;
     out = SweepPlan{};
-    for (int d = 0; d < nd; d++)
-        for (int k = s.dir_lvl_off[d]; k + 1 < s.dir_lvl_off[d + 1]; k++)
+    for (size_t e = 0; e < (size_t)nd * ncomp; e++)
+        for (int k = s.dir_lvl_off[e]; k + 1 < s.dir_lvl_off[e + 1]; k++)
             out.max_width = std::max(out.max_width, s.lvl_ptr[k + 1] - s.lvl_ptr[k]);
     int ring = 1;
     while (ring < std::max(min_ring, out.max_width)) ring *= 2;
@@ -606,14 +629,19 @@ Error build_sweep_plan(const FlatMesh &m, const Angles &a, const Schedule &s, in
     std::vector<std::string> dir_err(nd);
     auto work = [&](int d) {
         const int *lc = &s.lvl_cells[(size_t)d * nc];
-        const int *lp = &s.lvl_ptr[s.dir_lvl_off[d]];
-        const int nl = s.dir_lvl_off[d + 1] - s.dir_lvl_off[d] - 1;
-        std::vector<int> po(nc), lev(nc), last_read(nc, -1);
-        for (int l = 0; l < nl; l++)
-            for (int pos = lp[l]; pos < lp[l + 1]; pos++) {
-                po[lc[pos]] = pos;
-                lev[pos] = l;
-            }
+        // level (within its component) and level end of every position
+        std::vector<int> po(nc), lev(nc), lend(nc), last_read(nc, -1);
+        for (int k = 0; k < ncomp; k++) {
+            const size_t e = (size_t)d * ncomp + k;
+            const int *lp = &s.lvl_ptr[s.dir_lvl_off[e]];
+            const int nl = s.dir_lvl_off[e + 1] - s.dir_lvl_off[e] - 1;
+            for (int l = 0; l < nl; l++)
+                for (int pos = lp[l]; pos < lp[l + 1]; pos++) {
+                    po[lc[pos]] = pos;
+                    lev[pos] = l;
+                    lend[pos] = lp[l + 1];
+                }
+        }
         const size_t P0 = (size_t)d * nc;
         for (int pos = 0; pos < nc; pos++) {
             const size_t P = P0 + pos;
@@ -635,7 +663,7 @@ Error build_sweep_plan(const FlatMesh &m, const Angles &a, const Schedule &s, in
                     const int q = po[m.cf_nbr[k]];
                     out.np[4 * P + nin] = q;
                     out.a[4 * P + nin] = av;
-                    if (q < lp[lev[pos] + 1] - ring) {
+                    if (q < lend[pos] - ring) {
                         last_read[q] = std::max(last_read[q], lev[pos]);
                         dir_refs[d]++;
                     }
@@ -645,32 +673,41 @@ Error build_sweep_plan(const FlatMesh &m, const Angles &a, const Schedule &s, in
             out.sig[P] = sig;
             out.nin[P] = nin;
         }
-        // far slots: a slot is taken at its writer's level and free again
-        // from the level after its last reader's
-        std::vector<int> slot(nc, -1), freel;
-        std::vector<std::vector<int>> release(nl + 1);
-        int nslots = 0;
-        for (int l = 0; l < nl; l++) {
-            for (int sl : release[l]) freel.push_back(sl);
-            for (int pos = lp[l]; pos < lp[l + 1]; pos++) {
-                if (last_read[pos] < 0) continue;
-                int sl;
-                if (!freel.empty()) {
-                    sl = freel.back();
-                    freel.pop_back();
-                } else {
-                    sl = nslots++;
+        // far slots, per component (one sweep CTA walks one component): a
+        // slot is taken at its writer's level and free again from the level
+        // after its last reader's
+        std::vector<int> slot(nc, -1);
+        int maxslots = 0;
+        for (int k = 0; k < ncomp; k++) {
+            const size_t e = (size_t)d * ncomp + k;
+            const int *lp = &s.lvl_ptr[s.dir_lvl_off[e]];
+            const int nl = s.dir_lvl_off[e + 1] - s.dir_lvl_off[e] - 1;
+            std::vector<int> freel;
+            std::vector<std::vector<int>> release(nl + 1);
+            int nslots = 0;
+            for (int l = 0; l < nl; l++) {
+                for (int sl : release[l]) freel.push_back(sl);
+                for (int pos = lp[l]; pos < lp[l + 1]; pos++) {
+                    if (last_read[pos] < 0) continue;
+                    int sl;
+                    if (!freel.empty()) {
+                        sl = freel.back();
+                        freel.pop_back();
+                    } else {
+                        sl = nslots++;
+                    }
+                    slot[pos] = sl;
+                    release[last_read[pos] + 1].push_back(sl);
                 }
-                slot[pos] = sl;
-                release[last_read[pos] + 1].push_back(sl);
             }
+            maxslots = std::max(maxslots, nslots);
         }
-        dir_slots[d] = nslots;
+        dir_slots[d] = maxslots;
         for (int pos = 0; pos < nc; pos++) {
             const size_t P = P0 + pos;
             for (int jj = 0; jj < 4; jj++) {
                 const int q = out.np[4 * P + jj];
-                np_far[4 * P + jj] = (jj < out.nin[P] && q < lp[lev[pos] + 1] - ring) ? -(1 + slot[q]) : q;
+                np_far[4 * P + jj] = (jj < out.nin[P] && q < lend[pos] - ring) ? -(1 + slot[q]) : q;
             }
         }
         for (int pos = 0; pos < nc; pos++) out.far_w[P0 + pos] = slot[pos];
@@ -693,6 +730,50 @@ Error build_sweep_plan(const FlatMesh &m, const Angles &a, const Schedule &s, in
         out.np.swap(np_far);
     else
         std::fill(out.far_w.begin(), out.far_w.end(), -1);
+    return {0, ""};
+}
+
+Error make_union(const std::vector<RawMesh> &meshes, const std::vector<BCs> &bcs, RawMesh &out, BCs &out_bcs) {
+    const int n = (int)meshes.size();
+    if (n <= 0 || (int)bcs.size() != n) return {-1, "a batch needs at least one geometry and one BC table each"};
+    int span = 1;  // tags of geometry k are shifted by k * span
+    for (int k = 0; k < n; k++) {
+        for (int t : meshes[k].btag) span = std::max(span, t + 1);
+        for (int t : bcs[k].tag) span = std::max(span, t + 1);
+        for (int t : bcs[k].type)
+            if (t < 0) span = std::max(span, -t + 1);
+    }
+    out = RawMesh();
+    out_bcs = BCs();
+    out.dim = meshes[0].dim;
+    out.Lx = meshes[0].Lx;
+    out.Ly = meshes[0].Ly;
+    out.Lz = meshes[0].Lz;
+    out.cptr.assign(1, 0);
+    out.bptr.assign(1, 0);
+    out.comp_ptr.assign(1, 0);
+    int node0 = 0;
+    for (int k = 0; k < n; k++) {
+        const RawMesh &m = meshes[k];
+        if (m.dim != out.dim) return {-1, "the geometries of a batch must have one dimension"};
+        if (m.Lx != out.Lx) return {-1, "the geometries of a batch must share ScaleX (it scales the LSQ stencils)"};
+        if ((long long)out.nc() + m.nc() > 0x7fffffff / 2) return {-1, "batch too large"};
+        out.xyz.insert(out.xyz.end(), m.xyz.begin(), m.xyz.end());
+        for (int c = 0; c < m.nc(); c++) out.cptr.push_back(out.cptr.back() + (m.cptr[c + 1] - m.cptr[c]));
+        for (int v : m.cverts) out.cverts.push_back(v + node0);
+        out.creg.insert(out.creg.end(), m.creg.begin(), m.creg.end());
+        for (int e = 0; e < m.nbe(); e++) out.bptr.push_back(out.bptr.back() + (m.bptr[e + 1] - m.bptr[e]));
+        for (int v : m.bverts) out.bverts.push_back(v + node0);
+        for (int t : m.btag) out.btag.push_back(t + k * span);
+        for (size_t i = 0; i < bcs[k].tag.size(); i++) {
+            const int ty = bcs[k].type[i];
+            out_bcs.tag.push_back(bcs[k].tag[i] + k * span);
+            out_bcs.type.push_back(ty < 0 ? -(-ty + k * span) : ty);
+            out_bcs.value.push_back(bcs[k].value[i]);
+        }
+        out.comp_ptr.push_back(out.nc());
+        node0 += m.nn();
+    }
     return {0, ""};
 }
 

@@ -454,7 +454,7 @@ __device__ __forceinline__ double sweep_div(double x, double y) { return x / y; 
 // rvec: the band chunk of a residual row is copied in 16-byte pieces (its
 // byte size, offset and the row pitch are multiples of 16).
 template <typename S, int LOOK, int LCAP>
-__global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int nbc, int ring_n, int nfar, int rvec,
+__global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int ncomp, int nbc, int ring_n, int nfar, int rvec,
                                                const int *__restrict__ lvl_ptr, const int *__restrict__ dir_lvl_off,
                                                const SweepRec<S> *__restrict__ rec, const int *__restrict__ lvl_cells,
                                                const double *__restrict__ kbv, const S *__restrict__ Rlo,
@@ -467,9 +467,10 @@ __global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int nbc, int ring
     int *lp = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(far) +
                                       (((size_t)nfar * nbc * sizeof(S) + 15) & ~(size_t)15));
     const int nchunks = (nb + nbc - 1) / nbc;
-    const int d = blockIdx.x / nchunks, chunk = blockIdx.x % nchunks;
+    const int ent = blockIdx.x / nchunks, chunk = blockIdx.x % nchunks;  // (direction, component), band chunk
+    const int d = ent / ncomp;
     const int b0 = chunk * nbc, nbl = min(nbc, nb - b0);
-    const int nlev = dir_lvl_off[d + 1] - dir_lvl_off[d] - 1;
+    const int nlev = dir_lvl_off[ent + 1] - dir_lvl_off[ent] - 1;
     const size_t base = (size_t)d * nc;
     const int tid = threadIdx.x, bd = blockDim.x;
     const int lb = tid % nbc, lc0 = tid / nbc, cpp = bd / nbc;  // band of this thread, cell offset, cells per pass
@@ -481,7 +482,7 @@ __global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int nbc, int ring
     const int unit = rvec ? 16 : (int)sizeof(S);
     const int K = nbl * (int)sizeof(S) / unit;
     const int rk = tid % K, rc0 = tid / K, rstep = bd / K;
-    for (int i = tid; i <= nlev; i += bd) lp[i] = lvl_ptr[dir_lvl_off[d] + i];
+    for (int i = tid; i <= nlev; i += bd) lp[i] = lvl_ptr[dir_lvl_off[ent] + i];
     __syncthreads();
     auto issue = [&](int l) {
         if (l >= nlev) return;
@@ -993,10 +994,15 @@ __device__ __forceinline__ void atomic_max_nonneg(double *addr, double v) {
 }
 
 // margins: out = {max|T|, sum|T-Told|, max|q|, sum||q|-|qold||, sum (T1-T)^2}
-__global__ void k_margins(int n, const double *__restrict__ T, const double *__restrict__ Told,
-                          const double *__restrict__ q, const double *__restrict__ qold, double *out) {
+// per component (blockIdx.y; cells comp_ptr[y] .. comp_ptr[y+1]): max |T|,
+// sum |T - Told|, max |q|, sum ||q| - |qold|| into out[4 y .. 4 y + 3]
+__global__ void k_margins(const int *__restrict__ comp_ptr, const double *__restrict__ T,
+                          const double *__restrict__ Told, const double *__restrict__ q,
+                          const double *__restrict__ qold, double *out) {
     double tmax = 0, s1 = 0, hmax = 0, s2 = 0;
-    for (size_t i = gtid(); i < (size_t)n; i += gstride()) {
+    out += 4 * blockIdx.y;
+    const size_t c0 = comp_ptr[blockIdx.y], c1 = comp_ptr[blockIdx.y + 1];
+    for (size_t i = c0 + gtid(); i < c1; i += gstride()) {
         tmax = fmax(tmax, fabs(T[i]));
         s1 += sqrt(pow(T[i] - Told[i], 2));
         const double h = sqrt(pow(q[3 * i], 2) + pow(q[3 * i + 1], 2) + pow(q[3 * i + 2], 2));
@@ -1031,6 +1037,30 @@ __global__ void k_margins(int n, const double *__restrict__ T, const double *__r
         atomic_max_nonneg(&out[2], hmax);
         atomicAdd(&out[3], s2);
     }
+}
+
+// per component (blockIdx.y): sum (a - b)^2 into out[y]
+__global__ void k_sqdiff_comp(const int *__restrict__ comp_ptr, const double *__restrict__ a,
+                              const double *__restrict__ b, double *out) {
+    double s = 0;
+    const size_t c0 = comp_ptr[blockIdx.y], c1 = comp_ptr[blockIdx.y + 1];
+    for (size_t i = c0 + gtid(); i < c1; i += gstride()) s += pow(a[i] - b[i], 2);
+    __shared__ double sh[32];
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) s += sh[w];
+        atomicAdd(&out[blockIdx.y], s);
+    }
+}
+
+// cells of the components flagged done get their value before the step back
+__global__ void k_restore_comp(const int *__restrict__ comp_ptr, const int *__restrict__ done,
+                               const double *__restrict__ before, double *__restrict__ T) {
+    if (!done[blockIdx.y]) return;
+    const size_t c0 = comp_ptr[blockIdx.y], c1 = comp_ptr[blockIdx.y + 1];
+    for (size_t i = c0 + gtid(); i < c1; i += gstride()) T[i] = before[i];
 }
 
 __global__ void k_sqdiff(int n, const double *__restrict__ a, const double *__restrict__ b, double *out) {
@@ -1454,6 +1484,7 @@ Solver::~Solver() {
     if (cfg.stream) cudaStreamSynchronize(cfg.stream);
     for (void *p : allocs_) cudaFree(p);
     if (h_pinned_) cudaFreeHost(h_pinned_);
+    if (h_comp_) cudaFreeHost(h_comp_);
     for (auto &e : ev_)
         if (e) cudaEventDestroy(e);
     if (cfg.own_stream && cfg.stream) cudaStreamDestroy(cfg.stream);
@@ -1877,7 +1908,10 @@ Error Solver::alloc_all() {
     TV_ = (double *)A(nslot * 8);
     rhs_ = (double *)A(nc * 8);
     T1_ = (double *)A(nc * 8);
-    red_ = (double *)A(8 * 8);
+    ncomp_ = std::max(1, mesh.ncomp());
+    red_ = (double *)A(std::max<size_t>(8, 4 * (size_t)ncomp_ + 4) * 8);
+    comp_ptr_d_ = (int *)A((size_t)(ncomp_ + 1) * sizeof(int));
+    comp_done_d_ = (int *)A((size_t)ncomp_ * sizeof(int));
     cg_r_ = (double *)A(nc * 8);
     cg_z_ = (double *)A(nc * 8);
     cg_p_ = (double *)A(nc * 8);
@@ -1888,7 +1922,15 @@ Error Solver::alloc_all() {
             return {-6, "device allocation failed (" + std::to_string(ne * S * (3 + mesh.dim) / 1048576) +
                             " MiB of band state)"};
     if (cudaMallocHost((void **)&h_pinned_, 16 * sizeof(double)) != cudaSuccess) return {-6, "pinned allocation failed"};
+    if (cudaMallocHost((void **)&h_comp_, 4 * (size_t)ncomp_ * sizeof(double)) != cudaSuccess)
+        return {-6, "pinned allocation failed"};
+    if (!red_ || !comp_ptr_d_ || !comp_done_d_) return {-6, "device allocation failed (reductions)"};
     cudaStream_t s = cfg.stream;
+    {
+        std::vector<int> cp = mesh.comp_ptr.empty() ? std::vector<int>{0, (int)nc} : mesh.comp_ptr;
+        CUDA_TRY(cudaMemcpyAsync(comp_ptr_d_, cp.data(), cp.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+    }
     CUDA_TRY(cudaMemsetAsync(eb_, 0, nd * nbs * nb * 8, s));
     CUDA_TRY(cudaMemsetAsync(Tbase_, 0, nc * 8, s));
     CUDA_TRY(cudaMemsetAsync(gTb_, 0, nc * 3 * 8, s));
@@ -1943,6 +1985,36 @@ Error Solver::set_initial(const double *T0, const double *q0, const double *bth)
 // called from SolutionAll::_Fourier_Solver, Solution.cpp:236-255): Picard on
 // the non-orthogonal correction until the mean squared change is <= 1e-5,
 // starting from the current initial temperature (Tref for a deck).
+// One Picard step of a batch, after the solve: every geometry follows its
+// own loop. Geometries already done (their test met in an earlier step) get
+// their temperature before this step back; the others are tested with
+// their own mean squared change against `limit` and marked done when they
+// meet it. internal = the largest mean change of the geometries still
+// stepping before this step (0 when none is left).
+Error Solver::picard_components(double limit, std::vector<char> &done, double &internal) {
+    cudaStream_t s = cfg.stream;
+    const int nc = mesh.nc;
+    const int blocks = std::max(1, std::min(148, (nc / ncomp_ + kThreads - 1) / kThreads));
+    GL(K_COPY, k_restore_comp<<<dim3(blocks, ncomp_), kThreads, 0, s>>>(comp_ptr_d_, comp_done_d_, T1_, T_));
+    CUDA_TRY(cudaMemsetAsync(red_, 0, 8 * (size_t)ncomp_, s));
+    GL(K_REDUCE, k_sqdiff_comp<<<dim3(blocks, ncomp_), kThreads, 0, s>>>(comp_ptr_d_, T1_, T_, red_));
+    CUDA_TRY(cudaMemcpyAsync(h_comp_, red_, 8 * (size_t)ncomp_, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    internal = 0;
+    std::vector<int> flags(ncomp_);
+    for (int k = 0; k < ncomp_; k++) {
+        if (!done[k]) {
+            const double ik = h_comp_[k] / (double)(mesh.comp_ptr[k + 1] - mesh.comp_ptr[k]);
+            internal = std::isnan(ik) ? ik : std::max(internal, ik);
+            if (ik <= limit) done[k] = 1;
+        }
+        flags[k] = done[k];
+    }
+    CUDA_TRY(cudaMemcpyAsync(comp_done_d_, flags.data(), sizeof(int) * ncomp_, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return {0, ""};
+}
+
 Error Solver::fourier_initial() {
     if (!initialised) return {-1, "solver not initialised"};
     if (fourier_singular_) return {-8, "Fourier pre-solve: no isothermal or temperature-jump boundary (singular system)"};
@@ -1953,6 +2025,8 @@ Error Solver::fourier_initial() {
     double internal = 1000;
     long long it = 0;
     int steps = 0;
+    std::vector<char> done(ncomp_, 0);
+    if (ncomp_ > 1) CUDA_TRY(cudaMemsetAsync(comp_done_d_, 0, sizeof(int) * ncomp_, s));
     while (internal > 1e-5) {
         GL(K_COPY, k_copy<<<gC, kThreads, 0, s>>>(T_, T1_, nc));
         GL(K_TINTERP, k_tinterp<<<gN, kThreads, 0, s>>>(dm_, T_, TV_));
@@ -1963,6 +2037,10 @@ Error Solver::fourier_initial() {
                            cg_r_, cg_z_, cg_p_, cg_Ap_, T1_, &sq);
         if (e.code) return e;
         internal = sq / nc;
+        if (ncomp_ > 1) {
+            Error pe = picard_components(1e-5, done, internal);
+            if (pe.code) return pe;
+        }
         if (cfg.verbose) printf("iterations residual: %.17g\n", internal);
         if (!std::isfinite(internal) || ++steps >= 1000) return {-4, "Fourier pre-solve does not converge"};
     }
@@ -2268,6 +2346,8 @@ Error Solver::solve_t(SolveStats &st) {
     EView<S, DIM> ev{eps, g, Tbase_, gTb_, nb, nc};
     const int gE = grid_for(ne), gB = grid_for((size_t)nd * nbs * nb), gE8 = grid_for(ne / 4);
     const int gC = (nc + kThreads - 1) / kThreads, gN = (nslot + kThreads - 1) / kThreads;
+    // blocks per geometry of the per-geometry reductions
+    const int comp_blocks = std::max(1, std::min(148, (nc / ncomp_ + kThreads - 1) / kThreads));
     constexpr int LOOK = 4, LCAP = 128;
     // sweep: nb split into equal chunks of at most sweep_bands bands
     // (default 8 in FP32, 4 in FP64: the fastest on the 17,939-cell 40-band
@@ -2288,7 +2368,7 @@ Error Solver::solve_t(SolveStats &st) {
         if (wsmem <= 220 * 1024 || wnbc == 1) break;
     }
     if (wsmem > 220 * 1024) return {-8, "sweep level too wide for the shared-memory correction ring"};
-    const int wide_threads = std::max(wnbc, (256 / wnbc) * wnbc), wide_blocks = nd * wchunks;
+    const int wide_threads = std::max(wnbc, (256 / wnbc) * wnbc), wide_blocks = nd * ncomp_ * wchunks;
     const int wlast = nb - (wchunks - 1) * wnbc;  // bands of the last chunk
     const int wrvec = ((wnbc * sizeof(S)) % 16 == 0 && (nb * sizeof(S)) % 16 == 0 && (wlast * sizeof(S)) % 16 == 0) ? 1 : 0;
     CUDA_TRY(cudaFuncSetAttribute(k_sweep<S, LOOK, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsmem));
@@ -2337,7 +2417,7 @@ Error Solver::solve_t(SolveStats &st) {
             GL(K_RESIDUAL, (k_residual<S, DIM><<<gE, kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, pos_of_, R)));
         }
         GL(K_SWEEP, (k_sweep<S, LOOK, LCAP><<<wide_blocks, wide_threads, wsmem, s>>>(
-                        nb, nc, wnbc, wring, far_slots_, wrvec, lvl_ptr_, dir_lvl_off_, (const SweepRec<S> *)rec_, lvl_cells_, kb_,
+                        nb, nc, ncomp_, wnbc, wring, far_slots_, wrvec, lvl_ptr_, dir_lvl_off_, (const SweepRec<S> *)rec_, lvl_cells_, kb_,
                         R, (S *)corr_)));
         GL(K_MOMENTS, (k_moments<S><<<gM, cpb * nb, msmem, s>>>(dm_, dp_, cpb, eps, (const S *)corr_, Tbase_, wtab_, Tlat_, E_,
                                                                 q_, Tband_, Th_, Q_, 1)));
@@ -2353,6 +2433,9 @@ Error Solver::solve_t(SolveStats &st) {
         GL(K_COPY, k_copy<<<gC, kThreads, 0, s>>>(Tlat_, T_, nc));
         double internal = 1000, prev_internal = 0;
         int inner = 0, inner_inc = 0;
+        // per geometry of a batch: Picard done (its own test met in an earlier step)
+        std::vector<char> done(ncomp_, 0);
+        if (ncomp_ > 1) CUDA_TRY(cudaMemsetAsync(comp_done_d_, 0, sizeof(int) * ncomp_, s));
         while (internal > 1e-6) {
             GL(K_COPY, k_copy<<<gC, kThreads, 0, s>>>(T_, T1_, nc));
             GL(K_TINTERP, k_tinterp<<<gN, kThreads, 0, s>>>(dm_, T_, TV_));
@@ -2383,6 +2466,10 @@ Error Solver::solve_t(SolveStats &st) {
             }
             if (e.code) return e;
             internal = sq / nc;
+            if (ncomp_ > 1) {
+                Error pe = picard_components(1e-6, done, internal);
+                if (pe.code) return pe;
+            }
             inner++;
             if (inner > 1 && internal > prev_internal) inner_inc++;
             prev_internal = internal;
@@ -2393,9 +2480,9 @@ Error Solver::solve_t(SolveStats &st) {
         st.inner_iterations = inner;
         CUDA_TRY(cudaEventRecord(ev_[2], s));
         // margins
-        CUDA_TRY(cudaMemsetAsync(red_, 0, 4 * 8, s));
-        GL(K_REDUCE, k_margins<<<std::min(gC, 148), kThreads, 0, s>>>(nc, T_, Told_, q_, qold_, red_));
-        CUDA_TRY(cudaMemcpyAsync(h_pinned_, red_, 4 * 8, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaMemsetAsync(red_, 0, 4 * 8 * (size_t)ncomp_, s));
+        GL(K_REDUCE, k_margins<<<dim3(comp_blocks, ncomp_), kThreads, 0, s>>>(comp_ptr_d_, T_, Told_, q_, qold_, red_));
+        CUDA_TRY(cudaMemcpyAsync(h_comp_, red_, 4 * 8 * (size_t)ncomp_, cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaEventRecord(ev_[3], s));
         CUDA_TRY(cudaStreamSynchronize(s));
             prof_collect(st);
@@ -2406,8 +2493,16 @@ Error Solver::solve_t(SolveStats &st) {
         ms_transport += a;
         ms_macro += b2;
         ms_total += c2;
-        const double err = h_pinned_[1] / nc / h_pinned_[0];
-        const double errq = h_pinned_[3] / nc / h_pinned_[2];
+        // L1-relative margins (_get_magin_check_error :2565-2611), the
+        // largest over the independent geometries of a batch
+        double err = 0, errq = 0;
+        for (int k = 0; k < ncomp_; k++) {
+            const double nck = ncomp_ == 1 ? (double)nc : (double)(mesh.comp_ptr[k + 1] - mesh.comp_ptr[k]);
+            const double *r = h_comp_ + 4 * k;
+            const double ek = r[1] / nck / r[0], eqk = r[3] / nck / r[2];
+            err = k == 0 ? ek : (std::isnan(ek) ? ek : std::max(err, ek));
+            errq = k == 0 ? eqk : (std::isnan(eqk) ? eqk : std::max(errq, eqk));
+        }
         if (cfg.verbose)
             printf("Iteration #%d\t Margin per band per cell: Temperature:%.6g Heat Flux:%.6g\n", nt, err, errq);
         if ((err > errOld && errq > errOldq) || std::isnan(err) || std::isnan(errq) || std::isinf(err) || std::isinf(errq))
@@ -2518,6 +2613,7 @@ Error Solver::fourier_initial_noalloc() {
     if (!initialised) return {-1, "solver not initialised"};
     if (!have_initial_) return {-1, "set an initial temperature first"};
     if (fourier_singular_) return {-8, "Fourier pre-solve: no isothermal or temperature-jump boundary (singular system)"};
+    if (ncomp_ > 1) return {-8, "the allocation-free Fourier pre-solve serves single-geometry handles"};
     const int nc = mesh.nc, nslot = mesh.nn * mesh.nmat;
     if (nc > kNoAllocMaxCells || nslot > kNoAllocMaxCells)
         return {-1, "the allocation-free Fourier pre-solve holds at most " + std::to_string(kNoAllocMaxCells) +

@@ -157,6 +157,13 @@ private:
     double *K_val_ = nullptr, *K_dinv_ = nullptr;
     double *cg_r_ = nullptr, *cg_z_ = nullptr, *cg_p_ = nullptr, *cg_Ap_ = nullptr, *cg_scal_ = nullptr;
     double *h_pinned_ = nullptr;
+    // independent geometries of a batched solve (1 otherwise): cell ranges on
+    // the device, and pinned per-geometry reduction results
+    int ncomp_ = 1;
+    int *comp_ptr_d_ = nullptr;
+    int *comp_done_d_ = nullptr;  // per geometry: its Picard loop is done
+    Error picard_components(double limit, std::vector<char> &done, double &internal);
+    double *h_comp_ = nullptr;
     bool have_initial_ = false;
     bool started_ = false;
     int coop_blocks_ = 0;

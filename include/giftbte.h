@@ -191,6 +191,25 @@ void gbte_default_options(gbte_options *opt);
 int gbte_create(const gbte_mesh_view *mesh, const gbte_band_table *bands, const gbte_bc_table *bcs,
                 const gbte_angle_spec *angles, const gbte_options *opt, gbte_handle **out);
 
+/* Batched solve of `num` independent geometries (no counterpart in the
+ * reference, which solves one geometry per run): one handle over their
+ * disjoint union, so every kernel launch of the outer iteration serves all
+ * geometries at once (each sweep CTA walks one geometry's levels of one
+ * direction). All geometries share the band table, the angular quadrature,
+ * ScaleX and the options; meshes[k] and bcs[k] describe geometry k with its
+ * own boundary tags. The fields of the handle (gbte_set_initial,
+ * gbte_get_fields, options.cell_heat) are the geometries' cell arrays
+ * concatenated in order; gbte_batch_geometries gives the offsets. The outer
+ * iteration stops when every geometry's own margins are below the limits,
+ * and the macro Picard loop when every geometry's own change is. */
+int gbte_batch_create(int num, const gbte_mesh_view *meshes, const gbte_band_table *bands,
+                      const gbte_bc_table *bcs, const gbte_angle_spec *angles, const gbte_options *opt,
+                      gbte_handle **out);
+
+/* Number of geometries of a handle (1 for gbte_create) and, when
+ * cell_offsets is not NULL, their cell ranges [num + 1]. */
+int gbte_batch_geometries(gbte_handle *h, int *num, int *cell_offsets);
+
 /* Reads <dir>/input/{CONTROL,GEOMETRY,PHONON} and the files they name
  * (relative paths resolved against <dir>, like the reference's CWD).
  * Options from CONTROL (Order, margins, MaxNumIter) override *opt. */

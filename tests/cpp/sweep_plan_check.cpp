@@ -10,6 +10,8 @@
 //           exactly as the device sweep does (np >= lo: ring, np < 0: far
 //           slot), each level reading all its operands before any of its
 //           cells writes (the device's level-parallel order).
+// With a copies argument > 1 the check runs on a batch of that many copies
+// of the deck (disjoint union, one level list per copy and direction).
 // Prints "far_refs <n> far_slots <n> ring <n> max_abs_diff <x>" and exits 1
 // if the sweeps differ or a far reference found neither ring nor slot.
 #include <cmath>
@@ -23,7 +25,7 @@
 
 int main(int argc, char **argv) {
     if (argc < 3) {
-        std::fprintf(stderr, "usage: %s deck_dir min_ring\n", argv[0]);
+        std::fprintf(stderr, "usage: %s deck_dir min_ring [perturb|plain] [copies]\n", argv[0]);
         return 2;
     }
     gbte::Deck deck;
@@ -35,8 +37,18 @@ int main(int argc, char **argv) {
     gbte::Angles ang;
     e = gbte::make_angles(deck.angle_method, deck.n_theta, deck.n_phi, deck.bands.material_dim, ang);
     if (e.code) return std::fprintf(stderr, "angles: %s\n", e.msg.c_str()), 2;
+    // optional: a batch of `copies` copies of the deck (disjoint union)
+    const int copies = argc > 4 ? std::atoi(argv[4]) : 1;
+    gbte::RawMesh raw = deck.mesh;
+    gbte::BCs bcs = deck.bcs;
+    if (copies > 1) {
+        std::vector<gbte::RawMesh> ms(copies, deck.mesh);
+        std::vector<gbte::BCs> bs(copies, deck.bcs);
+        e = gbte::make_union(ms, bs, raw, bcs);
+        if (e.code) return std::fprintf(stderr, "union: %s\n", e.msg.c_str()), 2;
+    }
     gbte::FlatMesh fm;
-    e = gbte::build_flat_mesh(deck.mesh, deck.bcs, deck.bands, fm);
+    e = gbte::build_flat_mesh(raw, bcs, deck.bands, fm);
     if (e.code) return std::fprintf(stderr, "mesh: %s\n", e.msg.c_str()), 2;
     gbte::Schedule sch;
     gbte::build_schedule(fm, ang, sch, 4);
@@ -44,6 +56,7 @@ int main(int argc, char **argv) {
     e = gbte::build_sweep_plan(fm, ang, sch, std::atoi(argv[2]), 1 << 20, sp);
     if (e.code) return std::fprintf(stderr, "plan: %s\n", e.msg.c_str()), 2;
     if (!sp.far_enabled) return std::fprintf(stderr, "far slots not enabled\n"), 1;
+    if (fm.ncomp() != copies || sch.ncomp != copies) return std::fprintf(stderr, "components lost\n"), 1;
     if (argc > 3 && std::string(argv[3]) == "perturb" && sp.far_slots > 1) {
         // plant one wrong far slot in the plan (the check must then fail)
         for (size_t k = 0; k < sp.np.size(); k++)
@@ -58,9 +71,10 @@ int main(int argc, char **argv) {
     double maxdiff = 0;
     bool bad = false;
     const double kb = 0.7;
-    for (int d = 0; d < nd; d++) {
-        const int *lp = &sch.lvl_ptr[sch.dir_lvl_off[d]];
-        const int nl = sch.dir_lvl_off[d + 1] - sch.dir_lvl_off[d] - 1;
+    for (int e = 0; e < nd * sch.ncomp; e++) {
+        const int d = e / sch.ncomp;
+        const int *lp = &sch.lvl_ptr[sch.dir_lvl_off[e]];
+        const int nl = sch.dir_lvl_off[e + 1] - sch.dir_lvl_off[e] - 1;
         const size_t P0 = (size_t)d * nc;
         std::vector<double> R(nc), direct(nc), ringv(ring, NAN), far(std::max(1, sp.far_slots), NAN), lvl(nc);
         for (int i = 0; i < nc; i++) R[i] = U(rng);

@@ -55,6 +55,17 @@ def test_ring_and_far_slots_match_direct_sweep(checker, tmp_path, name, min_ring
     assert ring & (ring - 1) == 0
 
 
+@pytest.mark.parametrize("name", ["config2_4bands", "periodic_jitter"])
+def test_batch_of_copies_matches_direct_sweep(checker, tmp_path, name):
+    # three copies as one batched problem: per-copy levels, ring and far
+    # slots, tags remapped per copy (periodic partners stay in their copy)
+    _decks()[name].write(str(tmp_path))
+    r = subprocess.run([checker, str(tmp_path), "1", "plain", "3"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    f = dict(zip(r.stdout.split()[0::2], r.stdout.split()[1::2]))
+    assert float(f["max_abs_diff"]) == 0.0
+
+
 def test_planted_wrong_slot_is_caught(checker, tmp_path):
     d = decks.config2_deck(h_nm=3.0, n_bands=4, n_phi=16, seed=0)
     d.write(str(tmp_path))
