@@ -421,6 +421,8 @@ int gbte_solve(gbte_handle *h, gbte_stats *st) {
             st->lagged_faces = h->solver.sched.lagged_faces;
             st->inner_iterations = s.inner_iterations;
             st->kernel_launches = s.launches;
+            const int fixed = h->solver.cfg.sweep_bands;
+            st->sweep_bands = (fixed >= 1 && fixed <= 32) ? fixed : h->solver.tuned_sweep_bands_;
             for (int k = 0; k < GBTE_NUM_KERNELS && k < gbte::K_NUM; k++) {
                 st->kernel_ms[k] = s.kernel_ms[k];
                 st->kernel_count[k] = s.kernel_count[k];

@@ -2349,29 +2349,48 @@ Error Solver::solve_t(SolveStats &st) {
     // blocks per geometry of the per-geometry reductions
     const int comp_blocks = std::max(1, std::min(148, (nc / ncomp_ + kThreads - 1) / kThreads));
     constexpr int LOOK = 4, LCAP = 128;
-    // sweep: nb split into equal chunks of at most sweep_bands bands
-    // (default 8 in FP32, 4 in FP64: the fastest on the 17,939-cell 40-band
-    // cell); the ring holds at least one whole level (distinct slots for the
-    // cells written in one level) and 512 positions or more; more chunks
-    // when that does not fit in shared memory
-    const int wring = ring_;
-    const int wcap = (cfg.sweep_bands >= 1 && cfg.sweep_bands <= 32) ? cfg.sweep_bands : (sizeof(S) == 4 ? 8 : 4);
+    // sweep launch geometry for a cap on the bands per CTA: nb split into
+    // equal chunks of at most `cap` bands; the ring holds at least one whole
+    // level (distinct slots for the cells written in one level) and 512
+    // positions or more; more chunks when that does not fit in shared memory
+    struct SweepLaunch {
+        int nbc = 0, chunks = 0, threads = 0, blocks = 0, rvec = 0;
+        size_t smem = 0;
+    };
     const size_t wlp = ((size_t)(sched.max_levels + 1) * sizeof(int) + 15) & ~(size_t)15;
-    int wchunks = 0, wnbc = 0;
-    size_t wslot = 0, wsmem = 0;
-    for (int cap = wcap; cap >= 1; cap--) {
-        wnbc = (nb + (nb + cap - 1) / cap - 1) / ((nb + cap - 1) / cap);  // equal chunks of <= cap bands
-        wchunks = (nb + wnbc - 1) / wnbc;                                // every chunk non-empty
-        wslot = (size_t)LCAP * sizeof(SweepRec<S>) + (((size_t)LCAP * wnbc * sizeof(S) + 15) & ~(size_t)15);
-        wsmem = LOOK * wslot + (((size_t)wring * wnbc * sizeof(S) + 15) & ~(size_t)15) +
-                (((size_t)far_slots_ * wnbc * sizeof(S) + 15) & ~(size_t)15) + wlp;
-        if (wsmem <= 220 * 1024 || wnbc == 1) break;
-    }
-    if (wsmem > 220 * 1024) return {-8, "sweep level too wide for the shared-memory correction ring"};
-    const int wide_threads = std::max(wnbc, (256 / wnbc) * wnbc), wide_blocks = nd * ncomp_ * wchunks;
-    const int wlast = nb - (wchunks - 1) * wnbc;  // bands of the last chunk
-    const int wrvec = ((wnbc * sizeof(S)) % 16 == 0 && (nb * sizeof(S)) % 16 == 0 && (wlast * sizeof(S)) % 16 == 0) ? 1 : 0;
-    CUDA_TRY(cudaFuncSetAttribute(k_sweep<S, LOOK, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsmem));
+    auto sweep_launch = [&](int wcap, SweepLaunch &L) -> bool {
+        for (int cap = wcap; cap >= 1; cap--) {
+            L.nbc = (nb + (nb + cap - 1) / cap - 1) / ((nb + cap - 1) / cap);  // equal chunks of <= cap bands
+            L.chunks = (nb + L.nbc - 1) / L.nbc;                               // every chunk non-empty
+            const size_t slot = (size_t)LCAP * sizeof(SweepRec<S>) + (((size_t)LCAP * L.nbc * sizeof(S) + 15) & ~(size_t)15);
+            L.smem = LOOK * slot + (((size_t)ring_ * L.nbc * sizeof(S) + 15) & ~(size_t)15) +
+                     (((size_t)far_slots_ * L.nbc * sizeof(S) + 15) & ~(size_t)15) + wlp;
+            if (L.smem <= 220 * 1024 || L.nbc == 1) break;
+        }
+        if (L.smem > 220 * 1024) return false;
+        L.threads = std::max(L.nbc, (256 / L.nbc) * L.nbc);
+        L.blocks = nd * ncomp_ * L.chunks;
+        const int last = nb - (L.chunks - 1) * L.nbc;  // bands of the last chunk
+        L.rvec = ((L.nbc * sizeof(S)) % 16 == 0 && (nb * sizeof(S)) % 16 == 0 && (last * sizeof(S)) % 16 == 0) ? 1 : 0;
+        return true;
+    };
+    auto launch_sweep = [&](const SweepLaunch &L) -> cudaError_t {
+        cudaError_t e = cudaFuncSetAttribute(k_sweep<S, LOOK, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)L.smem);
+        if (e != cudaSuccess) return e;
+        k_sweep<S, LOOK, LCAP><<<L.blocks, L.threads, L.smem, s>>>(nb, nc, ncomp_, L.nbc, ring_, far_slots_, L.rvec,
+                                                                   lvl_ptr_, dir_lvl_off_, (const SweepRec<S> *)rec_,
+                                                                   lvl_cells_, kb_, R, (S *)corr_);
+        return cudaGetLastError();
+    };
+    // a fixed cap (options.sweep_bands), or the one the autotuner picked
+    // on this handle's first outer iteration (8 in FP32, 4 in FP64 before)
+    const bool tune = (cfg.sweep_bands < 1 || cfg.sweep_bands > 32) && tuned_sweep_bands_ == 0;
+    int wcap = (cfg.sweep_bands >= 1 && cfg.sweep_bands <= 32) ? cfg.sweep_bands
+               : tuned_sweep_bands_ > 0                         ? tuned_sweep_bands_
+                                                                : (sizeof(S) == 4 ? 8 : 4);
+    SweepLaunch SL;
+    if (!sweep_launch(wcap, SL)) return {-8, "sweep level too wide for the shared-memory correction ring"};
     const int cpb = std::max(1, 256 / nb);
     const int gM = (nc + cpb - 1) / cpb;
     const size_t msmem = ((size_t)nd * kWTab + (size_t)cpb * nb * kMomSlots) * sizeof(double);
@@ -2416,9 +2435,42 @@ Error Solver::solve_t(SolveStats &st) {
             GL(K_GRADIENT, (k_gradient<S, DIM><<<gE, kThreads, 0, s>>>(dm_, dp_, w, eps, g)));
             GL(K_RESIDUAL, (k_residual<S, DIM><<<gE, kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, pos_of_, R)));
         }
-        GL(K_SWEEP, (k_sweep<S, LOOK, LCAP><<<wide_blocks, wide_threads, wsmem, s>>>(
-                        nb, nc, ncomp_, wnbc, wring, far_slots_, wrvec, lvl_ptr_, dir_lvl_off_, (const SweepRec<S> *)rec_, lvl_cells_, kb_,
-                        R, (S *)corr_)));
+        if (tune && nt == 0) {
+            // autotuner: every cap on the bands per CTA that gives a distinct
+            // chunking, timed on this iteration's residual (the sweep only
+            // reads R and rewrites every correction, so the trials leave no
+            // trace; the band chunking does not change any arithmetic)
+            float best = 1e30f;
+            int best_cap = wcap, last_nbc = -1;
+            cudaEvent_t t0, t1;
+            CUDA_TRY(cudaEventCreate(&t0));
+            CUDA_TRY(cudaEventCreate(&t1));
+            for (int cap : {32, 16, 10, 8, 5, 4, 2, 1}) {
+                SweepLaunch L;
+                if (cap > nb || !sweep_launch(cap, L) || L.nbc == last_nbc) continue;
+                last_nbc = L.nbc;
+                float ms = 1e30f;
+                for (int rep = 0; rep < 2; rep++) {
+                    CUDA_TRY(cudaEventRecord(t0, s));
+                    CUDA_TRY(launch_sweep(L));
+                    CUDA_TRY(cudaEventRecord(t1, s));
+                    CUDA_TRY(cudaEventSynchronize(t1));
+                    float m = 0;
+                    CUDA_TRY(cudaEventElapsedTime(&m, t0, t1));
+                    ms = std::min(ms, m);
+                }
+                if (ms < best) {
+                    best = ms;
+                    best_cap = cap;
+                }
+            }
+            cudaEventDestroy(t0);
+            cudaEventDestroy(t1);
+            tuned_sweep_bands_ = best_cap;
+            wcap = best_cap;
+            sweep_launch(wcap, SL);
+        }
+        GL(K_SWEEP, CUDA_TRY(launch_sweep(SL)));
         GL(K_MOMENTS, (k_moments<S><<<gM, cpb * nb, msmem, s>>>(dm_, dp_, cpb, eps, (const S *)corr_, Tbase_, wtab_, Tlat_, E_,
                                                                 q_, Tband_, Th_, Q_, 1)));
         GL(K_BOUND_OUT, (k_bound_out<S, DIM><<<gB, kThreads, 0, s>>>(dm_, dp_, ev, eb_)));

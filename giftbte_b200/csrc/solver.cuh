@@ -100,6 +100,7 @@ public:
     SolverConfig cfg;
     bool initialised = false;
     std::string last_error;
+    int tuned_sweep_bands_ = 0;  // bands-per-CTA cap the sweep autotuner picked (0 = not yet)
 
 private:
     template <typename S, int DIM> Error solve_t(SolveStats &st);

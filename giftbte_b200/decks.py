@@ -626,41 +626,47 @@ def config3_deck(h_nm: float = 2.5, n_bands: int = 40, n_theta: int = 4, n_phi: 
     return Deck(mesh=mesh, bands=bands, bcs=bcs, scale=(1e-9, 1e-9, 1e-9), **kw)
 
 
-def porous_population(n: int, seed: int = 5, h_nm: Tuple[float, float] = (2.0, 6.0),
-                      r_nm: Tuple[float, float] = (40.0, 120.0), pores: Tuple[int, int] = (1, 3),
-                      n_bands: int = 20, n_phi: int = 8, side_nm: float = 300.0, **kw) -> List[Deck]:
-    """n independent periodic cells for a batched solve (seeded): each a
-    side_nm square with 1-3 circular diffuse pores of radius U(r_nm) placed
-    by rejection sampling (inside the cell, at least one mesh spacing from
-    the cell faces and from each other; a pore that does not fit after 200
-    tries is dropped), meshed with spacing U(h_nm); all cells share the
-    sine-dispersion table of n_bands bands, 4 * n_phi directions, x-periodic
-    with a 1 K jump, y-periodic (the config-2 boundary conditions)."""
-    rng = np.random.default_rng(seed)
+def porous_population_member(i: int, seed: int = 5, h_nm: Tuple[float, float] = (2.0, 6.0),
+                             r_nm: Tuple[float, float] = (40.0, 120.0), pores: Tuple[int, int] = (1, 3),
+                             n_bands: int = 20, n_phi: int = 8, side_nm: float = 300.0, **kw) -> Deck:
+    """Cell i of a seeded population of periodic cells for a batched solve
+    (its own random stream, seeded by (seed, i), so any member can be built
+    alone): a side_nm square with 1-3 circular diffuse pores of radius
+    U(r_nm) placed by rejection sampling (inside the cell, at least one mesh
+    spacing from the cell faces and from each other; a pore that does not
+    fit after 200 tries is dropped), meshed with spacing U(h_nm); the
+    sine-dispersion table of n_bands bands, 4 * n_phi directions,
+    x-periodic with a 1 K jump, y-periodic (the config-2 boundary
+    conditions)."""
+    rng = np.random.default_rng([seed, i])
     bands = sine_dispersion_bands(n_bands)
-    out = []
-    for i in range(n):
-        h = rng.uniform(*h_nm)
-        want = int(rng.integers(pores[0], pores[1] + 1))
-        placed: List[Tuple[float, float, float]] = []
-        for _ in range(want):
-            r = rng.uniform(*r_nm)
-            for _try in range(200):
-                cx, cy = rng.uniform(r + h, side_nm - r - h, size=2) if side_nm - 2 * (r + h) > 0 else (None, None)
-                if cx is None:
-                    break
-                if all(np.hypot(cx - px, cy - py) > r + pr + h for px, py, pr in placed):
-                    placed.append((cx, cy, r))
-                    break
-        if not placed:  # always at least one pore: the smallest radius, centred
-            placed.append((side_nm / 2, side_nm / 2, r_nm[0]))
-        mesh = porous_cell_mesh(h / side_nm, [(x / side_nm, y / side_nm, r / side_nm) for x, y, r in placed],
-                                seed=seed * 100003 + i)
-        bcs = [BC(1, -2, 1.0), BC(2, -1, 0.0), BC(3, -4, 0.0), BC(4, -3, 0.0)]
-        bcs += [BC(5 + k, 2, 0.0) for k in range(len(placed))]
-        kwd = dict(kw)
-        kwd.setdefault("n_phi", n_phi)
-        kwd.setdefault("angle_method", 1)
-        kwd.setdefault("tref", 0.0)
-        out.append(Deck(mesh=mesh, bands=bands, bcs=bcs, scale=(side_nm * 1e-9, side_nm * 1e-9), **kwd))
-    return out
+    h = rng.uniform(*h_nm)
+    want = int(rng.integers(pores[0], pores[1] + 1))
+    placed: List[Tuple[float, float, float]] = []
+    for _ in range(want):
+        r = rng.uniform(*r_nm)
+        if side_nm - 2 * (r + h) <= 0:
+            continue
+        for _try in range(200):
+            cx, cy = rng.uniform(r + h, side_nm - r - h, size=2)
+            if all(np.hypot(cx - px, cy - py) > r + pr + h for px, py, pr in placed):
+                placed.append((cx, cy, r))
+                break
+    if not placed:  # always at least one pore: the smallest radius, centred
+        placed.append((side_nm / 2, side_nm / 2, r_nm[0]))
+    mesh = porous_cell_mesh(h / side_nm, [(x / side_nm, y / side_nm, r / side_nm) for x, y, r in placed],
+                            seed=seed * 100003 + i)
+    bcs = [BC(1, -2, 1.0), BC(2, -1, 0.0), BC(3, -4, 0.0), BC(4, -3, 0.0)]
+    bcs += [BC(5 + k, 2, 0.0) for k in range(len(placed))]
+    kw.setdefault("n_phi", n_phi)
+    kw.setdefault("angle_method", 1)
+    kw.setdefault("tref", 0.0)
+    return Deck(mesh=mesh, bands=bands, bcs=bcs, scale=(side_nm * 1e-9, side_nm * 1e-9), **kw)
+
+
+def porous_population(n: int, seed: int = 5, **kw) -> List[Deck]:
+    """The first n members of the seeded population
+    (:func:`porous_population_member`): by default 300 nm cells, 1-3 pores
+    of radius U(40, 120) nm, mesh spacing U(2, 6) nm, 20 bands, 32
+    directions (the batched-solve workload)."""
+    return [porous_population_member(i, seed=seed, **kw) for i in range(n)]

@@ -151,6 +151,8 @@ typedef struct {
     long long kernel_launches;            /* kernels launched by this solve */
     double kernel_ms[GBTE_NUM_KERNELS];   /* per-kernel device time when options.profile = 1 */
     long long kernel_count[GBTE_NUM_KERNELS];
+    int sweep_bands;          /* bands-per-CTA cap of the sweep in use (options.sweep_bands, or
+                                 the autotuner's pick on the handle's first outer iteration) */
 } gbte_stats;
 
 /* Name of kernel slot i of gbte_stats.kernel_ms (NULL past the last one). */
