@@ -65,7 +65,7 @@ class Options(ctypes.Structure):
                 ("err_temp", ctypes.c_double), ("err_flux", ctypes.c_double), ("cell_heat", _c_dbl_p),
                 ("stream", ctypes.c_void_p), ("device", ctypes.c_int), ("verbose", ctypes.c_int),
                 ("macro_rtol", ctypes.c_double), ("profile", ctypes.c_int), ("sweep_bands", ctypes.c_int),
-                ("sweep_far_slots", ctypes.c_int)]
+                ("sweep_far_slots", ctypes.c_int), ("direction_batch", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -76,7 +76,7 @@ class Stats(ctypes.Structure):
                 ("num_cells", ctypes.c_int), ("max_levels", ctypes.c_int), ("lagged_faces", ctypes.c_int),
                 ("inner_iterations", ctypes.c_int), ("kernel_launches", ctypes.c_longlong),
                 ("kernel_ms", ctypes.c_double * 16), ("kernel_count", ctypes.c_longlong * 16),
-                ("sweep_bands", ctypes.c_int)]
+                ("sweep_bands", ctypes.c_int), ("direction_batch", ctypes.c_int)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("kernel_ms", "kernel_count")}

@@ -107,6 +107,7 @@ int create_common(const gbte::RawMesh &raw, const gbte::Bands &bands_in, const g
     cfg.profile = opt.profile;
     cfg.sweep_bands = opt.sweep_bands;
     cfg.sweep_far_slots = opt.sweep_far_slots;
+    cfg.direction_batch = opt.direction_batch;
     cfg.device = opt.device;
     cfg.stream = (cudaStream_t)opt.stream;
     if (opt.precision != GBTE_FP64 && opt.precision != GBTE_FP32_MIXED)
@@ -423,6 +424,7 @@ int gbte_solve(gbte_handle *h, gbte_stats *st) {
             st->kernel_launches = s.launches;
             const int fixed = h->solver.cfg.sweep_bands;
             st->sweep_bands = (fixed >= 1 && fixed <= 32) ? fixed : h->solver.tuned_sweep_bands_;
+            st->direction_batch = h->solver.ndb_;
             for (int k = 0; k < GBTE_NUM_KERNELS && k < gbte::K_NUM; k++) {
                 st->kernel_ms[k] = s.kernel_ms[k];
                 st->kernel_count[k] = s.kernel_count[k];

@@ -121,14 +121,14 @@ __global__ void k_cell_lsq_grad(DMesh m, const double *__restrict__ T, double *_
 // are broadcasts and the neighbour loads are coalesced over bands)
 template <typename S, int DIM>
 __global__ void __launch_bounds__(256) k_gradient(DMesh m, DPhys p, const S *__restrict__ w, const S *__restrict__ eps,
-                                                  S *__restrict__ g) {
+                                                  S *__restrict__ g, int d0, int ndb) {
     const int nb = p.nb, nc = m.nc;
-    const size_t total = (size_t)p.nd * nc * nb;
+    const size_t total = (size_t)ndb * nc * nb;
     for (size_t t = gtid(); t < total; t += gstride()) {
         const int b = (int)(t % nb);
-        const size_t dc = t / nb;
+        const size_t dc = t / nb;  // (batch direction, cell)
         const int c = (int)(dc % nc);
-        const S *ed = eps + (dc - c) * nb + b;
+        const S *ed = eps + ((size_t)d0 * nc + dc - c) * nb + b;
         const S ec = ed[(size_t)c * nb];
         S gx = 0, gy = 0, gz = 0;
         const int q1 = m.nbr_ptr[c + 1];
@@ -147,14 +147,15 @@ __global__ void __launch_bounds__(256) k_gradient(DMesh m, DPhys p, const S *__r
 
 template <typename S, int DIM>
 struct EView {
-    const S *eps, *g;
+    const S *eps, *g;  // eps: all directions; g: directions gd0 .. of the current batch
     const double *Tb, *gTb;
     int nb, nc;
+    int gd0;
     __device__ __forceinline__ double e(size_t d, int c, int b, double Cb) const {
         return Cb * Tb[c] + (double)eps[(d * nc + c) * nb + b];
     }
     __device__ __forceinline__ double gdot(size_t d, int c, int b, double Cb, double rx, double ry, double rz) const {
-        const S *gp = g + (d * nc + c) * DIM * nb + b;
+        const S *gp = g + ((d - gd0) * nc + c) * DIM * nb + b;
         double v = ((double)gp[0] + Cb * gTb[3 * c]) * rx + ((double)gp[nb] + Cb * gTb[3 * c + 1]) * ry;
         if (DIM == 3) v += ((double)gp[2 * nb] + Cb * gTb[3 * c + 2]) * rz;
         return v;
@@ -167,14 +168,15 @@ struct EView {
 template <typename S, int DIM>
 __global__ void __launch_bounds__(256) k_residual(DMesh m, DPhys p, EView<S, DIM> ev, const double *__restrict__ Told,
                                                   const double *__restrict__ eb, const int *__restrict__ pos_of,
-                                                  S *__restrict__ Rlo) {
+                                                  S *__restrict__ Rlo, int d0, int ndb) {
     const int nb = p.nb, nc = m.nc;
-    const size_t total = (size_t)p.nd * nc * nb;
+    const size_t total = (size_t)ndb * nc * nb;
     for (size_t t = gtid(); t < total; t += gstride()) {
         const int b = (int)(t % nb);
-        const size_t dc = t / nb;
-        const int c = (int)(dc % nc);
-        const size_t d = dc / nc;
+        const size_t dcl = t / nb;  // (batch direction, cell)
+        const int c = (int)(dcl % nc);
+        const size_t d = d0 + dcl / nc;
+        const size_t dc = d * nc + c;
         const double Cb = p.C[b], tau = p.tau[b], vm = p.vmag[b];
         const double vx = vm * p.sx[d], vy = vm * p.sy[d], vz = vm * p.sz[d];
         const double ec = ev.e(d, c, b, Cb);
@@ -194,7 +196,7 @@ __global__ void __launch_bounds__(256) k_residual(DMesh m, DPhys p, EView<S, DIM
             acc += tv * m.cf_area[k] * vn * x;
         }
         const double r = Cb * Told[c] + m.heat[c] * p.hr[b] * tau - ec - acc;
-        Rlo[(d * nc + pos_of[dc]) * nb + b] = (S)r;
+        Rlo[((d - d0) * nc + pos_of[dc]) * nb + b] = (S)r;
     }
 }
 
@@ -235,14 +237,14 @@ __device__ __forceinline__ void st8(S *p, const S (&v)[BC]) {
 
 template <typename S, int DIM, int BC>
 __global__ void __launch_bounds__(256) k_gradient8(DMesh m, DPhys p, const S *__restrict__ w, const S *__restrict__ eps,
-                                                   S *__restrict__ g) {
+                                                   S *__restrict__ g, int d0, int ndb) {
     const int nb = p.nb, nc = m.nc, nbc = nb / BC;
-    const size_t total = (size_t)p.nd * nc * nbc;
+    const size_t total = (size_t)ndb * nc * nbc;
     for (size_t t = gtid(); t < total; t += gstride()) {
         const int bc = (int)(t % nbc);
-        const size_t dc = t / nbc;
+        const size_t dc = t / nbc;  // (batch direction, cell): g is batch-local, eps is not
         const int c = (int)(dc % nc);
-        const S *ed = eps + (dc - c) * nb + BC * bc;
+        const S *ed = eps + ((size_t)d0 * nc + dc - c) * nb + BC * bc;
         S ec[BC], gx[BC], gy[BC], gz[BC];
         ld8(ed + (size_t)c * nb, ec);
 #pragma unroll
@@ -327,16 +329,17 @@ __global__ void __launch_bounds__(256) k_base_flux(DMesh m, DPhys p, const doubl
 template <typename S, int DIM, int BC>
 __global__ void __launch_bounds__(256, sizeof(S) == 4 ? 4 : 2) k_residual8(DMesh m, DPhys p, EView<S, DIM> ev, const double *__restrict__ Bf,
                                                    const double *__restrict__ Told, const double *__restrict__ eb,
-                                                   const int *__restrict__ pos_of, S *__restrict__ Rlo) {
+                                                   const int *__restrict__ pos_of, S *__restrict__ Rlo, int d0,
+                                                   int ndb) {
     const int nb = p.nb, nc = m.nc, nbc = nb / BC;
-    const size_t total = (size_t)p.nd * nc * nbc;
+    const size_t total = (size_t)ndb * nc * nbc;
     for (size_t t = gtid(); t < total; t += gstride()) {
         const int bc = (int)(t % nbc), b0 = BC * bc;
-        const size_t dc = t / nbc;
-        const int c = (int)(dc % nc);
-        const size_t d = dc / nc;
+        const size_t dcl = t / nbc;  // (batch direction, cell)
+        const int c = (int)(dcl % nc);
+        const size_t d = d0 + dcl / nc, dc = d * nc + c;
         const double sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
-        const size_t dbase = d * nc;
+        const size_t dbase = d * nc, gbase = (d - d0) * nc;  // all directions / this batch
         S ec[BC], acc[BC], gxv[BC], gyv[BC], gzv[BC];
         const double invV = 1.0 / m.vol[c], tb = ev.Tb[c];
         ld8(ev.eps + (dbase + c) * nb + b0, ec);
@@ -348,7 +351,7 @@ __global__ void __launch_bounds__(256, sizeof(S) == 4 ? 4 : 2) k_residual8(DMesh
             const S a = (S)(m.cf_area[k] * invV * sn);
             if (sn >= 0) {
                 if (!have_gc) {
-                    const S *gp = ev.g + (dbase + c) * DIM * nb + b0;
+                    const S *gp = ev.g + (gbase + c) * DIM * nb + b0;
                     ld8(gp, gxv);
                     ld8(gp + nb, gyv);
                     if (DIM == 3) ld8(gp + 2 * nb, gzv);
@@ -366,7 +369,7 @@ __global__ void __launch_bounds__(256, sizeof(S) == 4 ? 4 : 2) k_residual8(DMesh
                 const int j = m.cf_nbr[k];
                 S ej[BC], hx[BC], hy[BC], hz[BC];
                 ld8(ev.eps + (dbase + j) * nb + b0, ej);
-                const S *gp = ev.g + (dbase + j) * DIM * nb + b0;
+                const S *gp = ev.g + (gbase + j) * DIM * nb + b0;
                 ld8(gp, hx);
                 ld8(gp + nb, hy);
                 if (DIM == 3) ld8(gp + 2 * nb, hz);
@@ -392,7 +395,7 @@ __global__ void __launch_bounds__(256, sizeof(S) == 4 ? 4 : 2) k_residual8(DMesh
             const S fixed = (S)(p.C[b0 + i] * (dT - tv * B) + hc * p.hr[b0 + i] * p.tau[b0 + i]);
             out[i] = fixed - ec[i] - (S)tv * acc[i];
         }
-        st8(Rlo + (dbase + pos_of[dc]) * nb + b0, out);
+        st8(Rlo + (gbase + pos_of[dc]) * nb + b0, out);
     }
 }
 
@@ -454,7 +457,7 @@ __device__ __forceinline__ double sweep_div(double x, double y) { return x / y; 
 // rvec: the band chunk of a residual row is copied in 16-byte pieces (its
 // byte size, offset and the row pitch are multiples of 16).
 template <typename S, int LOOK, int LCAP>
-__global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int ncomp, int nbc, int ring_n, int nfar, int rvec,
+__global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int ncomp, int d0, int nbc, int ring_n, int nfar, int rvec,
                                                const int *__restrict__ lvl_ptr, const int *__restrict__ dir_lvl_off,
                                                const SweepRec<S> *__restrict__ rec, const int *__restrict__ lvl_cells,
                                                const double *__restrict__ kbv, const S *__restrict__ Rlo,
@@ -467,11 +470,14 @@ __global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int ncomp, int nb
     int *lp = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(far) +
                                       (((size_t)nfar * nbc * sizeof(S) + 15) & ~(size_t)15));
     const int nchunks = (nb + nbc - 1) / nbc;
-    const int ent = blockIdx.x / nchunks, chunk = blockIdx.x % nchunks;  // (direction, component), band chunk
-    const int d = ent / ncomp;
+    // (batch direction, component) and band chunk of this CTA; R and Dc hold
+    // the batch's directions (local base), records and cell lists all of
+    // them (global base)
+    const int entl = blockIdx.x / nchunks, chunk = blockIdx.x % nchunks;
+    const int dl = entl / ncomp, d = d0 + dl, ent = d * ncomp + entl % ncomp;
     const int b0 = chunk * nbc, nbl = min(nbc, nb - b0);
     const int nlev = dir_lvl_off[ent + 1] - dir_lvl_off[ent] - 1;
-    const size_t base = (size_t)d * nc;
+    const size_t base = (size_t)d * nc, lbase = (size_t)dl * nc;
     const int tid = threadIdx.x, bd = blockDim.x;
     const int lb = tid % nbc, lc0 = tid / nbc, cpp = bd / nbc;  // band of this thread, cell offset, cells per pass
     const bool band_ok = lb < nbl;
@@ -488,7 +494,7 @@ __global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int ncomp, int nb
         if (l >= nlev) return;
         unsigned char *slot = wsm + (l % LOOK) * slot_bytes;
         const int c0 = lp[l], n = min(lp[l + 1] - c0, LCAP);
-        const size_t P0 = base + c0;
+        const size_t P0 = base + c0, L0 = lbase + c0;
         const unsigned char *src = reinterpret_cast<const unsigned char *>(rec + P0);
         const int npieces = n * (int)(sizeof(SweepRec<S>) / 16);
         for (int i = tid; i < npieces; i += bd) cp_async(slot + 16 * i, src + 16 * i, 16);
@@ -496,7 +502,7 @@ __global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int ncomp, int nb
         if (rc0 < rstep)
             for (int ci = rc0; ci < n; ci += rstep)
                 cp_async(sR + (size_t)ci * nbc * sizeof(S) + rk * unit,
-                         reinterpret_cast<const unsigned char *>(Rlo + (P0 + ci) * nb + b0) + rk * unit, unit);
+                         reinterpret_cast<const unsigned char *>(Rlo + (L0 + ci) * nb + b0) + rk * unit, unit);
     };
 #pragma unroll
     for (int k = 0; k < LOOK - 1; k++) {
@@ -515,10 +521,10 @@ __global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int ncomp, int nb
         const int c0 = lp[l], c1 = lp[l + 1], n = c1 - c0;
         const int lo = c1 - ring_n;
         for (int li = lc0; li < n; li += cpp) {
-            const size_t P = base + c0 + li;
+            const size_t P = base + c0 + li, L = lbase + c0 + li;
             const bool st = li < LCAP;
             const SweepRec<S> r = st ? srec[li] : rec[P];
-            const S r0 = st ? sR[li * nbc + lb] : Rlo[P * nb + b0 + lb];
+            const S r0 = st ? sR[li * nbc + lb] : Rlo[L * nb + b0 + lb];
             const int nin = r.meta & 7, fw = (r.meta >> 3) - 1;
             S sum = (S)0;
 #pragma unroll
@@ -527,12 +533,12 @@ __global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int ncomp, int nb
                 if (j < nin) {
                     const S dj = q >= lo  ? ring[(q & mask) * nbc + lb]
                                  : q < 0 ? far[(-1 - q) * nbc + lb]
-                                         : Dc[(base + lvl_cells[base + q]) * nb + b0 + lb];
+                                         : Dc[(lbase + lvl_cells[base + q]) * nb + b0 + lb];
                     sum += r.a[j] * dj;
                 }
             }
             const S dl = sweep_div(r0 - kb * sum, (S)1 + kb * r.sig);
-            Dc[(base + r.cell) * nb + b0 + lb] = dl;
+            Dc[(lbase + r.cell) * nb + b0 + lb] = dl;
             if (fw >= 0) far[fw * nbc + lb] = dl;
             ring[((c0 + li) & mask) * nbc + lb] = dl;
         }
@@ -562,7 +568,8 @@ __global__ void __launch_bounds__(256) k_moments(DMesh m, DPhys p, int cpb, S *_
                                                  const double *__restrict__ wtab, double *__restrict__ Tlat,
                                                  double *__restrict__ E, double *__restrict__ q,
                                                  double *__restrict__ Tband, double *__restrict__ Th,
-                                                 double *__restrict__ Q, int apply) {
+                                                 double *__restrict__ Q, int apply, int d0, int ndb,
+                                                 int accumulate) {
     extern __shared__ double sm_dyn[];
     double *wt = sm_dyn;                           // [nd][kWTab]
     double *part = sm_dyn + (size_t)p.nd * kWTab;  // [blockDim][kMomSlots]
@@ -579,31 +586,35 @@ __global__ void __launch_bounds__(256) k_moments(DMesh m, DPhys p, int cpb, S *_
 #pragma unroll
         for (int i = 0; i < kWTab; i++) a[i] = 0;
         const size_t stride = (size_t)nc * nb;
-        S *e0 = eps + (size_t)c * nb + b;
-        const S *d0 = Dc + (size_t)c * nb + b;
-        for (int d = 0; d < nd; d += kMomUnroll) {
+        // directions d0 .. d0 + ndb: eps by direction, Dc by batch direction
+        S *e0 = eps + ((size_t)d0 * nc + c) * nb + b;
+        const S *c0 = Dc + (size_t)c * nb + b;
+        for (int d = 0; d < ndb; d += kMomUnroll) {
             S ev[kMomUnroll], dv[kMomUnroll];
 #pragma unroll
             for (int u = 0; u < kMomUnroll; u++) {
                 ev[u] = (S)0;
                 dv[u] = (S)0;
-                if (d + u < nd) {
+                if (d + u < ndb) {
                     ev[u] = e0[(size_t)(d + u) * stride];
-                    if (apply) dv[u] = d0[(size_t)(d + u) * stride];
+                    if (apply) dv[u] = c0[(size_t)(d + u) * stride];
                 }
             }
 #pragma unroll
             for (int u = 0; u < kMomUnroll; u++) {
-                if (d + u >= nd) break;
+                if (d + u >= ndb) break;
                 const S en = ev[u] + dv[u];
                 if (apply) e0[(size_t)(d + u) * stride] = en;
                 const double e = base + (double)en;
-                const double *w = wt + kWTab * (d + u);
+                const double *w = wt + kWTab * (d0 + d + u);
 #pragma unroll
                 for (int i = 0; i < kWTab; i++) a[i] += w[i] * e;
             }
         }
-        Tband[(size_t)b * nc + c] = a[0] / Cb;
+        if (accumulate)
+            Tband[(size_t)b * nc + c] += a[0] / Cb;
+        else
+            Tband[(size_t)b * nc + c] = a[0] / Cb;
         const double vm = p.vmag[b], lat = p.lat[b];
         const double tl = lat * a[0] / Cb;
         const bool syn = p.hr[b] > 0;
@@ -624,25 +635,20 @@ __global__ void __launch_bounds__(256) k_moments(DMesh m, DPhys p, int cpb, S *_
         if (cc >= nc) continue;
         double sum = 0;
         for (int bb = 0; bb < nb; bb++) sum += part[((size_t)i * nb + bb) * kMomSlots + j];
-        if (j == 0)
-            Tlat[cc] = sum;
-        else if (j == 1)
-            E[cc] = sum;
-        else if (j < 5)
-            q[3 * cc + j - 2] = sum;
-        else if (j == 5)
-            Th[cc] = p.kappa * sum;
-        else
-            Q[6 * cc + j - 6] = sum;
+        // later direction batches add to the first one's moments
+        double *dst = j == 0 ? &Tlat[cc] : j == 1 ? &E[cc] : j < 5 ? &q[3 * cc + j - 2] : j == 5 ? &Th[cc] : &Q[6 * cc + j - 6];
+        if (j == 5) sum *= p.kappa;
+        *dst = accumulate ? *dst + sum : sum;
     }
 }
 
 // outgoing boundary values: e_c(new) + g_c(pre-sweep) . (x_f - x_c)
 template <typename S, int DIM>
-__global__ void k_bound_out(DMesh m, DPhys p, EView<S, DIM> ev, double *__restrict__ eb) {
+__global__ void k_bound_out(DMesh m, DPhys p, EView<S, DIM> ev, double *__restrict__ eb, int d0, int ndb) {
     const int nb = p.nb;
-    const size_t total = (size_t)p.nd * m.nbs * nb;
-    for (size_t t = gtid(); t < total; t += gstride()) {
+    const size_t total = (size_t)ndb * m.nbs * nb;
+    for (size_t tl = gtid(); tl < total; tl += gstride()) {
+        const size_t t = tl + (size_t)d0 * m.nbs * nb;  // index over all directions
         const int b = (int)(t % nb);
         const int s = (int)((t / nb) % m.nbs);
         const size_t d = t / ((size_t)nb * m.nbs);
@@ -1881,9 +1887,6 @@ Error Solver::alloc_all() {
     const size_t ne = nd * nc * nb;
     auto A = [&](size_t bytes) { return dalloc(bytes); };
     eps_ = A(ne * S);
-    grad_ = A(ne * mesh.dim * S);
-    res_ = A(ne * S);
-    corr_ = A(ne * S);
     Tbase_ = (double *)A(nc * 8);
     Bflux_ = (double *)A((size_t)nd * nc * 8);
     dsum_ = (double *)A(std::max<size_t>(1, nbs) * nb * 8);
@@ -1917,7 +1920,23 @@ Error Solver::alloc_all() {
     cg_p_ = (double *)A(nc * 8);
     cg_Ap_ = (double *)A(nc * 8);
     cg_scal_ = (double *)A(65536 * 8);
-    for (void *pp : {eps_, grad_, res_, corr_, (void *)Tbase_, (void *)Bflux_, (void *)eb_, (void *)cg_scal_})
+    if (!eps_) return {-6, "device allocation failed (" + std::to_string(ne * S / 1048576) + " MiB of intensities)"};
+    // the gradient, residual and correction buffers per direction: all
+    // directions when they fit in 90% of the free device memory, else
+    // batches of directions (the intensities, records and schedules stay whole)
+    {
+        const size_t per_dir = nc * nb * S * (mesh.dim + 2);
+        size_t fr = 0, tot = 0;
+        CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+        const size_t room = fr > (size_t)512 << 20 ? (size_t)((fr - ((size_t)512 << 20)) * 0.9) : 0;
+        ndb_ = (int)std::min<size_t>(nd, room / per_dir);
+        if (cfg.direction_batch > 0) ndb_ = std::min(ndb_, cfg.direction_batch);
+        if (ndb_ < 1) return {-6, "device memory too small for one direction's gradient/residual buffers"};
+        grad_ = A((size_t)ndb_ * nc * nb * mesh.dim * S);
+        res_ = A((size_t)ndb_ * nc * nb * S);
+        corr_ = A((size_t)ndb_ * nc * nb * S);
+    }
+    for (void *pp : {grad_, res_, corr_, (void *)Tbase_, (void *)Bflux_, (void *)eb_, (void *)cg_scal_})
         if (!pp)
             return {-6, "device allocation failed (" + std::to_string(ne * S * (3 + mesh.dim) / 1048576) +
                             " MiB of band state)"};
@@ -2343,8 +2362,13 @@ Error Solver::solve_t(SolveStats &st) {
     const size_t ne = (size_t)nd * nc * nb;
     S *eps = (S *)eps_, *g = (S *)grad_, *R = (S *)res_;
     const S *w = std::is_same<S, float>::value ? (const S *)dm_.lsq_wf : (const S *)dm_.lsq_w;
-    EView<S, DIM> ev{eps, g, Tbase_, gTb_, nb, nc};
-    const int gE = grid_for(ne), gB = grid_for((size_t)nd * nbs * nb), gE8 = grid_for(ne / 4);
+    EView<S, DIM> ev{eps, g, Tbase_, gTb_, nb, nc, 0};
+    const int gE = grid_for(ne);
+    // direction batches: the gradient, residual and correction buffers hold
+    // ndb_ directions (all of them when they fit in device memory)
+    const int ndb = ndb_;
+    const int gB = grid_for((size_t)nd * nbs * nb);
+    (void)gE;
     const int gC = (nc + kThreads - 1) / kThreads, gN = (nslot + kThreads - 1) / kThreads;
     // blocks per geometry of the per-geometry reductions
     const int comp_blocks = std::max(1, std::min(148, (nc / ncomp_ + kThreads - 1) / kThreads));
@@ -2374,11 +2398,12 @@ Error Solver::solve_t(SolveStats &st) {
         L.rvec = ((L.nbc * sizeof(S)) % 16 == 0 && (nb * sizeof(S)) % 16 == 0 && (last * sizeof(S)) % 16 == 0) ? 1 : 0;
         return true;
     };
-    auto launch_sweep = [&](const SweepLaunch &L) -> cudaError_t {
+    auto launch_sweep = [&](const SweepLaunch &L, int d0, int nbt) -> cudaError_t {
         cudaError_t e = cudaFuncSetAttribute(k_sweep<S, LOOK, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)L.smem);
         if (e != cudaSuccess) return e;
-        k_sweep<S, LOOK, LCAP><<<L.blocks, L.threads, L.smem, s>>>(nb, nc, ncomp_, L.nbc, ring_, far_slots_, L.rvec,
+        const int blocks = nbt * ncomp_ * L.chunks;
+        k_sweep<S, LOOK, LCAP><<<blocks, L.threads, L.smem, s>>>(nb, nc, ncomp_, d0, L.nbc, ring_, far_slots_, L.rvec,
                                                                    lvl_ptr_, dir_lvl_off_, (const SweepRec<S> *)rec_,
                                                                    lvl_cells_, kb_, R, (S *)corr_);
         return cudaGetLastError();
@@ -2406,9 +2431,15 @@ Error Solver::solve_t(SolveStats &st) {
     };
     if (!started_) {
         // _set_initial (:765-782) and the initial boundary values (StaticBTESyntheticSolver.cpp:45-62)
-        GL(K_INIT, k_init_eps<S><<<gE, kThreads, 0, s>>>(dm_, dp_, T_, Tbase_, eps));
-        GL(K_GRADIENT, (k_gradient<S, DIM><<<gE, kThreads, 0, s>>>(dm_, dp_, w, eps, g)));
-        GL(K_BOUND_OUT, (k_bound_out<S, DIM><<<gB, kThreads, 0, s>>>(dm_, dp_, ev, eb_)));
+        GL(K_INIT, k_init_eps<S><<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, T_, Tbase_, eps));
+        for (int d0 = 0; d0 < nd; d0 += ndb) {
+            const int nbt = std::min(ndb, nd - d0);
+            ev.gd0 = d0;
+            GL(K_GRADIENT, (k_gradient<S, DIM><<<grid_for((size_t)nbt * nc * nb), kThreads, 0, s>>>(dm_, dp_, w, eps, g,
+                                                                                                 d0, nbt)));
+            GL(K_BOUND_OUT, (k_bound_out<S, DIM><<<grid_for((size_t)nbt * nbs * nb), kThreads, 0, s>>>(dm_, dp_, ev,
+                                                                                                   eb_, d0, nbt)));
+        }
         gather();
         CUDA_TRY(cudaGetLastError());
         started_ = true;
@@ -2428,14 +2459,20 @@ Error Solver::solve_t(SolveStats &st) {
         // copy() (:2655-2690)
         CUDA_TRY(cudaMemcpyAsync(Told_, T_, nc * 8, cudaMemcpyDeviceToDevice, s));
         CUDA_TRY(cudaMemcpyAsync(qold_, q_, (size_t)nc * 24, cudaMemcpyDeviceToDevice, s));
+        for (int d0 = 0; d0 < nd; d0 += ndb) {
+        const int nbt = std::min(ndb, nd - d0);
+        const size_t nbe = (size_t)nbt * nc * nb;
+        ev.gd0 = d0;
         if (nb % 4 == 0) {
-            GL(K_GRADIENT, (k_gradient8<S, DIM, 4><<<gE8, kThreads, 0, s>>>(dm_, dp_, w, eps, g)));
-            GL(K_RESIDUAL, (k_residual8<S, DIM, 4><<<gE8, kThreads, 0, s>>>(dm_, dp_, ev, Bflux_, Told_, eb_, pos_of_, R)));
+            GL(K_GRADIENT, (k_gradient8<S, DIM, 4><<<grid_for(nbe / 4), kThreads, 0, s>>>(dm_, dp_, w, eps, g, d0, nbt)));
+            GL(K_RESIDUAL, (k_residual8<S, DIM, 4><<<grid_for(nbe / 4), kThreads, 0, s>>>(dm_, dp_, ev, Bflux_, Told_, eb_,
+                                                                                          pos_of_, R, d0, nbt)));
         } else {
-            GL(K_GRADIENT, (k_gradient<S, DIM><<<gE, kThreads, 0, s>>>(dm_, dp_, w, eps, g)));
-            GL(K_RESIDUAL, (k_residual<S, DIM><<<gE, kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, pos_of_, R)));
+            GL(K_GRADIENT, (k_gradient<S, DIM><<<grid_for(nbe), kThreads, 0, s>>>(dm_, dp_, w, eps, g, d0, nbt)));
+            GL(K_RESIDUAL, (k_residual<S, DIM><<<grid_for(nbe), kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, pos_of_, R,
+                                                                                  d0, nbt)));
         }
-        if (tune && nt == 0) {
+        if (tune && nt == 0 && d0 == 0) {
             // autotuner: every cap on the bands per CTA that gives a distinct
             // chunking, timed on this iteration's residual (the sweep only
             // reads R and rewrites every correction, so the trials leave no
@@ -2452,7 +2489,7 @@ Error Solver::solve_t(SolveStats &st) {
                 float ms = 1e30f;
                 for (int rep = 0; rep < 2; rep++) {
                     CUDA_TRY(cudaEventRecord(t0, s));
-                    CUDA_TRY(launch_sweep(L));
+                    CUDA_TRY(launch_sweep(L, d0, nbt));
                     CUDA_TRY(cudaEventRecord(t1, s));
                     CUDA_TRY(cudaEventSynchronize(t1));
                     float m = 0;
@@ -2470,10 +2507,13 @@ Error Solver::solve_t(SolveStats &st) {
             wcap = best_cap;
             sweep_launch(wcap, SL);
         }
-        GL(K_SWEEP, CUDA_TRY(launch_sweep(SL)));
-        GL(K_MOMENTS, (k_moments<S><<<gM, cpb * nb, msmem, s>>>(dm_, dp_, cpb, eps, (const S *)corr_, Tbase_, wtab_, Tlat_, E_,
-                                                                q_, Tband_, Th_, Q_, 1)));
-        GL(K_BOUND_OUT, (k_bound_out<S, DIM><<<gB, kThreads, 0, s>>>(dm_, dp_, ev, eb_)));
+        GL(K_SWEEP, CUDA_TRY(launch_sweep(SL, d0, nbt)));
+        GL(K_MOMENTS, (k_moments<S><<<gM, cpb * nb, msmem, s>>>(dm_, dp_, cpb, eps, (const S *)corr_, Tbase_, wtab_,
+                                                                Tlat_, E_, q_, Tband_, Th_, Q_, 1, d0, nbt,
+                                                                d0 > 0 ? 1 : 0)));
+        GL(K_BOUND_OUT, (k_bound_out<S, DIM><<<grid_for((size_t)nbt * nbs * nb), kThreads, 0, s>>>(dm_, dp_, ev, eb_, d0,
+                                                                                               nbt)));
+        }
         GL(K_SIDE_MOMENTS, k_side_moments<<<gW, kThreads, 0, s>>>(dm_, dp_, eb_, Ths_, Qs_));
         GL(K_NODE_INTERP, k_node_interp<<<gN, kThreads, 0, s>>>(dm_, Th_, Q_, Ths_, Qs_, ThV_, QV_));
         GL(K_REMACRO, k_remacro<<<gC, kThreads, 0, s>>>(dm_, Th_, Q_, Ths_, Qs_, ThV_, QV_, remacro_));

@@ -49,6 +49,7 @@ struct SolverConfig {
     int profile = 0;
     int sweep_bands = 0;      // bands per sweep CTA, 0 = automatic
     int sweep_far_slots = 0;  // far-slot cap of the sweep plan: 0 = automatic, < 0 = none
+    int direction_batch = 0;  // most directions per transport batch, 0 = automatic
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -101,6 +102,7 @@ public:
     bool initialised = false;
     std::string last_error;
     int tuned_sweep_bands_ = 0;  // bands-per-CTA cap the sweep autotuner picked (0 = not yet)
+    int ndb_ = 1;                // directions per batch of the gradient/residual/correction buffers
 
 private:
     template <typename S, int DIM> Error solve_t(SolveStats &st);
@@ -116,8 +118,9 @@ private:
     DMesh dm_{};
     DPhys dp_{};
     // state
-    // storage-type arrays [nd][nc][nb]: deviations, gradients (x DIM),
-    // residuals (level order) and sweep corrections (cell order)
+    // storage-type arrays: deviations [nd][nc][nb]; gradients (x DIM),
+    // residuals (level order) and sweep corrections (cell order) for one
+    // batch of ndb_ directions [ndb_][nc][nb]
     void *eps_ = nullptr, *grad_ = nullptr, *res_ = nullptr, *corr_ = nullptr;
     double *Tbase_ = nullptr, *gTb_ = nullptr;
     double *Bflux_ = nullptr;  // [nd][nc] base-field face flux sums of the residual

@@ -128,6 +128,8 @@ typedef struct {
     int sweep_bands;          /* bands per CTA of the upwind sweep (1..32); 0 = automatic */
     int sweep_far_slots;      /* on-chip slots per direction for upwind reads older than the sweep's
                                  ring: 0 = automatic (2048), < 0 = none (such reads go to memory) */
+    int direction_batch;      /* most directions whose gradient/residual/correction buffers are held at
+                                 once; 0 = automatic (all that fit in device memory) */
 } gbte_options;
 
 #define GBTE_NUM_KERNELS 16
@@ -153,6 +155,7 @@ typedef struct {
     long long kernel_count[GBTE_NUM_KERNELS];
     int sweep_bands;          /* bands-per-CTA cap of the sweep in use (options.sweep_bands, or
                                  the autotuner's pick on the handle's first outer iteration) */
+    int direction_batch;      /* directions per batch of the transport stage */
 } gbte_stats;
 
 /* Name of kernel slot i of gbte_stats.kernel_ms (NULL past the last one). */

@@ -126,3 +126,21 @@ def test_sweep_variants_match_oracle_3d(opts):
     s.close()
     assert rel(f["T"], o["T"]) <= TOL_FP64, rel(f["T"], o["T"])
     assert rel(f["q"], o["q"]) <= 1e-8
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [g.GBTE_FP64, g.GBTE_FP32_MIXED])
+def test_direction_batches_match_oracle_3d(prec):
+    # the transport stage in uneven batches of 5 directions (32 = 6 x 5 + 2):
+    # batch-sized gradient/residual/correction buffers, moments accumulated
+    # over batches; same fixed point
+    d = small_block()
+    o = oracle_fields(False)
+    kw = {} if prec == g.GBTE_FP64 else {"err_temp": 1e-9, "err_flux": 1e-7}
+    s = g.StaticBTESynthetic.from_deck(d, precision=prec, direction_batch=5, **kw)
+    st = s.solve(allow_not_converged=prec != g.GBTE_FP64)
+    f = s.fields()
+    s.close()
+    assert st["direction_batch"] == 5
+    tol = TOL_FP64 if prec == g.GBTE_FP64 else TOL_FP32
+    assert rel(f["T"], o["T"]) <= tol, rel(f["T"], o["T"])
