@@ -2149,6 +2149,9 @@ Error Solver::cg_plan(const std::vector<int> &ptr, const std::vector<int> &idx, 
     if (n < C) return {0, ""};
     int max_smem = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, cfg.device));
+    // eight vectors of a part alone must fit: otherwise no plan (larger
+    // systems take the grid-wide kernel), before any partitioning work
+    if ((size_t)64 * ((n + C - 1) / C) > (size_t)max_smem) return {0, ""};
     const int NA = C * kCgAgg;
     std::vector<int> perm(n), abounds{0}, bounds(C + 1);
     for (int i = 0; i < n; i++) perm[i] = i;
