@@ -247,7 +247,8 @@ int gbte_fourier_initial(gbte_handle *h);
  * calls that overlap on the GPU (other threads or streams) race; the CG
  * reduction slots are cleared on every solve, everything else is written
  * before it is read. Results go to the handle exactly as with
- * gbte_fourier_initial. */
+ * gbte_fourier_initial. Handles of a batched solve (gbte_batch_create) get
+ * GBTE_ERR_UNSUPPORTED. */
 int gbte_fourier_initial_noalloc(gbte_handle *h);
 
 /* Runs the outer source iteration until both margins are below the limits
