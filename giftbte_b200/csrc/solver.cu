@@ -1609,10 +1609,6 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
     lvl_cells_ = up_i(sched.lvl_cells);
     lvl_ptr_ = up_i(sched.lvl_ptr);
     dir_lvl_off_ = up_i(sched.dir_lvl_off);
-    max_lvl_width_ = 0;
-    for (int d = 0; d + 1 < (int)sched.dir_lvl_off.size(); d++)
-        for (int k = sched.dir_lvl_off[d]; k + 1 < sched.dir_lvl_off[d + 1]; k++)
-            max_lvl_width_ = std::max(max_lvl_width_, sched.lvl_ptr[k + 1] - sched.lvl_ptr[k]);
     if (!sched.lag.empty()) {
         void *pl = dalloc(sched.lag.size());
         if (!pl) return {-6, "device allocation failed (lag mask)"};

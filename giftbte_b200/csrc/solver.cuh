@@ -136,7 +136,6 @@ private:
     bool need_snapshot_ = false;
     // schedule on device
     int *lvl_cells_ = nullptr, *lvl_ptr_ = nullptr, *dir_lvl_off_ = nullptr;
-    int max_lvl_width_ = 0;  // widest level of any direction (cells)
     int ring_ = 0;           // on-chip ring of the sweep (positions, power of two)
     int far_slots_ = 0;      // on-chip far slots of the sweep (0: far reads go to memory)
     // level-ordered sweep records per direction: sum of outgoing A/V (s.n)
