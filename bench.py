@@ -169,7 +169,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     s_bytes = 4 if prec == g.GBTE_FP32_MIXED else 8
 
     solver = g.StaticBTESynthetic.from_deck(deck, precision=prec, device=local_rank, profile=1,
-                                            stream=ctypes_stream(stream))
+                                            stream=ctypes_stream(stream), cell_order=args.cell_order)
     nb, nd = solver.num_bands, solver.num_directions
     upd_per_step = nb * nd * nc
     # warm-up (not timed)
@@ -244,6 +244,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             "data": "synthetic: seeded mesh and band table generated in-process (no dataset)",
             "config": {"workload": desc, "cells": nc, "bands": nb, "directions": nd,
                        "updates_per_step": upd_per_step, "precision": args.precision,
+                       "cell_order": "morton" if args.cell_order == 0 else "deck",
                        "l2": f"band state {upd_per_step * s_bytes / 1e6:.0f} MB per copy, larger than the 126 MB L2",
                        "parallelism": f"replicas x{world} (independent seeded cells)" if world > 1 else "1 GPU"},
             "roofline": roofline, "hbm_kernels": hbm_kernels, "kernels": kernel_table, "cpu_baseline": cpu,
@@ -267,7 +268,7 @@ def e2e_solves(args, deck, prec, device, world):
 
     nc = deck.mesh.n_cells
     solver = g.StaticBTESynthetic.from_deck(deck, precision=prec, device=device, max_iter=args.max_iter_e2e,
-                                            err_temp=1e-8, err_flux=1e-8)
+                                            err_temp=1e-8, err_flux=1e-8, cell_order=args.cell_order)
     nb = solver.num_bands
     T0 = torch.full((nc,), float(deck.tref), dtype=torch.float64).pin_memory().numpy()
     out = {k: np.zeros(n) for k, n in (("E", nc), ("T", nc), ("q", 3 * nc), ("Tb", nb * nc))}
@@ -304,7 +305,7 @@ def fp64_reference_run(args, deck, device):
     fields = {}
     for prec, name in ((g.GBTE_FP64, "fp64"), (g.GBTE_FP32_MIXED, "fp32")):
         s = g.StaticBTESynthetic.from_deck(deck, precision=prec, device=device, max_iter=args.max_iter_e2e,
-                                           err_temp=1e-8, err_flux=1e-8)
+                                           err_temp=1e-8, err_flux=1e-8, cell_order=args.cell_order)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         st = s.solve()
@@ -424,7 +425,7 @@ def run_config5(args, rank: int):
     cells = [d.mesh.n_cells for d in pop]
     nb, nd = pop[0].bands.n_bands, 4 * pop[0].n_phi
     upd = nb * nd * sum(cells)
-    b = g.StaticBTESynthetic.from_decks(pop, precision=g.GBTE_FP32_MIXED)
+    b = g.StaticBTESynthetic.from_decks(pop, precision=g.GBTE_FP32_MIXED, cell_order=args.cell_order)
     b.solve(max_iter=args.warmup, err_temp=0.0, err_flux=0.0)
     torch.cuda.synchronize()
     clocks = ClockSampler(0)
@@ -435,7 +436,7 @@ def run_config5(args, rank: int):
     b.close()
     seq_ms = 0.0
     for d in pop:
-        s = g.StaticBTESynthetic.from_deck(d, precision=g.GBTE_FP64)
+        s = g.StaticBTESynthetic.from_deck(d, precision=g.GBTE_FP64, cell_order=args.cell_order)
         s.solve(max_iter=args.warmup, err_temp=0.0, err_flux=0.0)
         seq_ms += s.solve(max_iter=args.steps, err_temp=0.0, err_flux=0.0)["solve_ms"]
         s.close()
@@ -468,6 +469,8 @@ def main():
     ap.add_argument("--workload", choices=["config2", "config1", "config3", "config5"], default="config2")
     ap.add_argument("--batch", type=int, default=256, help="config5: number of independent cells")
     ap.add_argument("--h-nm", type=float, default=0.0, help="config3 mesh spacing (default 2.5 nm)")
+    ap.add_argument("--cell-order", type=int, choices=[0, 1], default=0,
+                    help="0: cells renumbered along a Morton curve inside the library; 1: the deck's order")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--max-iter-e2e", type=int, default=2000)
     ap.add_argument("--ref-steps", type=int, default=2)

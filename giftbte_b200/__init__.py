@@ -65,7 +65,8 @@ class Options(ctypes.Structure):
                 ("err_temp", ctypes.c_double), ("err_flux", ctypes.c_double), ("cell_heat", _c_dbl_p),
                 ("stream", ctypes.c_void_p), ("device", ctypes.c_int), ("verbose", ctypes.c_int),
                 ("macro_rtol", ctypes.c_double), ("profile", ctypes.c_int), ("sweep_bands", ctypes.c_int),
-                ("sweep_far_slots", ctypes.c_int), ("direction_batch", ctypes.c_int)]
+                ("sweep_far_slots", ctypes.c_int), ("direction_batch", ctypes.c_int),
+                ("cell_order", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):

@@ -22,6 +22,23 @@ struct gbte_handle {
     gbte::FlatMesh *mesh() { return &solver.mesh; }
     std::string err;
     double setup_ms = 0;
+    // cell order: internal cell k is the caller's cell perm[k]; empty = same order
+    std::vector<int> perm;
+    // caller's array of nc rows of w values -> internal order
+    std::vector<double> to_internal(const double *user, int w) const {
+        const size_t nc = perm.size();
+        std::vector<double> v(nc * w);
+        for (size_t k = 0; k < nc; k++)
+            for (int j = 0; j < w; j++) v[k * w + j] = user[(size_t)perm[k] * w + j];
+        return v;
+    }
+    // internal array of nc rows of w values -> caller's order, in place
+    void to_user(double *a, int w) const {
+        const size_t nc = perm.size();
+        std::vector<double> v(a, a + nc * w);
+        for (size_t k = 0; k < nc; k++)
+            for (int j = 0; j < w; j++) a[(size_t)perm[k] * w + j] = v[k * w + j];
+    }
 };
 
 namespace {
@@ -79,7 +96,12 @@ int finish_bands(gbte::Bands &bands) {
     return GBTE_OK;
 }
 
-int create_common(const gbte::RawMesh &raw, const gbte::Bands &bands_in, const gbte::BCs &bcs, const gbte_angle_spec &as,
+// Cells are renumbered inside the library along a Morton curve of their
+// centres (per geometry of a batch) unless options.cell_order = 1: upwind and
+// stencil neighbours then sit close in memory, so the gathers of the sweep,
+// the gradient and the residual hit fewer distinct lines. Every cell array of
+// the ABI is mapped back to the caller's order.
+int create_common(const gbte::RawMesh &raw_in, const gbte::Bands &bands_in, const gbte::BCs &bcs, const gbte_angle_spec &as,
                   const gbte_options &opt, const std::vector<double> &cell_heat, gbte_handle **out) {
     double t0 = now_ms();
     std::unique_ptr<gbte_handle> h(new (std::nothrow) gbte_handle());
@@ -93,6 +115,19 @@ int create_common(const gbte::RawMesh &raw, const gbte::Bands &bands_in, const g
     gbte::Angles ang;
     gbte::Error e = gbte::make_angles(as.method, as.n_theta, as.n_phi, bands.material_dim, ang);
     if (e.code) return fail(nullptr, e), status_of(e.code);
+    if (opt.cell_order != 0 && opt.cell_order != 1)
+        return fail(nullptr, {-1, "cell_order must be 0 (automatic) or 1 (caller's order)"}), GBTE_ERR_ARG;
+    const gbte::RawMesh *rp = &raw_in;
+    gbte::RawMesh reordered;
+    std::vector<double> heat = cell_heat;
+    if (opt.cell_order == 0) {
+        gbte::locality_order(raw_in, h->perm);
+        reordered = raw_in;
+        gbte::reorder_cells(reordered, h->perm);
+        rp = &reordered;
+        if (!heat.empty()) heat = h->to_internal(cell_heat.data(), 1);
+    }
+    const gbte::RawMesh &raw = *rp;
     gbte::FlatMesh fm;
     e = gbte::build_flat_mesh(raw, bcs, bands, fm);
     if (e.code) return fail(nullptr, e), status_of(e.code);
@@ -112,7 +147,6 @@ int create_common(const gbte::RawMesh &raw, const gbte::Bands &bands_in, const g
     cfg.stream = (cudaStream_t)opt.stream;
     if (opt.precision != GBTE_FP64 && opt.precision != GBTE_FP32_MIXED)
         return fail(nullptr, {-1, "precision must be GBTE_FP64 or GBTE_FP32_MIXED"}), GBTE_ERR_ARG;
-    std::vector<double> heat = cell_heat;
     e = h->solver.init(fm, bands, ang, heat, cfg);
     if (e.code) return fail(nullptr, e), status_of(e.code);
     h->setup_ms = now_ms() - t0;
@@ -185,7 +219,7 @@ static int convert_views(const gbte_mesh_view *mv, const gbte_band_table *bt, co
 }
 
 // host-only build of everything gbte_create would put on the device
-static int inspect_common(const gbte::RawMesh &raw, const gbte::Bands &bands_in, const gbte::BCs &bcs,
+static int inspect_common(const gbte::RawMesh &raw_in, const gbte::Bands &bands_in, const gbte::BCs &bcs,
                           const gbte_angle_spec &as, gbte_deck_info *info) {
     gbte::Bands bands = bands_in;
     int brc = finish_bands(bands);
@@ -193,6 +227,11 @@ static int inspect_common(const gbte::RawMesh &raw, const gbte::Bands &bands_in,
     gbte::Angles ang;
     gbte::Error e = gbte::make_angles(as.method, as.n_theta, as.n_phi, bands.material_dim, ang);
     if (e.code) return fail(nullptr, e), status_of(e.code);
+    // the cell order gbte_create uses by default
+    std::vector<int> perm;
+    gbte::locality_order(raw_in, perm);
+    gbte::RawMesh raw = raw_in;
+    gbte::reorder_cells(raw, perm);
     gbte::FlatMesh fm;
     e = gbte::build_flat_mesh(raw, bcs, bands, fm);
     if (e.code) return fail(nullptr, e), status_of(e.code);
@@ -376,7 +415,14 @@ int gbte_create_from_deck(const char *dir, const gbte_options *opt_in, gbte_hand
 int gbte_set_initial(gbte_handle *h, const double *T0, const double *q0, const double *bth) {
     if (!h) return GBTE_ERR_ARG;
     try {
-        gbte::Error e = h->solver.set_initial(T0, q0, bth);
+        gbte::Error e;
+        if (h->perm.empty() || !T0) {
+            e = h->solver.set_initial(T0, q0, bth);
+        } else {
+            std::vector<double> T = h->to_internal(T0, 1), q;
+            if (q0) q = h->to_internal(q0, 3);
+            e = h->solver.set_initial(T.data(), q0 ? q.data() : nullptr, bth);
+        }
         if (e.code) return fail(h, e), status_of(e.code);
         return GBTE_OK;
     } catch (const std::exception &ex) {
@@ -462,6 +508,14 @@ int gbte_get_fields(gbte_handle *h, double *TE, double *TL, double *q, double *T
     if (!h) return GBTE_ERR_ARG;
     gbte::Error e = h->solver.get_fields(TE, TL, q, TB);
     if (e.code) return fail(h, e), status_of(e.code);
+    if (!h->perm.empty()) {
+        const size_t nc = h->perm.size();
+        if (TE) h->to_user(TE, 1);
+        if (TL) h->to_user(TL, 1);
+        if (q) h->to_user(q, 3);
+        if (TB)
+            for (int b = 0; b < h->solver.bands.nb; b++) h->to_user(TB + b * nc, 1);
+    }
     return GBTE_OK;
 }
 
@@ -477,13 +531,14 @@ int gbte_get_sizes(gbte_handle *h, int *nc, int *nb, int *nd, int *nbs) {
 int gbte_get_geometry(gbte_handle *h, double *centers, double *volumes) {
     if (!h) return GBTE_ERR_ARG;
     const gbte::FlatMesh &m = h->solver.mesh;
-    for (int c = 0; c < m.nc; c++) {
+    for (int k = 0; k < m.nc; k++) {
+        const int c = h->perm.empty() ? k : h->perm[k];
         if (centers) {
-            centers[3 * c] = m.cx[c];
-            centers[3 * c + 1] = m.cy[c];
-            centers[3 * c + 2] = m.cz[c];
+            centers[3 * c] = m.cx[k];
+            centers[3 * c + 1] = m.cy[k];
+            centers[3 * c + 2] = m.cz[k];
         }
-        if (volumes) volumes[c] = m.vol[c];
+        if (volumes) volumes[c] = m.vol[k];
     }
     return GBTE_OK;
 }
@@ -495,6 +550,15 @@ int gbte_write_outputs(gbte_handle *h, const char *dir) {
     std::vector<double> TE(nc), TL(nc), q(3 * (size_t)nc), TB((size_t)nb * nc);
     int rc = gbte_get_fields(h, TE.data(), TL.data(), q.data(), TB.data());
     if (rc != GBTE_OK) return rc;
+    // files list cells in the caller's order: row i is internal cell at[i]
+    std::vector<int> at(nc);
+    for (int k = 0; k < nc; k++) at[h->perm.empty() ? k : h->perm[k]] = k;
+    std::vector<double> cx(nc), cy(nc), cz(nc);
+    for (int i = 0; i < nc; i++) {
+        cx[i] = m.cx[at[i]];
+        cy[i] = m.cy[at[i]];
+        cz[i] = m.cz[at[i]];
+    }
     std::string d(dir);
     auto open = [&](const char *name, std::ofstream &f) {
         f.open(d + "/" + name);
@@ -504,19 +568,19 @@ int gbte_write_outputs(gbte_handle *h, const char *dir) {
     std::ofstream f;
     // TempLattice.dat / Tempband.dat / Temperature.dat / HeatFlux.dat (StaticBTESynthetic.cpp:2613-2653)
     if (!open("TempLattice.dat", f)) return fail(h, {-2, "cannot write TempLattice.dat"}), GBTE_ERR_IO;
-    for (int i = 0; i < nc; i++) f << m.cx[i] << " " << m.cy[i] << " " << m.cz[i] << " " << TL[i] << "\n";
+    for (int i = 0; i < nc; i++) f << cx[i] << " " << cy[i] << " " << cz[i] << " " << TL[i] << "\n";
     f.close();
     if (!open("Tempband.dat", f)) return fail(h, {-2, "cannot write Tempband.dat"}), GBTE_ERR_IO;
     for (int j = 0; j < nb; j++)
         for (int i = 0; i < nc; i++)
-            f << j + 1 << " " << m.cx[i] << " " << m.cy[i] << " " << m.cz[i] << " " << TB[(size_t)j * nc + i] << "\n";
+            f << j + 1 << " " << cx[i] << " " << cy[i] << " " << cz[i] << " " << TB[(size_t)j * nc + i] << "\n";
     f.close();
     if (!open("Temperature.dat", f)) return fail(h, {-2, "cannot write Temperature.dat"}), GBTE_ERR_IO;
-    for (int i = 0; i < nc; i++) f << m.cx[i] << " " << m.cy[i] << " " << m.cz[i] << " " << TE[i] << "\n";
+    for (int i = 0; i < nc; i++) f << cx[i] << " " << cy[i] << " " << cz[i] << " " << TE[i] << "\n";
     f.close();
     if (!open("HeatFlux.dat", f)) return fail(h, {-2, "cannot write HeatFlux.dat"}), GBTE_ERR_IO;
     for (int i = 0; i < nc; i++) {
-        double v[6] = {m.cx[i], m.cy[i], m.cz[i], q[3 * i], q[3 * i + 1], q[3 * i + 2]};
+        double v[6] = {cx[i], cy[i], cz[i], q[3 * i], q[3 * i + 1], q[3 * i + 2]};
         for (double x : v) f << " " << std::setw(24) << x;
         f << "\n";
     }
@@ -529,13 +593,15 @@ int gbte_write_outputs(gbte_handle *h, const char *dir) {
     size_t total = 0;
     for (int c = 0; c < nc; c++) total += m.cptr[c + 1] - m.cptr[c] + 1;
     f << "\nCELLS " << nc << " " << total << "\n";
-    for (int c = 0; c < nc; c++) {
+    for (int i = 0; i < nc; i++) {
+        const int c = at[i];
         f << m.cptr[c + 1] - m.cptr[c];
         for (int k = m.cptr[c]; k < m.cptr[c + 1]; k++) f << " " << m.cverts[k];
         f << "\n";
     }
     f << "\nCELL_TYPES " << nc << "\n";
-    for (int c = 0; c < nc; c++) {
+    for (int i = 0; i < nc; i++) {
+        const int c = at[i];
         int nv = m.cptr[c + 1] - m.cptr[c];
         f << (m.dim == 2 ? (nv == 4 ? 8 : 5) : 10) << "\n";
     }

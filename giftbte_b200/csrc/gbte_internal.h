@@ -142,6 +142,14 @@ struct SweepPlan {
     std::vector<int> far_w;   // [nd*nc] far slot this cell stores into, -1 none
 };
 
+// Cell order for locality: cells sorted by the Morton code of their centre
+// (within each component, so components keep their ranges). perm[k] = the
+// original index of the cell placed at k. Only the order of cells changes:
+// faces, neighbours and stencils are the same sets, so results agree to
+// rounding.
+void locality_order(const RawMesh &raw, std::vector<int> &perm);
+void reorder_cells(RawMesh &raw, const std::vector<int> &perm);
+
 // Disjoint union of independent geometries for one batched solve: nodes,
 // cells and boundary elements concatenated, the boundary tags of geometry k
 // (and the tags its periodic types name) shifted by k * (largest tag + 1),

@@ -733,6 +733,63 @@ Error build_sweep_plan(const FlatMesh &m, const Angles &a, const Schedule &s, in
     return {0, ""};
 }
 
+void locality_order(const RawMesh &raw, std::vector<int> &perm) {
+    const int nc = raw.nc();
+    std::vector<double> c(3 * (size_t)nc, 0.0);
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int i = 0; i < nc; i++) {
+        const int n = raw.cptr[i + 1] - raw.cptr[i];
+        for (int k = raw.cptr[i]; k < raw.cptr[i + 1]; k++)
+            for (int a = 0; a < 3; a++) c[3 * (size_t)i + a] += raw.xyz[3 * (size_t)raw.cverts[k] + a] / n;
+        for (int a = 0; a < 3; a++) {
+            lo[a] = std::min(lo[a], c[3 * (size_t)i + a]);
+            hi[a] = std::max(hi[a], c[3 * (size_t)i + a]);
+        }
+    }
+    // Morton code of the centre quantised to 21 bits per axis
+    auto spread = [](uint64_t v) {
+        v &= 0x1fffff;
+        v = (v | v << 32) & 0x1f00000000ffffULL;
+        v = (v | v << 16) & 0x1f0000ff0000ffULL;
+        v = (v | v << 8) & 0x100f00f00f00f00fULL;
+        v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+        v = (v | v << 2) & 0x1249249249249249ULL;
+        return v;
+    };
+    std::vector<uint64_t> key(nc);
+    for (int i = 0; i < nc; i++) {
+        uint64_t q[3];
+        for (int a = 0; a < 3; a++) {
+            const double span = hi[a] - lo[a];
+            const double t = span > 0 ? (c[3 * (size_t)i + a] - lo[a]) / span : 0.0;
+            q[a] = (uint64_t)std::min(2097151.0, std::max(0.0, t * 2097151.0));
+        }
+        key[i] = spread(q[0]) | spread(q[1]) << 1 | spread(q[2]) << 2;
+    }
+    perm.resize(nc);
+    const std::vector<int> cp = raw.comp_ptr.empty() ? std::vector<int>{0, nc} : raw.comp_ptr;
+    for (size_t k = 0; k + 1 < cp.size(); k++) {
+        for (int i = cp[k]; i < cp[k + 1]; i++) perm[i] = i;
+        std::stable_sort(perm.begin() + cp[k], perm.begin() + cp[k + 1],
+                         [&](int a, int b) { return key[a] < key[b]; });
+    }
+}
+
+void reorder_cells(RawMesh &raw, const std::vector<int> &perm) {
+    const int nc = raw.nc();
+    std::vector<int> cptr(1, 0), cverts, creg(nc);
+    cverts.reserve(raw.cverts.size());
+    for (int k = 0; k < nc; k++) {
+        const int c = perm[k];
+        for (int j = raw.cptr[c]; j < raw.cptr[c + 1]; j++) cverts.push_back(raw.cverts[j]);
+        cptr.push_back((int)cverts.size());
+        creg[k] = raw.creg[c];
+    }
+    raw.cptr.swap(cptr);
+    raw.cverts.swap(cverts);
+    raw.creg.swap(creg);
+}
+
 Error make_union(const std::vector<RawMesh> &meshes, const std::vector<BCs> &bcs, RawMesh &out, BCs &out_bcs) {
     const int n = (int)meshes.size();
     if (n <= 0 || (int)bcs.size() != n) return {-1, "a batch needs at least one geometry and one BC table each"};

@@ -130,6 +130,10 @@ typedef struct {
                                  ring: 0 = automatic (2048), < 0 = none (such reads go to memory) */
     int direction_batch;      /* most directions whose gradient/residual/correction buffers are held at
                                  once; 0 = automatic (all that fit in device memory) */
+    int cell_order;           /* 0 = automatic: cells are renumbered inside the library along a Morton
+                                 curve of their centres (per geometry of a batch) for memory locality;
+                                 1 = keep the caller's order. Every cell array of this ABI is in the
+                                 caller's order either way; results agree to rounding. */
 } gbte_options;
 
 #define GBTE_NUM_KERNELS 16

@@ -12,10 +12,16 @@
 //           cells writes (the device's level-parallel order).
 // With a copies argument > 1 the check runs on a batch of that many copies
 // of the deck (disjoint union, one level list per copy and direction).
+// With a fifth argument "morton" the cells are first renumbered by the
+// library's locality order; the check then also requires that order to be a
+// permutation inside each copy, and the renumbered mesh to keep the volume,
+// faces and boundary sides of the original. It prints the median index gap
+// between face neighbours before and after ("gap_before", "gap_after").
 // Prints "far_refs <n> far_slots <n> ring <n> max_abs_diff <x>" and exits 1
 // if the sweeps differ or a far reference found neither ring nor slot.
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <cstdlib>
 #include <random>
 #include <string>
@@ -47,9 +53,55 @@ int main(int argc, char **argv) {
         e = gbte::make_union(ms, bs, raw, bcs);
         if (e.code) return std::fprintf(stderr, "union: %s\n", e.msg.c_str()), 2;
     }
+    // median index gap between interior face neighbours
+    auto gap = [](const gbte::FlatMesh &m) {
+        std::vector<int> g;
+        for (int c = 0; c < m.nc; c++)
+            for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++)
+                if (m.cf_nbr[k] >= 0) g.push_back(std::abs(m.cf_nbr[k] - c));
+        if (g.empty()) return 0;
+        std::nth_element(g.begin(), g.begin() + g.size() / 2, g.end());
+        return g[g.size() / 2];
+    };
     gbte::FlatMesh fm;
-    e = gbte::build_flat_mesh(raw, bcs, deck.bands, fm);
-    if (e.code) return std::fprintf(stderr, "mesh: %s\n", e.msg.c_str()), 2;
+    if (argc > 5 && std::string(argv[5]) == "morton") {
+        gbte::FlatMesh f0;
+        e = gbte::build_flat_mesh(raw, bcs, deck.bands, f0);
+        if (e.code) return std::fprintf(stderr, "mesh: %s\n", e.msg.c_str()), 2;
+        std::vector<int> perm;
+        gbte::locality_order(raw, perm);
+        const std::vector<int> cp = raw.comp_ptr.empty() ? std::vector<int>{0, raw.nc()} : raw.comp_ptr;
+        std::vector<char> seen(raw.nc(), 0);
+        for (size_t q = 0; q + 1 < cp.size(); q++)
+            for (int k = cp[q]; k < cp[q + 1]; k++) {
+                const int c = perm[k];
+                if (c < cp[q] || c >= cp[q + 1] || seen[c]) return std::fprintf(stderr, "not a permutation\n"), 1;
+                seen[c] = 1;
+            }
+        gbte::reorder_cells(raw, perm);
+        e = gbte::build_flat_mesh(raw, bcs, deck.bands, fm);
+        if (e.code) return std::fprintf(stderr, "mesh: %s\n", e.msg.c_str()), 2;
+        double v0 = 0, v1 = 0, dv = 0;
+        for (int k = 0; k < fm.nc; k++) {
+            v0 += f0.vol[perm[k]];
+            v1 += fm.vol[k];
+            dv = std::max(dv, std::fabs(fm.vol[k] - f0.vol[perm[k]]));
+        }
+        if (fm.nf() != f0.nf() || fm.nbd() != f0.nbd() || dv > 1e-12 * std::fabs(v0) / fm.nc ||
+            std::fabs(v1 - v0) > 1e-12 * std::fabs(v0))
+            return std::fprintf(stderr, "renumbered mesh differs\n"), 1;
+        for (int b = 0; b < fm.nbd(); b++) {
+            const int s0 = f0.bs_cell[2 * b] >= 0 ? perm[fm.bs_cell[2 * b]] : -1;
+            const int s1 = f0.bs_cell[2 * b + 1] >= 0 ? perm[fm.bs_cell[2 * b + 1]] : -1;
+            const bool same = (s0 == f0.bs_cell[2 * b] && s1 == f0.bs_cell[2 * b + 1]) ||
+                              (s0 == f0.bs_cell[2 * b + 1] && s1 == f0.bs_cell[2 * b]);
+            if (f0.b_type[b] != fm.b_type[b] || !same) return std::fprintf(stderr, "boundary sides differ\n"), 1;
+        }
+        std::printf("gap_before %d gap_after %d ", gap(f0), gap(fm));
+    } else {
+        e = gbte::build_flat_mesh(raw, bcs, deck.bands, fm);
+        if (e.code) return std::fprintf(stderr, "mesh: %s\n", e.msg.c_str()), 2;
+    }
     gbte::Schedule sch;
     gbte::build_schedule(fm, ang, sch, 4);
     gbte::SweepPlan sp;

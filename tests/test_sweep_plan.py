@@ -66,6 +66,20 @@ def test_batch_of_copies_matches_direct_sweep(checker, tmp_path, name):
     assert float(f["max_abs_diff"]) == 0.0
 
 
+@pytest.mark.parametrize("name,copies", [("config2_4bands", 1), ("periodic_jitter", 1), ("porous_msh", 2),
+                                         ("quad_heat_specular", 1)])
+def test_locality_order_keeps_the_mesh(checker, tmp_path, name, copies):
+    # cells renumbered along a Morton curve of their centres (inside each
+    # copy of a batch): same cells, faces and boundary sides, neighbours
+    # closer in memory, and the ring/far-slot sweep still exact
+    _decks()[name].write(str(tmp_path))
+    r = subprocess.run([checker, str(tmp_path), "1", "plain", str(copies), "morton"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    f = dict(zip(r.stdout.split()[0::2], r.stdout.split()[1::2]))
+    assert float(f["max_abs_diff"]) == 0.0
+    assert int(f["gap_after"]) <= max(8, int(f["gap_before"]))
+
+
 def test_planted_wrong_slot_is_caught(checker, tmp_path):
     d = decks.config2_deck(h_nm=3.0, n_bands=4, n_phi=16, seed=0)
     d.write(str(tmp_path))
