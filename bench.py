@@ -405,6 +405,53 @@ def _population_one(i: int, seed: int):
     return decks.porous_population_member(i, seed=seed)
 
 
+def run_config4(args, rank: int):
+    """Adjoint workload: the config-2 cell with a partially specular pore
+    wall (p = 0.3) and log-normal per-cell scattering multipliers (sigma 0.2,
+    seed 2), 40 bands, 64 directions, FP64. The forward solve runs to the
+    given residual from the reference's Tref start; then gbte_vjp gives the
+    gradient of k_x with respect to the 40 band tau multipliers, every cell's
+    multiplier and p. Reported: the adjoint's device time against the
+    forward's (the target is <= 2x) and both iteration counts."""
+    import torch
+
+    import giftbte_b200 as g
+    from giftbte_b200 import decks
+
+    torch.cuda.init()
+    d = decks.config4_deck(h_nm=3.0, n_bands=40, n_phi=16, seed=0, specularity=0.3)
+    nc = d.mesh.n_cells
+    sc = decks.lognormal_scatter(nc, sigma=0.2, seed=2)
+    s = g.StaticBTESynthetic.from_deck(d, precision=g.GBTE_FP64, cell_scatter=sc, max_iter=args.max_iter_e2e)
+    clocks = ClockSampler(0)
+    clocks.start()
+    st = s.solve(err_temp=args.adj_residual, err_flux=args.adj_residual, max_iter=args.max_iter_e2e)
+    qb = s.keff_cotangent(axis=0, length=300e-9, delta_T=1.0)
+    a = s.vjp(q_bar=qb, tol=args.adj_residual)
+    clk = clocks.stop()
+    keff = float(np.sum(qb * s.fields()["q"]))
+    nb, nd = s.num_bands, s.num_directions
+    s.close()
+    fwd_ms, adj_ms = st["solve_ms"], a["stats"]["vjp_ms"]
+    adj_updates = a["stats"]["iterations"] * nb * nd * nc
+    return {
+        "metric": "adjoint band*dir*cell updates/s (gradient of k_x; adjoint time over forward time alongside)",
+        "value": adj_updates / (adj_ms * 1e-3), "unit": "updates/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+        "ms_per_step": adj_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: seeded mesh, band table and multiplier field generated in-process (no dataset)",
+        "config": {"workload": f"config-2 cell with a partially specular pore wall p=0.3, log-normal cell "
+                               f"scattering multipliers sigma 0.2 seed 2 ({nc} triangles), 40 bands, 64 directions",
+                   "residual": args.adj_residual, "objective": "k_x"},
+        "forward": {"ms": fwd_ms, "iterations": st["iterations"]},
+        "adjoint": {"ms": adj_ms, "iterations": a["stats"]["iterations"], "change": a["stats"]["change"],
+                    "picard_steps": a["stats"]["picard_steps"]},
+        "adjoint_over_forward": adj_ms / fwd_ms, "k_x": keff,
+        "grad_norms": {"tau": float(np.linalg.norm(a["tau"])), "scatter": float(np.linalg.norm(a["scatter"])),
+                       "specularity": float(a["specularity"][[b.tag for b in d.bcs].index(5)])},
+        "gpu_launches": int(st["kernel_launches"]), "clocks": clk,
+    }
+
+
 def run_config5(args, rank: int):
     """Batched solve of 256 independent porous cells (one handle over their
     disjoint union: one launch per kernel stage for all cells, the sweep's
@@ -466,7 +513,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
-    ap.add_argument("--workload", choices=["config2", "config1", "config3", "config5"], default="config2")
+    ap.add_argument("--workload", choices=["config2", "config1", "config3", "config4", "config5"], default="config2")
+    ap.add_argument("--adj-residual", type=float, default=1e-10, help="config4: forward margins and adjoint tolerance")
     ap.add_argument("--batch", type=int, default=256, help="config5: number of independent cells")
     ap.add_argument("--h-nm", type=float, default=0.0, help="config3 mesh spacing (default 2.5 nm)")
     ap.add_argument("--cell-order", type=int, choices=[0, 1], default=0,
@@ -491,6 +539,10 @@ def main():
     if args.workload == "config5":
         if rank == 0:
             print(json.dumps(run_config5(args, rank)), flush=True)
+        return
+    if args.workload == "config4":
+        if rank == 0:
+            print(json.dumps(run_config4(args, rank)), flush=True)
         return
     if world > 1:
         import datetime

@@ -66,7 +66,7 @@ class Options(ctypes.Structure):
                 ("stream", ctypes.c_void_p), ("device", ctypes.c_int), ("verbose", ctypes.c_int),
                 ("macro_rtol", ctypes.c_double), ("profile", ctypes.c_int), ("sweep_bands", ctypes.c_int),
                 ("sweep_far_slots", ctypes.c_int), ("direction_batch", ctypes.c_int),
-                ("cell_order", ctypes.c_int)]
+                ("cell_scatter", _c_dbl_p), ("cell_order", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -92,6 +92,11 @@ class Stats(ctypes.Structure):
         return d
 
 
+class VjpStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("picard_steps", ctypes.c_int), ("change", ctypes.c_double),
+                ("vjp_ms", ctypes.c_double)]
+
+
 class DeckInfo(ctypes.Structure):
     _fields_ = [("dimension", ctypes.c_int), ("num_nodes", ctypes.c_int), ("num_cells", ctypes.c_int),
                 ("num_faces", ctypes.c_int), ("num_boundaries", ctypes.c_int),
@@ -110,7 +115,8 @@ class DeckInfo(ctypes.Structure):
 EXPORTS = ["gbte_inspect_deck", "gbte_inspect_mesh", "gbte_default_options", "gbte_create", "gbte_create_from_deck", "gbte_set_initial",
            "gbte_fourier_initial", "gbte_solve", "gbte_get_fields", "gbte_write_outputs", "gbte_get_sizes",
            "gbte_get_geometry", "gbte_last_error", "gbte_status_string", "gbte_destroy", "gbte_kernel_name",
-           "gbte_solve_with", "gbte_fourier_initial_noalloc", "gbte_batch_create", "gbte_batch_geometries"]
+           "gbte_solve_with", "gbte_fourier_initial_noalloc", "gbte_batch_create", "gbte_batch_geometries",
+           "gbte_vjp"]
 
 _lib = None
 
@@ -147,6 +153,8 @@ def library():
                                           ctypes.POINTER(BCTable), ctypes.POINTER(AngleSpec),
                                           ctypes.POINTER(Options), ctypes.POINTER(ctypes.c_void_p)]
         lib.gbte_batch_geometries.argtypes = [ctypes.c_void_p, _c_int_p, _c_int_p]
+        lib.gbte_vjp.argtypes = [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, ctypes.c_int, ctypes.c_double, _c_dbl_p,
+                                 _c_dbl_p, _c_dbl_p, ctypes.POINTER(VjpStats)]
         lib.gbte_inspect_deck.argtypes = [ctypes.c_char_p, ctypes.POINTER(DeckInfo)]
         lib.gbte_inspect_mesh.argtypes = [ctypes.POINTER(MeshView), ctypes.POINTER(BandTableC),
                                           ctypes.POINTER(BCTable), ctypes.POINTER(AngleSpec),
@@ -186,6 +194,7 @@ class StaticBTESynthetic:
         self.num_cells, self.num_bands, self.num_directions, self.num_boundary_sides = (
             nc.value, nb.value, nd.value, nbs.value)
         self.stats: Optional[dict] = None
+        self._n_bc_rows = 0  # boundary-table rows given at creation (known for in-memory decks)
 
     # --- construction -----------------------------------------------------
     @classmethod
@@ -201,8 +210,11 @@ class StaticBTESynthetic:
 
     @classmethod
     def from_deck(cls, deck, precision: int = GBTE_FP64, device: int = 0, verbose: int = 0,
-                  cell_heat: Optional[np.ndarray] = None, **opt) -> "StaticBTESynthetic":
-        """Build from a :class:`giftbte_b200.decks.Deck` held in memory."""
+                  cell_heat: Optional[np.ndarray] = None, cell_scatter: Optional[np.ndarray] = None,
+                  **opt) -> "StaticBTESynthetic":
+        """Build from a :class:`giftbte_b200.decks.Deck` held in memory.
+        ``cell_scatter`` (per cell, > 0) multiplies the scattering rate of
+        each cell in the transport (no counterpart in the reference)."""
         lib = library()
         v = _views(deck)
         nc = deck.mesh.n_cells
@@ -213,12 +225,17 @@ class StaticBTESynthetic:
         kw.update(opt)
         o = default_options(precision, device=device, verbose=verbose, **kw)
         o.cell_heat = _ptr(heat, ctypes.c_double)
+        scat = np.ascontiguousarray(cell_scatter, dtype=np.float64) if cell_scatter is not None else None
+        if scat is not None and scat.shape != (nc,):
+            raise ValueError("cell_scatter needs one value per cell")
+        o.cell_scatter = _ptr(scat, ctypes.c_double)
         h = ctypes.c_void_p()
         rc = lib.gbte_create(ctypes.byref(v["mv"]), ctypes.byref(v["bt"]), ctypes.byref(v["bc"]),
                              ctypes.byref(v["an"]), ctypes.byref(o), ctypes.byref(h))
         if rc != GBTE_OK:
             raise GBTEError(rc, lib.gbte_last_error(None).decode())
         s = cls(h)
+        s._n_bc_rows = len(deck.bcs)
         s.set_initial(np.full(nc, deck.tref))
         return s
 
@@ -343,6 +360,37 @@ class StaticBTESynthetic:
         c = np.zeros(3 * nc); v = np.zeros(nc)
         self._check(library().gbte_get_geometry(self._h, _ptr(c, ctypes.c_double), _ptr(v, ctypes.c_double)))
         return c.reshape(nc, 3), v
+
+    def vjp(self, T_bar: Optional[np.ndarray] = None, q_bar: Optional[np.ndarray] = None, max_iter: int = 10000,
+            tol: float = 1e-12) -> dict:
+        """Gradient of J = <T_bar, T> + <q_bar, q> at the fixed point the last
+        solve reached (gbte_vjp): ``tau`` (per band, multiplier on its
+        relaxation time), ``scatter`` (per cell, its scattering multiplier),
+        ``specularity`` (per boundary-table row; partially specular rows)."""
+        nc, nb = self.num_cells, self.num_bands
+        Tb = np.ascontiguousarray(T_bar, dtype=np.float64) if T_bar is not None else None
+        qb = np.ascontiguousarray(q_bar, dtype=np.float64).reshape(-1) if q_bar is not None else None
+        if Tb is not None and Tb.shape != (nc,):
+            raise ValueError("T_bar needs one value per cell")
+        if qb is not None and qb.shape != (3 * nc,):
+            raise ValueError("q_bar needs three values per cell")
+        g_tau = np.zeros(nb)
+        g_cell = np.zeros(nc)
+        g_spec = np.zeros(self._n_bc_rows) if self._n_bc_rows else None
+        st = VjpStats()
+        self._check(library().gbte_vjp(self._h, _ptr(Tb, ctypes.c_double), _ptr(qb, ctypes.c_double), int(max_iter),
+                                       float(tol), _ptr(g_tau, ctypes.c_double), _ptr(g_cell, ctypes.c_double),
+                                       _ptr(g_spec, ctypes.c_double), ctypes.byref(st)))
+        return {"tau": g_tau, "scatter": g_cell, "specularity": g_spec,
+                "stats": {k: getattr(st, k) for k, _ in st._fields_}}
+
+    def keff_cotangent(self, axis: int = 0, length: float = 1.0, delta_T: float = 1.0) -> np.ndarray:
+        """q_bar of the effective conductivity k = <q_axis>_V length / delta_T
+        (volume average of the heat flux over the domain)."""
+        _, vol = self.geometry()
+        qb = np.zeros((self.num_cells, 3))
+        qb[:, axis] = vol / vol.sum() * length / delta_T
+        return qb
 
     def write_outputs(self, path: str) -> None:
         self._check(library().gbte_write_outputs(self._h, path.encode()))

@@ -24,6 +24,7 @@ struct gbte_handle {
     double setup_ms = 0;
     // cell order: internal cell k is the caller's cell perm[k]; empty = same order
     std::vector<int> perm;
+    std::vector<int> bc_tags;  // tags of the boundary table's rows, in its order
     // caller's array of nc rows of w values -> internal order
     std::vector<double> to_internal(const double *user, int w) const {
         const size_t nc = perm.size();
@@ -117,6 +118,8 @@ int create_common(const gbte::RawMesh &raw_in, const gbte::Bands &bands_in, cons
     if (e.code) return fail(nullptr, e), status_of(e.code);
     if (opt.cell_order != 0 && opt.cell_order != 1)
         return fail(nullptr, {-1, "cell_order must be 0 (automatic) or 1 (caller's order)"}), GBTE_ERR_ARG;
+    std::vector<double> scatter;
+    if (opt.cell_scatter) scatter.assign(opt.cell_scatter, opt.cell_scatter + raw_in.nc());
     const gbte::RawMesh *rp = &raw_in;
     gbte::RawMesh reordered;
     std::vector<double> heat = cell_heat;
@@ -126,6 +129,7 @@ int create_common(const gbte::RawMesh &raw_in, const gbte::Bands &bands_in, cons
         gbte::reorder_cells(reordered, h->perm);
         rp = &reordered;
         if (!heat.empty()) heat = h->to_internal(cell_heat.data(), 1);
+        if (!scatter.empty()) scatter = h->to_internal(scatter.data(), 1);
     }
     const gbte::RawMesh &raw = *rp;
     gbte::FlatMesh fm;
@@ -143,12 +147,14 @@ int create_common(const gbte::RawMesh &raw_in, const gbte::Bands &bands_in, cons
     cfg.sweep_bands = opt.sweep_bands;
     cfg.sweep_far_slots = opt.sweep_far_slots;
     cfg.direction_batch = opt.direction_batch;
+    cfg.cell_scatter = scatter;
     cfg.device = opt.device;
     cfg.stream = (cudaStream_t)opt.stream;
     if (opt.precision != GBTE_FP64 && opt.precision != GBTE_FP32_MIXED)
         return fail(nullptr, {-1, "precision must be GBTE_FP64 or GBTE_FP32_MIXED"}), GBTE_ERR_ARG;
     e = h->solver.init(fm, bands, ang, heat, cfg);
     if (e.code) return fail(nullptr, e), status_of(e.code);
+    h->bc_tags = bcs.tag;
     h->setup_ms = now_ms() - t0;
     *out = h.release();
     return GBTE_OK;
@@ -611,6 +617,46 @@ int gbte_write_outputs(gbte_handle *h, const char *dir) {
     for (int c = 0; c < nc; c++) f << q[3 * c] << " " << q[3 * c + 1] << " " << q[3 * c + 2] << "\n";
     f.close();
     return GBTE_OK;
+}
+
+int gbte_vjp(gbte_handle *h, const double *T_bar, const double *q_bar, int max_iter, double tol, double *grad_tau,
+             double *grad_scatter, double *grad_specularity, gbte_vjp_stats *st) {
+    if (!h) return GBTE_ERR_ARG;
+    try {
+        const gbte::FlatMesh &m = h->solver.mesh;
+        std::vector<double> Tb, qb, gc(grad_scatter ? m.nc : 0), gb(m.nbd());
+        if (!h->perm.empty()) {
+            if (T_bar) Tb = h->to_internal(T_bar, 1), T_bar = Tb.data();
+            if (q_bar) qb = h->to_internal(q_bar, 3), q_bar = qb.data();
+        }
+        gbte::VjpStats vs;
+        gbte::Error e = h->solver.vjp(T_bar, q_bar, max_iter, tol, grad_tau, grad_scatter ? gc.data() : nullptr,
+                                      gb.data(), vs);
+        if (e.code) return fail(h, e), status_of(e.code);
+        if (grad_scatter) {
+            std::memcpy(grad_scatter, gc.data(), gc.size() * sizeof(double));
+            if (!h->perm.empty()) h->to_user(grad_scatter, 1);
+        }
+        if (grad_specularity) {
+            for (size_t r = 0; r < h->bc_tags.size(); r++) grad_specularity[r] = 0;
+            for (int ib = 0; ib < m.nbd(); ib++)
+                for (size_t r = 0; r < h->bc_tags.size(); r++)
+                    if (h->bc_tags[r] == m.b_tag[ib]) grad_specularity[r] += gb[ib];
+        }
+        if (st) {
+            st->iterations = vs.iterations;
+            st->picard_steps = vs.picard_steps;
+            st->change = vs.change;
+            st->vjp_ms = vs.ms;
+        }
+        return GBTE_OK;
+    } catch (const std::bad_alloc &) {
+        h->err = "host allocation failed";
+        return GBTE_ERR_NOMEM;
+    } catch (const std::exception &ex) {
+        h->err = ex.what();
+        return GBTE_ERR_ARG;
+    }
 }
 
 const char *gbte_kernel_name(int i) { return gbte::kernel_name(i); }

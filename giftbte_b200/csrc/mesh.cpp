@@ -311,6 +311,14 @@ Error build_flat_mesh(const RawMesh &raw, const BCs &bcs, const Bands &bands, Fl
     for (int ib = 0; ib < nbd; ib++) {
         m.b_type[ib] = types[b_row[ib]];
         m.b_T[ib] = vals[b_row[ib]];
+        if (m.b_type[ib] == 6) {
+            // partially specular wall, value = specularity p: the ends of the
+            // range are the diffuse (2) and specular (3) walls themselves
+            if (!(m.b_T[ib] >= 0 && m.b_T[ib] <= 1))
+                return {-1, "partially specular wall (type 6): the specularity must lie in [0, 1]"};
+            if (m.b_T[ib] == 0) m.b_type[ib] = 2;
+            else if (m.b_T[ib] == 1) m.b_type[ib] = 3;
+        }
         m.b_tag[ib] = tags[b_row[ib]];
         for (int ic = 0; ic < (int)b_sides[ib].size(); ic++) {
             int c = b_sides[ib][ic].first, k = m.cf_ptr[c] + b_sides[ib][ic].second;

@@ -162,7 +162,7 @@ struct EView {
     }
 };
 
-// R = C_b T_old + Q hr tau - e - sum_f tau (v.n) A/V x_f  (second-order upwind
+// R = C_b T_old + Q hr tau_c - e - sum_f tau_c (v.n) A/V x_f, tau_c = tau / s_c  (second-order upwind
 // x_f), written in the direction's level order Rlo[d][pos][b] so that the
 // sweep reads each level as one contiguous block
 template <typename S, int DIM>
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(256) k_residual(DMesh m, DPhys p, EView<S, DIM
         const double Cb = p.C[b], tau = p.tau[b], vm = p.vmag[b];
         const double vx = vm * p.sx[d], vy = vm * p.sy[d], vz = vm * p.sz[d];
         const double ec = ev.e(d, c, b, Cb);
-        const double cx = m.cx[c], cy = m.cy[c], cz = m.cz[c], tv = tau / m.vol[c];
+        const double cx = m.cx[c], cy = m.cy[c], cz = m.cz[c], tsc = m.tsc[c], tv = tau * tsc / m.vol[c];
         double acc = 0;
         for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
             const double vn = vx * m.cf_nx[k] + vy * m.cf_ny[k] + (DIM == 3 ? vz * m.cf_nz[k] : vz * 0.0);
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(256) k_residual(DMesh m, DPhys p, EView<S, DIM
             }
             acc += tv * m.cf_area[k] * vn * x;
         }
-        const double r = Cb * Told[c] + m.heat[c] * p.hr[b] * tau - ec - acc;
+        const double r = Cb * Told[c] + m.heat[c] * p.hr[b] * tau * tsc - ec - acc;
         Rlo[((d - d0) * nc + pos_of[dc]) * nb + b] = (S)r;
     }
 }
@@ -280,7 +280,8 @@ __global__ void __launch_bounds__(256) k_gradient8(DMesh m, DPhys p, const S *__
 }
 
 // Band-independent part of the face fluxes of the FP32 form's base field:
-// B[d][c] = sum_f A_f/V (s.n_f) beta_f, beta_f the second-order upwind face
+// B[d][c] = (1/s_c) sum_f A_f/V (s.n_f) beta_f (s_c the cell's scattering
+// multiplier, 1 by default), beta_f the second-order upwind face
 // value of T_base (T_base + grad T_base . r from the upwind cell; T_base of
 // the cell itself on boundary inflow faces). With it the residual's band
 // loop only handles the stored deviations. Zero in the FP64 form, whose
@@ -294,7 +295,7 @@ __global__ void __launch_bounds__(256) k_base_flux(DMesh m, DPhys p, const doubl
         const int c = (int)(t % nc);
         const size_t d = t / nc;
         const double sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
-        const double invV = 1.0 / m.vol[c];
+        const double invV = m.tsc[c] / m.vol[c];
         double acc = 0;
         for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
             const double sn = sx * m.cf_nx[k] + sy * m.cf_ny[k] + (DIM == 3 ? sz * m.cf_nz[k] : 0.0);
@@ -318,8 +319,8 @@ __global__ void __launch_bounds__(256) k_base_flux(DMesh m, DPhys p, const doubl
 
 // Residual, BC bands per thread, in the storage precision S on the stored
 // deviations eps = e - C_b T_base (the base part enters through B):
-//   R = C_b (T_old - T_base - tau|v| B) + Q hr tau
-//       - eps_c - tau|v| sum_f A_f/V (s.n_f) y_f
+//   R = C_b (T_old - T_base - tau|v| B) + Q hr tau / s_c
+//       - eps_c - tau|v| / s_c sum_f A_f/V (s.n_f) y_f
 // with y_f the deviation of the second-order upwind face value
 // (eps + g . r of the upwind cell; e_wall - C_b T_base on boundary inflow
 // faces). The first two terms are formed in FP64 and rounded once. The
@@ -341,7 +342,7 @@ __global__ void __launch_bounds__(256, sizeof(S) == 4 ? 4 : 2) k_residual8(DMesh
         const double sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
         const size_t dbase = d * nc, gbase = (d - d0) * nc;  // all directions / this batch
         S ec[BC], acc[BC], gxv[BC], gyv[BC], gzv[BC];
-        const double invV = 1.0 / m.vol[c], tb = ev.Tb[c];
+        const double tsc = m.tsc[c], invV = tsc / m.vol[c], tb = ev.Tb[c];
         ld8(ev.eps + (dbase + c) * nb + b0, ec);
 #pragma unroll
         for (int i = 0; i < BC; i++) acc[i] = (S)0;
@@ -387,7 +388,7 @@ __global__ void __launch_bounds__(256, sizeof(S) == 4 ? 4 : 2) k_residual8(DMesh
                 for (int i = 0; i < BC; i++) acc[i] += a * (S)(e[i] - p.C[b0 + i] * tb);
             }
         }
-        const double dT = Told[c] - tb, B = Bf[dc], hc = m.heat[c];
+        const double dT = Told[c] - tb, B = Bf[dc], hc = m.heat[c] * tsc;
         S out[BC];
 #pragma unroll
         for (int i = 0; i < BC; i++) {
@@ -819,7 +820,7 @@ __global__ void k_diffuse_sum(DMesh m, DPhys p, const double *__restrict__ dif_w
     const size_t total = (size_t)m.nbs * nb;
     for (size_t t = gtid(); t < total; t += gstride()) {
         const int b = (int)(t % nb), s = (int)(t / nb);
-        if (m.bs_cell[s] < 0 || m.b_type[s >> 1] != 2) continue;
+        if (m.bs_cell[s] < 0 || (m.b_type[s >> 1] != 2 && m.b_type[s >> 1] != 6)) continue;
         double acc = 0;
         const double *w = dif_w + (size_t)s * p.nd;
         for (int q = 0; q < p.nd; q++) {
@@ -855,6 +856,11 @@ __global__ void k_gather(DMesh m, DPhys p, const double *__restrict__ dsum, cons
             const int src = spec_src[(size_t)s * p.nd + d];
             const double *from = snap ? snap : eb;
             val = from[((size_t)src * m.nbs + s) * nb + b];
+        } else if (type == 6) {
+            // p specular + (1 - p) diffuse, p = the wall's specularity
+            const double pr = m.b_T[ib];
+            const int src = spec_src[(size_t)s * p.nd + d];
+            val = pr * eb[((size_t)src * m.nbs + s) * nb + b] + (1.0 - pr) * dsum[(size_t)s * nb + b];
         } else if (type < 0) {
             const int cb = m.b_connect[ib];
             const int ps = 2 * cb + (s & 1);
@@ -1519,7 +1525,13 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
         return {-8, "more than one material is not supported by this solver (interfaces between materials)"};
     if (cfg.use_limiter) return {-8, "Order=2limit (gradient limiter) is not supported by this solver"};
     for (int t : mesh.b_type)
-        if (!(t == 1 || t == 2 || t == 3 || t < 0)) return {-8, "boundary type " + std::to_string(t) + " is not supported"};
+        if (!(t == 1 || t == 2 || t == 3 || t == 6 || t < 0))
+            return {-8, "boundary type " + std::to_string(t) + " is not supported"};
+    if (!cfg.cell_scatter.empty()) {
+        if ((int)cfg.cell_scatter.size() != mesh.nc) return {-1, "cell_scatter must hold one value per cell"};
+        for (double v : cfg.cell_scatter)
+            if (!(v > 0) || !std::isfinite(v)) return {-1, "cell_scatter values must be positive and finite"};
+    }
     int ndev = 0;
     CUDA_TRY(cudaGetDeviceCount(&ndev));
     if (cfg.device < 0 || cfg.device >= ndev) return {-1, "CUDA device ordinal out of range"};
@@ -1565,6 +1577,9 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
     std::vector<double> heat = cell_heat;
     heat.resize(mesh.nc, 0.0);
     d.heat = up_d(heat);
+    std::vector<double> tsc(mesh.nc, 1.0);
+    for (size_t i = 0; i < cfg.cell_scatter.size(); i++) tsc[i] = 1.0 / cfg.cell_scatter[i];
+    d.tsc = up_d(tsc);
     d.nbr_ptr = up_i(mesh.nbr_ptr);
     d.nbr_idx = up_i(mesh.nbr_idx);
     d.lsq_w = up_d(mesh.lsq_w);
@@ -1639,7 +1654,14 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
             recf.assign((size_t)nd * nc2, SweepRec<float>{});
         else
             recd.assign((size_t)nd * nc2, SweepRec<double>{});
+        // a per-cell relaxation-time scale 1/s_c multiplies row c of the
+        // upwind operator: the record's coefficients and outgoing sum
+        std::vector<double> rs(nc2, 1.0);
+        for (size_t i = 0; i < cfg.cell_scatter.size(); i++) rs[i] = 1.0 / cfg.cell_scatter[i];
         for (size_t P = 0; P < (size_t)nd * nc2; P++) {
+            const double f = rs[sp.cell[P]];
+            for (int q = 0; q < 4; q++) sp.a[4 * P + q] *= f;
+            sp.sig[P] *= f;
             const int meta = sp.nin[P] | ((sp.far_w[P] + 1) << 3);
             if (f32) {
                 SweepRec<float> &r = recf[P];
@@ -1693,7 +1715,7 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
         int k = mesh.bs_cf[sd];
         int type = mesh.b_type[sd >> 1];
         double nx = mesh.cf_nx[k], ny = mesh.cf_ny[k], nz = mesh.cf_nz[k];
-        if (type == 2) {
+        if (type == 2 || type == 6) {
             double tot = 0;
             for (int q = 0; q < nd; q++) {
                 double dn = ang.sx[q] * nx + ang.sy[q] * ny + ang.sz[q] * nz;
@@ -1703,7 +1725,8 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
                 double dn = ang.sx[q] * nx + ang.sy[q] * ny + ang.sz[q] * nz;
                 if (dn >= 0) difw[(size_t)sd * nd + q] = dn * ang.w[q] / tot;
             }
-        } else if (type == 3) {
+        }
+        if (type == 3) {
             std::vector<int> res(nd, -1);
             std::vector<char> old_incoming(nd, 0);
             for (int q = 0; q < nd; q++) {
@@ -1737,6 +1760,30 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
                 if (old_incoming[q]) need_snapshot_ = true;
             }
             for (int q = 0; q < nd; q++) spec[(size_t)sd * nd + q] = res[q];
+        } else if (type == 6) {
+            // partially specular wall: the specular part of an incoming
+            // direction comes from the outgoing direction nearest to its
+            // mirror image (so it never reads another incoming value)
+            for (int q = 0; q < nd; q++) {
+                double d1 = ang.sx[q] * nx + ang.sy[q] * ny + ang.sz[q] * nz;
+                if (d1 >= 0) {
+                    spec[(size_t)sd * nd + q] = q;
+                    continue;
+                }
+                double rx = ang.sx[q] - nx * d1 * 2, ry = ang.sy[q] - ny * d1 * 2, rz = ang.sz[q] - nz * d1 * 2;
+                double close = 1e300;
+                int nf = -1;
+                for (int t = 0; t < nd; t++) {
+                    if (ang.sx[t] * nx + ang.sy[t] * ny + ang.sz[t] * nz < 0) continue;
+                    double l = std::pow(rx - ang.sx[t], 2) + std::pow(ry - ang.sy[t], 2) + std::pow(rz - ang.sz[t], 2);
+                    if (l < close) {
+                        nf = t;
+                        close = l;
+                    }
+                }
+                if (nf < 0) return {-8, "partially specular wall: no outgoing quadrature direction"};
+                spec[(size_t)sd * nd + q] = nf;
+            }
         }
     }
     dif_w_ = up_d(difw);
@@ -2569,6 +2616,7 @@ Error Solver::solve_t(SolveStats &st) {
             if (cfg.verbose) printf("internal residual: %.17g\n", internal);
         }
         st.inner_iterations = inner;
+        last_inner_ = inner;
         CUDA_TRY(cudaEventRecord(ev_[2], s));
         // margins
         CUDA_TRY(cudaMemsetAsync(red_, 0, 4 * 8 * (size_t)ncomp_, s));
@@ -2753,6 +2801,788 @@ Error Solver::fourier_initial_noalloc() {
     started_ = false;
     last_margin_ = 1.0;
     std::fill(warm_ok_.begin(), warm_ok_.end(), 0);
+    return {0, ""};
+}
+
+
+// ------------------------------------------------------------ adjoint (VJP) --
+//
+// The converged outer iteration is a fixed point F(e) = 0 of the FP64 form,
+// affine in the band intensities e:
+//   F(e) = C_b T*(e) + Q hr tau_c - e - tau_c/V sum_f A (v.n) x_f(e, G e, eb_in)
+// with G the LSQ gradient, x_f the second-order upwind face value, eb_in the
+// incoming wall values (gathered from the outgoing ones, themselves
+// extrapolated from e and G e) and T* = P^N(T_lat(e)) the macro temperature
+// after the N Picard steps of the synthetic correction, each
+//   T_{k+1} = Kneg^{-1} (-r_k),  r_k = remacro(e, eb) - heat V
+//             - sum_wall kappa A/(n.a) bTm(eb) - kappa sum_f A a2 . t_f(TV(T_k)).
+// For an objective J = <Tbar, T*> + <qbar, q(e)> the adjoint state lambda
+// solves (dF/de)^T lambda + dJ/de = 0. It is found by the transposed source
+// iteration lambda += A^-T [(dF/de)^T lambda + dJ/de], A the first-order
+// upwind operator of each direction, whose transpose is a sweep in the
+// opposite direction: A_s^T = D A_{-s} D^-1, D = diag(V_c s_c). That
+// iteration has the spectrum of the forward one, so it converges at the
+// forward's rate. Then dJ/dtheta = lambda^T dF/dtheta + <Tbar, dT*/dtheta>:
+//   tau multiplier of band b:  sum lambda (e - C_b T*) (residual) plus the
+//                              synthetic correction's kappa_bulk and tensor
+//                              moment, both proportional to tau_b
+//   cell multiplier s_c:       -(1/s_c) sum lambda (e - C_b T*)
+//   specularity p of a wall:   sum over its incoming entries of
+//                              ebar_in (e_mirror - e_diffuse)
+// Every kernel below is the transpose of a forward kernel named beside it.
+namespace {
+
+__global__ void k_adj_axpy(const double *__restrict__ x, double *__restrict__ y, int n) {
+    const int i = (int)gtid();
+    if (i < n) y[i] += x[i];
+}
+__global__ void k_adj_neg(const double *__restrict__ x, double *__restrict__ y, int n) {
+    const int i = (int)gtid();
+    if (i < n) y[i] = -x[i];
+}
+
+// transpose of the side-moment and wall-temperature reads of one wall entry
+// (k_side_moments, k_macro_bc): the cotangent of eb[d][s][b]
+__device__ __forceinline__ double adj_side_entry(const DMesh &m, const DPhys &p, int d, int s, int b,
+                                                 const double *Thsbar, const double *Qsbar, const double *bTmbar) {
+    const double w = p.w[d], Cb = p.C[b];
+    double v = p.lat[b] * w / Cb * bTmbar[s];
+    if (p.hr[b] > 0) {
+        const double sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
+        const double f = w * p.tau[b] * p.vmag[b] * p.vmag[b];
+        const double *q = Qsbar + 6 * (size_t)s;
+        v += p.kappa * p.lat[b] * w / Cb * Thsbar[s] +
+             f * (q[0] * sx * sx + q[1] * sx * sy + q[2] * sx * sz + q[3] * sy * sy + q[4] * sy * sz + q[5] * sz * sz);
+    }
+    return v;
+}
+
+// adds coef . d(tangential gradient of face k)/d(node values) into out
+// (transpose of tangential())
+__device__ __forceinline__ void tangential_T(const DMesh &m, int k, double cx_, double cy_, double cz_, double *out,
+                                             int stride, int comp) {
+    if (m.dim == 2) {
+        const int v0 = m.cf_v[3 * k], v1 = m.cf_v[3 * k + 1];
+        const double mx = m.node_x[v1] - m.node_x[v0], my = m.node_y[v1] - m.node_y[v0];
+        const double a = (cx_ * mx + cy_ * my) / (mx * mx + my * my);
+        atomicAdd(&out[(size_t)v1 * stride + comp], a);
+        atomicAdd(&out[(size_t)v0 * stride + comp], -a);
+    } else {
+        const int f = m.cf_face[k];
+        const int k0 = m.f_cf0[f];
+        const double *W = m.face_w + 9 * (size_t)f;
+        for (int t = 0; t < 2; t++) {
+            const int j = t + 1;
+            const double u = (cx_ * W[j] + cy_ * W[3 + j] + cz_ * W[6 + j]) * m.inv_Lx;
+            const int a = m.cf_v[3 * k0 + t + 1], b = m.cf_v[3 * k0 + t];
+            atomicAdd(&out[(size_t)a * stride + comp], u);
+            atomicAdd(&out[(size_t)b * stride + comp], -u);
+        }
+    }
+}
+
+// Tbar[c] = Tuser[c] + sum_{d,b} C_b lam[d][c][b]  (the C_b T* term of F)
+__global__ void k_adj_tbar(DMesh m, DPhys p, const double *__restrict__ lam, const double *__restrict__ Tuser,
+                           double *__restrict__ Tbar) {
+    const int c = (int)(gtid() >> 5), lane = threadIdx.x & 31;
+    if (c >= m.nc) return;
+    const int n = p.nd * p.nb;
+    double acc = 0;
+    for (int i = lane; i < n; i += 32) {
+        const int d = i / p.nb, b = i % p.nb;
+        acc += p.C[b] * lam[((size_t)d * m.nc + c) * p.nb + b];
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) Tbar[c] = acc + (Tuser ? Tuser[c] : 0.0);
+}
+
+// one reverse Picard step (transpose of k_tinterp + k_macro_rhs's
+// non-orthogonal term): TVbar += kappa A a2 z_c through the tangential gradient
+__global__ void k_adj_macro_tv(DMesh m, double kappa, const double *__restrict__ z, double *TVbar) {
+    const int c = (int)gtid();
+    if (c >= m.nc) return;
+    const double zc = z[c];
+    for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+        const double nx = m.cf_nx[k], ny = m.cf_ny[k], nz = m.cf_nz[k], A = m.cf_area[k];
+        const int bnd = m.cf_bound[k];
+        double ax, ay, az;
+        if (bnd >= 0) {
+            if (m.b_type[bnd] == 3) continue;
+            ax = m.cf_fx[k] - m.cx[c];
+            ay = m.cf_fy[k] - m.cy[c];
+            az = m.cf_fz[k] - m.cz[c];
+        } else {
+            const int j = m.cf_nbr[k];
+            ax = m.cx[j] - m.cx[c];
+            ay = m.cy[j] - m.cy[c];
+            az = m.cz[j] - m.cz[c];
+        }
+        const double an = ax * nx + ay * ny + az * nz;
+        const double f = kappa * A * zc;
+        tangential_T(m, k, f * (nx - ax / an), f * (ny - ay / an), f * (nz - az / an), TVbar, 1, 0);
+    }
+}
+
+// transpose of k_tinterp: Tbar[c] += sum_i nt_w TVbar[i]
+__global__ void k_adj_tinterp(DMesh m, const double *__restrict__ TVbar, double *Tbar) {
+    const int i = (int)gtid();
+    if (i >= m.nslot) return;
+    const double v = TVbar[i];
+    if (v == 0) return;
+    for (int k = m.nt_ptr[i]; k < m.nt_ptr[i + 1]; k++) atomicAdd(&Tbar[m.nt_src[k]], m.nt_w[k] * v);
+}
+
+// wall temperatures' cotangent (transpose of k_macro_rhs's wall term);
+// overridden (periodic jump) sides are constants
+__global__ void k_adj_bTm(DMesh m, double kappa, const double *__restrict__ zsum, const double *__restrict__ ovr,
+                          double *__restrict__ bTmbar) {
+    const int s = (int)gtid();
+    if (s >= m.nbs) return;
+    double v = 0;
+    const int c = m.bs_cell[s];
+    if (c >= 0 && m.b_type[s >> 1] != 3 && !(ovr[s] == ovr[s])) {
+        const int k = m.bs_cf[s];
+        const double ax = m.cf_fx[k] - m.cx[c], ay = m.cf_fy[k] - m.cy[c], az = m.cf_fz[k] - m.cz[c];
+        v = kappa * m.cf_area[k] / (m.cf_nx[k] * ax + m.cf_ny[k] * ay + m.cf_nz[k] * az) * zsum[c];
+    }
+    bTmbar[s] = v;
+}
+
+// transpose of k_remacro: cotangent rbar of ReMacro to (Th, Q) of cells and
+// wall sides and (ThV, QV) of nodes
+__global__ void k_adj_remacro(DMesh m, const double *__restrict__ rbar, double *Thbar, double *Qbar, double *Thsbar,
+                              double *Qsbar, double *ThVbar, double *QVbar) {
+    const int c = (int)gtid();
+    if (c >= m.nc) return;
+    const double rho = rbar[c];
+    if (rho == 0) return;
+    for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+        const double nx = m.cf_nx[k], ny = m.cf_ny[k], nz = m.cf_nz[k], A = m.cf_area[k];
+        double rx, ry, rz, *thn, *qn;
+        const int bnd = m.cf_bound[k];
+        if (bnd < 0) {
+            const int j = m.cf_nbr[k];
+            rx = m.cx[j] - m.cx[c];
+            ry = m.cy[j] - m.cy[c];
+            rz = m.cz[j] - m.cz[c];
+            thn = &Thbar[j];
+            qn = &Qbar[6 * (size_t)j];
+        } else {
+            if (m.b_type[bnd] == 3) continue;
+            const int s = m.cf_bside[k];
+            rx = m.cf_fx[k] - m.cx[c];
+            ry = m.cf_fy[k] - m.cy[c];
+            rz = m.cf_fz[k] - m.cz[c];
+            thn = &Thsbar[s];
+            qn = &Qsbar[6 * (size_t)s];
+        }
+        const double alpha = (rx * nx + ry * ny + rz * nz) / (rx * rx + ry * ry + rz * rz);
+        const double nn = nx * nx + ny * ny + nz * nz;
+        const double f = A * rho;
+        // Fourier part: alpha (Th_nb - Th_c) |n|^2 + n . t(ThV)
+        atomicAdd(thn, f * alpha * nn);
+        atomicAdd(&Thbar[c], -f * alpha * nn);
+        tangential_T(m, k, f * nx, f * ny, f * nz, ThVbar, 1, 0);
+        // BTE part (subtracted): alpha n^T (Q_nb - Q_c) n + n . t(QV)
+        const double nq[6] = {nx * nx, 2 * nx * ny, 2 * nx * nz, ny * ny, 2 * ny * nz, nz * nz};
+        for (int i = 0; i < 6; i++) {
+            atomicAdd(&qn[i], -f * alpha * nq[i]);
+            atomicAdd(&Qbar[6 * (size_t)c + i], f * alpha * nq[i]);
+        }
+        const double wv[6][3] = {{nx, 0, 0}, {ny, nx, 0}, {nz, 0, nx}, {0, ny, 0}, {0, nz, ny}, {0, 0, nz}};
+        for (int i = 0; i < 6; i++) tangential_T(m, k, -f * wv[i][0], -f * wv[i][1], -f * wv[i][2], QVbar, 6, i);
+    }
+}
+
+// transpose of k_node_interp
+__global__ void k_adj_node(DMesh m, const double *__restrict__ ThVbar, const double *__restrict__ QVbar, double *Thbar,
+                           double *Qbar, double *Thsbar, double *Qsbar) {
+    const int i = (int)gtid();
+    if (i >= m.nslot) return;
+    const double tv = ThVbar[i];
+    double q6[6];
+    for (int j = 0; j < 6; j++) q6[j] = QVbar[6 * (size_t)i + j];
+    for (int k = m.nv_ptr[i]; k < m.nv_ptr[i + 1]; k++) {
+        const int src = m.nv_src[k];
+        const double w = m.nv_w[k];
+        double *th, *q;
+        if (src >= 0) {
+            th = &Thbar[src];
+            q = &Qbar[6 * (size_t)src];
+        } else {
+            th = &Thsbar[-1 - src];
+            q = &Qsbar[6 * (size_t)(-1 - src)];
+        }
+        atomicAdd(th, w * tv);
+        for (int j = 0; j < 6; j++) atomicAdd(&q[j], w * q6[j]);
+    }
+}
+
+// Transport part of (dF/de)^T lam + dJ/de, one thread per (direction, cell,
+// band): -lam, the cell's own outgoing faces and its downwind neighbours'
+// incoming faces (transpose of k_residual), the cell moments' cotangents
+// (transpose of k_moments: T_lat, Th, Q and the objective's q) into ebar;
+// the face-value gradients' cotangents into gbar[d][c][DIM][b]; the incoming
+// wall entries' cotangents (residual + side moments) into ebb.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adj_transport(DMesh m, DPhys p, const double *__restrict__ lam,
+                                                       const double *__restrict__ Tlbar, const double *__restrict__ Thbar,
+                                                       const double *__restrict__ Qbar, const double *__restrict__ qbar,
+                                                       const double *__restrict__ Thsbar, const double *__restrict__ Qsbar,
+                                                       const double *__restrict__ bTmbar, double *__restrict__ ebar,
+                                                       double *__restrict__ gbar, double *__restrict__ ebb) {
+    const int nb = p.nb, nc = m.nc;
+    const size_t total = (size_t)p.nd * nc * nb;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b = (int)(t % nb);
+        const size_t dc = t / nb;
+        const int c = (int)(dc % nc);
+        const int d = (int)(dc / nc);
+        const double vm = p.vmag[b], tau = p.tau[b], Cb = p.C[b], w = p.w[d];
+        const double sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
+        const double lc = lam[t];
+        const double oc = tau * m.tsc[c] / m.vol[c] * lc;  // own coefficient
+        // moments and objective
+        double e = -lc + w * p.lat[b] / Cb * Tlbar[c];
+        if (p.hr[b] > 0) {
+            const double *q = Qbar + 6 * (size_t)c;
+            e += p.kappa * p.lat[b] * w / Cb * Thbar[c] +
+                 w * tau * vm * vm *
+                     (q[0] * sx * sx + q[1] * sx * sy + q[2] * sx * sz + q[3] * sy * sy + q[4] * sy * sz + q[5] * sz * sz);
+        }
+        if (qbar) e += vm * w * (sx * qbar[3 * c] + sy * qbar[3 * c + 1] + sz * qbar[3 * c + 2]);
+        double gx = 0, gy = 0, gz = 0;
+        for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+            const double vn = vm * (sx * m.cf_nx[k] + sy * m.cf_ny[k] + (DIM == 3 ? sz * m.cf_nz[k] : 0.0));
+            const double A = m.cf_area[k];
+            if (vn >= 0) {
+                double f = -oc * A * vn;
+                if (m.cf_bound[k] < 0) {
+                    const int j = m.cf_nbr[k];
+                    f += tau * m.tsc[j] / m.vol[j] * A * vn * lam[((size_t)d * nc + j) * nb + b];
+                }
+                e += f;
+                gx += f * (m.cf_fx[k] - m.cx[c]);
+                gy += f * (m.cf_fy[k] - m.cy[c]);
+                if (DIM == 3) gz += f * (m.cf_fz[k] - m.cz[c]);
+            } else if (m.cf_bound[k] >= 0) {
+                const int s = m.cf_bside[k];
+                ebb[((size_t)d * m.nbs + s) * nb + b] =
+                    -oc * A * vn + adj_side_entry(m, p, d, s, b, Thsbar, Qsbar, bTmbar);
+            }
+        }
+        ebar[t] = e;
+        double *gp = gbar + dc * DIM * nb + b;
+        gp[0] = gx;
+        gp[nb] = gy;
+        if (DIM == 3) gp[2 * nb] = gz;
+    }
+}
+
+// per (wall side, band): sum of the incoming entries' cotangents (the
+// diffuse re-emission's transpose reads it once per outgoing direction)
+__global__ void k_adj_dsum(DMesh m, DPhys p, const double *__restrict__ ebb, double *__restrict__ dbar) {
+    const int nb = p.nb;
+    const size_t total = (size_t)m.nbs * nb;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b = (int)(t % nb), s = (int)(t / nb);
+        const int c = m.bs_cell[s];
+        const int type = c >= 0 ? m.b_type[s >> 1] : 0;
+        double acc = 0;
+        if (c >= 0 && (type == 2 || type == 6) && p.hr[b] != 0) {
+            const int k = m.bs_cf[s];
+            for (int d = 0; d < p.nd; d++) {
+                const double vn = p.sx[d] * m.cf_nx[k] + p.sy[d] * m.cf_ny[k] + p.sz[d] * m.cf_nz[k];
+                if (vn < 0) acc += ebb[((size_t)d * m.nbs + s) * nb + b];
+            }
+        }
+        dbar[t] = acc;
+    }
+}
+
+// outgoing wall entries: side-moment cotangent plus the transpose of the
+// incoming gather (k_diffuse_sum + k_gather) from this side or, for
+// periodic walls, from the sides that read it
+__global__ void k_adj_ebout(DMesh m, DPhys p, const double *__restrict__ dif_w, const int *__restrict__ spec_src,
+                            const double *__restrict__ dbar, const int *__restrict__ per_ptr,
+                            const int *__restrict__ per_idx, const double *__restrict__ Thsbar,
+                            const double *__restrict__ Qsbar, const double *__restrict__ bTmbar, double *ebb) {
+    const int nb = p.nb;
+    const size_t total = (size_t)p.nd * m.nbs * nb;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b = (int)(t % nb);
+        const int s = (int)((t / nb) % m.nbs);
+        const int d = (int)(t / ((size_t)nb * m.nbs));
+        const int c = m.bs_cell[s];
+        if (c < 0) continue;
+        const int k = m.bs_cf[s];
+        const double nx = m.cf_nx[k], ny = m.cf_ny[k], nz = m.cf_nz[k];
+        if (p.sx[d] * nx + p.sy[d] * ny + p.sz[d] * nz < 0) continue;  // incoming entry
+        double v = adj_side_entry(m, p, d, s, b, Thsbar, Qsbar, bTmbar);
+        const int ib = s >> 1, type = m.b_type[ib];
+        if (p.hr[b] != 0) {
+            if (type == 2 || type == 6) {
+                const double f = type == 6 ? 1.0 - m.b_T[ib] : 1.0;
+                v += f * dif_w[(size_t)s * p.nd + d] * dbar[(size_t)s * nb + b];
+            }
+            if (type == 3 || type == 6) {
+                const double f = type == 6 ? m.b_T[ib] : 1.0;
+                for (int q = 0; q < p.nd; q++) {
+                    if (p.sx[q] * nx + p.sy[q] * ny + p.sz[q] * nz >= 0) continue;
+                    if (spec_src[(size_t)s * p.nd + q] == d) v += f * ebb[((size_t)q * m.nbs + s) * nb + b];
+                }
+            }
+            for (int r = per_ptr[s]; r < per_ptr[s + 1]; r++) {
+                const int s2 = per_idx[r];
+                const int k2 = m.bs_cf[s2];
+                if (p.sx[d] * m.cf_nx[k2] + p.sy[d] * m.cf_ny[k2] + p.sz[d] * m.cf_nz[k2] < 0)
+                    v += ebb[((size_t)d * m.nbs + s2) * nb + b];
+            }
+        }
+        ebb[t] = v;
+    }
+}
+
+// transpose of k_bound_out: outgoing wall entries to the cell value and the
+// gradient's face offset (boundary cells only)
+template <int DIM>
+__global__ void k_adj_bout(DMesh m, DPhys p, const int *__restrict__ bcell, int nbcell, const double *__restrict__ ebb,
+                           double *ebar, double *gbar) {
+    const int nb = p.nb;
+    const size_t total = (size_t)p.nd * nbcell * nb;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b = (int)(t % nb);
+        const int i = (int)((t / nb) % nbcell);
+        const int d = (int)(t / ((size_t)nb * nbcell));
+        const int c = bcell[i];
+        const size_t dc = (size_t)d * m.nc + c;
+        double e = 0, gx = 0, gy = 0, gz = 0;
+        for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+            if (m.cf_bound[k] < 0) continue;
+            if (p.sx[d] * m.cf_nx[k] + p.sy[d] * m.cf_ny[k] + p.sz[d] * m.cf_nz[k] < 0) continue;
+            const double v = ebb[((size_t)d * m.nbs + m.cf_bside[k]) * nb + b];
+            e += v;
+            gx += v * (m.cf_fx[k] - m.cx[c]);
+            gy += v * (m.cf_fy[k] - m.cy[c]);
+            gz += v * (m.cf_fz[k] - m.cz[c]);
+        }
+        ebar[dc * nb + b] += e;
+        double *gp = gbar + dc * DIM * nb + b;
+        gp[0] += gx;
+        gp[nb] += gy;
+        if (DIM == 3) gp[2 * nb] += gz;
+    }
+}
+
+// transpose of k_gradient, then D^-1 = tsc/V and the scatter into the level
+// order of the opposite direction's sweep
+template <int DIM>
+__global__ void __launch_bounds__(256) k_adj_gradT(DMesh m, DPhys p, const int *__restrict__ tptr,
+                                                   const int *__restrict__ tidx, const double *__restrict__ tw,
+                                                   const double *__restrict__ wsum, const int *__restrict__ opp,
+                                                   const int *__restrict__ pos_of, const double *__restrict__ ebar,
+                                                   const double *__restrict__ gbar, double *__restrict__ Rlo) {
+    const int nb = p.nb, nc = m.nc;
+    const size_t total = (size_t)p.nd * nc * nb;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b = (int)(t % nb);
+        const size_t dc = t / nb;
+        const int j = (int)(dc % nc);
+        const int d = (int)(dc / nc);
+        const double *gd = gbar + ((size_t)d * nc) * DIM * nb + b;
+        double acc = ebar[t];
+        for (int q = tptr[j]; q < tptr[j + 1]; q++) {
+            const double *g = gd + (size_t)tidx[q] * DIM * nb;
+            acc += tw[3 * q] * g[0] + tw[3 * q + 1] * g[nb];
+            if (DIM == 3) acc += tw[3 * q + 2] * g[2 * nb];
+        }
+        const double *g = gd + (size_t)j * DIM * nb;
+        acc -= wsum[3 * j] * g[0] + wsum[3 * j + 1] * g[nb];
+        if (DIM == 3) acc -= wsum[3 * j + 2] * g[2 * nb];
+        const int od = opp[d];
+        Rlo[((size_t)od * nc + pos_of[(size_t)od * nc + j]) * nb + b] = acc * m.tsc[j] / m.vol[j];
+    }
+}
+
+// lam += D mu with mu the opposite direction's sweep output; sums of the
+// squares of the step and of the state
+__global__ void k_adj_update(DMesh m, DPhys p, const int *__restrict__ opp, const double *__restrict__ Dc,
+                             double *lam, double *red) {
+    const int nb = p.nb, nc = m.nc;
+    const size_t total = (size_t)p.nd * nc * nb;
+    double s1 = 0, s2 = 0;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b = (int)(t % nb);
+        const size_t dc = t / nb;
+        const int c = (int)(dc % nc);
+        const int d = (int)(dc / nc);
+        const double mu = Dc[((size_t)opp[d] * nc + c) * nb + b] * m.vol[c] / m.tsc[c];
+        const double l = lam[t] + mu;
+        lam[t] = l;
+        s1 += mu * mu;
+        s2 += l * l;
+    }
+    s1 = warp_sum(s1);
+    s2 = warp_sum(s2);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&red[0], s1);
+        atomicAdd(&red[1], s2);
+    }
+}
+
+// sum_i A_f (BTE part of the face source) + heat V: the part of the macro
+// right-hand side that does not scale with kappa_bulk
+__global__ void k_adj_u(DMesh m, const double *__restrict__ Q, const double *__restrict__ Qs,
+                        const double *__restrict__ QV, double *__restrict__ U) {
+    const int c = (int)gtid();
+    if (c >= m.nc) return;
+    double acc = 0;
+    for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+        const double nx = m.cf_nx[k], ny = m.cf_ny[k], nz = m.cf_nz[k], A = m.cf_area[k];
+        double rx, ry, rz;
+        const double *qn;
+        const int bnd = m.cf_bound[k];
+        if (bnd < 0) {
+            const int j = m.cf_nbr[k];
+            rx = m.cx[j] - m.cx[c];
+            ry = m.cy[j] - m.cy[c];
+            rz = m.cz[j] - m.cz[c];
+            qn = Q + 6 * (size_t)j;
+        } else {
+            if (m.b_type[bnd] == 3) continue;
+            rx = m.cf_fx[k] - m.cx[c];
+            ry = m.cf_fy[k] - m.cy[c];
+            rz = m.cf_fz[k] - m.cz[c];
+            qn = Qs + 6 * (size_t)m.cf_bside[k];
+        }
+        const double alpha = (rx * nx + ry * ny + rz * nz) / (rx * rx + ry * ry + rz * rz);
+        double dq[6];
+        for (int i = 0; i < 6; i++) dq[i] = qn[i] - Q[6 * (size_t)c + i];
+        double gx, gy, gz;
+        symv(dq, nx, ny, nz, gx, gy, gz);
+        double bte = alpha * (nx * gx + ny * gy + nz * gz);
+        double tq[6][3];
+        for (int i = 0; i < 6; i++) tangential(m, c, k, QV, 6, i, true, tq[i][0], tq[i][1], tq[i][2]);
+        bte += nx * (tq[0][0] + tq[1][1] + tq[2][2]) + ny * (tq[1][0] + tq[3][1] + tq[4][2]) +
+               nz * (tq[2][0] + tq[4][1] + tq[5][2]);
+        acc += A * bte;
+    }
+    U[c] = acc + m.heat[c] * m.vol[c];
+}
+
+// gradient assembly over cells: warp per cell, lanes over (direction, band).
+// Gamma = lam (e - C_b T*) gives the residual's tau and s_c derivatives; the
+// tensor moment's tau derivative is v_b^2 (w s s^T e) : Qbar. Per-band sums
+// go through shared memory (nb <= 256) into g_tau.
+__global__ void k_adj_assemble(DMesh m, DPhys p, const double *__restrict__ lam, const double *__restrict__ eps,
+                               const double *__restrict__ T, const double *__restrict__ Qbar, double *g_cell,
+                               double *g_tau) {
+    extern __shared__ double sb[];
+    for (int i = threadIdx.x; i < p.nb; i += blockDim.x) sb[i] = 0;
+    __syncthreads();
+    const int c = (int)(gtid() >> 5), lane = threadIdx.x & 31;
+    if (c < m.nc) {
+        const int n = p.nd * p.nb;
+        const double *q = Qbar + 6 * (size_t)c;
+        double gs = 0;
+        for (int i = lane; i < n; i += 32) {
+            const int d = i / p.nb, b = i % p.nb;
+            const double e = eps[((size_t)d * m.nc + c) * p.nb + b];
+            const double G = lam[((size_t)d * m.nc + c) * p.nb + b] * (e - p.C[b] * T[c]);
+            gs += G;
+            double tb = G;  // d/d(ln tau_b) of the residual
+            if (p.hr[b] > 0) {
+                const double sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
+                tb += p.tau[b] * p.vmag[b] * p.vmag[b] * p.w[d] * e *
+                      (q[0] * sx * sx + q[1] * sx * sy + q[2] * sx * sz + q[3] * sy * sy + q[4] * sy * sz + q[5] * sz * sz);
+            }
+            atomicAdd(&sb[b], tb);
+        }
+        gs = warp_sum(gs);
+        if (lane == 0) g_cell[c] = -gs * m.tsc[c];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < p.nb; i += blockDim.x) atomicAdd(&g_tau[i], sb[i]);
+}
+
+// the tensor moment's tau derivative on wall sides, and the specularity
+// derivative of partially specular walls: warp per side
+__global__ void k_adj_assemble_sides(DMesh m, DPhys p, const double *__restrict__ eb, const double *__restrict__ ebb,
+                                     const double *__restrict__ dsum, const int *__restrict__ spec_src,
+                                     const double *__restrict__ Qsbar, double *g_tau, double *g_bnd) {
+    extern __shared__ double sb[];
+    for (int i = threadIdx.x; i < p.nb; i += blockDim.x) sb[i] = 0;
+    __syncthreads();
+    const int s = (int)(gtid() >> 5), lane = threadIdx.x & 31;
+    if (s < m.nbs && m.bs_cell[s] >= 0) {
+        const int n = p.nd * p.nb, k = m.bs_cf[s], ib = s >> 1;
+        const double *q = Qsbar + 6 * (size_t)s;
+        const bool partial = m.b_type[ib] == 6;
+        double gp = 0;
+        for (int i = lane; i < n; i += 32) {
+            const int d = i / p.nb, b = i % p.nb;
+            if (!(p.hr[b] > 0)) continue;
+            const double sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
+            const double x = eb[((size_t)d * m.nbs + s) * p.nb + b];
+            atomicAdd(&sb[b], p.tau[b] * p.vmag[b] * p.vmag[b] * p.w[d] * x *
+                                  (q[0] * sx * sx + q[1] * sx * sy + q[2] * sx * sz + q[3] * sy * sy + q[4] * sy * sz +
+                                   q[5] * sz * sz));
+            if (partial && sx * m.cf_nx[k] + sy * m.cf_ny[k] + sz * m.cf_nz[k] < 0) {
+                const int src = spec_src[(size_t)s * p.nd + d];
+                gp += ebb[((size_t)d * m.nbs + s) * p.nb + b] *
+                      (eb[((size_t)src * m.nbs + s) * p.nb + b] - dsum[(size_t)s * p.nb + b]);
+            }
+        }
+        gp = warp_sum(gp);
+        if (lane == 0 && partial) atomicAdd(&g_bnd[ib], gp);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < p.nb; i += blockDim.x) atomicAdd(&g_tau[i], sb[i]);
+}
+
+}  // namespace
+
+// host tables of the adjoint: transposed LSQ stencil, boundary cells,
+// periodic readers of each wall side, opposite directions
+Error Solver::adj_setup() {
+    if (adj_lam_) return {0, ""};
+    cudaStream_t s = cfg.stream;
+    const int nc = mesh.nc, nd = ang.nd, nbs = mesh.nbs();
+    // opposite directions (the quadratures here are point-symmetric)
+    std::vector<int> opp(nd, -1);
+    for (int d = 0; d < nd; d++)
+        for (int q = 0; q < nd; q++)
+            if (std::fabs(ang.sx[q] + ang.sx[d]) < 1e-12 && std::fabs(ang.sy[q] + ang.sy[d]) < 1e-12 &&
+                std::fabs(ang.sz[q] + ang.sz[d]) < 1e-12)
+                opp[d] = q;
+    for (int d = 0; d < nd; d++)
+        if (opp[d] < 0) return {-8, "adjoint: the direction set has no opposite of a direction"};
+    // transposed stencil: T(j) = {(c, w_cj)} and w-sums per cell
+    std::vector<int> tptr(nc + 1, 0), tidx;
+    std::vector<double> tw, wsum(3 * (size_t)nc, 0.0);
+    for (int c = 0; c < nc; c++)
+        for (int q = mesh.nbr_ptr[c]; q < mesh.nbr_ptr[c + 1]; q++) tptr[mesh.nbr_idx[q] + 1]++;
+    for (int c = 0; c < nc; c++) tptr[c + 1] += tptr[c];
+    tidx.resize(tptr[nc]);
+    tw.resize(3 * (size_t)tptr[nc]);
+    {
+        std::vector<int> fill(tptr.begin(), tptr.end() - 1);
+        for (int c = 0; c < nc; c++)
+            for (int q = mesh.nbr_ptr[c]; q < mesh.nbr_ptr[c + 1]; q++) {
+                const int j = mesh.nbr_idx[q], at = fill[j]++;
+                tidx[at] = c;
+                for (int r = 0; r < 3; r++) {
+                    tw[3 * (size_t)at + r] = mesh.lsq_w[3 * (size_t)q + r];
+                    wsum[3 * (size_t)c + r] += mesh.lsq_w[3 * (size_t)q + r];
+                }
+            }
+    }
+    std::vector<int> bcell;
+    for (int c = 0; c < nc; c++)
+        for (int k = mesh.cf_ptr[c]; k < mesh.cf_ptr[c + 1]; k++)
+            if (mesh.cf_bound[k] >= 0) {
+                bcell.push_back(c);
+                break;
+            }
+    // side s2 of a periodic wall reads side 2 connect(s2) + (s2 & 1)
+    std::vector<int> pptr(nbs + 1, 0), pidx;
+    std::vector<std::vector<int>> readers(nbs);
+    for (int s2 = 0; s2 < nbs; s2++) {
+        if (mesh.bs_cell[s2] < 0 || mesh.b_type[s2 >> 1] >= 0) continue;
+        const int src = 2 * mesh.b_connect[s2 >> 1] + (s2 & 1);
+        if (src >= 0 && src < nbs) readers[src].push_back(s2);
+    }
+    for (int q = 0; q < nbs; q++) {
+        pptr[q + 1] = pptr[q] + (int)readers[q].size();
+        for (int r : readers[q]) pidx.push_back(r);
+    }
+    adj_nT_ = tidx.size();
+    adj_nbcell_ = bcell.size();
+    adj_nper_ = pidx.size();
+    std::vector<int> ints;
+    for (auto *v : {&tptr, &tidx, &bcell, &pptr, &pidx, &opp}) ints.insert(ints.end(), v->begin(), v->end());
+    std::vector<double> dbl(tw);
+    dbl.insert(dbl.end(), wsum.begin(), wsum.end());
+    bool ok = true;
+    adj_int_ = upload(this, allocs_, ints, s, ok);
+    adj_wt_ = upload(this, allocs_, dbl, s, ok);
+    const size_t ne = (size_t)nd * nc * bands.nb;
+    const size_t nslot = (size_t)mesh.nn * mesh.nmat;
+    adj_ebar_ = (double *)dalloc(ne * 8);
+    adj_ebb_ = (double *)dalloc((size_t)nd * nbs * bands.nb * 8);
+    adj_dbar_ = (double *)dalloc((size_t)nbs * bands.nb * 8);
+    // per cell: 16 (Tbar, z, zsum, rbar, Thbar, Qbar x6, U, Tuser, qbar x3);
+    // per node slot: 8 (TVbar, ThVbar, QVbar x6); per wall side: 8 (Thsbar,
+    // Qsbar x6, bTmbar); then g_tau, g_bnd and two reduction slots
+    adj_cell_ = (double *)dalloc((16 * (size_t)nc + 8 * nslot + 8 * (size_t)nbs + bands.nb + mesh.nbd() + 8) * 8);
+    adj_lam_ = (double *)dalloc(ne * 8);
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (!ok || !adj_ebar_ || !adj_ebb_ || !adj_dbar_ || !adj_cell_ || !adj_lam_) {
+        adj_lam_ = nullptr;
+        return {-6, "device allocation failed (adjoint state)"};
+    }
+    return {0, ""};
+}
+
+Error Solver::vjp(const double *Tbar_h, const double *qbar_h, int max_iter, double tol, double *g_tau, double *g_cell,
+                  double *g_bnd, VjpStats &st) {
+    if (!initialised) return {-1, "solver not initialised"};
+    if (cfg.precision != 0) return {-8, "the adjoint is implemented for the FP64 form (GBTE_FP64) only"};
+    if (ncomp_ > 1) return {-8, "the adjoint is not implemented for batched handles"};
+    if (!started_ || last_inner_ < 1) return {-1, "call gbte_solve (to convergence) before gbte_vjp"};
+    if (need_snapshot_) return {-8, "the adjoint does not support chained specular reflections"};
+    if (ndb_ < ang.nd) return {-8, "the adjoint needs every direction's buffers resident (direction_batch)"};
+    if (max_iter < 1 || !(tol > 0)) return {-1, "invalid adjoint limits"};
+    CUDA_TRY(cudaSetDevice(cfg.device));
+    Error e = adj_setup();
+    if (e.code) return e;
+    cudaStream_t s = cfg.stream;
+    const int nc = mesh.nc, nb = bands.nb, nd = ang.nd, nbs = mesh.nbs(), nbd = mesh.nbd();
+    const int nslot = mesh.nn * mesh.nmat, dim = mesh.dim;
+    const size_t ne = (size_t)nd * nc * nb;
+    // device scratch layout
+    double *Tb = adj_cell_, *z = Tb + nc, *zsum = z + nc, *rbar = zsum + nc, *Thbar = rbar + nc,
+           *Qbar = Thbar + nc, *U = Qbar + 6 * (size_t)nc, *Tuser = U + nc, *qbar = Tuser + nc;
+    double *TVbar = qbar + 3 * (size_t)nc, *ThVbar = TVbar + nslot, *QVbar = ThVbar + nslot,
+           *Thsbar = QVbar + 6 * (size_t)nslot, *Qsbar = Thsbar + nbs, *bTmbar = Qsbar + 6 * (size_t)nbs,
+           *gtau = bTmbar + nbs, *gbnd = gtau + nb, *red = gbnd + nbd, *gcell = z;  // g_cell reuses z at the end
+    const int *tptr = adj_int_, *tidx = tptr + nc + 1, *bcell = tidx + adj_nT_, *pptr = bcell + adj_nbcell_,
+              *pidx = pptr + nbs + 1, *opp = pidx + adj_nper_;
+    const double *tw = adj_wt_, *wsum = adj_wt_ + 3 * adj_nT_;
+    double *lam = adj_lam_, *ebar = adj_ebar_, *ebb = adj_ebb_, *gbar = (double *)grad_, *Rlo = (double *)res_;
+    const double *eps = (const double *)eps_;
+    if (Tbar_h) CUDA_TRY(cudaMemcpyAsync(Tuser, Tbar_h, (size_t)nc * 8, cudaMemcpyHostToDevice, s));
+    else CUDA_TRY(cudaMemsetAsync(Tuser, 0, (size_t)nc * 8, s));
+    if (qbar_h) CUDA_TRY(cudaMemcpyAsync(qbar, qbar_h, (size_t)nc * 24, cudaMemcpyHostToDevice, s));
+    else CUDA_TRY(cudaMemsetAsync(qbar, 0, (size_t)nc * 24, s));
+    CUDA_TRY(cudaMemsetAsync(lam, 0, ne * 8, s));
+    CUDA_TRY(cudaEventRecord(ev_[0], s));
+    const int gC = (nc + kThreads - 1) / kThreads, gN = (nslot + kThreads - 1) / kThreads;
+    const int gS = (nbs + kThreads - 1) / kThreads;
+    const int gWc = (int)(((size_t)nc * 32 + kThreads - 1) / kThreads);
+    const int gWs = (int)(((size_t)nbs * 32 + kThreads - 1) / kThreads);
+    const double kappa = dp_.kappa;
+    // sweep launch (FP64 records; the forward's band chunking)
+    constexpr int LOOK = 4, LCAP = 128;
+    const int fixed = cfg.sweep_bands;
+    int cap = (fixed >= 1 && fixed <= 32) ? fixed : tuned_sweep_bands_ > 0 ? tuned_sweep_bands_ : 4;
+    int nbc = 0, chunks = 0;
+    size_t smem = 0;
+    const size_t wlp = ((size_t)(sched.max_levels + 1) * sizeof(int) + 15) & ~(size_t)15;
+    for (; cap >= 1; cap--) {
+        nbc = (nb + (nb + cap - 1) / cap - 1) / ((nb + cap - 1) / cap);
+        chunks = (nb + nbc - 1) / nbc;
+        const size_t slot = (size_t)LCAP * sizeof(SweepRec<double>) + (((size_t)LCAP * nbc * 8 + 15) & ~(size_t)15);
+        smem = LOOK * slot + (((size_t)ring_ * nbc * 8 + 15) & ~(size_t)15) +
+               (((size_t)far_slots_ * nbc * 8 + 15) & ~(size_t)15) + wlp;
+        if (smem <= 220 * 1024 || nbc == 1) break;
+    }
+    if (smem > 220 * 1024) return {-8, "sweep level too wide for the shared-memory correction ring"};
+    const int sthreads = std::max(nbc, (256 / nbc) * nbc);
+    const int last = nb - (chunks - 1) * nbc;
+    const int rvec = ((nbc * 8) % 16 == 0 && (nb * 8) % 16 == 0 && (last * 8) % 16 == 0) ? 1 : 0;
+    CUDA_TRY(cudaFuncSetAttribute(k_sweep<double, LOOK, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int N = last_inner_;
+    long long cg_its = 0;
+    // one evaluation of (dF/de)^T lam + dJ/de (without the gradient's
+    // transpose) and of the macro cotangents
+    auto evaluate = [&]() -> Error {
+        k_adj_tbar<<<gWc, kThreads, 0, s>>>(dm_, dp_, lam, Tuser, Tb);
+        CUDA_TRY(cudaMemsetAsync(zsum, 0, (size_t)nc * 8, s));
+        for (int k = N - 1; k >= 0; k--) {
+            CUDA_TRY(cudaMemsetAsync(z, 0, (size_t)nc * 8, s));
+            Error ce = cg_solve(kplan_, K_ptr_, K_idx_, K_val_, K_dinv_, z, Tb, cfg.macro_rtol, 0.0, cg_its, cg_scal_,
+                                cg_r_, cg_z_, cg_p_, cg_Ap_, nullptr, nullptr);
+            if (ce.code) return ce;
+            CUDA_TRY(cudaMemsetAsync(TVbar, 0, (size_t)nslot * 8, s));
+            k_adj_macro_tv<<<gC, kThreads, 0, s>>>(dm_, kappa, z, TVbar);
+            CUDA_TRY(cudaMemsetAsync(Tb, 0, (size_t)nc * 8, s));
+            k_adj_tinterp<<<gN, kThreads, 0, s>>>(dm_, TVbar, Tb);
+            k_adj_axpy<<<gC, kThreads, 0, s>>>(z, zsum, nc);
+        }
+        // Tb now holds the cotangent of T_lat; remacro's is -zsum
+        k_adj_neg<<<gC, kThreads, 0, s>>>(zsum, rbar, nc);
+        k_adj_bTm<<<gS, kThreads, 0, s>>>(dm_, kappa, zsum, bTovr_, bTmbar);
+        CUDA_TRY(cudaMemsetAsync(Thbar, 0, (size_t)nc * 8 * 7, s));  // Thbar, Qbar
+        CUDA_TRY(cudaMemsetAsync(ThVbar, 0, (size_t)nslot * 8 * 7, s));
+        CUDA_TRY(cudaMemsetAsync(Thsbar, 0, (size_t)nbs * 8 * 7, s));
+        k_adj_remacro<<<gC, kThreads, 0, s>>>(dm_, rbar, Thbar, Qbar, Thsbar, Qsbar, ThVbar, QVbar);
+        k_adj_node<<<gN, kThreads, 0, s>>>(dm_, ThVbar, QVbar, Thbar, Qbar, Thsbar, Qsbar);
+        if (dim == 2)
+            k_adj_transport<2><<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, lam, Tb, Thbar, Qbar, qbar, Thsbar, Qsbar,
+                                                                  bTmbar, ebar, gbar, ebb);
+        else
+            k_adj_transport<3><<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, lam, Tb, Thbar, Qbar, qbar, Thsbar, Qsbar,
+                                                                  bTmbar, ebar, gbar, ebb);
+        k_adj_dsum<<<grid_for((size_t)nbs * nb), kThreads, 0, s>>>(dm_, dp_, ebb, adj_dbar_);
+        k_adj_ebout<<<grid_for((size_t)nd * nbs * nb), kThreads, 0, s>>>(dm_, dp_, dif_w_, spec_src_, adj_dbar_, pptr,
+                                                                          pidx, Thsbar, Qsbar, bTmbar, ebb);
+        if (adj_nbcell_) {
+            if (dim == 2)
+                k_adj_bout<2><<<grid_for((size_t)nd * adj_nbcell_ * nb), kThreads, 0, s>>>(dm_, dp_, bcell,
+                                                                                        (int)adj_nbcell_, ebb, ebar, gbar);
+            else
+                k_adj_bout<3><<<grid_for((size_t)nd * adj_nbcell_ * nb), kThreads, 0, s>>>(dm_, dp_, bcell,
+                                                                                        (int)adj_nbcell_, ebb, ebar, gbar);
+        }
+        CUDA_TRY(cudaGetLastError());
+        return {0, ""};
+    };
+    double change = 0;
+    int it = 0;
+    for (;; it++) {
+        Error ee = evaluate();
+        if (ee.code) return ee;
+        if (it > 0 && change <= tol) break;
+        if (it >= max_iter) break;
+        if (dim == 2)
+            k_adj_gradT<2><<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, tptr, tidx, tw, wsum, opp, pos_of_, ebar, gbar,
+                                                              Rlo);
+        else
+            k_adj_gradT<3><<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, tptr, tidx, tw, wsum, opp, pos_of_, ebar, gbar,
+                                                              Rlo);
+        k_sweep<double, LOOK, LCAP><<<nd * chunks, sthreads, smem, s>>>(nb, nc, 1, 0, nbc, ring_, far_slots_, rvec,
+                                                                        lvl_ptr_, dir_lvl_off_,
+                                                                        (const SweepRec<double> *)rec_, lvl_cells_, kb_,
+                                                                        Rlo, (double *)corr_);
+        CUDA_TRY(cudaMemsetAsync(red, 0, 2 * 8, s));
+        k_adj_update<<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, opp, (const double *)corr_, lam, red);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(h_pinned_, red, 2 * 8, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        change = h_pinned_[1] > 0 ? std::sqrt(h_pinned_[0] / h_pinned_[1]) : 0.0;
+        if (!std::isfinite(change)) return {-4, "the adjoint iteration diverged"};
+    }
+    // assembly at the final lam (the evaluation above used it)
+    CUDA_TRY(cudaMemsetAsync(gtau, 0, (size_t)(nb + nbd) * 8, s));
+    k_adj_u<<<gC, kThreads, 0, s>>>(dm_, Q_, Qs_, QV_, U);
+    k_adj_assemble<<<gWc, kThreads, nb * 8, s>>>(dm_, dp_, lam, eps, T_, Qbar, gcell, gtau);
+    k_adj_assemble_sides<<<gWs, kThreads, nb * 8, s>>>(dm_, dp_, eb_, ebb, dsum_, spec_src_, Qsbar, gtau, gbnd);
+    CUDA_TRY(cudaGetLastError());
+    std::vector<double> hz(nc), hu(nc), ht(nb), hb(nbd);
+    CUDA_TRY(cudaMemcpyAsync(hz.data(), zsum, (size_t)nc * 8, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(hu.data(), U, (size_t)nc * 8, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(ht.data(), gtau, (size_t)nb * 8, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(hb.data(), gbnd, (size_t)nbd * 8, cudaMemcpyDeviceToHost, s));
+    if (g_cell) CUDA_TRY(cudaMemcpyAsync(g_cell, gcell, (size_t)nc * 8, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaEventRecord(ev_[1], s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    // kappa_bulk = sum_b C v^2 tau_b / dim: its cotangent -<zsum, U>/kappa
+    double zu = 0;
+    for (int c = 0; c < nc; c++) zu += hz[c] * hu[c];
+    const double kbar = -zu / kappa;
+    const double mdim = bands.material_dim == 2 ? 2.0 : 3.0;
+    if (g_tau)
+        for (int b = 0; b < nb; b++)
+            g_tau[b] = ht[b] + kbar * bands.C[b] * bands.v[b] * bands.v[b] * bands.tau[b] / mdim;
+    if (g_bnd)
+        for (int ib = 0; ib < nbd; ib++) g_bnd[ib] = hb[ib];
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
+    st.iterations = it;
+    st.picard_steps = N;
+    st.change = change;
+    st.ms = ms;
     return {0, ""};
 }
 

@@ -16,6 +16,7 @@ struct DMesh {
     const int *cf_ptr, *cf_nbr, *cf_bside, *cf_bound, *cf_v, *cf_face;
     const double *cf_area, *cf_nx, *cf_ny, *cf_nz, *cf_fx, *cf_fy, *cf_fz;
     const double *vol, *cx, *cy, *cz, *heat;
+    const double *tsc;  // 1 / s_c: per-cell scale of the relaxation time (scattering multiplier s_c)
     const int *nbr_ptr, *nbr_idx;
     const double *lsq_w;
     const float *lsq_wf;
@@ -50,6 +51,7 @@ struct SolverConfig {
     int sweep_bands = 0;      // bands per sweep CTA, 0 = automatic
     int sweep_far_slots = 0;  // far-slot cap of the sweep plan: 0 = automatic, < 0 = none
     int direction_batch = 0;  // most directions per transport batch, 0 = automatic
+    std::vector<double> cell_scatter;  // scattering-rate multiplier s_c per cell (empty: 1)
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -60,6 +62,11 @@ enum KernelId {
     K_GATHER, K_MACRO_BC, K_TINTERP, K_MACRO_RHS, K_PCG, K_REDUCE, K_COPY, K_INIT, K_NUM
 };
 const char *kernel_name(int k);
+
+struct VjpStats {
+    int iterations = 0, picard_steps = 0;
+    double change = 0, ms = 0;
+};
 
 struct SolveStats {
     int iterations = 0, inner_iterations = 0;
@@ -93,6 +100,14 @@ public:
     int fourier_iterations = 0;
     Error solve(SolveStats &st);
     Error get_fields(double *T_energy, double *T_lattice, double *q, double *T_band);
+    // Vector-Jacobian product of the converged fixed point: given cotangents
+    // of the lattice temperature (Tbar, nc) and heat flux (qbar, 3 nc), the
+    // derivatives of <Tbar, T> + <qbar, q> with respect to a multiplier on
+    // each band's relaxation time (g_tau, nb), each cell's scattering
+    // multiplier (g_cell, nc) and each boundary's specularity (g_bnd, nbd;
+    // partially specular walls only)
+    Error vjp(const double *Tbar, const double *qbar, int max_iter, double tol, double *g_tau, double *g_cell,
+              double *g_bnd, VjpStats &st);
 
     FlatMesh mesh;
     Bands bands;
@@ -179,6 +194,14 @@ private:
     void prof_end();
     void prof_collect(SolveStats &st);
     long long launches_ = 0;
+    int last_inner_ = 0;  // Picard steps of the last outer iteration's macro correction
+    // adjoint state and scratch (allocated by the first vjp)
+    double *adj_lam_ = nullptr, *adj_ebar_ = nullptr, *adj_ebb_ = nullptr, *adj_dbar_ = nullptr;
+    double *adj_cell_ = nullptr;  // per-cell / per-side / per-node cotangents, one block
+    int *adj_int_ = nullptr;      // transposed stencil, boundary cells, periodic readers, opposite directions
+    double *adj_wt_ = nullptr;    // transposed stencil weights and stencil weight sums
+    size_t adj_nT_ = 0, adj_nbcell_ = 0, adj_nper_ = 0;
+    Error adj_setup();
 };
 
 }  // namespace gbte

@@ -484,8 +484,8 @@ def write_band_database(path: str, bands: BandTable) -> None:
 @dataclasses.dataclass
 class BC:
     tag: int
-    type: int      # 1 isothermal, 2 diffuse, 3 specular, <0 periodic (partner = -type)
-    value: float   # wall temperature / periodic temperature jump
+    type: int      # 1 isothermal, 2 diffuse, 3 specular, <0 periodic (partner = -type), 6 partially specular
+    value: float   # wall temperature / periodic temperature jump / specularity (type 6)
 
 
 @dataclasses.dataclass
@@ -602,6 +602,20 @@ def config2_deck(h_nm: float = 3.0, n_bands: int = 40, n_phi: int = 16, seed: in
     kw.setdefault("angle_method", 1)
     kw.setdefault("tref", 0.0)
     return Deck(mesh=mesh, bands=bands, bcs=bcs, scale=(L, L), **kw)
+
+
+def config4_deck(h_nm: float = 3.0, n_bands: int = 40, n_phi: int = 16, seed: int = 0, specularity: float = 0.3,
+                 **kw) -> Deck:
+    """The config-2 cell with a partially specular pore wall (BC type 6,
+    value = specularity p): the geometry of the adjoint workload."""
+    d = config2_deck(h_nm=h_nm, n_bands=n_bands, n_phi=n_phi, seed=seed, **kw)
+    d.bcs = [b if b.tag != 5 else BC(5, 6, float(specularity)) for b in d.bcs]
+    return d
+
+
+def lognormal_scatter(n_cells: int, sigma: float = 0.2, seed: int = 2) -> np.ndarray:
+    """Per-cell scattering multipliers drawn log-normal (median 1)."""
+    return np.exp(np.random.default_rng(seed).normal(0.0, sigma, n_cells))
 
 
 def config3_deck(h_nm: float = 2.5, n_bands: int = 40, n_theta: int = 4, n_phi: int = 4, seed: int = 1,

@@ -99,7 +99,12 @@ typedef struct {
 } gbte_band_table;
 
 /* Boundary conditions: type 1 isothermal (value = wall T), 2 diffuse,
- * 3 specular, < 0 periodic (partner tag = -type, value = temperature jump). */
+ * 3 specular, < 0 periodic (partner tag = -type, value = temperature jump),
+ * 6 partially specular (value = specularity p in [0, 1]; no counterpart in
+ * the reference): an incoming intensity is p times the outgoing value of the
+ * outgoing direction nearest its mirror image plus (1 - p) times the diffuse
+ * value; the synthetic (macro) correction treats the wall as diffuse; p = 0
+ * and p = 1 are exactly types 2 and 3. */
 typedef struct {
     int num;
     const int *tag;
@@ -130,6 +135,9 @@ typedef struct {
                                  ring: 0 = automatic (2048), < 0 = none (such reads go to memory) */
     int direction_batch;      /* most directions whose gradient/residual/correction buffers are held at
                                  once; 0 = automatic (all that fit in device memory) */
+    const double *cell_scatter; /* [num_cells] scattering-rate multiplier s_c > 0 (no counterpart in the
+                                 reference): the transport uses tau_b / s_c in cell c; the synthetic
+                                 correction keeps the band table's tau; NULL = 1 everywhere */
     int cell_order;           /* 0 = automatic: cells are renumbered inside the library along a Morton
                                  curve of their centres (per geometry of a batch) for memory locality;
                                  1 = keep the caller's order. Every cell array of this ABI is in the
@@ -283,6 +291,38 @@ int gbte_get_sizes(gbte_handle *h, int *num_cells, int *num_bands, int *num_dire
 
 /* Cell centres [Nc*3] and volumes [Nc] as the solver sees them. */
 int gbte_get_geometry(gbte_handle *h, double *centers, double *volumes);
+
+/* Adjoint of the converged solve (no counterpart in the reference, which
+ * has no derivatives). For the objective
+ *   J = sum_c T_bar[c] T[c] + sum_c q_bar[c] . q[c]
+ * of the fields gbte_get_fields returns (T the macro lattice temperature, q
+ * the heat flux; either cotangent may be NULL = 0), it writes:
+ *   grad_tau[Nb]        dJ/d alpha_b for a multiplier alpha_b on band b's
+ *                       relaxation time (transport and synthetic correction
+ *                       alike), at alpha = 1
+ *   grad_scatter[Nc]    dJ/d s_c for the cell scattering multipliers
+ *                       (options.cell_scatter), at their current values
+ *   grad_specularity[n] dJ/dp per row of the boundary table given at
+ *                       creation (partially specular rows, type 6; 0 for the
+ *                       other rows)
+ * Any output may be NULL. It differentiates the fixed point the last
+ * gbte_solve reached, implicitly: the adjoint state solves the transposed
+ * equations by the transposed source iteration (sweeps in the opposite
+ * directions, the transposed synthetic correction), until its relative
+ * change is <= tol or max_iter iterations ran. Call it after a solve that
+ * converged to tight margins; the gradient is that of the state the solve
+ * left. FP64 handles only (GBTE_ERR_UNSUPPORTED otherwise), not batched
+ * handles. It keeps one more band-state array (Nd*Nc*Nb doubles) and
+ * reuses the transport scratch; a later gbte_solve continues unchanged. */
+typedef struct {
+    int iterations;     /* transposed source iterations */
+    int picard_steps;   /* Picard steps of the synthetic correction, transposed */
+    double change;      /* last relative change of the adjoint state */
+    double vjp_ms;      /* device time of the adjoint solve and the assembly */
+} gbte_vjp_stats;
+
+int gbte_vjp(gbte_handle *h, const double *T_bar, const double *q_bar, int max_iter, double tol, double *grad_tau,
+             double *grad_scatter, double *grad_specularity, gbte_vjp_stats *st);
 
 const char *gbte_last_error(const gbte_handle *h);
 const char *gbte_status_string(int status);

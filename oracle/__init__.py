@@ -47,12 +47,15 @@ def _p(a, t):
 
 def solve(deck, T0: Optional[np.ndarray] = None, max_iter: Optional[int] = None,
           err_T: Optional[float] = None, err_q: Optional[float] = None,
-          cell_heat: Optional[np.ndarray] = None) -> Dict[str, np.ndarray]:
+          cell_heat: Optional[np.ndarray] = None,
+          cell_scatter: Optional[np.ndarray] = None) -> Dict[str, np.ndarray]:
     """Run the restated FP64 solve on a ``giftbte_b200.decks.Deck``.
 
     Returns the macro temperature ``T`` (TempLattice.dat), the energy
     temperature ``E`` (Temperature.dat), heat flux ``q`` (Nc x 3), band
     temperatures ``Tband`` (Nb x Nc), iteration count and final margins.
+    ``cell_scatter`` (extension, no reference counterpart) scales the
+    relaxation time of cell c by 1/s_c in the transport.
     """
     m = deck.mesh
     dim = deck.dimension
@@ -86,6 +89,8 @@ def solve(deck, T0: Optional[np.ndarray] = None, max_iter: Optional[int] = None,
         cell_heat = deck.cell_heat()
     if cell_heat is not None:
         cell_heat = np.ascontiguousarray(cell_heat, dtype=np.float64)
+    if cell_scatter is not None:
+        cell_scatter = np.ascontiguousarray(cell_scatter, dtype=np.float64)
     out_T = np.zeros(nc); out_E = np.zeros(nc); out_q = np.zeros(3 * nc); out_Tb = np.zeros(nb * nc)
     iters = ctypes.c_int(0)
     err = np.zeros(2)
@@ -101,7 +106,8 @@ def solve(deck, T0: Optional[np.ndarray] = None, max_iter: Optional[int] = None,
         ctypes.c_double(err_T if err_T is not None else deck.residual_temp),
         ctypes.c_double(err_q if err_q is not None else deck.residual_flux), 0,
         _p(out_T, ctypes.c_double), _p(out_E, ctypes.c_double), _p(out_q, ctypes.c_double),
-        _p(out_Tb, ctypes.c_double), ctypes.byref(iters), _p(err, ctypes.c_double))
+        _p(out_Tb, ctypes.c_double), ctypes.byref(iters), _p(err, ctypes.c_double),
+        _p(cell_scatter, ctypes.c_double))
     if rc != 0:
         raise RuntimeError(f"oracle_solve failed with code {rc}")
     return {"T": out_T, "E": out_E, "q": out_q.reshape(nc, 3), "Tband": out_Tb.reshape(nb, nc),

@@ -23,6 +23,11 @@
 // 2D decks by tests/test_oracle_pin.py. The 3D branch follows the
 // dimension-generic formulas of the reference; the reference's own 3D mesh
 // code is stripped from its public release, so 3D parity is unpinned.
+// Two extensions without a reference counterpart, each reducing to the
+// reference at its neutral value: a per-cell scattering multiplier s_c (the
+// transport uses tau / s_c in cell c; s_c = 1 is the reference) and the
+// partially specular wall, type 6 with value p (p = 0 and p = 1 become the
+// reference's types 2 and 3).
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -353,6 +358,7 @@ struct Oracle {
     std::vector<std::vector<double>> e;         // [p][nc], p = d*nb + b
     std::vector<double> ebound;                 // [b][d][ib][2]
     std::vector<double> T, Told, Tlat, Tband, E, qx, qy, qz, qxo, qyo, qzo, ReMacro, heat;
+    std::vector<double> tsc;                    // 1 / s_c: per-cell relaxation-time scale (extension, 1 = reference)
     std::vector<std::array<double, 2>> bTmacro;
     double errOld = 0, errOldq = 0, err = 0, errq = 0;
     int errInc = 0;
@@ -501,6 +507,13 @@ int build_mesh(Oracle &o, int dim, int nn, const double *xyz, int nc, const int 
                 b.face = r.faces;
                 b.type = types[j];
                 b.T = vals[j];
+                // extension: partially specular wall (type 6, value = p); its
+                // ends are the reference's diffuse and specular walls
+                if (b.type == 6) {
+                    if (!(b.T >= 0 && b.T <= 1)) return -4;
+                    if (b.T == 0) b.type = 2;
+                    else if (b.T == 1) b.type = 3;
+                }
                 o.bnd.push_back(b);
             }
     for (int i = 0; i < (int)o.bnd.size(); i++)
@@ -662,7 +675,7 @@ void bte_pair(Oracle &o, int b, int d, PairWork &w, std::vector<double> &remacro
         const Cell &c = o.cell[ie];
         int m = c.matter;
         V3 vv = o.v(m, b, d);
-        double t = o.tau[m * o.nb + b];
+        double t = o.tau[m * o.nb + b] * o.tsc[ie];
         for (const Face &f : c.f) {
             double dp = dot(vv, f.n);
             double temp = t * f.area / c.vol * dp;
@@ -687,7 +700,7 @@ void bte_pair(Oracle &o, int b, int d, PairWork &w, std::vector<double> &remacro
             V3 vv = o.v(c.matter, b, d);
             double dp = dot(vv, f.n);
             if (dp < 0) {
-                double temp = o.tau[c.matter * o.nb + b] * f.area / c.vol * dp;
+                double temp = o.tau[c.matter * o.nb + b] * o.tsc[ie] * f.area / c.vol * dp;
                 w.R[ie] -= temp * o.eb(b, d, ib, ic);
             }
         }
@@ -700,7 +713,7 @@ void bte_pair(Oracle &o, int b, int d, PairWork &w, std::vector<double> &remacro
         for (int ie = 0; ie < nc; ie++) {
             const Cell &c = o.cell[ie];
             V3 vv = o.v(c.matter, b, d);
-            double t = o.tau[c.matter * o.nb + b];
+            double t = o.tau[c.matter * o.nb + b] * o.tsc[ie];
             double vd = 0;
             for (const Face &f : c.f) {
                 double dp = dot(vv, f.n);
@@ -914,6 +927,31 @@ void set_bound_ee_1(Oracle &o) {
                             }
                         }
                         e = o.eb(b, nf, ib, ic);
+                    } else if (B.type == 6) {
+                        // extension: p x (outgoing direction nearest the
+                        // mirror image) + (1 - p) x the diffuse value
+                        double s1 = 0, s2 = 0;
+                        for (int k = 0; k < o.nd; k++) {
+                            double d1 = dot(o.v(m, b, k), f.n);
+                            if (d1 >= 0) {
+                                s1 += o.eb(b, k, ib, ic) * (d1 * o.mw[k]);
+                                s2 += (d1 * o.mw[k]);
+                            }
+                        }
+                        double d1 = dot(o.dir[d], f.n);
+                        V3 r = {o.dir[d].x - f.n.x * d1 * 2, o.dir[d].y - f.n.y * d1 * 2, o.dir[d].z - f.n.z * d1 * 2};
+                        double close = 1e300;
+                        int nf = -1;
+                        for (int k = 0; k < o.nd; k++) {
+                            if (dot(o.dir[k], f.n) < 0) continue;
+                            double l = std::pow(r.x - o.dir[k].x, 2) + std::pow(r.y - o.dir[k].y, 2) +
+                                       std::pow(r.z - o.dir[k].z, 2);
+                            if (l < close) {
+                                nf = k;
+                                close = l;
+                            }
+                        }
+                        e = B.T * o.eb(b, nf, ib, ic) + (1.0 - B.T) * (s1 / s2);
                     } else if (B.type < 0) {
                         e = o.eb(b, d, B.connect, ic) + o.C[m * o.nb + b] * (B.T - o.bnd[B.connect].T);
                     } else {
@@ -1089,7 +1127,8 @@ int oracle_solve(int dim, int nn, const double *xyz, int nc, const int *cptr, co
                  const double *C, const double *lat, const double *hr, const int *reg_mat, int nreg, int material_dim,
                  int angle_method, int ntheta, int nphi, double Lx, const double *cell_heat, const double *T0,
                  const double *q0, int max_iter, double errT, double errq, int use_limiter, double *out_Tlat,
-                 double *out_E, double *out_q, double *out_Tband, int *out_iters, double *out_err) {
+                 double *out_E, double *out_q, double *out_Tband, int *out_iters, double *out_err,
+                 const double *cell_scatter) {
     Oracle o;
     o.nmat = nmat;
     o.nb = nband;
@@ -1099,6 +1138,9 @@ int oracle_solve(int dim, int nn, const double *xyz, int nc, const int *cptr, co
                         reg_mat, nreg);
     if (rc) return rc;
     for (int i = 0; i < nc; i++) o.cell[i].heat = cell_heat ? cell_heat[i] : 0.0;
+    o.tsc.assign(nc, 1.0);
+    if (cell_scatter)
+        for (int i = 0; i < nc; i++) o.tsc[i] = 1.0 / cell_scatter[i];
     o.vg.assign(v, v + nmat * nband);
     o.tau.assign(tau, tau + nmat * nband);
     o.C.assign(C, C + nmat * nband);

@@ -1,0 +1,211 @@
+"""GPU: the adjoint (gbte_vjp) of the converged FP64 solve.
+
+The parameters are those of the adjoint workload:
+- a multiplier on each band's relaxation time;
+- a per-cell scattering multiplier field, log-normal with sigma 0.2 and seed 2;
+- the specularity p = 0.3 of a partially specular pore wall.
+The objective is k_x, the effective conductivity along the 1 K periodic jump.
+
+The adjoint gradient is checked against central finite differences (relative
+step 1e-6) of the forward solve run on the GPU, and against central
+differences of the CPU oracle's solve (the FP64 reference gradient). Both
+sides are converged to 1e-12 margins. The agreement asked for is 1e-4.
+First, the two forward extensions (per-cell multiplier, partial specularity)
+are checked against the oracle.
+"""
+import dataclasses
+import functools
+
+import numpy as np
+import pytest
+
+import giftbte_b200 as g
+import oracle
+from giftbte_b200 import decks
+
+pytestmark = pytest.mark.gpu
+
+L = 300e-9      # cell side: k_x = <q_x>_V L / dT with dT = 1 K
+TOL = 1e-4      # adjoint vs finite differences
+H = 1e-6        # relative central-difference step
+
+
+@functools.lru_cache(maxsize=None)
+def base_deck():
+    """Config-4 cell at h = 20 nm (405 cells), 4 bands, 16 directions."""
+    return decks.config4_deck(h_nm=20.0, n_bands=4, n_phi=4, seed=2, residual_temp=1e-12, residual_flux=1e-12,
+                              max_iter=8000)
+
+
+@functools.lru_cache(maxsize=None)
+def scatter():
+    return decks.lognormal_scatter(base_deck().mesh.n_cells, sigma=0.2, seed=2)
+
+
+def variant(tau_mult=None, p=None):
+    d = base_deck()
+    bands = d.bands
+    if tau_mult is not None:
+        bands = dataclasses.replace(bands, tau=bands.tau * tau_mult)
+    bcs = [b if (b.tag != 5 or p is None) else decks.BC(5, 6, p) for b in d.bcs]
+    return dataclasses.replace(d, bands=bands, bcs=bcs)
+
+
+def keff_from(q, vol):
+    return float(np.sum(q[:, 0] * vol) / vol.sum() * L / 1.0)
+
+
+def solve_gpu(d, s_c):
+    s = g.StaticBTESynthetic.from_deck(d, precision=g.GBTE_FP64, cell_scatter=s_c)
+    s.solve(allow_not_converged=False)
+    return s
+
+
+def keff_gpu(d, s_c):
+    s = solve_gpu(d, s_c)
+    _, vol = s.geometry()
+    k = keff_from(s.fields()["q"], vol)
+    s.close()
+    return k
+
+
+@functools.lru_cache(maxsize=None)
+def volumes():
+    s = g.StaticBTESynthetic.from_deck(base_deck(), precision=g.GBTE_FP64)
+    _, vol = s.geometry()
+    s.close()
+    return vol
+
+
+def keff_oracle(d, s_c):
+    o = oracle.solve(d, cell_scatter=s_c)
+    return keff_from(o["q"], volumes())
+
+
+@functools.lru_cache(maxsize=None)
+def adjoint():
+    s = solve_gpu(base_deck(), scatter())
+    qb = s.keff_cotangent(axis=0, length=L, delta_T=1.0)
+    out = s.vjp(q_bar=qb)
+    out["J"] = float(np.sum(qb * s.fields()["q"]))
+    s.close()
+    return out
+
+
+def components(n_cells=5):
+    """(name, perturbed deck and multipliers) pairs for the checked
+    components: every band multiplier, the pore wall's specularity, the
+    cells with the largest adjoint sensitivity, and a seeded random
+    direction over all cell multipliers."""
+    a = adjoint()
+    nb = base_deck().bands.n_bands
+    out = []
+    for b in range(nb):
+        def f(h, b=b):
+            m = np.ones(nb)
+            m[b] += h
+            return variant(tau_mult=m), scatter()
+        out.append((f"tau[{b}]", a["tau"][b], f))
+
+    def fp(h):
+        return variant(p=0.3 + h), scatter()
+    spec_row = [i for i, b in enumerate(base_deck().bcs) if b.tag == 5][0]
+    out.append(("p", a["specularity"][spec_row], fp))
+    top = np.argsort(-np.abs(a["scatter"]))[:n_cells]
+    for c in top:
+        def fc(h, c=int(c)):
+            s = scatter().copy()
+            s[c] *= 1 + h
+            return base_deck(), s
+        # d/d(ln s_c) = s_c dJ/ds_c
+        out.append((f"s[{c}]", a["scatter"][c] * scatter()[c], fc))
+    v = np.random.default_rng(20).standard_normal(base_deck().mesh.n_cells)
+
+    def fv(h):
+        return base_deck(), scatter() * (1 + h * v)
+    out.append(("s.v", float(np.dot(a["scatter"] * scatter(), v)), fv))
+    return out
+
+
+def check(keff, label):
+    rows = []
+    scale = max(abs(x) for _, x, _ in components())
+    for name, g_adj, make in components():
+        kp = keff(*make(H))
+        km = keff(*make(-H))
+        fd = (kp - km) / (2 * H)
+        err = abs(g_adj - fd) / max(abs(fd), 1e-2 * scale)
+        rows.append((name, g_adj, fd, err))
+    text = "\n".join(f"{label} {n:8s} adjoint {a: .10e} fd {f: .10e} rel {e:.2e}" for n, a, f, e in rows)
+    print(text)
+    assert max(r[3] for r in rows) <= TOL, text
+
+
+def test_extensions_match_oracle():
+    # per-cell scattering multipliers and a partially specular wall: the
+    # CUDA forward against the oracle
+    d = base_deck()
+    s = solve_gpu(d, scatter())
+    f = s.fields()
+    s.close()
+    o = oracle.solve(d, cell_scatter=scatter())
+    assert np.max(np.abs(f["T"] - o["T"])) / np.max(np.abs(o["T"])) <= 1e-9
+    assert np.max(np.abs(f["q"] - o["q"])) / np.max(np.abs(o["q"])) <= 1e-8
+
+
+def test_adjoint_converged():
+    st = adjoint()["stats"]
+    assert st["change"] <= 1e-12 and st["picard_steps"] >= 1 and st["iterations"] > 1
+
+
+def test_adjoint_matches_gpu_finite_differences():
+    check(keff_gpu, "gpu-fd")
+
+
+def test_adjoint_matches_oracle_finite_differences():
+    check(keff_oracle, "oracle-fd")
+
+
+def test_temperature_objective():
+    # mean macro temperature of the cells with x < L/4: the temperature
+    # cotangent enters through the transposed synthetic correction
+    s = solve_gpu(base_deck(), scatter())
+    cen, vol = s.geometry()
+    sel = cen[:, 0] < 0.25 * L
+    Tb = np.where(sel, vol, 0.0) / vol[sel].sum()
+    a = s.vjp(T_bar=Tb)
+    s.close()
+
+    def J(d, s_c):
+        t = solve_gpu(d, s_c)
+        v = float(np.dot(Tb, t.fields()["T"]))
+        t.close()
+        return v
+    nb = base_deck().bands.n_bands
+    for b in (0, nb - 1):
+        m = np.ones(nb)
+        m[b] += H
+        jp = J(variant(tau_mult=m), scatter())
+        m[b] -= 2 * H
+        jm = J(variant(tau_mult=m), scatter())
+        fd = (jp - jm) / (2 * H)
+        scale = np.max(np.abs(a["tau"]))
+        assert abs(a["tau"][b] - fd) <= TOL * max(abs(fd), 1e-2 * scale), (b, a["tau"][b], fd)
+    jp = J(variant(p=0.3 + H), scatter())
+    jm = J(variant(p=0.3 - H), scatter())
+    fd = (jp - jm) / (2 * H)
+    row = [i for i, b in enumerate(base_deck().bcs) if b.tag == 5][0]
+    assert abs(a["specularity"][row] - fd) <= TOL * max(abs(fd), 1e-12), (a["specularity"][row], fd)
+
+
+def test_adjoint_rejects_unsupported():
+    d = base_deck()
+    s = g.StaticBTESynthetic.from_deck(d, precision=g.GBTE_FP32_MIXED)
+    s.solve(max_iter=3, err_temp=0.0, err_flux=0.0)
+    with pytest.raises(g.GBTEError):
+        s.vjp(q_bar=np.zeros((d.mesh.n_cells, 3)))
+    s.close()
+    s = g.StaticBTESynthetic.from_deck(d, precision=g.GBTE_FP64)
+    with pytest.raises(g.GBTEError):
+        s.vjp(q_bar=np.zeros((d.mesh.n_cells, 3)))
+    s.close()
