@@ -422,12 +422,12 @@ def run_config4(args, rank: int):
     d = decks.config4_deck(h_nm=3.0, n_bands=40, n_phi=16, seed=0, specularity=0.3)
     nc = d.mesh.n_cells
     sc = decks.lognormal_scatter(nc, sigma=0.2, seed=2)
-    s = g.StaticBTESynthetic.from_deck(d, precision=g.GBTE_FP64, cell_scatter=sc, max_iter=args.max_iter_e2e)
+    s = g.StaticBTESynthetic.from_deck(d, precision=g.GBTE_FP64, cell_scatter=sc, max_iter=args.adj_max_iter)
     clocks = ClockSampler(0)
     clocks.start()
-    st = s.solve(err_temp=args.adj_residual, err_flux=args.adj_residual, max_iter=args.max_iter_e2e)
+    st = s.solve(err_temp=args.adj_residual, err_flux=args.adj_residual, max_iter=args.adj_max_iter)
     qb = s.keff_cotangent(axis=0, length=300e-9, delta_T=1.0)
-    a = s.vjp(q_bar=qb, tol=args.adj_residual)
+    a = s.vjp(q_bar=qb, tol=args.adj_residual, max_iter=args.adj_max_iter)
     clk = clocks.stop()
     keff = float(np.sum(qb * s.fields()["q"]))
     nb, nd = s.num_bands, s.num_directions
@@ -514,7 +514,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
     ap.add_argument("--workload", choices=["config2", "config1", "config3", "config4", "config5"], default="config2")
-    ap.add_argument("--adj-residual", type=float, default=1e-10, help="config4: forward margins and adjoint tolerance")
+    ap.add_argument("--adj-residual", type=float, default=1e-8, help="config4: forward margins and adjoint tolerance")
+    ap.add_argument("--adj-max-iter", type=int, default=20000, help="config4: adjoint iteration cap")
     ap.add_argument("--batch", type=int, default=256, help="config5: number of independent cells")
     ap.add_argument("--h-nm", type=float, default=0.0, help="config3 mesh spacing (default 2.5 nm)")
     ap.add_argument("--cell-order", type=int, choices=[0, 1], default=0,

@@ -362,11 +362,13 @@ class StaticBTESynthetic:
         return c.reshape(nc, 3), v
 
     def vjp(self, T_bar: Optional[np.ndarray] = None, q_bar: Optional[np.ndarray] = None, max_iter: int = 10000,
-            tol: float = 1e-12) -> dict:
+            tol: float = 1e-10) -> dict:
         """Gradient of J = <T_bar, T> + <q_bar, q> at the fixed point the last
         solve reached (gbte_vjp): ``tau`` (per band, multiplier on its
         relaxation time), ``scatter`` (per cell, its scattering multiplier),
-        ``specularity`` (per boundary-table row; partially specular rows)."""
+        ``specularity`` (per boundary-table row; partially specular rows).
+        The transposed iteration stops when the gradient's relative change
+        between iterations is <= tol."""
         nc, nb = self.num_cells, self.num_bands
         Tb = np.ascontiguousarray(T_bar, dtype=np.float64) if T_bar is not None else None
         qb = np.ascontiguousarray(q_bar, dtype=np.float64).reshape(-1) if q_bar is not None else None

@@ -1494,6 +1494,7 @@ void *Solver::dalloc(size_t bytes) {
 Solver::~Solver() {
     if (cfg.device >= 0) cudaSetDevice(cfg.device);
     if (cfg.stream) cudaStreamSynchronize(cfg.stream);
+    if (tgraph_) cudaGraphExecDestroy(tgraph_);
     for (void *p : allocs_) cudaFree(p);
     if (h_pinned_) cudaFreeHost(h_pinned_);
     if (h_comp_) cudaFreeHost(h_comp_);
@@ -1788,6 +1789,7 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
     }
     dif_w_ = up_d(difw);
     spec_src_ = up_i(spec);
+    spec_h_ = spec;
     // periodic macro-temperature overrides (StaticBTESynthetic.cpp:2258-2273)
     std::vector<double> ovr(nbs, std::numeric_limits<double>::quiet_NaN());
     for (int ib = 0; ib < mesh.nbd(); ib++)
@@ -1983,7 +1985,7 @@ Error Solver::alloc_all() {
         if (!pp)
             return {-6, "device allocation failed (" + std::to_string(ne * S * (3 + mesh.dim) / 1048576) +
                             " MiB of band state)"};
-    if (cudaMallocHost((void **)&h_pinned_, 16 * sizeof(double)) != cudaSuccess) return {-6, "pinned allocation failed"};
+    if (cudaMallocHost((void **)&h_pinned_, 64 * sizeof(double)) != cudaSuccess) return {-6, "pinned allocation failed"};
     if (cudaMallocHost((void **)&h_comp_, 4 * (size_t)ncomp_ * sizeof(double)) != cudaSuccess)
         return {-6, "pinned allocation failed"};
     if (!red_ || !comp_ptr_d_ || !comp_done_d_) return {-6, "device allocation failed (reductions)"};
@@ -2444,10 +2446,10 @@ Error Solver::solve_t(SolveStats &st) {
         L.rvec = ((L.nbc * sizeof(S)) % 16 == 0 && (nb * sizeof(S)) % 16 == 0 && (last * sizeof(S)) % 16 == 0) ? 1 : 0;
         return true;
     };
+    // every sweep launch stays within 220 KB of dynamic shared memory: the
+    // limit is raised once, outside any stream capture
+    CUDA_TRY(cudaFuncSetAttribute(k_sweep<S, LOOK, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
     auto launch_sweep = [&](const SweepLaunch &L, int d0, int nbt) -> cudaError_t {
-        cudaError_t e = cudaFuncSetAttribute(k_sweep<S, LOOK, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)L.smem);
-        if (e != cudaSuccess) return e;
         const int blocks = nbt * ncomp_ * L.chunks;
         k_sweep<S, LOOK, LCAP><<<blocks, L.threads, L.smem, s>>>(nb, nc, ncomp_, d0, L.nbc, ring_, far_slots_, L.rvec,
                                                                    lvl_ptr_, dir_lvl_off_, (const SweepRec<S> *)rec_,
@@ -2502,6 +2504,10 @@ Error Solver::solve_t(SolveStats &st) {
     bool converged = false;
     for (nt = 0; nt < cfg.max_iter; nt++) {
         CUDA_TRY(cudaEventRecord(ev_[0], s));
+        // transport stage, copy() through the wall temperatures: from the
+        // first iteration after the autotuner on, one CUDA graph replayed
+        // per iteration (its kernels and arguments do not change)
+        auto transport = [&]() -> Error {
         // copy() (:2655-2690)
         CUDA_TRY(cudaMemcpyAsync(Told_, T_, nc * 8, cudaMemcpyDeviceToDevice, s));
         CUDA_TRY(cudaMemcpyAsync(qold_, q_, (size_t)nc * 24, cudaMemcpyDeviceToDevice, s));
@@ -2566,6 +2572,37 @@ Error Solver::solve_t(SolveStats &st) {
         gather();
         GL(K_MACRO_BC, k_macro_bc<<<gW, kThreads, 0, s>>>(dm_, dp_, eb_, bTovr_, bTm_));
         CUDA_TRY(cudaGetLastError());
+        return {0, ""};
+        };
+        const bool graphable = graph_ok_ && !(tune && nt == 0) && !cfg.profile;
+        if (graphable && !tgraph_) {
+            // capture once; any failure leaves the direct launches in place
+            cudaGraph_t gr = nullptr;
+            const long long l0 = launches_;
+            if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                Error te = transport();
+                const cudaError_t ce = cudaStreamEndCapture(s, &gr);
+                if (te.code == 0 && ce == cudaSuccess && gr &&
+                    cudaGraphInstantiate(&tgraph_, gr, 0) == cudaSuccess) {
+                    tgraph_launches_ = launches_ - l0;
+                } else {
+                    tgraph_ = nullptr;
+                    graph_ok_ = false;
+                }
+                if (gr) cudaGraphDestroy(gr);
+            } else {
+                graph_ok_ = false;
+            }
+            launches_ = l0;
+            cudaGetLastError();
+        }
+        if (graphable && tgraph_) {
+            CUDA_TRY(cudaGraphLaunch(tgraph_, s));
+            launches_ += tgraph_launches_;
+        } else {
+            Error te = transport();
+            if (te.code) return te;
+        }
         CUDA_TRY(cudaEventRecord(ev_[1], s));
         // _marco_solution: Picard on the non-orthogonal correction
         GL(K_COPY, k_copy<<<gC, kThreads, 0, s>>>(Tlat_, T_, nc));
@@ -3079,6 +3116,133 @@ __global__ void __launch_bounds__(256) k_adj_transport(DMesh m, DPhys p, const d
     }
 }
 
+// k_adj_transport for BC consecutive bands per thread (nb a multiple of
+// BC): the cell's geometry and moment cotangents are loaded once for BC
+// bands and the band values move as 16-byte vectors; tvc = (1/s_c)/V_c
+template <int DIM, int BC>
+__global__ void __launch_bounds__(256) k_adj_transport4(DMesh m, DPhys p, const double *__restrict__ tvc,
+                                                        const double *__restrict__ lam, const double *__restrict__ Tlbar,
+                                                        const double *__restrict__ Thbar, const double *__restrict__ Qbar,
+                                                        const double *__restrict__ qbar, const double *__restrict__ Thsbar,
+                                                        const double *__restrict__ Qsbar, const double *__restrict__ bTmbar,
+                                                        double *__restrict__ ebar, double *__restrict__ gbar,
+                                                        double *__restrict__ ebb) {
+    const int nb = p.nb, nc = m.nc, nbc = nb / BC;
+    const size_t total = (size_t)p.nd * nc * nbc;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b0 = BC * (int)(t % nbc);
+        const size_t dc = t / nbc;
+        const int c = (int)(dc % nc);
+        const int d = (int)(dc / nc);
+        const double w = p.w[d], sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
+        double lc[BC], e[BC], oc[BC], gx[BC], gy[BC], gz[BC], tau[BC], vm[BC];
+        ld8(lam + dc * nb + b0, lc);
+        const double tl = Tlbar[c], th = Thbar[c], tv = tvc[c];
+        const double *q = Qbar + 6 * (size_t)c;
+        const double qss = q[0] * sx * sx + q[1] * sx * sy + q[2] * sx * sz + q[3] * sy * sy + q[4] * sy * sz + q[5] * sz * sz;
+        const double qs = qbar ? sx * qbar[3 * c] + sy * qbar[3 * c + 1] + sz * qbar[3 * c + 2] : 0.0;
+#pragma unroll
+        for (int i = 0; i < BC; i++) {
+            const int b = b0 + i;
+            tau[i] = p.tau[b];
+            vm[i] = p.vmag[b];
+            const double lw = p.lat[b] * w / p.C[b];
+            e[i] = -lc[i] + lw * tl + vm[i] * w * qs;
+            if (p.hr[b] > 0) e[i] += p.kappa * lw * th + w * tau[i] * vm[i] * vm[i] * qss;
+            oc[i] = tau[i] * tv * lc[i];
+            gx[i] = gy[i] = gz[i] = 0;
+        }
+        for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+            const double sn = sx * m.cf_nx[k] + sy * m.cf_ny[k] + (DIM == 3 ? sz * m.cf_nz[k] : 0.0);
+            const double A = m.cf_area[k];
+            if (sn >= 0) {
+                const double rx = m.cf_fx[k] - m.cx[c], ry = m.cf_fy[k] - m.cy[c], rz = m.cf_fz[k] - m.cz[c];
+                double f[BC];
+#pragma unroll
+                for (int i = 0; i < BC; i++) f[i] = -oc[i];
+                if (m.cf_bound[k] < 0) {
+                    const int j = m.cf_nbr[k];
+                    double lj[BC];
+                    ld8(lam + ((size_t)d * nc + j) * nb + b0, lj);
+                    const double tj = tvc[j];
+#pragma unroll
+                    for (int i = 0; i < BC; i++) f[i] += tau[i] * tj * lj[i];
+                }
+#pragma unroll
+                for (int i = 0; i < BC; i++) {
+                    const double fi = f[i] * A * vm[i] * sn;
+                    e[i] += fi;
+                    gx[i] += fi * rx;
+                    gy[i] += fi * ry;
+                    if (DIM == 3) gz[i] += fi * rz;
+                }
+            } else if (m.cf_bound[k] >= 0) {
+                const int s = m.cf_bside[k];
+                double o[BC];
+#pragma unroll
+                for (int i = 0; i < BC; i++)
+                    o[i] = -oc[i] * A * vm[i] * sn + adj_side_entry(m, p, d, s, b0 + i, Thsbar, Qsbar, bTmbar);
+                st8(ebb + ((size_t)d * m.nbs + s) * nb + b0, o);
+            }
+        }
+        st8(ebar + dc * nb + b0, e);
+        double *gp = gbar + dc * DIM * nb + b0;
+        st8(gp, gx);
+        st8(gp + nb, gy);
+        if (DIM == 3) st8(gp + 2 * nb, gz);
+    }
+}
+
+// k_adj_gradT for BC consecutive bands per thread
+template <int DIM, int BC>
+__global__ void __launch_bounds__(256) k_adj_gradT4(DMesh m, DPhys p, const double *__restrict__ tvc,
+                                                    const int *__restrict__ tptr, const int *__restrict__ tidx,
+                                                    const double *__restrict__ tw, const double *__restrict__ wsum,
+                                                    const int *__restrict__ opp, const int *__restrict__ pos_of,
+                                                    const double *__restrict__ ebar, const double *__restrict__ gbar,
+                                                    double *__restrict__ Rlo) {
+    const int nb = p.nb, nc = m.nc, nbc = nb / BC;
+    const size_t total = (size_t)p.nd * nc * nbc;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b0 = BC * (int)(t % nbc);
+        const size_t dc = t / nbc;
+        const int j = (int)(dc % nc);
+        const int d = (int)(dc / nc);
+        const double *gd = gbar + ((size_t)d * nc) * DIM * nb + b0;
+        double acc[BC], gx[BC], gy[BC], gz[BC];
+        ld8(ebar + dc * nb + b0, acc);
+        for (int q = tptr[j]; q < tptr[j + 1]; q++) {
+            const double *g = gd + (size_t)tidx[q] * DIM * nb;
+            const double wx = tw[3 * q], wy = tw[3 * q + 1], wz = tw[3 * q + 2];
+            ld8(g, gx);
+            ld8(g + nb, gy);
+            if (DIM == 3) ld8(g + 2 * nb, gz);
+#pragma unroll
+            for (int i = 0; i < BC; i++) {
+                acc[i] += wx * gx[i] + wy * gy[i];
+                if (DIM == 3) acc[i] += wz * gz[i];
+            }
+        }
+        {
+            const double *g = gd + (size_t)j * DIM * nb;
+            const double wx = wsum[3 * j], wy = wsum[3 * j + 1], wz = wsum[3 * j + 2];
+            ld8(g, gx);
+            ld8(g + nb, gy);
+            if (DIM == 3) ld8(g + 2 * nb, gz);
+#pragma unroll
+            for (int i = 0; i < BC; i++) {
+                acc[i] -= wx * gx[i] + wy * gy[i];
+                if (DIM == 3) acc[i] -= wz * gz[i];
+            }
+        }
+        const double tv = tvc[j];
+#pragma unroll
+        for (int i = 0; i < BC; i++) acc[i] *= tv;
+        const int od = opp[d];
+        st8(Rlo + ((size_t)od * nc + pos_of[(size_t)od * nc + j]) * nb + b0, acc);
+    }
+}
+
 // per (wall side, band): sum of the incoming entries' cotangents (the
 // diffuse re-emission's transpose reads it once per outgoing direction)
 __global__ void k_adj_dsum(DMesh m, DPhys p, const double *__restrict__ ebb, double *__restrict__ dbar) {
@@ -3103,8 +3267,8 @@ __global__ void k_adj_dsum(DMesh m, DPhys p, const double *__restrict__ ebb, dou
 // outgoing wall entries: side-moment cotangent plus the transpose of the
 // incoming gather (k_diffuse_sum + k_gather) from this side or, for
 // periodic walls, from the sides that read it
-__global__ void k_adj_ebout(DMesh m, DPhys p, const double *__restrict__ dif_w, const int *__restrict__ spec_src,
-                            const double *__restrict__ dbar, const int *__restrict__ per_ptr,
+__global__ void k_adj_ebout(DMesh m, DPhys p, const double *__restrict__ dif_w, const int *__restrict__ sinv_ptr,
+                            const int *__restrict__ sinv_idx, const double *__restrict__ dbar, const int *__restrict__ per_ptr,
                             const int *__restrict__ per_idx, const double *__restrict__ Thsbar,
                             const double *__restrict__ Qsbar, const double *__restrict__ bTmbar, double *ebb) {
     const int nb = p.nb;
@@ -3126,11 +3290,11 @@ __global__ void k_adj_ebout(DMesh m, DPhys p, const double *__restrict__ dif_w, 
                 v += f * dif_w[(size_t)s * p.nd + d] * dbar[(size_t)s * nb + b];
             }
             if (type == 3 || type == 6) {
+                // the incoming directions whose mirror source is d
                 const double f = type == 6 ? m.b_T[ib] : 1.0;
-                for (int q = 0; q < p.nd; q++) {
-                    if (p.sx[q] * nx + p.sy[q] * ny + p.sz[q] * nz >= 0) continue;
-                    if (spec_src[(size_t)s * p.nd + q] == d) v += f * ebb[((size_t)q * m.nbs + s) * nb + b];
-                }
+                const size_t sd = (size_t)s * p.nd + d;
+                for (int r = sinv_ptr[sd]; r < sinv_ptr[sd + 1]; r++)
+                    v += f * ebb[((size_t)sinv_idx[r] * m.nbs + s) * nb + b];
             }
             for (int r = per_ptr[s]; r < per_ptr[s + 1]; r++) {
                 const int s2 = per_idx[r];
@@ -3396,13 +3560,43 @@ Error Solver::adj_setup() {
         pptr[q + 1] = pptr[q] + (int)readers[q].size();
         for (int r : readers[q]) pidx.push_back(r);
     }
+    // inverse specular map: for (side, outgoing direction) the incoming
+    // directions that read it
+    std::vector<int> sptr((size_t)nbs * nd + 1, 0), sidx;
+    for (int sd = 0; sd < nbs; sd++) {
+        const int c = mesh.bs_cell[sd];
+        const int type = c >= 0 ? mesh.b_type[sd >> 1] : 0;
+        if (type != 3 && type != 6) continue;
+        const int k = mesh.bs_cf[sd];
+        for (int q = 0; q < nd; q++)
+            if (ang.sx[q] * mesh.cf_nx[k] + ang.sy[q] * mesh.cf_ny[k] + ang.sz[q] * mesh.cf_nz[k] < 0)
+                sptr[(size_t)sd * nd + spec_h_[(size_t)sd * nd + q] + 1]++;
+    }
+    for (size_t i = 0; i < (size_t)nbs * nd; i++) sptr[i + 1] += sptr[i];
+    sidx.resize(sptr.back());
+    {
+        std::vector<int> fill(sptr.begin(), sptr.end() - 1);
+        for (int sd = 0; sd < nbs; sd++) {
+            const int c = mesh.bs_cell[sd];
+            const int type = c >= 0 ? mesh.b_type[sd >> 1] : 0;
+            if (type != 3 && type != 6) continue;
+            const int k = mesh.bs_cf[sd];
+            for (int q = 0; q < nd; q++)
+                if (ang.sx[q] * mesh.cf_nx[k] + ang.sy[q] * mesh.cf_ny[k] + ang.sz[q] * mesh.cf_nz[k] < 0)
+                    sidx[fill[(size_t)sd * nd + spec_h_[(size_t)sd * nd + q]]++] = q;
+        }
+    }
     adj_nT_ = tidx.size();
+    adj_nsinv_ = sidx.size();
     adj_nbcell_ = bcell.size();
     adj_nper_ = pidx.size();
     std::vector<int> ints;
-    for (auto *v : {&tptr, &tidx, &bcell, &pptr, &pidx, &opp}) ints.insert(ints.end(), v->begin(), v->end());
+    for (auto *v : {&tptr, &tidx, &bcell, &pptr, &pidx, &opp, &sptr, &sidx}) ints.insert(ints.end(), v->begin(), v->end());
     std::vector<double> dbl(tw);
     dbl.insert(dbl.end(), wsum.begin(), wsum.end());
+    // tau scale over volume per cell: (1/s_c) / V_c
+    for (int c = 0; c < nc; c++)
+        dbl.push_back((cfg.cell_scatter.empty() ? 1.0 : 1.0 / cfg.cell_scatter[c]) / mesh.vol[c]);
     bool ok = true;
     adj_int_ = upload(this, allocs_, ints, s, ok);
     adj_wt_ = upload(this, allocs_, dbl, s, ok);
@@ -3414,7 +3608,7 @@ Error Solver::adj_setup() {
     // per cell: 16 (Tbar, z, zsum, rbar, Thbar, Qbar x6, U, Tuser, qbar x3);
     // per node slot: 8 (TVbar, ThVbar, QVbar x6); per wall side: 8 (Thsbar,
     // Qsbar x6, bTmbar); then g_tau, g_bnd and two reduction slots
-    adj_cell_ = (double *)dalloc((16 * (size_t)nc + 8 * nslot + 8 * (size_t)nbs + bands.nb + mesh.nbd() + 8) * 8);
+    adj_cell_ = (double *)dalloc((16 * (size_t)nc + 8 * nslot + 8 * (size_t)nbs + bands.nb + mesh.nbd() + 40) * 8);
     adj_lam_ = (double *)dalloc(ne * 8);
     CUDA_TRY(cudaStreamSynchronize(s));
     if (!ok || !adj_ebar_ || !adj_ebb_ || !adj_dbar_ || !adj_cell_ || !adj_lam_) {
@@ -3447,8 +3641,8 @@ Error Solver::vjp(const double *Tbar_h, const double *qbar_h, int max_iter, doub
            *Thsbar = QVbar + 6 * (size_t)nslot, *Qsbar = Thsbar + nbs, *bTmbar = Qsbar + 6 * (size_t)nbs,
            *gtau = bTmbar + nbs, *gbnd = gtau + nb, *red = gbnd + nbd, *gcell = z;  // g_cell reuses z at the end
     const int *tptr = adj_int_, *tidx = tptr + nc + 1, *bcell = tidx + adj_nT_, *pptr = bcell + adj_nbcell_,
-              *pidx = pptr + nbs + 1, *opp = pidx + adj_nper_;
-    const double *tw = adj_wt_, *wsum = adj_wt_ + 3 * adj_nT_;
+              *pidx = pptr + nbs + 1, *opp = pidx + adj_nper_, *sptr = opp + nd, *sidx = sptr + (size_t)nbs * nd + 1;
+    const double *tw = adj_wt_, *wsum = adj_wt_ + 3 * adj_nT_, *tvc = wsum + 3 * (size_t)nc;
     double *lam = adj_lam_, *ebar = adj_ebar_, *ebb = adj_ebb_, *gbar = (double *)grad_, *Rlo = (double *)res_;
     const double *eps = (const double *)eps_;
     if (Tbar_h) CUDA_TRY(cudaMemcpyAsync(Tuser, Tbar_h, (size_t)nc * 8, cudaMemcpyHostToDevice, s));
@@ -3484,16 +3678,31 @@ Error Solver::vjp(const double *Tbar_h, const double *qbar_h, int max_iter, doub
     CUDA_TRY(cudaFuncSetAttribute(k_sweep<double, LOOK, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int N = last_inner_;
     long long cg_its = 0;
+    // warm starts of the reverse Picard solves: each step's solution of the
+    // previous adjoint iteration
+    if (adj_warm_n_ < N) {
+        adj_warm_ = (double *)dalloc((size_t)N * nc * 8);
+        if (!adj_warm_) return {-6, "device allocation failed (adjoint warm starts)"};
+        adj_warm_n_ = N;
+    }
+    bool warm = false;
     // one evaluation of (dF/de)^T lam + dJ/de (without the gradient's
     // transpose) and of the macro cotangents
-    auto evaluate = [&]() -> Error {
-        k_adj_tbar<<<gWc, kThreads, 0, s>>>(dm_, dp_, lam, Tuser, Tb);
+    auto evaluate = [&](const double *L, bool obj, bool warm_ok) -> Error {
+        warm = warm && warm_ok;
+        const double *Tu = obj ? Tuser : nullptr, *qu = obj ? qbar : nullptr;
+        k_adj_tbar<<<gWc, kThreads, 0, s>>>(dm_, dp_, L, Tu, Tb);
         CUDA_TRY(cudaMemsetAsync(zsum, 0, (size_t)nc * 8, s));
         for (int k = N - 1; k >= 0; k--) {
-            CUDA_TRY(cudaMemsetAsync(z, 0, (size_t)nc * 8, s));
-            Error ce = cg_solve(kplan_, K_ptr_, K_idx_, K_val_, K_dinv_, z, Tb, cfg.macro_rtol, 0.0, cg_its, cg_scal_,
-                                cg_r_, cg_z_, cg_p_, cg_Ap_, nullptr, nullptr);
+            double *wk = adj_warm_ + (size_t)k * nc;
+            if (warm)
+                CUDA_TRY(cudaMemcpyAsync(z, wk, (size_t)nc * 8, cudaMemcpyDeviceToDevice, s));
+            else
+                CUDA_TRY(cudaMemsetAsync(z, 0, (size_t)nc * 8, s));
+            Error ce = cg_solve(kplan_, K_ptr_, K_idx_, K_val_, K_dinv_, z, Tb, cfg.macro_rtol, warm ? kWarmEta : 0.0,
+                                cg_its, cg_scal_, cg_r_, cg_z_, cg_p_, cg_Ap_, nullptr, nullptr);
             if (ce.code) return ce;
+            CUDA_TRY(cudaMemcpyAsync(wk, z, (size_t)nc * 8, cudaMemcpyDeviceToDevice, s));
             CUDA_TRY(cudaMemsetAsync(TVbar, 0, (size_t)nslot * 8, s));
             k_adj_macro_tv<<<gC, kThreads, 0, s>>>(dm_, kappa, z, TVbar);
             CUDA_TRY(cudaMemsetAsync(Tb, 0, (size_t)nc * 8, s));
@@ -3508,14 +3717,22 @@ Error Solver::vjp(const double *Tbar_h, const double *qbar_h, int max_iter, doub
         CUDA_TRY(cudaMemsetAsync(Thsbar, 0, (size_t)nbs * 8 * 7, s));
         k_adj_remacro<<<gC, kThreads, 0, s>>>(dm_, rbar, Thbar, Qbar, Thsbar, Qsbar, ThVbar, QVbar);
         k_adj_node<<<gN, kThreads, 0, s>>>(dm_, ThVbar, QVbar, Thbar, Qbar, Thsbar, Qsbar);
-        if (dim == 2)
-            k_adj_transport<2><<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, lam, Tb, Thbar, Qbar, qbar, Thsbar, Qsbar,
+        if (nb % 4 == 0) {
+            if (dim == 2)
+                k_adj_transport4<2, 4><<<grid_for(ne / 4), kThreads, 0, s>>>(dm_, dp_, tvc, L, Tb, Thbar, Qbar, qu,
+                                                                             Thsbar, Qsbar, bTmbar, ebar, gbar, ebb);
+            else
+                k_adj_transport4<3, 4><<<grid_for(ne / 4), kThreads, 0, s>>>(dm_, dp_, tvc, L, Tb, Thbar, Qbar, qu,
+                                                                             Thsbar, Qsbar, bTmbar, ebar, gbar, ebb);
+        } else if (dim == 2) {
+            k_adj_transport<2><<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, L, Tb, Thbar, Qbar, qu, Thsbar, Qsbar,
                                                                   bTmbar, ebar, gbar, ebb);
-        else
-            k_adj_transport<3><<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, lam, Tb, Thbar, Qbar, qbar, Thsbar, Qsbar,
+        } else {
+            k_adj_transport<3><<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, L, Tb, Thbar, Qbar, qu, Thsbar, Qsbar,
                                                                   bTmbar, ebar, gbar, ebb);
+        }
         k_adj_dsum<<<grid_for((size_t)nbs * nb), kThreads, 0, s>>>(dm_, dp_, ebb, adj_dbar_);
-        k_adj_ebout<<<grid_for((size_t)nd * nbs * nb), kThreads, 0, s>>>(dm_, dp_, dif_w_, spec_src_, adj_dbar_, pptr,
+        k_adj_ebout<<<grid_for((size_t)nd * nbs * nb), kThreads, 0, s>>>(dm_, dp_, dif_w_, sptr, sidx, adj_dbar_, pptr,
                                                                           pidx, Thsbar, Qsbar, bTmbar, ebb);
         if (adj_nbcell_) {
             if (dim == 2)
@@ -3526,57 +3743,96 @@ Error Solver::vjp(const double *Tbar_h, const double *qbar_h, int max_iter, doub
                                                                                         (int)adj_nbcell_, ebb, ebar, gbar);
         }
         CUDA_TRY(cudaGetLastError());
+        warm = true;
         return {0, ""};
     };
-    double change = 0;
-    int it = 0;
-    for (;; it++) {
-        Error ee = evaluate();
-        if (ee.code) return ee;
-        if (it > 0 && change <= tol) break;
-        if (it >= max_iter) break;
-        if (dim == 2)
+    // the rest of A^-T [(dF/de)^T L + dJ/de] after evaluate(): the
+    // gradient's transpose, the opposite-direction sweep
+    auto finish = [&]() -> Error {
+        if (nb % 4 == 0) {
+            if (dim == 2)
+                k_adj_gradT4<2, 4><<<grid_for(ne / 4), kThreads, 0, s>>>(dm_, dp_, tvc, tptr, tidx, tw, wsum, opp,
+                                                                         pos_of_, ebar, gbar, Rlo);
+            else
+                k_adj_gradT4<3, 4><<<grid_for(ne / 4), kThreads, 0, s>>>(dm_, dp_, tvc, tptr, tidx, tw, wsum, opp,
+                                                                         pos_of_, ebar, gbar, Rlo);
+        } else if (dim == 2) {
             k_adj_gradT<2><<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, tptr, tidx, tw, wsum, opp, pos_of_, ebar, gbar,
                                                               Rlo);
-        else
+        } else {
             k_adj_gradT<3><<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, tptr, tidx, tw, wsum, opp, pos_of_, ebar, gbar,
                                                               Rlo);
+        }
         k_sweep<double, LOOK, LCAP><<<nd * chunks, sthreads, smem, s>>>(nb, nc, 1, 0, nbc, ring_, far_slots_, rvec,
                                                                         lvl_ptr_, dir_lvl_off_,
                                                                         (const SweepRec<double> *)rec_, lvl_cells_, kb_,
                                                                         Rlo, (double *)corr_);
+        CUDA_TRY(cudaGetLastError());
+        return {0, ""};
+    };
+    // the gradient of the current lam (after evaluate(lam, true, ..)):
+    // per band, per cell, per boundary
+    k_adj_u<<<gC, kThreads, 0, s>>>(dm_, Q_, Qs_, QV_, U);
+    std::vector<double> hu(nc), hz(nc);
+    CUDA_TRY(cudaMemcpyAsync(hu.data(), U, (size_t)nc * 8, cudaMemcpyDeviceToHost, s));
+    const double mdim = bands.material_dim == 2 ? 2.0 : 3.0;
+    auto assemble = [&](std::vector<double> &gt, std::vector<double> &gc, std::vector<double> &gb) -> Error {
+        CUDA_TRY(cudaMemsetAsync(gtau, 0, (size_t)(nb + nbd) * 8, s));
+        k_adj_assemble<<<gWc, kThreads, nb * 8, s>>>(dm_, dp_, lam, eps, T_, Qbar, gcell, gtau);
+        k_adj_assemble_sides<<<gWs, kThreads, nb * 8, s>>>(dm_, dp_, eb_, ebb, dsum_, spec_src_, Qsbar, gtau, gbnd);
+        CUDA_TRY(cudaGetLastError());
+        gt.resize(nb);
+        gc.resize(nc);
+        gb.resize(nbd);
+        CUDA_TRY(cudaMemcpyAsync(hz.data(), zsum, (size_t)nc * 8, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaMemcpyAsync(gt.data(), gtau, (size_t)nb * 8, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaMemcpyAsync(gb.data(), gbnd, (size_t)nbd * 8, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaMemcpyAsync(gc.data(), gcell, (size_t)nc * 8, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        // kappa_bulk = sum_b C v^2 tau_b / dim: its cotangent -<zsum, U>/kappa
+        double zu = 0;
+        for (int c = 0; c < nc; c++) zu += hz[c] * hu[c];
+        const double kbar = -zu / kappa;
+        for (int b = 0; b < nb; b++) gt[b] += kbar * bands.C[b] * bands.v[b] * bands.v[b] * bands.tau[b] / mdim;
+        return {0, ""};
+    };
+    // Transposed source iteration. It stops when the gradient's relative
+    // change between iterations is <= tol (the adjoint counterpart of the
+    // forward's margins, which are relative changes of its outputs): the
+    // adjoint state itself keeps a slowly decaying component that the
+    // gradient hardly sees.
+    std::vector<double> gt, gc, gb, pt, pc, pb;
+    double change = 1.0;
+    int it = 0;
+    for (;; it++) {
+        Error ee = evaluate(lam, true, true);
+        if (ee.code) return ee;
+        ee = assemble(gt, gc, gb);
+        if (ee.code) return ee;
+        if (it > 0) {
+            double num = 0, den = 0;
+            for (int b = 0; b < nb; b++) num += (gt[b] - pt[b]) * (gt[b] - pt[b]), den += gt[b] * gt[b];
+            for (int c = 0; c < nc; c++) num += (gc[c] - pc[c]) * (gc[c] - pc[c]), den += gc[c] * gc[c];
+            for (int i = 0; i < nbd; i++) num += (gb[i] - pb[i]) * (gb[i] - pb[i]), den += gb[i] * gb[i];
+            change = den > 0 ? std::sqrt(num / den) : 0.0;
+            if (!std::isfinite(change)) return {-4, "the adjoint iteration diverged"};
+            if (change <= tol) break;
+        }
+        if (it >= max_iter) break;
+        pt.swap(gt);
+        pc.swap(gc);
+        pb.swap(gb);
+        ee = finish();
+        if (ee.code) return ee;
         CUDA_TRY(cudaMemsetAsync(red, 0, 2 * 8, s));
         k_adj_update<<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, opp, (const double *)corr_, lam, red);
         CUDA_TRY(cudaGetLastError());
-        CUDA_TRY(cudaMemcpyAsync(h_pinned_, red, 2 * 8, cudaMemcpyDeviceToHost, s));
-        CUDA_TRY(cudaStreamSynchronize(s));
-        change = h_pinned_[1] > 0 ? std::sqrt(h_pinned_[0] / h_pinned_[1]) : 0.0;
-        if (!std::isfinite(change)) return {-4, "the adjoint iteration diverged"};
     }
-    // assembly at the final lam (the evaluation above used it)
-    CUDA_TRY(cudaMemsetAsync(gtau, 0, (size_t)(nb + nbd) * 8, s));
-    k_adj_u<<<gC, kThreads, 0, s>>>(dm_, Q_, Qs_, QV_, U);
-    k_adj_assemble<<<gWc, kThreads, nb * 8, s>>>(dm_, dp_, lam, eps, T_, Qbar, gcell, gtau);
-    k_adj_assemble_sides<<<gWs, kThreads, nb * 8, s>>>(dm_, dp_, eb_, ebb, dsum_, spec_src_, Qsbar, gtau, gbnd);
-    CUDA_TRY(cudaGetLastError());
-    std::vector<double> hz(nc), hu(nc), ht(nb), hb(nbd);
-    CUDA_TRY(cudaMemcpyAsync(hz.data(), zsum, (size_t)nc * 8, cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaMemcpyAsync(hu.data(), U, (size_t)nc * 8, cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaMemcpyAsync(ht.data(), gtau, (size_t)nb * 8, cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaMemcpyAsync(hb.data(), gbnd, (size_t)nbd * 8, cudaMemcpyDeviceToHost, s));
-    if (g_cell) CUDA_TRY(cudaMemcpyAsync(g_cell, gcell, (size_t)nc * 8, cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaEventRecord(ev_[1], s));
     CUDA_TRY(cudaStreamSynchronize(s));
-    // kappa_bulk = sum_b C v^2 tau_b / dim: its cotangent -<zsum, U>/kappa
-    double zu = 0;
-    for (int c = 0; c < nc; c++) zu += hz[c] * hu[c];
-    const double kbar = -zu / kappa;
-    const double mdim = bands.material_dim == 2 ? 2.0 : 3.0;
-    if (g_tau)
-        for (int b = 0; b < nb; b++)
-            g_tau[b] = ht[b] + kbar * bands.C[b] * bands.v[b] * bands.v[b] * bands.tau[b] / mdim;
-    if (g_bnd)
-        for (int ib = 0; ib < nbd; ib++) g_bnd[ib] = hb[ib];
+    if (g_tau) std::copy(gt.begin(), gt.end(), g_tau);
+    if (g_cell) std::copy(gc.begin(), gc.end(), g_cell);
+    if (g_bnd) std::copy(gb.begin(), gb.end(), g_bnd);
     float ms = 0;
     cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
     st.iterations = it;

@@ -195,12 +195,21 @@ private:
     void prof_collect(SolveStats &st);
     long long launches_ = 0;
     int last_inner_ = 0;  // Picard steps of the last outer iteration's macro correction
+    // the transport stage of one outer iteration as a CUDA graph (built on
+    // the first iteration that is not the autotuner's; off when the stream
+    // cannot be captured)
+    cudaGraphExec_t tgraph_ = nullptr;
+    long long tgraph_launches_ = 0;
+    bool graph_ok_ = true;
     // adjoint state and scratch (allocated by the first vjp)
     double *adj_lam_ = nullptr, *adj_ebar_ = nullptr, *adj_ebb_ = nullptr, *adj_dbar_ = nullptr;
     double *adj_cell_ = nullptr;  // per-cell / per-side / per-node cotangents, one block
     int *adj_int_ = nullptr;      // transposed stencil, boundary cells, periodic readers, opposite directions
     double *adj_wt_ = nullptr;    // transposed stencil weights and stencil weight sums
-    size_t adj_nT_ = 0, adj_nbcell_ = 0, adj_nper_ = 0;
+    size_t adj_nT_ = 0, adj_nbcell_ = 0, adj_nper_ = 0, adj_nsinv_ = 0;
+    std::vector<int> spec_h_;  // specular source per (wall side, direction), host copy
+    double *adj_warm_ = nullptr;  // reverse Picard solutions of the previous adjoint iteration
+    int adj_warm_n_ = 0;
     Error adj_setup();
 };
 

@@ -308,8 +308,9 @@ int gbte_get_geometry(gbte_handle *h, double *centers, double *volumes);
  * Any output may be NULL. It differentiates the fixed point the last
  * gbte_solve reached, implicitly: the adjoint state solves the transposed
  * equations by the transposed source iteration (sweeps in the opposite
- * directions, the transposed synthetic correction), until its relative
- * change is <= tol or max_iter iterations ran. Call it after a solve that
+ * directions, the transposed synthetic correction), until the gradient's
+ * relative change between iterations is <= tol (like the forward's margins)
+ * or max_iter iterations ran. Call it after a solve that
  * converged to tight margins; the gradient is that of the state the solve
  * left. FP64 handles only (GBTE_ERR_UNSUPPORTED otherwise), not batched
  * handles. It keeps one more band-state array (Nd*Nc*Nb doubles) and
@@ -317,7 +318,7 @@ int gbte_get_geometry(gbte_handle *h, double *centers, double *volumes);
 typedef struct {
     int iterations;     /* transposed source iterations */
     int picard_steps;   /* Picard steps of the synthetic correction, transposed */
-    double change;      /* last relative change of the adjoint state */
+    double change;      /* last relative change of the gradient */
     double vjp_ms;      /* device time of the adjoint solve and the assembly */
 } gbte_vjp_stats;
 
