@@ -162,13 +162,15 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     torch.cuda.set_device(local_rank)
     torch.cuda.init()
-    stream = torch.cuda.current_stream()
+    # a stream of its own (capturable: the library replays its transport
+    # stage as a CUDA graph on it)
+    stream = torch.cuda.Stream()
     deck, desc = build_deck(args.workload, seed=rank, h_nm=args.h_nm)
     nc = deck.mesh.n_cells
     prec = g.GBTE_FP32_MIXED if args.precision == "fp32" else g.GBTE_FP64
     s_bytes = 4 if prec == g.GBTE_FP32_MIXED else 8
 
-    solver = g.StaticBTESynthetic.from_deck(deck, precision=prec, device=local_rank, profile=1,
+    solver = g.StaticBTESynthetic.from_deck(deck, precision=prec, device=local_rank, profile=0,
                                             stream=ctypes_stream(stream), cell_order=args.cell_order)
     nb, nd = solver.num_bands, solver.num_directions
     upd_per_step = nb * nd * nc
@@ -195,9 +197,14 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         ms = float(t.item())
     value = upd_per_step * args.steps * world / (ms * 1e-3)
 
-    # roofline of the dominant kernel (per-launch CUDA events on the solver's
-    # stream), and of every streaming kernel
-    kern = st["kernels"]
+    # roofline of the dominant kernel, and of every streaming kernel: per-launch
+    # CUDA events on the solver's stream, from K more iterations launched
+    # kernel by kernel (after the timed region)
+    solver.set_profile(True)
+    kst = solver.solve(max_iter=args.steps, err_temp=0.0, err_flux=0.0)
+    solver.set_profile(False)
+    torch.cuda.synchronize()
+    kern = kst["kernels"]
     peak, peak_kind = measured_peak_gbs()
     total_ms = sum(v["ms"] for v in kern.values())
     dim = 2 if deck.mesh.nodes.shape[1] == 2 else 3

@@ -116,7 +116,7 @@ EXPORTS = ["gbte_inspect_deck", "gbte_inspect_mesh", "gbte_default_options", "gb
            "gbte_fourier_initial", "gbte_solve", "gbte_get_fields", "gbte_write_outputs", "gbte_get_sizes",
            "gbte_get_geometry", "gbte_last_error", "gbte_status_string", "gbte_destroy", "gbte_kernel_name",
            "gbte_solve_with", "gbte_fourier_initial_noalloc", "gbte_batch_create", "gbte_batch_geometries",
-           "gbte_vjp"]
+           "gbte_vjp", "gbte_set_profile"]
 
 _lib = None
 
@@ -153,6 +153,7 @@ def library():
                                           ctypes.POINTER(BCTable), ctypes.POINTER(AngleSpec),
                                           ctypes.POINTER(Options), ctypes.POINTER(ctypes.c_void_p)]
         lib.gbte_batch_geometries.argtypes = [ctypes.c_void_p, _c_int_p, _c_int_p]
+        lib.gbte_set_profile.argtypes = [ctypes.c_void_p, ctypes.c_int]
         lib.gbte_vjp.argtypes = [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, ctypes.c_int, ctypes.c_double, _c_dbl_p,
                                  _c_dbl_p, _c_dbl_p, ctypes.POINTER(VjpStats)]
         lib.gbte_inspect_deck.argtypes = [ctypes.c_char_p, ctypes.POINTER(DeckInfo)]
@@ -385,6 +386,10 @@ class StaticBTESynthetic:
                                        _ptr(g_spec, ctypes.c_double), ctypes.byref(st)))
         return {"tau": g_tau, "scatter": g_cell, "specularity": g_spec,
                 "stats": {k: getattr(st, k) for k, _ in st._fields_}}
+
+    def set_profile(self, on: bool) -> None:
+        """Per-launch kernel timing for the next solves (gbte_set_profile)."""
+        self._check(library().gbte_set_profile(self._h, int(bool(on))))
 
     def keff_cotangent(self, axis: int = 0, length: float = 1.0, delta_T: float = 1.0) -> np.ndarray:
         """q_bar of the effective conductivity k = <q_axis>_V length / delta_T

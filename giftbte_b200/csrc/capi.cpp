@@ -659,6 +659,12 @@ int gbte_vjp(gbte_handle *h, const double *T_bar, const double *q_bar, int max_i
     }
 }
 
+int gbte_set_profile(gbte_handle *h, int on) {
+    if (!h) return GBTE_ERR_ARG;
+    h->solver.cfg.profile = on ? 1 : 0;
+    return GBTE_OK;
+}
+
 const char *gbte_kernel_name(int i) { return gbte::kernel_name(i); }
 
 const char *gbte_last_error(const gbte_handle *h) {

@@ -2534,7 +2534,7 @@ Error Solver::solve_t(SolveStats &st) {
             cudaEvent_t t0, t1;
             CUDA_TRY(cudaEventCreate(&t0));
             CUDA_TRY(cudaEventCreate(&t1));
-            for (int cap : {32, 16, 10, 8, 5, 4, 2, 1}) {
+            for (int cap : {32, 16, 10, 8, 6, 5, 4, 3, 2, 1}) {
                 SweepLaunch L;
                 if (cap > nb || !sweep_launch(cap, L) || L.nbc == last_nbc) continue;
                 last_nbc = L.nbc;

@@ -325,6 +325,11 @@ typedef struct {
 int gbte_vjp(gbte_handle *h, const double *T_bar, const double *q_bar, int max_iter, double tol, double *grad_tau,
              double *grad_scatter, double *grad_specularity, gbte_vjp_stats *st);
 
+/* Turns per-launch kernel timing (options.profile) on or off for the next
+ * solves of a handle. While it is on, the transport stage is launched kernel
+ * by kernel instead of as the CUDA graph. No counterpart in the reference. */
+int gbte_set_profile(gbte_handle *h, int on);
+
 const char *gbte_last_error(const gbte_handle *h);
 const char *gbte_status_string(int status);
 int gbte_destroy(gbte_handle *h);
