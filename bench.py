@@ -171,7 +171,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     s_bytes = 4 if prec == g.GBTE_FP32_MIXED else 8
 
     solver = g.StaticBTESynthetic.from_deck(deck, precision=prec, device=local_rank, profile=0,
-                                            stream=ctypes_stream(stream), cell_order=args.cell_order)
+                                            stream=ctypes_stream(stream), cell_order=args.cell_order,
+                                            sweep_bands=args.sweep_bands)
     nb, nd = solver.num_bands, solver.num_directions
     upd_per_step = nb * nd * nc
     # warm-up (not timed)
@@ -252,6 +253,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             "config": {"workload": desc, "cells": nc, "bands": nb, "directions": nd,
                        "updates_per_step": upd_per_step, "precision": args.precision,
                        "cell_order": "morton" if args.cell_order == 0 else "deck",
+                       "sweep_bands": st.get("sweep_bands"),
                        "l2": f"band state {upd_per_step * s_bytes / 1e6:.0f} MB per copy, larger than the 126 MB L2",
                        "parallelism": f"replicas x{world} (independent seeded cells)" if world > 1 else "1 GPU"},
             "roofline": roofline, "hbm_kernels": hbm_kernels, "kernels": kernel_table, "cpu_baseline": cpu,
@@ -275,7 +277,8 @@ def e2e_solves(args, deck, prec, device, world):
 
     nc = deck.mesh.n_cells
     solver = g.StaticBTESynthetic.from_deck(deck, precision=prec, device=device, max_iter=args.max_iter_e2e,
-                                            err_temp=1e-8, err_flux=1e-8, cell_order=args.cell_order)
+                                            err_temp=1e-8, err_flux=1e-8, cell_order=args.cell_order,
+                                            sweep_bands=args.sweep_bands)
     nb = solver.num_bands
     T0 = torch.full((nc,), float(deck.tref), dtype=torch.float64).pin_memory().numpy()
     out = {k: np.zeros(n) for k, n in (("E", nc), ("T", nc), ("q", 3 * nc), ("Tb", nb * nc))}
@@ -525,6 +528,8 @@ def main():
     ap.add_argument("--adj-max-iter", type=int, default=20000, help="config4: adjoint iteration cap")
     ap.add_argument("--batch", type=int, default=256, help="config5: number of independent cells")
     ap.add_argument("--h-nm", type=float, default=0.0, help="config3 mesh spacing (default 2.5 nm)")
+    ap.add_argument("--sweep-bands", type=int, default=0,
+                    help="bands per sweep CTA (1..32); 0 lets the autotuner pick on the first iteration")
     ap.add_argument("--cell-order", type=int, choices=[0, 1], default=0,
                     help="0: cells renumbered along a Morton curve inside the library; 1: the deck's order")
     ap.add_argument("--e2e-steps", type=int, default=2)

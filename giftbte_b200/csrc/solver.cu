@@ -3059,8 +3059,8 @@ __global__ void k_adj_node(DMesh m, const double *__restrict__ ThVbar, const dou
 // band): -lam, the cell's own outgoing faces and its downwind neighbours'
 // incoming faces (transpose of k_residual), the cell moments' cotangents
 // (transpose of k_moments: T_lat, Th, Q and the objective's q) into ebar;
-// the face-value gradients' cotangents into gbar[d][c][DIM][b]; the incoming
-// wall entries' cotangents (residual + side moments) into ebb.
+// the face-value gradients' cotangents into gbar[d][c][DIM][b]. The
+// incoming wall entries' cotangents are k_adj_ebin's.
 template <int DIM>
 __global__ void __launch_bounds__(256) k_adj_transport(DMesh m, DPhys p, const double *__restrict__ lam,
                                                        const double *__restrict__ Tlbar, const double *__restrict__ Thbar,
@@ -3102,10 +3102,6 @@ __global__ void __launch_bounds__(256) k_adj_transport(DMesh m, DPhys p, const d
                 gx += f * (m.cf_fx[k] - m.cx[c]);
                 gy += f * (m.cf_fy[k] - m.cy[c]);
                 if (DIM == 3) gz += f * (m.cf_fz[k] - m.cz[c]);
-            } else if (m.cf_bound[k] >= 0) {
-                const int s = m.cf_bside[k];
-                ebb[((size_t)d * m.nbs + s) * nb + b] =
-                    -oc * A * vn + adj_side_entry(m, p, d, s, b, Thsbar, Qsbar, bTmbar);
             }
         }
         ebar[t] = e;
@@ -3120,13 +3116,11 @@ __global__ void __launch_bounds__(256) k_adj_transport(DMesh m, DPhys p, const d
 // BC): the cell's geometry and moment cotangents are loaded once for BC
 // bands and the band values move as 16-byte vectors; tvc = (1/s_c)/V_c
 template <int DIM, int BC>
-__global__ void __launch_bounds__(256) k_adj_transport4(DMesh m, DPhys p, const double *__restrict__ tvc,
+__global__ void __launch_bounds__(256, DIM == 2 ? 4 : 3) k_adj_transport_v(DMesh m, DPhys p, const double *__restrict__ tvc,
                                                         const double *__restrict__ lam, const double *__restrict__ Tlbar,
                                                         const double *__restrict__ Thbar, const double *__restrict__ Qbar,
-                                                        const double *__restrict__ qbar, const double *__restrict__ Thsbar,
-                                                        const double *__restrict__ Qsbar, const double *__restrict__ bTmbar,
-                                                        double *__restrict__ ebar, double *__restrict__ gbar,
-                                                        double *__restrict__ ebb) {
+                                                        const double *__restrict__ qbar, double *__restrict__ ebar,
+                                                        double *__restrict__ gbar) {
     const int nb = p.nb, nc = m.nc, nbc = nb / BC;
     const size_t total = (size_t)p.nd * nc * nbc;
     for (size_t t = gtid(); t < total; t += gstride()) {
@@ -3135,54 +3129,48 @@ __global__ void __launch_bounds__(256) k_adj_transport4(DMesh m, DPhys p, const 
         const int c = (int)(dc % nc);
         const int d = (int)(dc / nc);
         const double w = p.w[d], sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
-        double lc[BC], e[BC], oc[BC], gx[BC], gy[BC], gz[BC], tau[BC], vm[BC];
+        double lc[BC], e[BC], gx[BC], gy[BC], gz[BC];
         ld8(lam + dc * nb + b0, lc);
-        const double tl = Tlbar[c], th = Thbar[c], tv = tvc[c];
-        const double *q = Qbar + 6 * (size_t)c;
-        const double qss = q[0] * sx * sx + q[1] * sx * sy + q[2] * sx * sz + q[3] * sy * sy + q[4] * sy * sz + q[5] * sz * sz;
-        const double qs = qbar ? sx * qbar[3 * c] + sy * qbar[3 * c + 1] + sz * qbar[3 * c + 2] : 0.0;
+        {
+            const double tl = Tlbar[c], th = Thbar[c];
+            const double *q = Qbar + 6 * (size_t)c;
+            const double qss =
+                q[0] * sx * sx + q[1] * sx * sy + q[2] * sx * sz + q[3] * sy * sy + q[4] * sy * sz + q[5] * sz * sz;
+            const double qs = qbar ? sx * qbar[3 * c] + sy * qbar[3 * c + 1] + sz * qbar[3 * c + 2] : 0.0;
 #pragma unroll
-        for (int i = 0; i < BC; i++) {
-            const int b = b0 + i;
-            tau[i] = p.tau[b];
-            vm[i] = p.vmag[b];
-            const double lw = p.lat[b] * w / p.C[b];
-            e[i] = -lc[i] + lw * tl + vm[i] * w * qs;
-            if (p.hr[b] > 0) e[i] += p.kappa * lw * th + w * tau[i] * vm[i] * vm[i] * qss;
-            oc[i] = tau[i] * tv * lc[i];
-            gx[i] = gy[i] = gz[i] = 0;
+            for (int i = 0; i < BC; i++) {
+                const int b = b0 + i;
+                const double vm = p.vmag[b], lw = p.lat[b] * w / p.C[b];
+                e[i] = -lc[i] + lw * tl + vm * w * qs;
+                if (p.hr[b] > 0) e[i] += p.kappa * lw * th + w * p.tau[b] * vm * vm * qss;
+                gx[i] = gy[i] = gz[i] = 0;
+            }
         }
+        // own outgoing faces (-tau_c/V_c) and the downwind neighbours'
+        // incoming faces (+tau_j/V_j): f = A (s.n) |v| tau (tv_j lam_j - tv_c lam_c)
+        const double tv = tvc[c];
         for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
             const double sn = sx * m.cf_nx[k] + sy * m.cf_ny[k] + (DIM == 3 ? sz * m.cf_nz[k] : 0.0);
-            const double A = m.cf_area[k];
-            if (sn >= 0) {
-                const double rx = m.cf_fx[k] - m.cx[c], ry = m.cf_fy[k] - m.cy[c], rz = m.cf_fz[k] - m.cz[c];
-                double f[BC];
+            if (sn < 0) continue;
+            const double as = m.cf_area[k] * sn;
+            const double rx = m.cf_fx[k] - m.cx[c], ry = m.cf_fy[k] - m.cy[c], rz = m.cf_fz[k] - m.cz[c];
+            double lj[BC];
+            double tj = 0;
+            if (m.cf_bound[k] < 0) {
+                const int j = m.cf_nbr[k];
+                ld8(lam + ((size_t)d * nc + j) * nb + b0, lj);
+                tj = tvc[j];
+            } else {
 #pragma unroll
-                for (int i = 0; i < BC; i++) f[i] = -oc[i];
-                if (m.cf_bound[k] < 0) {
-                    const int j = m.cf_nbr[k];
-                    double lj[BC];
-                    ld8(lam + ((size_t)d * nc + j) * nb + b0, lj);
-                    const double tj = tvc[j];
+                for (int i = 0; i < BC; i++) lj[i] = 0;
+            }
 #pragma unroll
-                    for (int i = 0; i < BC; i++) f[i] += tau[i] * tj * lj[i];
-                }
-#pragma unroll
-                for (int i = 0; i < BC; i++) {
-                    const double fi = f[i] * A * vm[i] * sn;
-                    e[i] += fi;
-                    gx[i] += fi * rx;
-                    gy[i] += fi * ry;
-                    if (DIM == 3) gz[i] += fi * rz;
-                }
-            } else if (m.cf_bound[k] >= 0) {
-                const int s = m.cf_bside[k];
-                double o[BC];
-#pragma unroll
-                for (int i = 0; i < BC; i++)
-                    o[i] = -oc[i] * A * vm[i] * sn + adj_side_entry(m, p, d, s, b0 + i, Thsbar, Qsbar, bTmbar);
-                st8(ebb + ((size_t)d * m.nbs + s) * nb + b0, o);
+            for (int i = 0; i < BC; i++) {
+                const double fi = as * p.vmag[b0 + i] * p.tau[b0 + i] * (tj * lj[i] - tv * lc[i]);
+                e[i] += fi;
+                gx[i] += fi * rx;
+                gy[i] += fi * ry;
+                if (DIM == 3) gz[i] += fi * rz;
             }
         }
         st8(ebar + dc * nb + b0, e);
@@ -3190,6 +3178,29 @@ __global__ void __launch_bounds__(256) k_adj_transport4(DMesh m, DPhys p, const 
         st8(gp, gx);
         st8(gp + nb, gy);
         if (DIM == 3) st8(gp + 2 * nb, gz);
+    }
+}
+
+// incoming wall entries' cotangents: the residual's boundary inflow term
+// (transpose of k_residual's wall read) plus the side moments' and wall
+// temperatures' reads
+__global__ void k_adj_ebin(DMesh m, DPhys p, const double *__restrict__ tvc, const double *__restrict__ lam,
+                           const double *__restrict__ Thsbar, const double *__restrict__ Qsbar,
+                           const double *__restrict__ bTmbar, double *__restrict__ ebb) {
+    const int nb = p.nb;
+    const size_t total = (size_t)p.nd * m.nbs * nb;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b = (int)(t % nb);
+        const int s = (int)((t / nb) % m.nbs);
+        const int d = (int)(t / ((size_t)nb * m.nbs));
+        const int c = m.bs_cell[s];
+        if (c < 0) continue;
+        const int k = m.bs_cf[s];
+        const double sn = p.sx[d] * m.cf_nx[k] + p.sy[d] * m.cf_ny[k] + p.sz[d] * m.cf_nz[k];
+        if (!(sn < 0)) continue;
+        const double l = lam[((size_t)d * m.nc + c) * nb + b];
+        ebb[t] = -p.tau[b] * tvc[c] * l * m.cf_area[k] * p.vmag[b] * sn +
+                 adj_side_entry(m, p, d, s, b, Thsbar, Qsbar, bTmbar);
     }
 }
 
@@ -3717,13 +3728,14 @@ Error Solver::vjp(const double *Tbar_h, const double *qbar_h, int max_iter, doub
         CUDA_TRY(cudaMemsetAsync(Thsbar, 0, (size_t)nbs * 8 * 7, s));
         k_adj_remacro<<<gC, kThreads, 0, s>>>(dm_, rbar, Thbar, Qbar, Thsbar, Qsbar, ThVbar, QVbar);
         k_adj_node<<<gN, kThreads, 0, s>>>(dm_, ThVbar, QVbar, Thbar, Qbar, Thsbar, Qsbar);
-        if (nb % 4 == 0) {
+        if (nb % 2 == 0) {
+            // two bands per thread: four CTAs per SM in 2D, three in 3D
             if (dim == 2)
-                k_adj_transport4<2, 4><<<grid_for(ne / 4), kThreads, 0, s>>>(dm_, dp_, tvc, L, Tb, Thbar, Qbar, qu,
-                                                                             Thsbar, Qsbar, bTmbar, ebar, gbar, ebb);
+                k_adj_transport_v<2, 2><<<grid_for(ne / 2), kThreads, 0, s>>>(dm_, dp_, tvc, L, Tb, Thbar, Qbar, qu,
+                                                                              ebar, gbar);
             else
-                k_adj_transport4<3, 4><<<grid_for(ne / 4), kThreads, 0, s>>>(dm_, dp_, tvc, L, Tb, Thbar, Qbar, qu,
-                                                                             Thsbar, Qsbar, bTmbar, ebar, gbar, ebb);
+                k_adj_transport_v<3, 2><<<grid_for(ne / 2), kThreads, 0, s>>>(dm_, dp_, tvc, L, Tb, Thbar, Qbar, qu,
+                                                                              ebar, gbar);
         } else if (dim == 2) {
             k_adj_transport<2><<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, L, Tb, Thbar, Qbar, qu, Thsbar, Qsbar,
                                                                   bTmbar, ebar, gbar, ebb);
@@ -3731,6 +3743,7 @@ Error Solver::vjp(const double *Tbar_h, const double *qbar_h, int max_iter, doub
             k_adj_transport<3><<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, L, Tb, Thbar, Qbar, qu, Thsbar, Qsbar,
                                                                   bTmbar, ebar, gbar, ebb);
         }
+        k_adj_ebin<<<grid_for((size_t)nd * nbs * nb), kThreads, 0, s>>>(dm_, dp_, tvc, L, Thsbar, Qsbar, bTmbar, ebb);
         k_adj_dsum<<<grid_for((size_t)nbs * nb), kThreads, 0, s>>>(dm_, dp_, ebb, adj_dbar_);
         k_adj_ebout<<<grid_for((size_t)nd * nbs * nb), kThreads, 0, s>>>(dm_, dp_, dif_w_, sptr, sidx, adj_dbar_, pptr,
                                                                           pidx, Thsbar, Qsbar, bTmbar, ebb);

@@ -290,3 +290,22 @@ def test_3d_hotspot_temperature():
     ])
     for name, ga, fd in rows:
         assert abs(ga - fd) <= TOL * max(abs(fd), 1e-3 * max(abs(r[2]) for r in rows)), (name, ga, fd)
+
+
+def test_forward_state_survives_vjp():
+    # the adjoint reuses only the transport scratch: a solve continued after
+    # gbte_vjp matches one that was never interrupted, bit for bit
+    d = base_deck()
+    qb = None
+    out = []
+    for with_vjp in (True, False):
+        s = g.StaticBTESynthetic.from_deck(d, precision=g.GBTE_FP64, cell_scatter=scatter())
+        s.solve(max_iter=40, err_temp=0.0, err_flux=0.0)
+        if with_vjp:
+            qb = s.keff_cotangent(axis=0, length=L, delta_T=1.0)
+            s.vjp(q_bar=qb, max_iter=20)
+        s.solve(max_iter=15, err_temp=0.0, err_flux=0.0)
+        out.append(s.fields())
+        s.close()
+    for k in ("T", "E", "q", "Tband"):
+        assert np.array_equal(out[0][k], out[1][k]), k
