@@ -253,7 +253,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             "config": {"workload": desc, "cells": nc, "bands": nb, "directions": nd,
                        "updates_per_step": upd_per_step, "precision": args.precision,
                        "cell_order": "morton" if args.cell_order == 0 else "deck",
-                       "sweep_bands": st.get("sweep_bands"),
+                       "sweep_bands": st.get("sweep_bands"), "sweep_stage_levels": st.get("sweep_stage_levels"),
                        "l2": f"band state {upd_per_step * s_bytes / 1e6:.0f} MB per copy, larger than the 126 MB L2",
                        "parallelism": f"replicas x{world} (independent seeded cells)" if world > 1 else "1 GPU"},
             "roofline": roofline, "hbm_kernels": hbm_kernels, "kernels": kernel_table, "cpu_baseline": cpu,

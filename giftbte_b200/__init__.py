@@ -77,7 +77,8 @@ class Stats(ctypes.Structure):
                 ("num_cells", ctypes.c_int), ("max_levels", ctypes.c_int), ("lagged_faces", ctypes.c_int),
                 ("inner_iterations", ctypes.c_int), ("kernel_launches", ctypes.c_longlong),
                 ("kernel_ms", ctypes.c_double * 16), ("kernel_count", ctypes.c_longlong * 16),
-                ("sweep_bands", ctypes.c_int), ("direction_batch", ctypes.c_int)]
+                ("sweep_bands", ctypes.c_int), ("direction_batch", ctypes.c_int),
+                ("sweep_stage_levels", ctypes.c_int)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("kernel_ms", "kernel_count")}

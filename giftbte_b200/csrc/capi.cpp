@@ -477,6 +477,7 @@ int gbte_solve(gbte_handle *h, gbte_stats *st) {
             const int fixed = h->solver.cfg.sweep_bands;
             st->sweep_bands = (fixed >= 1 && fixed <= 32) ? fixed : h->solver.tuned_sweep_bands_;
             st->direction_batch = h->solver.ndb_;
+            st->sweep_stage_levels = h->solver.tuned_sweep_look_;
             for (int k = 0; k < GBTE_NUM_KERNELS && k < gbte::K_NUM; k++) {
                 st->kernel_ms[k] = s.kernel_ms[k];
                 st->kernel_count[k] = s.kernel_count[k];

@@ -2420,22 +2420,24 @@ Error Solver::solve_t(SolveStats &st) {
     const int gC = (nc + kThreads - 1) / kThreads, gN = (nslot + kThreads - 1) / kThreads;
     // blocks per geometry of the per-geometry reductions
     const int comp_blocks = std::max(1, std::min(148, (nc / ncomp_ + kThreads - 1) / kThreads));
-    constexpr int LOOK = 4, LCAP = 128;
+    constexpr int LCAP = 128;
     // sweep launch geometry for a cap on the bands per CTA: nb split into
     // equal chunks of at most `cap` bands; the ring holds at least one whole
     // level (distinct slots for the cells written in one level) and 512
-    // positions or more; more chunks when that does not fit in shared memory
+    // positions or more; more chunks when that does not fit in shared memory.
+    // look = levels staged in shared memory (2..4: 1..3 levels of prefetch)
     struct SweepLaunch {
-        int nbc = 0, chunks = 0, threads = 0, blocks = 0, rvec = 0;
+        int nbc = 0, chunks = 0, threads = 0, blocks = 0, rvec = 0, look = 4;
         size_t smem = 0;
     };
     const size_t wlp = ((size_t)(sched.max_levels + 1) * sizeof(int) + 15) & ~(size_t)15;
-    auto sweep_launch = [&](int wcap, SweepLaunch &L) -> bool {
+    auto sweep_launch = [&](int wcap, SweepLaunch &L, int look) -> bool {
+        L.look = look;
         for (int cap = wcap; cap >= 1; cap--) {
             L.nbc = (nb + (nb + cap - 1) / cap - 1) / ((nb + cap - 1) / cap);  // equal chunks of <= cap bands
             L.chunks = (nb + L.nbc - 1) / L.nbc;                               // every chunk non-empty
             const size_t slot = (size_t)LCAP * sizeof(SweepRec<S>) + (((size_t)LCAP * L.nbc * sizeof(S) + 15) & ~(size_t)15);
-            L.smem = LOOK * slot + (((size_t)ring_ * L.nbc * sizeof(S) + 15) & ~(size_t)15) +
+            L.smem = look * slot + (((size_t)ring_ * L.nbc * sizeof(S) + 15) & ~(size_t)15) +
                      (((size_t)far_slots_ * L.nbc * sizeof(S) + 15) & ~(size_t)15) + wlp;
             if (L.smem <= 220 * 1024 || L.nbc == 1) break;
         }
@@ -2448,12 +2450,21 @@ Error Solver::solve_t(SolveStats &st) {
     };
     // every sweep launch stays within 220 KB of dynamic shared memory: the
     // limit is raised once, outside any stream capture
-    CUDA_TRY(cudaFuncSetAttribute(k_sweep<S, LOOK, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_sweep<S, 4, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_sweep<S, 3, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+    CUDA_TRY(cudaFuncSetAttribute(k_sweep<S, 2, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
     auto launch_sweep = [&](const SweepLaunch &L, int d0, int nbt) -> cudaError_t {
         const int blocks = nbt * ncomp_ * L.chunks;
-        k_sweep<S, LOOK, LCAP><<<blocks, L.threads, L.smem, s>>>(nb, nc, ncomp_, d0, L.nbc, ring_, far_slots_, L.rvec,
-                                                                   lvl_ptr_, dir_lvl_off_, (const SweepRec<S> *)rec_,
-                                                                   lvl_cells_, kb_, R, (S *)corr_);
+        const auto *rc = (const SweepRec<S> *)rec_;
+        if (L.look == 2)
+            k_sweep<S, 2, LCAP><<<blocks, L.threads, L.smem, s>>>(nb, nc, ncomp_, d0, L.nbc, ring_, far_slots_, L.rvec,
+                                                                  lvl_ptr_, dir_lvl_off_, rc, lvl_cells_, kb_, R, (S *)corr_);
+        else if (L.look == 3)
+            k_sweep<S, 3, LCAP><<<blocks, L.threads, L.smem, s>>>(nb, nc, ncomp_, d0, L.nbc, ring_, far_slots_, L.rvec,
+                                                                  lvl_ptr_, dir_lvl_off_, rc, lvl_cells_, kb_, R, (S *)corr_);
+        else
+            k_sweep<S, 4, LCAP><<<blocks, L.threads, L.smem, s>>>(nb, nc, ncomp_, d0, L.nbc, ring_, far_slots_, L.rvec,
+                                                                  lvl_ptr_, dir_lvl_off_, rc, lvl_cells_, kb_, R, (S *)corr_);
         return cudaGetLastError();
     };
     // a fixed cap (options.sweep_bands), or the one the autotuner picked
@@ -2463,7 +2474,8 @@ Error Solver::solve_t(SolveStats &st) {
                : tuned_sweep_bands_ > 0                         ? tuned_sweep_bands_
                                                                 : (sizeof(S) == 4 ? 8 : 4);
     SweepLaunch SL;
-    if (!sweep_launch(wcap, SL)) return {-8, "sweep level too wide for the shared-memory correction ring"};
+    if (!sweep_launch(wcap, SL, tuned_sweep_look_))
+        return {-8, "sweep level too wide for the shared-memory correction ring"};
     const int cpb = std::max(1, 256 / nb);
     const int gM = (nc + cpb - 1) / cpb;
     const size_t msmem = ((size_t)nd * kWTab + (size_t)cpb * nb * kMomSlots) * sizeof(double);
@@ -2528,17 +2540,15 @@ Error Solver::solve_t(SolveStats &st) {
             // autotuner: every cap on the bands per CTA that gives a distinct
             // chunking, timed on this iteration's residual (the sweep only
             // reads R and rewrites every correction, so the trials leave no
-            // trace; the band chunking does not change any arithmetic)
+            // trace; neither the band chunking nor the staging depth changes
+            // any arithmetic)
             float best = 1e30f;
-            int best_cap = wcap, last_nbc = -1;
+            int best_cap = wcap, best_look = 4, last_nbc = -1;
             cudaEvent_t t0, t1;
             CUDA_TRY(cudaEventCreate(&t0));
             CUDA_TRY(cudaEventCreate(&t1));
-            for (int cap : {32, 16, 10, 8, 6, 5, 4, 3, 2, 1}) {
-                SweepLaunch L;
-                if (cap > nb || !sweep_launch(cap, L) || L.nbc == last_nbc) continue;
-                last_nbc = L.nbc;
-                float ms = 1e30f;
+            auto trial = [&](const SweepLaunch &L, float &ms) -> Error {
+                ms = 1e30f;
                 for (int rep = 0; rep < 2; rep++) {
                     CUDA_TRY(cudaEventRecord(t0, s));
                     CUDA_TRY(launch_sweep(L, d0, nbt));
@@ -2548,16 +2558,39 @@ Error Solver::solve_t(SolveStats &st) {
                     CUDA_TRY(cudaEventElapsedTime(&m, t0, t1));
                     ms = std::min(ms, m);
                 }
+                return {0, ""};
+            };
+            // the band cap at four staged levels, then fewer staged levels
+            // (less shared memory, more resident CTAs) for the best cap
+            for (int cap : {32, 16, 10, 8, 6, 5, 4, 3, 2, 1}) {
+                SweepLaunch L;
+                if (cap > nb || !sweep_launch(cap, L, 4) || L.nbc == last_nbc) continue;
+                last_nbc = L.nbc;
+                float ms = 0;
+                Error te = trial(L, ms);
+                if (te.code) return te;
                 if (ms < best) {
                     best = ms;
                     best_cap = cap;
                 }
             }
+            for (int look : {3, 2}) {
+                SweepLaunch L;
+                if (!sweep_launch(best_cap, L, look)) continue;
+                float ms = 0;
+                Error te = trial(L, ms);
+                if (te.code) return te;
+                if (ms < best) {
+                    best = ms;
+                    best_look = look;
+                }
+            }
             cudaEventDestroy(t0);
             cudaEventDestroy(t1);
             tuned_sweep_bands_ = best_cap;
+            tuned_sweep_look_ = best_look;
             wcap = best_cap;
-            sweep_launch(wcap, SL);
+            sweep_launch(wcap, SL, best_look);
         }
         GL(K_SWEEP, CUDA_TRY(launch_sweep(SL, d0, nbt)));
         GL(K_MOMENTS, (k_moments<S><<<gM, cpb * nb, msmem, s>>>(dm_, dp_, cpb, eps, (const S *)corr_, Tbase_, wtab_,

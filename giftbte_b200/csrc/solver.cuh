@@ -117,6 +117,7 @@ public:
     bool initialised = false;
     std::string last_error;
     int tuned_sweep_bands_ = 0;  // bands-per-CTA cap the sweep autotuner picked (0 = not yet)
+    int tuned_sweep_look_ = 4;   // levels the sweep stages in shared memory (the autotuner's pick)
     int ndb_ = 1;                // directions per batch of the gradient/residual/correction buffers
 
 private:

@@ -168,6 +168,7 @@ typedef struct {
     int sweep_bands;          /* bands-per-CTA cap of the sweep in use (options.sweep_bands, or
                                  the autotuner's pick on the handle's first outer iteration) */
     int direction_batch;      /* directions per batch of the transport stage */
+    int sweep_stage_levels;   /* levels the sweep stages ahead in shared memory (autotuned, 2..4) */
 } gbte_stats;
 
 /* Name of kernel slot i of gbte_stats.kernel_ms (NULL past the last one). */
