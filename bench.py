@@ -140,10 +140,10 @@ def kernel_algorithmic_bytes(name: str, s: int, dim: int, nb: int, nd: int, nc: 
 
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
-# one ncu capture of each kernel on the 17,939-cell 40-band cell, FP32 form;
-# see profiles/transport_kernels_config2_fp32.md for the command.
-NCU_TRAFFIC_CONFIG2_FP32 = {"residual": 757.636864e6, "sweep": 391.150336e6, "gradient": 518.09664e6,
-                            "moments": 516.764928e6, "pcg": 1.895424e6}
+# one ncu --set full capture of each kernel of the third outer iteration on
+# the 17,939-cell 40-band cell, FP32 form, 8 bands per sweep CTA.
+NCU_TRAFFIC_CONFIG2_FP32 = {"residual": 746.86208e6, "sweep": 393.522944e6, "gradient": 509.391616e6,
+                            "moments": 517.57696e6, "pcg": 1.89568e6}
 
 
 def macro_nnz(deck) -> int:
