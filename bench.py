@@ -154,6 +154,25 @@ def macro_nnz(deck) -> int:
     return m.n_cells + sum(len(c) for c in m.cells) - len(m.edges)
 
 
+def ranks_reduce(value: float, op: str, world: int, device) -> float:
+    """A per-rank scalar reduced over the ranks ("max" or "sum"); the value
+    itself on one rank."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def whole_job_rate(units_local: float, seconds_local: float, world: int, device) -> float:
+    """Units that all ranks processed over the slowest rank's time."""
+    units = ranks_reduce(units_local, "sum", world, device)
+    return units / ranks_reduce(seconds_local, "max", world, device)
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
     import torch
     import torch.distributed as dist
@@ -191,12 +210,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     ev1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = upd_per_step * args.steps * world / (ms * 1e-3)
+    ms_local = ev0.elapsed_time(ev1)
+    ms = ranks_reduce(ms_local, "max", world, "cuda")
+    value = whole_job_rate(upd_per_step * args.steps, ms_local * 1e-3, world, "cuda")
 
     # roofline of the dominant kernel, and of every streaming kernel: per-launch
     # CUDA events on the solver's stream, from K more iterations launched
@@ -296,7 +312,7 @@ def e2e_solves(args, deck, prec, device, world):
         ups.append(st["updates"])
     solver.close()
     t = max(times)
-    e2e = {"value": sum(ups) / sum(times) * world, "unit": "updates/s",
+    e2e = {"value": whole_job_rate(sum(ups), sum(times), world, "cuda"), "unit": "updates/s",
            "h2d_bytes_per_step": int(nc * 8), "d2h_bytes_per_step": int(nc * 8 * (2 + 3 + nb)),
            "steps": nsteps, "step": "set_initial from pinned host + solve to residual 1e-8 + read all fields"}
     ttr = {"seconds": float(np.median(times)), "iterations": int(np.median(iters)), "residual": 1e-8,

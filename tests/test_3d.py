@@ -5,6 +5,7 @@ to the CPU oracle restatement (FP64, dimension-generic formulas), not to
 reference outputs. Host-only tests check the deck tooling; the GPU tests
 compare the CUDA path with the oracle.
 """
+import dataclasses
 import functools
 
 import numpy as np
@@ -144,3 +145,19 @@ def test_direction_batches_match_oracle_3d(prec):
     assert st["direction_batch"] == 5
     tol = TOL_FP64 if prec == g.GBTE_FP64 else TOL_FP32
     assert rel(f["T"], o["T"]) <= tol, rel(f["T"], o["T"])
+
+
+@pytest.mark.gpu
+def test_extensions_match_oracle_3d():
+    # partially specular side walls (p = 0.4) and per-cell scattering
+    # multipliers on tetrahedra: the CUDA forward against the oracle
+    d = dataclasses.replace(small_block(), bcs=[decks.BC(1, 1, 300.0), decks.BC(2, 2, 0.0)] +
+                            [decks.BC(t, 6, 0.4) for t in (3, 4, 5, 6)])
+    sc = decks.lognormal_scatter(d.mesh.n_cells, sigma=0.2, seed=7)
+    o = oracle.solve(d, cell_scatter=sc)
+    s = g.StaticBTESynthetic.from_deck(d, precision=g.GBTE_FP64, cell_scatter=sc)
+    s.solve(allow_not_converged=False)
+    f = s.fields()
+    s.close()
+    assert rel(f["T"], o["T"]) <= TOL_FP64, rel(f["T"], o["T"])
+    assert rel(f["q"], o["q"]) <= 1e-8
