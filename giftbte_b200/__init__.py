@@ -66,7 +66,8 @@ class Options(ctypes.Structure):
                 ("stream", ctypes.c_void_p), ("device", ctypes.c_int), ("verbose", ctypes.c_int),
                 ("macro_rtol", ctypes.c_double), ("profile", ctypes.c_int), ("sweep_bands", ctypes.c_int),
                 ("sweep_far_slots", ctypes.c_int), ("direction_batch", ctypes.c_int),
-                ("cell_scatter", _c_dbl_p), ("cell_order", ctypes.c_int)]
+                ("cell_scatter", _c_dbl_p), ("cell_order", ctypes.c_int), ("order", ctypes.c_int),
+                ("scheme", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -223,7 +224,8 @@ class StaticBTESynthetic:
         if cell_heat is None:
             cell_heat = deck.cell_heat()
         heat = np.ascontiguousarray(cell_heat, dtype=np.float64) if cell_heat is not None else None
-        kw = {"max_iter": deck.max_iter, "err_temp": deck.residual_temp, "err_flux": deck.residual_flux}
+        kw = {"max_iter": deck.max_iter, "err_temp": deck.residual_temp, "err_flux": deck.residual_flux,
+              "order": 1 if deck.order == "1" else 2, "scheme": 1 if deck.scheme == "Sequential" else 0}
         kw.update(opt)
         o = default_options(precision, device=device, verbose=verbose, **kw)
         o.cell_heat = _ptr(heat, ctypes.c_double)
@@ -266,7 +268,8 @@ class StaticBTESynthetic:
             heat = np.ascontiguousarray(np.concatenate([h if h is not None else np.zeros(d.mesh.n_cells)
                                                         for h, d in zip(heats, decks)]), dtype=np.float64)
         d0 = decks[0]
-        kw = {"max_iter": d0.max_iter, "err_temp": d0.residual_temp, "err_flux": d0.residual_flux}
+        kw = {"max_iter": d0.max_iter, "err_temp": d0.residual_temp, "err_flux": d0.residual_flux,
+              "order": 1 if d0.order == "1" else 2, "scheme": 1 if d0.scheme == "Sequential" else 0}
         kw.update(opt)
         o = default_options(precision, device=device, verbose=verbose, **kw)
         o.cell_heat = _ptr(heat, ctypes.c_double)

@@ -148,6 +148,12 @@ int create_common(const gbte::RawMesh &raw_in, const gbte::Bands &bands_in, cons
     cfg.sweep_far_slots = opt.sweep_far_slots;
     cfg.direction_batch = opt.direction_batch;
     cfg.cell_scatter = scatter;
+    if (opt.order != 0 && opt.order != 1 && opt.order != 2)
+        return fail(nullptr, {-1, "order must be 1 or 2 (0 = 2)"}), GBTE_ERR_ARG;
+    if (opt.scheme != 0 && opt.scheme != 1)
+        return fail(nullptr, {-1, "scheme must be 0 (Synthetic) or 1 (Sequential)"}), GBTE_ERR_ARG;
+    cfg.order = opt.order == 1 ? 1 : 2;
+    cfg.sequential = opt.scheme == 1;
     cfg.device = opt.device;
     cfg.stream = (cudaStream_t)opt.stream;
     if (opt.precision != GBTE_FP64 && opt.precision != GBTE_FP32_MIXED)
@@ -389,10 +395,16 @@ int gbte_create_from_deck(const char *dir, const gbte_options *opt_in, gbte_hand
         if (e.code) return fail(nullptr, e), status_of(e.code);
         if (deck.order == "2limit")
             opt.use_limiter = 1;
-        else if (deck.order != "2")
-            return fail(nullptr, {-8, "only Order=2 / 2limit (second-order synthetic) is implemented"}), GBTE_ERR_UNSUPPORTED;
-        if (deck.method != "Synthetic")
-            return fail(nullptr, {-8, "only IterativeScheme=Synthetic is implemented"}), GBTE_ERR_UNSUPPORTED;
+        else if (deck.order == "1")
+            opt.order = 1;
+        else if (deck.order == "2")
+            opt.order = 2;
+        else
+            return fail(nullptr, {-8, "Order must be 1, 2 or 2limit"}), GBTE_ERR_UNSUPPORTED;
+        if (deck.method == "Sequential")
+            opt.scheme = 1;
+        else if (deck.method != "Synthetic")
+            return fail(nullptr, {-8, "IterativeScheme must be Synthetic or Sequential"}), GBTE_ERR_UNSUPPORTED;
         opt.max_iter = deck.max_iter;
         opt.err_temp = deck.err_temp;
         opt.err_flux = deck.err_flux;

@@ -2025,9 +2025,10 @@ Error Solver::set_initial(const double *T0, const double *q0, const double *bth)
     // base of the stored deviation: T0 in the FP32 form, 0 in the FP64 form
     if (cfg.precision == 1) {
         CUDA_TRY(cudaMemcpyAsync(Tbase_, T0, nc * 8, cudaMemcpyHostToDevice, s));
-        // gradient of the base with the same stencil (host, FP64)
+        // gradient of the base with the same stencil (host, FP64); zero in
+        // the first-order form
         std::vector<double> g(nc * 3, 0.0);
-        for (size_t c = 0; c < nc; c++)
+        for (size_t c = 0; c < (cfg.order == 2 ? nc : 0); c++)
             for (int q = mesh.nbr_ptr[c]; q < mesh.nbr_ptr[c + 1]; q++) {
                 double de = T0[mesh.nbr_idx[q]] - T0[c];
                 for (int r = 0; r < 3; r++) g[3 * c + r] += mesh.lsq_w[3 * (size_t)q + r] * de;
@@ -2489,14 +2490,18 @@ Error Solver::solve_t(SolveStats &st) {
         GL(K_GATHER, k_diffuse_sum<<<grid_for((size_t)nbs * nb), kThreads, 0, s>>>(dm_, dp_, dif_w_, eb_, dsum_));
         GL(K_GATHER, k_gather<<<gB, kThreads, 0, s>>>(dm_, dp_, dsum_, spec_src_, need_snapshot_ ? eb_snap_ : nullptr, eb_));
     };
+    // first order (solve_firstorder, StaticBTESyntheticSolver.cpp:487-726):
+    // upwind cell values on the faces, i.e. zero gradients throughout
+    if (cfg.order == 1) CUDA_TRY(cudaMemsetAsync(grad_, 0, (size_t)ndb * nc * nb * DIM * sizeof(S), s));
     if (!started_) {
         // _set_initial (:765-782) and the initial boundary values (StaticBTESyntheticSolver.cpp:45-62)
         GL(K_INIT, k_init_eps<S><<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, T_, Tbase_, eps));
         for (int d0 = 0; d0 < nd; d0 += ndb) {
             const int nbt = std::min(ndb, nd - d0);
             ev.gd0 = d0;
-            GL(K_GRADIENT, (k_gradient<S, DIM><<<grid_for((size_t)nbt * nc * nb), kThreads, 0, s>>>(dm_, dp_, w, eps, g,
-                                                                                                 d0, nbt)));
+            if (cfg.order == 2)
+                GL(K_GRADIENT, (k_gradient<S, DIM><<<grid_for((size_t)nbt * nc * nb), kThreads, 0, s>>>(dm_, dp_, w, eps,
+                                                                                                     g, d0, nbt)));
             GL(K_BOUND_OUT, (k_bound_out<S, DIM><<<grid_for((size_t)nbt * nbs * nb), kThreads, 0, s>>>(dm_, dp_, ev,
                                                                                                    eb_, d0, nbt)));
         }
@@ -2528,11 +2533,14 @@ Error Solver::solve_t(SolveStats &st) {
         const size_t nbe = (size_t)nbt * nc * nb;
         ev.gd0 = d0;
         if (nb % 4 == 0) {
-            GL(K_GRADIENT, (k_gradient8<S, DIM, 4><<<grid_for(nbe / 4), kThreads, 0, s>>>(dm_, dp_, w, eps, g, d0, nbt)));
+            if (cfg.order == 2)
+                GL(K_GRADIENT, (k_gradient8<S, DIM, 4><<<grid_for(nbe / 4), kThreads, 0, s>>>(dm_, dp_, w, eps, g, d0,
+                                                                                              nbt)));
             GL(K_RESIDUAL, (k_residual8<S, DIM, 4><<<grid_for(nbe / 4), kThreads, 0, s>>>(dm_, dp_, ev, Bflux_, Told_, eb_,
                                                                                           pos_of_, R, d0, nbt)));
         } else {
-            GL(K_GRADIENT, (k_gradient<S, DIM><<<grid_for(nbe), kThreads, 0, s>>>(dm_, dp_, w, eps, g, d0, nbt)));
+            if (cfg.order == 2)
+                GL(K_GRADIENT, (k_gradient<S, DIM><<<grid_for(nbe), kThreads, 0, s>>>(dm_, dp_, w, eps, g, d0, nbt)));
             GL(K_RESIDUAL, (k_residual<S, DIM><<<grid_for(nbe), kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, pos_of_, R,
                                                                                   d0, nbt)));
         }
@@ -2599,11 +2607,15 @@ Error Solver::solve_t(SolveStats &st) {
         GL(K_BOUND_OUT, (k_bound_out<S, DIM><<<grid_for((size_t)nbt * nbs * nb), kThreads, 0, s>>>(dm_, dp_, ev, eb_, d0,
                                                                                                nbt)));
         }
-        GL(K_SIDE_MOMENTS, k_side_moments<<<gW, kThreads, 0, s>>>(dm_, dp_, eb_, Ths_, Qs_));
-        GL(K_NODE_INTERP, k_node_interp<<<gN, kThreads, 0, s>>>(dm_, Th_, Q_, Ths_, Qs_, ThV_, QV_));
-        GL(K_REMACRO, k_remacro<<<gC, kThreads, 0, s>>>(dm_, Th_, Q_, Ths_, Qs_, ThV_, QV_, remacro_));
+        // the synthetic source and wall temperatures (not in the Sequential
+        // scheme, solve_DOM, StaticBTESyntheticSolver.cpp:968-1179)
+        if (!cfg.sequential) {
+            GL(K_SIDE_MOMENTS, k_side_moments<<<gW, kThreads, 0, s>>>(dm_, dp_, eb_, Ths_, Qs_));
+            GL(K_NODE_INTERP, k_node_interp<<<gN, kThreads, 0, s>>>(dm_, Th_, Q_, Ths_, Qs_, ThV_, QV_));
+            GL(K_REMACRO, k_remacro<<<gC, kThreads, 0, s>>>(dm_, Th_, Q_, Ths_, Qs_, ThV_, QV_, remacro_));
+        }
         gather();
-        GL(K_MACRO_BC, k_macro_bc<<<gW, kThreads, 0, s>>>(dm_, dp_, eb_, bTovr_, bTm_));
+        if (!cfg.sequential) GL(K_MACRO_BC, k_macro_bc<<<gW, kThreads, 0, s>>>(dm_, dp_, eb_, bTovr_, bTm_));
         CUDA_TRY(cudaGetLastError());
         return {0, ""};
         };
@@ -2637,9 +2649,10 @@ Error Solver::solve_t(SolveStats &st) {
             if (te.code) return te;
         }
         CUDA_TRY(cudaEventRecord(ev_[1], s));
-        // _marco_solution: Picard on the non-orthogonal correction
+        // _marco_solution: Picard on the non-orthogonal correction; the
+        // Sequential scheme keeps the moment temperature
         GL(K_COPY, k_copy<<<gC, kThreads, 0, s>>>(Tlat_, T_, nc));
-        double internal = 1000, prev_internal = 0;
+        double internal = cfg.sequential ? 0.0 : 1000, prev_internal = 0;
         int inner = 0, inner_inc = 0;
         // per geometry of a batch: Picard done (its own test met in an earlier step)
         std::vector<char> done(ncomp_, 0);
@@ -2737,7 +2750,10 @@ Error Solver::solve_t(SolveStats &st) {
                 GL(K_INIT, k_copy<<<gC, kThreads, 0, s>>>(Tbase_, T1_, nc));
                 GL(K_INIT, k_copy<<<gC, kThreads, 0, s>>>(T_, Tbase_, nc));
                 GL(K_INIT, k_rebase<S><<<gE, kThreads, 0, s>>>(dm_, dp_, T1_, Tbase_, eps));
-                GL(K_INIT, k_cell_lsq_grad<<<gC, kThreads, 0, s>>>(dm_, Tbase_, gTb_));
+                if (cfg.order == 2)
+                    GL(K_INIT, k_cell_lsq_grad<<<gC, kThreads, 0, s>>>(dm_, Tbase_, gTb_));
+                else
+                    CUDA_TRY(cudaMemsetAsync(gTb_, 0, (size_t)nc * 3 * 8, s));
                 GL(K_INIT, (k_base_flux<DIM><<<grid_for((size_t)nd * nc), kThreads, 0, s>>>(dm_, dp_, Tbase_, gTb_,
                                                                                             Bflux_)));
             }
@@ -2859,7 +2875,10 @@ Error Solver::fourier_initial_noalloc() {
     // deviation from this temperature
     if (cfg.precision == 1) {
         CUDA_TRY(cudaMemcpyAsync(Tbase_, T_, (size_t)nc * sizeof(double), cudaMemcpyDeviceToDevice, s));
-        GL(K_INIT, k_cell_lsq_grad<<<gC, kThreads, 0, s>>>(dm_, Tbase_, gTb_));
+        if (cfg.order == 2)
+            GL(K_INIT, k_cell_lsq_grad<<<gC, kThreads, 0, s>>>(dm_, Tbase_, gTb_));
+        else
+            CUDA_TRY(cudaMemsetAsync(gTb_, 0, (size_t)nc * 3 * 8, s));
     } else {
         CUDA_TRY(cudaMemsetAsync(Tbase_, 0, (size_t)nc * sizeof(double), s));
         CUDA_TRY(cudaMemsetAsync(gTb_, 0, (size_t)nc * 3 * sizeof(double), s));
@@ -3669,6 +3688,8 @@ Error Solver::vjp(const double *Tbar_h, const double *qbar_h, int max_iter, doub
     if (ncomp_ > 1) return {-8, "the adjoint is not implemented for batched handles"};
     if (!started_ || last_inner_ < 1) return {-1, "call gbte_solve (to convergence) before gbte_vjp"};
     if (need_snapshot_) return {-8, "the adjoint does not support chained specular reflections"};
+    if (cfg.order != 2 || cfg.sequential)
+        return {-8, "the adjoint is implemented for the second-order Synthetic scheme only"};
     if (ndb_ < ang.nd) return {-8, "the adjoint needs every direction's buffers resident (direction_batch)"};
     if (max_iter < 1 || !(tol > 0)) return {-1, "invalid adjoint limits"};
     CUDA_TRY(cudaSetDevice(cfg.device));

@@ -52,6 +52,8 @@ struct SolverConfig {
     int sweep_far_slots = 0;  // far-slot cap of the sweep plan: 0 = automatic, < 0 = none
     int direction_batch = 0;  // most directions per transport batch, 0 = automatic
     std::vector<double> cell_scatter;  // scattering-rate multiplier s_c per cell (empty: 1)
+    int order = 2;            // 2: second-order upwind faces (solve); 1: first order (solve_firstorder)
+    bool sequential = false;  // Sequential scheme (solve_DOM): no macro correction, T = T_lat
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;

@@ -504,7 +504,8 @@ class Deck:
     residual_temp: float = 1e-8
     residual_flux: float = 1e-8
     max_iter: int = 10000
-    order: str = "2"
+    order: str = "2"                      # CONTROL Order: "1" or "2"
+    scheme: str = "Synthetic"             # CONTROL IterativeScheme: "Synthetic" or "Sequential"
     heat_source: Optional[float] = None   # uniform volumetric heat (W/m^3)
     mesh_format: str = "COMSOL"           # COMSOL or MSH (3D meshes: MSH)
     region_heat: Optional[List[float]] = None  # heat per region (W/m^3), HeatType REGION
@@ -545,9 +546,9 @@ class Deck:
             for b in self.bcs:
                 f.write(f"{b.tag} {b.type} {b.value:.17g}\n")
         with open(os.path.join(d, "CONTROL"), "w") as f:
-            f.write("State=\nSteady\nOrder=\n%s\nIterativeScheme=\nSynthetic\nMatrixSolver=\nLU\n"
+            f.write("State=\nSteady\nOrder=\n%s\nIterativeScheme=\n%s\nMatrixSolver=\nLU\n"
                     "Tref=\n%.17g\nMaxNumIter=\n%d\nResidualTemp=\n%.17g\nResidualFlux=\n%.17g\n"
-                    % (self.order, self.tref, self.max_iter, self.residual_temp, self.residual_flux))
+                    % (self.order, self.scheme, self.tref, self.max_iter, self.residual_temp, self.residual_flux))
         with open(os.path.join(d, "GEOMETRY"), "w") as f:
             f.write("GeometryDimension=\n%d\nScaleX=\n%.17g\nScaleY=\n%.17g\n"
                     % (self.dimension, self.scale[0], self.scale[1]))

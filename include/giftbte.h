@@ -142,6 +142,12 @@ typedef struct {
                                  curve of their centres (per geometry of a batch) for memory locality;
                                  1 = keep the caller's order. Every cell array of this ABI is in the
                                  caller's order either way; results agree to rounding. */
+    int order;                /* spatial order of the transport: 0 or 2 = second order (CONTROL Order=2,
+                                 StaticBTESynthetic::solve), 1 = first order (Order=1, solve_firstorder:
+                                 upwind cell values, no gradient reconstruction) */
+    int scheme;               /* 0 = Synthetic (IterativeScheme=Synthetic: the macro correction), 1 =
+                                 Sequential (IterativeScheme=Sequential, solve_DOM /
+                                 solve_DOM_firstorder: plain source iteration, T from the moments) */
 } gbte_options;
 
 #define GBTE_NUM_KERNELS 16

@@ -107,7 +107,8 @@ def solve(deck, T0: Optional[np.ndarray] = None, max_iter: Optional[int] = None,
         ctypes.c_double(err_q if err_q is not None else deck.residual_flux), 0,
         _p(out_T, ctypes.c_double), _p(out_E, ctypes.c_double), _p(out_q, ctypes.c_double),
         _p(out_Tb, ctypes.c_double), ctypes.byref(iters), _p(err, ctypes.c_double),
-        _p(cell_scatter, ctypes.c_double))
+        _p(cell_scatter, ctypes.c_double), 1 if getattr(deck, "order", "2") == "1" else 2,
+        1 if getattr(deck, "scheme", "Synthetic") == "Sequential" else 0)
     if rc != 0:
         raise RuntimeError(f"oracle_solve failed with code {rc}")
     return {"T": out_T, "E": out_E, "q": out_q.reshape(nc, 3), "Tband": out_Tb.reshape(nb, nc),

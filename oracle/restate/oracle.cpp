@@ -359,6 +359,8 @@ struct Oracle {
     std::vector<double> ebound;                 // [b][d][ib][2]
     std::vector<double> T, Told, Tlat, Tband, E, qx, qy, qz, qxo, qyo, qzo, ReMacro, heat;
     std::vector<double> tsc;                    // 1 / s_c: per-cell relaxation-time scale (extension, 1 = reference)
+    int order = 2;                              // 1: solve_firstorder (zero face gradients)
+    bool sequential = false;                    // IterativeScheme=Sequential: no macro correction
     std::vector<std::array<double, 2>> bTmacro;
     double errOld = 0, errOldq = 0, err = 0, errq = 0;
     int errInc = 0;
@@ -610,6 +612,7 @@ void setup_lsq(Oracle &o) {
 void gradient(const Oracle &o, const std::vector<double> &e, int b, int d, std::vector<V3> &g, std::vector<double> &lim) {
     g.assign(o.nc, V3());
     lim.assign(o.nc, 1.0);
+    if (o.order == 1) return;  // solve_firstorder: gradients stay zero (StaticBTESyntheticSolver.cpp:530-535)
     for (int i = 0; i < o.nc; i++) {
         int k = (int)o.nbr[i].size();
         if (k < 3) continue;
@@ -1128,7 +1131,7 @@ int oracle_solve(int dim, int nn, const double *xyz, int nc, const int *cptr, co
                  int angle_method, int ntheta, int nphi, double Lx, const double *cell_heat, const double *T0,
                  const double *q0, int max_iter, double errT, double errq, int use_limiter, double *out_Tlat,
                  double *out_E, double *out_q, double *out_Tband, int *out_iters, double *out_err,
-                 const double *cell_scatter) {
+                 const double *cell_scatter, int order, int sequential) {
     Oracle o;
     o.nmat = nmat;
     o.nb = nband;
@@ -1138,6 +1141,8 @@ int oracle_solve(int dim, int nn, const double *xyz, int nc, const int *cptr, co
                         reg_mat, nreg);
     if (rc) return rc;
     for (int i = 0; i < nc; i++) o.cell[i].heat = cell_heat ? cell_heat[i] : 0.0;
+    o.order = order == 1 ? 1 : 2;
+    o.sequential = sequential != 0;
     o.tsc.assign(nc, 1.0);
     if (cell_scatter)
         for (int i = 0; i < nc; i++) o.tsc[i] = 1.0 / cell_scatter[i];
@@ -1246,8 +1251,10 @@ int oracle_solve(int dim, int nn, const double *xyz, int nc, const int *cptr, co
         o.Tband = Tb;
         o.ReMacro = RM;
         set_bound_ee_1(o);
-        macro_bc(o);
-        macro_solution(o);
+        if (!o.sequential) {  // solve_DOM (StaticBTESyntheticSolver.cpp:968-1179) keeps T_lat
+            macro_bc(o);
+            macro_solution(o);
+        }
         iters = nt + 1;
         bool stop = margins(o, errT, errq);
         if (stop || o.errInc >= 10) break;

@@ -60,6 +60,25 @@ def cases():
         bcs=[decks.BC(1, -2, 1.0), decks.BC(2, -1, 0.0), decks.BC(3, -4, 0.0), decks.BC(4, -3, 0.0),
              decks.BC(5, 2, 0.0)],
         scale=(3e-7, 3e-7), material_dim=2, angle_method=2, n_phi=4, tref=0.0, mesh_format="MSH")
+    # 5.-7. the solver variants: first order (Order=1, solve_firstorder),
+    #    Sequential without the synthetic correction (solve_DOM), and both
+    #    (solve_DOM_firstorder)
+    m = decks.porous_cell_mesh(0.1, [(0.5, 0.5, 0.25)], seed=4)
+    out["porous_firstorder"] = decks.Deck(
+        mesh=m, bands=decks.sine_dispersion_bands(4),
+        bcs=[decks.BC(1, -2, 1.0), decks.BC(2, -1, 0.0), decks.BC(3, -4, 0.0), decks.BC(4, -3, 0.0),
+             decks.BC(5, 2, 0.0)],
+        scale=(3e-7, 3e-7), material_dim=2, angle_method=2, n_phi=4, tref=0.0, order="1")
+    m = decks.jitter_interior(decks.square_tri_mesh(16, 16), 0.2 / 16, seed=3)
+    out["periodic_sequential"] = decks.Deck(
+        mesh=m, bands=decks.sine_dispersion_bands(3),
+        bcs=[decks.BC(1, -2, 1.0), decks.BC(2, -1, 0.0), decks.BC(3, 3, 0.0), decks.BC(4, 3, 0.0)],
+        scale=(1e-7, 1e-7), material_dim=2, angle_method=1, n_phi=4, tref=0.0, scheme="Sequential")
+    out["quad_firstorder_sequential"] = decks.Deck(
+        mesh=decks.square_quad_mesh(16, 16), bands=decks.sine_dispersion_bands(2),
+        bcs=[decks.BC(1, 1, 300.0), decks.BC(2, 1, 300.0), decks.BC(3, 3, 0.0), decks.BC(4, 3, 0.0)],
+        scale=(1e-7, 1e-7), material_dim=3, angle_method=2, n_theta=2, n_phi=2, tref=300.0,
+        heat_source=1e16, order="1", scheme="Sequential")
     for d in out.values():
         d.residual_temp = 1e-12
         d.residual_flux = 1e-12
@@ -70,7 +89,7 @@ def cases():
 def deck_params(d: decks.Deck) -> dict:
     return {"scale": list(d.scale), "material_dim": d.material_dim, "angle_method": d.angle_method,
             "n_theta": d.n_theta, "n_phi": d.n_phi, "tref": d.tref, "heat_source": d.heat_source,
-            "mesh_format": d.mesh_format,
+            "mesh_format": d.mesh_format, "order": d.order, "scheme": d.scheme,
             "bcs": [[b.tag, b.type, b.value] for b in d.bcs]}
 
 
@@ -105,13 +124,15 @@ def load(name: str):
     d = decks.Deck(mesh=mesh, bands=bands, bcs=[decks.BC(int(t), int(ty), float(v)) for t, ty, v in p["bcs"]],
                    scale=tuple(p["scale"]), material_dim=p["material_dim"], angle_method=p["angle_method"],
                    n_theta=p["n_theta"], n_phi=p["n_phi"], tref=p["tref"], heat_source=p["heat_source"],
-                   mesh_format=p["mesh_format"], residual_temp=1e-12, residual_flux=1e-12, max_iter=3000)
+                   mesh_format=p["mesh_format"], order=p.get("order", "2"), scheme=p.get("scheme", "Synthetic"),
+                   residual_temp=1e-12, residual_flux=1e-12, max_iter=3000)
     ref = {k: z[k] for k in ("T", "E", "q", "Tband", "xyz", "Tf", "qf", "margins") if k in z}
     ref["iters"] = int(z["iters"])
     return d, ref
 
 
-CASES = ["gray_square_tri", "quad_heat_specular", "periodic_jitter", "porous_msh"]
+CASES = ["gray_square_tri", "quad_heat_specular", "periodic_jitter", "porous_msh", "porous_firstorder",
+         "periodic_sequential", "quad_firstorder_sequential"]
 
 if __name__ == "__main__":
     want = sys.argv[1:] or CASES

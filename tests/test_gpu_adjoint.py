@@ -309,3 +309,16 @@ def test_forward_state_survives_vjp():
         s.close()
     for k in ("T", "E", "q", "Tband"):
         assert np.array_equal(out[0][k], out[1][k]), k
+
+
+def test_adjoint_rejects_solver_variants():
+    # the adjoint transposes the second-order Synthetic scheme only
+    import make_golden as mg
+
+    for case in ("porous_firstorder", "periodic_sequential"):
+        d, _ = mg.load(case)
+        s = g.StaticBTESynthetic.from_deck(d, precision=g.GBTE_FP64)
+        s.solve(max_iter=3, err_temp=0.0, err_flux=0.0)
+        with pytest.raises(g.GBTEError):
+            s.vjp(q_bar=np.zeros((d.mesh.n_cells, 3)))
+        s.close()

@@ -37,7 +37,7 @@ def solve_pair(deck, prec, T0=None, heat=None, iters=None):
 @pytest.mark.parametrize("case", mg.CASES)
 def test_orders_agree_on_golden_decks(case):
     deck, ref = mg.load(case)
-    (fa, ga), (fb, gb) = solve_pair(deck, g.GBTE_FP64)
+    (fa, ga), (fb, gb) = solve_pair(deck, g.GBTE_FP64, T0=ref["Tf"])
     assert np.array_equal(ga[0], gb[0]) and np.array_equal(ga[1], gb[1])
     for k in ("T", "E", "q", "Tband"):
         assert rel(fa[k], fb[k]) <= 1e-10, (k, rel(fa[k], fb[k]))

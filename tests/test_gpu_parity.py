@@ -22,6 +22,9 @@ def rel(a, b):
 def test_fp64_matches_reference(case):
     deck, ref = mg.load(case)
     s = StaticBTESynthetic.from_deck(deck, precision=GBTE_FP64)
+    # the reference's start (its Fourier pre-solve): the Sequential scheme
+    # without isothermal walls keeps the start's temperature level
+    s.set_initial(ref["Tf"], ref["qf"])
     st = s.solve(allow_not_converged=False)
     f = s.fields()
     assert st["err_temp"] <= 1e-12 and st["err_flux"] <= 1e-12
@@ -37,9 +40,25 @@ def test_fp32_mixed_close_to_reference(case):
     deck.residual_temp = 1e-9
     deck.residual_flux = 1e-7
     s = StaticBTESynthetic.from_deck(deck, precision=GBTE_FP32_MIXED)
+    s.set_initial(ref["Tf"], ref["qf"])
     s.solve()
     f = s.fields()
     # relative to the temperature variation, which is what the FP32 deviation form resolves
     span = np.max(ref["T"]) - np.min(ref["T"])
     assert np.max(np.abs(f["T"] - ref["T"])) / max(span, 1e-30) <= 1e-4
     assert rel(f["T"], ref["T"]) <= TOL_FP32
+
+
+@pytest.mark.parametrize("case", ["porous_firstorder", "periodic_sequential", "quad_firstorder_sequential"])
+def test_variant_decks_from_files_match_reference(case, tmp_path):
+    # Order=1 / IterativeScheme=Sequential read from the CONTROL file of a
+    # deck directory select the same variants as the in-memory options
+    deck, ref = mg.load(case)
+    deck.write(str(tmp_path))
+    s = StaticBTESynthetic.from_deck_dir(str(tmp_path), precision=GBTE_FP64)
+    s.set_initial(ref["Tf"], ref["qf"])
+    s.solve(allow_not_converged=False)
+    f = s.fields()
+    s.close()
+    assert rel(f["T"], ref["T"]) <= TOL_FP64, rel(f["T"], ref["T"])
+    assert rel(f["q"], ref["q"]) <= 1e-8
