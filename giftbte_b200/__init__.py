@@ -67,7 +67,7 @@ class Options(ctypes.Structure):
                 ("macro_rtol", ctypes.c_double), ("profile", ctypes.c_int), ("sweep_bands", ctypes.c_int),
                 ("sweep_far_slots", ctypes.c_int), ("direction_batch", ctypes.c_int),
                 ("cell_scatter", _c_dbl_p), ("cell_order", ctypes.c_int), ("order", ctypes.c_int),
-                ("scheme", ctypes.c_int)]
+                ("scheme", ctypes.c_int), ("macro_exact", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -225,7 +225,8 @@ class StaticBTESynthetic:
             cell_heat = deck.cell_heat()
         heat = np.ascontiguousarray(cell_heat, dtype=np.float64) if cell_heat is not None else None
         kw = {"max_iter": deck.max_iter, "err_temp": deck.residual_temp, "err_flux": deck.residual_flux,
-              "order": 1 if deck.order == "1" else 2, "scheme": 1 if deck.scheme == "Sequential" else 0}
+              "order": 1 if deck.order == "1" else 2, "scheme": 1 if deck.scheme == "Sequential" else 0,
+              "use_limiter": 1 if deck.order == "2limit" else 0}
         kw.update(opt)
         o = default_options(precision, device=device, verbose=verbose, **kw)
         o.cell_heat = _ptr(heat, ctypes.c_double)

@@ -154,6 +154,7 @@ int create_common(const gbte::RawMesh &raw_in, const gbte::Bands &bands_in, cons
         return fail(nullptr, {-1, "scheme must be 0 (Synthetic) or 1 (Sequential)"}), GBTE_ERR_ARG;
     cfg.order = opt.order == 1 ? 1 : 2;
     cfg.sequential = opt.scheme == 1;
+    cfg.macro_exact = opt.macro_exact != 0;
     cfg.device = opt.device;
     cfg.stream = (cudaStream_t)opt.stream;
     if (opt.precision != GBTE_FP64 && opt.precision != GBTE_FP32_MIXED)

@@ -145,6 +145,61 @@ __global__ void __launch_bounds__(256) k_gradient(DMesh m, DPhys p, const S *__r
     }
 }
 
+// Order=2limit: the limiter of _get_gradient_larger (StaticBTESynthetic.cpp:
+// 1372-1422) on the FP64 form. Per (direction, cell, band): the extremes of
+// the cell value, its face neighbours' values and the incoming wall values
+// (side 0 of the wall, not on specular walls), then for each face in order
+// phi(y) = (y^2 + 2y) / (y^2 + y + 2) wherever the limited face value leaves
+// them; the gradient is stored multiplied by phi, which is how every face
+// value and outgoing wall value uses it.
+template <int DIM>
+__global__ void k_limit(DMesh m, DPhys p, const double *__restrict__ e, const double *__restrict__ eb,
+                        double *__restrict__ g, int d0, int ndb) {
+    const int nb = p.nb, nc = m.nc;
+    const size_t total = (size_t)ndb * nc * nb;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b = (int)(t % nb);
+        const size_t dc = t / nb;  // (batch direction, cell)
+        const int c = (int)(dc % nc);
+        const size_t d = d0 + dc / nc;
+        const double *ed = e + d * nc * nb + b;
+        const double sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
+        const double ec = ed[(size_t)c * nb];
+        double mx = ec, mn = ec;
+        for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+            const int bnd = m.cf_bound[k];
+            double v;
+            if (bnd < 0) {
+                v = ed[(size_t)m.cf_nbr[k] * nb];
+            } else {
+                if (m.b_type[bnd] == 3 || !(sx * m.cf_nx[k] + sy * m.cf_ny[k] + sz * m.cf_nz[k] < 0)) continue;
+                v = eb[(d * m.nbs + 2 * (size_t)bnd) * nb + b];
+            }
+            mx = v > mx ? v : mx;
+            mn = v < mn ? v : mn;
+        }
+        double *gp = g + dc * DIM * nb + b;
+        const double gx = gp[0], gy = gp[nb], gz = DIM == 3 ? gp[2 * nb] : 0.0;
+        double lim = 1.0;
+        for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+            const double del = gx * (m.cf_fx[k] - m.cx[c]) + gy * (m.cf_fy[k] - m.cy[c]) + gz * (m.cf_fz[k] - m.cz[c]);
+            if (del * lim + ec < mn) {
+                const double y = (mn - ec) / del;
+                lim = (y * y + 2 * y) / (y * y + y + 2);
+            }
+            if (del * lim + ec > mx) {
+                const double y = (mx - ec) / del;
+                lim = (y * y + 2 * y) / (y * y + y + 2);
+            }
+        }
+        if (lim != 1.0) {
+            gp[0] = gx * lim;
+            gp[nb] = gy * lim;
+            if (DIM == 3) gp[2 * nb] = gz * lim;
+        }
+    }
+}
+
 template <typename S, int DIM>
 struct EView {
     const S *eps, *g;  // eps: all directions; g: directions gd0 .. of the current batch
@@ -1524,7 +1579,9 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
     cfg = c;
     if (bands.nmat != 1)
         return {-8, "more than one material is not supported by this solver (interfaces between materials)"};
-    if (cfg.use_limiter) return {-8, "Order=2limit (gradient limiter) is not supported by this solver"};
+    if (cfg.use_limiter && cfg.precision != 0)
+        return {-8, "Order=2limit (the gradient limiter) needs the FP64 form (GBTE_FP64)"};
+    if (cfg.use_limiter && cfg.order != 2) return {-1, "the gradient limiter applies to the second-order scheme"};
     for (int t : mesh.b_type)
         if (!(t == 1 || t == 2 || t == 3 || t == 6 || t < 0))
             return {-8, "boundary type " + std::to_string(t) + " is not supported"};
@@ -2502,6 +2559,9 @@ Error Solver::solve_t(SolveStats &st) {
             if (cfg.order == 2)
                 GL(K_GRADIENT, (k_gradient<S, DIM><<<grid_for((size_t)nbt * nc * nb), kThreads, 0, s>>>(dm_, dp_, w, eps,
                                                                                                      g, d0, nbt)));
+            if (cfg.use_limiter)
+                GL(K_GRADIENT, (k_limit<DIM><<<grid_for((size_t)nbt * nc * nb), kThreads, 0, s>>>(
+                                   dm_, dp_, (const double *)eps, eb_, (double *)g, d0, nbt)));
             GL(K_BOUND_OUT, (k_bound_out<S, DIM><<<grid_for((size_t)nbt * nbs * nb), kThreads, 0, s>>>(dm_, dp_, ev,
                                                                                                    eb_, d0, nbt)));
         }
@@ -2536,11 +2596,17 @@ Error Solver::solve_t(SolveStats &st) {
             if (cfg.order == 2)
                 GL(K_GRADIENT, (k_gradient8<S, DIM, 4><<<grid_for(nbe / 4), kThreads, 0, s>>>(dm_, dp_, w, eps, g, d0,
                                                                                               nbt)));
+            if (cfg.use_limiter)
+                GL(K_GRADIENT, (k_limit<DIM><<<grid_for(nbe), kThreads, 0, s>>>(dm_, dp_, (const double *)eps, eb_,
+                                                                               (double *)g, d0, nbt)));
             GL(K_RESIDUAL, (k_residual8<S, DIM, 4><<<grid_for(nbe / 4), kThreads, 0, s>>>(dm_, dp_, ev, Bflux_, Told_, eb_,
                                                                                           pos_of_, R, d0, nbt)));
         } else {
             if (cfg.order == 2)
                 GL(K_GRADIENT, (k_gradient<S, DIM><<<grid_for(nbe), kThreads, 0, s>>>(dm_, dp_, w, eps, g, d0, nbt)));
+            if (cfg.use_limiter)
+                GL(K_GRADIENT, (k_limit<DIM><<<grid_for(nbe), kThreads, 0, s>>>(dm_, dp_, (const double *)eps, eb_,
+                                                                               (double *)g, d0, nbt)));
             GL(K_RESIDUAL, (k_residual<S, DIM><<<grid_for(nbe), kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, pos_of_, R,
                                                                                   d0, nbt)));
         }
@@ -2669,7 +2735,7 @@ Error Solver::solve_t(SolveStats &st) {
                 CUDA_TRY(cudaMemcpyAsync(T_, warm_[step], (size_t)nc * 8, cudaMemcpyDeviceToDevice, s));
             // from a warm start the residual must drop by kWarmEta; the
             // absolute floor macro_rtol * |b| still bounds the final error
-            const bool warm = step < (int)warm_.size() && warm_[step] && warm_ok_[step];
+            const bool warm = step < (int)warm_.size() && warm_[step] && warm_ok_[step] && !cfg.macro_exact;
             double sq = 0;
             Error e = cg_solve(kplan_, K_ptr_, K_idx_, K_val_, K_dinv_, T_, rhs_, cfg.macro_rtol,
                                warm ? kWarmEta : 0.0, st.cg_iterations, cg_scal_, cg_r_, cg_z_, cg_p_, cg_Ap_, T1_, &sq);
@@ -3688,8 +3754,8 @@ Error Solver::vjp(const double *Tbar_h, const double *qbar_h, int max_iter, doub
     if (ncomp_ > 1) return {-8, "the adjoint is not implemented for batched handles"};
     if (!started_ || last_inner_ < 1) return {-1, "call gbte_solve (to convergence) before gbte_vjp"};
     if (need_snapshot_) return {-8, "the adjoint does not support chained specular reflections"};
-    if (cfg.order != 2 || cfg.sequential)
-        return {-8, "the adjoint is implemented for the second-order Synthetic scheme only"};
+    if (cfg.order != 2 || cfg.sequential || cfg.use_limiter)
+        return {-8, "the adjoint is implemented for the second-order Synthetic scheme without limiter only"};
     if (ndb_ < ang.nd) return {-8, "the adjoint needs every direction's buffers resident (direction_batch)"};
     if (max_iter < 1 || !(tol > 0)) return {-1, "invalid adjoint limits"};
     CUDA_TRY(cudaSetDevice(cfg.device));

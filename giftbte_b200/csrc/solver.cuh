@@ -54,6 +54,7 @@ struct SolverConfig {
     std::vector<double> cell_scatter;  // scattering-rate multiplier s_c per cell (empty: 1)
     int order = 2;            // 2: second-order upwind faces (solve); 1: first order (solve_firstorder)
     bool sequential = false;  // Sequential scheme (solve_DOM): no macro correction, T = T_lat
+    bool macro_exact = false; // macro CG solves to macro_rtol even from a warm start
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;

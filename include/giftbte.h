@@ -120,7 +120,8 @@ typedef struct {
 
 typedef struct {
     int precision;            /* GBTE_FP64 or GBTE_FP32_MIXED */
-    int use_limiter;          /* Order=2limit */
+    int use_limiter;          /* Order=2limit: the gradient limiter of _get_gradient_larger
+                                 (StaticBTESynthetic.cpp:1372-1422); GBTE_FP64 only */
     int max_iter;
     double err_temp;          /* ResidualTemp */
     double err_flux;          /* ResidualFlux */
@@ -148,6 +149,11 @@ typedef struct {
     int scheme;               /* 0 = Synthetic (IterativeScheme=Synthetic: the macro correction), 1 =
                                  Sequential (IterativeScheme=Sequential, solve_DOM /
                                  solve_DOM_firstorder: plain source iteration, T from the moments) */
+    int macro_exact;          /* 1: every macro CG solve reaches macro_rtol from its start, as the
+                                 reference's LU solve is exact, so the outer iterates follow the
+                                 reference's step by step; 0 (default): a solve warm-started from the
+                                 previous outer iteration stops after a 1e-4 residual reduction (same
+                                 fixed point, fewer CG iterations) */
 } gbte_options;
 
 #define GBTE_NUM_KERNELS 16

@@ -104,7 +104,8 @@ def solve(deck, T0: Optional[np.ndarray] = None, max_iter: Optional[int] = None,
         ctypes.c_double(deck.scale[0]), _p(cell_heat, ctypes.c_double), _p(T0, ctypes.c_double), None,
         int(max_iter if max_iter is not None else deck.max_iter),
         ctypes.c_double(err_T if err_T is not None else deck.residual_temp),
-        ctypes.c_double(err_q if err_q is not None else deck.residual_flux), 0,
+        ctypes.c_double(err_q if err_q is not None else deck.residual_flux),
+        1 if getattr(deck, "order", "2") == "2limit" else 0,
         _p(out_T, ctypes.c_double), _p(out_E, ctypes.c_double), _p(out_q, ctypes.c_double),
         _p(out_Tb, ctypes.c_double), ctypes.byref(iters), _p(err, ctypes.c_double),
         _p(cell_scatter, ctypes.c_double), 1 if getattr(deck, "order", "2") == "1" else 2,

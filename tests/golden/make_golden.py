@@ -34,6 +34,9 @@ from giftbte_b200 import decks  # noqa: E402
 import oracle  # noqa: E402
 
 
+LIMITER_ITERS = 40
+
+
 def cases():
     out = {}
     # 1. the gray 2D square (3200 triangles, 32 CADOM directions)
@@ -74,6 +77,13 @@ def cases():
         mesh=m, bands=decks.sine_dispersion_bands(3),
         bcs=[decks.BC(1, -2, 1.0), decks.BC(2, -1, 0.0), decks.BC(3, 3, 0.0), decks.BC(4, 3, 0.0)],
         scale=(1e-7, 1e-7), material_dim=2, angle_method=1, n_phi=4, tref=0.0, scheme="Sequential")
+    # 8. the gradient limiter (Order=2limit) on the porous cell
+    m = decks.porous_cell_mesh(0.1, [(0.5, 0.5, 0.25)], seed=4)
+    out["porous_limiter"] = decks.Deck(
+        mesh=m, bands=decks.sine_dispersion_bands(4),
+        bcs=[decks.BC(1, -2, 1.0), decks.BC(2, -1, 0.0), decks.BC(3, -4, 0.0), decks.BC(4, -3, 0.0),
+             decks.BC(5, 2, 0.0)],
+        scale=(3e-7, 3e-7), material_dim=2, angle_method=2, n_phi=4, tref=0.0, order="2limit")
     out["quad_firstorder_sequential"] = decks.Deck(
         mesh=decks.square_quad_mesh(16, 16), bands=decks.sine_dispersion_bands(2),
         bcs=[decks.BC(1, 1, 300.0), decks.BC(2, 1, 300.0), decks.BC(3, 3, 0.0), decks.BC(4, 3, 0.0)],
@@ -83,6 +93,10 @@ def cases():
         d.residual_temp = 1e-12
         d.residual_flux = 1e-12
         d.max_iter = 3000
+    # the limited scheme does not settle to 1e-12 (its margins stall near
+    # 1e-4 on this deck): the fixture is the reference's state after 40
+    # outer iterations from its Fourier start
+    out["porous_limiter"].max_iter = LIMITER_ITERS
     return out
 
 
@@ -125,14 +139,17 @@ def load(name: str):
                    scale=tuple(p["scale"]), material_dim=p["material_dim"], angle_method=p["angle_method"],
                    n_theta=p["n_theta"], n_phi=p["n_phi"], tref=p["tref"], heat_source=p["heat_source"],
                    mesh_format=p["mesh_format"], order=p.get("order", "2"), scheme=p.get("scheme", "Synthetic"),
-                   residual_temp=1e-12, residual_flux=1e-12, max_iter=3000)
+                   residual_temp=1e-12, residual_flux=1e-12,
+                   max_iter=LIMITER_ITERS if p.get("order") == "2limit" else 3000)
     ref = {k: z[k] for k in ("T", "E", "q", "Tband", "xyz", "Tf", "qf", "margins") if k in z}
     ref["iters"] = int(z["iters"])
     return d, ref
 
 
 CASES = ["gray_square_tri", "quad_heat_specular", "periodic_jitter", "porous_msh", "porous_firstorder",
-         "periodic_sequential", "quad_firstorder_sequential"]
+         "periodic_sequential", "quad_firstorder_sequential", "porous_limiter"]
+# the cases solved to 1e-12 margins (all but the limited one, a fixed count)
+CONVERGED = [c for c in CASES if c != "porous_limiter"]
 
 if __name__ == "__main__":
     want = sys.argv[1:] or CASES

@@ -29,7 +29,7 @@ def iterations_to(margins, tol):
     return int(ok[0]) + 1 if len(ok) else None
 
 
-@pytest.mark.parametrize("case", mg.CASES)
+@pytest.mark.parametrize("case", mg.CONVERGED)
 def test_iterations_from_fourier_start_match_reference(case):
     # from the same (Fourier) start the outer iteration follows the
     # reference's: the number of iterations to margins 1e-8 agrees (near

@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 import make_golden as mg
-from giftbte_b200 import GBTE_FP32_MIXED, GBTE_FP64, StaticBTESynthetic
+from giftbte_b200 import GBTE_FP32_MIXED, GBTE_FP64, GBTEError, StaticBTESynthetic
 
 pytestmark = pytest.mark.gpu
 
@@ -21,20 +21,28 @@ def rel(a, b):
 @pytest.mark.parametrize("case", mg.CASES)
 def test_fp64_matches_reference(case):
     deck, ref = mg.load(case)
-    s = StaticBTESynthetic.from_deck(deck, precision=GBTE_FP64)
+    # a fixed iteration count (the limited scheme) compares iterates, which
+    # follow the reference's only with exact macro solves
+    s = StaticBTESynthetic.from_deck(deck, precision=GBTE_FP64, macro_exact=int(case not in mg.CONVERGED))
     # the reference's start (its Fourier pre-solve): the Sequential scheme
     # without isothermal walls keeps the start's temperature level
     s.set_initial(ref["Tf"], ref["qf"])
-    st = s.solve(allow_not_converged=False)
+    if case in mg.CONVERGED:
+        st = s.solve(allow_not_converged=False)
+        assert st["err_temp"] <= 1e-12 and st["err_flux"] <= 1e-12
+    else:
+        # the limited scheme: the reference's state after a fixed number of
+        # outer iterations, the same count here
+        st = s.solve(max_iter=ref["iters"], err_temp=0.0, err_flux=0.0)
+        assert st["iterations"] == ref["iters"]
     f = s.fields()
-    assert st["err_temp"] <= 1e-12 and st["err_flux"] <= 1e-12
     assert rel(f["T"], ref["T"]) <= TOL_FP64, rel(f["T"], ref["T"])
     assert rel(f["E"], ref["E"]) <= TOL_FP64
     assert rel(f["Tband"], ref["Tband"]) <= TOL_FP64
     assert rel(f["q"], ref["q"]) <= 1e-8
 
 
-@pytest.mark.parametrize("case", mg.CASES)
+@pytest.mark.parametrize("case", mg.CONVERGED)
 def test_fp32_mixed_close_to_reference(case):
     deck, ref = mg.load(case)
     deck.residual_temp = 1e-9
@@ -49,16 +57,46 @@ def test_fp32_mixed_close_to_reference(case):
     assert rel(f["T"], ref["T"]) <= TOL_FP32
 
 
-@pytest.mark.parametrize("case", ["porous_firstorder", "periodic_sequential", "quad_firstorder_sequential"])
+@pytest.mark.parametrize("case", ["porous_firstorder", "periodic_sequential", "quad_firstorder_sequential",
+                                  "porous_limiter"])
 def test_variant_decks_from_files_match_reference(case, tmp_path):
-    # Order=1 / IterativeScheme=Sequential read from the CONTROL file of a
-    # deck directory select the same variants as the in-memory options
+    # Order=1 / 2limit and IterativeScheme=Sequential read from the CONTROL
+    # file of a deck directory select the same variants as the in-memory
+    # options
     deck, ref = mg.load(case)
     deck.write(str(tmp_path))
-    s = StaticBTESynthetic.from_deck_dir(str(tmp_path), precision=GBTE_FP64)
+    s = StaticBTESynthetic.from_deck_dir(str(tmp_path), precision=GBTE_FP64,
+                                         macro_exact=int(case not in mg.CONVERGED))
     s.set_initial(ref["Tf"], ref["qf"])
-    s.solve(allow_not_converged=False)
+    if case in mg.CONVERGED:
+        s.solve(allow_not_converged=False)
+    else:
+        s.solve(max_iter=ref["iters"], err_temp=0.0, err_flux=0.0)
     f = s.fields()
     s.close()
     assert rel(f["T"], ref["T"]) <= TOL_FP64, rel(f["T"], ref["T"])
     assert rel(f["q"], ref["q"]) <= 1e-8
+
+
+def test_limiter_needs_the_fp64_form():
+    deck, _ = mg.load("porous_limiter")
+    with pytest.raises(GBTEError):
+        StaticBTESynthetic.from_deck(deck, precision=GBTE_FP32_MIXED)
+
+
+@pytest.mark.parametrize("case", ["porous_msh", "porous_firstorder", "periodic_sequential", "porous_limiter"])
+def test_iterates_follow_reference_step_by_step(case):
+    # with exact macro solves (options.macro_exact) the outer iterates
+    # themselves follow the reference's: five iterations from the same start
+    # against the CPU restatement, which repeats the reference's arithmetic
+    import oracle
+
+    deck, ref = mg.load(case)
+    s = StaticBTESynthetic.from_deck(deck, precision=GBTE_FP64, macro_exact=1)
+    s.set_initial(ref["Tf"])
+    s.solve(max_iter=5, err_temp=0.0, err_flux=0.0)
+    f = s.fields()
+    s.close()
+    o = oracle.solve(deck, T0=ref["Tf"], max_iter=5, err_T=0.0, err_q=0.0)
+    assert rel(f["T"], o["T"]) <= 1e-10, rel(f["T"], o["T"])
+    assert rel(f["q"], o["q"]) <= 1e-9, rel(f["q"], o["q"])

@@ -21,8 +21,13 @@ def test_oracle_matches_reference(case):
     # from the reference's own start, its Fourier pre-solve: in the
     # Sequential scheme with only periodic and specular walls the
     # temperature level is a neutral mode, so the start sets it
-    o = oracle.solve(deck, T0=ref["Tf"])
-    assert o["err"][0] <= 1e-12 and o["err"][1] <= 1e-12
+    if case in mg.CONVERGED:
+        o = oracle.solve(deck, T0=ref["Tf"])
+        assert o["err"][0] <= 1e-12 and o["err"][1] <= 1e-12
+    else:
+        # the limited scheme: the same fixed number of outer iterations
+        o = oracle.solve(deck, T0=ref["Tf"], err_T=0.0, err_q=0.0)
+        assert o["iters"] == ref["iters"]
     assert rel(o["T"], ref["T"]) <= TOL
     assert rel(o["E"], ref["E"]) <= TOL
     assert rel(o["Tband"], ref["Tband"]) <= TOL
