@@ -152,7 +152,7 @@ typedef struct {
     int macro_exact;          /* 1: every macro CG solve reaches macro_rtol from its start, as the
                                  reference's LU solve is exact, so the outer iterates follow the
                                  reference's step by step; 0 (default): a solve warm-started from the
-                                 previous outer iteration stops after a 1e-4 residual reduction (same
+                                 previous outer iteration stops after a 3e-3 residual reduction (same
                                  fixed point, fewer CG iterations) */
 } gbte_options;
 
