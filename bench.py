@@ -184,7 +184,10 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     # a stream of its own (capturable: the library replays its transport
     # stage as a CUDA graph on it)
     stream = torch.cuda.Stream()
-    deck, desc = build_deck(args.workload, seed=rank, h_nm=args.h_nm)
+    # replicas: a seeded cell per rank; direction shards: one cell, its
+    # directions split over the ranks
+    by_dirs = args.shard == "directions"
+    deck, desc = build_deck(args.workload, seed=0 if by_dirs else rank, h_nm=args.h_nm)
     nc = deck.mesh.n_cells
     prec = g.GBTE_FP32_MIXED if args.precision == "fp32" else g.GBTE_FP64
     s_bytes = 4 if prec == g.GBTE_FP32_MIXED else 8
@@ -194,6 +197,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                                             sweep_bands=args.sweep_bands)
     nb, nd = solver.num_bands, solver.num_directions
     upd_per_step = nb * nd * nc
+    upd_local = upd_per_step
+    if by_dirs:
+        upd_local = nb * attach_shard(solver, rank, world) * nc
     # warm-up (not timed)
     solver.solve(max_iter=args.warmup, err_temp=0.0, err_flux=0.0)
     torch.cuda.synchronize()
@@ -212,7 +218,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     clk = clocks.stop()
     ms_local = ev0.elapsed_time(ev1)
     ms = ranks_reduce(ms_local, "max", world, "cuda")
-    value = whole_job_rate(upd_per_step * args.steps, ms_local * 1e-3, world, "cuda")
+    value = whole_job_rate(upd_local * args.steps, ms_local * 1e-3, world, "cuda")
 
     # roofline of the dominant kernel, and of every streaming kernel: per-launch
     # CUDA events on the solver's stream, from K more iterations launched
@@ -252,7 +258,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     solver.close()
 
     # end to end through the public API: host in, solve to 1e-8, host out
-    e2e, ttr = e2e_solves(args, deck, prec, local_rank, world)
+    e2e, ttr = e2e_solves(args, deck, prec, local_rank, world, rank if by_dirs else None)
 
     out = None
     if rank == 0:
@@ -263,7 +269,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         out = {
             "metric": "band*dir*cell updates/s (time to residual 1e-8 alongside); FP32-mixed vs FP64 on 1 B200",
             "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong" if by_dirs else "weak", "vs_baseline": None,
             "dtype": "f32" if prec == g.GBTE_FP32_MIXED else "f64",
             "data": "synthetic: seeded mesh and band table generated in-process (no dataset)",
             "config": {"workload": desc, "cells": nc, "bands": nb, "directions": nd,
@@ -271,7 +278,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                        "cell_order": "morton" if args.cell_order == 0 else "deck",
                        "sweep_bands": st.get("sweep_bands"), "sweep_stage_levels": st.get("sweep_stage_levels"),
                        "l2": f"band state {upd_per_step * s_bytes / 1e6:.0f} MB per copy, larger than the 126 MB L2",
-                       "parallelism": f"replicas x{world} (independent seeded cells)" if world > 1 else "1 GPU"},
+                       "parallelism": (f"direction shards x{world} of one cell (NCCL all-reduce of the moments and "
+                                       "boundary values every outer iteration)" if by_dirs and world > 1 else
+                                       f"replicas x{world} (independent seeded cells)" if world > 1 else "1 GPU")},
             "roofline": roofline, "hbm_kernels": hbm_kernels, "kernels": kernel_table, "cpu_baseline": cpu,
             "e2e": e2e,
             "time_to_residual": ttr, "gpu_launches": int(st["kernel_launches"]), "clocks": clk,
@@ -286,7 +295,19 @@ def ctypes_stream(stream) -> int:
     return int(stream.cuda_stream)
 
 
-def e2e_solves(args, deck, prec, device, world):
+def attach_shard(solver, rank: int, world: int) -> int:
+    """Give the solver rank's block of directions, exchanging over the
+    default process group (NCCL); one rank holds every direction and its
+    exchange is the identity. Returns the block's size."""
+    from giftbte_b200 import shard
+
+    b, n = shard.direction_blocks(solver.num_directions, world)[rank]
+    ex = shard.torch_exchange() if world > 1 else (lambda buf, count, stream: None)
+    solver.set_direction_shard(b, n, ex)
+    return n
+
+
+def e2e_solves(args, deck, prec, device, world, shard_rank=None):
     import torch
 
     import giftbte_b200 as g
@@ -296,6 +317,8 @@ def e2e_solves(args, deck, prec, device, world):
                                             err_temp=1e-8, err_flux=1e-8, cell_order=args.cell_order,
                                             sweep_bands=args.sweep_bands)
     nb = solver.num_bands
+    if shard_rank is not None:
+        attach_shard(solver, shard_rank, world)
     T0 = torch.full((nc,), float(deck.tref), dtype=torch.float64).pin_memory().numpy()
     out = {k: np.zeros(n) for k, n in (("E", nc), ("T", nc), ("q", 3 * nc), ("Tb", nb * nc))}
     nsteps = max(1, min(args.steps, args.e2e_steps))
@@ -554,6 +577,9 @@ def main():
     ap.add_argument("--ref-timeout", type=float, default=1500.0)
     ap.add_argument("--no-fp64", dest="compare_fp64", action="store_false")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--shard", choices=["replicas", "directions"], default="replicas",
+                    help="N > 1: a seeded cell per rank (weak scaling), or one cell's directions split over "
+                         "the ranks (strong scaling)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -31,7 +31,8 @@ GBTE_FP32_MIXED = 1
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "input/output error", -3: "CUDA error", -4: "diverged",
           -5: "device wait timed out", -6: "out of memory", -7: "mesh topology error", -8: "unsupported input",
-          1: "not converged within max_iter"}
+          -9: "direction shard exchange failed", 1: "not converged within max_iter"}
+GBTE_ERR_EXCHANGE = -9
 
 _c_int_p = ctypes.POINTER(ctypes.c_int)
 _c_dbl_p = ctypes.POINTER(ctypes.c_double)
@@ -118,7 +119,10 @@ EXPORTS = ["gbte_inspect_deck", "gbte_inspect_mesh", "gbte_default_options", "gb
            "gbte_fourier_initial", "gbte_solve", "gbte_get_fields", "gbte_write_outputs", "gbte_get_sizes",
            "gbte_get_geometry", "gbte_last_error", "gbte_status_string", "gbte_destroy", "gbte_kernel_name",
            "gbte_solve_with", "gbte_fourier_initial_noalloc", "gbte_batch_create", "gbte_batch_geometries",
-           "gbte_vjp", "gbte_set_profile"]
+           "gbte_vjp", "gbte_set_profile", "gbte_set_direction_shard"]
+
+# int (*gbte_exchange_fn)(void *user, double *buf, size_t count, void *stream)
+EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
 
 _lib = None
 
@@ -156,6 +160,8 @@ def library():
                                           ctypes.POINTER(Options), ctypes.POINTER(ctypes.c_void_p)]
         lib.gbte_batch_geometries.argtypes = [ctypes.c_void_p, _c_int_p, _c_int_p]
         lib.gbte_set_profile.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        lib.gbte_set_direction_shard.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, EXCHANGE_FN,
+                                                 ctypes.c_void_p]
         lib.gbte_vjp.argtypes = [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, ctypes.c_int, ctypes.c_double, _c_dbl_p,
                                  _c_dbl_p, _c_dbl_p, ctypes.POINTER(VjpStats)]
         lib.gbte_inspect_deck.argtypes = [ctypes.c_char_p, ctypes.POINTER(DeckInfo)]
@@ -392,6 +398,32 @@ class StaticBTESynthetic:
         return {"tau": g_tau, "scatter": g_cell, "specularity": g_spec,
                 "stats": {k: getattr(st, k) for k, _ in st._fields_}}
 
+    def set_direction_shard(self, begin: int, count: int, exchange) -> None:
+        """Transport over directions [begin, begin + count) only; the moments
+        and boundary values are summed over the shard set every outer
+        iteration by ``exchange(buf, count, stream)`` (gbte_set_direction_shard;
+        ``giftbte_b200.shard`` has exchanges over torch.distributed and over
+        threads of one process). ``exchange`` sums ``count`` doubles of
+        device memory at address ``buf`` in place, ordered on the CUDA stream
+        ``stream``; an exception makes the solve fail with
+        GBTE_ERR_EXCHANGE. count = 0 or exchange = None: all directions."""
+        self._xerr = None
+        if exchange is None or count == 0:
+            self._xcb = None
+            self._check(library().gbte_set_direction_shard(self._h, 0, 0, EXCHANGE_FN(), None))
+            return
+
+        def cb(user, buf, n, stream):
+            try:
+                exchange(buf or 0, int(n), stream or 0)
+                return 0
+            except BaseException as e:  # reported by the solve that called it
+                self._xerr = e
+                return 1
+
+        self._xcb = EXCHANGE_FN(cb)
+        self._check(library().gbte_set_direction_shard(self._h, int(begin), int(count), self._xcb, None))
+
     def set_profile(self, on: bool) -> None:
         """Per-launch kernel timing for the next solves (gbte_set_profile)."""
         self._check(library().gbte_set_profile(self._h, int(bool(on))))
@@ -420,7 +452,11 @@ class StaticBTESynthetic:
 
     def _check(self, rc: int) -> None:
         if rc != GBTE_OK:
-            raise GBTEError(rc, library().gbte_last_error(self._h).decode())
+            msg = library().gbte_last_error(self._h).decode()
+            xerr = getattr(self, "_xerr", None)
+            if rc == GBTE_ERR_EXCHANGE and xerr is not None:
+                raise GBTEError(rc, f"{msg}: {xerr!r}") from xerr
+            raise GBTEError(rc, msg)
 
 
 def _views(deck) -> dict:

@@ -64,6 +64,7 @@ int status_of(int code) {
     case -6: return GBTE_ERR_NOMEM;
     case -7: return GBTE_ERR_MESH;
     case -8: return GBTE_ERR_UNSUPPORTED;
+    case -9: return GBTE_ERR_EXCHANGE;
     default: return GBTE_ERR_ARG;
     }
 }
@@ -673,6 +674,13 @@ int gbte_vjp(gbte_handle *h, const double *T_bar, const double *q_bar, int max_i
     }
 }
 
+int gbte_set_direction_shard(gbte_handle *h, int dir_begin, int dir_count, gbte_exchange_fn exchange, void *user) {
+    if (!h) return GBTE_ERR_ARG;
+    gbte::Error e = h->solver.set_shard(dir_begin, dir_count, exchange, user);
+    if (e.code) return fail(h, e), status_of(e.code);
+    return GBTE_OK;
+}
+
 int gbte_set_profile(gbte_handle *h, int on) {
     if (!h) return GBTE_ERR_ARG;
     h->solver.cfg.profile = on ? 1 : 0;
@@ -697,6 +705,7 @@ const char *gbte_status_string(int s) {
     case GBTE_ERR_NOMEM: return "out of memory";
     case GBTE_ERR_MESH: return "mesh topology error";
     case GBTE_ERR_UNSUPPORTED: return "unsupported input";
+    case GBTE_ERR_EXCHANGE: return "direction shard exchange failed";
     case GBTE_ERR_NOT_CONVERGED: return "not converged within max_iter";
     default: return "unknown status";
     }

@@ -33,6 +33,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <unordered_map>
 #include <chrono>
 #include <cmath>
@@ -1553,6 +1554,7 @@ Solver::~Solver() {
     if (cfg.device >= 0) cudaSetDevice(cfg.device);
     if (cfg.stream) cudaStreamSynchronize(cfg.stream);
     if (tgraph_) cudaGraphExecDestroy(tgraph_);
+    if (tgraph2_) cudaGraphExecDestroy(tgraph2_);
     for (void *p : allocs_) cudaFree(p);
     if (h_pinned_) cudaFreeHost(h_pinned_);
     if (h_comp_) cudaFreeHost(h_comp_);
@@ -1996,18 +1998,28 @@ Error Solver::alloc_all() {
     Bflux_ = (double *)A((size_t)nd * nc * 8);
     dsum_ = (double *)A(std::max<size_t>(1, nbs) * nb * 8);
     gTb_ = (double *)A(nc * 3 * 8);
-    eb_ = (double *)A(nd * nbs * nb * 8);
+    // the moments and the boundary values in one block (each part padded to
+    // 256 bytes): a direction-sharded solve sums the block over its handles
+    {
+        auto pad = [](size_t n) { return (n + 31) & ~(size_t)31; };
+        const size_t part[7] = {nc, nc, 3 * nc, nb * nc, nc, 6 * nc, nd * nbs * nb};
+        xch_n_ = 0;
+        for (size_t n : part) xch_n_ += pad(n);
+        xch_ = (double *)A(xch_n_ * 8);
+        if (!xch_) return {-6, "device allocation failed (moments)"};
+        double *x = xch_;
+        double **dst[7] = {&Tlat_, &E_, &q_, &Tband_, &Th_, &Q_, &eb_};
+        for (int i = 0; i < 7; i++) {
+            *dst[i] = x;
+            x += pad(part[i]);
+        }
+        CUDA_TRY(cudaMemsetAsync(xch_, 0, xch_n_ * 8, cfg.stream));
+    }
     eb_snap_ = need_snapshot_ ? (double *)A(nd * nbs * nb * 8) : nullptr;
     T_ = (double *)A(nc * 8);
     Told_ = (double *)A(nc * 8);
-    Tlat_ = (double *)A(nc * 8);
-    E_ = (double *)A(nc * 8);
-    q_ = (double *)A(nc * 3 * 8);
     qold_ = (double *)A(nc * 3 * 8);
-    Tband_ = (double *)A(nb * nc * 8);
     remacro_ = (double *)A(nc * 8);
-    Th_ = (double *)A(nc * 8);
-    Q_ = (double *)A(nc * 6 * 8);
     Ths_ = (double *)A(nbs * 8);
     Qs_ = (double *)A(nbs * 6 * 8);
     ThV_ = (double *)A(nslot * 8);
@@ -2476,6 +2488,9 @@ Error Solver::solve_t(SolveStats &st) {
     // direction batches: the gradient, residual and correction buffers hold
     // ndb_ directions (all of them when they fit in device memory)
     const int ndb = ndb_;
+    // this handle's directions: all of them, or its block of a direction shard
+    const int dlo = dlo_, dhi = dhi_ < 0 ? nd : dhi_;
+    const bool sharded = xfn_ != nullptr;
     const int gB = grid_for((size_t)nd * nbs * nb);
     (void)gE;
     const int gC = (nc + kThreads - 1) / kThreads, gN = (nslot + kThreads - 1) / kThreads;
@@ -2587,12 +2602,13 @@ Error Solver::solve_t(SolveStats &st) {
         // transport stage, copy() through the wall temperatures: from the
         // first iteration after the autotuner on, one CUDA graph replayed
         // per iteration (its kernels and arguments do not change)
-        auto transport = [&]() -> Error {
+        // (a sharded solve: the directions, the exchange, the rest)
+        auto transport_dirs = [&]() -> Error {
         // copy() (:2655-2690)
         CUDA_TRY(cudaMemcpyAsync(Told_, T_, nc * 8, cudaMemcpyDeviceToDevice, s));
         CUDA_TRY(cudaMemcpyAsync(qold_, q_, (size_t)nc * 24, cudaMemcpyDeviceToDevice, s));
-        for (int d0 = 0; d0 < nd; d0 += ndb) {
-        const int nbt = std::min(ndb, nd - d0);
+        for (int d0 = dlo; d0 < dhi; d0 += ndb) {
+        const int nbt = std::min(ndb, dhi - d0);
         const size_t nbe = (size_t)nbt * nc * nb;
         ev.gd0 = d0;
         if (nb % 4 == 0) {
@@ -2613,7 +2629,7 @@ Error Solver::solve_t(SolveStats &st) {
             GL(K_RESIDUAL, (k_residual<S, DIM><<<grid_for(nbe), kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, pos_of_, R,
                                                                                   d0, nbt)));
         }
-        if (tune && nt == 0 && d0 == 0) {
+        if (tune && nt == 0 && d0 == dlo) {
             // autotuner: every cap on the bands per CTA that gives a distinct
             // chunking, timed on this iteration's residual (the sweep only
             // reads R and rewrites every correction, so the trials leave no
@@ -2672,10 +2688,18 @@ Error Solver::solve_t(SolveStats &st) {
         GL(K_SWEEP, CUDA_TRY(launch_sweep(SL, d0, nbt)));
         GL(K_MOMENTS, (k_moments<S><<<gM, cpb * nb, msmem, s>>>(dm_, dp_, cpb, eps, (const S *)corr_, Tbase_, wtab_,
                                                                 Tlat_, E_, q_, Tband_, Th_, Q_, 1, d0, nbt,
-                                                                d0 > 0 ? 1 : 0)));
+                                                                d0 > dlo ? 1 : 0)));
         GL(K_BOUND_OUT, (k_bound_out<S, DIM><<<grid_for((size_t)nbt * nbs * nb), kThreads, 0, s>>>(dm_, dp_, ev, eb_, d0,
                                                                                                nbt)));
         }
+        // a shard keeps the boundary values of its own directions only, so
+        // that the exchange's sum is their union (x + 0 = x exactly)
+        if (sharded && dlo > 0) CUDA_TRY(cudaMemsetAsync(eb_, 0, (size_t)dlo * nbs * nb * 8, s));
+        if (sharded && dhi < nd)
+            CUDA_TRY(cudaMemsetAsync(eb_ + (size_t)dhi * nbs * nb, 0, (size_t)(nd - dhi) * nbs * nb * 8, s));
+        return {0, ""};
+        };
+        auto transport_post = [&]() -> Error {
         // the synthetic source and wall temperatures (not in the Sequential
         // scheme, solve_DOM, StaticBTESyntheticSolver.cpp:968-1179)
         if (!cfg.sequential) {
@@ -2688,19 +2712,29 @@ Error Solver::solve_t(SolveStats &st) {
         CUDA_TRY(cudaGetLastError());
         return {0, ""};
         };
+        auto transport = [&]() -> Error {
+            Error te = transport_dirs();
+            if (te.code) return te;
+            return transport_post();
+        };
+        // the moments and boundary values summed over the shard set
+        auto exchange = [&](double *buf, size_t n) -> Error {
+            const int rc = xfn_(xuser_, buf, n, (void *)s);
+            if (rc) return {-9, "direction shard exchange failed (" + std::to_string(rc) + ")"};
+            return {0, ""};
+        };
         const bool graphable = graph_ok_ && !(tune && nt == 0) && !cfg.profile;
-        if (graphable && !tgraph_) {
-            // capture once; any failure leaves the direct launches in place
+        // capture once; any failure leaves the direct launches in place
+        auto capture = [&](const std::function<Error()> &stage, cudaGraphExec_t &gx, long long &nl) {
             cudaGraph_t gr = nullptr;
             const long long l0 = launches_;
             if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-                Error te = transport();
+                Error te = stage();
                 const cudaError_t ce = cudaStreamEndCapture(s, &gr);
-                if (te.code == 0 && ce == cudaSuccess && gr &&
-                    cudaGraphInstantiate(&tgraph_, gr, 0) == cudaSuccess) {
-                    tgraph_launches_ = launches_ - l0;
+                if (te.code == 0 && ce == cudaSuccess && gr && cudaGraphInstantiate(&gx, gr, 0) == cudaSuccess) {
+                    nl = launches_ - l0;
                 } else {
-                    tgraph_ = nullptr;
+                    gx = nullptr;
                     graph_ok_ = false;
                 }
                 if (gr) cudaGraphDestroy(gr);
@@ -2709,12 +2743,27 @@ Error Solver::solve_t(SolveStats &st) {
             }
             launches_ = l0;
             cudaGetLastError();
-        }
-        if (graphable && tgraph_) {
-            CUDA_TRY(cudaGraphLaunch(tgraph_, s));
-            launches_ += tgraph_launches_;
+        };
+        auto run = [&](const std::function<Error()> &stage, cudaGraphExec_t gx, long long nl) -> Error {
+            if (graphable && gx) {
+                CUDA_TRY(cudaGraphLaunch(gx, s));
+                launches_ += nl;
+                return {0, ""};
+            }
+            return stage();
+        };
+        if (!sharded) {
+            if (graphable && !tgraph_) capture(transport, tgraph_, tgraph_launches_);
+            Error te = run(transport, tgraph_, tgraph_launches_);
+            if (te.code) return te;
         } else {
-            Error te = transport();
+            if (graphable && !tgraph_) capture(transport_dirs, tgraph_, tgraph_launches_);
+            if (graphable && graph_ok_ && !tgraph2_) capture(transport_post, tgraph2_, tgraph2_launches_);
+            Error te = run(transport_dirs, tgraph_, tgraph_launches_);
+            if (te.code) return te;
+            te = exchange(xch_, xch_n_);
+            if (te.code) return te;
+            te = run(transport_post, tgraph2_, tgraph2_launches_);
             if (te.code) return te;
         }
         CUDA_TRY(cudaEventRecord(ev_[1], s));
@@ -2773,6 +2822,13 @@ Error Solver::solve_t(SolveStats &st) {
         // margins
         CUDA_TRY(cudaMemsetAsync(red_, 0, 4 * 8 * (size_t)ncomp_, s));
         GL(K_REDUCE, k_margins<<<dim3(comp_blocks, ncomp_), kThreads, 0, s>>>(comp_ptr_d_, T_, Told_, q_, qold_, red_));
+        if (sharded) {
+            // every handle of the shard set takes the margins of the one that
+            // holds direction 0, so that all of them stop at the same iteration
+            if (dlo > 0) CUDA_TRY(cudaMemsetAsync(red_, 0, 4 * 8 * (size_t)ncomp_, s));
+            Error xe = exchange(red_, 4 * (size_t)ncomp_);
+            if (xe.code) return xe;
+        }
         CUDA_TRY(cudaMemcpyAsync(h_comp_, red_, 4 * 8 * (size_t)ncomp_, cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaEventRecord(ev_[3], s));
         CUDA_TRY(cudaStreamSynchronize(s));
@@ -2806,7 +2862,7 @@ Error Solver::solve_t(SolveStats &st) {
         st.err_temp = err;
         st.err_flux = errq;
         st.iterations = nt + 1;
-        st.updates += (long long)nd * nc * nb;
+        st.updates += (long long)(dhi - dlo) * nc * nb;
         if (err <= cfg.err_temp && errq <= cfg.err_flux) {
             converged = true;
             break;
@@ -2853,6 +2909,30 @@ Error Solver::solve(SolveStats &st) {
     }
     if (cfg.precision == 1) return solve_t<float, 3>(st);
     return solve_t<double, 3>(st);
+}
+
+Error Solver::set_shard(int begin, int count, ExchangeFn fn, void *user) {
+    if (!initialised) return {-1, "solver not initialised"};
+    const int nd = ang.nd;
+    if (begin < 0 || count < 0 || begin + count > nd) return {-1, "direction shard outside [0, number of directions)"};
+    CUDA_TRY(cudaSetDevice(cfg.device));
+    CUDA_TRY(cudaStreamSynchronize(cfg.stream));
+    // the captured transport stage covers the old direction range
+    if (tgraph_) cudaGraphExecDestroy(tgraph_);
+    if (tgraph2_) cudaGraphExecDestroy(tgraph2_);
+    tgraph_ = tgraph2_ = nullptr;
+    if (count == 0 || !fn) {
+        dlo_ = 0;
+        dhi_ = -1;
+        xfn_ = nullptr;
+        xuser_ = nullptr;
+        return {0, ""};
+    }
+    dlo_ = begin;
+    dhi_ = begin + count;
+    xfn_ = fn;
+    xuser_ = user;
+    return {0, ""};
 }
 
 Error Solver::get_fields(double *TE, double *TL, double *q, double *TB) {
@@ -3760,6 +3840,7 @@ Error Solver::vjp(const double *Tbar_h, const double *qbar_h, int max_iter, doub
     if (cfg.order != 2 || cfg.sequential || cfg.use_limiter)
         return {-8, "the adjoint is implemented for the second-order Synthetic scheme without limiter only"};
     if (ndb_ < ang.nd) return {-8, "the adjoint needs every direction's buffers resident (direction_batch)"};
+    if (xfn_) return {-8, "the adjoint is not implemented for direction-sharded handles"};
     if (max_iter < 1 || !(tol > 0)) return {-1, "invalid adjoint limits"};
     CUDA_TRY(cudaSetDevice(cfg.device));
     Error e = adj_setup();

@@ -92,6 +92,11 @@ struct CgPlan {
     double *ell_val = nullptr, *diag = nullptr, *ainv = nullptr;
 };
 
+// Sum of `count` doubles of device memory over the handles of a direction
+// shard set, in place, after the work already enqueued on `stream`; the
+// solver enqueues its next work on `stream` once the call returns. 0 = ok.
+typedef int (*ExchangeFn)(void *user, double *buf, size_t count, void *stream);
+
 class Solver {
 public:
     ~Solver();
@@ -111,6 +116,13 @@ public:
     // partially specular walls only)
     Error vjp(const double *Tbar, const double *qbar, int max_iter, double tol, double *g_tau, double *g_cell,
               double *g_bnd, VjpStats &st);
+    // Direction shard: this handle's transport covers directions
+    // [begin, begin + count) only, and every outer iteration sums the moments
+    // and boundary values over the shard set through `fn` (count = 0 or
+    // fn = NULL: all directions, no exchange)
+    Error set_shard(int begin, int count, ExchangeFn fn, void *user);
+    int shard_begin() const { return dlo_; }
+    int shard_end() const { return dhi_ < 0 ? ang.nd : dhi_; }
 
     FlatMesh mesh;
     Bands bands;
@@ -204,6 +216,17 @@ private:
     // cannot be captured)
     cudaGraphExec_t tgraph_ = nullptr;
     long long tgraph_launches_ = 0;
+    // a direction-sharded solve: the stage after the exchange as a second graph
+    cudaGraphExec_t tgraph2_ = nullptr;
+    long long tgraph2_launches_ = 0;
+    // direction shard [dlo_, dhi_) (dhi_ < 0: all directions) and its exchange
+    int dlo_ = 0, dhi_ = -1;
+    ExchangeFn xfn_ = nullptr;
+    void *xuser_ = nullptr;
+    // Tlat, E, q, Tband, Th, Q and the boundary values in one block, the
+    // buffer of the exchange (xch_n_ doubles)
+    double *xch_ = nullptr;
+    size_t xch_n_ = 0;
     bool graph_ok_ = true;
     // adjoint state and scratch (allocated by the first vjp)
     double *adj_lam_ = nullptr, *adj_ebar_ = nullptr, *adj_ebb_ = nullptr, *adj_dbar_ = nullptr;

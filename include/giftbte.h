@@ -41,6 +41,8 @@
 #ifndef GIFTBTE_B200_H
 #define GIFTBTE_B200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -57,6 +59,7 @@ extern "C" {
 #define GBTE_ERR_NOMEM -6        /* device allocation failed */
 #define GBTE_ERR_MESH -7         /* mesh topology error (open face, no periodic partner) */
 #define GBTE_ERR_UNSUPPORTED -8  /* input outside the implemented scope */
+#define GBTE_ERR_EXCHANGE -9     /* the exchange function of a direction shard returned non-zero */
 #define GBTE_ERR_NOT_CONVERGED 1 /* max_iter reached before the margins (not an error) */
 
 /* precision of the band intensities */
@@ -337,6 +340,37 @@ typedef struct {
 
 int gbte_vjp(gbte_handle *h, const double *T_bar, const double *q_bar, int max_iter, double tol, double *grad_tau,
              double *grad_scatter, double *grad_specularity, gbte_vjp_stats *st);
+
+/* Direction sharding of one solve over several handles (one per GPU and
+ * process, or several in one process): the reference's decomposition of the
+ * directions over MPI ranks (StaticBTESynthetic.cpp:247-300), with its
+ * per-iteration MPI_Allreduce of the moments (StaticBTESyntheticSolver.cpp:
+ * 130-136) and MPI_Allgather of the boundary intensities
+ * (StaticBTESynthetic.cpp:2220-2226). Here one sum over a contiguous block
+ * replaces both: every handle zeroes the boundary values of the directions
+ * it does not hold, so the sum of those is their union.
+ *
+ * After the call, the handle's transport stage covers directions
+ * [dir_begin, dir_begin + dir_count) only. Every outer iteration then calls
+ *   exchange(user, buf, count, stream)
+ * twice: once on the moments and boundary values of the iteration, once on
+ * the margins. buf is device memory of `count` doubles; the function must
+ * replace it, in place, by its element-wise sum over all handles of the
+ * shard set (an NCCL all-reduce of ncclDouble/ncclSum on `stream`, a
+ * cudaStream_t, does exactly that), ordered after the work enqueued on
+ * `stream` and before the work enqueued after it returns. It returns 0, or
+ * a non-zero code that makes gbte_solve return GBTE_ERR_EXCHANGE. Every
+ * handle of a set must be created from the same inputs and options, its
+ * blocks must cover every direction exactly once, and all of them must call
+ * gbte_set_initial (or gbte_fourier_initial) and gbte_solve alike: the
+ * margins of the handle holding direction 0 decide for all of them, so
+ * they stop at the same iteration. Fields are the whole solve's on every
+ * handle. dir_count = 0 or exchange = NULL returns to all directions. Not
+ * for gbte_vjp (GBTE_ERR_UNSUPPORTED). No counterpart in the reference
+ * beyond its MPI decomposition. */
+typedef int (*gbte_exchange_fn)(void *user, double *buf, size_t count, void *stream);
+
+int gbte_set_direction_shard(gbte_handle *h, int dir_begin, int dir_count, gbte_exchange_fn exchange, void *user);
 
 /* Turns per-launch kernel timing (options.profile) on or off for the next
  * solves of a handle. While it is on, the transport stage is launched kernel

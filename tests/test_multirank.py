@@ -48,7 +48,7 @@ def _rank_main(rank, world, port, out):
 @pytest.mark.timeout(600)
 def test_two_ranks_reduce_like_the_bench():
     world = 2
-    with mp.Manager() as man:
+    with mp.get_context("spawn").Manager() as man:
         out = man.dict()
         mp.start_processes(_rank_main, args=(world, free_port(), out), nprocs=world, join=True, start_method="spawn")
         res = dict(out)
