@@ -142,7 +142,7 @@ def kernel_algorithmic_bytes(name: str, s: int, dim: int, nb: int, nd: int, nc: 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
 # one ncu --set full capture of each kernel of the third outer iteration on
 # the 17,939-cell 40-band cell, FP32 form, 8 bands per sweep CTA.
-NCU_TRAFFIC_CONFIG2_FP32 = {"residual": 746.86208e6, "sweep": 393.522944e6, "gradient": 509.391616e6,
+NCU_TRAFFIC_CONFIG2_FP32 = {"residual": 747.134464e6, "sweep": 392.428032e6, "gradient": 509.03552e6,
                             "moments": 517.57696e6, "pcg": 1.89568e6}
 
 
@@ -194,7 +194,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     solver = g.StaticBTESynthetic.from_deck(deck, precision=prec, device=local_rank, profile=0,
                                             stream=ctypes_stream(stream), cell_order=args.cell_order,
-                                            sweep_bands=args.sweep_bands)
+                                            sweep_bands=args.sweep_bands, sweep_vector=args.sweep_vector)
     nb, nd = solver.num_bands, solver.num_directions
     upd_per_step = nb * nd * nc
     upd_local = upd_per_step
@@ -277,6 +277,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                        "updates_per_step": upd_per_step, "precision": args.precision,
                        "cell_order": "morton" if args.cell_order == 0 else "deck",
                        "sweep_bands": st.get("sweep_bands"), "sweep_stage_levels": st.get("sweep_stage_levels"),
+                       "sweep_vector": st.get("sweep_vector"), "sweep_threads": st.get("sweep_threads"),
                        "l2": f"band state {upd_per_step * s_bytes / 1e6:.0f} MB per copy, larger than the 126 MB L2",
                        "parallelism": (f"direction shards x{world} of one cell (NCCL all-reduce of the moments and "
                                        "boundary values every outer iteration)" if by_dirs and world > 1 else
@@ -315,7 +316,7 @@ def e2e_solves(args, deck, prec, device, world, shard_rank=None):
     nc = deck.mesh.n_cells
     solver = g.StaticBTESynthetic.from_deck(deck, precision=prec, device=device, max_iter=args.max_iter_e2e,
                                             err_temp=1e-8, err_flux=1e-8, cell_order=args.cell_order,
-                                            sweep_bands=args.sweep_bands)
+                                            sweep_bands=args.sweep_bands, sweep_vector=args.sweep_vector)
     nb = solver.num_bands
     if shard_rank is not None:
         attach_shard(solver, shard_rank, world)
@@ -551,6 +552,7 @@ def run_config5(args, rank: int):
                             "note": "the same cells solved one after another with the plain FP64 form "
                                     "(device time of their outer iterations)"},
         "batch_over_sequential": value / seq, "sweep_bands_autotuned": st.get("sweep_bands"),
+        "sweep_vector_autotuned": st.get("sweep_vector"), "sweep_threads_autotuned": st.get("sweep_threads"),
         "gpu_launches": int(st["kernel_launches"]), "clocks": clk,
     }
 
@@ -569,6 +571,8 @@ def main():
     ap.add_argument("--h-nm", type=float, default=0.0, help="config3 mesh spacing (default 2.5 nm)")
     ap.add_argument("--sweep-bands", type=int, default=0,
                     help="bands per sweep CTA (1..32); 0 lets the autotuner pick on the first iteration")
+    ap.add_argument("--sweep-vector", type=int, choices=[0, 1, 2, 4], default=0,
+                    help="bands per sweep thread; 0 lets the autotuner pick")
     ap.add_argument("--cell-order", type=int, choices=[0, 1], default=0,
                     help="0: cells renumbered along a Morton curve inside the library; 1: the deck's order")
     ap.add_argument("--e2e-steps", type=int, default=2)

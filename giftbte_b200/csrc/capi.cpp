@@ -156,6 +156,9 @@ int create_common(const gbte::RawMesh &raw_in, const gbte::Bands &bands_in, cons
     cfg.order = opt.order == 1 ? 1 : 2;
     cfg.sequential = opt.scheme == 1;
     cfg.macro_exact = opt.macro_exact != 0;
+    if (opt.sweep_vector != 0 && opt.sweep_vector != 1 && opt.sweep_vector != 2 && opt.sweep_vector != 4)
+        return fail(nullptr, {-1, "sweep_vector must be 0 (automatic), 1, 2 or 4"}), GBTE_ERR_ARG;
+    cfg.sweep_vector = opt.sweep_vector;
     cfg.device = opt.device;
     cfg.stream = (cudaStream_t)opt.stream;
     if (opt.precision != GBTE_FP64 && opt.precision != GBTE_FP32_MIXED)
@@ -492,6 +495,8 @@ int gbte_solve(gbte_handle *h, gbte_stats *st) {
             st->sweep_bands = (fixed >= 1 && fixed <= 32) ? fixed : h->solver.tuned_sweep_bands_;
             st->direction_batch = h->solver.ndb_;
             st->sweep_stage_levels = h->solver.tuned_sweep_look_;
+            st->sweep_vector = h->solver.last_sweep_vb_;
+            st->sweep_threads = h->solver.last_sweep_threads_;
             for (int k = 0; k < GBTE_NUM_KERNELS && k < gbte::K_NUM; k++) {
                 st->kernel_ms[k] = s.kernel_ms[k];
                 st->kernel_count[k] = s.kernel_count[k];

@@ -496,11 +496,36 @@ static_assert(sizeof(SweepRec<float>) == 48 && sizeof(SweepRec<double>) == 64, "
 __device__ __forceinline__ float sweep_div(float x, float y) { return __fdividef(x, y); }
 __device__ __forceinline__ double sweep_div(double x, double y) { return x / y; }
 
+// VB consecutive bands of one row as one vector access (VB * sizeof(S) <= 16
+// bytes, the address a multiple of VB * sizeof(S))
+template <typename S, int VB> struct VecOf;
+template <> struct VecOf<float, 1> { using T = float; };
+template <> struct VecOf<float, 2> { using T = float2; };
+template <> struct VecOf<float, 4> { using T = float4; };
+template <> struct VecOf<double, 1> { using T = double; };
+template <> struct VecOf<double, 2> { using T = double2; };
+
+template <typename S, int VB>
+__device__ __forceinline__ void vld(const S *p, S (&v)[VB]) {
+    using V = typename VecOf<S, VB>::T;
+    const V x = *reinterpret_cast<const V *>(p);
+    memcpy(v, &x, sizeof(V));
+}
+template <typename S, int VB>
+__device__ __forceinline__ void vst(S *p, const S (&v)[VB]) {
+    using V = typename VecOf<S, VB>::T;
+    V x;
+    memcpy(&x, v, sizeof(V));
+    *reinterpret_cast<V *>(p) = x;
+}
+
 // Level-synchronous upwind sweep: A^-1 R for one direction and a chunk of
-// nbc <= 32 bands per CTA (blockDim = nbc * cells_per_pass). Each thread owns
-// one band (tid % nbc) for the whole sweep, so the per-level overhead (level
-// bounds, record staging, barrier) is shared by nbc bands of every cell.
-// d_c = (R_c - kb sum_j a_j d_j) / (1 + kb sig_c), kb = tau |v| of the band.
+// nbc <= 32 bands per CTA. Each thread owns VB consecutive bands of the chunk
+// (lane tid % (nbc / VB)) for the whole sweep, so the per-level overhead
+// (level bounds, record staging, barrier) is shared by nbc bands of every
+// cell, and the per-cell work (record, upwind positions) by VB bands.
+// d_c = (R_c - kb sum_j a_j d_j) / (1 + kb sig_c), kb = tau |v| of the band,
+// the same operations in the same order for every VB.
 // Records and residuals are in level order, so a level's operands are
 // contiguous: they are staged into shared memory LOOK-1 levels ahead with
 // cp.async. Every correction is stored in cell order, Dc[d][cell][b], for
@@ -515,8 +540,10 @@ __device__ __forceinline__ double sweep_div(double x, double y) { return x / y; 
 //   bounds [max_lev + 1] i32.
 // Levels longer than LCAP read their overflow records from global memory.
 // rvec: the band chunk of a residual row is copied in 16-byte pieces (its
-// byte size, offset and the row pitch are multiples of 16).
-template <typename S, int LOOK, int LCAP>
+// byte size, offset and the row pitch are multiples of 16). VB > 1 needs nb
+// and nbc to be multiples of VB (every vector access then stays aligned) and
+// blockDim a multiple of nbc / VB.
+template <typename S, int LOOK, int LCAP, int VB = 1>
 __global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int ncomp, int d0, int nbc, int ring_n, int nfar, int rvec,
                                                const int *__restrict__ lvl_ptr, const int *__restrict__ dir_lvl_off,
                                                const SweepRec<S> *__restrict__ rec, const int *__restrict__ lvl_cells,
@@ -539,9 +566,13 @@ __global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int ncomp, int d0
     const int nlev = dir_lvl_off[ent + 1] - dir_lvl_off[ent] - 1;
     const size_t base = (size_t)d * nc, lbase = (size_t)dl * nc;
     const int tid = threadIdx.x, bd = blockDim.x;
-    const int lb = tid % nbc, lc0 = tid / nbc, cpp = bd / nbc;  // band of this thread, cell offset, cells per pass
+    const int lpc = nbc / VB;  // threads per cell
+    // first band of this thread (within the chunk), cell offset, cells per pass
+    const int lb = (tid % lpc) * VB, lc0 = tid / lpc, cpp = bd / lpc;
     const bool band_ok = lb < nbl;
-    const S kb = band_ok ? (S)kbv[b0 + lb] : (S)0;
+    S kb[VB];
+#pragma unroll
+    for (int v = 0; v < VB; v++) kb[v] = band_ok ? (S)kbv[b0 + lb + v] : (S)0;
     const int mask = ring_n - 1;
     // residual staging: each cell's band chunk is K pieces of `unit` bytes;
     // thread tid copies piece rk of cells rc0, rc0 + rstep, ...
@@ -584,26 +615,92 @@ __global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int ncomp, int d0
             const size_t P = base + c0 + li, L = lbase + c0 + li;
             const bool st = li < LCAP;
             const SweepRec<S> r = st ? srec[li] : rec[P];
-            const S r0 = st ? sR[li * nbc + lb] : Rlo[L * nb + b0 + lb];
+            S r0[VB];
+            vld<S, VB>(st ? sR + li * nbc + lb : Rlo + L * nb + b0 + lb, r0);
             const int nin = r.meta & 7, fw = (r.meta >> 3) - 1;
-            S sum = (S)0;
+            S sum[VB];
+#pragma unroll
+            for (int v = 0; v < VB; v++) sum[v] = (S)0;
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const int q = r.np[j];
                 if (j < nin) {
-                    const S dj = q >= lo  ? ring[(q & mask) * nbc + lb]
-                                 : q < 0 ? far[(-1 - q) * nbc + lb]
-                                         : Dc[(lbase + lvl_cells[base + q]) * nb + b0 + lb];
-                    sum += r.a[j] * dj;
+                    S dj[VB];
+                    if (q >= lo)
+                        vld<S, VB>(ring + (q & mask) * nbc + lb, dj);
+                    else if (q < 0)
+                        vld<S, VB>(far + (-1 - q) * nbc + lb, dj);
+                    else
+                        vld<S, VB>(Dc + (lbase + lvl_cells[base + q]) * nb + b0 + lb, dj);
+#pragma unroll
+                    for (int v = 0; v < VB; v++) sum[v] += r.a[j] * dj[v];
                 }
             }
-            const S dl = sweep_div(r0 - kb * sum, (S)1 + kb * r.sig);
-            Dc[(lbase + r.cell) * nb + b0 + lb] = dl;
-            if (fw >= 0) far[fw * nbc + lb] = dl;
-            ring[((c0 + li) & mask) * nbc + lb] = dl;
+            S dv[VB];
+#pragma unroll
+            for (int v = 0; v < VB; v++) dv[v] = sweep_div(r0[v] - kb[v] * sum[v], (S)1 + kb[v] * r.sig);
+            vst<S, VB>(Dc + (lbase + r.cell) * nb + b0 + lb, dv);
+            if (fw >= 0) vst<S, VB>(far + fw * nbc + lb, dv);
+            vst<S, VB>(ring + ((c0 + li) & mask) * nbc + lb, dv);
         }
     }
     cp_async_wait<0>();
+}
+
+template <typename S, int LOOK, int LCAP, int VB>
+cudaError_t sweep_launch_t(int blocks, int threads, size_t smem, cudaStream_t s, int nb, int nc, int ncomp, int d0,
+                           int nbc, int ring, int nfar, int rvec, const int *lvl_ptr, const int *dir_lvl_off,
+                           const SweepRec<S> *rec, const int *lvl_cells, const double *kb, const S *R, S *Dc) {
+    k_sweep<S, LOOK, LCAP, VB><<<blocks, threads, smem, s>>>(nb, nc, ncomp, d0, nbc, ring, nfar, rvec, lvl_ptr,
+                                                             dir_lvl_off, rec, lvl_cells, kb, R, Dc);
+    return cudaGetLastError();
+}
+
+// k_sweep for a runtime staging depth (2..4) and bands per thread (1, 2; 4
+// in FP32)
+template <typename S, int LCAP>
+cudaError_t sweep_dispatch(int look, int vb, int blocks, int threads, size_t smem, cudaStream_t s, int nb, int nc,
+                           int ncomp, int d0, int nbc, int ring, int nfar, int rvec, const int *lvl_ptr,
+                           const int *dir_lvl_off, const SweepRec<S> *rec, const int *lvl_cells, const double *kb,
+                           const S *R, S *Dc) {
+#define GBTE_SWEEP_CASE(LK, V)                                                                                       \
+    if (look == LK && vb == V)                                                                                        \
+        return sweep_launch_t<S, LK, LCAP, V>(blocks, threads, smem, s, nb, nc, ncomp, d0, nbc, ring, nfar, rvec,     \
+                                              lvl_ptr, dir_lvl_off, rec, lvl_cells, kb, R, Dc);
+    GBTE_SWEEP_CASE(2, 1)
+    GBTE_SWEEP_CASE(3, 1)
+    GBTE_SWEEP_CASE(4, 1)
+    GBTE_SWEEP_CASE(2, 2)
+    GBTE_SWEEP_CASE(3, 2)
+    GBTE_SWEEP_CASE(4, 2)
+    if constexpr (sizeof(S) == 4) {
+        GBTE_SWEEP_CASE(2, 4)
+        GBTE_SWEEP_CASE(3, 4)
+        GBTE_SWEEP_CASE(4, 4)
+    }
+#undef GBTE_SWEEP_CASE
+    return cudaErrorInvalidValue;
+}
+
+// the dynamic shared-memory limit of every k_sweep that sweep_dispatch launches
+template <typename S, int LCAP>
+cudaError_t sweep_set_smem(int bytes) {
+    const void *fns[] = {(const void *)k_sweep<S, 2, LCAP, 1>, (const void *)k_sweep<S, 3, LCAP, 1>,
+                         (const void *)k_sweep<S, 4, LCAP, 1>, (const void *)k_sweep<S, 2, LCAP, 2>,
+                         (const void *)k_sweep<S, 3, LCAP, 2>, (const void *)k_sweep<S, 4, LCAP, 2>};
+    for (const void *f : fns) {
+        const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return e;
+    }
+    if constexpr (sizeof(S) == 4) {
+        const void *f4[] = {(const void *)k_sweep<S, 2, LCAP, 4>, (const void *)k_sweep<S, 3, LCAP, 4>,
+                            (const void *)k_sweep<S, 4, LCAP, 4>};
+        for (const void *f : f4) {
+            const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
 }
 
 // e += d (the sweep's corrections, cell order) fused with the moments, one
@@ -2501,24 +2598,30 @@ Error Solver::solve_t(SolveStats &st) {
     // equal chunks of at most `cap` bands; the ring holds at least one whole
     // level (distinct slots for the cells written in one level) and 512
     // positions or more; more chunks when that does not fit in shared memory.
-    // look = levels staged in shared memory (2..4: 1..3 levels of prefetch)
+    // look = levels staged in shared memory (2..4: 1..3 levels of prefetch);
+    // vb = bands per thread (1, 2, 4; chunks a multiple of vb bands);
+    // threads = a multiple of the threads per cell, nbc / vb, up to `tmax`
     struct SweepLaunch {
-        int nbc = 0, chunks = 0, threads = 0, blocks = 0, rvec = 0, look = 4;
+        int nbc = 0, chunks = 0, threads = 0, blocks = 0, rvec = 0, look = 4, vb = 1;
         size_t smem = 0;
     };
     const size_t wlp = ((size_t)(sched.max_levels + 1) * sizeof(int) + 15) & ~(size_t)15;
-    auto sweep_launch = [&](int wcap, SweepLaunch &L, int look) -> bool {
+    auto sweep_launch = [&](int wcap, SweepLaunch &L, int look, int vb = 1, int tmax = 256) -> bool {
         L.look = look;
+        L.vb = vb;
+        if (vb != 1 && (nb % vb != 0 || vb * (int)sizeof(S) > 16)) return false;
         for (int cap = wcap; cap >= 1; cap--) {
             L.nbc = (nb + (nb + cap - 1) / cap - 1) / ((nb + cap - 1) / cap);  // equal chunks of <= cap bands
+            L.nbc = (L.nbc + vb - 1) / vb * vb;                                // ... rounded up to vb bands
             L.chunks = (nb + L.nbc - 1) / L.nbc;                               // every chunk non-empty
             const size_t slot = (size_t)LCAP * sizeof(SweepRec<S>) + (((size_t)LCAP * L.nbc * sizeof(S) + 15) & ~(size_t)15);
             L.smem = look * slot + (((size_t)ring_ * L.nbc * sizeof(S) + 15) & ~(size_t)15) +
                      (((size_t)far_slots_ * L.nbc * sizeof(S) + 15) & ~(size_t)15) + wlp;
-            if (L.smem <= 220 * 1024 || L.nbc == 1) break;
+            if (L.smem <= 220 * 1024 || L.nbc <= vb) break;
         }
-        if (L.smem > 220 * 1024) return false;
-        L.threads = std::max(L.nbc, (256 / L.nbc) * L.nbc);
+        if (L.smem > 220 * 1024 || L.nbc > 32) return false;
+        const int lpc = L.nbc / vb;
+        L.threads = std::max(lpc, (std::min(256, tmax) / lpc) * lpc);
         L.blocks = nd * ncomp_ * L.chunks;
         const int last = nb - (L.chunks - 1) * L.nbc;  // bands of the last chunk
         L.rvec = ((L.nbc * sizeof(S)) % 16 == 0 && (nb * sizeof(S)) % 16 == 0 && (last * sizeof(S)) % 16 == 0) ? 1 : 0;
@@ -2526,32 +2629,28 @@ Error Solver::solve_t(SolveStats &st) {
     };
     // every sweep launch stays within 220 KB of dynamic shared memory: the
     // limit is raised once, outside any stream capture
-    CUDA_TRY(cudaFuncSetAttribute(k_sweep<S, 4, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-    CUDA_TRY(cudaFuncSetAttribute(k_sweep<S, 3, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-    CUDA_TRY(cudaFuncSetAttribute(k_sweep<S, 2, LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+    CUDA_TRY((sweep_set_smem<S, LCAP>(220 * 1024)));
     auto launch_sweep = [&](const SweepLaunch &L, int d0, int nbt) -> cudaError_t {
         const int blocks = nbt * ncomp_ * L.chunks;
-        const auto *rc = (const SweepRec<S> *)rec_;
-        if (L.look == 2)
-            k_sweep<S, 2, LCAP><<<blocks, L.threads, L.smem, s>>>(nb, nc, ncomp_, d0, L.nbc, ring_, far_slots_, L.rvec,
-                                                                  lvl_ptr_, dir_lvl_off_, rc, lvl_cells_, kb_, R, (S *)corr_);
-        else if (L.look == 3)
-            k_sweep<S, 3, LCAP><<<blocks, L.threads, L.smem, s>>>(nb, nc, ncomp_, d0, L.nbc, ring_, far_slots_, L.rvec,
-                                                                  lvl_ptr_, dir_lvl_off_, rc, lvl_cells_, kb_, R, (S *)corr_);
-        else
-            k_sweep<S, 4, LCAP><<<blocks, L.threads, L.smem, s>>>(nb, nc, ncomp_, d0, L.nbc, ring_, far_slots_, L.rvec,
-                                                                  lvl_ptr_, dir_lvl_off_, rc, lvl_cells_, kb_, R, (S *)corr_);
-        return cudaGetLastError();
+        return sweep_dispatch<S, LCAP>(L.look, L.vb, blocks, L.threads, L.smem, s, nb, nc, ncomp_, d0, L.nbc, ring_,
+                                       far_slots_, L.rvec, lvl_ptr_, dir_lvl_off_, (const SweepRec<S> *)rec_,
+                                       lvl_cells_, kb_, R, (S *)corr_);
     };
-    // a fixed cap (options.sweep_bands), or the one the autotuner picked
-    // on this handle's first outer iteration (8 in FP32, 4 in FP64 before)
-    const bool tune = (cfg.sweep_bands < 1 || cfg.sweep_bands > 32) && tuned_sweep_bands_ == 0;
-    int wcap = (cfg.sweep_bands >= 1 && cfg.sweep_bands <= 32) ? cfg.sweep_bands
-               : tuned_sweep_bands_ > 0                         ? tuned_sweep_bands_
-                                                                : (sizeof(S) == 4 ? 8 : 4);
+    // a fixed cap (options.sweep_bands) and bands per thread
+    // (options.sweep_vector), or the ones the autotuner picked on this
+    // handle's first outer iteration (8 bands, 1 per thread, in FP32 and 4 in
+    // FP64 before)
+    const bool fixed_cap = cfg.sweep_bands >= 1 && cfg.sweep_bands <= 32;
+    const bool fixed_vb = cfg.sweep_vector == 1 || cfg.sweep_vector == 2 || cfg.sweep_vector == 4;
+    const bool tune = !(fixed_cap && fixed_vb) && tuned_sweep_bands_ == 0;
+    int wcap = fixed_cap ? cfg.sweep_bands : tuned_sweep_bands_ > 0 ? tuned_sweep_bands_ : (sizeof(S) == 4 ? 8 : 4);
+    int wvb = fixed_vb ? cfg.sweep_vector : tuned_sweep_bands_ > 0 ? tuned_sweep_vb_ : 1;
     SweepLaunch SL;
-    if (!sweep_launch(wcap, SL, tuned_sweep_look_))
+    if (!sweep_launch(wcap, SL, tuned_sweep_look_, wvb, tuned_sweep_threads_) &&
+        !sweep_launch(wcap, SL, tuned_sweep_look_, 1, tuned_sweep_threads_))
         return {-8, "sweep level too wide for the shared-memory correction ring"};
+    last_sweep_vb_ = SL.vb;
+    last_sweep_threads_ = SL.threads;
     const int cpb = std::max(1, 256 / nb);
     const int gM = (nc + cpb - 1) / cpb;
     const size_t msmem = ((size_t)nd * kWTab + (size_t)cpb * nb * kMomSlots) * sizeof(double);
@@ -2653,23 +2752,50 @@ Error Solver::solve_t(SolveStats &st) {
                 }
                 return {0, ""};
             };
-            // the band cap at four staged levels, then fewer staged levels
-            // (less shared memory, more resident CTAs) for the best cap
-            for (int cap : {32, 16, 10, 8, 6, 5, 4, 3, 2, 1}) {
+            // the band cap and bands per thread at four staged levels and
+            // 256 threads, then smaller CTAs, then fewer staged levels (less
+            // shared memory, more resident CTAs) for the best of those
+            int best_vb = 1, best_threads = 256;
+            (void)last_nbc;
+            std::vector<long long> seen;
+            const std::vector<int> caps = fixed_cap ? std::vector<int>{wcap}
+                                                    : std::vector<int>{32, 16, 10, 8, 6, 5, 4, 3, 2, 1};
+            for (int cap : caps) {
+                if (cap > nb && !fixed_cap) continue;
+                for (int vb : {1, 2, 4}) {
+                    if (fixed_vb && vb != wvb) continue;
+                    SweepLaunch L;
+                    if (!sweep_launch(cap, L, 4, vb, 256)) continue;
+                    const long long key = (long long)L.nbc * 64 + L.vb;
+                    if (std::find(seen.begin(), seen.end(), key) != seen.end()) continue;
+                    seen.push_back(key);
+                    float ms = 0;
+                    Error te = trial(L, ms);
+                    if (te.code) return te;
+                    if (ms < best) {
+                        best = ms;
+                        best_cap = cap;
+                        best_vb = vb;
+                    }
+                }
+            }
+            for (int tmax : {128, 64}) {
                 SweepLaunch L;
-                if (cap > nb || !sweep_launch(cap, L, 4) || L.nbc == last_nbc) continue;
-                last_nbc = L.nbc;
+                if (!sweep_launch(best_cap, L, 4, best_vb, tmax)) continue;
+                SweepLaunch L256;
+                sweep_launch(best_cap, L256, 4, best_vb, 256);
+                if (L.threads == L256.threads) continue;
                 float ms = 0;
                 Error te = trial(L, ms);
                 if (te.code) return te;
                 if (ms < best) {
                     best = ms;
-                    best_cap = cap;
+                    best_threads = tmax;
                 }
             }
             for (int look : {3, 2}) {
                 SweepLaunch L;
-                if (!sweep_launch(best_cap, L, look)) continue;
+                if (!sweep_launch(best_cap, L, look, best_vb, best_threads)) continue;
                 float ms = 0;
                 Error te = trial(L, ms);
                 if (te.code) return te;
@@ -2682,8 +2808,12 @@ Error Solver::solve_t(SolveStats &st) {
             cudaEventDestroy(t1);
             tuned_sweep_bands_ = best_cap;
             tuned_sweep_look_ = best_look;
+            tuned_sweep_vb_ = best_vb;
+            tuned_sweep_threads_ = best_threads;
             wcap = best_cap;
-            sweep_launch(wcap, SL, best_look);
+            sweep_launch(wcap, SL, best_look, best_vb, best_threads);
+            last_sweep_vb_ = SL.vb;
+            last_sweep_threads_ = SL.threads;
         }
         GL(K_SWEEP, CUDA_TRY(launch_sweep(SL, d0, nbt)));
         GL(K_MOMENTS, (k_moments<S><<<gM, cpb * nb, msmem, s>>>(dm_, dp_, cpb, eps, (const S *)corr_, Tbase_, wtab_,

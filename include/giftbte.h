@@ -157,6 +157,9 @@ typedef struct {
                                  reference's step by step; 0 (default): a solve warm-started from the
                                  previous outer iteration stops after a 3e-3 residual reduction (same
                                  fixed point, fewer CG iterations) */
+    int sweep_vector;         /* bands each thread of the upwind sweep updates (1, 2, or 4 in FP32;
+                                 the band count must be a multiple); 0 = automatic. Results do not
+                                 depend on it. */
 } gbte_options;
 
 #define GBTE_NUM_KERNELS 16
@@ -184,6 +187,8 @@ typedef struct {
                                  the autotuner's pick on the handle's first outer iteration) */
     int direction_batch;      /* directions per batch of the transport stage */
     int sweep_stage_levels;   /* levels the sweep stages ahead in shared memory (autotuned, 2..4) */
+    int sweep_vector;         /* bands per sweep thread in use (options.sweep_vector or autotuned) */
+    int sweep_threads;        /* threads per sweep CTA in use */
 } gbte_stats;
 
 /* Name of kernel slot i of gbte_stats.kernel_ms (NULL past the last one). */

@@ -1,0 +1,63 @@
+"""GPU: bands per sweep thread (options.sweep_vector). Each thread of the
+upwind sweep updates 1, 2 or 4 consecutive bands of a cell with vector
+accesses; every band's arithmetic is the same, in the same order, so the
+fields are bit-identical whichever width runs. A width the band count does
+not divide falls back to one band per thread."""
+import numpy as np
+import pytest
+
+import giftbte_b200 as g
+import make_golden as mg
+from giftbte_b200 import decks
+
+pytestmark = pytest.mark.gpu
+
+
+def run(deck, prec, vb, bands=8, iters=15, batch=False):
+    kw = dict(precision=prec, sweep_bands=bands, sweep_vector=vb)
+    s = g.StaticBTESynthetic.from_decks(deck, **kw) if batch else g.StaticBTESynthetic.from_deck(deck, **kw)
+    st = s.solve(max_iter=iters, err_temp=0.0, err_flux=0.0)
+    f = s.fields()
+    s.close()
+    return f, st
+
+
+@pytest.mark.parametrize("prec,widths", [(g.GBTE_FP32_MIXED, (2, 4)), (g.GBTE_FP64, (2,))])
+def test_widths_are_bit_identical(prec, widths):
+    d = decks.config2_deck(h_nm=6.0, n_bands=16, n_phi=8, seed=2)
+    f1, s1 = run(d, prec, 1)
+    assert s1["sweep_vector"] == 1
+    for vb in widths:
+        for bands in (8, 16):
+            fv, sv = run(d, prec, vb, bands=bands)
+            assert sv["sweep_vector"] == vb and sv["sweep_bands"] == bands
+            for k in ("T", "E", "q", "Tband"):
+                assert np.array_equal(f1[k], fv[k]), (vb, bands, k)
+
+
+def test_batch_widths_are_bit_identical():
+    pop = decks.porous_population(3, seed=1, h_nm=(15.0, 22.0), r_nm=(40.0, 80.0), n_bands=8, n_phi=2)
+    f1, _ = run(pop, g.GBTE_FP32_MIXED, 1, batch=True)
+    f4, s4 = run(pop, g.GBTE_FP32_MIXED, 4, batch=True)
+    assert s4["sweep_vector"] == 4
+    assert np.array_equal(f1["T"], f4["T"])
+
+
+def test_width_that_does_not_divide_the_bands_falls_back():
+    deck, ref = mg.load("gray_square_tri")  # one band
+    s = g.StaticBTESynthetic.from_deck(deck, precision=g.GBTE_FP64, sweep_vector=2)
+    s.set_initial(ref["Tf"])
+    st = s.solve(allow_not_converged=False)
+    assert st["sweep_vector"] == 1
+    assert float(np.max(np.abs(s.fields()["T"] - ref["T"])) / np.max(np.abs(ref["T"]))) <= 1e-9
+    s.close()
+
+
+def test_autotuner_reports_its_pick():
+    d = decks.config2_deck(h_nm=6.0, n_bands=16, n_phi=8, seed=2)
+    s = g.StaticBTESynthetic.from_deck(d, precision=g.GBTE_FP32_MIXED)
+    st = s.solve(max_iter=3, err_temp=0.0, err_flux=0.0)
+    assert st["sweep_vector"] in (1, 2, 4)
+    assert 1 <= st["sweep_bands"] <= 16
+    assert 1 <= st["sweep_threads"] <= 256
+    s.close()
