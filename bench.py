@@ -194,7 +194,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     solver = g.StaticBTESynthetic.from_deck(deck, precision=prec, device=local_rank, profile=0,
                                             stream=ctypes_stream(stream), cell_order=args.cell_order,
-                                            sweep_bands=args.sweep_bands, sweep_vector=args.sweep_vector)
+                                            sweep_bands=args.sweep_bands, sweep_vector=args.sweep_vector,
+                                            sweep_kernel=args.sweep_kernel)
     nb, nd = solver.num_bands, solver.num_directions
     upd_per_step = nb * nd * nc
     upd_local = upd_per_step
@@ -278,6 +279,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                        "cell_order": "morton" if args.cell_order == 0 else "deck",
                        "sweep_bands": st.get("sweep_bands"), "sweep_stage_levels": st.get("sweep_stage_levels"),
                        "sweep_vector": st.get("sweep_vector"), "sweep_threads": st.get("sweep_threads"),
+                       "sweep_kernel": {1: "block", 2: "warp"}.get(st.get("sweep_kernel")),
                        "l2": f"band state {upd_per_step * s_bytes / 1e6:.0f} MB per copy, larger than the 126 MB L2",
                        "parallelism": (f"direction shards x{world} of one cell (NCCL all-reduce of the moments and "
                                        "boundary values every outer iteration)" if by_dirs and world > 1 else
@@ -316,7 +318,8 @@ def e2e_solves(args, deck, prec, device, world, shard_rank=None):
     nc = deck.mesh.n_cells
     solver = g.StaticBTESynthetic.from_deck(deck, precision=prec, device=device, max_iter=args.max_iter_e2e,
                                             err_temp=1e-8, err_flux=1e-8, cell_order=args.cell_order,
-                                            sweep_bands=args.sweep_bands, sweep_vector=args.sweep_vector)
+                                            sweep_bands=args.sweep_bands, sweep_vector=args.sweep_vector,
+                                            sweep_kernel=args.sweep_kernel)
     nb = solver.num_bands
     if shard_rank is not None:
         attach_shard(solver, shard_rank, world)
@@ -553,6 +556,7 @@ def run_config5(args, rank: int):
                                     "(device time of their outer iterations)"},
         "batch_over_sequential": value / seq, "sweep_bands_autotuned": st.get("sweep_bands"),
         "sweep_vector_autotuned": st.get("sweep_vector"), "sweep_threads_autotuned": st.get("sweep_threads"),
+        "sweep_kernel_autotuned": {1: "block", 2: "warp"}.get(st.get("sweep_kernel")),
         "gpu_launches": int(st["kernel_launches"]), "clocks": clk,
     }
 
@@ -573,6 +577,8 @@ def main():
                     help="bands per sweep CTA (1..32); 0 lets the autotuner pick on the first iteration")
     ap.add_argument("--sweep-vector", type=int, choices=[0, 1, 2, 4], default=0,
                     help="bands per sweep thread; 0 lets the autotuner pick")
+    ap.add_argument("--sweep-kernel", type=int, choices=[0, 1, 2], default=0,
+                    help="1: block sweep kernel, 2: warp-independent kernel, 0: the autotuner's pick")
     ap.add_argument("--cell-order", type=int, choices=[0, 1], default=0,
                     help="0: cells renumbered along a Morton curve inside the library; 1: the deck's order")
     ap.add_argument("--e2e-steps", type=int, default=2)

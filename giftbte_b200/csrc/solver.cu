@@ -647,6 +647,161 @@ __global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int ncomp, int d0
     cp_async_wait<0>();
 }
 
+// Warp-independent form of the same sweep: one warp per (direction, group of
+// VB consecutive bands), lanes over the cells of a level. A warp's ring and
+// far slots hold only its own bands, so every correction is written and read
+// by the same warp, and a level needs __syncwarp only: no warp waits for
+// another. Each warp stages its own copy of the level's records (the copies
+// of one direction meet in L2) and its own VB-band residual pieces, LOOK-1
+// levels ahead with cp.async. Shared memory per warp (wsmem bytes):
+//   LOOK slots of { SweepRec[LCAP], R[LCAP][VB] S }, the ring [ring_n][VB] S,
+//   the far slots [nfar][VB] S, the level bounds [max_lev + 1] i32.
+// Warps past nwarps exit at once (no block barrier anywhere). Needs nb a
+// multiple of VB and VB * sizeof(S) a cp.async size (4, 8 or 16 bytes).
+template <typename S, int LOOK, int LCAP, int VB>
+__global__ void __launch_bounds__(128) k_sweep_w(int nb, int nc, int ncomp, int d0, int nwarps, int ring_n, int nfar,
+                                                 int wsmem, const int *__restrict__ lvl_ptr,
+                                                 const int *__restrict__ dir_lvl_off, const SweepRec<S> *__restrict__ rec,
+                                                 const int *__restrict__ lvl_cells, const double *__restrict__ kbv,
+                                                 const S *__restrict__ Rlo, S *__restrict__ Dc) {
+    extern __shared__ __align__(16) unsigned char wsm[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int gw = blockIdx.x * (blockDim.x >> 5) + wib;
+    if (gw >= nwarps) return;
+    constexpr int RB = VB * (int)sizeof(S);  // bytes of a residual piece
+    const size_t rbytes = ((size_t)LCAP * RB + 15) & ~(size_t)15;
+    const size_t slot_bytes = (size_t)LCAP * sizeof(SweepRec<S>) + rbytes;
+    unsigned char *my = wsm + (size_t)wib * wsmem;
+    S *ring = reinterpret_cast<S *>(my + LOOK * slot_bytes);
+    S *far = reinterpret_cast<S *>(my + LOOK * slot_bytes + (((size_t)ring_n * RB + 15) & ~(size_t)15));
+    int *lp = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(far) + (((size_t)nfar * RB + 15) & ~(size_t)15));
+    const int ngroups = nb / VB;
+    const int entl = gw / ngroups, grp = gw % ngroups;
+    const int dl = entl / ncomp, d = d0 + dl, ent = d * ncomp + entl % ncomp;
+    const int b0 = grp * VB;
+    const int nlev = dir_lvl_off[ent + 1] - dir_lvl_off[ent] - 1;
+    const size_t base = (size_t)d * nc, lbase = (size_t)dl * nc;
+    S kb[VB];
+#pragma unroll
+    for (int v = 0; v < VB; v++) kb[v] = (S)kbv[b0 + v];
+    const int mask = ring_n - 1;
+    for (int i = lane; i <= nlev; i += 32) lp[i] = lvl_ptr[dir_lvl_off[ent] + i];
+    __syncwarp();
+    auto issue = [&](int l) {
+        if (l >= nlev) return;
+        unsigned char *slot = my + (l % LOOK) * slot_bytes;
+        const int c0 = lp[l], n = min(lp[l + 1] - c0, LCAP);
+        const unsigned char *src = reinterpret_cast<const unsigned char *>(rec + base + c0);
+        const int npieces = n * (int)(sizeof(SweepRec<S>) / 16);
+        for (int i = lane; i < npieces; i += 32) cp_async(slot + 16 * i, src + 16 * i, 16);
+        unsigned char *sR = slot + (size_t)LCAP * sizeof(SweepRec<S>);
+        for (int ci = lane; ci < n; ci += 32) cp_async(sR + (size_t)ci * RB, Rlo + (lbase + c0 + ci) * nb + b0, RB);
+    };
+#pragma unroll
+    for (int k = 0; k < LOOK - 1; k++) {
+        issue(k);
+        cp_async_commit();
+    }
+    for (int l = 0; l < nlev; l++) {
+        cp_async_wait<LOOK - 2>();
+        __syncwarp();
+        issue(l + LOOK - 1);
+        cp_async_commit();
+        const unsigned char *slot = my + (l % LOOK) * slot_bytes;
+        const SweepRec<S> *srec = reinterpret_cast<const SweepRec<S> *>(slot);
+        const S *sR = reinterpret_cast<const S *>(slot + (size_t)LCAP * sizeof(SweepRec<S>));
+        const int c0 = lp[l], c1 = lp[l + 1], n = c1 - c0;
+        const int lo = c1 - ring_n;
+        for (int li = lane; li < n; li += 32) {
+            const size_t P = base + c0 + li, L = lbase + c0 + li;
+            const bool st = li < LCAP;
+            const SweepRec<S> r = st ? srec[li] : rec[P];
+            S r0[VB];
+            vld<S, VB>(st ? sR + li * VB : Rlo + L * nb + b0, r0);
+            const int nin = r.meta & 7, fw = (r.meta >> 3) - 1;
+            S sum[VB];
+#pragma unroll
+            for (int v = 0; v < VB; v++) sum[v] = (S)0;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int q = r.np[j];
+                if (j < nin) {
+                    S dj[VB];
+                    if (q >= lo)
+                        vld<S, VB>(ring + (q & mask) * VB, dj);
+                    else if (q < 0)
+                        vld<S, VB>(far + (-1 - q) * VB, dj);
+                    else
+                        vld<S, VB>(Dc + (lbase + lvl_cells[base + q]) * nb + b0, dj);
+#pragma unroll
+                    for (int v = 0; v < VB; v++) sum[v] += r.a[j] * dj[v];
+                }
+            }
+            S dv[VB];
+#pragma unroll
+            for (int v = 0; v < VB; v++) dv[v] = sweep_div(r0[v] - kb[v] * sum[v], (S)1 + kb[v] * r.sig);
+            vst<S, VB>(Dc + (lbase + r.cell) * nb + b0, dv);
+            if (fw >= 0) vst<S, VB>(far + fw * VB, dv);
+            vst<S, VB>(ring + ((c0 + li) & mask) * VB, dv);
+        }
+    }
+    cp_async_wait<0>();
+}
+
+template <typename S, int LOOK, int LCAP, int VB>
+cudaError_t sweep_w_launch_t(int blocks, int threads, size_t smem, cudaStream_t s, int nb, int nc, int ncomp, int d0,
+                             int nwarps, int ring, int nfar, int wsmem, const int *lvl_ptr, const int *dir_lvl_off,
+                             const SweepRec<S> *rec, const int *lvl_cells, const double *kb, const S *R, S *Dc) {
+    k_sweep_w<S, LOOK, LCAP, VB><<<blocks, threads, smem, s>>>(nb, nc, ncomp, d0, nwarps, ring, nfar, wsmem, lvl_ptr,
+                                                               dir_lvl_off, rec, lvl_cells, kb, R, Dc);
+    return cudaGetLastError();
+}
+
+// k_sweep_w for a runtime staging depth (2..4) and bands per warp (1, 2; 4 in FP32)
+template <typename S, int LCAP>
+cudaError_t sweep_w_dispatch(int look, int vb, int blocks, int threads, size_t smem, cudaStream_t s, int nb, int nc,
+                             int ncomp, int d0, int nwarps, int ring, int nfar, int wsmem, const int *lvl_ptr,
+                             const int *dir_lvl_off, const SweepRec<S> *rec, const int *lvl_cells, const double *kb,
+                             const S *R, S *Dc) {
+#define GBTE_SWEEP_W_CASE(LK, V)                                                                                     \
+    if (look == LK && vb == V)                                                                                        \
+        return sweep_w_launch_t<S, LK, LCAP, V>(blocks, threads, smem, s, nb, nc, ncomp, d0, nwarps, ring, nfar,      \
+                                                wsmem, lvl_ptr, dir_lvl_off, rec, lvl_cells, kb, R, Dc);
+    GBTE_SWEEP_W_CASE(2, 1)
+    GBTE_SWEEP_W_CASE(3, 1)
+    GBTE_SWEEP_W_CASE(4, 1)
+    GBTE_SWEEP_W_CASE(2, 2)
+    GBTE_SWEEP_W_CASE(3, 2)
+    GBTE_SWEEP_W_CASE(4, 2)
+    if constexpr (sizeof(S) == 4) {
+        GBTE_SWEEP_W_CASE(2, 4)
+        GBTE_SWEEP_W_CASE(3, 4)
+        GBTE_SWEEP_W_CASE(4, 4)
+    }
+#undef GBTE_SWEEP_W_CASE
+    return cudaErrorInvalidValue;
+}
+
+template <typename S, int LCAP>
+cudaError_t sweep_w_set_smem(int bytes) {
+    const void *fns[] = {(const void *)k_sweep_w<S, 2, LCAP, 1>, (const void *)k_sweep_w<S, 3, LCAP, 1>,
+                         (const void *)k_sweep_w<S, 4, LCAP, 1>, (const void *)k_sweep_w<S, 2, LCAP, 2>,
+                         (const void *)k_sweep_w<S, 3, LCAP, 2>, (const void *)k_sweep_w<S, 4, LCAP, 2>};
+    for (const void *f : fns) {
+        const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return e;
+    }
+    if constexpr (sizeof(S) == 4) {
+        const void *f4[] = {(const void *)k_sweep_w<S, 2, LCAP, 4>, (const void *)k_sweep_w<S, 3, LCAP, 4>,
+                            (const void *)k_sweep_w<S, 4, LCAP, 4>};
+        for (const void *f : f4) {
+            const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
+}
+
 template <typename S, int LOOK, int LCAP, int VB>
 cudaError_t sweep_launch_t(int blocks, int threads, size_t smem, cudaStream_t s, int nb, int nc, int ncomp, int d0,
                            int nbc, int ring, int nfar, int rvec, const int *lvl_ptr, const int *dir_lvl_off,
@@ -2601,10 +2756,13 @@ Error Solver::solve_t(SolveStats &st) {
     // look = levels staged in shared memory (2..4: 1..3 levels of prefetch);
     // vb = bands per thread (1, 2, 4; chunks a multiple of vb bands);
     // threads = a multiple of the threads per cell, nbc / vb, up to `tmax`
+    // warp = 1: the warp-independent kernel (vb bands per warp, wpc warps
+    // per CTA, wsmem bytes of shared memory per warp)
     struct SweepLaunch {
-        int nbc = 0, chunks = 0, threads = 0, blocks = 0, rvec = 0, look = 4, vb = 1;
-        size_t smem = 0;
+        int nbc = 0, chunks = 0, threads = 0, blocks = 0, rvec = 0, look = 4, vb = 1, warp = 0, wpc = 1;
+        size_t smem = 0, wsmem = 0;
     };
+    constexpr int LCAPW = 64;
     const size_t wlp = ((size_t)(sched.max_levels + 1) * sizeof(int) + 15) & ~(size_t)15;
     auto sweep_launch = [&](int wcap, SweepLaunch &L, int look, int vb = 1, int tmax = 256) -> bool {
         L.look = look;
@@ -2630,7 +2788,34 @@ Error Solver::solve_t(SolveStats &st) {
     // every sweep launch stays within 220 KB of dynamic shared memory: the
     // limit is raised once, outside any stream capture
     CUDA_TRY((sweep_set_smem<S, LCAP>(220 * 1024)));
+    auto sweep_launch_w = [&](SweepLaunch &L, int look, int vb, int wpc) -> bool {
+        if (nb % vb != 0 || vb * (int)sizeof(S) > 16) return false;
+        const size_t rb = (size_t)vb * sizeof(S);
+        const size_t slot = (size_t)LCAPW * sizeof(SweepRec<S>) + (((size_t)LCAPW * rb + 15) & ~(size_t)15);
+        const size_t w = look * slot + (((size_t)ring_ * rb + 15) & ~(size_t)15) +
+                         (((size_t)far_slots_ * rb + 15) & ~(size_t)15) + wlp;
+        if (w * wpc > 220 * 1024) return false;
+        L = SweepLaunch();
+        L.warp = 1;
+        L.look = look;
+        L.vb = vb;
+        L.wpc = wpc;
+        L.wsmem = w;
+        L.smem = w * wpc;
+        L.threads = 32 * wpc;
+        L.nbc = vb;
+        L.chunks = nb / vb;
+        return true;
+    };
+    CUDA_TRY((sweep_w_set_smem<S, LCAPW>(220 * 1024)));
     auto launch_sweep = [&](const SweepLaunch &L, int d0, int nbt) -> cudaError_t {
+        if (L.warp) {
+            const int nwarps = nbt * ncomp_ * (nb / L.vb);
+            return sweep_w_dispatch<S, LCAPW>(L.look, L.vb, (nwarps + L.wpc - 1) / L.wpc, L.threads, L.smem, s, nb, nc,
+                                              ncomp_, d0, nwarps, ring_, far_slots_, (int)L.wsmem, lvl_ptr_,
+                                              dir_lvl_off_, (const SweepRec<S> *)rec_, lvl_cells_, kb_, R,
+                                              (S *)corr_);
+        }
         const int blocks = nbt * ncomp_ * L.chunks;
         return sweep_dispatch<S, LCAP>(L.look, L.vb, blocks, L.threads, L.smem, s, nb, nc, ncomp_, d0, L.nbc, ring_,
                                        far_slots_, L.rvec, lvl_ptr_, dir_lvl_off_, (const SweepRec<S> *)rec_,
@@ -2640,17 +2825,24 @@ Error Solver::solve_t(SolveStats &st) {
     // (options.sweep_vector), or the ones the autotuner picked on this
     // handle's first outer iteration (8 bands, 1 per thread, in FP32 and 4 in
     // FP64 before)
+    // (options.sweep_kernel: 1 = the block kernel, 2 = the warp kernel, 0 =
+    // either, the autotuner's pick)
     const bool fixed_cap = cfg.sweep_bands >= 1 && cfg.sweep_bands <= 32;
     const bool fixed_vb = cfg.sweep_vector == 1 || cfg.sweep_vector == 2 || cfg.sweep_vector == 4;
-    const bool tune = !(fixed_cap && fixed_vb) && tuned_sweep_bands_ == 0;
+    const bool want_warp = cfg.sweep_kernel == 2, want_block = cfg.sweep_kernel == 1;
+    const bool tune = !(fixed_vb && (want_warp || fixed_cap)) && tuned_sweep_bands_ == 0;
     int wcap = fixed_cap ? cfg.sweep_bands : tuned_sweep_bands_ > 0 ? tuned_sweep_bands_ : (sizeof(S) == 4 ? 8 : 4);
     int wvb = fixed_vb ? cfg.sweep_vector : tuned_sweep_bands_ > 0 ? tuned_sweep_vb_ : 1;
     SweepLaunch SL;
-    if (!sweep_launch(wcap, SL, tuned_sweep_look_, wvb, tuned_sweep_threads_) &&
+    const bool use_warp = want_warp || (!want_block && tuned_sweep_bands_ > 0 && tuned_sweep_warp_);
+    if (!(use_warp && (sweep_launch_w(SL, tuned_sweep_look_, wvb, tuned_sweep_wpc_) ||
+                       sweep_launch_w(SL, tuned_sweep_look_, 1, tuned_sweep_wpc_) || sweep_launch_w(SL, 2, 1, 1))) &&
+        !sweep_launch(wcap, SL, tuned_sweep_look_, wvb, tuned_sweep_threads_) &&
         !sweep_launch(wcap, SL, tuned_sweep_look_, 1, tuned_sweep_threads_))
         return {-8, "sweep level too wide for the shared-memory correction ring"};
     last_sweep_vb_ = SL.vb;
     last_sweep_threads_ = SL.threads;
+    last_sweep_warp_ = SL.warp;
     const int cpb = std::max(1, 256 / nb);
     const int gM = (nc + cpb - 1) / cpb;
     const size_t msmem = ((size_t)nd * kWTab + (size_t)cpb * nb * kMomSlots) * sizeof(double);
@@ -2779,7 +2971,29 @@ Error Solver::solve_t(SolveStats &st) {
                     }
                 }
             }
+            // the warp kernel: bands per warp and warps per CTA
+            int best_warp = 0, best_wpc = 1;
+            if (!want_block) {
+                if (want_warp) best = 1e30f;
+                for (int vb : {4, 2, 1}) {
+                    if (fixed_vb && vb != wvb) continue;
+                    for (int wpc : {1, 2, 4}) {
+                        SweepLaunch L;
+                        if (!sweep_launch_w(L, 4, vb, wpc)) continue;
+                        float ms = 0;
+                        Error te = trial(L, ms);
+                        if (te.code) return te;
+                        if (ms < best) {
+                            best = ms;
+                            best_warp = 1;
+                            best_vb = vb;
+                            best_wpc = wpc;
+                        }
+                    }
+                }
+            }
             for (int tmax : {128, 64}) {
+                if (best_warp) break;
                 SweepLaunch L;
                 if (!sweep_launch(best_cap, L, 4, best_vb, tmax)) continue;
                 SweepLaunch L256;
@@ -2795,7 +3009,9 @@ Error Solver::solve_t(SolveStats &st) {
             }
             for (int look : {3, 2}) {
                 SweepLaunch L;
-                if (!sweep_launch(best_cap, L, look, best_vb, best_threads)) continue;
+                if (best_warp ? !sweep_launch_w(L, look, best_vb, best_wpc)
+                              : !sweep_launch(best_cap, L, look, best_vb, best_threads))
+                    continue;
                 float ms = 0;
                 Error te = trial(L, ms);
                 if (te.code) return te;
@@ -2810,10 +3026,14 @@ Error Solver::solve_t(SolveStats &st) {
             tuned_sweep_look_ = best_look;
             tuned_sweep_vb_ = best_vb;
             tuned_sweep_threads_ = best_threads;
+            tuned_sweep_warp_ = best_warp;
+            tuned_sweep_wpc_ = best_wpc;
             wcap = best_cap;
-            sweep_launch(wcap, SL, best_look, best_vb, best_threads);
+            if (!(best_warp && sweep_launch_w(SL, best_look, best_vb, best_wpc)))
+                sweep_launch(wcap, SL, best_look, best_vb, best_threads);
             last_sweep_vb_ = SL.vb;
             last_sweep_threads_ = SL.threads;
+            last_sweep_warp_ = SL.warp;
         }
         GL(K_SWEEP, CUDA_TRY(launch_sweep(SL, d0, nbt)));
         GL(K_MOMENTS, (k_moments<S><<<gM, cpb * nb, msmem, s>>>(dm_, dp_, cpb, eps, (const S *)corr_, Tbase_, wtab_,

@@ -50,6 +50,7 @@ struct SolverConfig {
     int profile = 0;
     int sweep_bands = 0;      // bands per sweep CTA, 0 = automatic
     int sweep_vector = 0;     // bands per sweep thread (1, 2, 4), 0 = automatic
+    int sweep_kernel = 0;     // 1: block sweep kernel, 2: warp-independent kernel, 0 = automatic
     int sweep_far_slots = 0;  // far-slot cap of the sweep plan: 0 = automatic, < 0 = none
     int direction_batch = 0;  // most directions per transport batch, 0 = automatic
     std::vector<double> cell_scatter;  // scattering-rate multiplier s_c per cell (empty: 1)
@@ -136,7 +137,9 @@ public:
     int tuned_sweep_look_ = 4;   // levels the sweep stages in shared memory (the autotuner's pick)
     int tuned_sweep_vb_ = 1;     // bands per sweep thread (the autotuner's pick)
     int tuned_sweep_threads_ = 256;  // most threads per sweep CTA (the autotuner's pick)
-    int last_sweep_vb_ = 0, last_sweep_threads_ = 0;  // launch shape of the last solve's sweep
+    int tuned_sweep_warp_ = 0;   // 1: the warp-independent sweep kernel won (the autotuner's pick)
+    int tuned_sweep_wpc_ = 1;    // warps per CTA of that kernel
+    int last_sweep_vb_ = 0, last_sweep_threads_ = 0, last_sweep_warp_ = 0;  // launch shape of the last solve's sweep
     int ndb_ = 1;                // directions per batch of the gradient/residual/correction buffers
 
 private:

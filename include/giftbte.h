@@ -160,6 +160,10 @@ typedef struct {
     int sweep_vector;         /* bands each thread of the upwind sweep updates (1, 2, or 4 in FP32;
                                  the band count must be a multiple); 0 = automatic. Results do not
                                  depend on it. */
+    int sweep_kernel;         /* 1 = the block sweep (a CTA per direction and chunk of bands, one
+                                 barrier per level), 2 = the warp-independent sweep (a warp per
+                                 direction and sweep_vector bands, no block barrier), 0 = the faster
+                                 of the two on the first outer iteration. Results do not depend on it. */
 } gbte_options;
 
 #define GBTE_NUM_KERNELS 16
@@ -189,6 +193,7 @@ typedef struct {
     int sweep_stage_levels;   /* levels the sweep stages ahead in shared memory (autotuned, 2..4) */
     int sweep_vector;         /* bands per sweep thread in use (options.sweep_vector or autotuned) */
     int sweep_threads;        /* threads per sweep CTA in use */
+    int sweep_kernel;         /* sweep kernel in use: 1 block, 2 warp-independent */
 } gbte_stats;
 
 /* Name of kernel slot i of gbte_stats.kernel_ms (NULL past the last one). */

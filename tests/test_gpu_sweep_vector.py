@@ -1,8 +1,10 @@
-"""GPU: bands per sweep thread (options.sweep_vector). Each thread of the
-upwind sweep updates 1, 2 or 4 consecutive bands of a cell with vector
-accesses; every band's arithmetic is the same, in the same order, so the
-fields are bit-identical whichever width runs. A width the band count does
-not divide falls back to one band per thread."""
+"""GPU: the launch shapes of the upwind sweep. Each thread updates 1, 2 or 4
+consecutive bands of a cell with vector accesses (options.sweep_vector), in
+the block kernel (a CTA per direction and chunk of bands) or the
+warp-independent kernel (a warp per direction and group of bands,
+options.sweep_kernel = 2). Every band's arithmetic is the same, in the same
+order, so the fields are bit-identical whichever shape runs. A width the
+band count does not divide falls back to one band per thread."""
 import numpy as np
 import pytest
 
@@ -13,8 +15,8 @@ from giftbte_b200 import decks
 pytestmark = pytest.mark.gpu
 
 
-def run(deck, prec, vb, bands=8, iters=15, batch=False):
-    kw = dict(precision=prec, sweep_bands=bands, sweep_vector=vb)
+def run(deck, prec, vb, bands=8, iters=15, batch=False, kernel=1):
+    kw = dict(precision=prec, sweep_bands=bands, sweep_vector=vb, sweep_kernel=kernel)
     s = g.StaticBTESynthetic.from_decks(deck, **kw) if batch else g.StaticBTESynthetic.from_deck(deck, **kw)
     st = s.solve(max_iter=iters, err_temp=0.0, err_flux=0.0)
     f = s.fields()
@@ -61,3 +63,30 @@ def test_autotuner_reports_its_pick():
     assert 1 <= st["sweep_bands"] <= 16
     assert 1 <= st["sweep_threads"] <= 256
     s.close()
+
+
+@pytest.mark.parametrize("prec,widths", [(g.GBTE_FP32_MIXED, (1, 2, 4)), (g.GBTE_FP64, (1, 2))])
+def test_warp_kernel_is_bit_identical(prec, widths):
+    d = decks.config2_deck(h_nm=6.0, n_bands=16, n_phi=8, seed=2)
+    f1, _ = run(d, prec, 1)
+    for vb in widths:
+        fw, sw = run(d, prec, vb, kernel=2)
+        assert sw["sweep_kernel"] == 2 and sw["sweep_vector"] == vb
+        for k in ("T", "E", "q", "Tband"):
+            assert np.array_equal(f1[k], fw[k]), (vb, k)
+
+
+def test_warp_kernel_batch_and_golden():
+    pop = decks.porous_population(3, seed=1, h_nm=(15.0, 22.0), r_nm=(40.0, 80.0), n_bands=8, n_phi=2)
+    f1, _ = run(pop, g.GBTE_FP32_MIXED, 1, batch=True)
+    fw, sw = run(pop, g.GBTE_FP32_MIXED, 4, batch=True, kernel=2)
+    assert sw["sweep_kernel"] == 2
+    assert np.array_equal(f1["T"], fw["T"])
+    for case in ("quad_heat_specular", "porous_msh"):
+        deck, ref = mg.load(case)
+        s = g.StaticBTESynthetic.from_deck(deck, precision=g.GBTE_FP64, sweep_kernel=2)
+        s.set_initial(ref["Tf"])
+        st = s.solve(allow_not_converged=False)
+        assert st["sweep_kernel"] == 2
+        assert float(np.max(np.abs(s.fields()["T"] - ref["T"])) / np.max(np.abs(ref["T"]))) <= 1e-9
+        s.close()
