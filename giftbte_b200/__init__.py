@@ -32,6 +32,14 @@ GBTE_FP32_MIXED = 1
 STATUS = {0: "ok", -1: "invalid argument", -2: "input/output error", -3: "CUDA error", -4: "diverged",
           -5: "device wait timed out", -6: "out of memory", -7: "mesh topology error", -8: "unsupported input",
           -9: "direction shard exchange failed", 1: "not converged within max_iter"}
+GBTE_ERR_ARG = -1
+GBTE_ERR_IO = -2
+GBTE_ERR_CUDA = -3
+GBTE_ERR_DIVERGED = -4
+GBTE_ERR_TIMEOUT = -5
+GBTE_ERR_NOMEM = -6
+GBTE_ERR_MESH = -7
+GBTE_ERR_UNSUPPORTED = -8
 GBTE_ERR_EXCHANGE = -9
 
 _c_int_p = ctypes.POINTER(ctypes.c_int)

@@ -59,6 +59,9 @@ namespace gbte {
 namespace {
 
 constexpr int kThreads = 256;
+// reduction slots of the grid-wide CG (k_pcg): scalars of successive
+// iterations, so no slot is reused within one solve
+constexpr int kGridCgSlots = 65536;
 // residual reduction required of a macro CG solve that starts from the
 // previous outer iteration's solution of the same Picard step. It changes
 // the outer iterates, not the fixed point: at 3e-3 every golden deck still
@@ -2708,7 +2711,7 @@ Error Solver::cg_solve(const CgPlan &pl, const int *ptr, const int *idx, const d
         if (sq) *sq = t1 ? h_pinned_[9] : 0.0;
         return {0, ""};
     }
-    int nslots = 65536;
+    int nslots = kGridCgSlots;
     CUDA_TRY(cudaMemsetAsync(scal, 0, nslots * 8, s));
     void *args[] = {&n, (void *)&ptr, (void *)&idx, (void *)&val, (void *)&dinv, (void *)&b, &x, &r, &z, &p, &Ap,
                     &scal, &rtol, &eta, &maxit, &nslots};
@@ -3305,7 +3308,7 @@ Error Solver::get_fields(double *TE, double *TL, double *q, double *TB) {
 // iterate, node temperatures, right-hand side, the four CG vectors, then the
 // CG reduction slots.
 constexpr int kNoAllocMaxCells = 131072;
-constexpr int kNoAllocSlots = 65536;
+constexpr int kNoAllocSlots = kGridCgSlots;  // cg_solve clears and reads exactly these
 constexpr size_t kNoAllocDoubles = 7 * (size_t)kNoAllocMaxCells + kNoAllocSlots;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
@@ -3360,8 +3363,8 @@ Error Solver::fourier_initial_noalloc() {
         GL(K_TINTERP, k_tinterp<<<gN, kThreads, 0, s>>>(dm_, T_, TV));
         GL(K_MACRO_RHS, k_fourier_rhs<<<gC, kThreads, 0, s>>>(dm_, dp_.kappa, bF_dir_, bTF_, TV, rhs));
         CUDA_TRY(cudaGetLastError());
-        // cg_solve zeroes the kNoAllocSlots reduction slots (65536) itself
-        // when it takes the grid-wide kernel
+        // cg_solve zeroes the kNoAllocSlots (= kGridCgSlots) reduction slots
+        // itself when it takes the grid-wide kernel
         Error e = cg_solve(kfplan_, KF_ptr_, KF_idx_, KF_val_, KF_dinv_, T_, rhs, cfg.macro_rtol, 0.0, it, scal, r, z,
                            pv, Ap, T1, &h);
         if (e.code) return e;

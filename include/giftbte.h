@@ -280,13 +280,17 @@ int gbte_fourier_initial(gbte_handle *h);
  * pinned memory. Limits: at most 131072 cells and 131072 node slots (nodes x
  * materials); larger meshes get GBTE_ERR_ARG. The static array (about 7.9 MB)
  * is held by every GPU that loads the library until the process exits. The
- * first call on each device looks up the array's device address; make that
- * first call before any stream capture. All calls share the one array, so
- * calls that overlap on the GPU (other threads or streams) race; the CG
- * reduction slots are cleared on every solve, everything else is written
- * before it is read. Results go to the handle exactly as with
- * gbte_fourier_initial. Handles of a batched solve (gbte_batch_create) get
- * GBTE_ERR_UNSUPPORTED. */
+ * first call on each device looks up the array's device address and keeps
+ * it for the life of that device's primary context (a caller that tears the
+ * context down with cudaDeviceReset must not call this entry point again in
+ * the same process); make that first call before any stream capture. All
+ * calls share the one array, so calls that overlap on the GPU (other threads
+ * or streams) race; the CG reduction slots are cleared on every solve,
+ * everything else is written before it is read. Results go to the handle as
+ * with gbte_fourier_initial: the same temperature and flux; for an
+ * FP32-mixed handle the gradient of the stored base temperature is formed
+ * on the device here (on the host there), so it can differ in the last bits.
+ * Handles of a batched solve (gbte_batch_create) get GBTE_ERR_UNSUPPORTED. */
 int gbte_fourier_initial_noalloc(gbte_handle *h);
 
 /* Runs the outer source iteration until both margins are below the limits

@@ -23,11 +23,13 @@ REF_BIN = os.path.join(HERE, "_ref", "BTE_CPU")
 _lib = None
 
 
-def build(reference_root: str = "/root/reference") -> None:
-    """Compile the restatement, and the reference binary when its sources
-    are present (they are not on machines without the reference tree)."""
+def build(reference_root: Optional[str] = None) -> None:
+    """Compile the restatement, and the reference binary when a GiftBTE
+    source tree is given (argument, or the environment variable
+    GIFTBTE_REFERENCE); machines without the tree use the prebuilt binary."""
     subprocess.check_call(["make", "-s", "-C", HERE, "restate"])
-    if os.path.isdir(os.path.join(reference_root, "src")):
+    reference_root = reference_root or os.environ.get("GIFTBTE_REFERENCE", "")
+    if reference_root and os.path.isdir(os.path.join(reference_root, "src")):
         subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF={reference_root}", "-j8"])
 
 

@@ -14,8 +14,11 @@ the reference's full-precision fields:
          HeatFlux_macro.dat)
   margins per-iteration (temperature, heat-flux) margins from the log
 
-Usage (needs the reference tree, so it runs only where that exists):
+Usage (needs the compiled reference, oracle/_ref/BTE_CPU):
     python tests/golden/make_golden.py [case ...]
+    python tests/golden/make_golden.py config2_iter3 config2_converged
+The two config2 cases (the full-size benchmark cell) are not in the default
+list: the converged one takes hours of one core.
 """
 from __future__ import annotations
 
@@ -107,23 +110,56 @@ def deck_params(d: decks.Deck) -> dict:
             "bcs": [[b.tag, b.type, b.value] for b in d.bcs]}
 
 
+# The benchmarked 2D workload at full size: the 300 nm porous cell with a
+# 3 nm Poisson-disk Delaunay mesh (seed 0, 17,939 triangles), 40 bands, 64
+# CADOM directions. One reference outer iteration takes about 25 s on one
+# core, so the fixtures hold (a) the reference's state after CONFIG2_ITERS
+# outer iterations from its Fourier start, and (b) its state at margins
+# 1e-10. Only the band temperatures of CONFIG2_BANDS are stored (the full
+# 40-band field would be 5.7 MB).
+CONFIG2_ITERS = 3
+CONFIG2_BANDS = [0, 9, 19, 29, 39]
+BIG = {"config2_iter3": CONFIG2_ITERS, "config2_converged": 0}
+
+
+def big_cases():
+    out = {}
+    for name, iters in BIG.items():
+        d = decks.config2_deck(h_nm=3.0, n_bands=40, n_phi=16, seed=0)
+        if iters:
+            d.max_iter = iters
+            d.residual_temp = 0.0
+            d.residual_flux = 0.0
+        else:
+            d.max_iter = 3000
+            d.residual_temp = 1e-10
+            d.residual_flux = 1e-10
+        out[name] = d
+    return out
+
+
 def make(name: str, d: decks.Deck) -> None:
     work = tempfile.mkdtemp(prefix=f"golden_{name}_")
     try:
         d.write(work)
-        r = oracle.run_reference(work)
+        r = oracle.run_reference(work, timeout=6 * 3600.0)
     finally:
         shutil.rmtree(work, ignore_errors=True)
     m = d.mesh
     B = d.bands
+    extra = {}
+    Tband = r["Tband"]
+    if name in BIG:
+        extra["bands_kept"] = np.asarray(CONFIG2_BANDS)
+        Tband = Tband[CONFIG2_BANDS]
     np.savez_compressed(
         os.path.join(HERE, f"{name}.npz"),
         nodes=m.nodes, cells=np.asarray(m.cells), edges=m.edges, edge_tags=m.edge_tags,
         cell_region=m.cell_region,
         band_v=B.v, band_tau=B.tau, band_C=B.C, band_lat=B.lattice_ratio, band_hr=B.heat_ratio,
         params=json.dumps(deck_params(d)),
-        T=r["T"], E=r["E"], q=r["q"], Tband=r["Tband"], xyz=r["xyz"], iters=r["iters"],
-        Tf=r["Tf"], qf=r["qf"], margins=r["margins"])
+        T=r["T"], E=r["E"], q=r["q"], Tband=Tband, xyz=r["xyz"], iters=r["iters"],
+        Tf=r["Tf"], qf=r["qf"], margins=r["margins"], **extra)
     print(f"{name}: Nc={m.n_cells} Nb={B.n_bands} iters={r['iters']}")
 
 
@@ -141,9 +177,16 @@ def load(name: str):
                    mesh_format=p["mesh_format"], order=p.get("order", "2"), scheme=p.get("scheme", "Synthetic"),
                    residual_temp=1e-12, residual_flux=1e-12,
                    max_iter=LIMITER_ITERS if p.get("order") == "2limit" else 3000)
-    ref = {k: z[k] for k in ("T", "E", "q", "Tband", "xyz", "Tf", "qf", "margins") if k in z}
+    ref = {k: z[k] for k in ("T", "E", "q", "Tband", "xyz", "Tf", "qf", "margins", "bands_kept") if k in z}
     ref["iters"] = int(z["iters"])
+    if name in BIG:
+        d.max_iter = BIG[name] or 3000
+        d.residual_temp = d.residual_flux = 0.0 if BIG[name] else 1e-10
     return d, ref
+
+
+def have(name: str) -> bool:
+    return os.path.exists(os.path.join(HERE, f"{name}.npz"))
 
 
 CASES = ["gray_square_tri", "quad_heat_specular", "periodic_jitter", "porous_msh", "porous_firstorder",
@@ -154,5 +197,6 @@ CONVERGED = [c for c in CASES if c != "porous_limiter"]
 if __name__ == "__main__":
     want = sys.argv[1:] or CASES
     all_cases = cases()
+    all_cases.update(big_cases())
     for n in want:
         make(n, all_cases[n])

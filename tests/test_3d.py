@@ -84,7 +84,7 @@ def test_fp64_matches_oracle_3d(specular):
     assert rel(f["T"], o["T"]) <= TOL_FP64, rel(f["T"], o["T"])
     assert rel(f["E"], o["E"]) <= TOL_FP64
     assert rel(f["Tband"], o["Tband"]) <= TOL_FP64
-    assert rel(f["q"], o["q"]) <= 1e-8, rel(f["q"], o["q"])
+    assert rel(f["q"], o["q"]) <= 1e-9, rel(f["q"], o["q"])
 
 
 @pytest.mark.gpu
@@ -126,7 +126,7 @@ def test_sweep_variants_match_oracle_3d(opts):
     f = s.fields()
     s.close()
     assert rel(f["T"], o["T"]) <= TOL_FP64, rel(f["T"], o["T"])
-    assert rel(f["q"], o["q"]) <= 1e-8
+    assert rel(f["q"], o["q"]) <= 1e-9
 
 
 @pytest.mark.gpu
@@ -160,4 +160,4 @@ def test_extensions_match_oracle_3d():
     f = s.fields()
     s.close()
     assert rel(f["T"], o["T"]) <= TOL_FP64, rel(f["T"], o["T"])
-    assert rel(f["q"], o["q"]) <= 1e-8
+    assert rel(f["q"], o["q"]) <= 1e-9

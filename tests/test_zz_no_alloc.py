@@ -54,3 +54,76 @@ def test_noalloc_fourier_matches_allocating_entry_point(precision):
             s.solve(allow_not_converged=False)
             assert rel(s.fields()["T"], ref["T"]) <= TOL
         s.close()
+
+
+def test_noalloc_fp32_handle_solves_like_allocating_seed():
+    # an FP32-mixed handle seeded by the allocation-free call solves to the
+    # same fixed point as one seeded by gbte_fourier_initial, within the FP32
+    # tolerance of the other tests (the base temperature's gradient is formed
+    # on the device in one case, on the host in the other)
+    deck, ref = mg.load("gray_square_tri")
+    out = []
+    for noalloc in (False, True):
+        s = StaticBTESynthetic.from_deck(deck, precision=GBTE_FP32_MIXED, err_temp=1e-9, err_flux=1e-7)
+        s.fourier_initial_noalloc() if noalloc else s.fourier_initial()
+        s.solve()
+        out.append(s.fields()["T"])
+        s.close()
+    assert rel(out[1], out[0]) <= 1e-5
+    assert rel(out[1], ref["T"]) <= 1e-5
+
+
+def test_noalloc_grid_wide_cg_branch():
+    # 64,800 cells: the Fourier system no longer fits one cluster's shared
+    # memory, so both entry points take the grid-wide CG kernel; the
+    # allocation-free one then uses the array's four CG vectors and its
+    # reduction slots
+    from giftbte_b200 import decks
+
+    deck = decks.config1_deck(180)
+    assert 58112 < deck.mesh.n_cells <= 131072
+    expected = allocating_results(deck, GBTE_FP64)
+    s = StaticBTESynthetic.from_deck(deck, precision=GBTE_FP64)
+    for call in range(2):
+        s.fourier_initial_noalloc()
+        f = s.fields()
+        assert rel(f["T"], expected[call]["T"]) <= TOL
+        assert rel(f["q"], expected[call]["q"]) <= TOL
+    s.close()
+
+
+def test_noalloc_allocates_no_device_memory():
+    # after the first call has looked up the array's address, a further call
+    # changes the device's free memory by less than one 2 MiB allocation
+    # granule: it allocates nothing
+    import torch
+
+    deck, _ = mg.load("periodic_jitter")
+    s = StaticBTESynthetic.from_deck(deck, precision=GBTE_FP64)
+    s.fourier_initial_noalloc()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    for _ in range(3):
+        s.fourier_initial_noalloc()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    s.close()
+    assert free0 - free1 < 2 * 1024 * 1024, (free0, free1)
+
+
+def test_noalloc_refuses_batched_and_oversized_handles():
+    from giftbte_b200 import GBTE_ERR_ARG, GBTE_ERR_UNSUPPORTED, GBTEError, decks
+
+    d1, _ = mg.load("gray_square_tri")
+    d2, _ = mg.load("gray_square_tri")
+    b = StaticBTESynthetic.from_decks([d1, d2], precision=GBTE_FP64)
+    with pytest.raises(GBTEError) as ei:
+        b.fourier_initial_noalloc()
+    assert ei.value.status == GBTE_ERR_UNSUPPORTED
+    b.close()
+    big = decks.config1_deck(260, n_phi=1)  # 135,200 cells > 131,072
+    s = StaticBTESynthetic.from_deck(big, precision=GBTE_FP64)
+    with pytest.raises(GBTEError) as ei:
+        s.fourier_initial_noalloc()
+    assert ei.value.status == GBTE_ERR_ARG
+    s.close()
