@@ -159,9 +159,13 @@ int create_common(const gbte::RawMesh &raw_in, const gbte::Bands &bands_in, cons
     if (opt.sweep_vector != 0 && opt.sweep_vector != 1 && opt.sweep_vector != 2 && opt.sweep_vector != 4)
         return fail(nullptr, {-1, "sweep_vector must be 0 (automatic), 1, 2 or 4"}), GBTE_ERR_ARG;
     cfg.sweep_vector = opt.sweep_vector;
-    if (opt.sweep_kernel < 0 || opt.sweep_kernel > 2)
-        return fail(nullptr, {-1, "sweep_kernel must be 0 (automatic), 1 (block) or 2 (warp)"}), GBTE_ERR_ARG;
+    if (opt.sweep_kernel < 0 || opt.sweep_kernel > 3)
+        return fail(nullptr, {-1, "sweep_kernel must be 0 (automatic), 1 (block), 2 (warp) or 3 (wide)"}),
+               GBTE_ERR_ARG;
     cfg.sweep_kernel = opt.sweep_kernel;
+    if (opt.gradient_dirs != 0 && opt.gradient_dirs != 1 && opt.gradient_dirs != 2 && opt.gradient_dirs != 4)
+        return fail(nullptr, {-1, "gradient_dirs must be 0 (automatic), 1, 2 or 4"}), GBTE_ERR_ARG;
+    cfg.gradient_dirs = opt.gradient_dirs;
     cfg.device = opt.device;
     cfg.stream = (cudaStream_t)opt.stream;
     if (opt.precision != GBTE_FP64 && opt.precision != GBTE_FP32_MIXED)
@@ -500,7 +504,8 @@ int gbte_solve(gbte_handle *h, gbte_stats *st) {
             st->sweep_stage_levels = h->solver.tuned_sweep_look_;
             st->sweep_vector = h->solver.last_sweep_vb_;
             st->sweep_threads = h->solver.last_sweep_threads_;
-            st->sweep_kernel = h->solver.last_sweep_warp_ ? 2 : 1;
+            st->sweep_kernel = h->solver.last_sweep_warp_ == 1 ? 2 : h->solver.last_sweep_warp_ == 2 ? 3 : 1;
+            st->gradient_dirs = h->solver.last_grad_dirs_;
             for (int k = 0; k < GBTE_NUM_KERNELS && k < gbte::K_NUM; k++) {
                 st->kernel_ms[k] = s.kernel_ms[k];
                 st->kernel_count[k] = s.kernel_count[k];

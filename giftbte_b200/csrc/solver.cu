@@ -341,6 +341,92 @@ __global__ void __launch_bounds__(256) k_gradient8(DMesh m, DPhys p, const S *__
     }
 }
 
+// The stencil entry q of the gradient: weights (storage precision) and the
+// neighbour. FP32: one 16-byte load of {w_x, w_y, w_z, neighbour bits};
+// FP64: the double weights and the index.
+__device__ __forceinline__ void stencil_entry(const DMesh &m, const float4 *pk, int q, float &wx, float &wy, float &wz,
+                                              int &j) {
+    const float4 a = pk[q];
+    wx = a.x, wy = a.y, wz = a.z;
+    j = __float_as_int(a.w);
+}
+__device__ __forceinline__ void stencil_entry(const DMesh &m, const float4 *, int q, double &wx, double &wy,
+                                              double &wz, int &j) {
+    wx = m.lsq_w[3 * q], wy = m.lsq_w[3 * q + 1], wz = m.lsq_w[3 * q + 2];
+    j = m.nbr_idx[q];
+}
+
+// k_gradient8 for DG directions per thread: one thread per (group of DG
+// directions of the batch, cell, 4 consecutive bands). Each stencil entry is
+// loaded once for 4 * DG band-direction updates (the stencil is the same for
+// every direction and band). Per band and direction the arithmetic is
+// k_gradient8's, in the same order, so both give the same bits. A batch of
+// an odd number of directions repeats its last direction in the last group
+// without storing it.
+template <typename S, int DIM, int DG>
+__global__ void __launch_bounds__(256) k_gradient_md(DMesh m, DPhys p, const float4 *__restrict__ pk,
+                                                     const S *__restrict__ eps, S *__restrict__ g, int d0, int ndb) {
+    constexpr int BC = 4;
+    const int nb = p.nb, nc = m.nc, nbc = nb / BC;
+    const int ngrp = (ndb + DG - 1) / DG;
+    const size_t total = (size_t)ngrp * nc * nbc;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int bc = (int)(t % nbc);
+        const size_t rest = t / nbc;
+        const int c = (int)(rest % nc);
+        const int grp = (int)(rest / nc);
+        const S *ed[DG];
+        S ec[DG][BC], gx[DG][BC], gy[DG][BC], gz[DG][BC];
+#pragma unroll
+        for (int k = 0; k < DG; k++) {
+            const int dl = min(grp * DG + k, ndb - 1);
+            ed[k] = eps + (size_t)(d0 + dl) * nc * nb + BC * bc;
+            ld8(ed[k] + (size_t)c * nb, ec[k]);
+#pragma unroll
+            for (int i = 0; i < BC; i++) gx[k][i] = gy[k][i] = gz[k][i] = 0;
+        }
+        const int q1 = m.nbr_ptr[c + 1];
+        for (int q = m.nbr_ptr[c]; q < q1; q += 4) {
+            S wx[4], wy[4], wz[4];
+            int jn[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                if (q + u < q1)
+                    stencil_entry(m, pk, q + u, wx[u], wy[u], wz[u], jn[u]);
+                else
+                    wx[u] = wy[u] = wz[u] = 0, jn[u] = c;
+            }
+            S e4[4][DG][BC];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int k = 0; k < DG; k++) ld8(ed[k] + (size_t)jn[u] * nb, e4[u][k]);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                if (q + u >= q1) break;
+#pragma unroll
+                for (int k = 0; k < DG; k++)
+#pragma unroll
+                    for (int i = 0; i < BC; i++) {
+                        const S de = e4[u][k][i] - ec[k][i];
+                        gx[k][i] += wx[u] * de;
+                        gy[k][i] += wy[u] * de;
+                        if (DIM == 3) gz[k][i] += wz[u] * de;
+                    }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < DG; k++) {
+            const int dl = grp * DG + k;
+            if (dl >= ndb) break;
+            S *gp = g + ((size_t)dl * nc + c) * DIM * nb + BC * bc;
+            st8(gp, gx[k]);
+            st8(gp + nb, gy[k]);
+            if (DIM == 3) st8(gp + 2 * nb, gz[k]);
+        }
+    }
+}
+
 // Band-independent part of the face fluxes of the FP32 form's base field:
 // B[d][c] = (1/s_c) sum_f A_f/V (s.n_f) beta_f (s_c the cell's scattering
 // multiplier, 1 by default), beta_f the second-order upwind face
@@ -648,6 +734,97 @@ __global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int ncomp, int d0
         }
     }
     cp_async_wait<0>();
+}
+
+// Wide-level form of the same sweep, for meshes whose levels hold thousands
+// of cells (3D tetrahedra: up to ~15k on the hotspot block). An on-chip ring
+// that holds a whole level would leave room for a few bands per CTA only,
+// one CTA per SM. Here every correction goes to Dc (cell order) and upwind
+// corrections are read back from there (L2-resident: they were written one
+// or a few levels before), so the kernel uses no shared memory and runs at
+// full occupancy with any band chunk. Records, residual rows and cell lists
+// are read straight from memory, coalesced within a level; the level's
+// width hides their latency. One barrier per level: it orders the level's
+// Dc stores before the next level's loads within the CTA. Records must hold
+// level positions (no far slots). The arithmetic is that of k_sweep, in the
+// same order, so both give the same bits.
+template <typename S, int VB>
+__global__ void __launch_bounds__(1024) k_sweep_wide(int nb, int nc, int ncomp, int d0, int nbc,
+                                                    const int *__restrict__ lvl_ptr,
+                                                    const int *__restrict__ dir_lvl_off,
+                                                    const SweepRec<S> *__restrict__ rec,
+                                                    const int *__restrict__ lvl_cells,
+                                                    const double *__restrict__ kbv, const S *__restrict__ Rlo,
+                                                    S *Dc) {
+    const int nchunks = (nb + nbc - 1) / nbc;
+    const int entl = blockIdx.x / nchunks, chunk = blockIdx.x % nchunks;
+    const int dl = entl / ncomp, d = d0 + dl, ent = d * ncomp + entl % ncomp;
+    const int b0 = chunk * nbc, nbl = min(nbc, nb - b0);
+    const int lo0 = dir_lvl_off[ent], nlev = dir_lvl_off[ent + 1] - lo0 - 1;
+    const size_t base = (size_t)d * nc, lbase = (size_t)dl * nc;
+    const int tid = threadIdx.x, bd = blockDim.x;
+    const int lpc = nbc / VB;
+    const int lb = (tid % lpc) * VB, lc0 = tid / lpc, cpp = bd / lpc;
+    const bool band_ok = lb < nbl && lc0 < cpp;
+    S kb[VB];
+#pragma unroll
+    for (int v = 0; v < VB; v++) kb[v] = band_ok ? (S)kbv[b0 + lb + v] : (S)0;
+    const int *cells = lvl_cells + base;
+    S *Dd = Dc + lbase * nb + b0 + lb;
+    int c0 = lvl_ptr[lo0];
+    for (int l = 0; l < nlev; l++) {
+        const int c1 = lvl_ptr[lo0 + l + 1];
+        if (band_ok) {
+            for (int p = c0 + lc0; p < c1; p += cpp) {
+                const SweepRec<S> r = rec[base + p];
+                S r0[VB];
+                vld<S, VB>(Rlo + (lbase + p) * nb + b0 + lb, r0);
+                const int nin = r.meta & 7;
+                int cj[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) cj[j] = j < nin ? cells[r.np[j]] : 0;
+                S sum[VB];
+#pragma unroll
+                for (int v = 0; v < VB; v++) sum[v] = (S)0;
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    if (j < nin) {
+                        S dj[VB];
+                        vld<S, VB>(Dd + (size_t)cj[j] * nb, dj);
+#pragma unroll
+                        for (int v = 0; v < VB; v++) sum[v] += r.a[j] * dj[v];
+                    }
+                }
+                S dv[VB];
+#pragma unroll
+                for (int v = 0; v < VB; v++) dv[v] = sweep_div(r0[v] - kb[v] * sum[v], (S)1 + kb[v] * r.sig);
+                vst<S, VB>(Dd + (size_t)r.cell * nb, dv);
+            }
+        }
+        c0 = c1;
+        __syncthreads();
+    }
+}
+
+template <typename S>
+cudaError_t sweep_wide_dispatch(int vb, int blocks, int threads, cudaStream_t s, int nb, int nc, int ncomp, int d0,
+                                int nbc, const int *lvl_ptr, const int *dir_lvl_off, const SweepRec<S> *rec,
+                                const int *lvl_cells, const double *kb, const S *R, S *Dc) {
+    if (vb == 1)
+        k_sweep_wide<S, 1><<<blocks, threads, 0, s>>>(nb, nc, ncomp, d0, nbc, lvl_ptr, dir_lvl_off, rec, lvl_cells,
+                                                      kb, R, Dc);
+    else if (vb == 2)
+        k_sweep_wide<S, 2><<<blocks, threads, 0, s>>>(nb, nc, ncomp, d0, nbc, lvl_ptr, dir_lvl_off, rec, lvl_cells,
+                                                      kb, R, Dc);
+    else if constexpr (sizeof(S) == 4) {
+        if (vb == 4)
+            k_sweep_wide<S, 4><<<blocks, threads, 0, s>>>(nb, nc, ncomp, d0, nbc, lvl_ptr, dir_lvl_off, rec,
+                                                          lvl_cells, kb, R, Dc);
+        else
+            return cudaErrorInvalidValue;
+    } else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
 }
 
 // Warp-independent form of the same sweep: one warp per (direction, group of
@@ -1904,6 +2081,14 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
     {
         std::vector<float> wf(mesh.lsq_w.begin(), mesh.lsq_w.end());
         d.lsq_wf = upload(this, allocs_, wf, s, ok);
+        std::vector<float4> pk(mesh.nbr_idx.size());
+        for (size_t q = 0; q < pk.size(); q++) {
+            int j = mesh.nbr_idx[q];
+            float jf;
+            std::memcpy(&jf, &j, sizeof(float));
+            pk[q] = make_float4((float)mesh.lsq_w[3 * q], (float)mesh.lsq_w[3 * q + 1], (float)mesh.lsq_w[3 * q + 2], jf);
+        }
+        d.lsq_pk = upload(this, allocs_, pk, s, ok);
     }
     d.face_w = up_d(mesh.face_w);
     d.f_cf0 = up_i(mesh.f_cf0);
@@ -2761,8 +2946,10 @@ Error Solver::solve_t(SolveStats &st) {
     // threads = a multiple of the threads per cell, nbc / vb, up to `tmax`
     // warp = 1: the warp-independent kernel (vb bands per warp, wpc warps
     // per CTA, wsmem bytes of shared memory per warp)
+    // wide = 1: the wide-level kernel (no shared memory; records must hold
+    // level positions, i.e. the plan has no far slots)
     struct SweepLaunch {
-        int nbc = 0, chunks = 0, threads = 0, blocks = 0, rvec = 0, look = 4, vb = 1, warp = 0, wpc = 1;
+        int nbc = 0, chunks = 0, threads = 0, blocks = 0, rvec = 0, look = 4, vb = 1, warp = 0, wpc = 1, wide = 0;
         size_t smem = 0, wsmem = 0;
     };
     constexpr int LCAPW = 64;
@@ -2811,7 +2998,28 @@ Error Solver::solve_t(SolveStats &st) {
         return true;
     };
     CUDA_TRY((sweep_w_set_smem<S, LCAPW>(220 * 1024)));
+    // the wide-level kernel: equal chunks of at most `cap` bands (a multiple
+    // of vb), `threads` per CTA rounded down to whole cells
+    const bool wide_ok = far_slots_ == 0;
+    auto sweep_launch_wide = [&](int cap, SweepLaunch &L, int vb, int threads) -> bool {
+        if (!wide_ok || nb % vb != 0 || vb * (int)sizeof(S) > 16) return false;
+        L = SweepLaunch();
+        L.wide = 1;
+        L.vb = vb;
+        const int nch = (nb + cap - 1) / cap;
+        L.nbc = (nb + nch - 1) / nch;
+        L.nbc = (L.nbc + vb - 1) / vb * vb;
+        L.chunks = (nb + L.nbc - 1) / L.nbc;
+        const int lpc = L.nbc / vb;
+        if (lpc > threads) return false;
+        L.threads = (threads / lpc) * lpc;
+        return true;
+    };
     auto launch_sweep = [&](const SweepLaunch &L, int d0, int nbt) -> cudaError_t {
+        if (L.wide)
+            return sweep_wide_dispatch<S>(L.vb, nbt * ncomp_ * L.chunks, L.threads, s, nb, nc, ncomp_, d0, L.nbc,
+                                          lvl_ptr_, dir_lvl_off_, (const SweepRec<S> *)rec_, lvl_cells_, kb_, R,
+                                          (S *)corr_);
         if (L.warp) {
             const int nwarps = nbt * ncomp_ * (nb / L.vb);
             return sweep_w_dispatch<S, LCAPW>(L.look, L.vb, (nwarps + L.wpc - 1) / L.wpc, L.threads, L.smem, s, nb, nc,
@@ -2833,19 +3041,24 @@ Error Solver::solve_t(SolveStats &st) {
     const bool fixed_cap = cfg.sweep_bands >= 1 && cfg.sweep_bands <= 32;
     const bool fixed_vb = cfg.sweep_vector == 1 || cfg.sweep_vector == 2 || cfg.sweep_vector == 4;
     const bool want_warp = cfg.sweep_kernel == 2, want_block = cfg.sweep_kernel == 1;
+    const bool want_wide = cfg.sweep_kernel == 3;
     const bool tune = !(fixed_vb && (want_warp || fixed_cap)) && tuned_sweep_bands_ == 0;
+    (void)want_wide;
     int wcap = fixed_cap ? cfg.sweep_bands : tuned_sweep_bands_ > 0 ? tuned_sweep_bands_ : (sizeof(S) == 4 ? 8 : 4);
     int wvb = fixed_vb ? cfg.sweep_vector : tuned_sweep_bands_ > 0 ? tuned_sweep_vb_ : 1;
     SweepLaunch SL;
     const bool use_warp = want_warp || (!want_block && tuned_sweep_bands_ > 0 && tuned_sweep_warp_);
-    if (!(use_warp && (sweep_launch_w(SL, tuned_sweep_look_, wvb, tuned_sweep_wpc_) ||
+    const bool use_wide = (cfg.sweep_kernel == 3 || (cfg.sweep_kernel == 0 && tuned_sweep_bands_ > 0 &&
+                                                     tuned_sweep_wide_)) &&
+                          sweep_launch_wide(wcap, SL, wvb, tuned_sweep_threads_);
+    if (!use_wide && !(use_warp && (sweep_launch_w(SL, tuned_sweep_look_, wvb, tuned_sweep_wpc_) ||
                        sweep_launch_w(SL, tuned_sweep_look_, 1, tuned_sweep_wpc_) || sweep_launch_w(SL, 2, 1, 1))) &&
         !sweep_launch(wcap, SL, tuned_sweep_look_, wvb, tuned_sweep_threads_) &&
         !sweep_launch(wcap, SL, tuned_sweep_look_, 1, tuned_sweep_threads_))
         return {-8, "sweep level too wide for the shared-memory correction ring"};
     last_sweep_vb_ = SL.vb;
     last_sweep_threads_ = SL.threads;
-    last_sweep_warp_ = SL.warp;
+    last_sweep_warp_ = SL.warp ? 1 : SL.wide ? 2 : 0;
     const int cpb = std::max(1, 256 / nb);
     const int gM = (nc + cpb - 1) / cpb;
     const size_t msmem = ((size_t)nd * kWTab + (size_t)cpb * nb * kMomSlots) * sizeof(double);
@@ -2859,6 +3072,21 @@ Error Solver::solve_t(SolveStats &st) {
         GL(K_GATHER, k_diffuse_sum<<<grid_for((size_t)nbs * nb), kThreads, 0, s>>>(dm_, dp_, dif_w_, eb_, dsum_));
         GL(K_GATHER, k_gather<<<gB, kThreads, 0, s>>>(dm_, dp_, dsum_, spec_src_, need_snapshot_ ? eb_snap_ : nullptr, eb_));
     };
+    // LSQ gradient, 4 bands and grad_dg directions per thread (options.gradient_dirs,
+    // or timed on the first outer iteration: gtune)
+    const bool gtune = cfg.gradient_dirs == 0 && tuned_grad_dirs_ == 0 && nb % 4 == 0 && cfg.order == 2;
+    int grad_dg = cfg.gradient_dirs ? cfg.gradient_dirs : tuned_grad_dirs_ ? tuned_grad_dirs_ : 2;
+    auto launch_grad = [&](int dg, int d0, int nbt) -> cudaError_t {
+        const size_t items = (size_t)((nbt + dg - 1) / dg) * nc * (nb / 4);
+        if (dg == 2)
+            k_gradient_md<S, DIM, 2><<<grid_for(items), kThreads, 0, s>>>(dm_, dp_, dm_.lsq_pk, eps, g, d0, nbt);
+        else if (dg == 4)
+            k_gradient_md<S, DIM, 4><<<grid_for(items), kThreads, 0, s>>>(dm_, dp_, dm_.lsq_pk, eps, g, d0, nbt);
+        else
+            k_gradient8<S, DIM, 4><<<grid_for(items), kThreads, 0, s>>>(dm_, dp_, w, eps, g, d0, nbt);
+        return cudaGetLastError();
+    };
+    last_grad_dirs_ = nb % 4 == 0 ? grad_dg : 0;
     // first order (solve_firstorder, StaticBTESyntheticSolver.cpp:487-726):
     // upwind cell values on the faces, i.e. zero gradients throughout
     if (cfg.order == 1) CUDA_TRY(cudaMemsetAsync(grad_, 0, (size_t)ndb * nc * nb * DIM * sizeof(S), s));
@@ -2906,9 +3134,32 @@ Error Solver::solve_t(SolveStats &st) {
         const size_t nbe = (size_t)nbt * nc * nb;
         ev.gd0 = d0;
         if (nb % 4 == 0) {
-            if (cfg.order == 2)
-                GL(K_GRADIENT, (k_gradient8<S, DIM, 4><<<grid_for(nbe / 4), kThreads, 0, s>>>(dm_, dp_, w, eps, g, d0,
-                                                                                              nbt)));
+            if (cfg.order == 2 && gtune && nt == 0 && d0 == dlo) {
+                // directions per gradient thread: each candidate timed twice
+                // on this batch (they write the same bits to g)
+                cudaEvent_t t0, t1;
+                CUDA_TRY(cudaEventCreate(&t0));
+                CUDA_TRY(cudaEventCreate(&t1));
+                float best = 1e30f;
+                int best_dg = 1;
+                for (int dg : {1, 2, 4}) {
+                    for (int rep = 0; rep < 2; rep++) {
+                        CUDA_TRY(cudaEventRecord(t0, s));
+                        CUDA_TRY(launch_grad(dg, d0, nbt));
+                        CUDA_TRY(cudaEventRecord(t1, s));
+                        CUDA_TRY(cudaEventSynchronize(t1));
+                        float m = 0;
+                        CUDA_TRY(cudaEventElapsedTime(&m, t0, t1));
+                        if (m < best) best = m, best_dg = dg;
+                    }
+                }
+                cudaEventDestroy(t0);
+                cudaEventDestroy(t1);
+                tuned_grad_dirs_ = best_dg;
+                grad_dg = best_dg;
+                last_grad_dirs_ = best_dg;
+            }
+            if (cfg.order == 2) GL(K_GRADIENT, CUDA_TRY(launch_grad(grad_dg, d0, nbt)));
             if (cfg.use_limiter)
                 GL(K_GRADIENT, (k_limit<DIM><<<grid_for(nbe), kThreads, 0, s>>>(dm_, dp_, (const double *)eps, eb_,
                                                                                (double *)g, d0, nbt)));
@@ -2995,8 +3246,40 @@ Error Solver::solve_t(SolveStats &st) {
                     }
                 }
             }
+            // the wide-level kernel (plans without far slots): band chunks,
+            // bands per thread and CTA size
+            int best_wide = 0;
+            if (wide_ok && !want_block && !want_warp) {
+                if (want_wide) best = 1e30f;
+                std::vector<long long> seen_w;
+                for (int cap : {nb, (nb + 1) / 2, (nb + 3) / 4, (nb + 7) / 8}) {
+                    if (fixed_cap && cap != wcap) continue;
+                    for (int vb : {4, 2, 1}) {
+                        if (fixed_vb && vb != wvb) continue;
+                        if (!fixed_vb && vb == 1 && sizeof(S) == 4) continue;
+                        for (int threads : {256, 1024}) {
+                            SweepLaunch L;
+                            if (!sweep_launch_wide(cap, L, vb, threads)) continue;
+                            const long long key = ((long long)L.nbc * 8 + L.vb) * 2048 + L.threads;
+                            if (std::find(seen_w.begin(), seen_w.end(), key) != seen_w.end()) continue;
+                            seen_w.push_back(key);
+                            float ms = 0;
+                            Error te = trial(L, ms);
+                            if (te.code) return te;
+                            if (ms < best) {
+                                best = ms;
+                                best_wide = 1;
+                                best_warp = 0;
+                                best_cap = cap;
+                                best_vb = vb;
+                                best_threads = threads;
+                            }
+                        }
+                    }
+                }
+            }
             for (int tmax : {128, 64}) {
-                if (best_warp) break;
+                if (best_warp || best_wide) break;
                 SweepLaunch L;
                 if (!sweep_launch(best_cap, L, 4, best_vb, tmax)) continue;
                 SweepLaunch L256;
@@ -3011,6 +3294,7 @@ Error Solver::solve_t(SolveStats &st) {
                 }
             }
             for (int look : {3, 2}) {
+                if (best_wide) break;
                 SweepLaunch L;
                 if (best_warp ? !sweep_launch_w(L, look, best_vb, best_wpc)
                               : !sweep_launch(best_cap, L, look, best_vb, best_threads))
@@ -3031,12 +3315,14 @@ Error Solver::solve_t(SolveStats &st) {
             tuned_sweep_threads_ = best_threads;
             tuned_sweep_warp_ = best_warp;
             tuned_sweep_wpc_ = best_wpc;
+            tuned_sweep_wide_ = best_wide;
             wcap = best_cap;
-            if (!(best_warp && sweep_launch_w(SL, best_look, best_vb, best_wpc)))
+            if (!(best_wide && sweep_launch_wide(wcap, SL, best_vb, best_threads)) &&
+                !(best_warp && sweep_launch_w(SL, best_look, best_vb, best_wpc)))
                 sweep_launch(wcap, SL, best_look, best_vb, best_threads);
             last_sweep_vb_ = SL.vb;
             last_sweep_threads_ = SL.threads;
-            last_sweep_warp_ = SL.warp;
+            last_sweep_warp_ = SL.warp ? 1 : SL.wide ? 2 : 0;
         }
         GL(K_SWEEP, CUDA_TRY(launch_sweep(SL, d0, nbt)));
         GL(K_MOMENTS, (k_moments<S><<<gM, cpb * nb, msmem, s>>>(dm_, dp_, cpb, eps, (const S *)corr_, Tbase_, wtab_,
@@ -3076,7 +3362,7 @@ Error Solver::solve_t(SolveStats &st) {
             if (rc) return {-9, "direction shard exchange failed (" + std::to_string(rc) + ")"};
             return {0, ""};
         };
-        const bool graphable = graph_ok_ && !(tune && nt == 0) && !cfg.profile;
+        const bool graphable = graph_ok_ && !((tune || (gtune && tuned_grad_dirs_ == 0)) && nt == 0) && !cfg.profile;
         // capture once; any failure leaves the direct launches in place
         auto capture = [&](const std::function<Error()> &stage, cudaGraphExec_t &gx, long long &nl) {
             cudaGraph_t gr = nullptr;

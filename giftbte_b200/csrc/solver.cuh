@@ -20,6 +20,7 @@ struct DMesh {
     const int *nbr_ptr, *nbr_idx;
     const double *lsq_w;
     const float *lsq_wf;
+    const float4 *lsq_pk;  // per stencil entry {w_x, w_y, w_z, neighbour index bits} in FP32
     const double *face_w;
     const int *f_cf0;
     const int *b_type, *b_connect;
@@ -50,8 +51,9 @@ struct SolverConfig {
     int profile = 0;
     int sweep_bands = 0;      // bands per sweep CTA, 0 = automatic
     int sweep_vector = 0;     // bands per sweep thread (1, 2, 4), 0 = automatic
-    int sweep_kernel = 0;     // 1: block sweep kernel, 2: warp-independent kernel, 0 = automatic
+    int sweep_kernel = 0;     // 1: block sweep kernel, 2: warp-independent kernel, 3: wide-level kernel, 0 = automatic
     int sweep_far_slots = 0;  // far-slot cap of the sweep plan: 0 = automatic, < 0 = none
+    int gradient_dirs = 0;    // directions per gradient thread (1, 2, 4), 0 = automatic
     int direction_batch = 0;  // most directions per transport batch, 0 = automatic
     std::vector<double> cell_scatter;  // scattering-rate multiplier s_c per cell (empty: 1)
     int order = 2;            // 2: second-order upwind faces (solve); 1: first order (solve_firstorder)
@@ -139,7 +141,11 @@ public:
     int tuned_sweep_threads_ = 256;  // most threads per sweep CTA (the autotuner's pick)
     int tuned_sweep_warp_ = 0;   // 1: the warp-independent sweep kernel won (the autotuner's pick)
     int tuned_sweep_wpc_ = 1;    // warps per CTA of that kernel
-    int last_sweep_vb_ = 0, last_sweep_threads_ = 0, last_sweep_warp_ = 0;  // launch shape of the last solve's sweep
+    int tuned_sweep_wide_ = 0;   // 1: the wide-level sweep kernel won (the autotuner's pick)
+    int tuned_grad_dirs_ = 0;    // directions per gradient thread (1, 2 or 4; 0 = not yet tuned)
+    int last_grad_dirs_ = 0;     // the same, of the last solve's gradient launches (0: 1-band form)
+    // launch shape of the last solve's sweep (last_sweep_warp_: 0 block, 1 warp, 2 wide-level kernel)
+    int last_sweep_vb_ = 0, last_sweep_threads_ = 0, last_sweep_warp_ = 0;
     int ndb_ = 1;                // directions per batch of the gradient/residual/correction buffers
 
 private:

@@ -162,8 +162,15 @@ typedef struct {
                                  depend on it. */
     int sweep_kernel;         /* 1 = the block sweep (a CTA per direction and chunk of bands, one
                                  barrier per level), 2 = the warp-independent sweep (a warp per
-                                 direction and sweep_vector bands, no block barrier), 0 = the faster
-                                 of the two on the first outer iteration. Results do not depend on it. */
+                                 direction and sweep_vector bands, no block barrier), 3 = the
+                                 wide-level sweep (corrections read back from device memory, no
+                                 shared-memory ring: for levels of thousands of cells, e.g. 3D
+                                 tetrahedra; plans without far slots only), 0 = the fastest on the
+                                 first outer iteration. Results do not depend on it. */
+    int gradient_dirs;        /* directions each thread of the LSQ gradient covers (1, 2 or 4: one
+                                 load of a stencil entry serves 4 bands of that many directions);
+                                 0 = the fastest on the first outer iteration. Results do not
+                                 depend on it. */
 } gbte_options;
 
 #define GBTE_NUM_KERNELS 16
@@ -193,7 +200,8 @@ typedef struct {
     int sweep_stage_levels;   /* levels the sweep stages ahead in shared memory (autotuned, 2..4) */
     int sweep_vector;         /* bands per sweep thread in use (options.sweep_vector or autotuned) */
     int sweep_threads;        /* threads per sweep CTA in use */
-    int sweep_kernel;         /* sweep kernel in use: 1 block, 2 warp-independent */
+    int sweep_kernel;         /* sweep kernel in use: 1 block, 2 warp-independent, 3 wide-level */
+    int gradient_dirs;        /* directions per gradient thread in use (0: the 1-band form ran) */
 } gbte_stats;
 
 /* Name of kernel slot i of gbte_stats.kernel_ms (NULL past the last one). */

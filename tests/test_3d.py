@@ -114,7 +114,9 @@ def test_deck_dir_and_memory_decks_agree_3d(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("opts", [{"sweep_far_slots": -1}, {"sweep_bands": 3}, {"sweep_bands": 1, "sweep_far_slots": 4}])
+@pytest.mark.parametrize("opts", [{"sweep_far_slots": -1}, {"sweep_bands": 3}, {"sweep_bands": 1, "sweep_far_slots": 4},
+                                  {"sweep_far_slots": -1, "sweep_kernel": 3},
+                                  {"sweep_far_slots": -1, "sweep_kernel": 3, "sweep_bands": 3, "sweep_vector": 1}])
 def test_sweep_variants_match_oracle_3d(opts):
     # far slots off (upwind reads older than the ring go to memory), an odd
     # band chunk (element-wise residual staging) and a far-slot cap below

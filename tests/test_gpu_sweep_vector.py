@@ -90,3 +90,74 @@ def test_warp_kernel_batch_and_golden():
         assert st["sweep_kernel"] == 2
         assert float(np.max(np.abs(s.fields()["T"] - ref["T"])) / np.max(np.abs(ref["T"]))) <= 1e-9
         s.close()
+
+
+@pytest.mark.parametrize("prec,widths", [(g.GBTE_FP32_MIXED, (1, 2, 4)), (g.GBTE_FP64, (1, 2))])
+def test_wide_level_kernel_is_bit_identical(prec, widths):
+    # the wide-level kernel (options.sweep_kernel = 3) reads upwind
+    # corrections back from device memory instead of a shared ring; it needs
+    # records that hold level positions, so both runs plan without far slots
+    d = decks.config2_deck(h_nm=6.0, n_bands=16, n_phi=8, seed=2)
+
+    def run_w(vb, kernel, bands):
+        s = g.StaticBTESynthetic.from_deck(d, precision=prec, sweep_bands=bands, sweep_vector=vb,
+                                           sweep_kernel=kernel, sweep_far_slots=-1)
+        st = s.solve(max_iter=15, err_temp=0.0, err_flux=0.0)
+        f = s.fields()
+        s.close()
+        return f, st
+
+    f1, _ = run_w(1, 1, 8)
+    for vb in widths:
+        for bands in (8, 16):
+            fw, sw = run_w(vb, 3, bands)
+            assert sw["sweep_kernel"] == 3 and sw["sweep_vector"] == vb
+            for k in ("T", "E", "q", "Tband"):
+                assert np.array_equal(f1[k], fw[k]), (vb, bands, k)
+
+
+def test_wide_level_kernel_batch_and_golden():
+    pop = decks.porous_population(3, seed=1, h_nm=(15.0, 22.0), r_nm=(40.0, 80.0), n_bands=8, n_phi=2)
+    f1, _ = run(pop, g.GBTE_FP32_MIXED, 1, batch=True)
+    s = g.StaticBTESynthetic.from_decks(pop, precision=g.GBTE_FP32_MIXED, sweep_bands=8, sweep_vector=4,
+                                        sweep_kernel=3, sweep_far_slots=-1)
+    sw = s.solve(max_iter=15, err_temp=0.0, err_flux=0.0)
+    fw = s.fields()
+    s.close()
+    assert sw["sweep_kernel"] == 3
+    assert np.array_equal(f1["T"], fw["T"])
+    for case in ("quad_heat_specular", "porous_msh", "periodic_jitter"):
+        deck, ref = mg.load(case)
+        s = g.StaticBTESynthetic.from_deck(deck, precision=g.GBTE_FP64, sweep_kernel=3, sweep_far_slots=-1)
+        s.set_initial(ref["Tf"])
+        st = s.solve(allow_not_converged=False)
+        assert st["sweep_kernel"] == 3
+        assert float(np.max(np.abs(s.fields()["T"] - ref["T"])) / np.max(np.abs(ref["T"]))) <= 1e-9
+        s.close()
+
+
+@pytest.mark.parametrize("prec", [g.GBTE_FP32_MIXED, g.GBTE_FP64])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_gradient_direction_groups_are_bit_identical(prec, dim):
+    # the LSQ gradient with 1, 2 or 4 directions per thread
+    # (options.gradient_dirs): one stencil load serves more directions, the
+    # arithmetic per band and direction is unchanged. The 3D block runs in
+    # direction batches of 5, so groups of 2 and 4 meet a batch whose last
+    # group is short
+    if dim == 2:
+        d = decks.config2_deck(h_nm=6.0, n_bands=16, n_phi=8, seed=2)
+        kw = {}
+    else:
+        d = decks.config3_deck(h_nm=10.0, size_nm=(40.0, 40.0, 100.0), n_bands=8, n_theta=2, n_phi=2)
+        kw = {"direction_batch": 5}
+    out = {}
+    for dg in (1, 2, 4):
+        s = g.StaticBTESynthetic.from_deck(d, precision=prec, gradient_dirs=dg, sweep_bands=8, sweep_vector=1,
+                                           sweep_kernel=1, **kw)
+        st = s.solve(max_iter=10, err_temp=0.0, err_flux=0.0)
+        out[dg] = s.fields()
+        s.close()
+        assert st["gradient_dirs"] == dg
+    for dg in (2, 4):
+        for k in ("T", "E", "q", "Tband"):
+            assert np.array_equal(out[1][k], out[dg][k]), (dg, k)
