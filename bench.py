@@ -3,22 +3,31 @@
 
 One *step* is one outer source iteration (all bands x directions x cells:
 gradient, residual, upwind sweep, boundary, moments, synthetic correction,
-margins) of the named workload. The default workload is the non-gray 2D
-nanoporous cell: 300 nm periodic square with a centred r = 100 nm diffuse
-pore, Delaunay mesh with mean edge 3 nm (seed 0), 40 sine-dispersion bands,
-64 in-plane CADOM directions, x-periodic 1 K jump.
+margins) of the named workload. The default workload is the 3D hotspot
+block: a 100 x 100 x 500 nm box of 2.5 nm cubes split into 6 jittered
+tetrahedra each (1.92M tets, seed 1), 40 sine-dispersion bands, 128 Gauss
+directions, 1e18 W/m^3 in the top 20 nm, in the FP32-sweep form. The 2D
+nanoporous cell (config2: 300 nm periodic square, r = 100 nm diffuse pore,
+3 nm Delaunay mesh, 40 bands, 64 CADOM directions) stays selectable.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision fp32|fp64] [--workload config2|config1]
+                    [--precision fp32|fp64] [--workload config3|config2|config1|config4|config5]
 
 Prints one JSON line (rank 0). ``value`` is device-resident throughput in
 band*direction*cell updates/s over exactly K timed steps (CUDA events on the
-solver's stream, max over ranks). ``e2e`` is the same metric through the
-public API from host buffers: set the initial field from pinned host memory,
-solve to residual 1e-8, read every result field back. Under torchrun each
-rank solves an independent seeded cell (weak scaling, no collective on the
-data path). ``--impl reference`` times the reference's own CPU solver
-(oracle/_ref/BTE_CPU) on the same deck on rank 0.
+solver's stream, max over ranks). ``roofline`` is the whole outer iteration
+against HBM with the algorithmic 3*s bytes per update (s = 4 in the FP32
+form, 8 in FP64): one read of the intensities for gradient and residual,
+one write from the sweep, one read for the moments; ``hbm_kernels`` holds
+each streaming kernel's own fraction. ``e2e`` is the same metric through the
+public API from host buffers: on the 3D block, set the initial field from
+pinned host memory, K outer iterations, read every result field back; on
+the 2D cell, the same with a solve to residual 1e-8. Under torchrun each
+rank solves an independent seeded problem (weak scaling, no collective on
+the data path). ``--impl reference`` times the reference's own CPU solver
+(oracle/_ref/BTE_CPU) on the 2D decks; the reference cannot read 3D meshes,
+so on the 3D block it times the CPU restatement of its algorithm (the
+oracle port) on a bounded sample, labelled as such.
 """
 from __future__ import annotations
 
@@ -139,11 +148,14 @@ def kernel_algorithmic_bytes(name: str, s: int, dim: int, nb: int, nd: int, nc: 
     return None
 
 
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
-# one ncu --set full capture of each kernel of the third outer iteration on
-# the 17,939-cell 40-band cell, FP32 form, 8 bands per sweep CTA.
-NCU_TRAFFIC_CONFIG2_FP32 = {"residual": 747.134464e6, "sweep": 392.428032e6, "gradient": 509.03552e6,
-                            "moments": 517.57696e6, "pcg": 1.89568e6}
+# DRAM bytes per band*direction*cell update of each transport kernel
+# (dram__bytes_read.sum + dram__bytes_write.sum of one launch divided by the
+# updates it processed), from ncu captures; the profiles/ summaries give the
+# commands. The 2D figures are from the full-size 17,939-cell cell.
+NCU_TRAFFIC_PER_UPDATE = {
+    ("config2", "fp32"): {"residual": 747.134464e6 / 45921280, "sweep": 392.428032e6 / 45921280,
+                          "gradient": 509.03552e6 / 45921280, "moments": 517.57696e6 / 45921280},
+}
 
 
 def macro_nnz(deck) -> int:
@@ -173,9 +185,24 @@ def whole_job_rate(units_local: float, seconds_local: float, world: int, device)
     return units / ranks_reduce(seconds_local, "max", world, device)
 
 
+def workload_config(args, deck, desc: str, nb: int, nd: int) -> dict:
+    """The workload as both arms print it (same keys and values)."""
+    nc = deck.mesh.n_cells
+    s_bytes = 4 if args.precision == "fp32" else 8
+    return {"workload": desc, "cells": nc, "bands": nb, "directions": nd, "updates_per_step": nb * nd * nc,
+            "precision": args.precision,
+            "l2": f"band state {nb * nd * nc * s_bytes / 1e6:.0f} MB per copy, larger than the 126 MB L2"}
+
+
+def directions_of(deck) -> int:
+    return 4 * deck.n_phi if deck.material_dim == 2 else 8 * deck.n_theta * deck.n_phi
+
+
+METRIC = "band*dir*cell updates/s (time to residual 1e-8 alongside); FP32-mixed vs FP64 on 1 B200"
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
     import torch
-    import torch.distributed as dist
 
     import giftbte_b200 as g
 
@@ -184,28 +211,33 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     # a stream of its own (capturable: the library replays its transport
     # stage as a CUDA graph on it)
     stream = torch.cuda.Stream()
-    # replicas: a seeded cell per rank; direction shards: one cell, its
-    # directions split over the ranks
+    # replicas: a seeded problem per rank; direction shards: one problem,
+    # its directions split over the ranks
     by_dirs = args.shard == "directions"
     deck, desc = build_deck(args.workload, seed=0 if by_dirs else rank, h_nm=args.h_nm)
     nc = deck.mesh.n_cells
     prec = g.GBTE_FP32_MIXED if args.precision == "fp32" else g.GBTE_FP64
     s_bytes = 4 if prec == g.GBTE_FP32_MIXED else 8
 
+    t_setup = time.perf_counter()
     solver = g.StaticBTESynthetic.from_deck(deck, precision=prec, device=local_rank, profile=0,
                                             stream=ctypes_stream(stream), cell_order=args.cell_order,
                                             sweep_bands=args.sweep_bands, sweep_vector=args.sweep_vector,
                                             sweep_kernel=args.sweep_kernel)
+    setup_s = time.perf_counter() - t_setup
     nb, nd = solver.num_bands, solver.num_directions
     upd_per_step = nb * nd * nc
     upd_local = upd_per_step
     if by_dirs:
         upd_local = nb * attach_shard(solver, rank, world) * nc
-    # warm-up (not timed)
+    # warm-up (not timed; the first outer iteration also runs the
+    # autotuners and the next captures the transport stage as a CUDA graph)
     solver.solve(max_iter=args.warmup, err_temp=0.0, err_flux=0.0)
     torch.cuda.synchronize()
     # timed region: exactly K outer iterations (margins 0, so none stops early)
     if world > 1:
+        import torch.distributed as dist
+
         dist.barrier()
     torch.cuda.synchronize()
     clocks = ClockSampler(local_rank)
@@ -221,9 +253,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     ms = ranks_reduce(ms_local, "max", world, "cuda")
     value = whole_job_rate(upd_local * args.steps, ms_local * 1e-3, world, "cuda")
 
-    # roofline of the dominant kernel, and of every streaming kernel: per-launch
-    # CUDA events on the solver's stream, from K more iterations launched
-    # kernel by kernel (after the timed region)
+    # per-kernel times: CUDA events on the solver's stream around every
+    # launch of K more iterations launched kernel by kernel (after the timed
+    # region)
     solver.set_profile(True)
     kst = solver.solve(max_iter=args.steps, err_temp=0.0, err_flux=0.0)
     solver.set_profile(False)
@@ -233,61 +265,78 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     total_ms = sum(v["ms"] for v in kern.values())
     dim = 2 if deck.mesh.nodes.shape[1] == 2 else 3
     nnz = macro_nnz(deck)
+    traffic_per_update = NCU_TRAFFIC_PER_UPDATE.get((args.workload, args.precision), {})
 
     def kernel_roofline(name):
         k = kern[name]
         per_launch_ms = k["ms"] / k["launches"]
+        launches_per_step = k["launches"] / args.steps
         alg = kernel_algorithmic_bytes(name, s_bytes, dim, nb, nd, nc, nnz)
+        if alg and name in ("gradient", "residual", "sweep", "moments"):
+            alg = alg / launches_per_step  # direction batches: one launch covers a batch
         achieved = alg / (per_launch_ms * 1e-3) / 1e9 if alg else None
-        traffic = None
-        if args.workload == "config2" and prec == g.GBTE_FP32_MIXED:
-            traffic = NCU_TRAFFIC_CONFIG2_FP32.get(name)
+        tr = traffic_per_update.get(name)
         return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                "traffic": traffic, "algorithmic_bytes": alg, "launch_ms": per_launch_ms,
-                "kernel_share": k["ms"] / total_ms}
+                "traffic": tr * upd_per_step / launches_per_step if tr else None, "algorithmic_bytes": alg,
+                "launch_ms": per_launch_ms, "kernel_share": k["ms"] / total_ms}
 
+    # the whole outer iteration against HBM: 3 s algorithmic bytes per
+    # band*direction*cell update (read e for gradient and residual, write
+    # the sweep's update, read e for the moments pass)
+    ms_step = ms / args.steps
+    alg_step = 3 * s_bytes * upd_per_step
+    achieved = alg_step / (ms_step * 1e-3) / 1e9
+    tr_step = sum(traffic_per_update.values()) * upd_per_step if traffic_per_update else None
     dname = max(kern.items(), key=lambda kv: kv[1]["ms"])[0]
-    roofline = kernel_roofline(dname)
-    if dname == "pcg":
-        roofline["note"] = ("the macro CG is latency-bound (two cluster barriers per CG iteration on a "
-                            "shared-memory-resident system), not bandwidth-bound: its HBM fraction is "
-                            "near zero by construction; see hbm_kernels for the streaming kernels")
+    roofline = {"kernel": "outer iteration (transport stage replayed as one CUDA graph + macro correction)",
+                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": peak_kind, "traffic": tr_step, "algorithmic_bytes": alg_step,
+                "bytes_per_update": 3 * s_bytes, "launch_ms": ms_step, "dominant_kernel": dname,
+                "dominant_kernel_share": kern[dname]["ms"] / total_ms}
     hbm_kernels = {n: kernel_roofline(n) for n in ("residual", "sweep", "gradient", "moments") if n in kern}
     kernel_table = {k: {"ms_per_launch": v["ms"] / v["launches"], "launches": v["launches"],
-                        "share": v["ms"] / sum(x["ms"] for x in kern.values())} for k, v in kern.items()}
-    solver.close()
+                        "share": v["ms"] / total_ms} for k, v in kern.items()}
 
-    # end to end through the public API: host in, solve to 1e-8, host out
-    e2e, ttr = e2e_solves(args, deck, prec, local_rank, world, rank if by_dirs else None)
+    # end to end through the public API
+    if args.workload == "config3":
+        e2e = e2e_iterations(args, solver, deck, world)
+        ttr = None
+        solver.close()
+    else:
+        solver.close()
+        e2e, ttr = e2e_solves(args, deck, prec, local_rank, world, rank if by_dirs else None)
 
     out = None
     if rank == 0:
         fp64 = None
         if args.compare_fp64 and prec == g.GBTE_FP32_MIXED:
-            fp64 = fp64_reference_run(args, deck, local_rank)
+            if args.workload == "config3":
+                fp64 = fp64_rate_run(args, deck, local_rank, value)
+            else:
+                fp64 = fp64_reference_run(args, deck, local_rank)
         cpu = cpu_baseline(args, deck) if world == 1 else None
+        cfg = workload_config(args, deck, desc, nb, nd)
+        cfg.update({"cell_order": "morton" if args.cell_order == 0 else "deck",
+                    "parallelism": (f"direction shards x{world} of one problem (NCCL all-reduce of the moments "
+                                    "and boundary values every outer iteration)" if by_dirs and world > 1 else
+                                    f"replicas x{world} (independent seeded problems)" if world > 1 else "1 GPU")})
         out = {
-            "metric": "band*dir*cell updates/s (time to residual 1e-8 alongside); FP32-mixed vs FP64 on 1 B200",
+            "metric": METRIC,
             "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "strong" if by_dirs else "weak", "vs_baseline": None,
             "dtype": "f32" if prec == g.GBTE_FP32_MIXED else "f64",
             "data": "synthetic: seeded mesh and band table generated in-process (no dataset)",
-            "config": {"workload": desc, "cells": nc, "bands": nb, "directions": nd,
-                       "updates_per_step": upd_per_step, "precision": args.precision,
-                       "cell_order": "morton" if args.cell_order == 0 else "deck",
-                       "sweep_bands": st.get("sweep_bands"), "sweep_stage_levels": st.get("sweep_stage_levels"),
+            "config": cfg,
+            "tuning": {"sweep_bands": st.get("sweep_bands"), "sweep_stage_levels": st.get("sweep_stage_levels"),
                        "sweep_vector": st.get("sweep_vector"), "sweep_threads": st.get("sweep_threads"),
-                       "sweep_kernel": {1: "block", 2: "warp"}.get(st.get("sweep_kernel")),
-                       "l2": f"band state {upd_per_step * s_bytes / 1e6:.0f} MB per copy, larger than the 126 MB L2",
-                       "parallelism": (f"direction shards x{world} of one cell (NCCL all-reduce of the moments and "
-                                       "boundary values every outer iteration)" if by_dirs and world > 1 else
-                                       f"replicas x{world} (independent seeded cells)" if world > 1 else "1 GPU")},
+                       "sweep_kernel": {1: "block", 2: "warp", 3: "wide"}.get(st.get("sweep_kernel")),
+                       "gradient_dirs": st.get("gradient_dirs"), "direction_batch": st.get("direction_batch")},
             "roofline": roofline, "hbm_kernels": hbm_kernels, "kernels": kernel_table, "cpu_baseline": cpu,
-            "e2e": e2e,
-            "time_to_residual": ttr, "gpu_launches": int(st["kernel_launches"]), "clocks": clk,
+            "e2e": e2e, "time_to_residual": ttr, "gpu_launches": int(st["kernel_launches"]), "clocks": clk,
             "macro": {"ms_per_step": st["macro_ms"] / args.steps, "cg_iterations": st["macro_cg_iterations"]},
+            "setup_s": setup_s,
         }
         if fp64 is not None:
             out["fp64"] = fp64
@@ -310,6 +359,64 @@ def attach_shard(solver, rank: int, world: int) -> int:
     return n
 
 
+def e2e_iterations(args, solver, deck, world):
+    """End to end through the public API on a handle already created: the
+    initial field from pinned host memory (gbte_set_initial), K outer
+    iterations (gbte_solve_with), every result field read back
+    (gbte_get_fields), repeated e2e_steps times; updates/s over the wall
+    time of the calls."""
+    import torch
+
+    nc = deck.mesh.n_cells
+    nb = solver.num_bands
+    T0 = torch.full((nc,), float(deck.tref), dtype=torch.float64).pin_memory().numpy()
+    reps = max(1, args.e2e_steps)
+    times, ups = [], []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        solver.set_initial(T0)
+        st = solver.solve(max_iter=args.steps, err_temp=0.0, err_flux=0.0)
+        solver.fields()
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+        ups.append(st["updates"])
+    return {"value": whole_job_rate(sum(ups), sum(times), world, "cuda"), "unit": "updates/s",
+            "h2d_bytes_per_step": int(nc * 8 / args.steps),
+            "d2h_bytes_per_step": int(nc * 8 * (2 + 3 + nb) / args.steps), "steps": args.steps * reps,
+            "step": f"set_initial from pinned host + {args.steps} outer iterations + read all fields, x{reps}; "
+                    "bytes per step are the call's copies over its iterations"}
+
+
+def fp64_rate_run(args, deck, device, fp32_value):
+    """The plain FP64 GPU form on the same 3D block: device updates/s over a
+    few outer iterations after warm-up (time to residual 1e-8 of both forms
+    is measured separately: it takes hundreds of iterations)."""
+    import torch
+
+    import giftbte_b200 as g
+
+    k = max(1, min(args.steps, args.fp64_steps))
+    stream = torch.cuda.Stream()
+    s = g.StaticBTESynthetic.from_deck(deck, precision=g.GBTE_FP64, device=device, stream=ctypes_stream(stream),
+                                       cell_order=args.cell_order)
+    s.solve(max_iter=2, err_temp=0.0, err_flux=0.0)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    st = s.solve(max_iter=k, err_temp=0.0, err_flux=0.0)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    s.close()
+    v = st["updates"] / (ms * 1e-3)
+    return {"fp64": {"updates_per_s": v, "ms_per_step": ms / k, "steps": k,
+                     "direction_batch": st.get("direction_batch"), "gradient_dirs": st.get("gradient_dirs"),
+                     "sweep_kernel": {1: "block", 2: "warp", 3: "wide"}.get(st.get("sweep_kernel"))},
+            "fp32_over_fp64_per_iteration": fp32_value / v}
+
+
 def e2e_solves(args, deck, prec, device, world, shard_rank=None):
     import torch
 
@@ -325,7 +432,7 @@ def e2e_solves(args, deck, prec, device, world, shard_rank=None):
         attach_shard(solver, shard_rank, world)
     T0 = torch.full((nc,), float(deck.tref), dtype=torch.float64).pin_memory().numpy()
     out = {k: np.zeros(n) for k, n in (("E", nc), ("T", nc), ("q", 3 * nc), ("Tb", nb * nc))}
-    nsteps = max(1, min(args.steps, args.e2e_steps))
+    nsteps = max(2, min(args.steps, max(2, args.e2e_steps)))
     times, iters, ups = [], [], []
     for _ in range(nsteps):
         torch.cuda.synchronize()
@@ -373,57 +480,89 @@ def fp64_reference_run(args, deck, device):
     return res
 
 
-def cpu_baseline(args, deck):
-    """The oracle restatement (multithreaded FP64 CPU port) timed on the
-    host cores on a bounded sample: one outer iteration of the same deck,
-    measured as the difference of a 2-iteration and a 1-iteration run."""
+def cpu_sample_deck(args, deck):
+    """The bounded CPU sample of a workload: the 2D cell itself; for the 3D
+    block, a 50 x 50 x 5 nm piece of it (same spacing, jitter, bands and
+    directions; 4,800 tets, 1/400 of the block), whose per-update rate
+    stands for the block's."""
+    if args.workload != "config3":
+        return deck, "the same deck"
+    from giftbte_b200 import decks
+
+    h = args.h_nm or 2.5
+    d = decks.config3_deck(h_nm=h, size_nm=(50.0, 50.0, 5.0), seed=1)
+    return d, (f"a 50 x 50 x 5 nm piece of the block at h = {h} nm ({d.mesh.n_cells} tets), same bands and "
+               "directions")
+
+
+def timed_port_iterations(deck, warm: int, k: int) -> float:
+    """Seconds per outer iteration of the oracle port (multithreaded FP64
+    CPU restatement): the difference of a (warm + k)- and a warm-iteration
+    run over k."""
     import oracle
 
+    t = []
+    for n in (warm, warm + k):
+        t0 = time.perf_counter()
+        oracle.solve(deck, max_iter=n, err_T=0.0, err_q=0.0)
+        t.append(time.perf_counter() - t0)
+    return max(t[1] - t[0], 1e-9) / k
+
+
+def cpu_baseline(args, deck):
+    """The oracle restatement (multithreaded FP64 CPU port) timed on the
+    host cores on a bounded sample: one outer iteration of the workload's
+    CPU sample, measured as the difference of a 2-iteration and a
+    1-iteration run."""
     if args.skip_cpu:
         return None
     try:
-        t = []
-        for n in (1, 2):
-            t0 = time.perf_counter()
-            oracle.solve(deck, max_iter=n, err_T=0.0, err_q=0.0)
-            t.append(time.perf_counter() - t0)
-        per_iter = max(t[1] - t[0], 1e-9)
-        upd = deck.bands.n_bands * (4 * deck.n_phi if deck.material_dim == 2 else 8 * deck.n_theta * deck.n_phi) \
-            * deck.mesh.n_cells
+        sample, what = cpu_sample_deck(args, deck)
+        per_iter = timed_port_iterations(sample, 1, 1)
+        upd = sample.bands.n_bands * directions_of(sample) * sample.mesh.n_cells
         return {"value": upd / per_iter, "unit": "updates/s", "cores": os.cpu_count(), "kind": "port",
-                "sample": "one outer iteration of the same deck (difference of 2- and 1-iteration runs)"}
+                "sample": f"one outer iteration of {what} (difference of 2- and 1-iteration runs)"}
     except Exception as e:  # the baseline must not take the GPU line down
         return {"value": None, "unit": "updates/s", "cores": os.cpu_count(), "kind": "port",
                 "sample": f"failed: {e}"}
 
 
 def run_reference(args, rank: int):
-    """The unmodified reference CPU solver on the same deck (1 MPI rank via
-    the single-rank stub build), timed from its own per-iteration
-    'Time taken by inner loop' trace."""
+    """The reference's own CPU implementation of the path on the host cores,
+    for the same metric and config as the GPU arm, W warm-up and K timed
+    outer iterations. 2D decks: the unmodified compiled reference (1 MPI
+    rank through the single-rank stub build), timed from its own
+    per-iteration 'Time taken by inner loop' trace. The 3D block: the
+    reference's public release cannot read 3D meshes, so the oracle port
+    (its algorithm restated, multithreaded FP64) on the bounded sample of
+    cpu_sample_deck stands in, labelled kind 'port'."""
     if rank != 0:
         return None
     import oracle
 
-    if args.workload == "config3":
-        return {"impl": "reference", "unavailable": "the reference's public release has no 3D mesh code "
-                                                    "(3D decks cannot be read by it)"}
     deck, desc = build_deck(args.workload, seed=0, h_nm=args.h_nm)
     nb = deck.bands.n_bands
-    nd = 4 * deck.n_phi if deck.material_dim == 2 else 8 * deck.n_theta * deck.n_phi
+    nd = directions_of(deck)
     upd = nb * nd * deck.mesh.n_cells
-    k = max(1, min(args.steps, args.ref_steps))
-    w = min(args.warmup, 1)
-    base = {"impl": "reference", "metric": "band*dir*cell updates/s (time to residual 1e-8 alongside); "
-            "FP32-mixed vs FP64 on 1 B200", "unit": "updates/s", "higher_is_better": True, "n_gpus": 1,
+    k = max(1, args.steps)
+    w = max(0, args.warmup)
+    base = {"impl": "reference", "metric": METRIC, "unit": "updates/s", "higher_is_better": True, "n_gpus": 1,
             "steps": k, "warmup": w, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic: the same seeded deck", "config": {"workload": desc}}
-    if not os.path.exists(oracle.REF_BIN):
-        # the restatement stands in when the reference binary was not built
-        cpu = cpu_baseline(args, deck)
-        base.update({"value": cpu["value"], "cpu_baseline": cpu,
-                     "e2e": {"value": cpu["value"], "unit": "updates/s", "h2d_bytes_per_step": 0,
-                             "d2h_bytes_per_step": 0}})
+            "data": "synthetic: seeded mesh and band table generated in-process (no dataset)",
+            "config": workload_config(args, deck, desc, nb, nd)}
+    if args.workload == "config3" or not os.path.exists(oracle.REF_BIN):
+        sample, what = cpu_sample_deck(args, deck)
+        per_iter = timed_port_iterations(sample, max(1, w), k)
+        s_upd = sample.bands.n_bands * directions_of(sample) * sample.mesh.n_cells
+        value = s_upd / per_iter
+        why = ("the reference cannot read 3D meshes (its public release has no 3D mesh code)"
+               if args.workload == "config3" else "the reference binary was not built")
+        base.update({"value": value, "ms_per_step": upd / value * 1e3,
+                     "cpu_baseline": {"value": value, "unit": "updates/s", "cores": os.cpu_count(), "kind": "port",
+                                      "sample": f"{k} outer iterations of {what} after {max(1, w)} warm-up "
+                                                f"(difference of two runs); {why}, so the CPU restatement of its "
+                                                "algorithm is timed"},
+                     "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
         return base
     work = tempfile.mkdtemp(prefix="gbte_ref_")
     try:
@@ -556,7 +695,7 @@ def run_config5(args, rank: int):
                                     "(device time of their outer iterations)"},
         "batch_over_sequential": value / seq, "sweep_bands_autotuned": st.get("sweep_bands"),
         "sweep_vector_autotuned": st.get("sweep_vector"), "sweep_threads_autotuned": st.get("sweep_threads"),
-        "sweep_kernel_autotuned": {1: "block", 2: "warp"}.get(st.get("sweep_kernel")),
+        "sweep_kernel_autotuned": {1: "block", 2: "warp", 3: "wide"}.get(st.get("sweep_kernel")),
         "gpu_launches": int(st["kernel_launches"]), "clocks": clk,
     }
 
@@ -568,7 +707,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
-    ap.add_argument("--workload", choices=["config2", "config1", "config3", "config4", "config5"], default="config2")
+    ap.add_argument("--workload", choices=["config3", "config2", "config1", "config4", "config5"], default="config3")
     ap.add_argument("--adj-residual", type=float, default=1e-8, help="config4: forward margins and adjoint tolerance")
     ap.add_argument("--adj-max-iter", type=int, default=20000, help="config4: adjoint iteration cap")
     ap.add_argument("--batch", type=int, default=256, help="config5: number of independent cells")
@@ -577,13 +716,15 @@ def main():
                     help="bands per sweep CTA (1..32); 0 lets the autotuner pick on the first iteration")
     ap.add_argument("--sweep-vector", type=int, choices=[0, 1, 2, 4], default=0,
                     help="bands per sweep thread; 0 lets the autotuner pick")
-    ap.add_argument("--sweep-kernel", type=int, choices=[0, 1, 2], default=0,
-                    help="1: block sweep kernel, 2: warp-independent kernel, 0: the autotuner's pick")
+    ap.add_argument("--sweep-kernel", type=int, choices=[0, 1, 2, 3], default=0,
+                    help="1: block sweep kernel, 2: warp-independent kernel, 3: wide-level kernel, "
+                         "0: the autotuner's pick")
     ap.add_argument("--cell-order", type=int, choices=[0, 1], default=0,
                     help="0: cells renumbered along a Morton curve inside the library; 1: the deck's order")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=1,
+                    help="repetitions of the end-to-end call sequence (2D: solves to 1e-8, at least 2, at most K)")
     ap.add_argument("--max-iter-e2e", type=int, default=2000)
-    ap.add_argument("--ref-steps", type=int, default=2)
+    ap.add_argument("--fp64-steps", type=int, default=5, help="3D block: timed outer iterations of the FP64 form")
     ap.add_argument("--ref-timeout", type=float, default=1500.0)
     ap.add_argument("--no-fp64", dest="compare_fp64", action="store_false")
     ap.add_argument("--skip-cpu", action="store_true")
