@@ -66,7 +66,9 @@ class BCTable(ctypes.Structure):
 
 
 class AngleSpec(ctypes.Structure):
-    _fields_ = [("method", ctypes.c_int), ("n_theta", ctypes.c_int), ("n_phi", ctypes.c_int)]
+    _fields_ = [("method", ctypes.c_int), ("n_theta", ctypes.c_int), ("n_phi", ctypes.c_int),
+                ("num_directions", ctypes.c_int), ("direction_xyz", _c_dbl_p), ("weight", _c_dbl_p),
+                ("solid_angle", ctypes.c_double)]
 
 
 class Options(ctypes.Structure):

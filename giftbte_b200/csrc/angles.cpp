@@ -53,6 +53,21 @@ void gauss_legendre(double a, double b, int n, std::vector<double> &x, std::vect
 
 }  // namespace
 
+Error explicit_angles(int n, const double *xyz, const double *weight, double solid, Angles &A) {
+    A = Angles();
+    if (n <= 0 || !xyz || !weight) return {-1, "explicit angles: need num_directions > 0, direction_xyz and weight"};
+    if (!(solid > 0)) return {-1, "explicit angles: solid_angle must be positive"};
+    A.nd = n;
+    A.solid = solid;
+    for (int d = 0; d < n; d++) {
+        A.sx.push_back(xyz[3 * d]);
+        A.sy.push_back(xyz[3 * d + 1]);
+        A.sz.push_back(xyz[3 * d + 2]);
+        A.w.push_back(weight[d] / solid);
+    }
+    return {0, ""};
+}
+
 Error make_angles(int method, int ntheta, int nphi, int dm, Angles &A) {
     A = Angles();
     if (nphi <= 0 || (dm == 3 && ntheta <= 0)) return {-1, "Ntheta/Nphi must be positive"};

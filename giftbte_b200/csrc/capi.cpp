@@ -115,7 +115,9 @@ int create_common(const gbte::RawMesh &raw_in, const gbte::Bands &bands_in, cons
     int brc = finish_bands(bands);
     if (brc != GBTE_OK) return brc;
     gbte::Angles ang;
-    gbte::Error e = gbte::make_angles(as.method, as.n_theta, as.n_phi, bands.material_dim, ang);
+    gbte::Error e = as.method == 0 ? gbte::explicit_angles(as.num_directions, as.direction_xyz, as.weight,
+                                                           as.solid_angle, ang)
+                                   : gbte::make_angles(as.method, as.n_theta, as.n_phi, bands.material_dim, ang);
     if (e.code) return fail(nullptr, e), status_of(e.code);
     if (opt.cell_order != 0 && opt.cell_order != 1)
         return fail(nullptr, {-1, "cell_order must be 0 (automatic) or 1 (caller's order)"}), GBTE_ERR_ARG;
@@ -249,7 +251,9 @@ static int inspect_common(const gbte::RawMesh &raw_in, const gbte::Bands &bands_
     int brc = finish_bands(bands);
     if (brc != GBTE_OK) return brc;
     gbte::Angles ang;
-    gbte::Error e = gbte::make_angles(as.method, as.n_theta, as.n_phi, bands.material_dim, ang);
+    gbte::Error e = as.method == 0 ? gbte::explicit_angles(as.num_directions, as.direction_xyz, as.weight,
+                                                           as.solid_angle, ang)
+                                   : gbte::make_angles(as.method, as.n_theta, as.n_phi, bands.material_dim, ang);
     if (e.code) return fail(nullptr, e), status_of(e.code);
     // the cell order gbte_create uses by default
     std::vector<int> perm;

@@ -157,6 +157,8 @@ void reorder_cells(RawMesh &raw, const std::vector<int> &perm);
 Error make_union(const std::vector<RawMesh> &meshes, const std::vector<BCs> &bcs, RawMesh &out, BCs &out_bcs);
 
 Error make_angles(int method, int ntheta, int nphi, int material_dim, Angles &out);
+// an explicit direction set: unit vectors [n * 3], weights summing to the solid angle
+Error explicit_angles(int n, const double *xyz, const double *weight, double solid, Angles &out);
 Error build_flat_mesh(const RawMesh &raw, const BCs &bcs, const Bands &bands, FlatMesh &out);
 void build_schedule(const FlatMesh &m, const Angles &a, Schedule &out, int nthreads);
 // min_ring: the smallest ring (rounded up to a power of two and to the

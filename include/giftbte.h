@@ -116,9 +116,18 @@ typedef struct {
 } gbte_bc_table;
 
 typedef struct {
-    int method;   /* 1 = CADOM (uniform midpoint), 2 = Gauss-Legendre */
+    int method;   /* 1 = CADOM (uniform midpoint), 2 = Gauss-Legendre, 0 = the explicit list below */
     int n_theta;
     int n_phi;
+    /* method 0: the directions and weights as a caller already holds them
+     * (BTEAngle::direction / weight / SolidAngle, includes/BTEAngle/
+     * BTEAngle.h:12-14); the solver uses s_d = direction_d and the mode
+     * weight weight_d / solid_angle as the reference does
+     * (StaticBTESynthetic.cpp:603-610) */
+    int num_directions;
+    const double *direction_xyz;  /* [num_directions * 3] */
+    const double *weight;         /* [num_directions] */
+    double solid_angle;           /* 2 pi (2D material) or 4 pi (3D material) */
 } gbte_angle_spec;
 
 typedef struct {

@@ -19,6 +19,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle_restate.so")
 REF_BIN = os.path.join(HERE, "_ref", "BTE_CPU")
+# the reference program with the B200 solver class dropped in (make -C oracle dropin)
+DROPIN_BIN = os.path.join(HERE, "_ref", "BTE_B200")
 
 _lib = None
 
@@ -31,6 +33,7 @@ def build(reference_root: Optional[str] = None) -> None:
     reference_root = reference_root or os.environ.get("GIFTBTE_REFERENCE", "")
     if reference_root and os.path.isdir(os.path.join(reference_root, "src")):
         subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF={reference_root}", "-j8"])
+        subprocess.check_call(["make", "-s", "-C", HERE, "dropin", f"REF={reference_root}", "-j8"])
 
 
 def lib():
@@ -118,14 +121,15 @@ def solve(deck, T0: Optional[np.ndarray] = None, max_iter: Optional[int] = None,
             "iters": int(iters.value), "err": err}
 
 
-def run_reference(deck_root: str, timeout: float = 3600.0) -> Dict[str, np.ndarray]:
-    """Run the compiled reference in ``deck_root`` (which holds ``input/``)
-    and parse its result files (17 significant digits, see
-    oracle/ref_shim/full_precision.cpp)."""
-    if not os.path.exists(REF_BIN):
-        raise FileNotFoundError(REF_BIN)
+def run_reference(deck_root: str, timeout: float = 3600.0, binary: Optional[str] = None) -> Dict[str, np.ndarray]:
+    """Run the compiled reference (or ``binary``, e.g. DROPIN_BIN) in
+    ``deck_root`` (which holds ``input/``) and parse its result files (17
+    significant digits, see oracle/ref_shim/full_precision.cpp)."""
+    binary = binary or REF_BIN
+    if not os.path.exists(binary):
+        raise FileNotFoundError(binary)
     with open(os.path.join(deck_root, "ref_run.log"), "w") as log:
-        subprocess.run([REF_BIN], cwd=deck_root, stdout=log, stderr=subprocess.STDOUT,
+        subprocess.run([binary], cwd=deck_root, stdout=log, stderr=subprocess.STDOUT,
                        timeout=timeout, check=True)
     return read_reference_outputs(deck_root)
 
