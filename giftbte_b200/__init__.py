@@ -79,7 +79,7 @@ class Options(ctypes.Structure):
                 ("sweep_far_slots", ctypes.c_int), ("direction_batch", ctypes.c_int),
                 ("cell_scatter", _c_dbl_p), ("cell_order", ctypes.c_int), ("order", ctypes.c_int),
                 ("scheme", ctypes.c_int), ("macro_exact", ctypes.c_int), ("sweep_vector", ctypes.c_int),
-                ("sweep_kernel", ctypes.c_int), ("gradient_dirs", ctypes.c_int)]
+                ("sweep_kernel", ctypes.c_int), ("gradient_dirs", ctypes.c_int), ("residual_form", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -92,7 +92,8 @@ class Stats(ctypes.Structure):
                 ("kernel_ms", ctypes.c_double * 16), ("kernel_count", ctypes.c_longlong * 16),
                 ("sweep_bands", ctypes.c_int), ("direction_batch", ctypes.c_int),
                 ("sweep_stage_levels", ctypes.c_int), ("sweep_vector", ctypes.c_int),
-                ("sweep_threads", ctypes.c_int), ("sweep_kernel", ctypes.c_int), ("gradient_dirs", ctypes.c_int)]
+                ("sweep_threads", ctypes.c_int), ("sweep_kernel", ctypes.c_int), ("gradient_dirs", ctypes.c_int),
+                ("residual_form", ctypes.c_int)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("kernel_ms", "kernel_count")}

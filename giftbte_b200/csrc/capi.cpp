@@ -165,9 +165,12 @@ int create_common(const gbte::RawMesh &raw_in, const gbte::Bands &bands_in, cons
         return fail(nullptr, {-1, "sweep_kernel must be 0 (automatic), 1 (block), 2 (warp) or 3 (wide)"}),
                GBTE_ERR_ARG;
     cfg.sweep_kernel = opt.sweep_kernel;
-    if (opt.gradient_dirs != 0 && opt.gradient_dirs != 1 && opt.gradient_dirs != 2 && opt.gradient_dirs != 4)
-        return fail(nullptr, {-1, "gradient_dirs must be 0 (automatic), 1, 2 or 4"}), GBTE_ERR_ARG;
+    if (opt.gradient_dirs < 0 || opt.gradient_dirs > 6 || opt.gradient_dirs == 3)
+        return fail(nullptr, {-1, "gradient_dirs must be 0 (automatic), 1, 2, 4, 5 or 6"}), GBTE_ERR_ARG;
     cfg.gradient_dirs = opt.gradient_dirs;
+    if (opt.residual_form != 0 && opt.residual_form != 1 && opt.residual_form != 5 && opt.residual_form != 6)
+        return fail(nullptr, {-1, "residual_form must be 0 (automatic), 1, 5 or 6"}), GBTE_ERR_ARG;
+    cfg.residual_form = opt.residual_form;
     cfg.device = opt.device;
     cfg.stream = (cudaStream_t)opt.stream;
     if (opt.precision != GBTE_FP64 && opt.precision != GBTE_FP32_MIXED)
@@ -510,6 +513,7 @@ int gbte_solve(gbte_handle *h, gbte_stats *st) {
             st->sweep_threads = h->solver.last_sweep_threads_;
             st->sweep_kernel = h->solver.last_sweep_warp_ == 1 ? 2 : h->solver.last_sweep_warp_ == 2 ? 3 : 1;
             st->gradient_dirs = h->solver.last_grad_dirs_;
+            st->residual_form = h->solver.last_res_form_;
             for (int k = 0; k < GBTE_NUM_KERNELS && k < gbte::K_NUM; k++) {
                 st->kernel_ms[k] = s.kernel_ms[k];
                 st->kernel_count[k] = s.kernel_count[k];

@@ -427,6 +427,79 @@ __global__ void __launch_bounds__(256) k_gradient_md(DMesh m, DPhys p, const flo
     }
 }
 
+// Warp-per-cell form of the LSQ gradient: one warp per (cell, group of
+// DS * DG directions), DS = 32 / nbc direction slots with nbc = nb / 4 <= 32
+// band groups; lane l covers bands 4 (l % nbc) .. 4 (l % nbc) + 3 of DG
+// directions of slot l / nbc (lanes past DS * nbc idle). Every lane walks
+// the same stencil, so a stencil entry is one broadcast load per warp, the
+// loop does not diverge, and a neighbour's band row is one contiguous read
+// per direction. Per band and direction the arithmetic is k_gradient8's.
+template <typename S, int DIM, int DG>
+__global__ void __launch_bounds__(256) k_gradient_wc(DMesh m, DPhys p, const float4 *__restrict__ pk,
+                                                     const S *__restrict__ eps, S *__restrict__ g, int d0, int ndb) {
+    constexpr int BC = 4;
+    const int nb = p.nb, nc = m.nc, nbc = nb / BC;
+    const int DS = 32 / nbc;
+    const int lane = threadIdx.x & 31, slot = lane / nbc, bc = lane % nbc;
+    const bool on = slot < DS;
+    const int dpw = DS * DG;
+    const size_t items = (size_t)((ndb + dpw - 1) / dpw) * nc;
+    const size_t wstr = ((size_t)gridDim.x * blockDim.x) >> 5;
+    for (size_t w = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < items; w += wstr) {
+        const int c = (int)(w % nc), grp = (int)(w / nc);
+        const S *ed[DG];
+        S ec[DG][BC], gx[DG][BC], gy[DG][BC], gz[DG][BC];
+#pragma unroll
+        for (int k = 0; k < DG; k++) {
+            const int dl = min(grp * dpw + slot * DG + k, ndb - 1);
+            ed[k] = eps + (size_t)(d0 + dl) * nc * nb + BC * bc;
+            ld8(ed[k] + (size_t)c * nb, ec[k]);
+#pragma unroll
+            for (int i = 0; i < BC; i++) gx[k][i] = gy[k][i] = gz[k][i] = 0;
+        }
+        const int q1 = m.nbr_ptr[c + 1];
+        for (int q = m.nbr_ptr[c]; q < q1; q += 4) {
+            S wx[4], wy[4], wz[4];
+            int jn[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                if (q + u < q1)
+                    stencil_entry(m, pk, q + u, wx[u], wy[u], wz[u], jn[u]);
+                else
+                    wx[u] = wy[u] = wz[u] = 0, jn[u] = c;
+            }
+            S e4[4][DG][BC];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int k = 0; k < DG; k++) ld8(ed[k] + (size_t)jn[u] * nb, e4[u][k]);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                if (q + u >= q1) break;
+#pragma unroll
+                for (int k = 0; k < DG; k++)
+#pragma unroll
+                    for (int i = 0; i < BC; i++) {
+                        const S de = e4[u][k][i] - ec[k][i];
+                        gx[k][i] += wx[u] * de;
+                        gy[k][i] += wy[u] * de;
+                        if (DIM == 3) gz[k][i] += wz[u] * de;
+                    }
+            }
+        }
+        if (!on) continue;
+#pragma unroll
+        for (int k = 0; k < DG; k++) {
+            const int dl = grp * dpw + slot * DG + k;
+            if (dl >= ndb) break;
+            S *gp = g + ((size_t)dl * nc + c) * DIM * nb + BC * bc;
+            st8(gp, gx[k]);
+            st8(gp + nb, gy[k]);
+            if (DIM == 3) st8(gp + 2 * nb, gz[k]);
+        }
+    }
+}
+
 // Band-independent part of the face fluxes of the FP32 form's base field:
 // B[d][c] = (1/s_c) sum_f A_f/V (s.n_f) beta_f (s_c the cell's scattering
 // multiplier, 1 by default), beta_f the second-order upwind face
@@ -545,6 +618,106 @@ __global__ void __launch_bounds__(256, sizeof(S) == 4 ? 4 : 2) k_residual8(DMesh
             out[i] = fixed - ec[i] - (S)tv * acc[i];
         }
         st8(Rlo + (gbase + pos_of[dc]) * nb + b0, out);
+    }
+}
+
+// Warp-per-cell form of k_residual8 (same lane layout as k_gradient_wc):
+// the cell's face geometry is read once per warp (broadcast) for the warp's
+// DS * DG directions, and the face loop has the same length on every lane.
+// Per band and direction the arithmetic is k_residual8's, face by face in
+// the same order, so both give the same bits.
+template <typename S, int DIM, int DG>
+__global__ void __launch_bounds__(256) k_residual_wc(DMesh m, DPhys p, EView<S, DIM> ev, const double *__restrict__ Bf,
+                                                     const double *__restrict__ Told, const double *__restrict__ eb,
+                                                     const int *__restrict__ pos_of, S *__restrict__ Rlo, int d0,
+                                                     int ndb) {
+    constexpr int BC = 4;
+    const int nb = p.nb, nc = m.nc, nbc = nb / BC;
+    const int DS = 32 / nbc;
+    const int lane = threadIdx.x & 31, slot = lane / nbc, bc = lane % nbc, b0 = BC * bc;
+    const bool on = slot < DS;
+    const int dpw = DS * DG;
+    const size_t items = (size_t)((ndb + dpw - 1) / dpw) * nc;
+    const size_t wstr = ((size_t)gridDim.x * blockDim.x) >> 5;
+    for (size_t w = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < items; w += wstr) {
+        const int c = (int)(w % nc), grp = (int)(w / nc);
+        const double tsc = m.tsc[c], invV = tsc / m.vol[c], tb = ev.Tb[c];
+        const double cx = m.cx[c], cy = m.cy[c], cz = DIM == 3 ? m.cz[c] : 0.0;
+        size_t d[DG];
+        double sx[DG], sy[DG], sz[DG];
+        S ec[DG][BC], acc[DG][BC], gxv[DG][BC], gyv[DG][BC], gzv[DG][BC];
+#pragma unroll
+        for (int k = 0; k < DG; k++) {
+            const int dl = min(grp * dpw + slot * DG + k, ndb - 1);
+            d[k] = (size_t)(d0 + dl);
+            sx[k] = p.sx[d[k]], sy[k] = p.sy[d[k]], sz[k] = p.sz[d[k]];
+            ld8(ev.eps + (d[k] * nc + c) * nb + b0, ec[k]);
+            const S *gp = ev.g + ((size_t)dl * nc + c) * DIM * nb + b0;
+            ld8(gp, gxv[k]);
+            ld8(gp + nb, gyv[k]);
+            if (DIM == 3) ld8(gp + 2 * nb, gzv[k]);
+#pragma unroll
+            for (int i = 0; i < BC; i++) acc[k][i] = (S)0;
+        }
+        for (int f = m.cf_ptr[c]; f < m.cf_ptr[c + 1]; f++) {
+            const double nx = m.cf_nx[f], ny = m.cf_ny[f], nz = DIM == 3 ? m.cf_nz[f] : 0.0;
+            const double fa = m.cf_area[f] * invV;
+            const int bound = m.cf_bound[f];
+            const int j = m.cf_nbr[f];
+            const double fx = m.cf_fx[f], fy = m.cf_fy[f], fz = DIM == 3 ? m.cf_fz[f] : 0.0;
+#pragma unroll
+            for (int k = 0; k < DG; k++) {
+                const double sn = sx[k] * nx + sy[k] * ny + (DIM == 3 ? sz[k] * nz : 0.0);
+                const S a = (S)(fa * sn);
+                if (sn >= 0) {
+                    const S rx = (S)(fx - cx), ry = (S)(fy - cy);
+                    const S rz = DIM == 3 ? (S)(fz - cz) : (S)0;
+#pragma unroll
+                    for (int i = 0; i < BC; i++) {
+                        S y = ec[k][i] + gxv[k][i] * rx + gyv[k][i] * ry;
+                        if (DIM == 3) y += gzv[k][i] * rz;
+                        acc[k][i] += a * y;
+                    }
+                } else if (bound < 0) {
+                    const int dl = (int)(d[k] - d0);
+                    S ej[BC], hx[BC], hy[BC], hz[BC];
+                    ld8(ev.eps + (d[k] * nc + j) * nb + b0, ej);
+                    const S *gp = ev.g + ((size_t)dl * nc + j) * DIM * nb + b0;
+                    ld8(gp, hx);
+                    ld8(gp + nb, hy);
+                    if (DIM == 3) ld8(gp + 2 * nb, hz);
+                    const S rx = (S)(fx - m.cx[j]), ry = (S)(fy - m.cy[j]);
+                    const S rz = DIM == 3 ? (S)(fz - m.cz[j]) : (S)0;
+#pragma unroll
+                    for (int i = 0; i < BC; i++) {
+                        S y = ej[i] + hx[i] * rx + hy[i] * ry;
+                        if (DIM == 3) y += hz[i] * rz;
+                        acc[k][i] += a * y;
+                    }
+                } else {
+                    const double *e = eb + (d[k] * m.nbs + m.cf_bside[f]) * nb + b0;
+#pragma unroll
+                    for (int i = 0; i < BC; i++) acc[k][i] += a * (S)(e[i] - p.C[b0 + i] * tb);
+                }
+            }
+        }
+        if (!on) continue;
+        const double dT = Told[c] - tb, hc = m.heat[c] * tsc;
+#pragma unroll
+        for (int k = 0; k < DG; k++) {
+            const int dl = grp * dpw + slot * DG + k;
+            if (dl >= ndb) break;
+            const size_t dc = d[k] * nc + c;
+            const double B = Bf[dc];
+            S out[BC];
+#pragma unroll
+            for (int i = 0; i < BC; i++) {
+                const double tv = p.tau[b0 + i] * p.vmag[b0 + i];
+                const S fixed = (S)(p.C[b0 + i] * (dT - tv * B) + hc * p.hr[b0 + i] * p.tau[b0 + i]);
+                out[i] = fixed - ec[k][i] - (S)tv * acc[k][i];
+            }
+            st8(Rlo + ((size_t)dl * nc + pos_of[dc]) * nb + b0, out);
+        }
     }
 }
 
@@ -3074,9 +3247,23 @@ Error Solver::solve_t(SolveStats &st) {
     };
     // LSQ gradient, 4 bands and grad_dg directions per thread (options.gradient_dirs,
     // or timed on the first outer iteration: gtune)
+    // (launch shapes: 1, 2, 4 = a thread per cell and 4 bands covering that
+    // many directions; 5, 6 = a warp per cell, lanes over band groups and
+    // directions, 1 or 2 directions per lane: needs nb / 4 <= 32)
+    const bool wc_ok = nb % 4 == 0 && nb / 4 <= 32;
     const bool gtune = cfg.gradient_dirs == 0 && tuned_grad_dirs_ == 0 && nb % 4 == 0 && cfg.order == 2;
     int grad_dg = cfg.gradient_dirs ? cfg.gradient_dirs : tuned_grad_dirs_ ? tuned_grad_dirs_ : 2;
+    if (!wc_ok && grad_dg > 4) grad_dg = 2;
     auto launch_grad = [&](int dg, int d0, int nbt) -> cudaError_t {
+        if (dg >= 5) {
+            const int dpw = (32 / (nb / 4)) * (dg - 4);
+            const size_t thr = (size_t)((nbt + dpw - 1) / dpw) * nc * 32;
+            if (dg == 5)
+                k_gradient_wc<S, DIM, 1><<<grid_for(thr), kThreads, 0, s>>>(dm_, dp_, dm_.lsq_pk, eps, g, d0, nbt);
+            else
+                k_gradient_wc<S, DIM, 2><<<grid_for(thr), kThreads, 0, s>>>(dm_, dp_, dm_.lsq_pk, eps, g, d0, nbt);
+            return cudaGetLastError();
+        }
         const size_t items = (size_t)((nbt + dg - 1) / dg) * nc * (nb / 4);
         if (dg == 2)
             k_gradient_md<S, DIM, 2><<<grid_for(items), kThreads, 0, s>>>(dm_, dp_, dm_.lsq_pk, eps, g, d0, nbt);
@@ -3087,6 +3274,28 @@ Error Solver::solve_t(SolveStats &st) {
         return cudaGetLastError();
     };
     last_grad_dirs_ = nb % 4 == 0 ? grad_dg : 0;
+    // the residual's launch shape (1 = a thread per cell and 4 bands; 5, 6 =
+    // a warp per cell as above), timed on the first outer iteration
+    const bool rtune = cfg.residual_form == 0 && tuned_res_form_ == 0 && wc_ok;
+    int res_form = cfg.residual_form ? cfg.residual_form : tuned_res_form_ ? tuned_res_form_ : 1;
+    if (!wc_ok) res_form = 1;
+    auto launch_res = [&](int form, int d0, int nbt) -> cudaError_t {
+        if (form >= 5) {
+            const int dpw = (32 / (nb / 4)) * (form - 4);
+            const size_t thr = (size_t)((nbt + dpw - 1) / dpw) * nc * 32;
+            if (form == 5)
+                k_residual_wc<S, DIM, 1><<<grid_for(thr), kThreads, 0, s>>>(dm_, dp_, ev, Bflux_, Told_, eb_, pos_of_,
+                                                                           R, d0, nbt);
+            else
+                k_residual_wc<S, DIM, 2><<<grid_for(thr), kThreads, 0, s>>>(dm_, dp_, ev, Bflux_, Told_, eb_, pos_of_,
+                                                                           R, d0, nbt);
+            return cudaGetLastError();
+        }
+        k_residual8<S, DIM, 4><<<grid_for((size_t)nbt * nc * nb / 4), kThreads, 0, s>>>(dm_, dp_, ev, Bflux_, Told_,
+                                                                                      eb_, pos_of_, R, d0, nbt);
+        return cudaGetLastError();
+    };
+    last_res_form_ = nb % 4 == 0 ? res_form : 0;
     // first order (solve_firstorder, StaticBTESyntheticSolver.cpp:487-726):
     // upwind cell values on the faces, i.e. zero gradients throughout
     if (cfg.order == 1) CUDA_TRY(cudaMemsetAsync(grad_, 0, (size_t)ndb * nc * nb * DIM * sizeof(S), s));
@@ -3142,7 +3351,8 @@ Error Solver::solve_t(SolveStats &st) {
                 CUDA_TRY(cudaEventCreate(&t1));
                 float best = 1e30f;
                 int best_dg = 1;
-                for (int dg : {1, 2, 4}) {
+                for (int dg : {1, 2, 4, 5, 6}) {
+                    if (dg >= 5 && !wc_ok) continue;
                     for (int rep = 0; rep < 2; rep++) {
                         CUDA_TRY(cudaEventRecord(t0, s));
                         CUDA_TRY(launch_grad(dg, d0, nbt));
@@ -3163,8 +3373,32 @@ Error Solver::solve_t(SolveStats &st) {
             if (cfg.use_limiter)
                 GL(K_GRADIENT, (k_limit<DIM><<<grid_for(nbe), kThreads, 0, s>>>(dm_, dp_, (const double *)eps, eb_,
                                                                                (double *)g, d0, nbt)));
-            GL(K_RESIDUAL, (k_residual8<S, DIM, 4><<<grid_for(nbe / 4), kThreads, 0, s>>>(dm_, dp_, ev, Bflux_, Told_, eb_,
-                                                                                          pos_of_, R, d0, nbt)));
+            if (rtune && nt == 0 && d0 == dlo) {
+                // the residual's launch shape: each candidate timed twice on
+                // this batch (they write the same bits to R)
+                cudaEvent_t t0, t1;
+                CUDA_TRY(cudaEventCreate(&t0));
+                CUDA_TRY(cudaEventCreate(&t1));
+                float best = 1e30f;
+                int best_form = 1;
+                for (int form : {1, 5, 6}) {
+                    for (int rep = 0; rep < 2; rep++) {
+                        CUDA_TRY(cudaEventRecord(t0, s));
+                        CUDA_TRY(launch_res(form, d0, nbt));
+                        CUDA_TRY(cudaEventRecord(t1, s));
+                        CUDA_TRY(cudaEventSynchronize(t1));
+                        float m = 0;
+                        CUDA_TRY(cudaEventElapsedTime(&m, t0, t1));
+                        if (m < best) best = m, best_form = form;
+                    }
+                }
+                cudaEventDestroy(t0);
+                cudaEventDestroy(t1);
+                tuned_res_form_ = best_form;
+                res_form = best_form;
+                last_res_form_ = best_form;
+            }
+            GL(K_RESIDUAL, CUDA_TRY(launch_res(res_form, d0, nbt)));
         } else {
             if (cfg.order == 2)
                 GL(K_GRADIENT, (k_gradient<S, DIM><<<grid_for(nbe), kThreads, 0, s>>>(dm_, dp_, w, eps, g, d0, nbt)));
@@ -3362,7 +3596,9 @@ Error Solver::solve_t(SolveStats &st) {
             if (rc) return {-9, "direction shard exchange failed (" + std::to_string(rc) + ")"};
             return {0, ""};
         };
-        const bool graphable = graph_ok_ && !((tune || (gtune && tuned_grad_dirs_ == 0)) && nt == 0) && !cfg.profile;
+        const bool graphable = graph_ok_ &&
+                               !((tune || (gtune && tuned_grad_dirs_ == 0) || (rtune && tuned_res_form_ == 0)) && nt == 0) &&
+                               !cfg.profile;
         // capture once; any failure leaves the direct launches in place
         auto capture = [&](const std::function<Error()> &stage, cudaGraphExec_t &gx, long long &nl) {
             cudaGraph_t gr = nullptr;

@@ -53,7 +53,8 @@ struct SolverConfig {
     int sweep_vector = 0;     // bands per sweep thread (1, 2, 4), 0 = automatic
     int sweep_kernel = 0;     // 1: block sweep kernel, 2: warp-independent kernel, 3: wide-level kernel, 0 = automatic
     int sweep_far_slots = 0;  // far-slot cap of the sweep plan: 0 = automatic, < 0 = none
-    int gradient_dirs = 0;    // directions per gradient thread (1, 2, 4), 0 = automatic
+    int gradient_dirs = 0;    // gradient launch shape (1, 2, 4: directions per thread; 5, 6: warp per cell), 0 = automatic
+    int residual_form = 0;    // residual launch shape (1: thread per cell; 5, 6: warp per cell), 0 = automatic
     int direction_batch = 0;  // most directions per transport batch, 0 = automatic
     std::vector<double> cell_scatter;  // scattering-rate multiplier s_c per cell (empty: 1)
     int order = 2;            // 2: second-order upwind faces (solve); 1: first order (solve_firstorder)
@@ -144,6 +145,8 @@ public:
     int tuned_sweep_wide_ = 0;   // 1: the wide-level sweep kernel won (the autotuner's pick)
     int tuned_grad_dirs_ = 0;    // directions per gradient thread (1, 2 or 4; 0 = not yet tuned)
     int last_grad_dirs_ = 0;     // the same, of the last solve's gradient launches (0: 1-band form)
+    int tuned_res_form_ = 0;     // residual launch shape (1 thread per cell, 5/6 warp per cell; 0 = not yet tuned)
+    int last_res_form_ = 0;      // the same, of the last solve's residual launches (0: 1-band form)
     // launch shape of the last solve's sweep (last_sweep_warp_: 0 block, 1 warp, 2 wide-level kernel)
     int last_sweep_vb_ = 0, last_sweep_threads_ = 0, last_sweep_warp_ = 0;
     int ndb_ = 1;                // directions per batch of the gradient/residual/correction buffers

@@ -176,10 +176,15 @@ typedef struct {
                                  shared-memory ring: for levels of thousands of cells, e.g. 3D
                                  tetrahedra; plans without far slots only), 0 = the fastest on the
                                  first outer iteration. Results do not depend on it. */
-    int gradient_dirs;        /* directions each thread of the LSQ gradient covers (1, 2 or 4: one
-                                 load of a stencil entry serves 4 bands of that many directions);
+    int gradient_dirs;        /* launch shape of the LSQ gradient: 1, 2 or 4 = a thread per cell and
+                                 4 bands covering that many directions (one load of a stencil entry
+                                 serves them all); 5, 6 = a warp per cell, lanes over band groups
+                                 and directions, 1 or 2 directions per lane (band count <= 128);
                                  0 = the fastest on the first outer iteration. Results do not
                                  depend on it. */
+    int residual_form;        /* launch shape of the second-order residual: 1 = a thread per cell
+                                 and 4 bands, 5, 6 = a warp per cell as for gradient_dirs; 0 = the
+                                 fastest on the first outer iteration. Results do not depend on it. */
 } gbte_options;
 
 #define GBTE_NUM_KERNELS 16
@@ -210,7 +215,8 @@ typedef struct {
     int sweep_vector;         /* bands per sweep thread in use (options.sweep_vector or autotuned) */
     int sweep_threads;        /* threads per sweep CTA in use */
     int sweep_kernel;         /* sweep kernel in use: 1 block, 2 warp-independent, 3 wide-level */
-    int gradient_dirs;        /* directions per gradient thread in use (0: the 1-band form ran) */
+    int gradient_dirs;        /* gradient launch shape in use (0: the 1-band form ran) */
+    int residual_form;        /* residual launch shape in use (0: the 1-band form ran) */
 } gbte_stats;
 
 /* Name of kernel slot i of gbte_stats.kernel_ms (NULL past the last one). */
