@@ -110,7 +110,7 @@ class Stats(ctypes.Structure):
 
 class VjpStats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("picard_steps", ctypes.c_int), ("change", ctypes.c_double),
-                ("vjp_ms", ctypes.c_double)]
+                ("vjp_ms", ctypes.c_double), ("residual", ctypes.c_double)]
 
 
 class DeckInfo(ctypes.Structure):
@@ -392,8 +392,8 @@ class StaticBTESynthetic:
         solve reached (gbte_vjp): ``tau`` (per band, multiplier on its
         relaxation time), ``scatter`` (per cell, its scattering multiplier),
         ``specularity`` (per boundary-table row; partially specular rows).
-        The transposed iteration stops when the gradient's relative change
-        between iterations is <= tol."""
+        The transposed iteration stops when the residual of the adjoint
+        equations relative to dJ/de is <= tol."""
         nc, nb = self.num_cells, self.num_bands
         Tb = np.ascontiguousarray(T_bar, dtype=np.float64) if T_bar is not None else None
         qb = np.ascontiguousarray(q_bar, dtype=np.float64).reshape(-1) if q_bar is not None else None

@@ -685,6 +685,7 @@ int gbte_vjp(gbte_handle *h, const double *T_bar, const double *q_bar, int max_i
             st->picard_steps = vs.picard_steps;
             st->change = vs.change;
             st->vjp_ms = vs.ms;
+            st->residual = vs.residual;
         }
         return GBTE_OK;
     } catch (const std::bad_alloc &) {

@@ -4457,6 +4457,14 @@ __global__ void __launch_bounds__(256) k_adj_gradT(DMesh m, DPhys p, const int *
 
 // lam += D mu with mu the opposite direction's sweep output; sums of the
 // squares of the step and of the state
+// sum of squares of x[0 .. n) into *out (atomics per warp)
+__global__ void k_sqnorm(size_t n, const double *__restrict__ x, double *out) {
+    double s2 = 0;
+    for (size_t t = gtid(); t < n; t += gstride()) s2 += x[t] * x[t];
+    s2 = warp_sum(s2);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, s2);
+}
+
 __global__ void k_adj_update(DMesh m, DPhys p, const int *__restrict__ opp, const double *__restrict__ Dc,
                              double *lam, double *red) {
     const int nb = p.nb, nc = m.nc;
@@ -4888,13 +4896,14 @@ Error Solver::vjp(const double *Tbar_h, const double *qbar_h, int max_iter, doub
         for (int b = 0; b < nb; b++) gt[b] += kbar * bands.C[b] * bands.v[b] * bands.v[b] * bands.tau[b] / mdim;
         return {0, ""};
     };
-    // Transposed source iteration. It stops when the gradient's relative
-    // change between iterations is <= tol (the adjoint counterpart of the
-    // forward's margins, which are relative changes of its outputs): the
-    // adjoint state itself keeps a slowly decaying component that the
-    // gradient hardly sees.
+    // Transposed source iteration lam <- lam + A^-T r(lam), with the
+    // transposed residual r(lam) = (dF/de)^T lam + dJ/de. It stops when
+    // ||r(lam)|| <= tol ||dJ/de|| (r at lam = 0 is dJ/de), a bound on the
+    // residual of the adjoint equations rather than on the step; the
+    // gradient returned is the one assembled from that lam. The relative
+    // change of the gradient over the last iteration is reported beside it.
     std::vector<double> gt, gc, gb, pt, pc, pb;
-    double change = 1.0;
+    double change = 1.0, res0 = 0, resid = 1.0;
     int it = 0;
     for (;; it++) {
         Error ee = evaluate(lam, true, true);
@@ -4908,14 +4917,23 @@ Error Solver::vjp(const double *Tbar_h, const double *qbar_h, int max_iter, doub
             for (int i = 0; i < nbd; i++) num += (gb[i] - pb[i]) * (gb[i] - pb[i]), den += gb[i] * gb[i];
             change = den > 0 ? std::sqrt(num / den) : 0.0;
             if (!std::isfinite(change)) return {-4, "the adjoint iteration diverged"};
-            if (change <= tol) break;
         }
-        if (it >= max_iter) break;
+        ee = finish();  // Rlo = r(lam) in level order, then A^-T r(lam)
+        if (ee.code) return ee;
+        CUDA_TRY(cudaMemsetAsync(red, 0, 8, s));
+        k_sqnorm<<<grid_for(ne), kThreads, 0, s>>>(ne, Rlo, red);
+        CUDA_TRY(cudaGetLastError());
+        double r2 = 0;
+        CUDA_TRY(cudaMemcpyAsync(&h_pinned_[10], red, 8, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        r2 = h_pinned_[10];
+        if (it == 0) res0 = r2;
+        resid = res0 > 0 ? std::sqrt(r2 / res0) : 0.0;
+        if (!std::isfinite(resid)) return {-4, "the adjoint iteration diverged"};
+        if (resid <= tol || it >= max_iter) break;
         pt.swap(gt);
         pc.swap(gc);
         pb.swap(gb);
-        ee = finish();
-        if (ee.code) return ee;
         CUDA_TRY(cudaMemsetAsync(red, 0, 2 * 8, s));
         k_adj_update<<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, opp, (const double *)corr_, lam, red);
         CUDA_TRY(cudaGetLastError());
@@ -4930,6 +4948,7 @@ Error Solver::vjp(const double *Tbar_h, const double *qbar_h, int max_iter, doub
     st.iterations = it;
     st.picard_steps = N;
     st.change = change;
+    st.residual = resid;
     st.ms = ms;
     return {0, ""};
 }

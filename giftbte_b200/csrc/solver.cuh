@@ -73,7 +73,7 @@ const char *kernel_name(int k);
 
 struct VjpStats {
     int iterations = 0, picard_steps = 0;
-    double change = 0, ms = 0;
+    double change = 0, ms = 0, residual = 0;
 };
 
 struct SolveStats {

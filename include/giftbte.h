@@ -361,8 +361,8 @@ int gbte_get_geometry(gbte_handle *h, double *centers, double *volumes);
  * Any output may be NULL. It differentiates the fixed point the last
  * gbte_solve reached, implicitly: the adjoint state solves the transposed
  * equations by the transposed source iteration (sweeps in the opposite
- * directions, the transposed synthetic correction), until the gradient's
- * relative change between iterations is <= tol (like the forward's margins)
+ * directions, the transposed synthetic correction), until the residual of
+ * the adjoint equations, ||(dF/de)^T lam + dJ/de||, is <= tol ||dJ/de||,
  * or max_iter iterations ran. Call it after a solve that
  * converged to tight margins; the gradient is that of the state the solve
  * left. FP64 handles only (GBTE_ERR_UNSUPPORTED otherwise), not batched
@@ -373,6 +373,7 @@ typedef struct {
     int picard_steps;   /* Picard steps of the synthetic correction, transposed */
     double change;      /* last relative change of the gradient */
     double vjp_ms;      /* device time of the adjoint solve and the assembly */
+    double residual;    /* ||(dF/de)^T lam + dJ/de|| / ||dJ/de|| at the returned gradient */
 } gbte_vjp_stats;
 
 int gbte_vjp(gbte_handle *h, const double *T_bar, const double *q_bar, int max_iter, double tol, double *grad_tau,

@@ -322,3 +322,63 @@ def test_adjoint_rejects_solver_variants():
         with pytest.raises(g.GBTEError):
             s.vjp(q_bar=np.zeros((d.mesh.n_cells, 3)))
         s.close()
+
+
+def test_config4_full_size_against_finite_differences():
+    # the adjoint workload at full size: the 300 nm porous cell (3 nm mesh,
+    # 17,939 triangles), 40 bands, 64 directions, pore wall p = 0.3,
+    # log-normal cell multipliers (sigma 0.2, seed 2); objective k_x. Twenty
+    # seeded components, each checked by central differences (relative step
+    # 1e-6) of forward solves converged to 1e-12: eight band tau multipliers
+    # (seeded draw), the specularity, and eleven seeded random directions
+    # over the cell multiplier field (one cell alone moves k_x by ~1e-10
+    # relative, below what the differences resolve). The adjoint stops on
+    # its residual bound.
+    d0 = decks.config4_deck(h_nm=3.0, n_bands=40, n_phi=16, seed=0, specularity=0.3, residual_temp=1e-12,
+                            residual_flux=1e-12, max_iter=20000)
+    nc = d0.mesh.n_cells
+    sc = decks.lognormal_scatter(nc, sigma=0.2, seed=2)
+    s = g.StaticBTESynthetic.from_deck(d0, precision=g.GBTE_FP64, cell_scatter=sc)
+    s.fourier_initial()
+    s.solve(allow_not_converged=False)
+    qb = s.keff_cotangent(axis=0, length=L, delta_T=1.0)
+    a = s.vjp(q_bar=qb, tol=1e-10, max_iter=20000)
+    T0 = s.fields()["T"]
+    s.close()
+    assert a["stats"]["residual"] <= 1e-10
+    rng = np.random.default_rng(20)
+    nb = d0.bands.n_bands
+    spec_row = [i for i, b in enumerate(d0.bcs) if b.tag == 5][0]
+
+    def keff(d, s_c):
+        h = g.StaticBTESynthetic.from_deck(d, precision=g.GBTE_FP64, cell_scatter=s_c)
+        h.set_initial(T0)
+        h.solve(allow_not_converged=False)
+        _, vol = h.geometry()
+        k = keff_from(h.fields()["q"], vol)
+        h.close()
+        return k
+
+    checks = []
+    for b in rng.choice(nb, size=8, replace=False):
+        def f(hh, b=int(b)):
+            m = np.ones(nb)
+            m[b] += hh
+            return dataclasses.replace(d0, bands=dataclasses.replace(d0.bands, tau=d0.bands.tau * m)), sc
+        checks.append((f"tau[{b}]", a["tau"][b], f))
+
+    def fp(hh):
+        return dataclasses.replace(d0, bcs=[b if b.tag != 5 else decks.BC(5, 6, 0.3 + hh) for b in d0.bcs]), sc
+    checks.append(("p", a["specularity"][spec_row], fp))
+    for i in range(11):
+        v = rng.standard_normal(nc)
+
+        def fv(hh, v=v):
+            return d0, sc * (1 + hh * v)
+        # d/dh J(s (1 + h v)) = sum_c v_c s_c dJ/ds_c
+        checks.append((f"cells.v{i}", float(np.sum(v * sc * a["scatter"])), fv))
+    for name, adj, make in checks:
+        kp = keff(*make(H))
+        km = keff(*make(-H))
+        fd = (kp - km) / (2 * H)
+        assert abs(adj - fd) <= TOL * max(abs(fd), 1e-30), (name, adj, fd)
