@@ -169,4 +169,17 @@ constexpr int kSweepFarCap = 2048;
 Error build_sweep_plan(const FlatMesh &m, const Angles &a, const Schedule &s, int min_ring, int far_cap,
                        SweepPlan &out);
 
+// Tiles of the shared-memory LSQ gradient: cells split into blocks of B
+// consecutive cells (the solver's Morton order); block k's union is its own
+// B cells (local index = position in the block) followed by every other
+// stencil neighbour of its cells in ascending order. loc[q] is the local
+// index of stencil entry q in its cell's block union.
+struct GradTiles {
+    int B = 0, nblk = 0, umax = 0, qmax = 0;
+    std::vector<int> ptr;            // [nblk + 1] offsets into cells
+    std::vector<int> cells;          // union cells of every block
+    std::vector<unsigned short> loc; // [stencil entries]
+};
+Error build_grad_tiles(const FlatMesh &m, int B, GradTiles &out);
+
 }  // namespace gbte

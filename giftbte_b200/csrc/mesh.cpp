@@ -842,4 +842,44 @@ Error make_union(const std::vector<RawMesh> &meshes, const std::vector<BCs> &bcs
     return {0, ""};
 }
 
+Error build_grad_tiles(const FlatMesh &m, int B, GradTiles &out) {
+    out = GradTiles();
+    if (B < 1 || B > 1024) return {-1, "gradient tile size out of range"};
+    const int nc = m.nc;
+    out.B = B;
+    out.nblk = (nc + B - 1) / B;
+    out.ptr.assign(1, 0);
+    out.loc.resize(m.nbr_idx.size());
+    // mark[k] = block that last listed cell k, slot[k] = its local index there
+    std::vector<int> mark(nc, -1), slot(nc, 0), halo;
+    for (int blk = 0; blk < out.nblk; blk++) {
+        const int c0 = blk * B, c1 = std::min(nc, c0 + B);
+        for (int c = c0; c < c1; c++) {
+            mark[c] = blk;
+            slot[c] = c - c0;
+            out.cells.push_back(c);
+        }
+        halo.clear();
+        for (int q = m.nbr_ptr[c0]; q < m.nbr_ptr[c1]; q++) {
+            const int k = m.nbr_idx[q];
+            if (mark[k] != blk) {
+                mark[k] = blk;
+                halo.push_back(k);
+            }
+        }
+        std::sort(halo.begin(), halo.end());
+        const int nu = (c1 - c0) + (int)halo.size();
+        if (nu > 65535) return {-8, "gradient tile union exceeds 16-bit local indices"};
+        for (size_t h = 0; h < halo.size(); h++) {
+            slot[halo[h]] = (c1 - c0) + (int)h;
+            out.cells.push_back(halo[h]);
+        }
+        for (int q = m.nbr_ptr[c0]; q < m.nbr_ptr[c1]; q++) out.loc[q] = (unsigned short)slot[m.nbr_idx[q]];
+        out.ptr.push_back((int)out.cells.size());
+        out.umax = std::max(out.umax, nu);
+        out.qmax = std::max(out.qmax, m.nbr_ptr[c1] - m.nbr_ptr[c0]);
+    }
+    return {0, ""};
+}
+
 }  // namespace gbte

@@ -736,6 +736,92 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
+// A stencil entry staged in shared memory: weights in the storage precision
+// and the neighbour's index in the block's union.
+template <typename S> struct TileW;
+template <> struct alignas(16) TileW<float> { float wx, wy, wz; int loc; };
+template <> struct alignas(16) TileW<double> { double wx, wy, wz; int loc, pad; };
+
+// Shared-memory tiled LSQ gradient. One CTA per (block of B consecutive
+// cells, chunk of nbc bands), looping over the batch's directions. The
+// block's stencil entries (weights, union-local neighbour index) are staged
+// in shared memory once per CTA; for each direction the rows of the block's
+// union (its own cells and every stencil neighbour, nbc bands each) are
+// copied in with 16-byte cp.async, and each thread (cell, 4 bands)
+// accumulates from shared memory only: every neighbour row crosses from L2
+// once per block and direction instead of once per stencil entry. Per band
+// and direction the arithmetic is k_gradient8's, entry by entry in the same
+// order, so both give the same bits. Needs nbc a multiple of 4 dividing nb,
+// nbc * sizeof(S) a multiple of 16. Shared memory: qmax TileW<S>, then
+// umax * nbc S.
+template <typename S, int DIM>
+__global__ void __launch_bounds__(512) k_gradient_tile(DMesh m, DPhys p, const float4 *__restrict__ pk,
+                                                       const int *__restrict__ tile_ptr,
+                                                       const int *__restrict__ tile_cells,
+                                                       const unsigned short *__restrict__ tile_loc, int B, int nbc,
+                                                       int qmax, const S *__restrict__ eps, S *__restrict__ g,
+                                                       int d0, int ndb) {
+    extern __shared__ __align__(16) unsigned char tsm[];
+    TileW<S> *wq = reinterpret_cast<TileW<S> *>(tsm);
+    S *et = reinterpret_cast<S *>(tsm + (size_t)qmax * sizeof(TileW<S>));
+    const int nb = p.nb, nc = m.nc, nchunk = nb / nbc;
+    const int blk = blockIdx.x / nchunk, ch = blockIdx.x % nchunk, b0 = ch * nbc;
+    const int c0 = blk * B, c1 = min(c0 + B, nc), ncell = c1 - c0;
+    const int qb0 = m.nbr_ptr[c0], qb1 = m.nbr_ptr[c1];
+    const int u0 = tile_ptr[blk], nu = tile_ptr[blk + 1] - u0;
+    const int tid = threadIdx.x, bd = blockDim.x;
+    for (int q = qb0 + tid; q < qb1; q += bd) {
+        TileW<S> t;
+        if constexpr (sizeof(S) == 4) {
+            const float4 a = pk[q];
+            t.wx = a.x, t.wy = a.y, t.wz = a.z;
+        } else {
+            t.wx = m.lsq_w[3 * q], t.wy = m.lsq_w[3 * q + 1], t.wz = m.lsq_w[3 * q + 2];
+        }
+        t.loc = tile_loc[q];
+        wq[q - qb0] = t;
+    }
+    const int per_row = nbc * (int)sizeof(S) / 16;  // 16-byte pieces of a row chunk
+    const int ngrp = nbc / 4;
+    const int items = ncell * ngrp;
+    for (int dl = 0; dl < ndb; dl++) {
+        const S *ed = eps + (size_t)(d0 + dl) * nc * nb + b0;
+        __syncthreads();  // the previous direction's reads of et are done
+        for (int i = tid; i < nu * per_row; i += bd) {
+            const int u = i / per_row, k = i - u * per_row;
+            cp_async(reinterpret_cast<unsigned char *>(et + (size_t)u * nbc) + 16 * k,
+                     reinterpret_cast<const unsigned char *>(ed + (size_t)tile_cells[u0 + u] * nb) + 16 * k, 16);
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        for (int it = tid; it < items; it += bd) {
+            const int i = it / ngrp, j = it - i * ngrp, c = c0 + i;
+            S ec[4], gx[4], gy[4], gz[4];
+            ld8(et + (size_t)i * nbc + 4 * j, ec);
+#pragma unroll
+            for (int v = 0; v < 4; v++) gx[v] = gy[v] = gz[v] = 0;
+            const int qa = m.nbr_ptr[c] - qb0, qe = m.nbr_ptr[c + 1] - qb0;
+            for (int q = qa; q < qe; q++) {
+                const TileW<S> t = wq[q];
+                S e[4];
+                ld8(et + (size_t)t.loc * nbc + 4 * j, e);
+#pragma unroll
+                for (int v = 0; v < 4; v++) {
+                    const S de = e[v] - ec[v];
+                    gx[v] += t.wx * de;
+                    gy[v] += t.wy * de;
+                    if (DIM == 3) gz[v] += t.wz * de;
+                }
+            }
+            S *gp = g + ((size_t)dl * nc + c) * DIM * nb + b0 + 4 * j;
+            st8(gp, gx);
+            st8(gp + nb, gy);
+            if (DIM == 3) st8(gp + 2 * nb, gz);
+        }
+    }
+}
+
 // One cell of a direction's level order, as the sweep reads it: up to four
 // upwind neighbours (their positions in the same level order, or -(1 +
 // far slot)) with their coefficients a_j = A_f/V (s.n_f) < 0, sig = sum of
@@ -3254,7 +3340,40 @@ Error Solver::solve_t(SolveStats &st) {
     const bool gtune = cfg.gradient_dirs == 0 && tuned_grad_dirs_ == 0 && nb % 4 == 0 && cfg.order == 2;
     int grad_dg = cfg.gradient_dirs ? cfg.gradient_dirs : tuned_grad_dirs_ ? tuned_grad_dirs_ : 2;
     if (!wc_ok && grad_dg > 4) grad_dg = 2;
+    // the tiled form (7, 8: tiles_[0], tiles_[1]): the widest band chunk
+    // whose shared memory leaves room for two CTAs per SM, else one
+    if (cfg.order == 2 && nb % 4 == 0) {
+        Error te = grad_tiles();
+        if (te.code) return te;
+        CUDA_TRY(cudaFuncSetAttribute(k_gradient_tile<S, DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      220 * 1024));
+    }
+    auto tile_shape = [&](int code, int &nbc, int &threads, size_t &smem) -> bool {
+        const int k = code - 7;
+        if (k < 0 || k >= (int)tiles_.size()) return false;
+        const TileDev &T = tiles_[k];
+        const size_t wbytes = (size_t)T.qmax * (sizeof(S) == 4 ? 16 : 32);
+        for (int limit : {113 * 1024, 220 * 1024})
+            for (nbc = nb; nbc >= 4; nbc -= 4) {
+                if (nb % nbc || (nbc * sizeof(S)) % 16) continue;
+                smem = wbytes + (size_t)T.umax * nbc * sizeof(S);
+                if (smem <= (size_t)limit) {
+                    threads = std::min(512, ((T.B * nbc / 4 + 31) / 32) * 32);
+                    return true;
+                }
+            }
+        return false;
+    };
     auto launch_grad = [&](int dg, int d0, int nbt) -> cudaError_t {
+        if (dg >= 7) {
+            int nbc = 0, threads = 0;
+            size_t smem = 0;
+            if (!tile_shape(dg, nbc, threads, smem)) return cudaErrorInvalidValue;
+            const TileDev &T = tiles_[dg - 7];
+            k_gradient_tile<S, DIM><<<T.nblk * (nb / nbc), threads, smem, s>>>(
+                dm_, dp_, dm_.lsq_pk, T.ptr, T.cells, T.loc, T.B, nbc, T.qmax, eps, g, d0, nbt);
+            return cudaGetLastError();
+        }
         if (dg >= 5) {
             const int dpw = (32 / (nb / 4)) * (dg - 4);
             const size_t thr = (size_t)((nbt + dpw - 1) / dpw) * nc * 32;
@@ -3273,6 +3392,11 @@ Error Solver::solve_t(SolveStats &st) {
             k_gradient8<S, DIM, 4><<<grid_for(items), kThreads, 0, s>>>(dm_, dp_, w, eps, g, d0, nbt);
         return cudaGetLastError();
     };
+    {
+        int nbc_ = 0, thr_ = 0;
+        size_t sm_ = 0;
+        if (grad_dg >= 7 && (cfg.order != 2 || !tile_shape(grad_dg, nbc_, thr_, sm_))) grad_dg = 2;
+    }
     last_grad_dirs_ = nb % 4 == 0 ? grad_dg : 0;
     // the residual's launch shape (1 = a thread per cell and 4 bands; 5, 6 =
     // a warp per cell as above), timed on the first outer iteration
@@ -3351,8 +3475,11 @@ Error Solver::solve_t(SolveStats &st) {
                 CUDA_TRY(cudaEventCreate(&t1));
                 float best = 1e30f;
                 int best_dg = 1;
-                for (int dg : {1, 2, 4, 5, 6}) {
-                    if (dg >= 5 && !wc_ok) continue;
+                for (int dg : {1, 2, 4, 5, 6, 7, 8}) {
+                    if (dg >= 5 && dg <= 6 && !wc_ok) continue;
+                    int nbc_ = 0, thr_ = 0;
+                    size_t sm_ = 0;
+                    if (dg >= 7 && !tile_shape(dg, nbc_, thr_, sm_)) continue;
                     for (int rep = 0; rep < 2; rep++) {
                         CUDA_TRY(cudaEventRecord(t0, s));
                         CUDA_TRY(launch_grad(dg, d0, nbt));
@@ -3818,6 +3945,30 @@ Error Solver::get_fields(double *TE, double *TL, double *q, double *TB) {
     if (TL) CUDA_TRY(cudaMemcpyAsync(TL, T_, nc * 8, cudaMemcpyDeviceToHost, s));
     if (q) CUDA_TRY(cudaMemcpyAsync(q, q_, nc * 24, cudaMemcpyDeviceToHost, s));
     if (TB) CUDA_TRY(cudaMemcpyAsync(TB, Tband_, nc * bands.nb * 8, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return {0, ""};
+}
+
+// Tiles of the shared-memory gradient for two block sizes (3D: 32 and 64
+// cells, whose unions of ~70-cell stencils stay a few hundred rows; 2D: 64
+// and 128), uploaded once.
+Error Solver::grad_tiles() {
+    if (tiles_built_) return {0, ""};
+    tiles_built_ = true;
+    const int cand[2] = {mesh.dim == 3 ? 32 : 64, mesh.dim == 3 ? 64 : 128};
+    cudaStream_t s = cfg.stream;
+    bool ok = true;
+    for (int B : cand) {
+        GradTiles t;
+        if (build_grad_tiles(mesh, B, t).code) continue;
+        TileDev d;
+        d.B = t.B, d.nblk = t.nblk, d.umax = t.umax, d.qmax = t.qmax;
+        d.ptr = upload(this, allocs_, t.ptr, s, ok);
+        d.cells = upload(this, allocs_, t.cells, s, ok);
+        d.loc = upload(this, allocs_, t.loc, s, ok);
+        if (!ok) return {-6, "device allocation failed (gradient tiles)"};
+        tiles_.push_back(d);
+    }
     CUDA_TRY(cudaStreamSynchronize(s));
     return {0, ""};
 }

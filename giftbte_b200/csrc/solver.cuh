@@ -145,6 +145,16 @@ public:
     int tuned_sweep_wide_ = 0;   // 1: the wide-level sweep kernel won (the autotuner's pick)
     int tuned_grad_dirs_ = 0;    // directions per gradient thread (1, 2 or 4; 0 = not yet tuned)
     int last_grad_dirs_ = 0;     // the same, of the last solve's gradient launches (0: 1-band form)
+    // tiles of the shared-memory gradient (gradient_dirs 7, 8), built by the
+    // first solve for two block sizes
+    struct TileDev {
+        int B = 0, nblk = 0, umax = 0, qmax = 0;
+        int *ptr = nullptr, *cells = nullptr;
+        unsigned short *loc = nullptr;
+    };
+    std::vector<TileDev> tiles_;
+    bool tiles_built_ = false;
+    Error grad_tiles();
     int tuned_res_form_ = 0;     // residual launch shape (1 thread per cell, 5/6 warp per cell; 0 = not yet tuned)
     int last_res_form_ = 0;      // the same, of the last solve's residual launches (0: 1-band form)
     // launch shape of the last solve's sweep (last_sweep_warp_: 0 block, 1 warp, 2 wide-level kernel)

@@ -180,6 +180,9 @@ typedef struct {
                                  4 bands covering that many directions (one load of a stencil entry
                                  serves them all); 5, 6 = a warp per cell, lanes over band groups
                                  and directions, 1 or 2 directions per lane (band count <= 128);
+                                 7, 8 = shared-memory tiles: a CTA per block of consecutive cells
+                                 (3D: 32 or 64, 2D: 64 or 128) stages the block's stencil once and,
+                                 direction by direction, the rows of the block's stencil union;
                                  0 = the fastest on the first outer iteration. Results do not
                                  depend on it. */
     int residual_form;        /* launch shape of the second-order residual: 1 = a thread per cell
