@@ -79,7 +79,8 @@ class Options(ctypes.Structure):
                 ("sweep_far_slots", ctypes.c_int), ("direction_batch", ctypes.c_int),
                 ("cell_scatter", _c_dbl_p), ("cell_order", ctypes.c_int), ("order", ctypes.c_int),
                 ("scheme", ctypes.c_int), ("macro_exact", ctypes.c_int), ("sweep_vector", ctypes.c_int),
-                ("sweep_kernel", ctypes.c_int), ("gradient_dirs", ctypes.c_int), ("residual_form", ctypes.c_int)]
+                ("sweep_kernel", ctypes.c_int), ("gradient_dirs", ctypes.c_int), ("residual_form", ctypes.c_int),
+                ("adjoint_history", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):

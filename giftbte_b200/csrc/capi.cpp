@@ -171,6 +171,9 @@ int create_common(const gbte::RawMesh &raw_in, const gbte::Bands &bands_in, cons
     if (opt.residual_form != 0 && opt.residual_form != 1 && opt.residual_form != 5 && opt.residual_form != 6)
         return fail(nullptr, {-1, "residual_form must be 0 (automatic), 1, 5 or 6"}), GBTE_ERR_ARG;
     cfg.residual_form = opt.residual_form;
+    if (opt.adjoint_history < -1 || opt.adjoint_history > 8)
+        return fail(nullptr, {-1, "adjoint_history must be -1 (plain), 0 (default) or 1..8"}), GBTE_ERR_ARG;
+    cfg.adjoint_anderson = opt.adjoint_history == 0 ? 6 : opt.adjoint_history < 0 ? 0 : opt.adjoint_history;
     cfg.device = opt.device;
     cfg.stream = (cudaStream_t)opt.stream;
     if (opt.precision != GBTE_FP64 && opt.precision != GBTE_FP32_MIXED)

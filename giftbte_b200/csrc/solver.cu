@@ -802,16 +802,42 @@ __global__ void __launch_bounds__(512) k_gradient_tile(DMesh m, DPhys p, const f
 #pragma unroll
             for (int v = 0; v < 4; v++) gx[v] = gy[v] = gz[v] = 0;
             const int qa = m.nbr_ptr[c] - qb0, qe = m.nbr_ptr[c + 1] - qb0;
-            for (int q = qa; q < qe; q++) {
-                const TileW<S> t = wq[q];
-                S e[4];
-                ld8(et + (size_t)t.loc * nbc + 4 * j, e);
+            if constexpr (sizeof(S) == 4) {
+                // two bands per instruction: packed f32x2 add and fma round
+                // each lane like the scalar fsub and (contracted) fma
+                const float2 n01 = make_float2(-ec[0], -ec[1]), n23 = make_float2(-ec[2], -ec[3]);
+                float2 x01 = make_float2(0.f, 0.f), x23 = x01, y01 = x01, y23 = x01, z01 = x01, z23 = x01;
+                for (int q = qa; q < qe; q++) {
+                    const TileW<S> t = wq[q];
+                    const float4 e = *reinterpret_cast<const float4 *>(et + (size_t)t.loc * nbc + 4 * j);
+                    const float2 d01 = __fadd2_rn(make_float2(e.x, e.y), n01);
+                    const float2 d23 = __fadd2_rn(make_float2(e.z, e.w), n23);
+                    const float2 wx = make_float2(t.wx, t.wx), wy = make_float2(t.wy, t.wy);
+                    x01 = __ffma2_rn(wx, d01, x01);
+                    x23 = __ffma2_rn(wx, d23, x23);
+                    y01 = __ffma2_rn(wy, d01, y01);
+                    y23 = __ffma2_rn(wy, d23, y23);
+                    if (DIM == 3) {
+                        const float2 wz = make_float2(t.wz, t.wz);
+                        z01 = __ffma2_rn(wz, d01, z01);
+                        z23 = __ffma2_rn(wz, d23, z23);
+                    }
+                }
+                gx[0] = x01.x, gx[1] = x01.y, gx[2] = x23.x, gx[3] = x23.y;
+                gy[0] = y01.x, gy[1] = y01.y, gy[2] = y23.x, gy[3] = y23.y;
+                gz[0] = z01.x, gz[1] = z01.y, gz[2] = z23.x, gz[3] = z23.y;
+            } else {
+                for (int q = qa; q < qe; q++) {
+                    const TileW<S> t = wq[q];
+                    S e[4];
+                    ld8(et + (size_t)t.loc * nbc + 4 * j, e);
 #pragma unroll
-                for (int v = 0; v < 4; v++) {
-                    const S de = e[v] - ec[v];
-                    gx[v] += t.wx * de;
-                    gy[v] += t.wy * de;
-                    if (DIM == 3) gz[v] += t.wz * de;
+                    for (int v = 0; v < 4; v++) {
+                        const S de = e[v] - ec[v];
+                        gx[v] += t.wx * de;
+                        gy[v] += t.wy * de;
+                        if (DIM == 3) gz[v] += t.wz * de;
+                    }
                 }
             }
             S *gp = g + ((size_t)dl * nc + c) * DIM * nb + b0 + 4 * j;
@@ -4608,6 +4634,83 @@ __global__ void __launch_bounds__(256) k_adj_gradT(DMesh m, DPhys p, const int *
 
 // lam += D mu with mu the opposite direction's sweep output; sums of the
 // squares of the step and of the state
+// The adjoint's fixed-point update f = G(lam) - lam: the opposite-direction
+// sweep's output mapped back (see k_adj_update), written to f.
+__global__ void k_adj_fvec(DMesh m, DPhys p, const int *__restrict__ opp, const double *__restrict__ Dc,
+                           double *__restrict__ f) {
+    const int nb = p.nb, nc = m.nc;
+    const size_t total = (size_t)p.nd * nc * nb;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b = (int)(t % nb);
+        const size_t dc = t / nb;
+        const int c = (int)(dc % nc);
+        const int d = (int)(dc / nc);
+        f[t] = Dc[((size_t)opp[d] * nc + c) * nb + b] * m.vol[c] / m.tsc[c];
+    }
+}
+
+// Anderson step, first pass: dF_new = f - f_prev (stored into dfn), f_prev =
+// f, and the dot products of dF_new and of f with the m stored dF vectors
+// and with dF_new, as per-block partial sums part[blk][2 (m + 1)] that the
+// host adds in block order (so the coefficients are reproducible).
+constexpr int kAAMax = 8;
+struct AAVecs {
+    const double *df[kAAMax];
+};
+__global__ void __launch_bounds__(256) k_aa_dots(size_t n, int mh, AAVecs H, const double *__restrict__ f,
+                                                 double *__restrict__ fprev, double *__restrict__ dfn,
+                                                 double *__restrict__ part) {
+    double acc[2 * (kAAMax + 1)];
+#pragma unroll
+    for (int i = 0; i < 2 * (kAAMax + 1); i++) acc[i] = 0;
+    for (size_t t = gtid(); t < n; t += gstride()) {
+        const double fv = f[t], d = fv - fprev[t];
+        dfn[t] = d;
+        fprev[t] = fv;
+#pragma unroll
+        for (int i = 0; i < kAAMax; i++)
+            if (i < mh) {
+                const double h = H.df[i][t];
+                acc[2 * i] += d * h;
+                acc[2 * i + 1] += fv * h;
+            }
+        acc[2 * kAAMax] += d * d;
+        acc[2 * kAAMax + 1] += fv * d;
+    }
+    __shared__ double sred[2 * (kAAMax + 1)][8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < 2 * (kAAMax + 1); i++) {
+        const double v = warp_sum(acc[i]);
+        if (lane == 0) sred[i][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * (kAAMax + 1)) {
+        double v = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += sred[threadIdx.x][w];
+        part[(size_t)blockIdx.x * 2 * (kAAMax + 1) + threadIdx.x] = v;
+    }
+}
+
+// Anderson step, second pass: step = f - sum_i gamma_i (dX_i + dF_i),
+// lam += step, and the step is stored as the next dX (dxn).
+struct AAHist {
+    const double *dx[kAAMax];
+    const double *df[kAAMax];
+    double g[kAAMax];
+};
+__global__ void k_aa_update(size_t n, int mh, AAHist H, const double *__restrict__ f, double *__restrict__ lam,
+                            double *__restrict__ dxn) {
+    for (size_t t = gtid(); t < n; t += gstride()) {
+        double st = f[t];
+#pragma unroll
+        for (int i = 0; i < kAAMax; i++)
+            if (i < mh) st -= H.g[i] * (H.dx[i][t] + H.df[i][t]);
+        lam[t] += st;
+        dxn[t] = st;
+    }
+}
+
 // sum of squares of x[0 .. n) into *out (atomics per warp)
 __global__ void k_sqnorm(size_t n, const double *__restrict__ x, double *out) {
     double s2 = 0;
@@ -5056,6 +5159,27 @@ Error Solver::vjp(const double *Tbar_h, const double *qbar_h, int max_iter, doub
     std::vector<double> gt, gc, gb, pt, pc, pb;
     double change = 1.0, res0 = 0, resid = 1.0;
     int it = 0;
+    // Anderson acceleration buffers (cfg.adjoint_anderson vectors of history;
+    // 0 = the plain iteration): f, the previous f, per-block dot partials,
+    // and aa_m pairs of differences (dX, dF)
+    const int aa_m = std::min(std::max(cfg.adjoint_anderson, 0), kAAMax);
+    double *aa_f = nullptr, *aa_fprev = nullptr, *aa_part = nullptr;
+    double *aa_dx[kAAMax] = {}, *aa_df[kAAMax] = {};
+    int aa_head = 0, aa_n = 0;
+    bool aa_have_prev = false;
+    double aa_best = 1e300;
+    std::vector<double> aa_G((size_t)kAAMax * kAAMax, 0.0);
+    if (aa_m > 0) {
+        if (adj_aa_n_ < aa_m) {
+            adj_aa_ = (double *)dalloc((size_t)(2 * aa_m + 2) * ne * 8 + (size_t)1184 * 2 * (kAAMax + 1) * 8);
+            if (!adj_aa_) return {-6, "device allocation failed (adjoint acceleration history)"};
+            adj_aa_n_ = aa_m;
+        }
+        aa_f = adj_aa_;
+        aa_fprev = aa_f + ne;
+        for (int i = 0; i < aa_m; i++) aa_dx[i] = aa_fprev + ne + (size_t)(2 * i) * ne, aa_df[i] = aa_dx[i] + ne;
+        aa_part = aa_fprev + ne + (size_t)2 * aa_m * ne;
+    }
     for (;; it++) {
         Error ee = evaluate(lam, true, true);
         if (ee.code) return ee;
@@ -5085,8 +5209,118 @@ Error Solver::vjp(const double *Tbar_h, const double *qbar_h, int max_iter, doub
         pt.swap(gt);
         pc.swap(gc);
         pb.swap(gb);
-        CUDA_TRY(cudaMemsetAsync(red, 0, 2 * 8, s));
-        k_adj_update<<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, opp, (const double *)corr_, lam, red);
+        if (aa_m == 0) {
+            CUDA_TRY(cudaMemsetAsync(red, 0, 2 * 8, s));
+            k_adj_update<<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, opp, (const double *)corr_, lam, red);
+            CUDA_TRY(cudaGetLastError());
+            continue;
+        }
+        // Anderson acceleration of lam <- lam + f(lam), f = A^-T r(lam)
+        // (Walker and Ni's form, memory aa_m): lam <- lam + f - sum_i
+        // gamma_i (dX_i + dF_i), gamma the least-squares fit of f by the
+        // last aa_m differences dF_i of f (normal equations with a small
+        // Tikhonov term); the history restarts when the residual grows
+        // tenfold over its best
+        k_adj_fvec<<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, opp, (const double *)corr_, aa_f);
+        CUDA_TRY(cudaGetLastError());
+        if (resid < aa_best) aa_best = resid;
+        if (resid > 10 * aa_best) aa_n = 0, aa_have_prev = false, aa_best = resid;
+        if (!aa_have_prev) {
+            // first step after a (re)start: plain iteration, remember f
+            CUDA_TRY(cudaMemcpyAsync(aa_fprev, aa_f, ne * 8, cudaMemcpyDeviceToDevice, s));
+            AAHist H{};
+            k_aa_update<<<grid_for(ne), kThreads, 0, s>>>(ne, 0, H, aa_f, lam, aa_dx[aa_head]);
+            CUDA_TRY(cudaGetLastError());
+            aa_have_prev = true;  // aa_dx[aa_head] holds a step whose dF comes next
+            continue;
+        }
+        // the newest pair: dX = the last step (already in aa_dx[aa_head]),
+        // dF = f - f_prev (formed now into aa_df[aa_head])
+        // the pairs kept beside the new one: at most aa_m - 1, the oldest
+        // dropped (the new pair takes the ring slot aa_head)
+        const int kept = std::min(aa_n, aa_m - 1);
+        AAVecs V{};
+        int order[kAAMax], mh = 0;
+        for (int i = 0; i < kept; i++) {
+            const int slot = (aa_head - kept + i + aa_m) % aa_m;
+            order[mh] = slot;
+            V.df[mh++] = aa_df[slot];
+        }
+        const int nbk = std::min(grid_for(ne), 1184);
+        k_aa_dots<<<nbk, kThreads, 0, s>>>(ne, mh, V, aa_f, aa_fprev, aa_df[aa_head], aa_part);
+        CUDA_TRY(cudaGetLastError());
+        const int K = 2 * (kAAMax + 1);
+        std::vector<double> hp((size_t)nbk * K);
+        CUDA_TRY(cudaMemcpyAsync(hp.data(), aa_part, hp.size() * 8, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        std::vector<double> dots(K, 0.0);
+        for (int b = 0; b < nbk; b++)
+            for (int i = 0; i < K; i++) dots[i] += hp[(size_t)b * K + i];
+        // Gram matrix of the kept dF (older entries as stored), then the new one
+        const int newslot = aa_head;
+        for (int i = 0; i < mh; i++) {
+            aa_G[order[i] * kAAMax + newslot] = aa_G[newslot * kAAMax + order[i]] = dots[2 * i];
+        }
+        aa_G[newslot * kAAMax + newslot] = dots[2 * kAAMax];
+        aa_head = (aa_head + 1) % aa_m;
+        aa_n = kept + 1;
+        // the fit over the kept pairs (oldest first), newest included
+        int slots[kAAMax];
+        double bvec[kAAMax];
+        for (int i = 0; i < aa_n; i++) slots[i] = (aa_head - aa_n + i + aa_m) % aa_m;
+        for (int i = 0; i < aa_n; i++) {
+            const int sl = slots[i];
+            if (sl == newslot) {
+                bvec[i] = dots[2 * kAAMax + 1];
+            } else {
+                int j = 0;
+                while (order[j] != sl) j++;
+                bvec[i] = dots[2 * j + 1];
+            }
+        }
+        std::vector<double> A((size_t)aa_n * aa_n);
+        double tr = 0;
+        for (int i = 0; i < aa_n; i++) tr += aa_G[slots[i] * kAAMax + slots[i]];
+        for (int i = 0; i < aa_n; i++)
+            for (int j = 0; j < aa_n; j++)
+                A[(size_t)i * aa_n + j] = aa_G[slots[i] * kAAMax + slots[j]] + (i == j ? 1e-12 * tr / aa_n : 0.0);
+        // Gaussian elimination with partial pivoting (aa_n <= kAAMax)
+        std::vector<double> gam(bvec, bvec + aa_n);
+        bool ok = true;
+        for (int k = 0; k < aa_n && ok; k++) {
+            int pr = k;
+            for (int i = k + 1; i < aa_n; i++)
+                if (std::fabs(A[(size_t)i * aa_n + k]) > std::fabs(A[(size_t)pr * aa_n + k])) pr = i;
+            if (!(std::fabs(A[(size_t)pr * aa_n + k]) > 0)) {
+                ok = false;
+                break;
+            }
+            if (pr != k) {
+                for (int j = 0; j < aa_n; j++) std::swap(A[(size_t)k * aa_n + j], A[(size_t)pr * aa_n + j]);
+                std::swap(gam[k], gam[pr]);
+            }
+            for (int i = k + 1; i < aa_n; i++) {
+                const double f = A[(size_t)i * aa_n + k] / A[(size_t)k * aa_n + k];
+                for (int j = k; j < aa_n; j++) A[(size_t)i * aa_n + j] -= f * A[(size_t)k * aa_n + j];
+                gam[i] -= f * gam[k];
+            }
+        }
+        for (int k = aa_n - 1; k >= 0 && ok; k--) {
+            for (int j = k + 1; j < aa_n; j++) gam[k] -= A[(size_t)k * aa_n + j] * gam[j];
+            gam[k] /= A[(size_t)k * aa_n + k];
+            if (!std::isfinite(gam[k])) ok = false;
+        }
+        AAHist H{};
+        int mu = 0;
+        if (ok)
+            for (int i = 0; i < aa_n; i++) {
+                H.dx[mu] = aa_dx[slots[i]];
+                H.df[mu] = aa_df[slots[i]];
+                H.g[mu++] = gam[i];
+            }
+        else
+            aa_n = 0;  // singular fit: plain step, history restarts
+        k_aa_update<<<grid_for(ne), kThreads, 0, s>>>(ne, mu, H, aa_f, lam, aa_dx[aa_head]);
         CUDA_TRY(cudaGetLastError());
     }
     CUDA_TRY(cudaEventRecord(ev_[1], s));

@@ -55,6 +55,7 @@ struct SolverConfig {
     int sweep_far_slots = 0;  // far-slot cap of the sweep plan: 0 = automatic, < 0 = none
     int gradient_dirs = 0;    // gradient launch shape (1, 2, 4: directions per thread; 5, 6: warp per cell), 0 = automatic
     int residual_form = 0;    // residual launch shape (1: thread per cell; 5, 6: warp per cell), 0 = automatic
+    int adjoint_anderson = 6; // history of the adjoint's Anderson acceleration (0: plain iteration)
     int direction_batch = 0;  // most directions per transport batch, 0 = automatic
     std::vector<double> cell_scatter;  // scattering-rate multiplier s_c per cell (empty: 1)
     int order = 2;            // 2: second-order upwind faces (solve); 1: first order (solve_firstorder)
@@ -263,6 +264,8 @@ private:
     std::vector<int> spec_h_;  // specular source per (wall side, direction), host copy
     double *adj_warm_ = nullptr;  // reverse Picard solutions of the previous adjoint iteration
     int adj_warm_n_ = 0;
+    double *adj_aa_ = nullptr;    // Anderson history of the adjoint iteration (adj_aa_n_ pairs)
+    int adj_aa_n_ = 0;
     Error adj_setup();
 };
 

@@ -188,6 +188,9 @@ typedef struct {
     int residual_form;        /* launch shape of the second-order residual: 1 = a thread per cell
                                  and 4 bands, 5, 6 = a warp per cell as for gradient_dirs; 0 = the
                                  fastest on the first outer iteration. Results do not depend on it. */
+    int adjoint_history;      /* gbte_vjp: Anderson acceleration of the transposed iteration with
+                                 this many difference pairs (1..8); 0 = 6; -1 = the plain iteration
+                                 lam += A^-T r. The fixed point, and the stopping rule, are the same. */
 } gbte_options;
 
 #define GBTE_NUM_KERNELS 16
@@ -364,9 +367,10 @@ int gbte_get_geometry(gbte_handle *h, double *centers, double *volumes);
  * Any output may be NULL. It differentiates the fixed point the last
  * gbte_solve reached, implicitly: the adjoint state solves the transposed
  * equations by the transposed source iteration (sweeps in the opposite
- * directions, the transposed synthetic correction), until the residual of
- * the adjoint equations, ||(dF/de)^T lam + dJ/de||, is <= tol ||dJ/de||,
- * or max_iter iterations ran. Call it after a solve that
+ * directions, the transposed synthetic correction, Anderson-accelerated by
+ * default: options.adjoint_history), until the residual of the adjoint
+ * equations, ||(dF/de)^T lam + dJ/de||, is <= tol ||dJ/de||, or max_iter
+ * iterations ran. Call it after a solve that
  * converged to tight margins; the gradient is that of the state the solve
  * left. FP64 handles only (GBTE_ERR_UNSUPPORTED otherwise), not batched
  * handles. It keeps one more band-state array (Nd*Nc*Nb doubles) and

@@ -382,3 +382,23 @@ def test_config4_full_size_against_finite_differences():
         km = keff(*make(-H))
         fd = (kp - km) / (2 * H)
         assert abs(adj - fd) <= TOL * max(abs(fd), 1e-30), (name, adj, fd)
+
+
+def test_anderson_and_plain_adjoint_agree():
+    # the Anderson-accelerated transposed iteration (default) and the plain
+    # one (adjoint_history = -1) solve the same adjoint equations: the same
+    # gradient, both at the residual bound, the accelerated one in fewer
+    # iterations
+    out = {}
+    for hist in (-1, 0):
+        s = g.StaticBTESynthetic.from_deck(base_deck(), precision=g.GBTE_FP64, cell_scatter=scatter(),
+                                           adjoint_history=hist)
+        s.solve(allow_not_converged=False)
+        qb = s.keff_cotangent(axis=0, length=L, delta_T=1.0)
+        out[hist] = s.vjp(q_bar=qb, tol=1e-10, max_iter=20000)
+        s.close()
+        assert out[hist]["stats"]["residual"] <= 1e-10
+    a, p = out[0], out[-1]
+    for k in ("tau", "scatter"):
+        assert np.max(np.abs(a[k] - p[k])) <= 1e-7 * np.max(np.abs(p[k])), k
+    assert a["stats"]["iterations"] <= p["stats"]["iterations"]
