@@ -802,31 +802,7 @@ __global__ void __launch_bounds__(512) k_gradient_tile(DMesh m, DPhys p, const f
 #pragma unroll
             for (int v = 0; v < 4; v++) gx[v] = gy[v] = gz[v] = 0;
             const int qa = m.nbr_ptr[c] - qb0, qe = m.nbr_ptr[c + 1] - qb0;
-            if constexpr (sizeof(S) == 4) {
-                // two bands per instruction: packed f32x2 add and fma round
-                // each lane like the scalar fsub and (contracted) fma
-                const float2 n01 = make_float2(-ec[0], -ec[1]), n23 = make_float2(-ec[2], -ec[3]);
-                float2 x01 = make_float2(0.f, 0.f), x23 = x01, y01 = x01, y23 = x01, z01 = x01, z23 = x01;
-                for (int q = qa; q < qe; q++) {
-                    const TileW<S> t = wq[q];
-                    const float4 e = *reinterpret_cast<const float4 *>(et + (size_t)t.loc * nbc + 4 * j);
-                    const float2 d01 = __fadd2_rn(make_float2(e.x, e.y), n01);
-                    const float2 d23 = __fadd2_rn(make_float2(e.z, e.w), n23);
-                    const float2 wx = make_float2(t.wx, t.wx), wy = make_float2(t.wy, t.wy);
-                    x01 = __ffma2_rn(wx, d01, x01);
-                    x23 = __ffma2_rn(wx, d23, x23);
-                    y01 = __ffma2_rn(wy, d01, y01);
-                    y23 = __ffma2_rn(wy, d23, y23);
-                    if (DIM == 3) {
-                        const float2 wz = make_float2(t.wz, t.wz);
-                        z01 = __ffma2_rn(wz, d01, z01);
-                        z23 = __ffma2_rn(wz, d23, z23);
-                    }
-                }
-                gx[0] = x01.x, gx[1] = x01.y, gx[2] = x23.x, gx[3] = x23.y;
-                gy[0] = y01.x, gy[1] = y01.y, gy[2] = y23.x, gy[3] = y23.y;
-                gz[0] = z01.x, gz[1] = z01.y, gz[2] = z23.x, gz[3] = z23.y;
-            } else {
+            {
                 for (int q = qa; q < qe; q++) {
                     const TileW<S> t = wq[q];
                     S e[4];
