@@ -133,7 +133,7 @@ EXPORTS = ["gbte_inspect_deck", "gbte_inspect_mesh", "gbte_default_options", "gb
            "gbte_fourier_initial", "gbte_solve", "gbte_get_fields", "gbte_write_outputs", "gbte_get_sizes",
            "gbte_get_geometry", "gbte_last_error", "gbte_status_string", "gbte_destroy", "gbte_kernel_name",
            "gbte_solve_with", "gbte_fourier_initial_noalloc", "gbte_batch_create", "gbte_batch_geometries",
-           "gbte_vjp", "gbte_set_profile", "gbte_set_direction_shard"]
+           "gbte_vjp", "gbte_set_profile", "gbte_set_direction_shard", "gbte_options_size"]
 
 # int (*gbte_exchange_fn)(void *user, double *buf, size_t count, void *stream)
 EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
@@ -153,6 +153,10 @@ def library():
         lib.gbte_last_error.argtypes = [ctypes.c_void_p]
         lib.gbte_status_string.restype = ctypes.c_char_p
         lib.gbte_kernel_name.restype = ctypes.c_char_p
+        lib.gbte_options_size.restype = ctypes.c_size_t
+        if lib.gbte_options_size() != ctypes.sizeof(Options):
+            raise RuntimeError("libgiftbte_b200 was built from another include/giftbte.h (options size "
+                               f"{lib.gbte_options_size()} vs {ctypes.sizeof(Options)}); rebuild it")
         lib.gbte_create.argtypes = [ctypes.POINTER(MeshView), ctypes.POINTER(BandTableC), ctypes.POINTER(BCTable),
                                     ctypes.POINTER(AngleSpec), ctypes.POINTER(Options),
                                     ctypes.POINTER(ctypes.c_void_p)]

@@ -190,6 +190,8 @@ int create_common(const gbte::RawMesh &raw_in, const gbte::Bands &bands_in, cons
 
 extern "C" {
 
+size_t gbte_options_size(void) { return sizeof(gbte_options); }
+
 void gbte_default_options(gbte_options *o) {
     if (!o) return;
     std::memset(o, 0, sizeof(*o));

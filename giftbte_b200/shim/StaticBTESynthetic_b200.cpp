@@ -22,6 +22,12 @@ namespace {
 
 StaticBTESynthetic::StaticBTESynthetic(BTEMesh *mesh, BTEBoundaryCondition *bcs, BTEBand *bands, BTEAngle *angles,
                                        int num_proc, int world_rank) {
+    if (gbte_options_size() != sizeof(gbte_options)) {
+        std::cout << "B200 solver: libgiftbte_b200 was built from another giftbte.h (options of "
+                  << gbte_options_size() << " bytes, this class expects " << sizeof(gbte_options)
+                  << "); rebuild the drop-in" << std::endl;
+        std::exit(1);
+    }
     // the reference's constructor reads the same objects
     // (src/StaticBTESynthetic/StaticBTESynthetic.cpp:224-626)
     dimension = mesh->Dimension;

@@ -260,6 +260,11 @@ int gbte_inspect_mesh(const gbte_mesh_view *mesh, const gbte_band_table *bands, 
 /* Default options (FP64, max_iter 10000, margins 1e-6/1e-4 as the reference). */
 void gbte_default_options(gbte_options *opt);
 
+/* sizeof(gbte_options) as this library was built: a caller compiled against
+ * another version of this header can check it before passing options (no
+ * counterpart in the reference). */
+size_t gbte_options_size(void);
+
 int gbte_create(const gbte_mesh_view *mesh, const gbte_band_table *bands, const gbte_bc_table *bcs,
                 const gbte_angle_spec *angles, const gbte_options *opt, gbte_handle **out);
 

@@ -128,9 +128,13 @@ def run_reference(deck_root: str, timeout: float = 3600.0, binary: Optional[str]
     binary = binary or REF_BIN
     if not os.path.exists(binary):
         raise FileNotFoundError(binary)
-    with open(os.path.join(deck_root, "ref_run.log"), "w") as log:
-        subprocess.run([binary], cwd=deck_root, stdout=log, stderr=subprocess.STDOUT,
-                       timeout=timeout, check=True)
+    logp = os.path.join(deck_root, "ref_run.log")
+    with open(logp, "w") as log:
+        rc = subprocess.run([binary], cwd=deck_root, stdout=log, stderr=subprocess.STDOUT, timeout=timeout).returncode
+    if rc != 0:
+        with open(logp, errors="replace") as f:
+            tail = f.read()[-2000:]
+        raise RuntimeError(f"{os.path.basename(binary)} exited with {rc}; end of its log:\n{tail}")
     return read_reference_outputs(deck_root)
 
 
