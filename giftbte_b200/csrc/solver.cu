@@ -90,7 +90,8 @@ __global__ void k_init_eps(DMesh m, DPhys p, const double *__restrict__ T0, cons
     for (size_t t = gtid(); t < total; t += gstride()) {
         int b = (int)(t % p.nb);
         int c = (int)((t / p.nb) % m.nc);
-        eps[t] = (S)(p.C[b] * T0[c] - p.C[b] * Tb[c]);
+        const int mo = mat_off(p, c);
+        eps[t] = (S)(p.C[mo + b] * T0[c] - p.C[mo + b] * Tb[c]);
     }
 }
 
@@ -103,7 +104,7 @@ __global__ void k_rebase(DMesh m, DPhys p, const double *__restrict__ Tb_old, co
     for (size_t t = gtid(); t < total; t += gstride()) {
         const int b = (int)(t % p.nb);
         const int c = (int)((t / p.nb) % m.nc);
-        eps[t] = (S)((double)eps[t] + p.C[b] * (Tb_old[c] - Tb_new[c]));
+        eps[t] = (S)((double)eps[t] + p.C[mat_off(p, c) + b] * (Tb_old[c] - Tb_new[c]));
     }
 }
 
@@ -239,7 +240,8 @@ __global__ void __launch_bounds__(256) k_residual(DMesh m, DPhys p, EView<S, DIM
         const int c = (int)(dcl % nc);
         const size_t d = d0 + dcl / nc;
         const size_t dc = d * nc + c;
-        const double Cb = p.C[b], tau = p.tau[b], vm = p.vmag[b];
+        const int mo = mat_off(p, c);
+        const double Cb = p.C[mo + b], tau = p.tau[mo + b], vm = p.vmag[mo + b];
         const double vx = vm * p.sx[d], vy = vm * p.sy[d], vz = vm * p.sz[d];
         const double ec = ev.e(d, c, b, Cb);
         const double cx = m.cx[c], cy = m.cy[c], cz = m.cz[c], tsc = m.tsc[c], tv = tau * tsc / m.vol[c];
@@ -257,7 +259,7 @@ __global__ void __launch_bounds__(256) k_residual(DMesh m, DPhys p, EView<S, DIM
             }
             acc += tv * m.cf_area[k] * vn * x;
         }
-        const double r = Cb * Told[c] + m.heat[c] * p.hr[b] * tau * tsc - ec - acc;
+        const double r = Cb * Told[c] + m.heat[c] * p.hr[mo + b] * tau * tsc - ec - acc;
         Rlo[((d - d0) * nc + pos_of[dc]) * nb + b] = (S)r;
     }
 }
@@ -559,6 +561,7 @@ __global__ void __launch_bounds__(256, sizeof(S) == 4 ? 4 : 2) k_residual8(DMesh
         const int bc = (int)(t % nbc), b0 = BC * bc;
         const size_t dcl = t / nbc;  // (batch direction, cell)
         const int c = (int)(dcl % nc);
+        const int mo = mat_off(p, c);
         const size_t d = d0 + dcl / nc, dc = d * nc + c;
         const double sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
         const size_t dbase = d * nc, gbase = (d - d0) * nc;  // all directions / this batch
@@ -606,15 +609,15 @@ __global__ void __launch_bounds__(256, sizeof(S) == 4 ? 4 : 2) k_residual8(DMesh
             } else {
                 const double *e = eb + (d * m.nbs + m.cf_bside[k]) * nb + b0;
 #pragma unroll
-                for (int i = 0; i < BC; i++) acc[i] += a * (S)(e[i] - p.C[b0 + i] * tb);
+                for (int i = 0; i < BC; i++) acc[i] += a * (S)(e[i] - p.C[mo + b0 + i] * tb);
             }
         }
         const double dT = Told[c] - tb, B = Bf[dc], hc = m.heat[c] * tsc;
         S out[BC];
 #pragma unroll
         for (int i = 0; i < BC; i++) {
-            const double tv = p.tau[b0 + i] * p.vmag[b0 + i];
-            const S fixed = (S)(p.C[b0 + i] * (dT - tv * B) + hc * p.hr[b0 + i] * p.tau[b0 + i]);
+            const double tv = p.tau[mo + b0 + i] * p.vmag[mo + b0 + i];
+            const S fixed = (S)(p.C[mo + b0 + i] * (dT - tv * B) + hc * p.hr[mo + b0 + i] * p.tau[mo + b0 + i]);
             out[i] = fixed - ec[i] - (S)tv * acc[i];
         }
         st8(Rlo + (gbase + pos_of[dc]) * nb + b0, out);
@@ -641,6 +644,7 @@ __global__ void __launch_bounds__(256) k_residual_wc(DMesh m, DPhys p, EView<S, 
     const size_t wstr = ((size_t)gridDim.x * blockDim.x) >> 5;
     for (size_t w = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < items; w += wstr) {
         const int c = (int)(w % nc), grp = (int)(w / nc);
+        const int mo = mat_off(p, c);
         const double tsc = m.tsc[c], invV = tsc / m.vol[c], tb = ev.Tb[c];
         const double cx = m.cx[c], cy = m.cy[c], cz = DIM == 3 ? m.cz[c] : 0.0;
         size_t d[DG];
@@ -697,7 +701,7 @@ __global__ void __launch_bounds__(256) k_residual_wc(DMesh m, DPhys p, EView<S, 
                 } else {
                     const double *e = eb + (d[k] * m.nbs + m.cf_bside[f]) * nb + b0;
 #pragma unroll
-                    for (int i = 0; i < BC; i++) acc[k][i] += a * (S)(e[i] - p.C[b0 + i] * tb);
+                    for (int i = 0; i < BC; i++) acc[k][i] += a * (S)(e[i] - p.C[mo + b0 + i] * tb);
                 }
             }
         }
@@ -712,8 +716,8 @@ __global__ void __launch_bounds__(256) k_residual_wc(DMesh m, DPhys p, EView<S, 
             S out[BC];
 #pragma unroll
             for (int i = 0; i < BC; i++) {
-                const double tv = p.tau[b0 + i] * p.vmag[b0 + i];
-                const S fixed = (S)(p.C[b0 + i] * (dT - tv * B) + hc * p.hr[b0 + i] * p.tau[b0 + i]);
+                const double tv = p.tau[mo + b0 + i] * p.vmag[mo + b0 + i];
+                const S fixed = (S)(p.C[mo + b0 + i] * (dT - tv * B) + hc * p.hr[mo + b0 + i] * p.tau[mo + b0 + i]);
                 out[i] = fixed - ec[k][i] - (S)tv * acc[k][i];
             }
             st8(Rlo + ((size_t)dl * nc + pos_of[dc]) * nb + b0, out);
@@ -967,7 +971,10 @@ __global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int ncomp, int d0
             const SweepRec<S> r = st ? srec[li] : rec[P];
             S r0[VB];
             vld<S, VB>(st ? sR + li * nbc + lb : Rlo + L * nb + b0 + lb, r0);
-            const int nin = r.meta & 7, fw = (r.meta >> 3) - 1;
+            const int nin = r.meta & 7, fw = ((r.meta >> 3) & 0xFFFFF) - 1, mt = r.meta >> 24;
+            S kc[VB];
+#pragma unroll
+            for (int v = 0; v < VB; v++) kc[v] = mt ? (S)kbv[mt * nb + b0 + lb + v] : kb[v];
             S sum[VB];
 #pragma unroll
             for (int v = 0; v < VB; v++) sum[v] = (S)0;
@@ -988,7 +995,7 @@ __global__ void __launch_bounds__(256) k_sweep(int nb, int nc, int ncomp, int d0
             }
             S dv[VB];
 #pragma unroll
-            for (int v = 0; v < VB; v++) dv[v] = sweep_div(r0[v] - kb[v] * sum[v], (S)1 + kb[v] * r.sig);
+            for (int v = 0; v < VB; v++) dv[v] = sweep_div(r0[v] - kc[v] * sum[v], (S)1 + kc[v] * r.sig);
             vst<S, VB>(Dc + (lbase + r.cell) * nb + b0 + lb, dv);
             if (fw >= 0) vst<S, VB>(far + fw * nbc + lb, dv);
             vst<S, VB>(ring + ((c0 + li) & mask) * nbc + lb, dv);
@@ -1040,7 +1047,10 @@ __global__ void __launch_bounds__(1024) k_sweep_wide(int nb, int nc, int ncomp, 
                 const SweepRec<S> r = rec[base + p];
                 S r0[VB];
                 vld<S, VB>(Rlo + (lbase + p) * nb + b0 + lb, r0);
-                const int nin = r.meta & 7;
+                const int nin = r.meta & 7, mt = r.meta >> 24;
+                S kc[VB];
+#pragma unroll
+                for (int v = 0; v < VB; v++) kc[v] = mt ? (S)kbv[mt * nb + b0 + lb + v] : kb[v];
                 int cj[4];
 #pragma unroll
                 for (int j = 0; j < 4; j++) cj[j] = j < nin ? cells[r.np[j]] : 0;
@@ -1058,7 +1068,7 @@ __global__ void __launch_bounds__(1024) k_sweep_wide(int nb, int nc, int ncomp, 
                 }
                 S dv[VB];
 #pragma unroll
-                for (int v = 0; v < VB; v++) dv[v] = sweep_div(r0[v] - kb[v] * sum[v], (S)1 + kb[v] * r.sig);
+                for (int v = 0; v < VB; v++) dv[v] = sweep_div(r0[v] - kc[v] * sum[v], (S)1 + kc[v] * r.sig);
                 vst<S, VB>(Dd + (size_t)r.cell * nb, dv);
             }
         }
@@ -1159,7 +1169,10 @@ __global__ void __launch_bounds__(128) k_sweep_w(int nb, int nc, int ncomp, int 
             const SweepRec<S> r = st ? srec[li] : rec[P];
             S r0[VB];
             vld<S, VB>(st ? sR + li * VB : Rlo + L * nb + b0, r0);
-            const int nin = r.meta & 7, fw = (r.meta >> 3) - 1;
+            const int nin = r.meta & 7, fw = ((r.meta >> 3) & 0xFFFFF) - 1, mt = r.meta >> 24;
+            S kc[VB];
+#pragma unroll
+            for (int v = 0; v < VB; v++) kc[v] = mt ? (S)kbv[mt * nb + b0 + v] : kb[v];
             S sum[VB];
 #pragma unroll
             for (int v = 0; v < VB; v++) sum[v] = (S)0;
@@ -1180,7 +1193,7 @@ __global__ void __launch_bounds__(128) k_sweep_w(int nb, int nc, int ncomp, int 
             }
             S dv[VB];
 #pragma unroll
-            for (int v = 0; v < VB; v++) dv[v] = sweep_div(r0[v] - kb[v] * sum[v], (S)1 + kb[v] * r.sig);
+            for (int v = 0; v < VB; v++) dv[v] = sweep_div(r0[v] - kc[v] * sum[v], (S)1 + kc[v] * r.sig);
             vst<S, VB>(Dc + (lbase + r.cell) * nb + b0, dv);
             if (fw >= 0) vst<S, VB>(far + fw * VB, dv);
             vst<S, VB>(ring + ((c0 + li) & mask) * VB, dv);
@@ -1333,7 +1346,8 @@ __global__ void __launch_bounds__(256) k_moments(DMesh m, DPhys p, int cpb, S *_
     const int c = blockIdx.x * cpb + lc;
     double *mine = part + (size_t)threadIdx.x * kMomSlots;
     if (lc < cpb && c < nc) {
-        const double Cb = p.C[b];
+        const int mo = mat_off(p, c);
+        const double Cb = p.C[mo + b];
         const double base = Cb * Tb[c];
         double a[kWTab];
 #pragma unroll
@@ -1368,12 +1382,12 @@ __global__ void __launch_bounds__(256) k_moments(DMesh m, DPhys p, int cpb, S *_
             Tband[(size_t)b * nc + c] += a[0] / Cb;
         else
             Tband[(size_t)b * nc + c] = a[0] / Cb;
-        const double vm = p.vmag[b], lat = p.lat[b];
+        const double vm = p.vmag[mo + b], lat = p.lat[mo + b];
         const double tl = lat * a[0] / Cb;
-        const bool syn = p.hr[b] > 0;
-        const double f = p.tau[b] * vm * vm;
+        const bool syn = p.hr[mo + b] > 0;
+        const double f = p.tau[mo + b] * vm * vm;
         mine[0] = tl;
-        mine[1] = a[0] / p.capb;
+        mine[1] = a[0] / (p.mat ? p.capm[p.mat[c]] : p.capb);
         mine[2] = vm * a[1];
         mine[3] = vm * a[2];
         mine[4] = vm * a[3];
@@ -1390,7 +1404,7 @@ __global__ void __launch_bounds__(256) k_moments(DMesh m, DPhys p, int cpb, S *_
         for (int bb = 0; bb < nb; bb++) sum += part[((size_t)i * nb + bb) * kMomSlots + j];
         // later direction batches add to the first one's moments
         double *dst = j == 0 ? &Tlat[cc] : j == 1 ? &E[cc] : j < 5 ? &q[3 * cc + j - 2] : j == 5 ? &Th[cc] : &Q[6 * cc + j - 6];
-        if (j == 5) sum *= p.kappa;
+        if (j == 5) sum *= p.mat ? p.kap[p.mat[cc]] : p.kappa;
         *dst = accumulate ? *dst + sum : sum;
     }
 }
@@ -1407,11 +1421,11 @@ __global__ void k_bound_out(DMesh m, DPhys p, EView<S, DIM> ev, double *__restri
         const size_t d = t / ((size_t)nb * m.nbs);
         const int c = m.bs_cell[s];
         if (c < 0) continue;
-        const int k = m.bs_cf[s];
-        const double vm = p.vmag[b];
+        const int k = m.bs_cf[s], mo = mat_off(p, c);
+        const double vm = p.vmag[mo + b];
         const double vn = vm * p.sx[d] * m.cf_nx[k] + vm * p.sy[d] * m.cf_ny[k] + vm * p.sz[d] * m.cf_nz[k];
         if (vn >= 0) {
-            const double Cb = p.C[b];
+            const double Cb = p.C[mo + b];
             eb[t] = ev.e(d, c, b, Cb) +
                     ev.gdot(d, c, b, Cb, m.cf_fx[k] - m.cx[c], m.cf_fy[k] - m.cy[c], m.cf_fz[k] - m.cz[c]);
         }
@@ -1426,13 +1440,14 @@ __global__ void k_side_moments(DMesh m, DPhys p, const double *__restrict__ eb, 
     const int s = (int)(gtid() >> 5), lane = threadIdx.x & 31;
     if (s >= m.nbs) return;
     double th = 0, q6[6] = {0, 0, 0, 0, 0, 0};
-    if (m.bs_cell[s] >= 0) {
-        const int n = p.nd * p.nb;
+    const int sc = m.bs_cell[s];
+    if (sc >= 0) {
+        const int n = p.nd * p.nb, mo = mat_off(p, sc);
         for (int i = lane; i < n; i += 32) {
-            const int d = i / p.nb, b = i % p.nb;
+            const int d = i / p.nb, b = mo + i % p.nb;
             if (!(p.hr[b] > 0)) continue;
             const double w = p.w[d], sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
-            const double x = eb[((size_t)d * m.nbs + s) * p.nb + b];
+            const double x = eb[((size_t)d * m.nbs + s) * p.nb + b - mo];
             th += p.lat[b] * x * w / p.C[b];
             const double f = w * p.tau[b] * p.vmag[b] * p.vmag[b] * x;
             q6[0] += f * sx * sx;
@@ -1446,7 +1461,7 @@ __global__ void k_side_moments(DMesh m, DPhys p, const double *__restrict__ eb, 
     th = warp_sum(th);
     for (int i = 0; i < 6; i++) q6[i] = warp_sum(q6[i]);
     if (lane == 0) {
-        Ths[s] = p.kappa * th;
+        Ths[s] = (p.mat && sc >= 0 ? p.kap[p.mat[sc]] : p.kappa) * th;
         for (int i = 0; i < 6; i++) Qs[6 * s + i] = q6[i];
     }
 }
@@ -1592,16 +1607,18 @@ __global__ void k_gather(DMesh m, DPhys p, const double *__restrict__ dsum, cons
         const int s = (int)((t / nb) % m.nbs);
         const int d = (int)(t / ((size_t)nb * m.nbs));
         const int c = m.bs_cell[s];
-        if (c < 0 || p.hr[b] == 0) continue;
+        if (c < 0) continue;
+        const int mo = mat_off(p, c);
+        if (p.hr[mo + b] == 0) continue;
         const int k = m.bs_cf[s];
-        const double vm = p.vmag[b];
+        const double vm = p.vmag[mo + b];
         const double vn = vm * p.sx[d] * m.cf_nx[k] + vm * p.sy[d] * m.cf_ny[k] + vm * p.sz[d] * m.cf_nz[k];
         if (!(vn < 0)) continue;
         const int ib = s >> 1;
         const int type = m.b_type[ib];
         double val;
         if (type == 1) {
-            val = p.C[b] * m.b_T[ib];
+            val = p.C[mo + b] * m.b_T[ib];
         } else if (type == 2) {
             val = dsum[(size_t)s * nb + b];
         } else if (type == 3) {
@@ -1616,7 +1633,7 @@ __global__ void k_gather(DMesh m, DPhys p, const double *__restrict__ dsum, cons
         } else if (type < 0) {
             const int cb = m.b_connect[ib];
             const int ps = 2 * cb + (s & 1);
-            val = eb[((size_t)d * m.nbs + ps) * nb + b] + p.C[b] * (m.b_T[ib] - m.b_T[cb]);
+            val = eb[((size_t)d * m.nbs + ps) * nb + b] + p.C[mo + b] * (m.b_T[ib] - m.b_T[cb]);
         } else {
             continue;
         }
@@ -1631,10 +1648,10 @@ __global__ void k_macro_bc(DMesh m, DPhys p, const double *__restrict__ eb, cons
     if (s >= m.nbs) return;
     double acc = 0;
     if (m.bs_cell[s] >= 0) {
-        const int n = p.nd * p.nb;
+        const int n = p.nd * p.nb, mo = mat_off(p, m.bs_cell[s]);
         for (int i = lane; i < n; i += 32) {
             const int d = i / p.nb, b = i % p.nb;
-            acc += p.lat[b] * eb[((size_t)d * m.nbs + s) * p.nb + b] / p.C[b] * p.w[d];
+            acc += p.lat[mo + b] * eb[((size_t)d * m.nbs + s) * p.nb + b] / p.C[mo + b] * p.w[d];
         }
     }
     acc = warp_sum(acc);
@@ -1654,10 +1671,12 @@ __global__ void k_tinterp(DMesh m, const double *__restrict__ T, double *__restr
 }
 
 // macro right-hand side (negated for the SPD form -K T = -rhs)
-__global__ void k_macro_rhs(DMesh m, double kappa, const double *__restrict__ remacro, const double *__restrict__ bTm,
+__global__ void k_macro_rhs(DMesh m, double kappa0, const double *__restrict__ kap_m, const int *__restrict__ mat,
+                            const double *__restrict__ remacro, const double *__restrict__ bTm,
                             const double *__restrict__ TV, double *__restrict__ rhs_neg) {
     const int c = (int)gtid();
     if (c >= m.nc) return;
+    const double kappa = mat ? kap_m[mat[c]] : kappa0;  // kappa_bulk of the cell's material
     double r = remacro[c] - m.heat[c] * m.vol[c];
     for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
         const double nx = m.cf_nx[k], ny = m.cf_ny[k], nz = m.cf_nz[k], A = m.cf_area[k];
@@ -2275,8 +2294,6 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
     bands = b;
     ang = a;
     cfg = c;
-    if (bands.nmat != 1)
-        return {-8, "more than one material is not supported by this solver (interfaces between materials)"};
     if (cfg.use_limiter && cfg.precision != 0)
         return {-8, "Order=2limit (the gradient limiter) needs the FP64 form (GBTE_FP64)"};
     if (cfg.use_limiter && cfg.order != 2) return {-1, "the gradient limiter applies to the second-order scheme"};
@@ -2372,13 +2389,17 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
     DPhys &p = dp_;
     p.nb = nb;
     p.nd = nd;
-    p.vmag = up_d(std::vector<double>(bands.v.begin(), bands.v.begin() + nb));
-    p.tau = up_d(std::vector<double>(bands.tau.begin(), bands.tau.begin() + nb));
-    p.C = up_d(std::vector<double>(bands.C.begin(), bands.C.begin() + nb));
-    p.lat = up_d(std::vector<double>(bands.lat.begin(), bands.lat.begin() + nb));
-    p.hr = up_d(std::vector<double>(bands.hr.begin(), bands.hr.begin() + nb));
+    p.nmat = bands.nmat;
+    p.vmag = up_d(bands.v);
+    p.tau = up_d(bands.tau);
+    p.C = up_d(bands.C);
+    p.lat = up_d(bands.lat);
+    p.hr = up_d(bands.hr);
     p.kappa = bands.kappa[0];
     p.capb = bands.capb[0];
+    p.kap = up_d(bands.kappa);
+    p.capm = up_d(bands.capb);
+    p.mat = bands.nmat > 1 ? up_i(mesh.matter) : nullptr;
     p.sx = up_d(ang.sx);
     p.sy = up_d(ang.sy);
     p.sz = up_d(ang.sz);
@@ -2426,7 +2447,9 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
             const double f = rs[sp.cell[P]];
             for (int q = 0; q < 4; q++) sp.a[4 * P + q] *= f;
             sp.sig[P] *= f;
-            const int meta = sp.nin[P] | ((sp.far_w[P] + 1) << 3);
+            // meta: neighbour count (bits 0-2), 1 + far slot (bits 3-22), the
+            // cell's material (bits 24-30; its kb row in the sweep)
+            const int meta = sp.nin[P] | ((sp.far_w[P] + 1) << 3) | (mesh.matter[sp.cell[P]] << 24);
             if (f32) {
                 SweepRec<float> &r = recf[P];
                 for (int q = 0; q < 4; q++) r.np[q] = sp.np[4 * P + q], r.a[q] = (float)sp.a[4 * P + q];
@@ -2447,8 +2470,8 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
         CUDA_TRY(cudaMemcpyAsync(rec_, f32 ? (const void *)recf.data() : (const void *)recd.data(), rec_bytes,
                                  cudaMemcpyHostToDevice, s));
         CUDA_TRY(cudaStreamSynchronize(s));
-        std::vector<double> kb(nb);
-        for (int b2 = 0; b2 < nb; b2++) kb[b2] = bands.tau[b2] * bands.v[b2];
+        std::vector<double> kb((size_t)bands.nmat * nb);
+        for (size_t b2 = 0; b2 < kb.size(); b2++) kb[b2] = bands.tau[b2] * bands.v[b2];
         kb_ = up_d(kb);
         // angular weights of the moments: w, w s, w s s^T (xx xy xz yy yz zz)
         std::vector<double> wt((size_t)nd * 10);
@@ -2564,18 +2587,23 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
             }
         }
     bTovr_ = up_d(ovr);
-    // macro matrix (_get_coefficient_macro, :842-884), stored negated
+    // macro matrix (_get_coefficient_macro, :842-884), stored negated; each
+    // row uses kappa_bulk of its cell's material. Interior faces join cells
+    // of one material (materials meet at interface walls, which the macro
+    // system treats as walls), so the matrix stays symmetric
     {
-        const double kap = bands.kappa[0];
         std::vector<int> ptr(mesh.nc + 1, 0), idx;
         std::vector<double> val, dinv(mesh.nc);
         for (int c2 = 0; c2 < mesh.nc; c2++) {
+            const double kap = bands.kappa[mesh.matter.empty() ? 0 : mesh.matter[c2]];
             double diag = 0;
             std::vector<std::pair<int, double>> row;
             for (int k = mesh.cf_ptr[c2]; k < mesh.cf_ptr[c2 + 1]; k++) {
                 double temp = kap * mesh.cf_area[k];
                 if (mesh.cf_bound[k] == -1) {
                     int j = mesh.cf_nbr[k];
+                    if (bands.nmat > 1 && mesh.matter[j] != mesh.matter[c2])
+                        return {-8, "cells of two materials share a face that is not an interface wall (BC type 5)"};
                     double ax = mesh.cx[j] - mesh.cx[c2], ay = mesh.cy[j] - mesh.cy[c2], az = mesh.cz[j] - mesh.cz[c2];
                     temp = temp / (mesh.cf_nx[k] * ax + mesh.cf_ny[k] * ay + mesh.cf_nz[k] * az);
                     diag += -temp;
@@ -2856,6 +2884,8 @@ Error Solver::picard_components(double limit, std::vector<char> &done, double &i
 Error Solver::fourier_initial() {
     if (!initialised) return {-1, "solver not initialised"};
     if (fourier_singular_) return {-8, "Fourier pre-solve: no isothermal or temperature-jump boundary (singular system)"};
+    if (bands.nmat > 1)
+        return {-8, "the device Fourier pre-solve covers one material (start a multi-material solve from a given field)"};
     if (!have_initial_) return {-1, "set an initial temperature first"};
     cudaStream_t s = cfg.stream;
     const int nc = mesh.nc, nslot = mesh.nn * mesh.nmat;
@@ -3782,7 +3812,8 @@ Error Solver::solve_t(SolveStats &st) {
         while (internal > 1e-6) {
             GL(K_COPY, k_copy<<<gC, kThreads, 0, s>>>(T_, T1_, nc));
             GL(K_TINTERP, k_tinterp<<<gN, kThreads, 0, s>>>(dm_, T_, TV_));
-            GL(K_MACRO_RHS, k_macro_rhs<<<gC, kThreads, 0, s>>>(dm_, dp_.kappa, remacro_, bTm_, TV_, rhs_));
+            GL(K_MACRO_RHS, k_macro_rhs<<<gC, kThreads, 0, s>>>(dm_, dp_.kappa, dp_.kap, dp_.mat, remacro_, bTm_, TV_,
+                                                               rhs_));
             CUDA_TRY(cudaGetLastError());
             // warm start from this Picard step's solution of the previous
             // outer iteration; tolerance tightens with the outer margin
@@ -4015,6 +4046,8 @@ Error Solver::fourier_initial_noalloc() {
     if (!initialised) return {-1, "solver not initialised"};
     if (!have_initial_) return {-1, "set an initial temperature first"};
     if (fourier_singular_) return {-8, "Fourier pre-solve: no isothermal or temperature-jump boundary (singular system)"};
+    if (bands.nmat > 1)
+        return {-8, "the device Fourier pre-solve covers one material (start a multi-material solve from a given field)"};
     if (ncomp_ > 1) return {-8, "the allocation-free Fourier pre-solve serves single-geometry handles"};
     const int nc = mesh.nc, nslot = mesh.nn * mesh.nmat;
     if (nc > kNoAllocMaxCells || nslot > kNoAllocMaxCells)
@@ -4952,6 +4985,7 @@ Error Solver::vjp(const double *Tbar_h, const double *qbar_h, int max_iter, doub
     if (need_snapshot_) return {-8, "the adjoint does not support chained specular reflections"};
     if (cfg.order != 2 || cfg.sequential || cfg.use_limiter)
         return {-8, "the adjoint is implemented for the second-order Synthetic scheme without limiter only"};
+    if (bands.nmat > 1) return {-8, "the adjoint covers one material"};
     if (ndb_ < ang.nd) return {-8, "the adjoint needs every direction's buffers resident (direction_batch)"};
     if (xfn_) return {-8, "the adjoint is not implemented for direction-sharded handles"};
     if (max_iter < 1 || !(tol > 0)) return {-1, "invalid adjoint limits"};

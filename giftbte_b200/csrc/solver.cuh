@@ -33,13 +33,18 @@ struct DMesh {
     const double *node_x, *node_y, *node_z;
 };
 
-// Single-material band/direction constants.
+// Band/direction constants. Band arrays are material-major [m * nb + b];
+// mat[c] is cell c's material (nullptr with one material, whose offset is 0).
 struct DPhys {
-    int nb, nd;
-    const double *vmag, *tau, *C, *lat, *hr;  // [nb]
-    double kappa, capb;
+    int nb, nd, nmat;
+    const double *vmag, *tau, *C, *lat, *hr;  // [nmat * nb]
+    double kappa, capb;                       // material 0's (the one material of most decks)
+    const double *kap, *capm;                 // [nmat] kappa_bulk and C_bulk per material
+    const int *mat;                           // [nc] or nullptr
     const double *sx, *sy, *sz, *w;           // [nd]
 };
+// band-array offset of cell c's material
+__host__ __device__ __forceinline__ int mat_off(const DPhys &p, int c) { return p.mat ? p.mat[c] * p.nb : 0; }
 
 struct SolverConfig {
     int precision = 0;
