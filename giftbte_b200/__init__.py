@@ -62,7 +62,8 @@ class BandTableC(ctypes.Structure):
 
 
 class BCTable(ctypes.Structure):
-    _fields_ = [("num", ctypes.c_int), ("tag", _c_int_p), ("type", _c_int_p), ("value", _c_dbl_p)]
+    _fields_ = [("num", ctypes.c_int), ("tag", _c_int_p), ("type", _c_int_p), ("value", _c_dbl_p),
+                ("transmissivity", _c_dbl_p)]
 
 
 class AngleSpec(ctypes.Structure):

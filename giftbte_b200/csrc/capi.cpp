@@ -244,10 +244,19 @@ static int convert_views(const gbte_mesh_view *mv, const gbte_band_table *bt, co
     B.region_material.assign(bt->region_material, bt->region_material + bt->num_regions);
     for (int r : B.region_material)
         if (r < 0 || r >= B.nmat) return fail(nullptr, {-1, "region_material out of range"}), GBTE_ERR_ARG;
+    bool any5 = false;
     for (int i = 0; i < bc->num; i++) {
         bcs.tag.push_back(bc->tag[i]);
         bcs.type.push_back(bc->type[i]);
         bcs.value.push_back(bc->value[i]);
+        if (bc->type[i] == 4)
+            return fail(nullptr, {-8, "BC type 4 has no steady-state branch in the reference solver"}), GBTE_ERR_UNSUPPORTED;
+        any5 = any5 || bc->type[i] == 5;
+    }
+    if (any5) {
+        if (!bc->transmissivity)
+            return fail(nullptr, {-1, "a type-5 interface row needs the transmissivity table"}), GBTE_ERR_ARG;
+        bcs.trans.assign(bc->transmissivity, bc->transmissivity + (size_t)bc->num * B.nmat * B.nb);
     }
     return GBTE_OK;
 }

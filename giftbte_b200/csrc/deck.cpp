@@ -321,17 +321,48 @@ Error read_deck(const std::string &root, Deck &D) {
         int num = 0;
         f >> num;
         for (int i = 0; i < 3; i++) std::getline(f, str);
+        std::vector<std::vector<double>> rows;  // transmissivity per row, [nmat * nb]
+        bool any5 = false;
         for (int i = 0; i < num; i++) {
             int idx, type;
             double val;
             if (!(f >> idx >> type)) return {-2, "BC file truncated"};
-            if (type == 4 || type == 5) return {-8, "interface boundaries (type 4/5) are not supported"};
+            if (type == 4) return {-8, "BC type 4 has no steady-state branch in the reference solver"};
             f >> val;
+            std::vector<double> tr((size_t)B.nmat * B.nb, 0.0);
+            if (type == 5) {
+                // interface wall: value, then the transmissivity file
+                // (BTEBoundaryCondition.cpp:22-35): blocks that start at a
+                // line naming "matter" (its first token the 0-based
+                // material), one value per line, ended by a short line
+                std::string tfile;
+                f >> tfile;
+                std::ifstream tf(resolve(root, tfile));
+                if (!tf.is_open()) return {-2, "interface file not open: " + tfile};
+                std::string line;
+                while (std::getline(tf, line)) {
+                    size_t at = line.find("matter");
+                    if (at == std::string::npos || at == 0) continue;
+                    const int mt = std::atoi(line.substr(0, line.find(' ')).c_str());
+                    if (mt < 0 || mt >= B.nmat) return {-2, "interface file names an unknown material: " + tfile};
+                    int b = 0;
+                    while (std::getline(tf, line)) {
+                        if (line.length() <= 1) break;
+                        if (b < B.nb) tr[(size_t)mt * B.nb + b] = std::atof(line.c_str());
+                        b++;
+                    }
+                    if (b != B.nb) return {-2, "interface file: band count differs from the band table: " + tfile};
+                }
+                any5 = true;
+            }
             std::getline(f, str);
             D.bcs.tag.push_back(idx);
             D.bcs.type.push_back(type);
             D.bcs.value.push_back(val);
+            rows.push_back(tr);
         }
+        if (any5)
+            for (auto &r : rows) D.bcs.trans.insert(D.bcs.trans.end(), r.begin(), r.end());
     }
     // mesh
     {

@@ -36,6 +36,7 @@ struct Bands {
 struct BCs {
     std::vector<int> tag, type;
     std::vector<double> value;
+    std::vector<double> trans;  // [rows][nmat * nb] transmissivity of type-5 rows (empty: none)
 };
 
 struct Angles {
@@ -71,6 +72,7 @@ struct FlatMesh {
     std::vector<int> b_type, b_connect, b_tag;
     std::vector<double> b_T;
     std::vector<int> bs_cell, bs_cf;  // [2*nbd], -1 if absent
+    std::vector<double> bs_trans;     // [2*nbd][nb] transmissivity seen from each side (type 5), else empty
     // node slots (node*nmat + matter): inverse-distance interpolation.
     // e-interpolation with boundary override (StaticBTESynthetic.cpp:1541-1616):
     // src >= 0 is a cell, src < 0 is boundary side (-1 - src)

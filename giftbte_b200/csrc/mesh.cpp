@@ -330,6 +330,20 @@ Error build_flat_mesh(const RawMesh &raw, const BCs &bcs, const Bands &bands, Fl
     }
     for (int k = 0; k < ncf; k++)
         if (m.cf_bound[k] < 0 && m.cf_nbr[k] < 0) return {-7, "a face is neither an interior face nor on a boundary in the BC table"};
+    // interface walls (type 5): each side's transmissivity is the table row
+    // of its cell's material (BTEMesh.cpp:495-510)
+    for (int ib = 0; ib < nbd; ib++) {
+        if (m.b_type[ib] != 5) continue;
+        if (m.bs_cell[2 * ib] < 0 || m.bs_cell[2 * ib + 1] < 0)
+            return {-7, "an interface wall (type 5) needs a cell on each side"};
+        if (bcs.trans.empty()) return {-1, "an interface wall (type 5) needs the transmissivity table"};
+        if (m.bs_trans.empty()) m.bs_trans.assign((size_t)2 * nbd * bands.nb, 0.0);
+        for (int ic = 0; ic < 2; ic++) {
+            const int mt = m.matter[m.bs_cell[2 * ib + ic]];
+            const double *row = &bcs.trans[((size_t)b_row[ib] * bands.nmat + mt) * bands.nb];
+            std::copy(row, row + bands.nb, m.bs_trans.begin() + (size_t)(2 * ib + ic) * bands.nb);
+        }
+    }
     for (int k = 0; k < ncf; k++)
         if (m.cf_bound[k] >= 0) m.cf_nbr[k] = m.cf_nbr[k];  // boundary faces keep their neighbour for the face list
     // periodic partners: candidates are the boundaries whose type names this
@@ -801,6 +815,8 @@ void reorder_cells(RawMesh &raw, const std::vector<int> &perm) {
 Error make_union(const std::vector<RawMesh> &meshes, const std::vector<BCs> &bcs, RawMesh &out, BCs &out_bcs) {
     const int n = (int)meshes.size();
     if (n <= 0 || (int)bcs.size() != n) return {-1, "a batch needs at least one geometry and one BC table each"};
+    for (int k = 0; k < n; k++)
+        if (!bcs[k].trans.empty()) return {-8, "interface walls (type 5) are not supported in a batched solve"};
     int span = 1;  // tags of geometry k are shifted by k * span
     for (int k = 0; k < n; k++) {
         for (int t : meshes[k].btag) span = std::max(span, t + 1);

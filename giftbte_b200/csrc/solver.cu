@@ -1587,9 +1587,24 @@ __global__ void k_diffuse_sum(DMesh m, DPhys p, const double *__restrict__ dif_w
     const size_t total = (size_t)m.nbs * nb;
     for (size_t t = gtid(); t < total; t += gstride()) {
         const int b = (int)(t % nb), s = (int)(t / nb);
-        if (m.bs_cell[s] < 0 || (m.b_type[s >> 1] != 2 && m.b_type[s >> 1] != 6)) continue;
+        const int type = m.b_type[s >> 1];
+        if (m.bs_cell[s] < 0 || (type != 2 && type != 6 && type != 5)) continue;
         double acc = 0;
         const double *w = dif_w + (size_t)s * p.nd;
+        if (type == 5) {
+            // interface: (1 - t) (|v_1| <e_out,1> + |v_2| <e_out,2>) / |v_1|,
+            // side 1 this one, side 2 the other, t this side's transmissivity
+            double a1 = 0, a2 = 0;
+            for (int q = 0; q < p.nd; q++) {
+                const double wq = w[q];
+                if (wq > 0) a1 += wq * eb[((size_t)q * m.nbs + s) * nb + b];
+                else if (wq < 0) a2 -= wq * eb[((size_t)q * m.nbs + (s ^ 1)) * nb + b];
+            }
+            const double v1 = p.vmag[mat_off(p, m.bs_cell[s]) + b], v2 = p.vmag[mat_off(p, m.bs_cell[s ^ 1]) + b];
+            const double tr = m.bs_trans[(size_t)s * nb + b];
+            dsum[t] = (v1 * a1 * (1 - tr) + v2 * a2 * (1 - tr)) / v1;
+            continue;
+        }
         for (int q = 0; q < p.nd; q++) {
             const double wq = w[q];
             if (wq != 0) acc += wq * eb[((size_t)q * m.nbs + s) * nb + b];
@@ -1619,7 +1634,7 @@ __global__ void k_gather(DMesh m, DPhys p, const double *__restrict__ dsum, cons
         double val;
         if (type == 1) {
             val = p.C[mo + b] * m.b_T[ib];
-        } else if (type == 2) {
+        } else if (type == 2 || type == 5) {
             val = dsum[(size_t)s * nb + b];
         } else if (type == 3) {
             const int src = spec_src[(size_t)s * p.nd + d];
@@ -2375,6 +2390,7 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
     d.b_T = up_d(mesh.b_T);
     d.bs_cell = up_i(mesh.bs_cell);
     d.bs_cf = up_i(mesh.bs_cf);
+    d.bs_trans = mesh.bs_trans.empty() ? nullptr : up_d(mesh.bs_trans);
     d.nv_ptr = up_i(mesh.nv_ptr);
     d.nv_src = up_i(mesh.nv_src);
     d.nv_w = up_d(mesh.nv_w);
@@ -2511,6 +2527,22 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
             for (int q = 0; q < nd; q++) {
                 double dn = ang.sx[q] * nx + ang.sy[q] * ny + ang.sz[q] * nz;
                 if (dn >= 0) difw[(size_t)sd * nd + q] = dn * ang.w[q] / tot;
+            }
+        }
+        if (type == 5) {
+            // interface wall (StaticBTESynthetic.cpp:2152-2190): the outgoing
+            // directions of this side (s.n >= 0) weigh its own outgoing values,
+            // the others the other side's; stored with a minus sign for the
+            // latter, each half normalised by its own sum of (s.n) w
+            double t1 = 0, t2 = 0;
+            for (int q = 0; q < nd; q++) {
+                double dn = ang.sx[q] * nx + ang.sy[q] * ny + ang.sz[q] * nz;
+                if (dn >= 0) t1 += dn * ang.w[q];
+                else t2 += dn * ang.w[q];
+            }
+            for (int q = 0; q < nd; q++) {
+                double dn = ang.sx[q] * nx + ang.sy[q] * ny + ang.sz[q] * nz;
+                difw[(size_t)sd * nd + q] = dn >= 0 ? dn * ang.w[q] / t1 : -(dn * ang.w[q] / t2);
             }
         }
         if (type == 3) {

@@ -26,6 +26,7 @@ struct DMesh {
     const int *b_type, *b_connect;
     const double *b_T;
     const int *bs_cell, *bs_cf;
+    const double *bs_trans;  // [2*nbd][nb] interface transmissivity per side, or nullptr
     const int *nv_ptr, *nv_src;
     const double *nv_w;
     const int *nt_ptr, *nt_src;

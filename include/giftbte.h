@@ -102,7 +102,8 @@ typedef struct {
 } gbte_band_table;
 
 /* Boundary conditions: type 1 isothermal (value = wall T), 2 diffuse,
- * 3 specular, < 0 periodic (partner tag = -type, value = temperature jump),
+ * 3 specular, 5 interface between two materials (transmissivity table
+ * below), < 0 periodic (partner tag = -type, value = temperature jump),
  * 6 partially specular (value = specularity p in [0, 1]; no counterpart in
  * the reference): an incoming intensity is p times the outgoing value of the
  * outgoing direction nearest its mirror image plus (1 - p) times the diffuse
@@ -113,6 +114,12 @@ typedef struct {
     const int *tag;
     const int *type;
     const double *value;
+    /* type 5 (interface wall between two materials,
+     * StaticBTESynthetic.cpp:2152-2190): the transmissivity of every band
+     * from each material's side, [num][num_materials * num_bands], rows of
+     * other types ignored (the interface file's "matter" blocks,
+     * BTEBoundaryCondition.cpp:22-35). NULL when no row has type 5. */
+    const double *transmissivity;
 } gbte_bc_table;
 
 typedef struct {
