@@ -503,19 +503,30 @@ def _views(deck) -> dict:
                   _ptr(cverts, ctypes.c_int), _ptr(creg, ctypes.c_int), _ptr(bptr, ctypes.c_int),
                   _ptr(bverts, ctypes.c_int), _ptr(btag, ctypes.c_int), deck.scale[0], deck.scale[1],
                   deck.scale[2] if len(deck.scale) > 2 else 1.0)
-    B = deck.bands
-    arrs = [np.ascontiguousarray(getattr(B, k), dtype=np.float64)
+    mats = deck.materials if hasattr(deck, "materials") else [deck.bands]
+    nb = mats[0].n_bands
+    arrs = [np.ascontiguousarray(np.concatenate([np.asarray(getattr(B, k), dtype=np.float64) for B in mats]))
             for k in ("v", "tau", "C", "lattice_ratio", "heat_ratio")]
-    reg = np.zeros(max(1, int(np.max(creg)) + 1), dtype=np.int32)
-    bt = BandTableC(1, B.n_bands, *[_ptr(a, ctypes.c_double) for a in arrs], len(reg),
+    nreg = max(1, int(np.max(creg)) + 1)
+    rmat = deck.region_materials() if hasattr(deck, "region_materials") else [0] * nreg
+    reg = np.zeros(nreg, dtype=np.int32)
+    reg[:min(nreg, len(rmat))] = np.asarray(rmat, dtype=np.int32)[:nreg]
+    bt = BandTableC(len(mats), nb, *[_ptr(a, ctypes.c_double) for a in arrs], len(reg),
                     _ptr(reg, ctypes.c_int), deck.material_dim)
     tags = np.asarray([b.tag for b in deck.bcs], dtype=np.int32)
     types = np.asarray([b.type for b in deck.bcs], dtype=np.int32)
     vals = np.asarray([b.value for b in deck.bcs], dtype=np.float64)
-    bc = BCTable(len(deck.bcs), _ptr(tags, ctypes.c_int), _ptr(types, ctypes.c_int), _ptr(vals, ctypes.c_double))
+    trans = None
+    if any(b.type == 5 for b in deck.bcs):
+        trans = np.zeros((len(deck.bcs), len(mats) * nb))
+        for i, b in enumerate(deck.bcs):
+            if b.type == 5:
+                trans[i] = np.asarray(b.trans, dtype=np.float64).reshape(-1)
+    bc = BCTable(len(deck.bcs), _ptr(tags, ctypes.c_int), _ptr(types, ctypes.c_int), _ptr(vals, ctypes.c_double),
+                 _ptr(trans, ctypes.c_double))
     an = AngleSpec(deck.angle_method, deck.n_theta, deck.n_phi)
     return {"mv": mv, "bt": bt, "bc": bc, "an": an,
-            "keep": (xyz, cptr, cverts, creg, bptr, bverts, btag, arrs, reg, tags, types, vals)}
+            "keep": (xyz, cptr, cverts, creg, bptr, bverts, btag, arrs, reg, tags, types, vals, trans)}
 
 
 def inspect(deck) -> dict:

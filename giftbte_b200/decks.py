@@ -481,11 +481,28 @@ def write_band_database(path: str, bands: BandTable) -> None:
                     f"{bands.lattice_ratio[i]:.17g} {bands.heat_ratio[i]:.17g}\n")
 
 
+def write_interface_file(path: str, trans) -> None:
+    """The reference's interface file: per material a line "<m> # matter
+    index" (0-based) and one transmissivity per band, blocks separated by
+    an empty line."""
+    t = np.asarray(trans, dtype=np.float64)
+    with open(path, "w") as f:
+        for m in range(t.shape[0]):
+            f.write(f"{m} # matter index\n")
+            for v in t[m]:
+                f.write(f"{v:.17g}\n")
+            f.write("\n")
+
+
 @dataclasses.dataclass
 class BC:
     tag: int
-    type: int      # 1 isothermal, 2 diffuse, 3 specular, <0 periodic (partner = -type), 6 partially specular
+    type: int      # 1 isothermal, 2 diffuse, 3 specular, 5 interface, <0 periodic (partner = -type),
+                   # 6 partially specular
     value: float   # wall temperature / periodic temperature jump / specularity (type 6)
+    # type 5: transmissivity of every band from each material's side,
+    # (n_materials, n_bands); written as the reference's interface file
+    trans: Optional[np.ndarray] = None
 
 
 @dataclasses.dataclass
@@ -509,6 +526,20 @@ class Deck:
     heat_source: Optional[float] = None   # uniform volumetric heat (W/m^3)
     mesh_format: str = "COMSOL"           # COMSOL or MSH (3D meshes: MSH)
     region_heat: Optional[List[float]] = None  # heat per region (W/m^3), HeatType REGION
+    # more materials: extra_materials[k] is material k + 1 (material 0 is
+    # `bands`, same band count); region_material[r] is region r's material
+    # (0-based; None: every region is material 0)
+    extra_materials: List[BandTable] = dataclasses.field(default_factory=list)
+    region_material: Optional[List[int]] = None
+
+    @property
+    def materials(self) -> List[BandTable]:
+        return [self.bands] + list(self.extra_materials)
+
+    def region_materials(self) -> List[int]:
+        if self.region_material is not None:
+            return list(self.region_material)
+        return [0] * self.n_regions
 
     @property
     def dimension(self) -> int:
@@ -539,12 +570,21 @@ class Deck:
             write_mphtxt(os.path.join(d, mesh_name), self.mesh)
         else:
             write_msh41(os.path.join(d, mesh_name), self.mesh)
-        write_band_database(os.path.join(d, "bands.dat"), self.bands)
+        band_files = []
+        for k, bt in enumerate(self.materials):
+            name = "bands.dat" if k == 0 else f"bands_{k + 1}.dat"
+            write_band_database(os.path.join(d, name), bt)
+            band_files.append(name)
         with open(os.path.join(d, "bc.dat"), "w") as f:
             f.write(f"{len(self.bcs)} #Number of boundaries\n\n")
             f.write("BoundaryIndex BoundaryType BoundaryValue\n")
             for b in self.bcs:
-                f.write(f"{b.tag} {b.type} {b.value:.17g}\n")
+                if b.type == 5:
+                    tname = f"interface_{b.tag}.dat"
+                    write_interface_file(os.path.join(d, tname), b.trans)
+                    f.write(f"{b.tag} {b.type} {b.value:.17g} input/{tname}\n")
+                else:
+                    f.write(f"{b.tag} {b.type} {b.value:.17g}\n")
         with open(os.path.join(d, "CONTROL"), "w") as f:
             f.write("State=\nSteady\nOrder=\n%s\nIterativeScheme=\n%s\nMatrixSolver=\nLU\n"
                     "Tref=\n%.17g\nMaxNumIter=\n%d\nResidualTemp=\n%.17g\nResidualFlux=\n%.17g\n"
@@ -565,11 +605,14 @@ class Deck:
                 f.write(f"{len(self.region_heat)}\n")
                 for i, q in enumerate(self.region_heat):
                     f.write(f"{i + 1} {q:.17g}\n")
+        rm = self.region_materials()
         with open(os.path.join(d, "PHONON"), "w") as f:
-            f.write("MaterialNumber=\n1\nBandNumber=\n%d\n\nMaterialFile 1= DATABASE\ninput/bands.dat\n\n"
-                    "GeometryMaterialType=\n%s\n\nMaterialDimension=\n%d\nAngle_method=\n%d\n"
+            f.write("MaterialNumber=\n%d\nBandNumber=\n%d\n\n" % (len(band_files), self.bands.n_bands))
+            for k, name in enumerate(band_files):
+                f.write("MaterialFile %d= DATABASE\ninput/%s\n\n" % (k + 1, name))
+            f.write("GeometryMaterialType=\n%s\n\nMaterialDimension=\n%d\nAngle_method=\n%d\n"
                     "Ntheta=\n%d\nNphi=\n%d\n"
-                    % (self.bands.n_bands, "\n".join(f"{r + 1} 1" for r in range(self.n_regions)),
+                    % ("\n".join(f"{r + 1} {rm[r] + 1}" for r in range(self.n_regions)),
                        self.material_dim, self.angle_method, self.n_theta, self.n_phi))
         return d
 
@@ -577,6 +620,43 @@ class Deck:
 # ----------------------------------------------------------------------------
 # the named workloads
 # ----------------------------------------------------------------------------
+def two_region_tri_mesh(nx: int, ny: int) -> Mesh2D:
+    """square_tri_mesh with the cells right of x = 1/2 in region 1 and the
+    edges on x = 1/2 as boundary elements of tag 5 (nx even): two materials
+    meeting at an interface wall."""
+    if nx % 2:
+        raise ValueError("nx must be even")
+    m = square_tri_mesh(nx, ny)
+    cen = m.nodes[np.asarray(m.cells)].mean(axis=1)
+    region = (cen[:, 0] > 0.5).astype(np.int64)
+
+    def nid(i, j):
+        return i * (ny + 1) + j
+    i = nx // 2
+    extra = [(nid(i, j), nid(i, j + 1)) for j in range(ny)]
+    edges = np.concatenate([np.asarray(m.edges), np.asarray(extra, dtype=np.int64)])
+    tags = np.concatenate([np.asarray(m.edge_tags), np.full(len(extra), 5, dtype=np.int64)])
+    return Mesh2D(nodes=m.nodes, cells=m.cells, edges=edges, edge_tags=tags, cell_region=region)
+
+
+def interface_deck(n: int = 16, n_bands: int = 4, n_phi: int = 4, **kw) -> Deck:
+    """Two materials in a 100 nm square, meeting at x = 50 nm across an
+    interface wall (BC type 5): left material the sine-dispersion bands,
+    right material the same bands with group velocities x0.6 and relaxation
+    times x1.5; band transmissivities from the left side 0.2 .. 0.8, from
+    the right side 0.7 .. 0.1. Left wall 301 K, right wall 299 K, top and
+    bottom specular."""
+    left = sine_dispersion_bands(n_bands)
+    right = dataclasses.replace(left, v=left.v * 0.6, tau=left.tau * 1.5)
+    t = np.stack([np.linspace(0.2, 0.8, n_bands), np.linspace(0.7, 0.1, n_bands)])
+    bcs = [BC(1, 1, 301.0), BC(2, 1, 299.0), BC(3, 3, 0.0), BC(4, 3, 0.0), BC(5, 5, 0.0, trans=t)]
+    kw.setdefault("n_phi", n_phi)
+    kw.setdefault("angle_method", 1)
+    kw.setdefault("tref", 300.0)
+    return Deck(mesh=two_region_tri_mesh(n, n), bands=left, bcs=bcs, scale=(1e-7, 1e-7),
+                extra_materials=[right], region_material=[0, 1], **kw)
+
+
 def config1_deck(n: int = 40, **kw) -> Deck:
     """Gray 2D square, 1 um x 1 um, n x n squares split into 2 triangles,
     |v| = 6400 m/s, MFP 100 nm, C = 1.66e6 J/m^3K, 32 CADOM directions,

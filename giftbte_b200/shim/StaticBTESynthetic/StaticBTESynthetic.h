@@ -95,7 +95,7 @@ private:
     // the handle, which is created by the first solve: the variant's order,
     // scheme and limiter are options of gbte_create)
     std::vector<double> node_xyz_, cell_heat_, band_v_, band_tau_, band_C_, band_lat_, band_hr_;
-    std::vector<double> dir_xyz_, dir_w_, bc_value_;
+    std::vector<double> dir_xyz_, dir_w_, bc_value_, bc_trans_;
     std::vector<int> cell_ptr_, cell_verts_, cell_region_, belem_ptr_, belem_verts_, belem_tag_;
     std::vector<int> region_material_, bc_tag_, bc_type_;
     double scale_[3] = {1, 1, 1};

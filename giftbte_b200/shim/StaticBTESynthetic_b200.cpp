@@ -58,13 +58,26 @@ StaticBTESynthetic::StaticBTESynthetic(BTEMesh *mesh, BTEBoundaryCondition *bcs,
         belem_ptr_.push_back((int)belem_verts_.size());
         belem_tag_.push_back(bcs->boundaryConditions[b.index].index);
     }
+    // bands, material-major; regions map to materials through geo_matter_index
+    num_materials_ = numBand > 0 ? (int)bands->bands[0].group_velocity.size() : 1;
+    bool any5 = false;
     for (const BoundaryCondition &bc : bcs->boundaryConditions) {
         bc_tag_.push_back(bc.index);
         bc_type_.push_back(bc.type);
         bc_value_.push_back(bc.temperature);
+        any5 = any5 || bc.type == 5;
     }
-    // bands, material-major; regions map to materials through geo_matter_index
-    num_materials_ = numBand > 0 ? (int)bands->bands[0].group_velocity.size() : 1;
+    // interface walls: each row's transmissivity per material and band, from
+    // the blocks the reference read from the interface file
+    if (any5) {
+        const size_t row = (size_t)num_materials_ * numBand;
+        bc_trans_.assign(bcs->boundaryConditions.size() * row, 0.0);
+        for (size_t i = 0; i < bcs->boundaryConditions.size(); i++)
+            for (const transcoeff &t : bcs->boundaryConditions[i].matter_trans)
+                for (int b = 0; b < numBand && b < (int)t.trans.size(); b++)
+                    if (t.matter >= 0 && t.matter < num_materials_)
+                        bc_trans_[i * row + (size_t)t.matter * numBand + b] = t.trans[b];
+    }
     for (int m = 0; m < num_materials_; m++)
         for (const Band &b : bands->bands) {
             band_v_.push_back(b.group_velocity[m]);
@@ -144,6 +157,7 @@ void StaticBTESynthetic::run(int order, int sequential, int Use_Backup, int max_
         bc.tag = bc_tag_.data();
         bc.type = bc_type_.data();
         bc.value = bc_value_.data();
+        bc.transmissivity = bc_trans_.empty() ? nullptr : bc_trans_.data();
         gbte_angle_spec as{};
         as.method = 0;
         as.num_directions = numDirection;

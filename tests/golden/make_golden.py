@@ -87,6 +87,8 @@ def cases():
         bcs=[decks.BC(1, -2, 1.0), decks.BC(2, -1, 0.0), decks.BC(3, -4, 0.0), decks.BC(4, -3, 0.0),
              decks.BC(5, 2, 0.0)],
         scale=(3e-7, 3e-7), material_dim=2, angle_method=2, n_phi=4, tref=0.0, order="2limit")
+    # 9. two materials meeting at an interface wall (BC type 5)
+    out["interface_2mat"] = decks.interface_deck(16)
     out["quad_firstorder_sequential"] = decks.Deck(
         mesh=decks.square_quad_mesh(16, 16), bands=decks.sine_dispersion_bands(2),
         bcs=[decks.BC(1, 1, 300.0), decks.BC(2, 1, 300.0), decks.BC(3, 3, 0.0), decks.BC(4, 3, 0.0)],
@@ -107,7 +109,12 @@ def deck_params(d: decks.Deck) -> dict:
     return {"scale": list(d.scale), "material_dim": d.material_dim, "angle_method": d.angle_method,
             "n_theta": d.n_theta, "n_phi": d.n_phi, "tref": d.tref, "heat_source": d.heat_source,
             "mesh_format": d.mesh_format, "order": d.order, "scheme": d.scheme,
-            "bcs": [[b.tag, b.type, b.value] for b in d.bcs]}
+            "bcs": [[b.tag, b.type, b.value] for b in d.bcs],
+            "bc_trans": [None if b.trans is None else np.asarray(b.trans).tolist() for b in d.bcs],
+            "extra_materials": [{k: np.asarray(getattr(m, k)).tolist()
+                                 for k in ("v", "tau", "C", "lattice_ratio", "heat_ratio")}
+                                for m in d.extra_materials],
+            "region_material": d.region_material}
 
 
 # The benchmarked 2D workload at full size: the 300 nm porous cell with a
@@ -171,7 +178,12 @@ def load(name: str):
                         cell_region=z["cell_region"])
     bands = decks.BandTable(v=z["band_v"], tau=z["band_tau"], C=z["band_C"], lattice_ratio=z["band_lat"],
                             heat_ratio=z["band_hr"])
-    d = decks.Deck(mesh=mesh, bands=bands, bcs=[decks.BC(int(t), int(ty), float(v)) for t, ty, v in p["bcs"]],
+    trans = p.get("bc_trans") or [None] * len(p["bcs"])
+    extra = [decks.BandTable(**{k: np.asarray(v) for k, v in m.items()}) for m in p.get("extra_materials", [])]
+    d = decks.Deck(mesh=mesh, bands=bands,
+                   bcs=[decks.BC(int(t), int(ty), float(v), trans=None if tr is None else np.asarray(tr))
+                        for (t, ty, v), tr in zip(p["bcs"], trans)],
+                   extra_materials=extra, region_material=p.get("region_material"),
                    scale=tuple(p["scale"]), material_dim=p["material_dim"], angle_method=p["angle_method"],
                    n_theta=p["n_theta"], n_phi=p["n_phi"], tref=p["tref"], heat_source=p["heat_source"],
                    mesh_format=p["mesh_format"], order=p.get("order", "2"), scheme=p.get("scheme", "Synthetic"),
@@ -190,9 +202,12 @@ def have(name: str) -> bool:
 
 
 CASES = ["gray_square_tri", "quad_heat_specular", "periodic_jitter", "porous_msh", "porous_firstorder",
-         "periodic_sequential", "quad_firstorder_sequential", "porous_limiter"]
+         "periodic_sequential", "quad_firstorder_sequential", "porous_limiter", "interface_2mat"]
 # the cases solved to 1e-12 margins (all but the limited one, a fixed count)
 CONVERGED = [c for c in CASES if c != "porous_limiter"]
+# the cases of one material (the CPU restatement and the device Fourier
+# pre-solve cover one material)
+ONE_MATERIAL = [c for c in CASES if c != "interface_2mat"]
 
 if __name__ == "__main__":
     want = sys.argv[1:] or CASES

@@ -87,11 +87,29 @@ def test_bad_lattice_ratio_is_argument_error():
     assert e.value.status == -1
 
 
-def test_interface_boundary_is_unsupported(tmp_path):
+def test_interface_deck_reads_on_the_host(tmp_path):
+    # two materials and an interface wall (BC type 5, transmissivity file)
+    # written in the reference's formats read back on the host; the same
+    # deck from memory gives the same sizes
+    d = decks.interface_deck(8)
+    d.write(str(tmp_path))
+    a = g.inspect_deck(str(tmp_path))
+    b = g.inspect(d)
+    assert a["num_materials"] == 2 and b["num_materials"] == 2
+    assert a["num_cells"] == b["num_cells"] == d.mesh.n_cells
+    assert a["num_boundaries"] == b["num_boundaries"]
+
+
+def test_interface_file_missing_and_type4_refused(tmp_path):
     d = decks.config1_deck(6)
     d.write(str(tmp_path))
     with open(tmp_path / "input" / "bc.dat", "w") as f:
         f.write("1 #n\n\nheader\n1 5 0 input/trans.dat\n")
+    with pytest.raises(g.GBTEError) as e:
+        g.inspect_deck(str(tmp_path))
+    assert e.value.status == -2
+    with open(tmp_path / "input" / "bc.dat", "w") as f:
+        f.write("1 #n\n\nheader\n1 4 0 input/trans.dat\n")
     with pytest.raises(g.GBTEError) as e:
         g.inspect_deck(str(tmp_path))
     assert e.value.status == -8

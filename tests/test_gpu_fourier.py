@@ -14,7 +14,7 @@ def rel(a, b):
     return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
 
 
-@pytest.mark.parametrize("case", mg.CASES)
+@pytest.mark.parametrize("case", mg.ONE_MATERIAL)
 def test_fourier_initial_matches_reference(case):
     deck, ref = mg.load(case)
     s = StaticBTESynthetic.from_deck(deck, precision=GBTE_FP64)
@@ -29,7 +29,15 @@ def iterations_to(margins, tol):
     return int(ok[0]) + 1 if len(ok) else None
 
 
-@pytest.mark.parametrize("case", mg.CONVERGED)
+def test_fourier_initial_refuses_several_materials():
+    deck, _ = mg.load("interface_2mat")
+    s = StaticBTESynthetic.from_deck(deck, precision=GBTE_FP64)
+    with pytest.raises(GBTEError):
+        s.fourier_initial()
+    s.close()
+
+
+@pytest.mark.parametrize("case", [c for c in mg.CONVERGED if c in mg.ONE_MATERIAL])
 def test_iterations_from_fourier_start_match_reference(case):
     # from the same (Fourier) start the outer iteration follows the
     # reference's: the number of iterations to margins 1e-8 agrees (near
