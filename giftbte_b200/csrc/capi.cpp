@@ -168,8 +168,8 @@ int create_common(const gbte::RawMesh &raw_in, const gbte::Bands &bands_in, cons
     if (opt.gradient_dirs < 0 || opt.gradient_dirs > 8 || opt.gradient_dirs == 3)
         return fail(nullptr, {-1, "gradient_dirs must be 0 (automatic), 1, 2, 4, 5, 6, 7 or 8"}), GBTE_ERR_ARG;
     cfg.gradient_dirs = opt.gradient_dirs;
-    if (opt.residual_form != 0 && opt.residual_form != 1 && opt.residual_form != 5 && opt.residual_form != 6)
-        return fail(nullptr, {-1, "residual_form must be 0 (automatic), 1, 5 or 6"}), GBTE_ERR_ARG;
+    if (opt.residual_form != 0 && opt.residual_form != 1 && (opt.residual_form < 5 || opt.residual_form > 8))
+        return fail(nullptr, {-1, "residual_form must be 0 (automatic), 1, 5, 6, 7 or 8"}), GBTE_ERR_ARG;
     cfg.residual_form = opt.residual_form;
     if (opt.adjoint_history < -1 || opt.adjoint_history > 8)
         return fail(nullptr, {-1, "adjoint_history must be -1 (plain), 0 (default) or 1..8"}), GBTE_ERR_ARG;

@@ -184,4 +184,14 @@ struct GradTiles {
 };
 Error build_grad_tiles(const FlatMesh &m, int B, GradTiles &out);
 
+// Tiles of the shared-memory residual: the same blocks, each union its own
+// cells then its cells' interior face neighbours outside it (ascending);
+// floc[k] is the union index of face slot k's neighbour (0xFFFF on walls).
+struct FaceTiles {
+    int B = 0, nblk = 0, umax = 0;
+    std::vector<int> ptr, cells;
+    std::vector<unsigned short> floc;  // [cell-face slots]
+};
+Error build_face_tiles(const FlatMesh &m, int B, FaceTiles &out);
+
 }  // namespace gbte

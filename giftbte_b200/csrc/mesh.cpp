@@ -898,4 +898,44 @@ Error build_grad_tiles(const FlatMesh &m, int B, GradTiles &out) {
     return {0, ""};
 }
 
+Error build_face_tiles(const FlatMesh &m, int B, FaceTiles &out) {
+    out = FaceTiles();
+    if (B < 1 || B > 1024) return {-1, "residual tile size out of range"};
+    const int nc = m.nc;
+    out.B = B;
+    out.nblk = (nc + B - 1) / B;
+    out.ptr.assign(1, 0);
+    out.floc.assign(m.cf_ptr[nc], 0xFFFF);
+    std::vector<int> mark(nc, -1), slot(nc, 0), halo;
+    for (int blk = 0; blk < out.nblk; blk++) {
+        const int c0 = blk * B, c1 = std::min(nc, c0 + B);
+        for (int c = c0; c < c1; c++) {
+            mark[c] = blk;
+            slot[c] = c - c0;
+            out.cells.push_back(c);
+        }
+        halo.clear();
+        for (int k = m.cf_ptr[c0]; k < m.cf_ptr[c1]; k++) {
+            if (m.cf_bound[k] >= 0) continue;
+            const int j = m.cf_nbr[k];
+            if (mark[j] != blk) {
+                mark[j] = blk;
+                halo.push_back(j);
+            }
+        }
+        std::sort(halo.begin(), halo.end());
+        const int nu = (c1 - c0) + (int)halo.size();
+        if (nu > 65535) return {-8, "residual tile union exceeds 16-bit local indices"};
+        for (size_t h = 0; h < halo.size(); h++) {
+            slot[halo[h]] = (c1 - c0) + (int)h;
+            out.cells.push_back(halo[h]);
+        }
+        for (int k = m.cf_ptr[c0]; k < m.cf_ptr[c1]; k++)
+            if (m.cf_bound[k] < 0) out.floc[k] = (unsigned short)slot[m.cf_nbr[k]];
+        out.ptr.push_back((int)out.cells.size());
+        out.umax = std::max(out.umax, nu);
+    }
+    return {0, ""};
+}
+
 }  // namespace gbte

@@ -828,6 +828,109 @@ __global__ void __launch_bounds__(512) k_gradient_tile(DMesh m, DPhys p, const f
     }
 }
 
+// Shared-memory tiled residual: one CTA per (block of B consecutive cells,
+// chunk of nbc bands), looping over the batch's directions. For each
+// direction the intensity and gradient rows of the block's union (its cells
+// and their interior face neighbours) are copied into shared memory with
+// 16-byte cp.async, so every neighbour row crosses from L2 once per block
+// and direction; each thread (cell, 4 bands) then forms k_residual8's
+// defect from shared memory, face by face in the same order with the same
+// operations, so both give the same bits. Needs nbc a multiple of 4
+// dividing nb and nbc * sizeof(S) a multiple of 16. Shared memory: umax
+// rows of (1 + DIM) * nbc S.
+template <typename S, int DIM>
+__global__ void __launch_bounds__(512) k_residual_tile(DMesh m, DPhys p, EView<S, DIM> ev,
+                                                       const double *__restrict__ Bf,
+                                                       const double *__restrict__ Told,
+                                                       const double *__restrict__ eb, const int *__restrict__ pos_of,
+                                                       const int *__restrict__ tile_ptr,
+                                                       const int *__restrict__ tile_cells,
+                                                       const unsigned short *__restrict__ floc, int B, int nbc,
+                                                       S *__restrict__ Rlo, int d0, int ndb) {
+    extern __shared__ __align__(16) unsigned char rsm[];
+    S *tl = reinterpret_cast<S *>(rsm);  // [u][1 + DIM][nbc]: e, then the DIM gradient rows
+    const int nb = p.nb, nc = m.nc, nchunk = nb / nbc, rowl = (1 + DIM) * nbc;
+    const int blk = blockIdx.x / nchunk, ch = blockIdx.x % nchunk, bb = ch * nbc;
+    const int c0 = blk * B, c1 = min(c0 + B, nc), ncell = c1 - c0;
+    const int u0 = tile_ptr[blk], nu = tile_ptr[blk + 1] - u0;
+    const int tid = threadIdx.x, bd = blockDim.x;
+    const int per = nbc * (int)sizeof(S) / 16;  // 16-byte pieces of one row chunk
+    const int ngrp = nbc / 4, items = ncell * ngrp;
+    for (int dl = 0; dl < ndb; dl++) {
+        const size_t d = (size_t)d0 + dl;
+        __syncthreads();
+        for (int i = tid; i < nu * (1 + DIM) * per; i += bd) {
+            const int u = i / ((1 + DIM) * per), r = (i / per) % (1 + DIM), k = i % per;
+            const int cell = tile_cells[u0 + u];
+            const S *src = r == 0 ? ev.eps + (d * nc + cell) * nb + bb
+                                  : ev.g + (((size_t)dl * nc + cell) * DIM + (r - 1)) * nb + bb;
+            cp_async(reinterpret_cast<unsigned char *>(tl + (size_t)u * rowl + r * nbc) + 16 * k,
+                     reinterpret_cast<const unsigned char *>(src) + 16 * k, 16);
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        const double sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
+        for (int it = tid; it < items; it += bd) {
+            const int i = it / ngrp, j = it - i * ngrp, c = c0 + i, b0 = bb + 4 * j;
+            const int mo = mat_off(p, c);
+            const size_t dc = d * nc + c;
+            const double tsc = m.tsc[c], invV = tsc / m.vol[c], tb = ev.Tb[c];
+            const S *own = tl + (size_t)i * rowl + 4 * j;
+            S ec[4], acc[4], gxv[4], gyv[4], gzv[4];
+            ld8(own, ec);
+            ld8(own + nbc, gxv);
+            ld8(own + 2 * nbc, gyv);
+            if (DIM == 3) ld8(own + 3 * nbc, gzv);
+#pragma unroll
+            for (int v = 0; v < 4; v++) acc[v] = (S)0;
+            for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+                const double sn = sx * m.cf_nx[k] + sy * m.cf_ny[k] + (DIM == 3 ? sz * m.cf_nz[k] : 0.0);
+                const S a = (S)(m.cf_area[k] * invV * sn);
+                if (sn >= 0) {
+                    const S rx = (S)(m.cf_fx[k] - m.cx[c]), ry = (S)(m.cf_fy[k] - m.cy[c]);
+                    const S rz = DIM == 3 ? (S)(m.cf_fz[k] - m.cz[c]) : (S)0;
+#pragma unroll
+                    for (int v = 0; v < 4; v++) {
+                        S y = ec[v] + gxv[v] * rx + gyv[v] * ry;
+                        if (DIM == 3) y += gzv[v] * rz;
+                        acc[v] += a * y;
+                    }
+                } else if (m.cf_bound[k] < 0) {
+                    const int jn = m.cf_nbr[k];
+                    const S *nr = tl + (size_t)floc[k] * rowl + 4 * j;
+                    S ej[4], hx[4], hy[4], hz[4];
+                    ld8(nr, ej);
+                    ld8(nr + nbc, hx);
+                    ld8(nr + 2 * nbc, hy);
+                    if (DIM == 3) ld8(nr + 3 * nbc, hz);
+                    const S rx = (S)(m.cf_fx[k] - m.cx[jn]), ry = (S)(m.cf_fy[k] - m.cy[jn]);
+                    const S rz = DIM == 3 ? (S)(m.cf_fz[k] - m.cz[jn]) : (S)0;
+#pragma unroll
+                    for (int v = 0; v < 4; v++) {
+                        S y = ej[v] + hx[v] * rx + hy[v] * ry;
+                        if (DIM == 3) y += hz[v] * rz;
+                        acc[v] += a * y;
+                    }
+                } else {
+                    const double *e = eb + (d * m.nbs + m.cf_bside[k]) * nb + b0;
+#pragma unroll
+                    for (int v = 0; v < 4; v++) acc[v] += a * (S)(e[v] - p.C[mo + b0 + v] * tb);
+                }
+            }
+            const double dT = Told[c] - tb, Bv = Bf[dc], hc = m.heat[c] * tsc;
+            S out[4];
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                const double tv = p.tau[mo + b0 + v] * p.vmag[mo + b0 + v];
+                const S fixed = (S)(p.C[mo + b0 + v] * (dT - tv * Bv) + hc * p.hr[mo + b0 + v] * p.tau[mo + b0 + v]);
+                out[v] = fixed - ec[v] - (S)tv * acc[v];
+            }
+            st8(Rlo + ((size_t)dl * nc + pos_of[dc]) * nb + b0, out);
+        }
+    }
+}
+
 // One cell of a direction's level order, as the sweep reads it: up to four
 // upwind neighbours (their positions in the same level order, or -(1 +
 // far slot)) with their coefficients a_j = A_f/V (s.n_f) < 0, sig = sum of
@@ -2313,7 +2416,7 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
         return {-8, "Order=2limit (the gradient limiter) needs the FP64 form (GBTE_FP64)"};
     if (cfg.use_limiter && cfg.order != 2) return {-1, "the gradient limiter applies to the second-order scheme"};
     for (int t : mesh.b_type)
-        if (!(t == 1 || t == 2 || t == 3 || t == 6 || t < 0))
+        if (!(t == 1 || t == 2 || t == 3 || t == 5 || t == 6 || t < 0))
             return {-8, "boundary type " + std::to_string(t) + " is not supported"};
     if (!cfg.cell_scatter.empty()) {
         if ((int)cfg.cell_scatter.size() != mesh.nc) return {-1, "cell_scatter must hold one value per cell"};
@@ -3411,7 +3514,24 @@ Error Solver::solve_t(SolveStats &st) {
         if (te.code) return te;
         CUDA_TRY(cudaFuncSetAttribute(k_gradient_tile<S, DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       220 * 1024));
+        CUDA_TRY(cudaFuncSetAttribute(k_residual_tile<S, DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      220 * 1024));
     }
+    auto rtile_shape = [&](int code, int &nbc, int &threads, size_t &smem) -> bool {
+        const int k = code - 7;
+        if (k < 0 || k >= (int)ftiles_.size() || nb % 4) return false;
+        const FaceTileDev &T = ftiles_[k];
+        for (int limit : {113 * 1024, 220 * 1024})
+            for (nbc = nb; nbc >= 4; nbc -= 4) {
+                if (nb % nbc || (nbc * sizeof(S)) % 16) continue;
+                smem = (size_t)T.umax * (1 + DIM) * nbc * sizeof(S);
+                if (smem <= (size_t)limit) {
+                    threads = std::min(512, ((T.B * nbc / 4 + 31) / 32) * 32);
+                    return true;
+                }
+            }
+        return false;
+    };
     auto tile_shape = [&](int code, int &nbc, int &threads, size_t &smem) -> bool {
         const int k = code - 7;
         if (k < 0 || k >= (int)tiles_.size()) return false;
@@ -3467,7 +3587,21 @@ Error Solver::solve_t(SolveStats &st) {
     const bool rtune = cfg.residual_form == 0 && tuned_res_form_ == 0 && wc_ok;
     int res_form = cfg.residual_form ? cfg.residual_form : tuned_res_form_ ? tuned_res_form_ : 1;
     if (!wc_ok) res_form = 1;
+    {
+        int nbc_ = 0, thr_ = 0;
+        size_t sm_ = 0;
+        if (res_form >= 7 && !rtile_shape(res_form, nbc_, thr_, sm_)) res_form = 1;
+    }
     auto launch_res = [&](int form, int d0, int nbt) -> cudaError_t {
+        if (form >= 7) {
+            int nbc = 0, threads = 0;
+            size_t smem = 0;
+            if (!rtile_shape(form, nbc, threads, smem)) return cudaErrorInvalidValue;
+            const FaceTileDev &T = ftiles_[form - 7];
+            k_residual_tile<S, DIM><<<T.nblk * (nb / nbc), threads, smem, s>>>(
+                dm_, dp_, ev, Bflux_, Told_, eb_, pos_of_, T.ptr, T.cells, T.floc, T.B, nbc, R, d0, nbt);
+            return cudaGetLastError();
+        }
         if (form >= 5) {
             const int dpw = (32 / (nb / 4)) * (form - 4);
             const size_t thr = (size_t)((nbt + dpw - 1) / dpw) * nc * 32;
@@ -3572,7 +3706,10 @@ Error Solver::solve_t(SolveStats &st) {
                 CUDA_TRY(cudaEventCreate(&t1));
                 float best = 1e30f;
                 int best_form = 1;
-                for (int form : {1, 5, 6}) {
+                for (int form : {1, 5, 6, 7, 8}) {
+                    int nbc_ = 0, thr_ = 0;
+                    size_t sm_ = 0;
+                    if (form >= 7 && !rtile_shape(form, nbc_, thr_, sm_)) continue;
                     for (int rep = 0; rep < 2; rep++) {
                         CUDA_TRY(cudaEventRecord(t0, s));
                         CUDA_TRY(launch_res(form, d0, nbt));
@@ -4033,6 +4170,18 @@ Error Solver::grad_tiles() {
         d.loc = upload(this, allocs_, t.loc, s, ok);
         if (!ok) return {-6, "device allocation failed (gradient tiles)"};
         tiles_.push_back(d);
+    }
+    // the residual's tiles: the same block sizes, unions of face neighbours
+    for (int B : cand) {
+        FaceTiles t;
+        if (build_face_tiles(mesh, B, t).code) continue;
+        FaceTileDev d;
+        d.B = t.B, d.nblk = t.nblk, d.umax = t.umax;
+        d.ptr = upload(this, allocs_, t.ptr, s, ok);
+        d.cells = upload(this, allocs_, t.cells, s, ok);
+        d.floc = upload(this, allocs_, t.floc, s, ok);
+        if (!ok) return {-6, "device allocation failed (residual tiles)"};
+        ftiles_.push_back(d);
     }
     CUDA_TRY(cudaStreamSynchronize(s));
     return {0, ""};
@@ -5018,6 +5167,8 @@ Error Solver::vjp(const double *Tbar_h, const double *qbar_h, int max_iter, doub
     if (cfg.order != 2 || cfg.sequential || cfg.use_limiter)
         return {-8, "the adjoint is implemented for the second-order Synthetic scheme without limiter only"};
     if (bands.nmat > 1) return {-8, "the adjoint covers one material"};
+    for (int t : mesh.b_type)
+        if (t == 5) return {-8, "the adjoint does not cover interface walls (type 5)"};
     if (ndb_ < ang.nd) return {-8, "the adjoint needs every direction's buffers resident (direction_batch)"};
     if (xfn_) return {-8, "the adjoint is not implemented for direction-sharded handles"};
     if (max_iter < 1 || !(tol > 0)) return {-1, "invalid adjoint limits"};

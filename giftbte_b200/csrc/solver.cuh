@@ -160,6 +160,12 @@ public:
         unsigned short *loc = nullptr;
     };
     std::vector<TileDev> tiles_;
+    struct FaceTileDev {
+        int B = 0, nblk = 0, umax = 0;
+        int *ptr = nullptr, *cells = nullptr;
+        unsigned short *floc = nullptr;
+    };
+    std::vector<FaceTileDev> ftiles_;  // tiles of the shared-memory residual (residual_form 7, 8)
     bool tiles_built_ = false;
     Error grad_tiles();
     int tuned_res_form_ = 0;     // residual launch shape (1 thread per cell, 5/6 warp per cell; 0 = not yet tuned)

@@ -193,8 +193,10 @@ typedef struct {
                                  0 = the fastest on the first outer iteration. Results do not
                                  depend on it. */
     int residual_form;        /* launch shape of the second-order residual: 1 = a thread per cell
-                                 and 4 bands, 5, 6 = a warp per cell as for gradient_dirs; 0 = the
-                                 fastest on the first outer iteration. Results do not depend on it. */
+                                 and 4 bands, 5, 6 = a warp per cell as for gradient_dirs, 7, 8 =
+                                 shared-memory tiles of the blocks of gradient_dirs 7, 8 (the
+                                 block's cells and face neighbours); 0 = the fastest on the first
+                                 outer iteration. Results do not depend on it. */
     int adjoint_history;      /* gbte_vjp: Anderson acceleration of the transposed iteration with
                                  this many difference pairs (1..8); 0 = 6; -1 = the plain iteration
                                  lam += A^-T r. The fixed point, and the stopping rule, are the same. */

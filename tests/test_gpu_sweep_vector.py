@@ -141,8 +141,8 @@ def test_wide_level_kernel_batch_and_golden():
 def test_gradient_and_residual_launch_shapes_are_bit_identical(prec, dim):
     # the LSQ gradient with 1, 2 or 4 directions per thread, a warp per cell
     # with 1 or 2 directions per lane (options.gradient_dirs 5, 6), or
-    # shared-memory tiles of two block sizes (7, 8), and
-    # the residual as a thread or a warp per cell (options.residual_form):
+    # shared-memory tiles of two block sizes (7, 8), and the residual as a
+    # thread, a warp per cell or a tile (options.residual_form):
     # the arithmetic per band and direction is unchanged. The 3D block runs
     # in direction batches of 5, so direction groups meet a batch whose last
     # group is short
@@ -153,7 +153,7 @@ def test_gradient_and_residual_launch_shapes_are_bit_identical(prec, dim):
         d = decks.config3_deck(h_nm=10.0, size_nm=(40.0, 40.0, 100.0), n_bands=8, n_theta=2, n_phi=2)
         kw = {"direction_batch": 5}
     out = {}
-    for dg, rf in ((1, 1), (2, 1), (4, 1), (5, 1), (6, 1), (7, 1), (8, 1), (1, 5), (1, 6)):
+    for dg, rf in ((1, 1), (2, 1), (4, 1), (5, 1), (6, 1), (7, 1), (8, 1), (1, 5), (1, 6), (1, 7), (1, 8)):
         s = g.StaticBTESynthetic.from_deck(d, precision=prec, gradient_dirs=dg, residual_form=rf, sweep_bands=8,
                                            sweep_vector=1, sweep_kernel=1, **kw)
         st = s.solve(max_iter=10, err_temp=0.0, err_flux=0.0)
