@@ -59,7 +59,7 @@ def measured_peak_gbs():
         return HBM_FALLBACK_GBS, "fallback"
 
 
-def build_deck(workload: str, seed: int, h_nm: float = 0.0):
+def build_deck(workload: str, seed: int, h_nm: float = 0.0, height_nm: float = 500.0):
     from giftbte_b200 import decks
 
     if workload == "config1":
@@ -67,8 +67,8 @@ def build_deck(workload: str, seed: int, h_nm: float = 0.0):
         desc = "gray 1 um square, 40x40x2 triangles (3200), 1 band, 32 CADOM directions"
     elif workload == "config3":
         h = h_nm or 2.5
-        d = decks.config3_deck(h_nm=h, seed=1 + seed)
-        desc = (f"3D hotspot block 100x100x500 nm, cubes of {h} nm split into 6 jittered tets "
+        d = decks.config3_deck(h_nm=h, seed=1 + seed, size_nm=(100.0, 100.0, height_nm))
+        desc = (f"3D hotspot block 100x100x{height_nm:g} nm, cubes of {h} nm split into 6 jittered tets "
                 f"({d.mesh.n_cells} tets), 40 sine-dispersion bands, 128 Gauss directions, "
                 f"1e18 W/m^3 in the top 20 nm, seed {1 + seed}")
     else:
@@ -214,7 +214,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     # replicas: a seeded problem per rank; direction shards: one problem,
     # its directions split over the ranks
     by_dirs = args.shard == "directions"
-    deck, desc = build_deck(args.workload, seed=0 if by_dirs else rank, h_nm=args.h_nm)
+    deck, desc = build_deck(args.workload, seed=0 if by_dirs else rank, h_nm=args.h_nm, height_nm=args.height_nm)
     nc = deck.mesh.n_cells
     prec = g.GBTE_FP32_MIXED if args.precision == "fp32" else g.GBTE_FP64
     s_bytes = 4 if prec == g.GBTE_FP32_MIXED else 8
@@ -223,7 +223,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     solver = g.StaticBTESynthetic.from_deck(deck, precision=prec, device=local_rank, profile=0,
                                             stream=ctypes_stream(stream), cell_order=args.cell_order,
                                             sweep_bands=args.sweep_bands, sweep_vector=args.sweep_vector,
-                                            sweep_kernel=args.sweep_kernel)
+                                            sweep_kernel=args.sweep_kernel, gradient_dirs=args.gradient_dirs,
+                                            residual_form=args.residual_form)
     setup_s = time.perf_counter() - t_setup
     nb, nd = solver.num_bands, solver.num_directions
     upd_per_step = nb * nd * nc
@@ -540,7 +541,7 @@ def run_reference(args, rank: int):
         return None
     import oracle
 
-    deck, desc = build_deck(args.workload, seed=0, h_nm=args.h_nm)
+    deck, desc = build_deck(args.workload, seed=0, h_nm=args.h_nm, height_nm=args.height_nm)
     nb = deck.bands.n_bands
     nd = directions_of(deck)
     upd = nb * nd * deck.mesh.n_cells
@@ -716,6 +717,8 @@ def main():
     ap.add_argument("--adj-max-iter", type=int, default=20000, help="config4: adjoint iteration cap")
     ap.add_argument("--batch", type=int, default=256, help="config5: number of independent cells")
     ap.add_argument("--h-nm", type=float, default=0.0, help="config3 mesh spacing (default 2.5 nm)")
+    ap.add_argument("--height-nm", type=float, default=500.0,
+                    help="config3 block height (default 500 nm; smaller blocks for profiling captures)")
     ap.add_argument("--sweep-bands", type=int, default=0,
                     help="bands per sweep CTA (1..32); 0 lets the autotuner pick on the first iteration")
     ap.add_argument("--sweep-vector", type=int, choices=[0, 1, 2, 4], default=0,
@@ -723,6 +726,10 @@ def main():
     ap.add_argument("--sweep-kernel", type=int, choices=[0, 1, 2, 3], default=0,
                     help="1: block sweep kernel, 2: warp-independent kernel, 3: wide-level kernel, "
                          "0: the autotuner's pick")
+    ap.add_argument("--gradient-dirs", type=int, choices=[0, 1, 2, 4, 5, 6, 7, 8], default=0,
+                    help="gradient launch shape (options.gradient_dirs); 0 lets the first iteration pick")
+    ap.add_argument("--residual-form", type=int, choices=[0, 1, 5, 6, 7, 8], default=0,
+                    help="residual launch shape (options.residual_form); 0 lets the first iteration pick")
     ap.add_argument("--cell-order", type=int, choices=[0, 1], default=0,
                     help="0: cells renumbered along a Morton curve inside the library; 1: the deck's order")
     ap.add_argument("--e2e-steps", type=int, default=1,
