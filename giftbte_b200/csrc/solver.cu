@@ -1601,10 +1601,14 @@ __device__ __forceinline__ void symv(const double *q, double x, double y, double
 // tangential gradient on face k of cell c of a node field (vals, stride st)
 __device__ __forceinline__ void tangential(const DMesh &m, int c, int k, const double *vals, int stride, int comp,
                                            bool use_slot, double &tx, double &ty, double &tz) {
+    // node values live in (node, material) slots: the slot of the cell's
+    // material (StaticBTESynthetic.cpp:2347-2363)
+    const int M = m.matter ? m.nmat : 1, mt = (use_slot && m.matter) ? m.matter[c] : 0;
     if (m.dim == 2) {
         const int v0 = m.cf_v[3 * k], v1 = m.cf_v[3 * k + 1];
         const double mx = m.node_x[v1] - m.node_x[v0], my = m.node_y[v1] - m.node_y[v0];
-        const double dv = vals[(size_t)v1 * stride + comp] - vals[(size_t)v0 * stride + comp];
+        const size_t s0 = (size_t)v0 * M + mt, s1 = (size_t)v1 * M + mt;
+        const double dv = vals[s1 * stride + comp] - vals[s0 * stride + comp];
         tx = dv / (mx * mx + my * my) * mx;
         ty = dv / (mx * mx + my * my) * my;
         tz = 0;
@@ -1614,7 +1618,7 @@ __device__ __forceinline__ void tangential(const DMesh &m, int c, int k, const d
         const double *W = m.face_w + 9 * (size_t)f;
         double d1[3] = {0, 0, 0};
         for (int t = 0; t < 2; t++) {
-            const int a = m.cf_v[3 * k0 + t + 1], b = m.cf_v[3 * k0 + t];
+            const int a = m.cf_v[3 * k0 + t + 1] * M + mt, b = m.cf_v[3 * k0 + t] * M + mt;
             d1[t + 1] = m.inv_Lx * (vals[(size_t)a * stride + comp] - vals[(size_t)b * stride + comp]);
         }
         tx = W[0] * d1[0] + W[1] * d1[1] + W[2] * d1[2];
@@ -2471,6 +2475,8 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
     std::vector<double> tsc(mesh.nc, 1.0);
     for (size_t i = 0; i < cfg.cell_scatter.size(); i++) tsc[i] = 1.0 / cfg.cell_scatter[i];
     d.tsc = up_d(tsc);
+    d.nmat = bands.nmat;
+    d.matter = bands.nmat > 1 ? up_i(mesh.matter) : nullptr;
     d.nbr_ptr = up_i(mesh.nbr_ptr);
     d.nbr_idx = up_i(mesh.nbr_idx);
     d.lsq_w = up_d(mesh.lsq_w);

@@ -17,6 +17,8 @@ struct DMesh {
     const double *cf_area, *cf_nx, *cf_ny, *cf_nz, *cf_fx, *cf_fy, *cf_fz;
     const double *vol, *cx, *cy, *cz, *heat;
     const double *tsc;  // 1 / s_c: per-cell scale of the relaxation time (scattering multiplier s_c)
+    int nmat;           // materials: node values are kept per (node, material) slot
+    const int *matter;  // [nc] cell material, nullptr with one material
     const int *nbr_ptr, *nbr_idx;
     const double *lsq_w;
     const float *lsq_wf;
