@@ -40,6 +40,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <mutex>
 #include <thread>
 #include <type_traits>
@@ -1569,6 +1570,84 @@ __global__ void k_side_moments(DMesh m, DPhys p, const double *__restrict__ eb, 
     }
 }
 
+// Moments of a cell under another material's band constants (the cross
+// values of wall faces): Th (before the kappa factor) and Q of cell
+// y_cell[y] with material y_mat[y]'s lat, C, tau, |v| and heat ratios,
+// over the directions d0 .. d0 + ndb (later batches add to the first).
+// One warp per (cell, material) pair, lanes over (direction, band).
+template <typename S>
+__global__ void k_cross_cell(DMesh m, DPhys p, const S *__restrict__ eps, const double *__restrict__ Tb,
+                             double *__restrict__ ThC, double *__restrict__ QC, int d0, int ndb, int accumulate) {
+    const int y = (int)(gtid() >> 5), lane = threadIdx.x & 31;
+    if (y >= m.ncross_y) return;
+    const int c = m.y_cell[y], mc = m.y_mat[y] * p.nb, ms = mat_off(p, c);
+    double th = 0, q6[6] = {0, 0, 0, 0, 0, 0};
+    const int n = ndb * p.nb;
+    for (int i = lane; i < n; i += 32) {
+        const int d = d0 + i / p.nb, b = i % p.nb;
+        if (!(p.hr[mc + b] > 0)) continue;
+        const double e = p.C[ms + b] * Tb[c] + (double)eps[((size_t)d * m.nc + c) * p.nb + b];
+        const double w = p.w[d], sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
+        th += p.lat[mc + b] * e * w / p.C[mc + b];
+        const double f = w * p.tau[mc + b] * p.vmag[mc + b] * p.vmag[mc + b] * e;
+        q6[0] += f * sx * sx;
+        q6[1] += f * sx * sy;
+        q6[2] += f * sx * sz;
+        q6[3] += f * sy * sy;
+        q6[4] += f * sy * sz;
+        q6[5] += f * sz * sz;
+    }
+    th = warp_sum(th);
+    for (int i = 0; i < 6; i++) q6[i] = warp_sum(q6[i]);
+    if (lane == 0) {
+        ThC[y] = accumulate ? ThC[y] + th : th;
+        for (int i = 0; i < 6; i++) QC[6 * y + i] = accumulate ? QC[6 * y + i] + q6[i] : q6[i];
+    }
+}
+
+// Cross node values: the inverse-distance interpolation of a slot's stencil
+// under the wall cell's material (cells through k_cross_cell, wall sides
+// formed here from their boundary values, before the incoming gather).
+// One warp per cross value.
+__global__ void k_cross_node(DMesh m, DPhys p, const double *__restrict__ eb, const double *__restrict__ ThC,
+                             const double *__restrict__ QC, double *__restrict__ ThX, double *__restrict__ QX) {
+    const int x = (int)(gtid() >> 5), lane = threadIdx.x & 31;
+    if (x >= m.ncross_x) return;
+    const int mc = m.x_mat[x] * p.nb;
+    double th = 0, q6[6] = {0, 0, 0, 0, 0, 0};
+    for (int k = m.xs_ptr[x]; k < m.xs_ptr[x + 1]; k++) {
+        const int src = m.xs_src[k];
+        const double wk = m.xs_w[k];
+        if (src >= 0) {
+            th += wk * ThC[src];
+            for (int i = 0; i < 6; i++) q6[i] += wk * QC[6 * src + i];
+            continue;
+        }
+        const int s = -1 - src;
+        double a = 0, a6[6] = {0, 0, 0, 0, 0, 0};
+        for (int i = lane; i < p.nd * p.nb; i += 32) {
+            const int d = i / p.nb, b = i % p.nb;
+            if (!(p.hr[mc + b] > 0)) continue;
+            const double w = p.w[d], sx = p.sx[d], sy = p.sy[d], sz = p.sz[d];
+            const double e = eb[((size_t)d * m.nbs + s) * p.nb + b];
+            a += p.lat[mc + b] * e * w / p.C[mc + b];
+            const double f = w * p.tau[mc + b] * p.vmag[mc + b] * p.vmag[mc + b] * e;
+            a6[0] += f * sx * sx;
+            a6[1] += f * sx * sy;
+            a6[2] += f * sx * sz;
+            a6[3] += f * sy * sy;
+            a6[4] += f * sy * sz;
+            a6[5] += f * sz * sz;
+        }
+        th += wk * warp_sum(a);
+        for (int i = 0; i < 6; i++) q6[i] += wk * warp_sum(a6[i]);
+    }
+    if (lane == 0) {
+        ThX[x] = p.kap[m.x_mat[x]] * th;
+        for (int i = 0; i < 6; i++) QX[6 * x + i] = q6[i];
+    }
+}
+
 // inverse-distance node values of (Th, Q) with boundary-side override
 __global__ void k_node_interp(DMesh m, const double *__restrict__ Th, const double *__restrict__ Q,
                               const double *__restrict__ Ths, const double *__restrict__ Qs, double *__restrict__ ThV,
@@ -1599,16 +1678,25 @@ __device__ __forceinline__ void symv(const double *q, double x, double y, double
 }
 
 // tangential gradient on face k of cell c of a node field (vals, stride st)
+// Node values live in (node, material) slots. Slot form: the slot of the
+// cell's material (StaticBTESynthetic.cpp:2347-2363, :1677-1687). Wall form
+// (xv != nullptr): the raw node index of the slot array, or the cross value
+// xv[cf_x] where that slot belongs to another material (:1741-1758).
 __device__ __forceinline__ void tangential(const DMesh &m, int c, int k, const double *vals, int stride, int comp,
-                                           bool use_slot, double &tx, double &ty, double &tz) {
-    // node values live in (node, material) slots: the slot of the cell's
-    // material (StaticBTESynthetic.cpp:2347-2363)
-    const int M = m.matter ? m.nmat : 1, mt = (use_slot && m.matter) ? m.matter[c] : 0;
+                                           bool use_slot, double &tx, double &ty, double &tz,
+                                           const double *xv = nullptr) {
+    const int M = (use_slot && m.matter) ? m.nmat : 1, mt = (use_slot && m.matter) ? m.matter[c] : 0;
+    auto val = [&](size_t q, int kk, int t) -> double {
+        if (xv && m.cf_x) {
+            const int x = m.cf_x[3 * (size_t)kk + t];
+            if (x >= 0) return xv[(size_t)x * stride + comp];
+        }
+        return vals[((size_t)q * M + mt) * stride + comp];
+    };
     if (m.dim == 2) {
         const int v0 = m.cf_v[3 * k], v1 = m.cf_v[3 * k + 1];
         const double mx = m.node_x[v1] - m.node_x[v0], my = m.node_y[v1] - m.node_y[v0];
-        const size_t s0 = (size_t)v0 * M + mt, s1 = (size_t)v1 * M + mt;
-        const double dv = vals[s1 * stride + comp] - vals[s0 * stride + comp];
+        const double dv = val(v1, k, 1) - val(v0, k, 0);
         tx = dv / (mx * mx + my * my) * mx;
         ty = dv / (mx * mx + my * my) * my;
         tz = 0;
@@ -1618,8 +1706,8 @@ __device__ __forceinline__ void tangential(const DMesh &m, int c, int k, const d
         const double *W = m.face_w + 9 * (size_t)f;
         double d1[3] = {0, 0, 0};
         for (int t = 0; t < 2; t++) {
-            const int a = m.cf_v[3 * k0 + t + 1] * M + mt, b = m.cf_v[3 * k0 + t] * M + mt;
-            d1[t + 1] = m.inv_Lx * (vals[(size_t)a * stride + comp] - vals[(size_t)b * stride + comp]);
+            const int a = m.cf_v[3 * k0 + t + 1], b = m.cf_v[3 * k0 + t];
+            d1[t + 1] = m.inv_Lx * (val(a, k0, t + 1) - val(b, k0, t));
         }
         tx = W[0] * d1[0] + W[1] * d1[1] + W[2] * d1[2];
         ty = W[3] * d1[0] + W[4] * d1[1] + W[5] * d1[2];
@@ -1632,7 +1720,8 @@ __device__ __forceinline__ void tangential(const DMesh &m, int c, int k, const d
 // with face gradient G(X) = alpha (X_nb - X_c) n + tangential(X at nodes).
 __global__ void k_remacro(DMesh m, const double *__restrict__ Th, const double *__restrict__ Q,
                           const double *__restrict__ Ths, const double *__restrict__ Qs, const double *__restrict__ ThV,
-                          const double *__restrict__ QV, double *__restrict__ remacro) {
+                          const double *__restrict__ QV, const double *__restrict__ ThX, const double *__restrict__ QX,
+                          double *__restrict__ remacro) {
     const int c = (int)gtid();
     if (c >= m.nc) return;
     double acc = 0;
@@ -1659,7 +1748,8 @@ __global__ void k_remacro(DMesh m, const double *__restrict__ Th, const double *
         const double alpha = (rx * nx + ry * ny + rz * nz) / (rx * rx + ry * ry + rz * rz);
         // Fourier part: n . (alpha dTh n + tangential)
         double tx, ty, tz;
-        tangential(m, c, k, ThV, 1, 0, true, tx, ty, tz);
+        const bool wall = bnd >= 0;
+        tangential(m, c, k, ThV, 1, 0, !wall, tx, ty, tz, wall ? ThX : nullptr);
         const double nn = nx * nx + ny * ny + nz * nz;
         double four = alpha * (thn - Th[c]) * nn + (nx * tx + ny * ty + nz * tz);
         // BTE part: n . [alpha (Q_nb - Q_c) n + (QV_v1 - QV_v0) tangential]
@@ -1670,7 +1760,7 @@ __global__ void k_remacro(DMesh m, const double *__restrict__ Th, const double *
         double bte = alpha * (nx * gx + ny * gy + nz * gz);
         // tangential part of the tensor moment: n^T QV t-hat per component
         double tq[6][3];
-        for (int i = 0; i < 6; i++) tangential(m, c, k, QV, 6, i, true, tq[i][0], tq[i][1], tq[i][2]);
+        for (int i = 0; i < 6; i++) tangential(m, c, k, QV, 6, i, !wall, tq[i][0], tq[i][1], tq[i][2], wall ? QX : nullptr);
         // n^T [sum_i comp_i(QV) tangent_i]: the tangential gradient of the
         // tensor field contracted with n on the left and the gradient index
         // on the right: sum_{a,b} n_a (dQ_ab/dx_t) ... evaluated as
@@ -2509,6 +2599,71 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
     d.node_x = up_d(mesh.node_x);
     d.node_y = up_d(mesh.node_y);
     d.node_z = up_d(mesh.node_z);
+    // Wall faces (all but specular) read their node energy densities at the
+    // raw node index of the (node, material) slot array
+    // (StaticBTESynthetic.cpp:1741-1742 and :1758, against the slot writes
+    // of :1559-1600), i.e. slot (node / M, node % M), and weigh them with the
+    // band constants of the wall cell's material (:1926-1931). With one
+    // material that is the node's own slot. With several, a slot of another
+    // material gets a cross value: its stencil's moments formed under the
+    // wall cell's material.
+    d.ncross_x = d.ncross_y = 0;
+    d.cf_x = d.x_mat = d.xs_ptr = d.xs_src = d.y_cell = d.y_mat = nullptr;
+    d.xs_w = nullptr;
+    if (mesh.nmat > 1) {
+        const int M = mesh.nmat, nv = mesh.dim == 2 ? 2 : 3;
+        std::vector<int> cfx(3 * (size_t)mesh.ncf(), -1), x_mat, xs_ptr{0}, xs_src, y_cell, y_mat;
+        std::vector<double> xs_w;
+        std::map<std::pair<int, int>, int> xid, yid;
+        for (int c = 0; c < mesh.nc; c++) {
+            const int mc = mesh.matter[c];
+            for (int k = mesh.cf_ptr[c]; k < mesh.cf_ptr[c + 1]; k++) {
+                const int bnd = mesh.cf_bound[k];
+                if (bnd < 0 || mesh.b_type[bnd] == 3) continue;
+                for (int t = 0; t < nv; t++) {
+                    const int r = mesh.cf_v[3 * (size_t)k + t];
+                    if (r % M == mc) continue;
+                    auto it = xid.find({r, mc});
+                    if (it == xid.end()) {
+                        it = xid.emplace(std::make_pair(r, mc), (int)x_mat.size()).first;
+                        x_mat.push_back(mc);
+                        for (int q = mesh.nv_ptr[r]; q < mesh.nv_ptr[r + 1]; q++) {
+                            const int src = mesh.nv_src[q];
+                            if (src >= 0) {
+                                auto jt = yid.find({src, mc});
+                                if (jt == yid.end()) {
+                                    jt = yid.emplace(std::make_pair(src, mc), (int)y_cell.size()).first;
+                                    y_cell.push_back(src);
+                                    y_mat.push_back(mc);
+                                }
+                                xs_src.push_back(jt->second);
+                            } else {
+                                xs_src.push_back(src);
+                            }
+                            xs_w.push_back(mesh.nv_w[q]);
+                        }
+                        xs_ptr.push_back((int)xs_src.size());
+                    }
+                    cfx[3 * (size_t)k + t] = it->second;
+                }
+            }
+        }
+        d.ncross_x = (int)x_mat.size();
+        d.ncross_y = (int)y_cell.size();
+        d.cf_x = up_i(cfx);
+        if (d.ncross_x > 0) {
+            d.x_mat = up_i(x_mat);
+            d.xs_ptr = up_i(xs_ptr);
+            if (!xs_src.empty()) {
+                d.xs_src = up_i(xs_src);
+                d.xs_w = up_d(xs_w);
+            }
+        }
+        if (d.ncross_y > 0) {
+            d.y_cell = up_i(y_cell);
+            d.y_mat = up_i(y_mat);
+        }
+    }
 
     const int nb = bands.nb, nd = ang.nd;
     DPhys &p = dp_;
@@ -2872,14 +3027,15 @@ Error Solver::alloc_all() {
     // 256 bytes): a direction-sharded solve sums the block over its handles
     {
         auto pad = [](size_t n) { return (n + 31) & ~(size_t)31; };
-        const size_t part[7] = {nc, nc, 3 * nc, nb * nc, nc, 6 * nc, nd * nbs * nb};
+        const size_t ny = (size_t)dm_.ncross_y;
+        const size_t part[9] = {nc, nc, 3 * nc, nb * nc, nc, 6 * nc, nd * nbs * nb, ny, 6 * ny};
         xch_n_ = 0;
         for (size_t n : part) xch_n_ += pad(n);
         xch_ = (double *)A(xch_n_ * 8);
         if (!xch_) return {-6, "device allocation failed (moments)"};
         double *x = xch_;
-        double **dst[7] = {&Tlat_, &E_, &q_, &Tband_, &Th_, &Q_, &eb_};
-        for (int i = 0; i < 7; i++) {
+        double **dst[9] = {&Tlat_, &E_, &q_, &Tband_, &Th_, &Q_, &eb_, &ThC_, &QC_};
+        for (int i = 0; i < 9; i++) {
             *dst[i] = x;
             x += pad(part[i]);
         }
@@ -2894,6 +3050,10 @@ Error Solver::alloc_all() {
     Qs_ = (double *)A(nbs * 6 * 8);
     ThV_ = (double *)A(nslot * 8);
     QV_ = (double *)A(nslot * 6 * 8);
+    if (dm_.ncross_x > 0) {
+        ThX_ = (double *)A((size_t)dm_.ncross_x * 8);
+        QX_ = (double *)A((size_t)dm_.ncross_x * 6 * 8);
+    }
     bTm_ = (double *)A(nbs * 8);
     TV_ = (double *)A(nslot * 8);
     rhs_ = (double *)A(nc * 8);
@@ -3896,6 +4056,9 @@ Error Solver::solve_t(SolveStats &st) {
         GL(K_MOMENTS, (k_moments<S><<<gM, cpb * nb, msmem, s>>>(dm_, dp_, cpb, eps, (const S *)corr_, Tbase_, wtab_,
                                                                 Tlat_, E_, q_, Tband_, Th_, Q_, 1, d0, nbt,
                                                                 d0 > dlo ? 1 : 0)));
+        if (dm_.ncross_y > 0)
+            GL(K_MOMENTS, (k_cross_cell<S><<<grid_for((size_t)dm_.ncross_y * 32), kThreads, 0, s>>>(
+                              dm_, dp_, (const S *)eps, Tbase_, ThC_, QC_, d0, nbt, d0 > dlo ? 1 : 0)));
         GL(K_BOUND_OUT, (k_bound_out<S, DIM><<<grid_for((size_t)nbt * nbs * nb), kThreads, 0, s>>>(dm_, dp_, ev, eb_, d0,
                                                                                                nbt)));
         }
@@ -3912,7 +4075,10 @@ Error Solver::solve_t(SolveStats &st) {
         if (!cfg.sequential) {
             GL(K_SIDE_MOMENTS, k_side_moments<<<gW, kThreads, 0, s>>>(dm_, dp_, eb_, Ths_, Qs_));
             GL(K_NODE_INTERP, k_node_interp<<<gN, kThreads, 0, s>>>(dm_, Th_, Q_, Ths_, Qs_, ThV_, QV_));
-            GL(K_REMACRO, k_remacro<<<gC, kThreads, 0, s>>>(dm_, Th_, Q_, Ths_, Qs_, ThV_, QV_, remacro_));
+            if (dm_.ncross_x > 0)
+                GL(K_NODE_INTERP, k_cross_node<<<grid_for((size_t)dm_.ncross_x * 32), kThreads, 0, s>>>(
+                                      dm_, dp_, eb_, ThC_, QC_, ThX_, QX_));
+            GL(K_REMACRO, k_remacro<<<gC, kThreads, 0, s>>>(dm_, Th_, Q_, Ths_, Qs_, ThV_, QV_, ThX_, QX_, remacro_));
         }
         gather();
         if (!cfg.sequential) GL(K_MACRO_BC, k_macro_bc<<<gW, kThreads, 0, s>>>(dm_, dp_, eb_, bTovr_, bTm_));

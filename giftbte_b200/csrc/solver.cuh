@@ -19,6 +19,16 @@ struct DMesh {
     const double *tsc;  // 1 / s_c: per-cell scale of the relaxation time (scattering multiplier s_c)
     int nmat;           // materials: node values are kept per (node, material) slot
     const int *matter;  // [nc] cell material, nullptr with one material
+    // Wall faces read their node values at the raw node index of the slot
+    // array; where that slot's material is not the wall cell's, the value is
+    // formed again with the cell material's coefficients ("cross" values):
+    // cf_x[3k + t] is the cross value of vertex t of cell-face k, or -1;
+    // cross value x interpolates the entries xs_ptr[x] .. xs_ptr[x + 1] of
+    // xs_src (y >= 0: cell y_cell[y] under material y_mat[y]; -1 - s: wall
+    // side s under material x_mat[x]) with weights xs_w.
+    int ncross_x, ncross_y;
+    const int *cf_x, *x_mat, *xs_ptr, *xs_src, *y_cell, *y_mat;
+    const double *xs_w;
     const int *nbr_ptr, *nbr_idx;
     const double *lsq_w;
     const float *lsq_wf;
@@ -201,6 +211,9 @@ private:
            *Tband_ = nullptr, *remacro_ = nullptr, *Th_ = nullptr, *Q_ = nullptr, *Ths_ = nullptr, *Qs_ = nullptr,
            *ThV_ = nullptr, *QV_ = nullptr, *bTm_ = nullptr, *bTovr_ = nullptr, *TV_ = nullptr, *rhs_ = nullptr,
            *T1_ = nullptr, *red_ = nullptr;
+    // cross values of wall faces (multi-material): per (cell, material) pair
+    // moments ThC/QC (in the exchanged block) and their node values ThX/QX
+    double *ThC_ = nullptr, *QC_ = nullptr, *ThX_ = nullptr, *QX_ = nullptr;
     // diffuse weights / specular map
     double *dif_w_ = nullptr;
     double *dsum_ = nullptr;  // [wall side][band] diffuse re-emission sums
