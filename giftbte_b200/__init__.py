@@ -124,7 +124,8 @@ class DeckInfo(ctypes.Structure):
                 ("capacity_bulk", ctypes.c_double), ("total_volume", ctypes.c_double),
                 ("max_iter_or_zero", ctypes.c_double), ("err_temp", ctypes.c_double),
                 ("err_flux", ctypes.c_double), ("max_level_width", ctypes.c_int), ("sweep_ring", ctypes.c_int),
-                ("far_slots", ctypes.c_int), ("far_refs", ctypes.c_longlong)]
+                ("far_slots", ctypes.c_int), ("far_refs", ctypes.c_longlong),
+                ("index_entries_checked", ctypes.c_longlong)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

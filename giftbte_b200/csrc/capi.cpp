@@ -304,6 +304,27 @@ static int inspect_common(const gbte::RawMesh &raw_in, const gbte::Bands &bands_
     info->sweep_ring = sp.ring;
     info->far_slots = sp.far_slots;
     info->far_refs = sp.far_refs;
+    if (gbte::index_checks_enabled()) {
+        e = gbte::check_indices(fm, bands.nb, sch, ang.nd, sp, info->index_entries_checked);
+        if (e.code) return fail(nullptr, e), status_of(e.code);
+        // the tiles the solver would build for the shared-memory gradient
+        // and residual forms
+        for (int B : {fm.dim == 3 ? 32 : 64, fm.dim == 3 ? 64 : 128}) {
+            gbte::GradTiles gt;
+            gbte::FaceTiles ft;
+            long long n = 0;
+            if (gbte::build_grad_tiles(fm, B, gt).code == 0) {
+                e = gbte::check_tiles(fm, &gt, nullptr, n);
+                if (e.code) return fail(nullptr, e), status_of(e.code);
+                info->index_entries_checked += n;
+            }
+            if (gbte::build_face_tiles(fm, B, ft).code == 0) {
+                e = gbte::check_tiles(fm, nullptr, &ft, n);
+                if (e.code) return fail(nullptr, e), status_of(e.code);
+                info->index_entries_checked += n;
+            }
+        }
+    }
     return GBTE_OK;
 }
 

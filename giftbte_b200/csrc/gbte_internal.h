@@ -194,4 +194,17 @@ struct FaceTiles {
 };
 Error build_face_tiles(const FlatMesh &m, int B, FaceTiles &out);
 
+// Index checks, the stand-in for a device memory checker: every CSR offset
+// and index array of the flattened mesh, the level schedule and the sweep
+// records is checked against the range it indexes (offsets monotone and
+// spanning their entries, every level order a permutation, every upwind
+// reference an earlier position or a far slot). Enabled by building with
+// -DGBTE_DEBUG or by a non-zero GBTE_DEBUG environment variable; gbte_create
+// and gbte_inspect_* then run it and fail with GBTE_ERR_MESH on the first
+// entry out of range. `checked` counts the entries looked at.
+bool index_checks_enabled();
+Error check_indices(const FlatMesh &m, int nb, const Schedule &s, int nd, const SweepPlan &sp, long long &checked);
+// the same for the shared-memory tiles (either may be null)
+Error check_tiles(const FlatMesh &m, const GradTiles *g, const FaceTiles *f, long long &checked);
+
 }  // namespace gbte

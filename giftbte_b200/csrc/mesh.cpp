@@ -16,6 +16,8 @@
 // 3D tetrahedra (stripped from the reference's public release) use face j =
 // the three vertices other than vertex j, area by Heron, outward normal.
 #include <algorithm>
+#include <cstdlib>
+#include <cstring>
 #include <cmath>
 #include <numeric>
 #include <queue>
@@ -935,6 +937,203 @@ Error build_face_tiles(const FlatMesh &m, int B, FaceTiles &out) {
         out.ptr.push_back((int)out.cells.size());
         out.umax = std::max(out.umax, nu);
     }
+    return {0, ""};
+}
+
+}  // namespace gbte
+
+namespace gbte {
+
+bool index_checks_enabled() {
+#ifdef GBTE_DEBUG
+    return true;
+#else
+    const char *v = std::getenv("GBTE_DEBUG");
+    return v && *v && std::strcmp(v, "0") != 0;
+#endif
+}
+
+namespace {
+
+// Range checks over index arrays; the first failure is kept.
+struct IndexCheck {
+    long long n = 0;
+    std::string err;
+    bool ok() const { return err.empty(); }
+    void fail(const std::string &what) {
+        if (err.empty()) err = what;
+    }
+    void size(const char *name, size_t got, size_t want) {
+        if (got != want)
+            fail(std::string(name) + ": " + std::to_string(got) + " entries, expected " + std::to_string(want));
+    }
+    void value(const char *name, size_t i, long long v, long long lo, long long hi) {
+        n++;
+        if (v < lo || v >= hi)
+            fail(std::string(name) + "[" + std::to_string(i) + "] = " + std::to_string(v) + " outside [" +
+                 std::to_string(lo) + ", " + std::to_string(hi) + ")");
+    }
+    void range(const char *name, const std::vector<int> &v, long long lo, long long hi) {
+        for (size_t i = 0; i < v.size() && ok(); i++) value(name, i, v[i], lo, hi);
+    }
+    // CSR offsets of `rows` rows over `total` entries
+    void offsets(const char *name, const std::vector<int> &p, size_t rows, long long total) {
+        size(name, p.size(), rows + 1);
+        if (!ok()) return;
+        if (p[0] != 0 || p[rows] != total) fail(std::string(name) + ": offsets do not span the entries");
+        for (size_t i = 0; i < rows && ok(); i++) {
+            n++;
+            if (p[i + 1] < p[i]) fail(std::string(name) + "[" + std::to_string(i + 1) + "] decreases");
+        }
+    }
+};
+
+}  // namespace
+
+Error check_indices(const FlatMesh &m, int nb, const Schedule &s, int nd, const SweepPlan &sp, long long &checked) {
+    IndexCheck c;
+    const int nc = m.nc, nn = m.nn, ncf = m.ncf(), nf = m.nf(), nbd = m.nbd(), nbs = m.nbs();
+    const size_t nslot = (size_t)nn * m.nmat;
+    // cells and cell faces
+    c.offsets("cf_ptr", m.cf_ptr, nc, ncf);
+    c.size("matter", m.matter.size(), nc);
+    c.range("matter", m.matter, 0, m.nmat);
+    c.size("cf_nbr", m.cf_nbr.size(), ncf);
+    c.size("cf_bound", m.cf_bound.size(), ncf);
+    c.size("cf_bside", m.cf_bside.size(), ncf);
+    c.size("cf_face", m.cf_face.size(), ncf);
+    c.size("cf_v", m.cf_v.size(), 3 * (size_t)ncf);
+    c.range("cf_bound", m.cf_bound, -1, nbd);
+    c.range("cf_face", m.cf_face, 0, nf);
+    for (int cc = 0; cc < nc && c.ok(); cc++)
+        for (int k = m.cf_ptr[cc]; k < m.cf_ptr[cc + 1] && c.ok(); k++) {
+            if (m.cf_bound[k] < 0) {
+                c.value("cf_nbr", k, m.cf_nbr[k], 0, nc);
+            } else {
+                c.value("cf_bside", k, m.cf_bside[k], 0, nbs);
+                if (c.ok() && (m.bs_cf[m.cf_bside[k]] != k || m.bs_cell[m.cf_bside[k]] != cc))
+                    c.fail("cf_bside[" + std::to_string(k) + "] names a wall side of another cell face");
+            }
+            for (int t = 0; t < m.dim && c.ok(); t++) c.value("cf_v", 3 * (size_t)k + t, m.cf_v[3 * (size_t)k + t], 0, nn);
+        }
+    // global faces
+    c.range("f_cell0", m.f_cell0, 0, nc);
+    c.range("f_cf0", m.f_cf0, 0, ncf);
+    c.range("f_cell1", m.f_cell1, -1, nc);
+    c.range("f_cf1", m.f_cf1, -1, ncf);
+    c.range("f_bound", m.f_bound, -1, nbd);
+    if (m.dim == 3) c.size("face_w", m.face_w.size(), 9 * (size_t)nf);
+    // least-squares stencil
+    c.offsets("nbr_ptr", m.nbr_ptr, nc, (long long)m.nbr_idx.size());
+    c.range("nbr_idx", m.nbr_idx, 0, nc);
+    c.size("lsq_w", m.lsq_w.size(), 3 * m.nbr_idx.size());
+    // walls
+    c.size("b_connect", m.b_connect.size(), nbd);
+    for (int ib = 0; ib < nbd && c.ok(); ib++)
+        if (m.b_type[ib] < 0) c.value("b_connect", ib, m.b_connect[ib], 0, nbd);
+    c.size("bs_cell", m.bs_cell.size(), nbs);
+    c.size("bs_cf", m.bs_cf.size(), nbs);
+    c.range("bs_cell", m.bs_cell, -1, nc);
+    c.range("bs_cf", m.bs_cf, -1, ncf);
+    if (!m.bs_trans.empty()) c.size("bs_trans", m.bs_trans.size(), (size_t)nbs * nb);
+    // node slots
+    c.offsets("nv_ptr", m.nv_ptr, nslot, (long long)m.nv_src.size());
+    c.range("nv_src", m.nv_src, -(long long)nbs, nc);
+    c.size("nv_w", m.nv_w.size(), m.nv_src.size());
+    c.offsets("nt_ptr", m.nt_ptr, nslot, (long long)m.nt_src.size());
+    c.range("nt_src", m.nt_src, 0, nc);
+    c.size("nt_w", m.nt_w.size(), m.nt_src.size());
+    c.size("node_x", m.node_x.size(), nn);
+    c.offsets("comp_ptr", m.comp_ptr, m.ncomp() < 0 ? 0 : m.ncomp(), nc);
+    // schedule: every direction's level order is a permutation of the cells
+    c.size("lvl_cells", s.lvl_cells.size(), (size_t)nd * nc);
+    c.size("dir_lvl_off", s.dir_lvl_off.size(), (size_t)nd * s.ncomp + 1);
+    if (!s.lag.empty()) c.size("lag", s.lag.size(), (size_t)nd * nc);
+    std::vector<int> seen(nc, -1);
+    for (int d = 0; d < nd && c.ok(); d++)
+        for (int pos = 0; pos < nc && c.ok(); pos++) {
+            const int cell = s.lvl_cells[(size_t)d * nc + pos];
+            c.value("lvl_cells", (size_t)d * nc + pos, cell, 0, nc);
+            if (c.ok() && seen[cell] == d) c.fail("lvl_cells: direction " + std::to_string(d) + " visits a cell twice");
+            if (c.ok()) seen[cell] = d;
+        }
+    for (size_t e = 0; e + 1 < s.dir_lvl_off.size() && c.ok(); e++) {
+        c.value("dir_lvl_off", e, s.dir_lvl_off[e], 0, (long long)s.lvl_ptr.size());
+        for (int l = s.dir_lvl_off[e]; l < s.dir_lvl_off[e + 1] && c.ok(); l++) {
+            c.value("lvl_ptr", l, s.lvl_ptr[l], 0, (long long)nc + 1);
+            if (c.ok() && l + 1 < s.dir_lvl_off[e + 1] && s.lvl_ptr[l + 1] < s.lvl_ptr[l])
+                c.fail("lvl_ptr[" + std::to_string(l + 1) + "] decreases");
+        }
+    }
+    // sweep records: upwind neighbours are earlier positions or far slots
+    const size_t np = (size_t)nd * nc;
+    c.size("sweep cell", sp.cell.size(), np);
+    c.size("sweep nin", sp.nin.size(), np);
+    c.size("sweep np", sp.np.size(), 4 * np);
+    c.size("sweep far_w", sp.far_w.size(), np);
+    for (size_t P = 0; P < np && c.ok(); P++) {
+        const int pos = (int)(P % nc);
+        c.value("sweep cell", P, sp.cell[P], 0, nc);
+        c.value("sweep nin", P, sp.nin[P], 0, 5);
+        c.value("sweep far_w", P, sp.far_w[P], -1, sp.far_enabled ? sp.far_slots : 0);
+        for (int j = 0; j < sp.nin[P] && c.ok(); j++) {
+            const int q = sp.np[4 * P + j];
+            if (q >= 0)
+                c.value("sweep np", 4 * P + j, q, 0, pos);
+            else
+                c.value("sweep np (far slot)", 4 * P + j, -1 - (long long)q, 0, sp.far_enabled ? sp.far_slots : 0);
+        }
+    }
+    checked = c.n;
+    if (!c.ok()) return {-7, "index check: " + c.err};
+    return {0, ""};
+}
+
+Error check_tiles(const FlatMesh &m, const GradTiles *g, const FaceTiles *f, long long &checked) {
+    IndexCheck c;
+    const int nc = m.nc;
+    auto tile = [&](const char *name, int B, int nblk, int umax, const std::vector<int> &ptr,
+                    const std::vector<int> &cells) {
+        c.size(name, (size_t)nblk, (size_t)((nc + B - 1) / std::max(1, B)));
+        c.offsets(name, ptr, nblk, (long long)cells.size());
+        c.range(name, cells, 0, nc);
+        for (int b = 0; b < nblk && c.ok(); b++) {
+            c.value(name, b, ptr[b + 1] - ptr[b], 0, (long long)umax + 1);
+            // a block's union starts with its own cells in order
+            for (int i = 0; i < std::min(B, nc - b * B) && c.ok(); i++)
+                if (cells[ptr[b] + i] != b * B + i) c.fail(std::string(name) + ": block does not start with its cells");
+        }
+    };
+    if (g) {
+        tile("gradient tile", g->B, g->nblk, g->umax, g->ptr, g->cells);
+        c.size("gradient tile loc", g->loc.size(), m.nbr_idx.size());
+        for (int cc = 0; cc < nc && c.ok(); cc++) {
+            const int b = cc / g->B, base = g->ptr[b], u = g->ptr[b + 1] - base;
+            for (int q = m.nbr_ptr[cc]; q < m.nbr_ptr[cc + 1] && c.ok(); q++) {
+                c.value("gradient tile loc", q, g->loc[q], 0, u);
+                if (c.ok() && g->cells[base + g->loc[q]] != m.nbr_idx[q])
+                    c.fail("gradient tile loc[" + std::to_string(q) + "] names another cell");
+            }
+        }
+    }
+    if (f) {
+        tile("residual tile", f->B, f->nblk, f->umax, f->ptr, f->cells);
+        c.size("residual tile floc", f->floc.size(), (size_t)m.ncf());
+        for (int cc = 0; cc < nc && c.ok(); cc++) {
+            const int b = cc / f->B, base = f->ptr[b], u = f->ptr[b + 1] - base;
+            for (int k = m.cf_ptr[cc]; k < m.cf_ptr[cc + 1] && c.ok(); k++) {
+                if (m.cf_bound[k] >= 0) {
+                    if (f->floc[k] != 0xFFFF) c.fail("residual tile floc[" + std::to_string(k) + "] set on a wall");
+                    continue;
+                }
+                c.value("residual tile floc", k, f->floc[k], 0, u);
+                if (c.ok() && f->cells[base + f->floc[k]] != m.cf_nbr[k])
+                    c.fail("residual tile floc[" + std::to_string(k) + "] names another cell");
+            }
+        }
+    }
+    checked = c.n;
+    if (!c.ok()) return {-7, "index check: " + c.err};
     return {0, ""};
 }
 

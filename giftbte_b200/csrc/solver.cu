@@ -2710,6 +2710,11 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
         Error pe = build_sweep_plan(mesh, ang, sched, kSweepMinRing,
                                     cfg.sweep_far_slots == 0 ? kSweepFarCap : std::max(0, cfg.sweep_far_slots), sp);
         if (pe.code) return pe;
+        if (index_checks_enabled()) {
+            long long checked = 0;
+            Error ce = check_indices(mesh, bands.nb, sched, nd, sp, checked);
+            if (ce.code) return ce;
+        }
         ring_ = sp.ring;
         far_slots_ = sp.far_enabled ? sp.far_slots : 0;
         std::vector<SweepRec<double>> recd;
@@ -4335,6 +4340,11 @@ Error Solver::grad_tiles() {
     for (int B : cand) {
         GradTiles t;
         if (build_grad_tiles(mesh, B, t).code) continue;
+        if (index_checks_enabled()) {
+            long long checked = 0;
+            Error ce = check_tiles(mesh, &t, nullptr, checked);
+            if (ce.code) return ce;
+        }
         TileDev d;
         d.B = t.B, d.nblk = t.nblk, d.umax = t.umax, d.qmax = t.qmax;
         d.ptr = upload(this, allocs_, t.ptr, s, ok);
@@ -4347,6 +4357,11 @@ Error Solver::grad_tiles() {
     for (int B : cand) {
         FaceTiles t;
         if (build_face_tiles(mesh, B, t).code) continue;
+        if (index_checks_enabled()) {
+            long long checked = 0;
+            Error ce = check_tiles(mesh, nullptr, &t, checked);
+            if (ce.code) return ce;
+        }
         FaceTileDev d;
         d.B = t.B, d.nblk = t.nblk, d.umax = t.umax;
         d.ptr = upload(this, allocs_, t.ptr, s, ok);

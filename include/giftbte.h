@@ -260,6 +260,7 @@ typedef struct {
     int sweep_ring;            /* on-chip correction ring of the sweep (positions) */
     int far_slots;             /* on-chip slots for upwind reads older than the ring */
     long long far_refs;        /* upwind reads older than the ring, all directions */
+    long long index_entries_checked; /* entries range-checked (0 unless GBTE_DEBUG is set or built in) */
 } gbte_deck_info;
 
 int gbte_inspect_deck(const char *dir, gbte_deck_info *info);

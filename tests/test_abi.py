@@ -123,3 +123,46 @@ def test_create_without_device_fails_cleanly():
     with pytest.raises(g.GBTEError) as e:
         g.StaticBTESynthetic.from_deck(decks.config1_deck(4))
     assert e.value.status == -3
+
+
+@pytest.mark.parametrize("make", [lambda: decks.config1_deck(12), lambda: decks.config2_deck(h_nm=15.0, n_bands=4, n_phi=4),
+                                  lambda: decks.interface_deck(8),
+                                  lambda: decks.config3_deck(h_nm=25.0, size_nm=(100.0, 100.0, 100.0), n_bands=4)],
+                         ids=["square", "porous", "interface", "block3d"])
+def test_index_checks_pass_on_built_meshes(make, monkeypatch):
+    # GBTE_DEBUG turns on the range checks of every CSR and index array the
+    # solver would upload (mesh, schedule, sweep records, gradient and
+    # residual tiles); they are off by default
+    d = make()
+    monkeypatch.delenv("GBTE_DEBUG", raising=False)
+    assert g.inspect(d)["index_entries_checked"] == 0
+    monkeypatch.setenv("GBTE_DEBUG", "1")
+    info = g.inspect(d)
+    assert info["index_entries_checked"] > 10 * info["num_cells"]
+
+
+def test_index_checks_catch_planted_entries(tmp_path):
+    # the checker itself, host only: tests/index_check_main.cpp builds the
+    # arrays the solver uploads for a porous-cell deck, expects them to pass,
+    # then plants one bad entry per array kind (a neighbour past the cells,
+    # decreasing offsets, a negative stencil index, a wall side past the
+    # range, a cell visited twice by a level order, a sweep record reading a
+    # later position, tile indices past or beside their unions) and expects
+    # each to be caught as a mesh error
+    import shutil
+    import subprocess
+
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("g++ not available")
+    csrc = os.path.join(ROOT, "giftbte_b200", "csrc")
+    exe = str(tmp_path / "index_check")
+    subprocess.check_call([gxx, "-std=c++17", "-O1", "-I", csrc, os.path.join(ROOT, "tests", "index_check_main.cpp")] +
+                          [os.path.join(csrc, f) for f in ("deck.cpp", "mesh.cpp", "angles.cpp")] +
+                          ["-lpthread", "-o", exe])
+    decks.config2_deck(h_nm=15.0, n_bands=4, n_phi=4).write(str(tmp_path / "deck"))
+    r = subprocess.run([exe, str(tmp_path / "deck")], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    lines = r.stdout.splitlines()
+    assert lines[0].startswith("built: pass") and lines[1].startswith("tiles: pass")
+    assert sum(": caught" in l for l in lines) == 8 and lines[-1] == "OK"
