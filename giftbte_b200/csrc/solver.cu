@@ -128,6 +128,34 @@ __global__ void k_cell_lsq_grad(DMesh m, const double *__restrict__ T, double *_
 // g[d][c][r][b] = sum_k w_ck (eps_k - eps_c), r < DIM (weights in the
 // storage precision; lanes of a warp share the cell, so the stencil loads
 // are broadcasts and the neighbour loads are coalesced over bands)
+// LSQ gradient g_c = sum_j w_j (e_j - e_c). The FP64 form sums the
+// differences entry by entry, as the reference does
+// (StaticBTESynthetic.cpp:1243-1290). The FP32 form sums w_j e_j and then
+// subtracts (sum_j w_j) e_c once per cell, with the weight sums lsq_ws
+// precomputed: one fewer operation per stencil entry, and its values are
+// deviations from the cell's base, so the extra rounding stays at the level
+// of e's own. Every FP32 gradient kernel uses this split, in the same order.
+template <typename S>
+__device__ __forceinline__ S nbr_term(S ej, S ec) {
+    if constexpr (sizeof(S) == 4)
+        return ej;
+    else
+        return ej - ec;
+}
+template <int BC, typename S>
+__device__ __forceinline__ void centre_term(const DMesh &m, int c, const S (&ec)[BC], S (&gx)[BC], S (&gy)[BC],
+                                            S (&gz)[BC]) {
+    if constexpr (sizeof(S) == 4) {
+        const float4 ws = m.lsq_ws[c];
+#pragma unroll
+        for (int i = 0; i < BC; i++) {
+            gx[i] = __fmaf_rn(-ws.x, ec[i], gx[i]);
+            gy[i] = __fmaf_rn(-ws.y, ec[i], gy[i]);
+            gz[i] = __fmaf_rn(-ws.z, ec[i], gz[i]);
+        }
+    }
+}
+
 template <typename S, int DIM>
 __global__ void __launch_bounds__(256) k_gradient(DMesh m, DPhys p, const S *__restrict__ w, const S *__restrict__ eps,
                                                   S *__restrict__ g, int d0, int ndb) {
@@ -142,10 +170,15 @@ __global__ void __launch_bounds__(256) k_gradient(DMesh m, DPhys p, const S *__r
         S gx = 0, gy = 0, gz = 0;
         const int q1 = m.nbr_ptr[c + 1];
         for (int q = m.nbr_ptr[c]; q < q1; q++) {
-            const S de = ed[(size_t)m.nbr_idx[q] * nb] - ec;
+            const S de = nbr_term(ed[(size_t)m.nbr_idx[q] * nb], ec);
             gx += w[3 * q] * de;
             gy += w[3 * q + 1] * de;
             if (DIM == 3) gz += w[3 * q + 2] * de;
+        }
+        if constexpr (sizeof(S) == 4) {
+            S ecv[1] = {ec}, gxv[1] = {gx}, gyv[1] = {gy}, gzv[1] = {gz};
+            centre_term<1>(m, c, ecv, gxv, gyv, gzv);
+            gx = gxv[0], gy = gyv[0], gz = gzv[0];
         }
         S *gp = g + dc * DIM * nb + b;
         gp[0] = gx;
@@ -330,13 +363,14 @@ __global__ void __launch_bounds__(256) k_gradient8(DMesh m, DPhys p, const S *__
                 const S wx = w[3 * (q + u)], wy = w[3 * (q + u) + 1], wz = DIM == 3 ? w[3 * (q + u) + 2] : S(0);
 #pragma unroll
                 for (int i = 0; i < BC; i++) {
-                    const S de = e4[u][i] - ec[i];
+                    const S de = nbr_term(e4[u][i], ec[i]);
                     gx[i] += wx * de;
                     gy[i] += wy * de;
                     if (DIM == 3) gz[i] += wz * de;
                 }
             }
         }
+        centre_term<BC>(m, c, ec, gx, gy, gz);
         S *gp = g + dc * DIM * nb + BC * bc;
         st8(gp, gx);
         st8(gp + nb, gy);
@@ -411,7 +445,7 @@ __global__ void __launch_bounds__(256) k_gradient_md(DMesh m, DPhys p, const flo
                 for (int k = 0; k < DG; k++)
 #pragma unroll
                     for (int i = 0; i < BC; i++) {
-                        const S de = e4[u][k][i] - ec[k][i];
+                        const S de = nbr_term(e4[u][k][i], ec[k][i]);
                         gx[k][i] += wx[u] * de;
                         gy[k][i] += wy[u] * de;
                         if (DIM == 3) gz[k][i] += wz[u] * de;
@@ -422,6 +456,7 @@ __global__ void __launch_bounds__(256) k_gradient_md(DMesh m, DPhys p, const flo
         for (int k = 0; k < DG; k++) {
             const int dl = grp * DG + k;
             if (dl >= ndb) break;
+            centre_term<BC>(m, c, ec[k], gx[k], gy[k], gz[k]);
             S *gp = g + ((size_t)dl * nc + c) * DIM * nb + BC * bc;
             st8(gp, gx[k]);
             st8(gp + nb, gy[k]);
@@ -483,7 +518,7 @@ __global__ void __launch_bounds__(256) k_gradient_wc(DMesh m, DPhys p, const flo
                 for (int k = 0; k < DG; k++)
 #pragma unroll
                     for (int i = 0; i < BC; i++) {
-                        const S de = e4[u][k][i] - ec[k][i];
+                        const S de = nbr_term(e4[u][k][i], ec[k][i]);
                         gx[k][i] += wx[u] * de;
                         gy[k][i] += wy[u] * de;
                         if (DIM == 3) gz[k][i] += wz[u] * de;
@@ -495,6 +530,7 @@ __global__ void __launch_bounds__(256) k_gradient_wc(DMesh m, DPhys p, const flo
         for (int k = 0; k < DG; k++) {
             const int dl = grp * dpw + slot * DG + k;
             if (dl >= ndb) break;
+            centre_term<BC>(m, c, ec[k], gx[k], gy[k], gz[k]);
             S *gp = g + ((size_t)dl * nc + c) * DIM * nb + BC * bc;
             st8(gp, gx[k]);
             st8(gp + nb, gy[k]);
@@ -814,13 +850,14 @@ __global__ void __launch_bounds__(512) k_gradient_tile(DMesh m, DPhys p, const f
                     ld8(et + (size_t)t.loc * nbc + 4 * j, e);
 #pragma unroll
                     for (int v = 0; v < 4; v++) {
-                        const S de = e[v] - ec[v];
+                        const S de = nbr_term(e[v], ec[v]);
                         gx[v] += t.wx * de;
                         gy[v] += t.wy * de;
                         if (DIM == 3) gz[v] += t.wz * de;
                     }
                 }
             }
+            centre_term<4>(m, c, ec, gx, gy, gz);
             S *gp = g + ((size_t)dl * nc + c) * DIM * nb + b0 + 4 * j;
             st8(gp, gx);
             st8(gp + nb, gy);
@@ -2581,6 +2618,18 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
             pk[q] = make_float4((float)mesh.lsq_w[3 * q], (float)mesh.lsq_w[3 * q + 1], (float)mesh.lsq_w[3 * q + 2], jf);
         }
         d.lsq_pk = upload(this, allocs_, pk, s, ok);
+        // per-cell sums of the FP32 weights (the FP32 gradient's centre term)
+        std::vector<float4> ws(mesh.nc, make_float4(0.f, 0.f, 0.f, 0.f));
+        for (int c = 0; c < mesh.nc; c++) {
+            double sx = 0, sy = 0, sz = 0;
+            for (int q = mesh.nbr_ptr[c]; q < mesh.nbr_ptr[c + 1]; q++) {
+                sx += (double)(float)mesh.lsq_w[3 * (size_t)q];
+                sy += (double)(float)mesh.lsq_w[3 * (size_t)q + 1];
+                sz += (double)(float)mesh.lsq_w[3 * (size_t)q + 2];
+            }
+            ws[c] = make_float4((float)sx, (float)sy, (float)sz, 0.f);
+        }
+        d.lsq_ws = upload(this, allocs_, ws, s, ok);
     }
     d.face_w = up_d(mesh.face_w);
     d.f_cf0 = up_i(mesh.f_cf0);

@@ -33,6 +33,7 @@ struct DMesh {
     const double *lsq_w;
     const float *lsq_wf;
     const float4 *lsq_pk;  // per stencil entry {w_x, w_y, w_z, neighbour index bits} in FP32
+    const float4 *lsq_ws;  // per cell {sum w_x, sum w_y, sum w_z, 0} of the FP32 weights
     const double *face_w;
     const int *f_cf0;
     const int *b_type, *b_connect;
