@@ -333,7 +333,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             "tuning": {"sweep_bands": st.get("sweep_bands"), "sweep_stage_levels": st.get("sweep_stage_levels"),
                        "sweep_vector": st.get("sweep_vector"), "sweep_threads": st.get("sweep_threads"),
                        "sweep_kernel": {1: "block", 2: "warp", 3: "wide"}.get(st.get("sweep_kernel")),
-                       "gradient_dirs": st.get("gradient_dirs"), "direction_batch": st.get("direction_batch")},
+                       "gradient_dirs": st.get("gradient_dirs"), "residual_form": st.get("residual_form"),
+                       "direction_batch": st.get("direction_batch")},
             "roofline": roofline, "hbm_kernels": hbm_kernels, "kernels": kernel_table, "cpu_baseline": cpu,
             "e2e": e2e, "time_to_residual": ttr, "gpu_launches": int(st["kernel_launches"]), "clocks": clk,
             "macro": {"ms_per_step": st["macro_ms"] / args.steps, "cg_iterations": st["macro_cg_iterations"]},

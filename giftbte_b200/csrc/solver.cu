@@ -577,6 +577,21 @@ __global__ void __launch_bounds__(256) k_base_flux(DMesh m, DPhys p, const doubl
     }
 }
 
+// Offset from a cell's centre to the centre of its face k, in the storage
+// precision: from the face's own cell (own) or from its neighbour across the
+// face. FP32 reads it precomputed per cell-face (the same FP64 difference
+// rounded once, so the same bits); FP64 forms the difference.
+template <typename S, int DIM>
+__device__ __forceinline__ void face_off(const DMesh &m, int k, int cell, bool own, S &rx, S &ry, S &rz) {
+    if constexpr (sizeof(S) == 4) {
+        const float4 r = own ? m.cf_r4[k] : m.cf_rn4[k];
+        rx = r.x, ry = r.y, rz = r.z;
+    } else {
+        rx = (S)(m.cf_fx[k] - m.cx[cell]), ry = (S)(m.cf_fy[k] - m.cy[cell]);
+        rz = DIM == 3 ? (S)(m.cf_fz[k] - m.cz[cell]) : (S)0;
+    }
+}
+
 // Residual, BC bands per thread, in the storage precision S on the stored
 // deviations eps = e - C_b T_base (the base part enters through B):
 //   R = C_b (T_old - T_base - tau|v| B) + Q hr tau / s_c
@@ -619,8 +634,8 @@ __global__ void __launch_bounds__(256, sizeof(S) == 4 ? 4 : 2) k_residual8(DMesh
                     if (DIM == 3) ld8(gp + 2 * nb, gzv);
                     have_gc = true;
                 }
-                const S rx = (S)(m.cf_fx[k] - m.cx[c]), ry = (S)(m.cf_fy[k] - m.cy[c]);
-                const S rz = DIM == 3 ? (S)(m.cf_fz[k] - m.cz[c]) : (S)0;
+                S rx, ry, rz;
+                face_off<S, DIM>(m, k, c, true, rx, ry, rz);
 #pragma unroll
                 for (int i = 0; i < BC; i++) {
                     S y = ec[i] + gxv[i] * rx + gyv[i] * ry;
@@ -635,8 +650,8 @@ __global__ void __launch_bounds__(256, sizeof(S) == 4 ? 4 : 2) k_residual8(DMesh
                 ld8(gp, hx);
                 ld8(gp + nb, hy);
                 if (DIM == 3) ld8(gp + 2 * nb, hz);
-                const S rx = (S)(m.cf_fx[k] - m.cx[j]), ry = (S)(m.cf_fy[k] - m.cy[j]);
-                const S rz = DIM == 3 ? (S)(m.cf_fz[k] - m.cz[j]) : (S)0;
+                S rx, ry, rz;
+                face_off<S, DIM>(m, k, j, false, rx, ry, rz);
 #pragma unroll
                 for (int i = 0; i < BC; i++) {
                     S y = ej[i] + hx[i] * rx + hy[i] * ry;
@@ -683,7 +698,6 @@ __global__ void __launch_bounds__(256) k_residual_wc(DMesh m, DPhys p, EView<S, 
         const int c = (int)(w % nc), grp = (int)(w / nc);
         const int mo = mat_off(p, c);
         const double tsc = m.tsc[c], invV = tsc / m.vol[c], tb = ev.Tb[c];
-        const double cx = m.cx[c], cy = m.cy[c], cz = DIM == 3 ? m.cz[c] : 0.0;
         size_t d[DG];
         double sx[DG], sy[DG], sz[DG];
         S ec[DG][BC], acc[DG][BC], gxv[DG][BC], gyv[DG][BC], gzv[DG][BC];
@@ -705,14 +719,13 @@ __global__ void __launch_bounds__(256) k_residual_wc(DMesh m, DPhys p, EView<S, 
             const double fa = m.cf_area[f] * invV;
             const int bound = m.cf_bound[f];
             const int j = m.cf_nbr[f];
-            const double fx = m.cf_fx[f], fy = m.cf_fy[f], fz = DIM == 3 ? m.cf_fz[f] : 0.0;
 #pragma unroll
             for (int k = 0; k < DG; k++) {
                 const double sn = sx[k] * nx + sy[k] * ny + (DIM == 3 ? sz[k] * nz : 0.0);
                 const S a = (S)(fa * sn);
                 if (sn >= 0) {
-                    const S rx = (S)(fx - cx), ry = (S)(fy - cy);
-                    const S rz = DIM == 3 ? (S)(fz - cz) : (S)0;
+                    S rx, ry, rz;
+                    face_off<S, DIM>(m, f, c, true, rx, ry, rz);
 #pragma unroll
                     for (int i = 0; i < BC; i++) {
                         S y = ec[k][i] + gxv[k][i] * rx + gyv[k][i] * ry;
@@ -727,8 +740,8 @@ __global__ void __launch_bounds__(256) k_residual_wc(DMesh m, DPhys p, EView<S, 
                     ld8(gp, hx);
                     ld8(gp + nb, hy);
                     if (DIM == 3) ld8(gp + 2 * nb, hz);
-                    const S rx = (S)(fx - m.cx[j]), ry = (S)(fy - m.cy[j]);
-                    const S rz = DIM == 3 ? (S)(fz - m.cz[j]) : (S)0;
+                    S rx, ry, rz;
+                    face_off<S, DIM>(m, f, j, false, rx, ry, rz);
 #pragma unroll
                     for (int i = 0; i < BC; i++) {
                         S y = ej[i] + hx[i] * rx + hy[i] * ry;
@@ -926,8 +939,8 @@ __global__ void __launch_bounds__(512) k_residual_tile(DMesh m, DPhys p, EView<S
                 const double sn = sx * m.cf_nx[k] + sy * m.cf_ny[k] + (DIM == 3 ? sz * m.cf_nz[k] : 0.0);
                 const S a = (S)(m.cf_area[k] * invV * sn);
                 if (sn >= 0) {
-                    const S rx = (S)(m.cf_fx[k] - m.cx[c]), ry = (S)(m.cf_fy[k] - m.cy[c]);
-                    const S rz = DIM == 3 ? (S)(m.cf_fz[k] - m.cz[c]) : (S)0;
+                    S rx, ry, rz;
+                    face_off<S, DIM>(m, k, c, true, rx, ry, rz);
 #pragma unroll
                     for (int v = 0; v < 4; v++) {
                         S y = ec[v] + gxv[v] * rx + gyv[v] * ry;
@@ -942,8 +955,8 @@ __global__ void __launch_bounds__(512) k_residual_tile(DMesh m, DPhys p, EView<S
                     ld8(nr + nbc, hx);
                     ld8(nr + 2 * nbc, hy);
                     if (DIM == 3) ld8(nr + 3 * nbc, hz);
-                    const S rx = (S)(m.cf_fx[k] - m.cx[jn]), ry = (S)(m.cf_fy[k] - m.cy[jn]);
-                    const S rz = DIM == 3 ? (S)(m.cf_fz[k] - m.cz[jn]) : (S)0;
+                    S rx, ry, rz;
+                    face_off<S, DIM>(m, k, jn, false, rx, ry, rz);
 #pragma unroll
                     for (int v = 0; v < 4; v++) {
                         S y = ej[v] + hx[v] * rx + hy[v] * ry;
@@ -2630,6 +2643,22 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
             ws[c] = make_float4((float)sx, (float)sy, (float)sz, 0.f);
         }
         d.lsq_ws = upload(this, allocs_, ws, s, ok);
+        // face-centre offsets of the FP32 residual: from the face's cell and
+        // from its neighbour across the face (interior faces)
+        std::vector<float4> r4(mesh.ncf(), make_float4(0.f, 0.f, 0.f, 0.f)), rn4 = r4;
+        for (int c = 0; c < mesh.nc; c++)
+            for (int k = mesh.cf_ptr[c]; k < mesh.cf_ptr[c + 1]; k++) {
+                const bool z = mesh.dim == 3;
+                r4[k] = make_float4((float)(mesh.cf_fx[k] - mesh.cx[c]), (float)(mesh.cf_fy[k] - mesh.cy[c]),
+                                    z ? (float)(mesh.cf_fz[k] - mesh.cz[c]) : 0.f, 0.f);
+                if (mesh.cf_bound[k] < 0) {
+                    const int j = mesh.cf_nbr[k];
+                    rn4[k] = make_float4((float)(mesh.cf_fx[k] - mesh.cx[j]), (float)(mesh.cf_fy[k] - mesh.cy[j]),
+                                         z ? (float)(mesh.cf_fz[k] - mesh.cz[j]) : 0.f, 0.f);
+                }
+            }
+        d.cf_r4 = upload(this, allocs_, r4, s, ok);
+        d.cf_rn4 = upload(this, allocs_, rn4, s, ok);
     }
     d.face_w = up_d(mesh.face_w);
     d.f_cf0 = up_i(mesh.f_cf0);

@@ -34,6 +34,7 @@ struct DMesh {
     const float *lsq_wf;
     const float4 *lsq_pk;  // per stencil entry {w_x, w_y, w_z, neighbour index bits} in FP32
     const float4 *lsq_ws;  // per cell {sum w_x, sum w_y, sum w_z, 0} of the FP32 weights
+    const float4 *cf_r4, *cf_rn4;  // per cell-face FP32 offsets to the face centre from the cell / its neighbour
     const double *face_w;
     const int *f_cf0;
     const int *b_type, *b_connect;
@@ -72,8 +73,10 @@ struct SolverConfig {
     int sweep_vector = 0;     // bands per sweep thread (1, 2, 4), 0 = automatic
     int sweep_kernel = 0;     // 1: block sweep kernel, 2: warp-independent kernel, 3: wide-level kernel, 0 = automatic
     int sweep_far_slots = 0;  // far-slot cap of the sweep plan: 0 = automatic, < 0 = none
-    int gradient_dirs = 0;    // gradient launch shape (1, 2, 4: directions per thread; 5, 6: warp per cell), 0 = automatic
-    int residual_form = 0;    // residual launch shape (1: thread per cell; 5, 6: warp per cell), 0 = automatic
+    int gradient_dirs = 0;    // gradient launch shape (1, 2, 4: directions per thread; 5, 6: warp per cell;
+                              // 7, 8: shared-memory tiles), 0 = automatic
+    int residual_form = 0;    // residual launch shape (1: thread per cell; 5, 6: warp per cell; 7, 8: tiles),
+                              // 0 = automatic
     int adjoint_anderson = 6; // history of the adjoint's Anderson acceleration (0: plain iteration)
     int direction_batch = 0;  // most directions per transport batch, 0 = automatic
     std::vector<double> cell_scatter;  // scattering-rate multiplier s_c per cell (empty: 1)
