@@ -155,6 +155,10 @@ def kernel_algorithmic_bytes(name: str, s: int, dim: int, nb: int, nd: int, nc: 
 NCU_TRAFFIC_PER_UPDATE = {
     ("config2", "fp32"): {"residual": 747.134464e6 / 45921280, "sweep": 392.428032e6 / 45921280,
                           "gradient": 509.03552e6 / 45921280, "moments": 517.57696e6 / 45921280},
+    # the 3D block's figures from its h = 5 nm, 100 nm tall piece (48,000 tets,
+    # 2.4576e8 updates per launch); traffic grows with the updates processed
+    ("config3", "fp32"): {"residual": 7.309474e9 / 245760000, "sweep": 2.267558e9 / 245760000,
+                          "gradient": 4.733219e9 / 245760000, "moments": 2.928845e9 / 245760000},
 }
 
 
