@@ -3914,9 +3914,16 @@ Error Solver::solve_t(SolveStats &st) {
         const size_t nbe = (size_t)nbt * nc * nb;
         ev.gd0 = d0;
         if (nb % 4 == 0) {
+            // the residual candidates are timed on the batch's first 16
+            // directions when those alone hold millions of (direction, cell)
+            // items, enough to fill the GPU; the chosen form then runs on the
+            // whole batch. The gradient's are timed on the whole batch: its
+            // tiled forms spread a per-block setup over the directions, which
+            // a subset would overweight.
+            const int ntune = (size_t)nc * 16 >= 2000000 ? std::min(nbt, 16) : nbt;
             if (cfg.order == 2 && gtune && nt == 0 && d0 == dlo) {
                 // directions per gradient thread: each candidate timed twice
-                // on this batch (they write the same bits to g)
+                // (they write the same bits to g)
                 cudaEvent_t t0, t1;
                 CUDA_TRY(cudaEventCreate(&t0));
                 CUDA_TRY(cudaEventCreate(&t1));
@@ -3935,6 +3942,7 @@ Error Solver::solve_t(SolveStats &st) {
                         float m = 0;
                         CUDA_TRY(cudaEventElapsedTime(&m, t0, t1));
                         if (m < best) best = m, best_dg = dg;
+                        if (m > 1.5f * best) break;  // a clear loser: one run is enough
                     }
                 }
                 cudaEventDestroy(t0);
@@ -3948,8 +3956,8 @@ Error Solver::solve_t(SolveStats &st) {
                 GL(K_GRADIENT, (k_limit<DIM><<<grid_for(nbe), kThreads, 0, s>>>(dm_, dp_, (const double *)eps, eb_,
                                                                                (double *)g, d0, nbt)));
             if (rtune && nt == 0 && d0 == dlo) {
-                // the residual's launch shape: each candidate timed twice on
-                // this batch (they write the same bits to R)
+                // the residual's launch shape: each candidate timed twice
+                // (they write the same bits to R)
                 cudaEvent_t t0, t1;
                 CUDA_TRY(cudaEventCreate(&t0));
                 CUDA_TRY(cudaEventCreate(&t1));
@@ -3961,12 +3969,13 @@ Error Solver::solve_t(SolveStats &st) {
                     if (form >= 7 && !rtile_shape(form, nbc_, thr_, sm_)) continue;
                     for (int rep = 0; rep < 2; rep++) {
                         CUDA_TRY(cudaEventRecord(t0, s));
-                        CUDA_TRY(launch_res(form, d0, nbt));
+                        CUDA_TRY(launch_res(form, d0, ntune));
                         CUDA_TRY(cudaEventRecord(t1, s));
                         CUDA_TRY(cudaEventSynchronize(t1));
                         float m = 0;
                         CUDA_TRY(cudaEventElapsedTime(&m, t0, t1));
                         if (m < best) best = m, best_form = form;
+                        if (m > 1.5f * best) break;
                     }
                 }
                 cudaEventDestroy(t0);
@@ -3996,6 +4005,9 @@ Error Solver::solve_t(SolveStats &st) {
             cudaEvent_t t0, t1;
             CUDA_TRY(cudaEventCreate(&t0));
             CUDA_TRY(cudaEventCreate(&t1));
+            // each trial runs twice unless its first run is already 1.5x the
+            // best so far (the whole batch: the sweep's parallelism is its
+            // directions, so a subset would rank the shapes differently)
             auto trial = [&](const SweepLaunch &L, float &ms) -> Error {
                 ms = 1e30f;
                 for (int rep = 0; rep < 2; rep++) {
@@ -4006,6 +4018,7 @@ Error Solver::solve_t(SolveStats &st) {
                     float m = 0;
                     CUDA_TRY(cudaEventElapsedTime(&m, t0, t1));
                     ms = std::min(ms, m);
+                    if (ms > 1.5f * best) break;
                 }
                 return {0, ""};
             };
