@@ -7,7 +7,9 @@
 // Relative file names are resolved against the deck directory, which plays
 // the role of the reference's working directory. Failures return an Error
 // instead of exiting.
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <fstream>
 #include <sstream>
 
@@ -209,6 +211,192 @@ Error read_msh(std::ifstream &in, int dim, double Lx, double Ly, double Lz, RawM
     return {0, ""};
 }
 
+// ---- band tables from first-principles mode lists (BTEBand.cpp:81-737) ----
+//
+// Both readers reduce a list of phonon modes (capacity C, |v|, kappa
+// contribution k), in the order the files give them, to nb bands of equal
+// mode count: with m = (number of modes) / nb (integer division), mode j goes
+// to band min(j / m, nb - 1), so the last band takes the remainder. Per band
+// the sums run in mode order: v = sum C v / sum C, C = sum C,
+// tau = sum k / C / v / v, then lattice_ratio = (C / tau) / sum_b (C / tau)
+// and heat_ratio = C / sum_b C (BTEBand.cpp:568-613, :691-724).
+struct Mode {
+    double C, v, k;
+};
+
+Error bin_modes(const std::vector<Mode> &modes, int nb, double *v, double *tau, double *C, double *lat,
+                double *hr, const std::string &what) {
+    const int n = (int)modes.size();
+    const int per = n / nb;
+    std::vector<double> sC(nb, 0.0), sCv(nb, 0.0), sk(nb, 0.0);
+    for (int j = 0; j < n; j++) {
+        const int b = per > 0 ? std::min(j / per, nb - 1) : nb - 1;
+        sC[b] += modes[j].C;
+        sCv[b] += modes[j].C * modes[j].v;
+        sk[b] += modes[j].k;
+    }
+    double sumL = 0, sumheat = 0;
+    for (int b = 0; b < nb; b++) {
+        v[b] = sCv[b] / sC[b];
+        C[b] = sC[b];
+        tau[b] = sk[b] / C[b] / v[b] / v[b];
+        sumL += C[b] / tau[b];
+        sumheat += C[b];
+    }
+    for (int b = 0; b < nb; b++) {
+        lat[b] = C[b] / tau[b] / sumL;
+        hr[b] = C[b] / sumheat;
+        if (!std::isfinite(v[b]) || !std::isfinite(tau[b]) || !std::isfinite(lat[b]))
+            return {-2, what + ": band " + std::to_string(b + 1) + " has no modes with a finite capacity"};
+    }
+    return {0, ""};
+}
+
+// whitespace-separated numbers of one line (NaN and inf as strtod reads them)
+std::vector<double> numbers(const std::string &line) {
+    std::vector<double> out;
+    const char *p = line.c_str();
+    while (*p) {
+        while (*p == ' ' || *p == '\t' || *p == '\r') p++;
+        if (!*p) break;
+        char *end = nullptr;
+        const double x = std::strtod(p, &end);
+        if (end == p) break;
+        out.push_back(x);
+        p = end;
+    }
+    return out;
+}
+
+// rows of numbers until the first line of at most one character
+std::vector<std::vector<double>> number_rows(std::ifstream &f) {
+    std::vector<std::vector<double>> rows;
+    std::string line;
+    while (std::getline(f, line)) {
+        if (line.length() <= 1) break;
+        rows.push_back(numbers(line));
+    }
+    return rows;
+}
+
+// ALAMODE lifetime file (BTEBand.cpp:629-731): after the "Phonon lifetime"
+// line, "# kpoint range k0 k1" and "# mode range b0 b1", a header line, then
+// one line per (k-point, branch): ik, is, frequency [cm^-1], lifetime [ps],
+// |v| [m/s], MFP, multiplicity and the nine per-mode conductivity tensor
+// entries xx .. zz. kappa = (xx + yy + zz) multiplicity,
+// C = kappa / v / v / tau (0 where tau or v is 0). `key_len` is the length of
+// the PHONON line that named the file: the reference accepts the
+// "Phonon lifetime" line only where the phrase starts before that column.
+Error read_alamode(const std::string &path, int nb, size_t key_len, double *v, double *tau, double *C,
+                   double *lat, double *hr) {
+    std::ifstream f(path);
+    if (!f.is_open()) return {-2, "ALAMODE band file not open: " + path};
+    std::string line;
+    while (std::getline(f, line)) {
+        const size_t at = line.find("Phonon lifetime");
+        if (!(at > 0 && at < key_len)) continue;
+        std::string w1, w2, w3;
+        long k0 = 0, k1 = -1, b0 = 0, b1 = -1;
+        if (!(f >> w1 >> w2 >> w3 >> k0 >> k1 >> w1 >> w2 >> w3 >> b0 >> b1))
+            return {-2, "ALAMODE: missing kpoint/mode ranges: " + path};
+        std::getline(f, line);
+        std::getline(f, line);
+        const long n = (b1 - b0 + 1) * (k1 - k0 + 1);
+        if (n <= 0) return {-2, "ALAMODE: empty mode range: " + path};
+        std::vector<Mode> modes((size_t)n);
+        for (long j = 0; j < n; j++) {
+            double iq, ib, freq, t, vel, mfp, mult, k[9];
+            if (!(f >> iq >> ib >> freq >> t >> vel >> mfp >> mult)) return {-2, "ALAMODE: truncated mode list: " + path};
+            for (double &x : k)
+                if (!(f >> x)) return {-2, "ALAMODE: truncated mode list: " + path};
+            Mode &m = modes[(size_t)j];
+            t *= 1e-12;
+            m.v = vel;
+            m.k = (k[0] + k[4] + k[8]) * mult;
+            m.C = (t == 0 || vel == 0) ? 0.0 : m.k / vel / vel / t;
+        }
+        return bin_modes(modes, nb, v, tau, C, lat, hr, "ALAMODE " + path);
+    }
+    return {-2, "ALAMODE: no \"Phonon lifetime\" section: " + path};
+}
+
+// ShengBTE output directory (BTEBand.cpp:81-617): CONTROL gives lfactor
+// [nm], the three lattice vectors and T; BTE.omega the frequencies [rad/ps]
+// per irreducible q-point (row) and branch (column); BTE.qpoints_full the
+// full grid (second column: the irreducible q-point, 1-based); BTE.w_final
+// and BTE.v one row per (branch, irreducible q-point), branch-major: the
+// scattering rate [1/ps] in column 2 and the group velocity [km/s]. Per
+// full-grid mode: C = (1/V) kB x^2 e^x / (e^x - 1)^2 / Nq with
+// x = hbar omega / (kB T), tau = 1 / w, kappa = C v^2 tau, taken branch by
+// branch over the full grid, skipping modes whose kappa is NaN or negative.
+// As in the reference: V is formed with lattvec(1,2) in place of
+// lattvec(2,1) in one term of the determinant, kB = 1.38062e-23 and
+// hbar = 1.05459e-34, and T comes from the last CONTROL line holding an
+// upper-case T past its first column and neither TRUE nor True.
+Error read_shengbte(const std::string &dir, int nb, double *v, double *tau, double *C, double *lat, double *hr) {
+    std::ifstream ctl(dir + "/CONTROL");
+    if (!ctl.is_open()) return {-2, "ShengBTE CONTROL file not open: " + dir};
+    double lf = 1.0, T = 0, a[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    std::string line;
+    auto after_eq = [](const std::string &l) { return l.substr(l.find('=') + 1); };
+    while (std::getline(ctl, line)) {
+        const size_t at_lf = line.find("lfactor");
+        if (at_lf > 0 && at_lf != std::string::npos) lf = std::strtod(after_eq(line).c_str(), nullptr);
+        for (int r = 0; r < 3; r++) {
+            const std::string key = "lattvec(:," + std::to_string(r + 1) + ")";
+            const size_t at = line.find(key);
+            if (at > 0 && at != std::string::npos) {
+                const std::vector<double> x = numbers(after_eq(line));
+                for (int c = 0; c < 3 && c < (int)x.size(); c++) a[r][c] = x[c];
+            }
+        }
+        const size_t at_t = line.find('T');
+        if (at_t > 0 && at_t != std::string::npos) {
+            const std::string rest = after_eq(line);
+            if (rest.find("TRUE") == std::string::npos && rest.find("True") == std::string::npos)
+                T = std::strtod(rest.c_str(), nullptr);
+        }
+    }
+    double V = (a[0][0] * a[1][1] * a[2][2] + a[1][0] * a[2][1] * a[0][2] + a[0][1] * a[1][2] * a[2][0] -
+                a[0][2] * a[1][1] * a[2][0] - a[0][1] * a[0][1] * a[2][2] - a[0][0] * a[1][2] * a[2][1]) *
+               lf * lf * lf;
+    V = std::fabs(V) * 1e-27;
+    if (!(T > 0) || !(V > 0)) return {-2, "ShengBTE CONTROL: no temperature or cell volume: " + dir};
+    std::vector<std::vector<double>> om, qf, wf, vf;
+    for (auto &p : {std::make_pair("/BTE.omega", &om), std::make_pair("/BTE.qpoints_full", &qf),
+                    std::make_pair("/BTE.w_final", &wf), std::make_pair("/BTE.v", &vf)}) {
+        std::ifstream g(dir + p.first);
+        if (!g.is_open()) return {-2, std::string("ShengBTE file not open: ") + dir + p.first};
+        *p.second = number_rows(g);
+    }
+    const int nirr = (int)om.size(), nq = (int)qf.size();
+    if (nirr == 0 || nq == 0) return {-2, "ShengBTE: empty BTE.omega or BTE.qpoints_full: " + dir};
+    const int nbr = (int)om.back().size();  // branches: the count of the last row
+    const double kb = 1.38062e-23, hbar = 1.05459e-34;
+    std::vector<Mode> modes;
+    for (int br = 0; br < nbr; br++)
+        for (int q = 0; q < nq; q++) {
+            if (qf[q].size() < 2) return {-2, "ShengBTE: short BTE.qpoints_full row: " + dir};
+            const int irr = (int)qf[q][1] - 1;
+            const size_t row = (size_t)br * nirr + irr;
+            if (irr < 0 || irr >= nirr || (int)om[irr].size() <= br || row >= wf.size() || row >= vf.size() ||
+                wf[row].size() < 2 || vf[row].size() < 3)
+                return {-2, "ShengBTE: q-point or branch outside the files: " + dir};
+            const double w = om[irr][br] * 1e12;
+            const double t = 1 / wf[row][1] * 1e-12;
+            const double vel = std::pow(std::pow(vf[row][0] * 1000, 2) + std::pow(vf[row][1] * 1000, 2) +
+                                            std::pow(vf[row][2] * 1000, 2),
+                                        0.5);
+            const double x = hbar * w / kb / T;
+            const double cap = 1 / V * kb * x * x * std::exp(x) / std::pow(std::exp(x) - 1, 2);
+            const double k = cap / nq * vel * vel * t;
+            if (std::isnan(k) || !(k >= 0)) continue;
+            modes.push_back({cap / nq, vel, k});
+        }
+    if (modes.empty()) return {-2, "ShengBTE: no mode with a finite conductivity: " + dir};
+    return bin_modes(modes, nb, v, tau, C, lat, hr, "ShengBTE " + dir);
+}
+
 }  // namespace
 
 Error read_deck(const std::string &root, Deck &D) {
@@ -286,14 +474,28 @@ Error read_deck(const std::string &root, Deck &D) {
             bool got = false;
             while (std::getline(g, str)) {
                 if (!has_word(str, "MaterialFile")) continue;
-                if (!has_word(str, "DATABASE")) return {-8, "only DATABASE material files are supported"};
+                // the source named on the line, in the reference's order of
+                // tests: DATABASE, ShengBTE, ALAMODE (BTEBand.cpp:60-81, :629)
+                const size_t at_db = str.find("DATABASE"), at_sh = str.find("ShengBTE"), at_al = str.find("ALAMODE");
                 std::string file;
                 g >> file;
-                std::ifstream t(resolve(root, file));
-                if (!t.is_open()) return {-2, "DATABASE band file not open: " + file};
-                for (int j = 0; j < nb; j++)
-                    if (!(t >> B.v[i * nb + j] >> B.tau[i * nb + j] >> B.C[i * nb + j] >> B.lat[i * nb + j] >> B.hr[i * nb + j]))
-                        return {-2, "DATABASE band file too short: " + file};
+                double *bv = &B.v[i * nb], *bt = &B.tau[i * nb], *bc = &B.C[i * nb], *bl = &B.lat[i * nb],
+                       *bh = &B.hr[i * nb];
+                if (at_db > 0 && at_db != std::string::npos) {
+                    std::ifstream t(resolve(root, file));
+                    if (!t.is_open()) return {-2, "DATABASE band file not open: " + file};
+                    for (int j = 0; j < nb; j++)
+                        if (!(t >> bv[j] >> bt[j] >> bc[j] >> bl[j] >> bh[j]))
+                            return {-2, "DATABASE band file too short: " + file};
+                } else if (at_sh > 0 && at_sh != std::string::npos) {
+                    Error e = read_shengbte(resolve(root, file), nb, bv, bt, bc, bl, bh);
+                    if (e.code) return e;
+                } else if (at_al > 0 && at_al != std::string::npos) {
+                    Error e = read_alamode(resolve(root, file), nb, str.length(), bv, bt, bc, bl, bh);
+                    if (e.code) return e;
+                } else {
+                    return {-8, "MaterialFile: unknown source (DATABASE, ShengBTE or ALAMODE)"};
+                }
                 got = true;
                 break;
             }

@@ -22,6 +22,7 @@ File formats follow the readers of the reference:
 from __future__ import annotations
 
 import dataclasses
+import math
 import os
 from typing import Dict, List, Optional, Sequence, Tuple
 
@@ -378,6 +379,238 @@ def sine_dispersion_bands(n_bands: int, T: float = 300.0, kmax: float = 1.1e10,
 
 
 # ----------------------------------------------------------------------------
+# first-principles mode lists (ALAMODE lifetime files, ShengBTE outputs)
+# ----------------------------------------------------------------------------
+def _div(a: float, b: float) -> float:
+    """a / b with IEEE semantics where Python raises (b == 0)."""
+    if b != 0.0:
+        return a / b
+    if a != a or a == 0.0:
+        return math.nan
+    return math.copysign(math.inf, a) * math.copysign(1.0, b)
+
+
+def bin_modes(C: Sequence[float], v: Sequence[float], k: Sequence[float], n_bands: int) -> BandTable:
+    """A mode list (capacity C, |v|, conductivity contribution k, in file
+    order) reduced to n_bands bands of equal mode count, the last taking the
+    remainder, as the reference's readers do (src/BTEBand/BTEBand.cpp:568-613,
+    :691-724): v = sum C v / sum C, C = sum C, tau = sum k / C / v / v,
+    lattice_ratio = (C / tau) / sum (C / tau), heat_ratio = C / sum C. The
+    sums run mode by mode in file order (plain float arithmetic, so the table
+    is the C++ reader's to the last bit)."""
+    n = len(C)
+    per = n // n_bands
+    sC = [0.0] * n_bands
+    sCv = [0.0] * n_bands
+    sk = [0.0] * n_bands
+    for j in range(n):
+        b = min(j // per, n_bands - 1) if per > 0 else n_bands - 1
+        sC[b] += float(C[j])
+        sCv[b] += float(C[j]) * float(v[j])
+        sk[b] += float(k[j])
+    vb, tb, cb = [], [], []
+    sumL = sumheat = 0.0
+    for b in range(n_bands):
+        vv = _div(sCv[b], sC[b])
+        cc = sC[b]
+        tt = _div(_div(_div(sk[b], cc), vv), vv)
+        vb.append(vv)
+        cb.append(cc)
+        tb.append(tt)
+        sumL += _div(cc, tt)
+        sumheat += cc
+    lat = [_div(_div(cb[b], tb[b]), sumL) for b in range(n_bands)]
+    hr = [_div(cb[b], sumheat) for b in range(n_bands)]
+    return BandTable(v=np.array(vb), tau=np.array(tb), C=np.array(cb), lattice_ratio=np.array(lat),
+                     heat_ratio=np.array(hr))
+
+
+@dataclasses.dataclass
+class AlamodeModes:
+    """An ALAMODE lifetime file (`anphon` result analyser output): per
+    (k-point, branch) the frequency [cm^-1], lifetime [ps], |v| [m/s], MFP
+    [nm], multiplicity and the per-mode conductivity tensor xx .. zz
+    [W/mK]."""
+
+    freq: np.ndarray     # (nk, nbr)
+    tau_ps: np.ndarray   # (nk, nbr)
+    vel: np.ndarray      # (nk, nbr)
+    mfp: np.ndarray      # (nk, nbr)
+    mult: np.ndarray     # (nk,) integers
+    kappa: np.ndarray    # (nk, nbr, 9)
+    seed: Optional[int] = None  # synthetic_alamode's seed, when it made them
+
+    def write(self, path: str) -> None:
+        nk, nbr = self.freq.shape
+        with open(path, "w") as f:
+            f.write("# Result analyzer ver. 1.0.5\n# Input file : synthetic.result\n")
+            f.write("# Phonon lifetime at temperature 300 K.\n")
+            f.write(f"# kpoint range 1 {nk}\n# mode   range 1 {nbr}\n")
+            f.write("#  ik,  is, Frequency [cm^{-1}], Lifetime [ps], |Velocity| [m/s], MFP [nm], Multiplicity, "
+                    "Thermal conductivity par mode (xx, xy, ...) [W/mK]\n")
+            for i in range(nk):
+                for b in range(nbr):
+                    f.write("%5d %4d %.17g %.17g %.17g %.17g %d %s\n" % (
+                        i + 1, b + 1, self.freq[i, b], self.tau_ps[i, b], self.vel[i, b], self.mfp[i, b],
+                        int(self.mult[i]), " ".join("%.17g" % x for x in self.kappa[i, b])))
+
+    def band_table(self, n_bands: int) -> BandTable:
+        """The reference's reduction (BTEBand.cpp:629-731): kappa = (xx + yy
+        + zz) multiplicity, C = kappa / v / v / tau (0 where tau or v is 0)."""
+        nk, nbr = self.freq.shape
+        C, v, k = [], [], []
+        for i in range(nk):
+            for b in range(nbr):
+                t = float(self.tau_ps[i, b]) * 1e-12
+                vel = float(self.vel[i, b])
+                kap = (float(self.kappa[i, b, 0]) + float(self.kappa[i, b, 4]) + float(self.kappa[i, b, 8])) \
+                    * float(self.mult[i])
+                C.append(0.0 if (t == 0.0 or vel == 0.0) else kap / vel / vel / t)
+                v.append(vel)
+                k.append(kap)
+        return bin_modes(C, v, k, n_bands)
+
+
+def synthetic_alamode(nk: int = 203, nbr: int = 6, seed: int = 0) -> AlamodeModes:
+    """Seeded synthetic modes in the ALAMODE layout: three acoustic and
+    nbr - 3 optical branches, the first k-point's acoustic modes at zero
+    frequency, lifetime and velocity (as at Gamma), the conductivity tensor
+    nearly isotropic with small off-diagonal terms."""
+    rng = np.random.default_rng(seed)
+    kk = (np.arange(nk) + 0.5) / nk
+    freq = np.zeros((nk, nbr))
+    for b in range(nbr):
+        top = 150.0 + 70.0 * b if b < 3 else 400.0 + 15.0 * b
+        freq[:, b] = top * (np.sin(0.5 * np.pi * kk) if b < 3 else 1.0 - 0.1 * kk) * rng.uniform(0.97, 1.03, nk)
+    tau_ps = np.exp(rng.uniform(np.log(0.5), np.log(300.0), (nk, nbr)))
+    vel = rng.uniform(300.0, 9000.0, (nk, nbr))
+    mult = rng.choice([1, 2, 4, 6, 8, 12, 24, 48], nk)
+    cmode = rng.uniform(20.0, 400.0, (nk, nbr))
+    kappa = np.zeros((nk, nbr, 9))
+    for i in range(9):
+        kappa[:, :, i] = cmode * vel ** 2 * tau_ps * 1e-12 / 3.0 / mult[:, None] * (
+            rng.uniform(0.9, 1.1, (nk, nbr)) if i in (0, 4, 8) else rng.uniform(-1e-3, 1e-3, (nk, nbr)))
+    freq[0, :3] = 1e-10
+    tau_ps[0, :3] = 0.0
+    vel[0, :3] = 0.0
+    kappa[0, :3, :] = 0.0
+    mfp = vel * tau_ps * 1e-3
+    return AlamodeModes(freq=freq, tau_ps=tau_ps, vel=vel, mfp=mfp, mult=mult, kappa=kappa, seed=seed)
+
+
+# the constants of the reference's ShengBTE reader (BTEBand.cpp:521-523)
+SHENGBTE_KB = 1.38062e-23
+SHENGBTE_HBAR = 1.05459e-34
+
+
+@dataclasses.dataclass
+class ShengBTEData:
+    """A ShengBTE output directory: CONTROL (lfactor [nm], lattice vectors,
+    T), BTE.omega (irreducible q-points x branches, rad/ps),
+    BTE.qpoints_full (full grid: index, irreducible index, coordinates),
+    BTE.w_final and BTE.v (one row per branch and irreducible q-point,
+    branch-major: frequency and scattering rate [1/ps]; velocity [km/s])."""
+
+    lfactor: float
+    lattvec: np.ndarray   # (3, 3), row r = lattvec(:, r + 1)
+    T: float
+    omega: np.ndarray     # (nirr, nbr)
+    q_irr: np.ndarray     # (nq,) 1-based irreducible index of each full-grid point
+    q_xyz: np.ndarray     # (nq, 3)
+    w: np.ndarray         # (nbr * nirr,) scattering rates
+    v: np.ndarray         # (nbr * nirr, 3)
+    seed: Optional[int] = None  # synthetic_shengbte's seed, when it made them
+
+    def write(self, directory: str) -> None:
+        os.makedirs(directory, exist_ok=True)
+        a = self.lattvec
+        with open(os.path.join(directory, "CONTROL"), "w") as f:
+            f.write("&allocations\n        nelements=1,\n        natoms=2,\n        ngrid(:)=5 5 5\n&end\n")
+            f.write("&crystal\n        lfactor=%.17g,\n" % self.lfactor)
+            for r in range(3):
+                f.write("        lattvec(:,%d)= %.17g %.17g %.17g\n" % (r + 1, a[r, 0], a[r, 1], a[r, 2]))
+            f.write('        elements="Xx"\n        types=1 1,\n&end\n')
+            f.write("&parameters\n        T=%.17g\n        scalebroad=1\n&end\n" % self.T)
+            f.write("&flags\n        convergence=.TRUE.\n        isotopes=.true.\n&end\n")
+        nirr, nbr = self.omega.shape
+        with open(os.path.join(directory, "BTE.omega"), "w") as f:
+            for i in range(nirr):
+                f.write(" ".join("%.17g" % x for x in self.omega[i]) + "\n")
+        with open(os.path.join(directory, "BTE.qpoints_full"), "w") as f:
+            for q in range(len(self.q_irr)):
+                f.write("%d %d %.17g %.17g %.17g\n" % (q + 1, int(self.q_irr[q]), *self.q_xyz[q]))
+        with open(os.path.join(directory, "BTE.w_final"), "w") as f:
+            for r in range(nbr * nirr):
+                f.write("%.17g %s\n" % (self.omega[r % nirr, r // nirr],
+                                         "NaN" if self.w[r] != self.w[r] else "%.17g" % self.w[r]))
+        with open(os.path.join(directory, "BTE.v"), "w") as f:
+            for r in range(nbr * nirr):
+                f.write("%.17g %.17g %.17g\n" % tuple(self.v[r]))
+
+    def cell_volume(self) -> float:
+        """The reference's cell volume (BTEBand.cpp:296), lattvec(1,2) in
+        place of lattvec(2,1) in one term, times lfactor^3 and 1e-27."""
+        a = [[float(x) for x in row] for row in self.lattvec]
+        lf = float(self.lfactor)
+        vol = (a[0][0] * a[1][1] * a[2][2] + a[1][0] * a[2][1] * a[0][2] + a[0][1] * a[1][2] * a[2][0]
+               - a[0][2] * a[1][1] * a[2][0] - a[0][1] * a[0][1] * a[2][2] - a[0][0] * a[1][2] * a[2][1]) \
+            * lf * lf * lf
+        return abs(vol) * 1e-27
+
+    def band_table(self, n_bands: int) -> BandTable:
+        """The reference's reduction (BTEBand.cpp:506-613): per full-grid mode,
+        branch by branch, C = (1/V) kB x^2 e^x / (e^x - 1)^2 / Nq with
+        x = hbar omega / (kB T), tau = 1 / w, k = C v^2 tau; modes whose k is
+        NaN or negative are dropped."""
+        nirr, nbr = self.omega.shape
+        nq = len(self.q_irr)
+        V = self.cell_volume()
+        T = float(self.T)
+        C, v, k = [], [], []
+        for b in range(nbr):
+            for q in range(nq):
+                irr = int(self.q_irr[q]) - 1
+                row = b * nirr + irr
+                om = float(self.omega[irr, b]) * 1e12
+                t = _div(1.0, float(self.w[row])) * 1e-12
+                vx, vy, vz = (float(x) * 1000 for x in self.v[row])
+                vel = math.pow(math.pow(vx, 2) + math.pow(vy, 2) + math.pow(vz, 2), 0.5)
+                x = SHENGBTE_HBAR * om / SHENGBTE_KB / T
+                ex = math.exp(x)
+                cap = _div(1 / V * SHENGBTE_KB * x * x * ex, math.pow(ex - 1, 2))
+                kk = cap / nq * vel * vel * t
+                if kk != kk or not kk >= 0:
+                    continue
+                C.append(cap / nq)
+                v.append(vel)
+                k.append(kk)
+        return bin_modes(C, v, k, n_bands)
+
+
+def synthetic_shengbte(nirr: int = 40, nq: int = 150, nbr: int = 6, seed: int = 1) -> ShengBTEData:
+    """Seeded synthetic ShengBTE outputs: a skewed cell (so the reference's
+    volume quirk matters), the first irreducible point at zero frequency with
+    a NaN rate (Gamma), one negative rate (its modes drop out), and every
+    full-grid point mapped to an irreducible one."""
+    rng = np.random.default_rng(seed)
+    lattvec = np.array([[0.0, 0.30, 0.28], [0.26, 0.0, 0.29], [0.27, 0.31, 0.0]]) * 10.0
+    kk = (np.arange(nirr) + 0.5) / nirr
+    omega = np.zeros((nirr, nbr))
+    for b in range(nbr):
+        top = 15.0 + 8.0 * b if b < 3 else 50.0 + 2.0 * b
+        omega[:, b] = top * (np.sin(0.5 * np.pi * kk) if b < 3 else 1.0 - 0.1 * kk) * rng.uniform(0.97, 1.03, nirr)
+    omega[0, :] = 0.0
+    w = np.exp(rng.uniform(np.log(1e-3), np.log(2.0), nbr * nirr))
+    w[[b * nirr for b in range(nbr)]] = np.nan
+    w[nirr + 7] = -w[nirr + 7]
+    v = rng.uniform(-8.0, 8.0, (nbr * nirr, 3))
+    q_irr = np.concatenate([[1], rng.integers(1, nirr + 1, nq - 1)])
+    q_xyz = rng.uniform(-0.5, 0.5, (nq, 3))
+    return ShengBTEData(lfactor=0.1, lattvec=lattvec, T=300.0, omega=omega, q_irr=q_irr, q_xyz=q_xyz, w=w, v=v,
+                        seed=seed)
+
+
+# ----------------------------------------------------------------------------
 # writers
 # ----------------------------------------------------------------------------
 def write_mphtxt(path: str, mesh: Mesh2D) -> None:
@@ -531,6 +764,11 @@ class Deck:
     # (0-based; None: every region is material 0)
     extra_materials: List[BandTable] = dataclasses.field(default_factory=list)
     region_material: Optional[List[int]] = None
+    # where each material's bands come from in the written deck: None (or a
+    # None entry) writes the band table as a DATABASE file; an AlamodeModes
+    # or ShengBTEData entry writes that mode list instead (MaterialFile
+    # ALAMODE / ShengBTE), whose reduction the material's BandTable must be
+    material_sources: Optional[List[object]] = None
 
     @property
     def materials(self) -> List[BandTable]:
@@ -570,11 +808,21 @@ class Deck:
             write_mphtxt(os.path.join(d, mesh_name), self.mesh)
         else:
             write_msh41(os.path.join(d, mesh_name), self.mesh)
-        band_files = []
+        band_files = []  # (PHONON source keyword, path under input/)
         for k, bt in enumerate(self.materials):
-            name = "bands.dat" if k == 0 else f"bands_{k + 1}.dat"
-            write_band_database(os.path.join(d, name), bt)
-            band_files.append(name)
+            src = self.material_sources[k] if self.material_sources and k < len(self.material_sources) else None
+            if isinstance(src, AlamodeModes):
+                name = f"alamode_{k + 1}.dat"
+                src.write(os.path.join(d, name))
+                band_files.append(("ALAMODE", name))
+            elif isinstance(src, ShengBTEData):
+                name = f"shengbte_{k + 1}"
+                src.write(os.path.join(d, name))
+                band_files.append(("ShengBTE", name))
+            else:
+                name = "bands.dat" if k == 0 else f"bands_{k + 1}.dat"
+                write_band_database(os.path.join(d, name), bt)
+                band_files.append(("DATABASE", name))
         with open(os.path.join(d, "bc.dat"), "w") as f:
             f.write(f"{len(self.bcs)} #Number of boundaries\n\n")
             f.write("BoundaryIndex BoundaryType BoundaryValue\n")
@@ -608,8 +856,8 @@ class Deck:
         rm = self.region_materials()
         with open(os.path.join(d, "PHONON"), "w") as f:
             f.write("MaterialNumber=\n%d\nBandNumber=\n%d\n\n" % (len(band_files), self.bands.n_bands))
-            for k, name in enumerate(band_files):
-                f.write("MaterialFile %d= DATABASE\ninput/%s\n\n" % (k + 1, name))
+            for k, (kind, name) in enumerate(band_files):
+                f.write("MaterialFile %d:  %s\ninput/%s\n\n" % (k + 1, kind, name))
             f.write("GeometryMaterialType=\n%s\n\nMaterialDimension=\n%d\nAngle_method=\n%d\n"
                     "Ntheta=\n%d\nNphi=\n%d\n"
                     % ("\n".join(f"{r + 1} {rm[r] + 1}" for r in range(self.n_regions)),
@@ -655,6 +903,25 @@ def interface_deck(n: int = 16, n_bands: int = 4, n_phi: int = 4, **kw) -> Deck:
     kw.setdefault("tref", 300.0)
     return Deck(mesh=two_region_tri_mesh(n, n), bands=left, bcs=bcs, scale=(1e-7, 1e-7),
                 extra_materials=[right], region_material=[0, 1], **kw)
+
+
+def mode_list_deck(kind: str, n: int = 12, n_bands: int = 12, seed: int = 0, **kw) -> Deck:
+    """A 100 nm square (n x n squares split into triangles) whose one
+    material's bands come from a seeded synthetic mode list in the
+    ALAMODE or ShengBTE layout (kind), reduced to n_bands bands; left 301 K,
+    right 299 K isothermal, top and bottom diffuse."""
+    if kind == "ALAMODE":
+        src = synthetic_alamode(seed=seed)
+    elif kind == "ShengBTE":
+        src = synthetic_shengbte(seed=seed)
+    else:
+        raise ValueError("kind must be ALAMODE or ShengBTE")
+    bcs = [BC(1, 1, 301.0), BC(2, 1, 299.0), BC(3, 2, 0.0), BC(4, 2, 0.0)]
+    kw.setdefault("n_phi", 4)
+    kw.setdefault("angle_method", 1)
+    kw.setdefault("tref", 300.0)
+    return Deck(mesh=square_tri_mesh(n, n), bands=src.band_table(n_bands), bcs=bcs, scale=(1e-7, 1e-7),
+                material_sources=[src], **kw)
 
 
 def config1_deck(n: int = 40, **kw) -> Deck:

@@ -89,6 +89,11 @@ def cases():
         scale=(3e-7, 3e-7), material_dim=2, angle_method=2, n_phi=4, tref=0.0, order="2limit")
     # 9. two materials meeting at an interface wall (BC type 5)
     out["interface_2mat"] = decks.interface_deck(16)
+    # 10.-11. bands reduced from first-principles mode lists in the ALAMODE
+    #    and ShengBTE layouts (seeded synthetic modes, MaterialFile ALAMODE /
+    #    ShengBTE): the reference's own readers make the band tables
+    out["alamode_square"] = decks.mode_list_deck("ALAMODE", 12)
+    out["shengbte_square"] = decks.mode_list_deck("ShengBTE", 12)
     out["quad_firstorder_sequential"] = decks.Deck(
         mesh=decks.square_quad_mesh(16, 16), bands=decks.sine_dispersion_bands(2),
         bcs=[decks.BC(1, 1, 300.0), decks.BC(2, 1, 300.0), decks.BC(3, 3, 0.0), decks.BC(4, 3, 0.0)],
@@ -114,7 +119,11 @@ def deck_params(d: decks.Deck) -> dict:
             "extra_materials": [{k: np.asarray(getattr(m, k)).tolist()
                                  for k in ("v", "tau", "C", "lattice_ratio", "heat_ratio")}
                                 for m in d.extra_materials],
-            "region_material": d.region_material}
+            "region_material": d.region_material,
+            "material_sources": [None if src is None else
+                                 {"kind": "ALAMODE" if isinstance(src, decks.AlamodeModes) else "ShengBTE",
+                                  "seed": src.seed}
+                                 for src in (d.material_sources or [])]}
 
 
 # The benchmarked 2D workload at full size: the 300 nm porous cell with a
@@ -190,11 +199,20 @@ def load(name: str):
                    mesh_format=p["mesh_format"], order=p.get("order", "2"), scheme=p.get("scheme", "Synthetic"),
                    residual_temp=1e-12, residual_flux=1e-12,
                    max_iter=LIMITER_ITERS if p.get("order") == "2limit" else 3000)
+    srcs = []
+    for m in p.get("material_sources") or []:
+        if m is None:
+            srcs.append(None)
+        elif m["kind"] == "ALAMODE":
+            srcs.append(decks.synthetic_alamode(seed=m["seed"]))
+        else:
+            srcs.append(decks.synthetic_shengbte(seed=m["seed"]))
+    d.material_sources = srcs or None
     ref = {k: z[k] for k in ("T", "E", "q", "Tband", "xyz", "Tf", "qf", "margins", "bands_kept") if k in z}
     ref["iters"] = int(z["iters"])
     if name in BIG:
         d.max_iter = BIG[name] or 3000
-        d.residual_temp = d.residual_flux = 0.0 if BIG[name] else 1e-10
+        d.residual_temp = d.residual_flux = 0.0 if BIG[name] else 1e-9
     return d, ref
 
 
@@ -203,7 +221,8 @@ def have(name: str) -> bool:
 
 
 CASES = ["gray_square_tri", "quad_heat_specular", "periodic_jitter", "porous_msh", "porous_firstorder",
-         "periodic_sequential", "quad_firstorder_sequential", "porous_limiter", "interface_2mat"]
+         "periodic_sequential", "quad_firstorder_sequential", "porous_limiter", "interface_2mat",
+         "alamode_square", "shengbte_square"]
 # the cases solved to 1e-12 margins (all but the limited one, a fixed count)
 CONVERGED = [c for c in CASES if c != "porous_limiter"]
 # the cases of one material (the CPU restatement and the device Fourier

@@ -166,3 +166,49 @@ def test_index_checks_catch_planted_entries(tmp_path):
     lines = r.stdout.splitlines()
     assert lines[0].startswith("built: pass") and lines[1].startswith("tiles: pass")
     assert sum(": caught" in l for l in lines) == 8 and lines[-1] == "OK"
+
+
+@pytest.mark.parametrize("kind", ["ALAMODE", "ShengBTE"])
+def test_mode_list_band_files_read_on_the_host(kind, tmp_path):
+    # a PHONON that names an ALAMODE lifetime file or a ShengBTE output
+    # directory: the library's reader and the Python restatement of the
+    # reference's reduction give the same band table to the last bit (through
+    # kappa_bulk = sum C v^2 tau / dim and C_bulk = sum C)
+    d = decks.mode_list_deck(kind)
+    d.write(str(tmp_path))
+    a = g.inspect_deck(str(tmp_path))
+    b = g.inspect(d)
+    assert a["num_bands"] == 12
+    assert a["kappa_bulk"] == b["kappa_bulk"] and a["capacity_bulk"] == b["capacity_bulk"]
+    t = d.bands
+    assert b["kappa_bulk"] == pytest.approx(float(np.sum(t.C * t.v ** 2 * t.tau)) / 2, rel=1e-13)
+    assert np.sum(t.lattice_ratio) == pytest.approx(1.0, abs=1e-12)
+    assert np.sum(t.heat_ratio) == pytest.approx(1.0, abs=1e-12)
+
+
+def test_mode_list_reductions_follow_the_reference_rules():
+    # equal mode counts in file order, the last band taking the remainder;
+    # ALAMODE: Gamma's zero modes count as modes of zero capacity; ShengBTE:
+    # NaN and negative-rate modes are dropped before binning
+    a = decks.synthetic_alamode(nk=7, nbr=6, seed=3)
+    t = a.band_table(4)  # 42 modes: 10, 10, 10, 12
+    kap = (a.kappa[..., 0] + a.kappa[..., 4] + a.kappa[..., 8]) * a.mult[:, None]
+    tau = a.tau_ps * 1e-12
+    with np.errstate(divide="ignore", invalid="ignore"):
+        C = np.where((tau == 0) | (a.vel == 0), 0.0, kap / a.vel ** 2 / tau).ravel()
+    assert t.C[0] == pytest.approx(C[:10].sum(), rel=1e-14)
+    assert t.C[3] == pytest.approx(C[30:].sum(), rel=1e-14)
+    s = decks.synthetic_shengbte(nirr=6, nq=20, nbr=3, seed=2)
+    ts = s.band_table(2)
+    assert np.all(np.isfinite(ts.v)) and np.all(ts.C > 0)
+
+
+def test_mode_list_missing_files_are_io_errors(tmp_path):
+    for kind, victim in (("ALAMODE", "input/alamode_1.dat"), ("ShengBTE", "input/shengbte_1/BTE.w_final")):
+        d = decks.mode_list_deck(kind)
+        root = tmp_path / kind
+        d.write(str(root))
+        os.remove(str(root / victim))
+        with pytest.raises(g.GBTEError) as e:
+            g.inspect_deck(str(root))
+        assert e.value.status == -2

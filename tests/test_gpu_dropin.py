@@ -33,7 +33,7 @@ def rel(a, b):
 
 @pytest.mark.parametrize("case", ["gray_square_tri", "quad_heat_specular", "periodic_jitter", "porous_msh",
                                   "porous_firstorder", "periodic_sequential", "quad_firstorder_sequential",
-                                  "porous_limiter", "interface_2mat"])
+                                  "porous_limiter", "interface_2mat", "alamode_square", "shengbte_square"])
 def test_reference_program_with_b200_solver_matches_reference(case, tmp_path):
     # every variant the CONTROL file selects (Order 1/2/2limit, Synthetic or
     # Sequential) goes through its own solve* method of the drop-in class

@@ -94,11 +94,12 @@ def test_fp32_mixed_close_to_reference(case):
 
 
 @pytest.mark.parametrize("case", ["porous_firstorder", "periodic_sequential", "quad_firstorder_sequential",
-                                  "porous_limiter"])
+                                  "porous_limiter", "alamode_square", "shengbte_square"])
 def test_variant_decks_from_files_match_reference(case, tmp_path):
     # Order=1 / 2limit and IterativeScheme=Sequential read from the CONTROL
     # file of a deck directory select the same variants as the in-memory
-    # options
+    # options; ALAMODE and ShengBTE mode lists named in PHONON reduce to the
+    # reference's band tables
     deck, ref = mg.load(case)
     deck.write(str(tmp_path))
     s = StaticBTESynthetic.from_deck_dir(str(tmp_path), precision=GBTE_FP64,
