@@ -115,6 +115,11 @@ class VjpStats(ctypes.Structure):
                 ("vjp_ms", ctypes.c_double), ("residual", ctypes.c_double)]
 
 
+class TransientStats(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_longlong), ("updates", ctypes.c_longlong), ("err_temp", ctypes.c_double),
+                ("err_flux", ctypes.c_double), ("solve_ms", ctypes.c_double)]
+
+
 class DeckInfo(ctypes.Structure):
     _fields_ = [("dimension", ctypes.c_int), ("num_nodes", ctypes.c_int), ("num_cells", ctypes.c_int),
                 ("num_faces", ctypes.c_int), ("num_boundaries", ctypes.c_int),
@@ -125,7 +130,8 @@ class DeckInfo(ctypes.Structure):
                 ("max_iter_or_zero", ctypes.c_double), ("err_temp", ctypes.c_double),
                 ("err_flux", ctypes.c_double), ("max_level_width", ctypes.c_int), ("sweep_ring", ctypes.c_int),
                 ("far_slots", ctypes.c_int), ("far_refs", ctypes.c_longlong),
-                ("index_entries_checked", ctypes.c_longlong)]
+                ("index_entries_checked", ctypes.c_longlong), ("transient", ctypes.c_int),
+                ("time_step", ctypes.c_double), ("total_time", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -135,7 +141,7 @@ EXPORTS = ["gbte_inspect_deck", "gbte_inspect_mesh", "gbte_default_options", "gb
            "gbte_fourier_initial", "gbte_solve", "gbte_get_fields", "gbte_write_outputs", "gbte_get_sizes",
            "gbte_get_geometry", "gbte_last_error", "gbte_status_string", "gbte_destroy", "gbte_kernel_name",
            "gbte_solve_with", "gbte_fourier_initial_noalloc", "gbte_batch_create", "gbte_batch_geometries",
-           "gbte_vjp", "gbte_set_profile", "gbte_set_direction_shard", "gbte_options_size"]
+           "gbte_vjp", "gbte_set_profile", "gbte_set_direction_shard", "gbte_options_size", "gbte_transient_solve"]
 
 # int (*gbte_exchange_fn)(void *user, double *buf, size_t count, void *stream)
 EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
@@ -184,6 +190,9 @@ def library():
                                                  ctypes.c_void_p]
         lib.gbte_vjp.argtypes = [ctypes.c_void_p, _c_dbl_p, _c_dbl_p, ctypes.c_int, ctypes.c_double, _c_dbl_p,
                                  _c_dbl_p, _c_dbl_p, ctypes.POINTER(VjpStats)]
+        lib.gbte_transient_solve.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_int, _c_dbl_p, ctypes.c_longlong,
+                                             ctypes.POINTER(TransientStats)]
         lib.gbte_inspect_deck.argtypes = [ctypes.c_char_p, ctypes.POINTER(DeckInfo)]
         lib.gbte_inspect_mesh.argtypes = [ctypes.POINTER(MeshView), ctypes.POINTER(BandTableC),
                                           ctypes.POINTER(BCTable), ctypes.POINTER(AngleSpec),
@@ -417,6 +426,28 @@ class StaticBTESynthetic:
                                        _ptr(g_spec, ctypes.c_double), ctypes.byref(st)))
         return {"tau": g_tau, "scatter": g_cell, "specularity": g_spec,
                 "stats": {k: getattr(st, k) for k, _ in st._fields_}}
+
+    def transient_solve(self, time_step: float, total_time: float, err_temp: float = 0.0, err_flux: float = 0.0,
+                        probe_cell: int = 0, history: bool = True) -> dict:
+        """The explicit transient solver from the thermal grating
+        T = cos(2 pi x / ScaleX) (gbte_transient_solve, the reference's
+        State=Transient): steps of time_step up to total_time, ending early
+        when both margins reach their limits. Returns the stats and, with
+        ``history``, the temperature of ``probe_cell`` after every step (the
+        reference's TTG.dat column); ``fields()`` then holds the final state."""
+        n = 0
+        x = total_time / time_step
+        while n < x:
+            n += 1
+        hist = np.zeros(n) if history else None
+        st = TransientStats()
+        self._check(library().gbte_transient_solve(self._h, float(time_step), float(total_time), float(err_temp),
+                                                   float(err_flux), int(probe_cell), _ptr(hist, ctypes.c_double),
+                                                   n if history else 0, ctypes.byref(st)))
+        out = {k: getattr(st, k) for k, _ in st._fields_}
+        if history:
+            out["history"] = hist[: st.steps]
+        return out
 
     def set_direction_shard(self, begin: int, count: int, exchange) -> None:
         """Transport over directions [begin, begin + count) only; the moments

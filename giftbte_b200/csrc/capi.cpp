@@ -356,6 +356,9 @@ int gbte_inspect_deck(const char *dir, gbte_deck_info *info) {
             info->max_iter_or_zero = deck.max_iter;
             info->err_temp = deck.err_temp;
             info->err_flux = deck.err_flux;
+            info->transient = deck.transient ? 1 : 0;
+            info->time_step = deck.time_step;
+            info->total_time = deck.total_time;
         }
         return rc;
     } catch (const std::exception &ex) {
@@ -689,6 +692,46 @@ int gbte_write_outputs(gbte_handle *h, const char *dir) {
     for (int c = 0; c < nc; c++) f << q[3 * c] << " " << q[3 * c + 1] << " " << q[3 * c + 2] << "\n";
     f.close();
     return GBTE_OK;
+}
+
+int gbte_transient_solve(gbte_handle *h, double time_step, double total_time, double err_temp, double err_flux,
+                         int probe_cell, double *probe_history, long long history_len, gbte_transient_stats *st) {
+    if (!h) return GBTE_ERR_ARG;
+    try {
+        const int nc = h->solver.mesh.nc;
+        if (probe_cell < 0 || probe_cell >= nc) return fail(h, {-1, "probe_cell out of range"}), GBTE_ERR_ARG;
+        if (history_len < 0 || !(err_temp >= 0) || !(err_flux >= 0))
+            return fail(h, {-1, "invalid transient limits"}), GBTE_ERR_ARG;
+        // internal indices of the caller's cells: the probe, and the cells
+        // numbered like the walls (the start's specular walls read them)
+        int probe = probe_cell;
+        std::vector<int> wall_cell;
+        if (!h->perm.empty()) {
+            std::vector<int> inv(nc);
+            for (int k = 0; k < nc; k++) inv[h->perm[k]] = k;
+            probe = inv[probe_cell];
+            wall_cell.assign(h->solver.mesh.nbd(), -1);
+            for (int ib = 0; ib < (int)wall_cell.size() && ib < nc; ib++) wall_cell[ib] = inv[ib];
+        }
+        gbte::TransientStats ts;
+        gbte::Error e = h->solver.transient(time_step, total_time, err_temp, err_flux, probe,
+                                            history_len > 0 ? probe_history : nullptr, history_len, wall_cell, ts);
+        if (e.code) return fail(h, e), status_of(e.code);
+        if (st) {
+            st->steps = ts.steps;
+            st->updates = ts.updates;
+            st->err_temp = ts.err_temp;
+            st->err_flux = ts.err_flux;
+            st->solve_ms = ts.ms;
+        }
+        return GBTE_OK;
+    } catch (const std::bad_alloc &) {
+        h->err = "host allocation failed";
+        return GBTE_ERR_NOMEM;
+    } catch (const std::exception &ex) {
+        h->err = ex.what();
+        return GBTE_ERR_ARG;
+    }
 }
 
 int gbte_vjp(gbte_handle *h, const double *T_bar, const double *q_bar, int max_iter, double tol, double *grad_tau,

@@ -417,9 +417,14 @@ Error read_deck(const std::string &root, Deck &D) {
             if (has_kw(str, "MaxNumIter")) f >> D.max_iter;
             if (has_kw(str, "ResidualTemp")) f >> D.err_temp;
             if (has_kw(str, "ResidualFlux")) f >> D.err_flux;
+            if (has_kw(str, "TimeStep")) f >> D.time_step;
+            if (has_kw(str, "TotalTime")) f >> D.total_time;
             if (has_kw(str, "InitialTemperatureFile")) return {-8, "InitialTemperatureFile is not supported"};
         }
-        if (state != "Steady") return {-8, "only State=Steady is implemented"};
+        if (state != "Steady" && state != "Transient") return {-8, "State must be Steady or Transient"};
+        D.transient = state == "Transient";
+        if (D.transient && (D.time_step == -1 || D.total_time == -1))
+            return {-2, "provide TimeStep and TotalTime for the transient solver"};
     }
     // GEOMETRY
     int gdim = -1;

@@ -118,6 +118,8 @@ struct Deck {
     std::string order = "2", method = "Sequential", matrix = "LU";
     int max_iter = 10000;
     double err_temp = 1e-6, err_flux = 1e-4, tref = 300, uniform_heat = 0;
+    bool transient = false;                      // CONTROL State=Transient
+    double time_step = -1, total_time = -1;      // CONTROL TimeStep, TotalTime
     std::vector<double> cell_heat;
 };
 Error read_deck(const std::string &dir, Deck &deck);

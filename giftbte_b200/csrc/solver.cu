@@ -1903,6 +1903,125 @@ __global__ void k_gather(DMesh m, DPhys p, const double *__restrict__ dsum, cons
     }
 }
 
+// ---------------------------------------------------------- transient ----
+// The explicit transient solver (src/TransientBTE/TransientSolver.cpp:11-302,
+// transient.cpp:586-1278), FP64 form (e stored whole: base 0).
+//
+// One explicit step of every (direction of the batch, cell, band):
+//   Re = sum_faces (A/V) (v.n) y_f - T_old C / tau + sum_inflow walls (A/V) (v.n) e_wall
+//   e <- e (1 - dt / tau) - dt Re
+// with y_f the second-order upwind face value (the cell's own on outflow
+// faces, the neighbour's on inflow interior faces; transient.cpp:1183-1276).
+// The new values go to `out` ([batch direction][cell][band]); every Re of
+// the step reads the old ones.
+template <int DIM>
+__global__ void k_tr_step(DMesh m, DPhys p, EView<double, DIM> ev, const double *__restrict__ Told,
+                          const double *__restrict__ eb, double dt, double *__restrict__ out, int d0, int ndb) {
+    const int nb = p.nb, nc = m.nc;
+    const size_t total = (size_t)ndb * nc * nb;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b = (int)(t % nb);
+        const int c = (int)((t / nb) % nc);
+        const size_t d = d0 + t / ((size_t)nb * nc);
+        const int mo = mat_off(p, c);
+        const double Cb = p.C[mo + b], tau = p.tau[mo + b] * m.tsc[c], vm = p.vmag[mo + b];
+        const double vx = vm * p.sx[d], vy = vm * p.sy[d], vz = vm * p.sz[d];
+        const double ec = ev.e(d, c, b, Cb);
+        double re = 0;
+        for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+            const double dot = vx * m.cf_nx[k] + vy * m.cf_ny[k] + vz * m.cf_nz[k];
+            const double a = m.cf_area[k] / m.vol[c] * dot;
+            if (dot >= 0) {
+                re += a * (ec + ev.gdot(d, c, b, Cb, m.cf_fx[k] - m.cx[c], m.cf_fy[k] - m.cy[c], m.cf_fz[k] - m.cz[c]));
+            } else if (m.cf_bound[k] < 0) {
+                const int j = m.cf_nbr[k];
+                re += a * (ev.e(d, j, b, Cb) +
+                           ev.gdot(d, j, b, Cb, m.cf_fx[k] - m.cx[j], m.cf_fy[k] - m.cy[j], m.cf_fz[k] - m.cz[j]));
+            }
+        }
+        re -= Told[c] * Cb / tau;
+        for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+            if (m.cf_bound[k] < 0) continue;
+            const double dot = vx * m.cf_nx[k] + vy * m.cf_ny[k] + vz * m.cf_nz[k];
+            if (dot < 0) re += m.cf_area[k] / m.vol[c] * dot * eb[(d * m.nbs + m.cf_bside[k]) * nb + b];
+        }
+        out[t] = ec * (1 - dt / tau) - dt * re;
+    }
+}
+
+// The incoming wall values the transient solver starts from
+// (TransientSolver.cpp:26-115), after a regular outgoing/incoming pass: for
+// every wall side whose cell sees the direction coming in, the value is
+// written to side 0 of its wall (both sides of an interface land there,
+// side 1 last): isothermal C T_wall; diffuse 0; specular the energy density
+// of the cell numbered like the wall in the caller's cell order
+// (wall_cell[ib], -1 past the last cell: left as is), in the nearest mirror
+// direction (spec_nf, searched from direction 0 with closeness 1); periodic
+// the partner side's cell value plus C (T_wall - T_partner); other types
+// leave it.
+__global__ void k_tr_wall_start(DMesh m, DPhys p, const double *__restrict__ e, const int *__restrict__ spec_nf,
+                                const int *__restrict__ wall_cell, double *__restrict__ eb) {
+    const int nb = p.nb, nbd = m.nbd;
+    const size_t total = (size_t)p.nd * nbd * nb;
+    for (size_t t = gtid(); t < total; t += gstride()) {
+        const int b = (int)(t % nb);
+        const int ib = (int)((t / nb) % nbd);
+        const size_t d = t / ((size_t)nb * nbd);
+        for (int icell = 0; icell < 2; icell++) {
+            const int s = 2 * ib + icell, c = m.bs_cell[s];
+            if (c < 0) continue;
+            const int mo = mat_off(p, c);
+            if (p.hr[mo + b] == 0) continue;
+            const int k = m.bs_cf[s];
+            const double vm = p.vmag[mo + b];
+            const double dot = vm * p.sx[d] * m.cf_nx[k] + vm * p.sy[d] * m.cf_ny[k] + vm * p.sz[d] * m.cf_nz[k];
+            if (!(dot < 0)) continue;
+            const int type = m.b_type[ib];
+            double *dst = &eb[(d * m.nbs + 2 * ib) * nb + b];
+            if (type == 1) {
+                *dst = p.C[mo + b] * m.b_T[ib];
+            } else if (type == 2) {
+                *dst = 0.0;
+            } else if (type == 3) {
+                const int nf = spec_nf[(size_t)s * p.nd + d], wc = wall_cell[ib];
+                if (wc >= 0) *dst = e[((size_t)nf * m.nc + wc) * nb + b];
+            } else if (type < 0) {
+                const int cb = m.b_connect[ib], pc = m.bs_cell[2 * cb + icell];
+                if (pc >= 0) *dst = e[(d * m.nc + pc) * nb + b] + p.C[mo + b] * (m.b_T[ib] - m.b_T[cb]);
+            }
+        }
+    }
+}
+
+// Margins of a transient step (transient.cpp:818-863), one block in cell
+// order: sum |T - T_old|, max |T|, sum ||q| - |q_old||, max |q|.
+__global__ void k_tr_margins(int nc, const double *__restrict__ T, const double *__restrict__ Told,
+                             const double *__restrict__ q, const double *__restrict__ qold, double *__restrict__ out) {
+    __shared__ double sh[4][1024];
+    double a = 0, mt = 0, h = 0, mq = 0;
+    for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+        a += fabs(T[i] - Told[i]);
+        mt = fmax(mt, fabs(T[i]));
+        const double q1 = sqrt(q[3 * i] * q[3 * i] + q[3 * i + 1] * q[3 * i + 1] + q[3 * i + 2] * q[3 * i + 2]);
+        const double q0 = sqrt(qold[3 * i] * qold[3 * i] + qold[3 * i + 1] * qold[3 * i + 1] +
+                               qold[3 * i + 2] * qold[3 * i + 2]);
+        h += fabs(q1 - q0);
+        mq = fmax(mq, q1);
+    }
+    sh[0][threadIdx.x] = a, sh[1][threadIdx.x] = mt, sh[2][threadIdx.x] = h, sh[3][threadIdx.x] = mq;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + o];
+            sh[1][threadIdx.x] = fmax(sh[1][threadIdx.x], sh[1][threadIdx.x + o]);
+            sh[2][threadIdx.x] += sh[2][threadIdx.x + o];
+            sh[3][threadIdx.x] = fmax(sh[3][threadIdx.x], sh[3][threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) out[threadIdx.x] = sh[threadIdx.x][0];
+}
+
 // macro boundary temperatures sum lat e w / C with periodic overrides
 __global__ void k_macro_bc(DMesh m, DPhys p, const double *__restrict__ eb, const double *__restrict__ ovr,
                            double *__restrict__ bTm) {
@@ -4381,6 +4500,157 @@ Error Solver::solve(SolveStats &st) {
     }
     if (cfg.precision == 1) return solve_t<float, 3>(st);
     return solve_t<double, 3>(st);
+}
+
+// The explicit transient solver (TransientSolver.cpp:11-302) on the FP64
+// form: T0 = cos(2 pi x / ScaleX) (transient.cpp:586-604), the regular
+// outgoing and incoming wall pass, the solver's own starting wall values
+// (k_tr_wall_start), then `steps` explicit steps, each: T_old, q_old <- T, q;
+// per direction batch the LSQ gradient of the old e, the explicit update
+// (k_tr_step), the outgoing wall values of the new e with the old gradient
+// and the moments; the incoming walls of every direction; the margins.
+// steps = the number of integers below total / dt; a step whose margins are
+// both at or below the limits ends the run, as do 10000 increases in a row.
+// probe: the cell whose temperature is recorded after every step (hist,
+// up to cap values), the reference's TTG.dat column.
+template <int DIM>
+Error Solver::transient_t(double dt, double total, double err_t, double err_q, int probe, double *hist,
+                          long long cap, const std::vector<int> &wall_cell, TransientStats &st) {
+    cudaStream_t s = cfg.stream;
+    const int nc = mesh.nc, nb = bands.nb, nd = ang.nd, nbs = mesh.nbs(), nbd = mesh.nbd();
+    const size_t ne = (size_t)nd * nc * nb;
+    double *eps = (double *)eps_, *g = (double *)grad_, *R = (double *)res_;
+    EView<double, DIM> ev{eps, g, Tbase_, gTb_, nb, nc, 0};
+    const int ndb = ndb_;
+    // start: T0 = cos(2 pi x / L_x), q = 0, e = C T0, base 0
+    std::vector<double> T0(nc);
+    for (int c = 0; c < nc; c++) T0[c] = std::cos(2 * M_PI / mesh.Lx * mesh.cx[c]);
+    CUDA_TRY(cudaMemcpyAsync(T_, T0.data(), (size_t)nc * 8, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemsetAsync(q_, 0, (size_t)nc * 24, s));
+    CUDA_TRY(cudaMemsetAsync(Tbase_, 0, (size_t)nc * 8, s));
+    CUDA_TRY(cudaMemsetAsync(gTb_, 0, (size_t)nc * 24, s));
+    k_init_eps<double><<<grid_for(ne), kThreads, 0, s>>>(dm_, dp_, T_, Tbase_, eps);
+    const double *w = dm_.lsq_w;
+    const int gB = grid_for((size_t)nd * nbs * nb);
+    auto gather = [&]() {
+        if (need_snapshot_) cudaMemcpyAsync(eb_snap_, eb_, (size_t)nd * nbs * nb * 8, cudaMemcpyDeviceToDevice, s);
+        k_diffuse_sum<<<grid_for((size_t)nbs * nb), kThreads, 0, s>>>(dm_, dp_, dif_w_, eb_, dsum_);
+        k_gather<<<gB, kThreads, 0, s>>>(dm_, dp_, dsum_, spec_src_, need_snapshot_ ? eb_snap_ : nullptr, eb_);
+    };
+    for (int d0 = 0; d0 < nd; d0 += ndb) {
+        const int nbt = std::min(ndb, nd - d0);
+        ev.gd0 = d0;
+        k_gradient<double, DIM><<<grid_for((size_t)nbt * nc * nb), kThreads, 0, s>>>(dm_, dp_, w, eps, g, d0, nbt);
+        k_bound_out<double, DIM><<<grid_for((size_t)nbt * nbs * nb), kThreads, 0, s>>>(dm_, dp_, ev, eb_, d0, nbt);
+    }
+    gather();
+    // the starting wall values: mirror directions searched from direction 0
+    {
+        std::vector<int> nf((size_t)nbs * nd, 0);
+        for (int sd = 0; sd < nbs; sd++) {
+            const int c = mesh.bs_cell[sd];
+            if (c < 0 || mesh.b_type[sd >> 1] != 3) continue;
+            const int k = mesh.bs_cf[sd];
+            const double nx = mesh.cf_nx[k], ny = mesh.cf_ny[k], nz = mesh.cf_nz[k];
+            for (int d = 0; d < nd; d++) {
+                const double d1 = ang.sx[d] * nx + ang.sy[d] * ny + ang.sz[d] * nz;
+                const double rx = ang.sx[d] - nx * d1 * 2, ry = ang.sy[d] - ny * d1 * 2, rz = ang.sz[d] - nz * d1 * 2;
+                double close = 1;
+                int best = 0;
+                for (int t = 0; t < nd; t++) {
+                    const double l = std::sqrt(std::pow(rx - ang.sx[t], 2) + std::pow(ry - ang.sy[t], 2) +
+                                               std::pow(rz - ang.sz[t], 2));
+                    if (l < close) best = t, close = l;
+                }
+                nf[(size_t)sd * nd + d] = best;
+            }
+        }
+        std::vector<int> wc(nbd, -1);
+        for (int ib = 0; ib < nbd; ib++)
+            if (ib < nc) wc[ib] = wall_cell.empty() ? ib : wall_cell[ib];
+        nf.insert(nf.end(), wc.begin(), wc.end());
+        if (!tr_nf_) tr_nf_ = (int *)dalloc(nf.size() * sizeof(int));
+        if (!tr_nf_) return {-6, "device allocation failed (transient wall start)"};
+        CUDA_TRY(cudaMemcpyAsync(tr_nf_, nf.data(), nf.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        k_tr_wall_start<<<grid_for((size_t)nd * nbd * nb), kThreads, 0, s>>>(dm_, dp_, eps, tr_nf_,
+                                                                             tr_nf_ + (size_t)nbs * nd, eb_);
+        CUDA_TRY(cudaStreamSynchronize(s));
+        CUDA_TRY(cudaGetLastError());
+    }
+    const double nmax = total / dt;
+    long long steps = 0;
+    while ((double)steps < nmax) steps++;
+    const int cpb = std::max(1, 256 / nb);
+    const int gM = (nc + cpb - 1) / cpb, gC = (nc + kThreads - 1) / kThreads;
+    const size_t msmem = ((size_t)nd * kWTab + (size_t)cpb * nb * kMomSlots) * sizeof(double);
+    if (msmem > 48 * 1024)
+        CUDA_TRY(cudaFuncSetAttribute(k_moments<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem));
+    double *mg = red_;
+    double errOld = 0, errOldq = 0;
+    int errInc = 0;
+    st = TransientStats();
+    CUDA_TRY(cudaEventRecord(ev_[0], s));
+    for (long long nt = 0; nt < steps; nt++) {
+        CUDA_TRY(cudaMemcpyAsync(Told_, T_, (size_t)nc * 8, cudaMemcpyDeviceToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(qold_, q_, (size_t)nc * 24, cudaMemcpyDeviceToDevice, s));
+        for (int d0 = 0; d0 < nd; d0 += ndb) {
+            const int nbt = std::min(ndb, nd - d0);
+            const size_t nbe = (size_t)nbt * nc * nb;
+            ev.gd0 = d0;
+            k_gradient<double, DIM><<<grid_for(nbe), kThreads, 0, s>>>(dm_, dp_, w, eps, g, d0, nbt);
+            k_tr_step<DIM><<<grid_for(nbe), kThreads, 0, s>>>(dm_, dp_, ev, Told_, eb_, dt, R, d0, nbt);
+            CUDA_TRY(cudaMemcpyAsync(eps + (size_t)d0 * nc * nb, R, nbe * 8, cudaMemcpyDeviceToDevice, s));
+            k_bound_out<double, DIM><<<grid_for((size_t)nbt * nbs * nb), kThreads, 0, s>>>(dm_, dp_, ev, eb_, d0, nbt);
+            k_moments<double><<<gM, cpb * nb, msmem, s>>>(dm_, dp_, cpb, eps, (const double *)corr_, Tbase_, wtab_,
+                                                          Tlat_, E_, q_, Tband_, Th_, Q_, 0, d0, nbt, d0 > 0 ? 1 : 0);
+        }
+        gather();
+        // the transient temperature is the lattice one (transient.cpp:789-796)
+        k_copy<<<gC, kThreads, 0, s>>>(Tlat_, T_, nc);
+        k_tr_margins<<<1, 1024, 0, s>>>(nc, T_, Told_, q_, qold_, mg);
+        CUDA_TRY(cudaMemcpyAsync(h_comp_, mg, 4 * 8, cudaMemcpyDeviceToHost, s));
+        if (hist && nt < cap) CUDA_TRY(cudaMemcpyAsync(hist + nt, T_ + probe, 8, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        CUDA_TRY(cudaGetLastError());
+        const double err = h_comp_[0] / nc / h_comp_[1], errq = h_comp_[2] / nc / h_comp_[3];
+        if (cfg.verbose)
+            printf("Iteration #%lld\t Margin per band per cell: Temperature:%.17g Heat Flux:%.17g\n", nt, err, errq);
+        if ((err > errOld && errq > errOldq) || std::isnan(err) || std::isnan(errq) || std::isinf(err) ||
+            std::isinf(errq))
+            errInc++;
+        else
+            errInc = 0;
+        errOld = err;
+        errOldq = errq;
+        st.steps = nt + 1;
+        st.err_temp = err;
+        st.err_flux = errq;
+        if (err <= err_t && errq <= err_q) break;
+        if (errInc >= 10000) break;
+    }
+    CUDA_TRY(cudaEventRecord(ev_[1], s));
+    CUDA_TRY(cudaEventSynchronize(ev_[1]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
+    st.ms = ms;
+    st.updates = st.steps * (long long)ne;
+    have_initial_ = true;
+    started_ = false;
+    return {0, ""};
+}
+
+Error Solver::transient(double dt, double total, double err_t, double err_q, int probe, double *hist, long long cap,
+                        const std::vector<int> &wall_cell, TransientStats &st) {
+    if (!initialised) return {-1, "solver not initialised"};
+    if (cfg.precision != 0) return {-8, "the transient solver runs on the FP64 form (GBTE_FP64)"};
+    if (ncomp_ > 1 || xfn_) return {-8, "the transient solver is not implemented for batched or sharded handles"};
+    if (cfg.order != 2) return {-8, "the transient solver is the second-order scheme (Order=2)"};
+    if (!(dt > 0) || !(total > 0) || !std::isfinite(total / dt)) return {-1, "invalid time step or total time"};
+    if (probe < 0 || probe >= mesh.nc) return {-1, "probe cell out of range"};
+    CUDA_TRY(cudaSetDevice(cfg.device));
+    if (!wall_cell.empty() && (int)wall_cell.size() != mesh.nbd()) return {-1, "wall_cell needs one entry per wall"};
+    if (mesh.dim == 2) return transient_t<2>(dt, total, err_t, err_q, probe, hist, cap, wall_cell, st);
+    return transient_t<3>(dt, total, err_t, err_q, probe, hist, cap, wall_cell, st);
 }
 
 Error Solver::set_shard(int begin, int count, ExchangeFn fn, void *user) {

@@ -99,6 +99,11 @@ struct VjpStats {
     double change = 0, ms = 0, residual = 0;
 };
 
+struct TransientStats {
+    long long steps = 0, updates = 0;
+    double err_temp = 0, err_flux = 0, ms = 0;
+};
+
 struct SolveStats {
     int iterations = 0, inner_iterations = 0;
     double err_temp = 0, err_flux = 0, solve_ms = 0, transport_ms = 0, macro_ms = 0;
@@ -144,6 +149,13 @@ public:
     // partially specular walls only)
     Error vjp(const double *Tbar, const double *qbar, int max_iter, double tol, double *g_tau, double *g_cell,
               double *g_bnd, VjpStats &st);
+    // Explicit transient run from the grating start (FP64 form): steps of dt
+    // up to total, stopping early when both margins reach their limits; the
+    // temperature of cell `probe` after each step goes to hist[0 .. cap);
+    // wall_cell[ib]: this handle's index of the cell numbered ib in the
+    // caller's order (empty: the same order), for the start's specular walls
+    Error transient(double dt, double total, double err_t, double err_q, int probe, double *hist, long long cap,
+                    const std::vector<int> &wall_cell, TransientStats &st);
     // Direction shard: this handle's transport covers directions
     // [begin, begin + count) only, and every outer iteration sums the moments
     // and boundary values over the shard set through `fn` (count = 0 or
@@ -192,6 +204,9 @@ public:
 
 private:
     template <typename S, int DIM> Error solve_t(SolveStats &st);
+    template <int DIM>
+    Error transient_t(double dt, double total, double err_t, double err_q, int probe, double *hist, long long cap,
+                      const std::vector<int> &wall_cell, TransientStats &st);
     Error alloc_all();
     Error cg_solve(const CgPlan &pl, const int *ptr, const int *idx, const double *val, const double *dinv, double *x,
                    const double *b, double rtol, double eta, long long &iters, double *scal, double *r, double *z,
@@ -222,6 +237,7 @@ private:
     double *dif_w_ = nullptr;
     double *dsum_ = nullptr;  // [wall side][band] diffuse re-emission sums
     int *spec_src_ = nullptr;
+    int *tr_nf_ = nullptr;  // transient start: mirror direction per (wall side, direction)
     bool need_snapshot_ = false;
     // schedule on device
     int *lvl_cells_ = nullptr, *lvl_ptr_ = nullptr, *dir_lvl_off_ = nullptr;

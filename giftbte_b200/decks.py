@@ -769,6 +769,10 @@ class Deck:
     # or ShengBTEData entry writes that mode list instead (MaterialFile
     # ALAMODE / ShengBTE), whose reduction the material's BandTable must be
     material_sources: Optional[List[object]] = None
+    # CONTROL State: "Steady", or "Transient" with TimeStep and TotalTime (s)
+    state: str = "Steady"
+    time_step: float = -1.0
+    total_time: float = -1.0
 
     @property
     def materials(self) -> List[BandTable]:
@@ -834,9 +838,12 @@ class Deck:
                 else:
                     f.write(f"{b.tag} {b.type} {b.value:.17g}\n")
         with open(os.path.join(d, "CONTROL"), "w") as f:
-            f.write("State=\nSteady\nOrder=\n%s\nIterativeScheme=\n%s\nMatrixSolver=\nLU\n"
+            f.write("State=\n%s\nOrder=\n%s\nIterativeScheme=\n%s\nMatrixSolver=\nLU\n"
                     "Tref=\n%.17g\nMaxNumIter=\n%d\nResidualTemp=\n%.17g\nResidualFlux=\n%.17g\n"
-                    % (self.order, self.scheme, self.tref, self.max_iter, self.residual_temp, self.residual_flux))
+                    % (self.state, self.order, self.scheme, self.tref, self.max_iter, self.residual_temp,
+                       self.residual_flux))
+            if self.state == "Transient":
+                f.write("TimeStep=\n%.17g\nTotalTime=\n%.17g\n" % (self.time_step, self.total_time))
         with open(os.path.join(d, "GEOMETRY"), "w") as f:
             f.write("GeometryDimension=\n%d\nScaleX=\n%.17g\nScaleY=\n%.17g\n"
                     % (self.dimension, self.scale[0], self.scale[1]))
@@ -922,6 +929,22 @@ def mode_list_deck(kind: str, n: int = 12, n_bands: int = 12, seed: int = 0, **k
     kw.setdefault("tref", 300.0)
     return Deck(mesh=square_tri_mesh(n, n), bands=src.band_table(n_bands), bcs=bcs, scale=(1e-7, 1e-7),
                 material_sources=[src], **kw)
+
+
+def grating_deck(nx: int = 24, ny: int = 6, n_bands: int = 3, steps: int = 40, **kw) -> Deck:
+    """A transient thermal-grating strip for the explicit solver: 300 x 75 nm
+    of triangles, x-periodic (no jump), specular top and bottom, sine-
+    dispersion bands; the reference's transient solver starts from
+    T = cos(2 pi x / ScaleX) and takes `steps` explicit steps of 1e-13 s."""
+    m = square_tri_mesh(nx, ny)
+    m = Mesh2D(nodes=m.nodes * np.array([1.0, 0.25]), cells=m.cells, edges=m.edges, edge_tags=m.edge_tags,
+               cell_region=m.cell_region)
+    bcs = [BC(1, -2, 0.0), BC(2, -1, 0.0), BC(3, 3, 0.0), BC(4, 3, 0.0)]
+    kw.setdefault("n_phi", 4)
+    kw.setdefault("angle_method", 1)
+    return Deck(mesh=m, bands=sine_dispersion_bands(n_bands), bcs=bcs, scale=(3e-7, 3e-7), tref=0.0,
+                state="Transient", time_step=1e-13, total_time=steps * 1e-13, residual_temp=1e-14,
+                residual_flux=1e-14, **kw)
 
 
 def config1_deck(n: int = 40, **kw) -> Deck:

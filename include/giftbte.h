@@ -261,6 +261,9 @@ typedef struct {
     int far_slots;             /* on-chip slots for upwind reads older than the ring */
     long long far_refs;        /* upwind reads older than the ring, all directions */
     long long index_entries_checked; /* entries range-checked (0 unless GBTE_DEBUG is set or built in) */
+    int transient;             /* CONTROL State=Transient (decks only) */
+    double time_step;          /* TimeStep and TotalTime from CONTROL (decks only; -1 if absent) */
+    double total_time;
 } gbte_deck_info;
 
 int gbte_inspect_deck(const char *dir, gbte_deck_info *info);
@@ -400,6 +403,33 @@ typedef struct {
 
 int gbte_vjp(gbte_handle *h, const double *T_bar, const double *q_bar, int max_iter, double tol, double *grad_tau,
              double *grad_scatter, double *grad_specularity, gbte_vjp_stats *st);
+
+/* The explicit transient solver (Transient::solve, src/TransientBTE/
+ * TransientSolver.cpp:11-302, which the reference runs for CONTROL
+ * State=Transient from src/Solution/Solution.cpp:500-520). It starts from the
+ * thermal grating T = cos(2 pi x / ScaleX) (transient.cpp:586-604), whatever
+ * gbte_set_initial gave, and the reference's starting wall values, then takes
+ * explicit steps e <- e (1 - dt / tau) - dt Re (second-order upwind fluxes,
+ * the equilibrium C T_old / tau, the incoming walls) for the integers
+ * n < total_time / time_step, stopping early when both margins (sum |T -
+ * T_old| / Nc / max |T|, and the same for |q|) reach err_temp and err_flux.
+ * After each step the lattice temperature of cell probe_cell (the caller's
+ * numbering) is written to probe_history[step] for the first history_len
+ * steps (the reference's TTG.dat records cell 0); may be NULL.
+ * gbte_get_fields then gives the final lattice temperature and heat flux.
+ * FP64 handles of one geometry, second order (GBTE_ERR_UNSUPPORTED
+ * otherwise). The TDTR heat pulses (IsTDTR) are not built: the reference
+ * stops there ("contact us", src/BTEMain.cpp:154-165). */
+typedef struct {
+    long long steps;   /* explicit steps taken */
+    long long updates; /* band * direction * cell updates */
+    double err_temp;   /* margins of the last step */
+    double err_flux;
+    double solve_ms;   /* device time */
+} gbte_transient_stats;
+
+int gbte_transient_solve(gbte_handle *h, double time_step, double total_time, double err_temp, double err_flux,
+                         int probe_cell, double *probe_history, long long history_len, gbte_transient_stats *st);
 
 /* Direction sharding of one solve over several handles (one per GPU and
  * process, or several in one process): the reference's decomposition of the

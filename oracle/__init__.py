@@ -139,6 +139,9 @@ def run_reference(deck_root: str, timeout: float = 3600.0, binary: Optional[str]
 
 
 def read_reference_outputs(deck_root: str) -> Dict[str, np.ndarray]:
+    if not os.path.exists(os.path.join(deck_root, "TempLattice.dat")) and \
+            os.path.exists(os.path.join(deck_root, "TTG.dat")):
+        return read_transient_outputs(deck_root)
     T = np.loadtxt(os.path.join(deck_root, "TempLattice.dat"))
     E = np.loadtxt(os.path.join(deck_root, "Temperature.dat"))
     q = np.loadtxt(os.path.join(deck_root, "HeatFlux.dat"))
@@ -164,3 +167,24 @@ def read_reference_outputs(deck_root: str) -> Dict[str, np.ndarray]:
     out["iters"] = iters
     out["margins"] = np.asarray(margins).reshape(-1, 2)
     return out
+
+
+def read_transient_outputs(deck_root: str) -> Dict[str, np.ndarray]:
+    """Outputs of the reference's transient solver (Transient::_print_out,
+    src/TransientBTE/transient.cpp:865-889, and TransientSolver.cpp:158):
+    Tempcell.dat (cell centre, lattice temperature), HeatFlux.dat (centre,
+    flux) and TTG.dat (time, temperature of cell 0 after each step); the
+    per-step margins from the log."""
+    T = np.loadtxt(os.path.join(deck_root, "Tempcell.dat"))
+    q = np.loadtxt(os.path.join(deck_root, "HeatFlux.dat"))
+    ttg = np.loadtxt(os.path.join(deck_root, "TTG.dat")).reshape(-1, 2)
+    margins = []
+    logp = os.path.join(deck_root, "ref_run.log")
+    if os.path.exists(logp):
+        with open(logp) as f:
+            for line in f:
+                if line.startswith("Iteration #"):
+                    margins.append((float(line.split("Temperature:")[1].split()[0]),
+                                    float(line.split("Heat Flux:")[1].split()[0])))
+    return {"xyz": T[:, :3], "T": T[:, 3], "q": q[:, 3:6], "ttg": ttg, "iters": len(margins),
+            "margins": np.asarray(margins).reshape(-1, 2)}

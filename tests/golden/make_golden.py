@@ -93,6 +93,9 @@ def cases():
     #    and ShengBTE layouts (seeded synthetic modes, MaterialFile ALAMODE /
     #    ShengBTE): the reference's own readers make the band tables
     out["alamode_square"] = decks.mode_list_deck("ALAMODE", 12)
+    # 12. the explicit transient solver (CONTROL State=Transient) on a
+    #     thermal-grating strip: 40 steps of 1e-13 s
+    out["grating_transient"] = decks.grating_deck()
     out["shengbte_square"] = decks.mode_list_deck("ShengBTE", 12)
     out["quad_firstorder_sequential"] = decks.Deck(
         mesh=decks.square_quad_mesh(16, 16), bands=decks.sine_dispersion_bands(2),
@@ -100,6 +103,8 @@ def cases():
         scale=(1e-7, 1e-7), material_dim=3, angle_method=2, n_theta=2, n_phi=2, tref=300.0,
         heat_source=1e16, order="1", scheme="Sequential")
     for d in out.values():
+        if d.state == "Transient":
+            continue  # margins 1e-14: the step count ends the run
         d.residual_temp = 1e-12
         d.residual_flux = 1e-12
         d.max_iter = 3000
@@ -120,6 +125,7 @@ def deck_params(d: decks.Deck) -> dict:
                                  for k in ("v", "tau", "C", "lattice_ratio", "heat_ratio")}
                                 for m in d.extra_materials],
             "region_material": d.region_material,
+            "state": d.state, "time_step": d.time_step, "total_time": d.total_time,
             "material_sources": [None if src is None else
                                  {"kind": "ALAMODE" if isinstance(src, decks.AlamodeModes) else "ShengBTE",
                                   "seed": src.seed}
@@ -165,18 +171,19 @@ def make(name: str, d: decks.Deck) -> None:
     m = d.mesh
     B = d.bands
     extra = {}
-    Tband = r["Tband"]
+    Tband = r.get("Tband")
     if name in BIG:
         extra["bands_kept"] = np.asarray(CONFIG2_BANDS)
         Tband = Tband[CONFIG2_BANDS]
+    fields = {k: r[k] for k in ("T", "E", "q", "xyz", "iters", "Tf", "qf", "margins", "ttg") if k in r}
+    if Tband is not None:
+        fields["Tband"] = Tband
     np.savez_compressed(
         os.path.join(HERE, f"{name}.npz"),
         nodes=m.nodes, cells=np.asarray(m.cells), edges=m.edges, edge_tags=m.edge_tags,
         cell_region=m.cell_region,
         band_v=B.v, band_tau=B.tau, band_C=B.C, band_lat=B.lattice_ratio, band_hr=B.heat_ratio,
-        params=json.dumps(deck_params(d)),
-        T=r["T"], E=r["E"], q=r["q"], Tband=Tband, xyz=r["xyz"], iters=r["iters"],
-        Tf=r["Tf"], qf=r["qf"], margins=r["margins"], **extra)
+        params=json.dumps(deck_params(d)), **fields, **extra)
     print(f"{name}: Nc={m.n_cells} Nb={B.n_bands} iters={r['iters']}")
 
 
@@ -208,7 +215,12 @@ def load(name: str):
         else:
             srcs.append(decks.synthetic_shengbte(seed=m["seed"]))
     d.material_sources = srcs or None
-    ref = {k: z[k] for k in ("T", "E", "q", "Tband", "xyz", "Tf", "qf", "margins", "bands_kept") if k in z}
+    d.state = p.get("state", "Steady")
+    d.time_step = p.get("time_step", -1.0)
+    d.total_time = p.get("total_time", -1.0)
+    if d.state == "Transient":
+        d.residual_temp = d.residual_flux = 1e-14
+    ref = {k: z[k] for k in ("T", "E", "q", "Tband", "xyz", "Tf", "qf", "margins", "bands_kept", "ttg") if k in z}
     ref["iters"] = int(z["iters"])
     if name in BIG:
         d.max_iter = BIG[name] or 3000
@@ -223,6 +235,8 @@ def have(name: str) -> bool:
 CASES = ["gray_square_tri", "quad_heat_specular", "periodic_jitter", "porous_msh", "porous_firstorder",
          "periodic_sequential", "quad_firstorder_sequential", "porous_limiter", "interface_2mat",
          "alamode_square", "shengbte_square"]
+# the explicit transient solver's cases (a fixed step count)
+TRANSIENT = ["grating_transient"]
 # the cases solved to 1e-12 margins (all but the limited one, a fixed count)
 CONVERGED = [c for c in CASES if c != "porous_limiter"]
 # the cases of one material (the CPU restatement and the device Fourier
@@ -230,7 +244,7 @@ CONVERGED = [c for c in CASES if c != "porous_limiter"]
 ONE_MATERIAL = [c for c in CASES if c != "interface_2mat"]
 
 if __name__ == "__main__":
-    want = sys.argv[1:] or CASES
+    want = sys.argv[1:] or CASES + TRANSIENT
     all_cases = cases()
     all_cases.update(big_cases())
     for n in want:

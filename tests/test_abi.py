@@ -212,3 +212,19 @@ def test_mode_list_missing_files_are_io_errors(tmp_path):
         with pytest.raises(g.GBTEError) as e:
             g.inspect_deck(str(root))
         assert e.value.status == -2
+
+
+def test_transient_deck_reads_on_the_host(tmp_path):
+    # CONTROL State=Transient with TimeStep and TotalTime; without them the
+    # deck is refused as the reference refuses it (src/BTEMain.cpp:197-200)
+    d = decks.grating_deck(steps=12)
+    d.write(str(tmp_path / "a"))
+    info = g.inspect_deck(str(tmp_path / "a"))
+    assert info["transient"] == 1 and info["time_step"] == 1e-13
+    assert info["total_time"] == pytest.approx(12e-13, rel=1e-15)
+    d.write(str(tmp_path / "b"))
+    ctl = tmp_path / "b" / "input" / "CONTROL"
+    ctl.write_text(ctl.read_text().split("TimeStep=")[0])
+    with pytest.raises(g.GBTEError) as e:
+        g.inspect_deck(str(tmp_path / "b"))
+    assert e.value.status == -2
