@@ -31,7 +31,7 @@
 #include "Eigen/SparseLU"
 typedef Eigen::Triplet<double> Tri;
 
-struct gbte_handle;
+#include "b200_deck_views.h"
 
 class StaticBTESynthetic {
 public:
@@ -94,13 +94,7 @@ private:
     // the reference's objects flattened into the C ABI's views (kept for
     // the handle, which is created by the first solve: the variant's order,
     // scheme and limiter are options of gbte_create)
-    std::vector<double> node_xyz_, cell_heat_, band_v_, band_tau_, band_C_, band_lat_, band_hr_;
-    std::vector<double> dir_xyz_, dir_w_, bc_value_, bc_trans_;
-    std::vector<int> cell_ptr_, cell_verts_, cell_region_, belem_ptr_, belem_verts_, belem_tag_;
-    std::vector<int> region_material_, bc_tag_, bc_type_;
-    double scale_[3] = {1, 1, 1};
-    double solid_angle_ = 0;
-    int num_materials_ = 1, material_dimension_ = 2;
+    B200DeckViews views_;
     gbte_handle *h_ = nullptr;
     int h_order_ = 0, h_sequential_ = 0, h_limiter_ = 0;
 };

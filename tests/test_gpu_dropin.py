@@ -2,8 +2,8 @@
 
 oracle/_ref/BTE_B200 is the reference's own program (BTEMain.cpp,
 Solution.cpp and the rest of its sources, unmodified) compiled against the
-B200 drop-in class of giftbte_b200/shim/ in place of its own
-StaticBTESynthetic (make -C oracle dropin). Run on a deck directory, it
+B200 drop-in classes of giftbte_b200/shim/ in place of its own
+StaticBTESynthetic and Transient (make -C oracle dropin). Run on a deck directory, it
 reads the deck with the reference's readers, runs the reference's Fourier
 pre-solve on the CPU, hands its fields to the drop-in class exactly as
 SolutionAll::_BTE_Solver does (src/Solution/Solution.cpp:262-414), solves
@@ -122,3 +122,18 @@ def test_output_files_match_reference_files(case, tmp_path):
     s.close()
     for f in files:
         assert_same_file(str(api_dir / f), str(ref_dir / f))
+
+
+def test_reference_program_transient_with_b200_solver(tmp_path):
+    # State=Transient: SolutionAll::_Transient_BTE_Solver (Solution.cpp:500-520)
+    # hands the drop-in Transient class its objects; the GPU run's TTG.dat,
+    # Tempcell.dat and HeatFlux.dat match the compiled reference's
+    deck, ref = mg.load("grating_transient")
+    deck.write(str(tmp_path))
+    out = oracle.run_reference(str(tmp_path), timeout=600, binary=oracle.DROPIN_BIN)
+    assert len(out["ttg"]) == len(ref["ttg"])
+    assert np.array_equal(out["ttg"][:, 0], ref["ttg"][:, 0])
+    assert rel(out["ttg"][:, 1], ref["ttg"][:, 1]) <= TOL, rel(out["ttg"][:, 1], ref["ttg"][:, 1])
+    assert np.array_equal(out["xyz"], ref["xyz"])
+    assert rel(out["T"], ref["T"]) <= TOL, rel(out["T"], ref["T"])
+    assert rel(out["q"], ref["q"]) <= TOL, rel(out["q"], ref["q"])
