@@ -16,6 +16,7 @@ constructor raises.
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 from typing import Optional
 
@@ -428,17 +429,15 @@ class StaticBTESynthetic:
                 "stats": {k: getattr(st, k) for k, _ in st._fields_}}
 
     def transient_solve(self, time_step: float, total_time: float, err_temp: float = 0.0, err_flux: float = 0.0,
-                        probe_cell: int = 0, history: bool = True) -> dict:
+                        probe_cell: int = 0, history: bool = True, history_cap: int = 1 << 26) -> dict:
         """The explicit transient solver from the thermal grating
         T = cos(2 pi x / ScaleX) (gbte_transient_solve, the reference's
         State=Transient): steps of time_step up to total_time, ending early
         when both margins reach their limits. Returns the stats and, with
         ``history``, the temperature of ``probe_cell`` after every step (the
-        reference's TTG.dat column); ``fields()`` then holds the final state."""
-        n = 0
-        x = total_time / time_step
-        while n < x:
-            n += 1
+        reference's TTG.dat column, the first ``history_cap`` steps);
+        ``fields()`` then holds the final state."""
+        n = min(max(0, math.ceil(total_time / time_step)), int(history_cap))
         hist = np.zeros(n) if history else None
         st = TransientStats()
         self._check(library().gbte_transient_solve(self._h, float(time_step), float(total_time), float(err_temp),
@@ -446,7 +445,7 @@ class StaticBTESynthetic:
                                                    n if history else 0, ctypes.byref(st)))
         out = {k: getattr(st, k) for k, _ in st._fields_}
         if history:
-            out["history"] = hist[: st.steps]
+            out["history"] = hist[: min(st.steps, n)]
         return out
 
     def set_direction_shard(self, begin: int, count: int, exchange) -> None:

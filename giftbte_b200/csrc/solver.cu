@@ -4577,9 +4577,8 @@ Error Solver::transient_t(double dt, double total, double err_t, double err_q, i
         CUDA_TRY(cudaStreamSynchronize(s));
         CUDA_TRY(cudaGetLastError());
     }
-    const double nmax = total / dt;
-    long long steps = 0;
-    while ((double)steps < nmax) steps++;
+    // the integers n >= 0 below total / dt
+    const long long steps = (long long)std::ceil(total / dt);
     const int cpb = std::max(1, 256 / nb);
     const int gM = (nc + cpb - 1) / cpb, gC = (nc + kThreads - 1) / kThreads;
     const size_t msmem = ((size_t)nd * kWTab + (size_t)cpb * nb * kMomSlots) * sizeof(double);

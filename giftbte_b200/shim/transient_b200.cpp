@@ -3,6 +3,8 @@
 // transient solve on the device.
 #include "TransientBTE/transient.h"
 
+#include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <fstream>
 #include <iomanip>
@@ -56,13 +58,13 @@ void Transient::solve(int Use_Backup, double error_temp_limit, double error_flux
     gbte_handle *h = nullptr;
     int rc = views_.create(opt, &h);
     if (rc != GBTE_OK) b200_stop("gbte_create", rc, nullptr);
-    // the steps the reference takes: the integers below totalT / deltaT
-    const double nmax = totalT / deltaT;
-    long long steps = 0;
-    while ((double)steps < nmax) steps++;
-    std::vector<double> ttg((size_t)steps, 0.0);
+    // the steps the reference takes: the integers below totalT / deltaT;
+    // TTG.dat keeps the first 2^26 of them
+    const long long steps = (long long)std::ceil(totalT / deltaT);
+    const long long kept = std::min(steps, 1LL << 26);
+    std::vector<double> ttg((size_t)kept, 0.0);
     gbte_transient_stats st{};
-    rc = gbte_transient_solve(h, deltaT, totalT, error_temp_limit, error_flux_limit, 0, ttg.data(), steps, &st);
+    rc = gbte_transient_solve(h, deltaT, totalT, error_temp_limit, error_flux_limit, 0, ttg.data(), kept, &st);
     if (rc != GBTE_OK) b200_stop("gbte_transient_solve", rc, h);
     std::vector<double> q(3 * (size_t)numCell);
     rc = gbte_get_fields(h, nullptr, temperature, q.data(), nullptr);
@@ -76,7 +78,8 @@ void Transient::solve(int Use_Backup, double error_temp_limit, double error_flux
     // never fills, written as zeros here
     const std::vector<double> &x = views_.center_x, &y = views_.center_y, &z = views_.center_z;
     std::ofstream ttgf("TTG.dat");
-    for (long long n = 0; n < st.steps; n++) ttgf << (n + 1) * deltaT << " " << ttg[(size_t)n] << std::endl;
+    for (long long n = 0; n < std::min(st.steps, kept); n++)
+        ttgf << (n + 1) * deltaT << " " << ttg[(size_t)n] << std::endl;
     std::ofstream t0("Tempcell.dat"), t1("Tempcell1.dat"), hs("HeatSource.dat"), hf("HeatFlux.dat");
     for (int i = 0; i < numCell; i++) {
         t0 << x[i] << " " << y[i] << " " << z[i] << " " << temperature[i] << std::endl;
