@@ -8,7 +8,7 @@ from giftbte_b200 import GBTE_FP32_MIXED, GBTE_FP64, GBTEError, StaticBTESynthet
 
 pytestmark = pytest.mark.gpu
 
-# FP64 drop-in form: reference fixed point to <= 1e-9 relative (north star);
+# FP64 drop-in form: reference fixed point to <= 1e-9 relative;
 # FP32 intensity form: <= 1e-5 relative temperature error.
 TOL_FP64 = 1e-9
 TOL_FP32 = 1e-5
@@ -171,7 +171,7 @@ def test_benchmark_cell_converged_matches_reference():
     # the same cell converged: with exact macro solves the outer iterates
     # follow the reference's, so stopping at the reference's margins (1e-9)
     # stops at its iteration; the fields and the effective conductivity
-    # k_x = <q_x>_V L / dT then agree to the north-star 1e-9
+    # k_x = <q_x>_V L / dT then agree to 1e-9
     deck, ref = mg.load("config2_converged")
     s = StaticBTESynthetic.from_deck(deck, precision=GBTE_FP64, macro_exact=1)
     s.set_initial(ref["Tf"], ref["qf"])
