@@ -558,7 +558,11 @@ Error read_deck(const std::string &root, Deck &D) {
                         if (b < B.nb) tr[(size_t)mt * B.nb + b] = std::atof(line.c_str());
                         b++;
                     }
-                    if (b != B.nb) return {-2, "interface file: band count differs from the band table: " + tfile};
+                    // the reference warns and goes on, reading past the end of
+                    // its table for the missing bands; here the deck is refused
+                    if (b != B.nb)
+                        return {-2, "interface file " + tfile + ": material " + std::to_string(mt) + " lists " +
+                                        std::to_string(b) + " transmissivities for " + std::to_string(B.nb) + " bands"};
                 }
                 any5 = true;
             }
