@@ -142,7 +142,7 @@ def test_index_checks_pass_on_built_meshes(make, monkeypatch):
 
 
 def test_index_checks_catch_planted_entries(tmp_path):
-    # the checker itself, host only: tests/index_check_main.cpp builds the
+    # the checker itself, host only: tests/cpp/index_check_main.cpp builds the
     # arrays the solver uploads for a porous-cell deck, expects them to pass,
     # then plants one bad entry per array kind (a neighbour past the cells,
     # decreasing offsets, a negative stencil index, a wall side past the
@@ -157,7 +157,7 @@ def test_index_checks_catch_planted_entries(tmp_path):
         pytest.skip("g++ not available")
     csrc = os.path.join(ROOT, "giftbte_b200", "csrc")
     exe = str(tmp_path / "index_check")
-    subprocess.check_call([gxx, "-std=c++17", "-O1", "-I", csrc, os.path.join(ROOT, "tests", "index_check_main.cpp")] +
+    subprocess.check_call([gxx, "-std=c++17", "-O1", "-I", csrc, os.path.join(ROOT, "tests", "cpp", "index_check_main.cpp")] +
                           [os.path.join(csrc, f) for f in ("deck.cpp", "mesh.cpp", "angles.cpp")] +
                           ["-lpthread", "-o", exe])
     decks.config2_deck(h_nm=15.0, n_bands=4, n_phi=4).write(str(tmp_path / "deck"))
