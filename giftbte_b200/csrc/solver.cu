@@ -3995,7 +3995,12 @@ Error Solver::solve_t(SolveStats &st) {
         for (int d0 = 0; d0 < nd; d0 += ndb) {
             const int nbt = std::min(ndb, nd - d0);
             ev.gd0 = d0;
-            if (cfg.order == 2)
+            // the gradient in the iteration's launch shape (every shape gives
+            // the same bits; the one-band form where bands are not a
+            // multiple of 4)
+            if (cfg.order == 2 && nb % 4 == 0)
+                GL(K_GRADIENT, CUDA_TRY(launch_grad(grad_dg, d0, nbt)));
+            else if (cfg.order == 2)
                 GL(K_GRADIENT, (k_gradient<S, DIM><<<grid_for((size_t)nbt * nc * nb), kThreads, 0, s>>>(dm_, dp_, w, eps,
                                                                                                      g, d0, nbt)));
             if (cfg.use_limiter)
