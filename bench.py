@@ -735,7 +735,7 @@ def main():
     ap.add_argument("--sweep-kernel", type=int, choices=[0, 1, 2, 3], default=0,
                     help="1: block sweep kernel, 2: warp-independent kernel, 3: wide-level kernel, "
                          "0: the autotuner's pick")
-    ap.add_argument("--gradient-dirs", type=int, choices=[0, 1, 2, 4, 5, 6, 7, 8], default=0,
+    ap.add_argument("--gradient-dirs", type=int, choices=[0, 1, 2, 4, 5, 6, 7, 8, 9, 10], default=0,
                     help="gradient launch shape (options.gradient_dirs); 0 lets the first iteration pick")
     ap.add_argument("--residual-form", type=int, choices=[0, 1, 5, 6, 7, 8], default=0,
                     help="residual launch shape (options.residual_form); 0 lets the first iteration pick")

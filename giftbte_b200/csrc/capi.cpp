@@ -165,8 +165,8 @@ int create_common(const gbte::RawMesh &raw_in, const gbte::Bands &bands_in, cons
         return fail(nullptr, {-1, "sweep_kernel must be 0 (automatic), 1 (block), 2 (warp) or 3 (wide)"}),
                GBTE_ERR_ARG;
     cfg.sweep_kernel = opt.sweep_kernel;
-    if (opt.gradient_dirs < 0 || opt.gradient_dirs > 8 || opt.gradient_dirs == 3)
-        return fail(nullptr, {-1, "gradient_dirs must be 0 (automatic), 1, 2, 4, 5, 6, 7 or 8"}), GBTE_ERR_ARG;
+    if (opt.gradient_dirs < 0 || opt.gradient_dirs > 10 || opt.gradient_dirs == 3)
+        return fail(nullptr, {-1, "gradient_dirs must be 0 (automatic), 1, 2, 4, 5, 6, 7, 8, 9 or 10"}), GBTE_ERR_ARG;
     cfg.gradient_dirs = opt.gradient_dirs;
     if (opt.residual_form != 0 && opt.residual_form != 1 && (opt.residual_form < 5 || opt.residual_form > 8))
         return fail(nullptr, {-1, "residual_form must be 0 (automatic), 1, 5, 6, 7 or 8"}), GBTE_ERR_ARG;

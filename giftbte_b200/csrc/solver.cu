@@ -879,6 +879,99 @@ __global__ void __launch_bounds__(512) k_gradient_tile(DMesh m, DPhys p, const f
     }
 }
 
+// The tiled gradient with eight lanes per cell (FP32 form). Lane l of a
+// cell takes the 16-byte piece l of the first 32 bands of the CTA's band
+// chunk and NS single bands 32 + 8 s + l, so the chunk is 32 + 8 NS bands.
+// A 16-byte shared load is served a quarter warp (8 lanes) at a time; here
+// each quarter warp reads one cell's row, whose eight pieces sit in eight
+// distinct bank groups, so those loads never conflict, whatever rows the
+// cells name. With four bands per lane across the chunk (k_gradient_tile at
+// 40 bands: ten lanes per cell), a quarter warp spans two cells' rows and
+// their pieces collide in about a quarter of the wavefronts. Per band and
+// direction the arithmetic is k_gradient_tile's, entry by entry in the same
+// order, so both give the same bits. Shared memory as k_gradient_tile's.
+template <int DIM, int NS>
+__global__ void __launch_bounds__(512) k_gradient_tile8(DMesh m, DPhys p, const float4 *__restrict__ pk,
+                                                        const int *__restrict__ tile_ptr,
+                                                        const int *__restrict__ tile_cells,
+                                                        const unsigned short *__restrict__ tile_loc, int B, int qmax,
+                                                        const float *__restrict__ eps, float *__restrict__ g, int d0,
+                                                        int ndb) {
+    constexpr int nbc = 32 + 8 * NS, per_row = nbc / 4, NV = 4 + NS;
+    extern __shared__ __align__(16) unsigned char tsm[];
+    TileW<float> *wq = reinterpret_cast<TileW<float> *>(tsm);
+    float *et = reinterpret_cast<float *>(tsm + (size_t)qmax * sizeof(TileW<float>));
+    const int nb = p.nb, nc = m.nc, nchunk = nb / nbc;
+    const int blk = blockIdx.x / nchunk, ch = blockIdx.x % nchunk, b0 = ch * nbc;
+    const int c0 = blk * B, c1 = min(c0 + B, nc), ncell = c1 - c0;
+    const int qb0 = m.nbr_ptr[c0], qb1 = m.nbr_ptr[c1];
+    const int u0 = tile_ptr[blk], nu = tile_ptr[blk + 1] - u0;
+    const int tid = threadIdx.x, bd = blockDim.x;
+    // the stencil entries, each neighbour's union index stored as the word
+    // offset of its row
+    for (int q = qb0 + tid; q < qb1; q += bd) {
+        const float4 a = pk[q];
+        TileW<float> t;
+        t.wx = a.x, t.wy = a.y, t.wz = a.z;
+        t.loc = (int)tile_loc[q] * nbc;
+        wq[q - qb0] = t;
+    }
+    const int i = tid >> 3, l = tid & 7;  // cell of the block, lane within it
+    const bool active = i < ncell;
+    const int c = c0 + (active ? i : 0);
+    const int qa = m.nbr_ptr[c] - qb0, qe = active ? m.nbr_ptr[c + 1] - qb0 : qa;
+    // this lane's bands within the chunk: 4 l .. 4 l + 3, then 32 + 8 s + l
+    const float *ev = et + 4 * l;
+    const float *es = et + 32 + l;
+    for (int dl = 0; dl < ndb; dl++) {
+        const float *ed = eps + (size_t)(d0 + dl) * nc * nb + b0;
+        __syncthreads();  // the previous direction's reads of et are done
+        for (int k = tid; k < nu * per_row; k += bd) {
+            const int u = k / per_row, r = k - u * per_row;
+            cp_async(et + (size_t)u * nbc + 4 * r, ed + (size_t)tile_cells[u0 + u] * nb + 4 * r, 16);
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        if (!active) continue;
+        float ec[NV], gx[NV], gy[NV], gz[NV];
+        {
+            const float4 a = *reinterpret_cast<const float4 *>(ev + i * nbc);
+            ec[0] = a.x, ec[1] = a.y, ec[2] = a.z, ec[3] = a.w;
+#pragma unroll
+            for (int s = 0; s < NS; s++) ec[4 + s] = es[i * nbc + 8 * s];
+        }
+#pragma unroll
+        for (int v = 0; v < NV; v++) gx[v] = gy[v] = gz[v] = 0;
+        for (int q = qa; q < qe; q++) {
+            const TileW<float> t = wq[q];
+            float e[NV];
+            const float4 a = *reinterpret_cast<const float4 *>(ev + t.loc);
+            e[0] = a.x, e[1] = a.y, e[2] = a.z, e[3] = a.w;
+#pragma unroll
+            for (int s = 0; s < NS; s++) e[4 + s] = es[t.loc + 8 * s];
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                const float de = nbr_term(e[v], ec[v]);
+                gx[v] += t.wx * de;
+                gy[v] += t.wy * de;
+                if (DIM == 3) gz[v] += t.wz * de;
+            }
+        }
+        centre_term<NV>(m, c, ec, gx, gy, gz);
+        float *gp = g + ((size_t)dl * nc + c) * DIM * nb + b0;
+        *reinterpret_cast<float4 *>(gp + 4 * l) = make_float4(gx[0], gx[1], gx[2], gx[3]);
+        *reinterpret_cast<float4 *>(gp + nb + 4 * l) = make_float4(gy[0], gy[1], gy[2], gy[3]);
+        if (DIM == 3) *reinterpret_cast<float4 *>(gp + 2 * nb + 4 * l) = make_float4(gz[0], gz[1], gz[2], gz[3]);
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            gp[32 + 8 * s + l] = gx[4 + s];
+            gp[nb + 32 + 8 * s + l] = gy[4 + s];
+            if (DIM == 3) gp[2 * nb + 32 + 8 * s + l] = gz[4 + s];
+        }
+    }
+}
+
 // Shared-memory tiled residual: one CTA per (block of B consecutive cells,
 // chunk of nbc bands), looping over the batch's directions. For each
 // direction the intensity and gradient rows of the block's union (its cells
@@ -3884,6 +3977,14 @@ Error Solver::solve_t(SolveStats &st) {
                                       220 * 1024));
         CUDA_TRY(cudaFuncSetAttribute(k_residual_tile<S, DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       220 * 1024));
+        if constexpr (sizeof(S) == 4) {
+            CUDA_TRY(cudaFuncSetAttribute(k_gradient_tile8<DIM, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          220 * 1024));
+            CUDA_TRY(cudaFuncSetAttribute(k_gradient_tile8<DIM, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          220 * 1024));
+            CUDA_TRY(cudaFuncSetAttribute(k_gradient_tile8<DIM, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          220 * 1024));
+        }
     }
     auto rtile_shape = [&](int code, int &nbc, int &threads, size_t &smem) -> bool {
         const int k = code - 7;
@@ -3916,7 +4017,46 @@ Error Solver::solve_t(SolveStats &st) {
             }
         return false;
     };
+    // the eight-lane tiled form (9, 10: tiles_[0], tiles_[1]; FP32 form):
+    // the widest chunk of 32 + 8 NS bands (NS <= 2) dividing the band count
+    // whose shared memory fits, at 8 threads per cell of the block
+    auto tile8_shape = [&](int code, int &ns, int &threads, size_t &smem) -> bool {
+        const int k = code - 9;
+        if (sizeof(S) != 4 || k < 0 || k >= (int)tiles_.size()) return false;
+        const TileDev &T = tiles_[k];
+        if (T.B * 8 > 512) return false;
+        for (ns = 2; ns >= 0; ns--) {
+            const int nbc = 32 + 8 * ns;
+            if (nb % nbc) continue;
+            smem = (size_t)T.qmax * 16 + (size_t)T.umax * nbc * 4;
+            if (smem > 220 * 1024) continue;
+            threads = T.B * 8;
+            return true;
+        }
+        return false;
+    };
     auto launch_grad = [&](int dg, int d0, int nbt) -> cudaError_t {
+        if (dg >= 9) {
+            int ns = 0, threads = 0;
+            size_t smem = 0;
+            if (!tile8_shape(dg, ns, threads, smem)) return cudaErrorInvalidValue;
+            if constexpr (sizeof(S) == 4) {
+                const TileDev &T = tiles_[dg - 9];
+                const int grid = T.nblk * (nb / (32 + 8 * ns));
+                const float *ef = (const float *)eps;
+                float *gf = (float *)g;
+                if (ns == 0)
+                    k_gradient_tile8<DIM, 0><<<grid, threads, smem, s>>>(dm_, dp_, dm_.lsq_pk, T.ptr, T.cells, T.loc,
+                                                                         T.B, T.qmax, ef, gf, d0, nbt);
+                else if (ns == 1)
+                    k_gradient_tile8<DIM, 1><<<grid, threads, smem, s>>>(dm_, dp_, dm_.lsq_pk, T.ptr, T.cells, T.loc,
+                                                                         T.B, T.qmax, ef, gf, d0, nbt);
+                else
+                    k_gradient_tile8<DIM, 2><<<grid, threads, smem, s>>>(dm_, dp_, dm_.lsq_pk, T.ptr, T.cells, T.loc,
+                                                                         T.B, T.qmax, ef, gf, d0, nbt);
+            }
+            return cudaGetLastError();
+        }
         if (dg >= 7) {
             int nbc = 0, threads = 0;
             size_t smem = 0;
@@ -3947,7 +4087,8 @@ Error Solver::solve_t(SolveStats &st) {
     {
         int nbc_ = 0, thr_ = 0;
         size_t sm_ = 0;
-        if (grad_dg >= 7 && (cfg.order != 2 || !tile_shape(grad_dg, nbc_, thr_, sm_))) grad_dg = 2;
+        if (grad_dg >= 9 && (cfg.order != 2 || !tile8_shape(grad_dg, nbc_, thr_, sm_))) grad_dg = 2;
+        if (grad_dg >= 7 && grad_dg <= 8 && (cfg.order != 2 || !tile_shape(grad_dg, nbc_, thr_, sm_))) grad_dg = 2;
     }
     last_grad_dirs_ = nb % 4 == 0 ? grad_dg : 0;
     // the residual's launch shape (1 = a thread per cell and 4 bands; 5, 6 =
@@ -4053,11 +4194,12 @@ Error Solver::solve_t(SolveStats &st) {
                 CUDA_TRY(cudaEventCreate(&t1));
                 float best = 1e30f;
                 int best_dg = 1;
-                for (int dg : {1, 2, 4, 5, 6, 7, 8}) {
+                for (int dg : {1, 2, 4, 5, 6, 7, 8, 9, 10}) {
                     if (dg >= 5 && dg <= 6 && !wc_ok) continue;
                     int nbc_ = 0, thr_ = 0;
                     size_t sm_ = 0;
-                    if (dg >= 7 && !tile_shape(dg, nbc_, thr_, sm_)) continue;
+                    if (dg >= 7 && dg <= 8 && !tile_shape(dg, nbc_, thr_, sm_)) continue;
+                    if (dg >= 9 && !tile8_shape(dg, nbc_, thr_, sm_)) continue;
                     for (int rep = 0; rep < 2; rep++) {
                         CUDA_TRY(cudaEventRecord(t0, s));
                         CUDA_TRY(launch_grad(dg, d0, nbt));

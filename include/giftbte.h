@@ -190,6 +190,8 @@ typedef struct {
                                  7, 8 = shared-memory tiles: a CTA per block of consecutive cells
                                  (3D: 32 or 64, 2D: 64 or 128) stages the block's stencil once and,
                                  direction by direction, the rows of the block's stencil union;
+                                 9, 10 = the tiles of 7, 8 with eight lanes per cell (FP32-mixed
+                                 form, band count a multiple of 32, 40 or 48; others run 2);
                                  0 = the fastest on the first outer iteration. Results do not
                                  depend on it. */
     int residual_form;        /* launch shape of the second-order residual: 1 = a thread per cell

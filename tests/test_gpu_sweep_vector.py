@@ -163,3 +163,32 @@ def test_gradient_and_residual_launch_shapes_are_bit_identical(prec, dim):
     for key, f in out.items():
         for k in ("T", "E", "q", "Tband"):
             assert np.array_equal(out[(1, 1)][k], f[k]), (key, k)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_eight_lane_gradient_tiles_are_bit_identical(dim):
+    # the tiled gradient with eight lanes per cell (options.gradient_dirs 9,
+    # 10; FP32-mixed form) against a thread per cell (1) and the four-band
+    # tiles (7): the band chunk is 32 + 8 NS bands, so 40 bands (3D: one
+    # 16-byte piece and one single band per lane) and 32 (2D: one piece).
+    # The 2D blocks of 128 cells would need 1024 threads: shape 10 falls back
+    # to 2 directions per thread there
+    if dim == 2:
+        d = decks.config2_deck(h_nm=6.0, n_bands=32, n_phi=4, seed=2)
+        shapes = (1, 7, 9, 10)
+        kw = {}
+    else:
+        d = decks.config3_deck(h_nm=10.0, size_nm=(40.0, 40.0, 100.0), n_bands=40, n_theta=2, n_phi=2)
+        shapes = (1, 7, 9, 10)
+        kw = {"direction_batch": 5}
+    out = {}
+    for dg in shapes:
+        s = g.StaticBTESynthetic.from_deck(d, precision=g.GBTE_FP32_MIXED, gradient_dirs=dg, residual_form=1,
+                                           sweep_bands=8, sweep_vector=1, sweep_kernel=1, **kw)
+        st = s.solve(max_iter=10, err_temp=0.0, err_flux=0.0)
+        out[dg] = s.fields()
+        s.close()
+        assert st["gradient_dirs"] == (2 if (dim == 2 and dg == 10) else dg)
+    for dg, f in out.items():
+        for k in ("T", "E", "q", "Tband"):
+            assert np.array_equal(out[1][k], f[k]), (dg, k)
