@@ -1,10 +1,38 @@
 // Host-side data structures of the B200 solver (not part of the C ABI).
 #pragma once
 #include <cstdint>
+#include <memory>
+#include <new>
+#include <type_traits>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace gbte {
+
+// An allocator whose resize leaves new elements default-initialised (no
+// zeroing for scalars), so that a large host array is first written, and
+// its pages first touched, by the threads that fill it.
+template <typename T>
+struct DefaultInitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = DefaultInitAlloc<U>;
+    };
+    DefaultInitAlloc() = default;
+    template <typename U>
+    DefaultInitAlloc(const DefaultInitAlloc<U> &) noexcept {}
+    template <typename U>
+    void construct(U *p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+        ::new (static_cast<void *>(p)) U;
+    }
+    template <typename U, typename... A>
+    void construct(U *p, A &&...a) {
+        ::new (static_cast<void *>(p)) U(std::forward<A>(a)...);
+    }
+};
+template <typename T>
+using HostArray = std::vector<T, DefaultInitAlloc<T>>;
 
 struct Error {
     int code;
@@ -138,12 +166,14 @@ struct SweepPlan {
     int ring = 0, max_width = 0, far_slots = 0;
     long long far_refs = 0;  // upwind references outside the ring (all directions)
     bool far_enabled = false;
-    std::vector<int> np;      // [nd*nc*4] position (>= 0) or -(1 + far slot)
-    std::vector<double> a;    // [nd*nc*4] A_f/V (s.n_f) of the upwind faces (< 0)
-    std::vector<double> sig;  // [nd*nc] sum of the outgoing A_f/V (s.n_f)
-    std::vector<int> nin;     // [nd*nc] upwind neighbours (<= 4)
-    std::vector<int> cell;    // [nd*nc] the cell at this position
-    std::vector<int> far_w;   // [nd*nc] far slot this cell stores into, -1 none
+    // (nd*nc records: built one direction per thread, each thread filling its
+    // direction's ranges, so the arrays skip the zeroing of resize)
+    HostArray<int> np;      // [nd*nc*4] position (>= 0) or -(1 + far slot); 0 past nin
+    HostArray<double> a;    // [nd*nc*4] A_f/V (s.n_f) of the upwind faces (< 0); 0 past nin
+    HostArray<double> sig;  // [nd*nc] sum of the outgoing A_f/V (s.n_f)
+    HostArray<int> nin;     // [nd*nc] upwind neighbours (<= 4)
+    HostArray<int> cell;    // [nd*nc] the cell at this position
+    HostArray<int> far_w;   // [nd*nc] far slot this cell stores into, -1 none
 };
 
 // Cell order for locality: cells sorted by the Morton code of their centre

@@ -76,6 +76,23 @@ void lsq_pinv(const std::vector<double> &J, int k, int dim, std::vector<double> 
         }
 }
 
+// f(lo, hi) over contiguous ranges of [0, n) on up to 64 of the host's
+// threads (one range when n is small); f must only write entries owned by
+// its range.
+template <typename F>
+void for_ranges(int n, F &&f) {
+    const int hw = std::min(64, (int)std::max(1u, std::thread::hardware_concurrency()));
+    const int nth = std::max(1, std::min(hw, n / 4096 + 1));
+    if (nth == 1) {
+        f(0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nth; t++)
+        pool.emplace_back([&f, n, nth, t]() { f((int)((long long)n * t / nth), (int)((long long)n * (t + 1) / nth)); });
+    for (auto &th : pool) th.join();
+}
+
 }  // namespace
 
 Error build_flat_mesh(const RawMesh &raw, const BCs &bcs, const Bands &bands, FlatMesh &m) {
@@ -247,18 +264,20 @@ Error build_flat_mesh(const RawMesh &raw, const BCs &bcs, const Bands &bands, Fl
         return false;
     };
     const int fnv = (dim == 2) ? 2 : 3;
-    // face neighbours
-    for (int c = 0; c < nc; c++)
-        for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
-            int v0 = m.cf_v[3 * k];
-            for (int q = nc_ptr[v0]; q < nc_ptr[v0 + 1]; q++) {
-                int o = nc_idx[q];
-                if (o == c) continue;
-                bool all = true;
-                for (int t = 0; t < fnv; t++) all = all && cell_has(o, m.cf_v[3 * k + t]);
-                if (all) m.cf_nbr[k] = o;
+    // face neighbours (each cell writes its own faces' entries)
+    for_ranges(nc, [&](int lo, int hi) {
+        for (int c = lo; c < hi; c++)
+            for (int k = m.cf_ptr[c]; k < m.cf_ptr[c + 1]; k++) {
+                int v0 = m.cf_v[3 * k];
+                for (int q = nc_ptr[v0]; q < nc_ptr[v0 + 1]; q++) {
+                    int o = nc_idx[q];
+                    if (o == c) continue;
+                    bool all = true;
+                    for (int t = 0; t < fnv; t++) all = all && cell_has(o, m.cf_v[3 * k + t]);
+                    if (all) m.cf_nbr[k] = o;
+                }
             }
-        }
+    });
     // boundary elements -> sides
     std::vector<std::vector<std::pair<int, int>>> bsides(nbe);
     for (int i = 0; i < nbe; i++) {
@@ -398,45 +417,57 @@ Error build_flat_mesh(const RawMesh &raw, const BCs &bcs, const Bands &bands, Fl
                 m.f_bound.push_back(m.cf_bound[k]);
             }
     }
-    // vertex-neighbour LSQ stencil
+    // vertex-neighbour LSQ stencil: every cell around each of the cell's
+    // vertices, in vertex order then node-to-cell order, once each, same
+    // material only. Two passes over ranges of cells (count, then fill and
+    // weigh), each thread with its own mark array.
     m.nbr_ptr.assign(nc + 1, 0);
     {
-        std::vector<std::vector<int>> lists(nc);
-        std::vector<int> mark(nc, -1);
-        for (int c = 0; c < nc; c++) {
+        auto stencil = [&](int c, std::vector<int> &mark, int *out) {
+            int k = 0;
             for (int q = raw.cptr[c]; q < raw.cptr[c + 1]; q++) {
                 int vtx = raw.cverts[q];
                 for (int t = nc_ptr[vtx]; t < nc_ptr[vtx + 1]; t++) {
                     int o = nc_idx[t];
                     if (o != c && mark[o] != c && m.matter[o] == m.matter[c]) {
                         mark[o] = c;
-                        lists[c].push_back(o);
+                        if (out) out[k] = o;
+                        k++;
                     }
                 }
             }
-            m.nbr_ptr[c + 1] = m.nbr_ptr[c] + (int)lists[c].size();
-        }
+            return k;
+        };
+        for_ranges(nc, [&](int lo, int hi) {
+            std::vector<int> mark(nc, -1);
+            for (int c = lo; c < hi; c++) m.nbr_ptr[c + 1] = stencil(c, mark, nullptr);
+        });
+        for (int c = 0; c < nc; c++) m.nbr_ptr[c + 1] += m.nbr_ptr[c];
         m.nbr_idx.resize(m.nbr_ptr[nc]);
         m.lsq_w.assign(3 * (size_t)m.nbr_ptr[nc], 0.0);
-        std::vector<double> J, W;
-        for (int c = 0; c < nc; c++) {
-            int k = (int)lists[c].size();
-            std::copy(lists[c].begin(), lists[c].end(), m.nbr_idx.begin() + m.nbr_ptr[c]);
-            if (k < 3) continue;  // zero gradient (StaticBTESynthetic.cpp:1290)
-            J.assign(3 * (size_t)k, 0.0);
-            for (int j = 0; j < k; j++) {
-                int o = lists[c][j];
-                J[3 * j] = 1.0 / m.Lx * (m.cx[o] - m.cx[c]);
-                J[3 * j + 1] = 1.0 / m.Lx * (m.cy[o] - m.cy[c]);
-                J[3 * j + 2] = dim == 3 ? 1.0 / m.Lx * (m.cz[o] - m.cz[c]) : 0.0;
+        for_ranges(nc, [&](int lo, int hi) {
+            std::vector<int> mark(nc, -1);
+            std::vector<double> J, W;
+            for (int c = lo; c < hi; c++) {
+                int *lst = m.nbr_idx.data() + m.nbr_ptr[c];
+                const int k = stencil(c, mark, lst);
+                if (k < 3) continue;  // zero gradient (StaticBTESynthetic.cpp:1290)
+                J.assign(3 * (size_t)k, 0.0);
+                for (int j = 0; j < k; j++) {
+                    int o = lst[j];
+                    J[3 * j] = 1.0 / m.Lx * (m.cx[o] - m.cx[c]);
+                    J[3 * j + 1] = 1.0 / m.Lx * (m.cy[o] - m.cy[c]);
+                    J[3 * j + 2] = dim == 3 ? 1.0 / m.Lx * (m.cz[o] - m.cz[c]) : 0.0;
+                }
+                lsq_pinv(J, k, dim, W);
+                bool bad = false;
+                for (double x : W) bad = bad || !std::isfinite(x);
+                if (bad) continue;  // singular stencil: the reference's NaN check zeroes the gradient
+                for (int j = 0; j < k; j++)
+                    for (int r = 0; r < dim; r++)
+                        m.lsq_w[3 * (size_t)(m.nbr_ptr[c] + j) + r] = W[r * (size_t)k + j] / m.Lx;
             }
-            lsq_pinv(J, k, dim, W);
-            bool bad = false;
-            for (double x : W) bad = bad || !std::isfinite(x);
-            if (bad) continue;  // singular stencil: the reference's NaN check zeroes the gradient
-            for (int j = 0; j < k; j++)
-                for (int r = 0; r < dim; r++) m.lsq_w[3 * (size_t)(m.nbr_ptr[c] + j) + r] = W[r * (size_t)k + j] / m.Lx;
-        }
+        });
     }
     // 3D face tangential LSQ
     if (dim == 3) {
@@ -641,13 +672,15 @@ Error build_sweep_plan(const FlatMesh &m, const Angles &a, const Schedule &s, in
     while (ring < std::max(min_ring, out.max_width)) ring *= 2;
     out.ring = ring;
     const size_t N = (size_t)nd * nc;
-    out.np.assign(4 * N, 0);
-    out.a.assign(4 * N, 0.0);
-    out.sig.assign(N, 0.0);
-    out.nin.assign(N, 0);
-    out.cell.assign(N, 0);
-    out.far_w.assign(N, -1);
-    std::vector<int> np_far(4 * N, 0);  // np with far references encoded as slots
+    // left uninitialised here: work(d) writes every entry of direction d's
+    // ranges (and clears np and a past each position's neighbours first)
+    out.np.resize(4 * N);
+    out.a.resize(4 * N);
+    out.sig.resize(N);
+    out.nin.resize(N);
+    out.cell.resize(N);
+    out.far_w.resize(N);
+    HostArray<int> np_far(4 * N);  // np with far references encoded as slots
     std::vector<int> dir_slots(nd, 0);
     std::vector<long long> dir_refs(nd, 0);
     std::vector<std::string> dir_err(nd);
@@ -667,6 +700,8 @@ Error build_sweep_plan(const FlatMesh &m, const Angles &a, const Schedule &s, in
                 }
         }
         const size_t P0 = (size_t)d * nc;
+        std::fill(out.np.begin() + 4 * P0, out.np.begin() + 4 * (P0 + nc), 0);
+        std::fill(out.a.begin() + 4 * P0, out.a.begin() + 4 * (P0 + nc), 0.0);
         for (int pos = 0; pos < nc; pos++) {
             const size_t P = P0 + pos;
             const int c = lc[pos];

@@ -3007,37 +3007,51 @@ Error Solver::init(const FlatMesh &m, const Bands &b, const Angles &a, const std
         }
         ring_ = sp.ring;
         far_slots_ = sp.far_enabled ? sp.far_slots : 0;
-        std::vector<SweepRec<double>> recd;
-        std::vector<SweepRec<float>> recf;
+        // packed by host threads over ranges of records, each record
+        // cleared (padding included) and filled by the thread that owns it
+        const size_t nrec = (size_t)nd * nc2;
+        HostArray<SweepRec<double>> recd;
+        HostArray<SweepRec<float>> recf;
         const bool f32 = cfg.precision == 1;
         if (f32)
-            recf.assign((size_t)nd * nc2, SweepRec<float>{});
+            recf.resize(nrec);
         else
-            recd.assign((size_t)nd * nc2, SweepRec<double>{});
+            recd.resize(nrec);
         // a per-cell relaxation-time scale 1/s_c multiplies row c of the
         // upwind operator: the record's coefficients and outgoing sum
         std::vector<double> rs(nc2, 1.0);
         for (size_t i = 0; i < cfg.cell_scatter.size(); i++) rs[i] = 1.0 / cfg.cell_scatter[i];
-        for (size_t P = 0; P < (size_t)nd * nc2; P++) {
-            const double f = rs[sp.cell[P]];
-            for (int q = 0; q < 4; q++) sp.a[4 * P + q] *= f;
-            sp.sig[P] *= f;
-            // meta: neighbour count (bits 0-2), 1 + far slot (bits 3-22), the
-            // cell's material (bits 24-30; its kb row in the sweep)
-            const int meta = sp.nin[P] | ((sp.far_w[P] + 1) << 3) | (mesh.matter[sp.cell[P]] << 24);
-            if (f32) {
-                SweepRec<float> &r = recf[P];
-                for (int q = 0; q < 4; q++) r.np[q] = sp.np[4 * P + q], r.a[q] = (float)sp.a[4 * P + q];
-                r.sig = (float)sp.sig[P];
-                r.meta = meta;
-                r.cell = sp.cell[P];
-            } else {
-                SweepRec<double> &r = recd[P];
-                for (int q = 0; q < 4; q++) r.np[q] = sp.np[4 * P + q], r.a[q] = sp.a[4 * P + q];
-                r.sig = sp.sig[P];
-                r.meta = meta;
-                r.cell = sp.cell[P];
+        auto pack = [&](size_t P0, size_t P1) {
+            for (size_t P = P0; P < P1; P++) {
+                const double f = rs[sp.cell[P]];
+                for (int q = 0; q < 4; q++) sp.a[4 * P + q] *= f;
+                sp.sig[P] *= f;
+                // meta: neighbour count (bits 0-2), 1 + far slot (bits 3-22),
+                // the cell's material (bits 24-30; its kb row in the sweep)
+                const int meta = sp.nin[P] | ((sp.far_w[P] + 1) << 3) | (mesh.matter[sp.cell[P]] << 24);
+                if (f32) {
+                    SweepRec<float> &r = recf[P];
+                    std::memset(&r, 0, sizeof(r));
+                    for (int q = 0; q < 4; q++) r.np[q] = sp.np[4 * P + q], r.a[q] = (float)sp.a[4 * P + q];
+                    r.sig = (float)sp.sig[P];
+                    r.meta = meta;
+                    r.cell = sp.cell[P];
+                } else {
+                    SweepRec<double> &r = recd[P];
+                    std::memset(&r, 0, sizeof(r));
+                    for (int q = 0; q < 4; q++) r.np[q] = sp.np[4 * P + q], r.a[q] = sp.a[4 * P + q];
+                    r.sig = sp.sig[P];
+                    r.meta = meta;
+                    r.cell = sp.cell[P];
+                }
             }
+        };
+        {
+            const size_t nth = std::max<size_t>(
+                1, std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), nrec / 65536 + 1));
+            std::vector<std::thread> pool;
+            for (size_t t = 0; t < nth; t++) pool.emplace_back(pack, nrec * t / nth, nrec * (t + 1) / nth);
+            for (auto &th : pool) th.join();
         }
         const size_t rec_bytes = f32 ? recf.size() * sizeof(SweepRec<float>) : recd.size() * sizeof(SweepRec<double>);
         rec_ = dalloc(rec_bytes);
