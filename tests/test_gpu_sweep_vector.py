@@ -165,21 +165,20 @@ def test_gradient_and_residual_launch_shapes_are_bit_identical(prec, dim):
             assert np.array_equal(out[(1, 1)][k], f[k]), (key, k)
 
 
-@pytest.mark.parametrize("dim", [2, 3])
-def test_eight_lane_gradient_tiles_are_bit_identical(dim):
+@pytest.mark.parametrize("dim,nb", [(2, 32), (3, 40), (3, 48)])
+def test_eight_lane_gradient_tiles_are_bit_identical(dim, nb):
     # the tiled gradient with eight lanes per cell (options.gradient_dirs 9,
     # 10; FP32-mixed form) against a thread per cell (1) and the four-band
-    # tiles (7): the band chunk is 32 + 8 NS bands, so 40 bands (3D: one
-    # 16-byte piece and one single band per lane) and 32 (2D: one piece).
-    # The 2D blocks of 128 cells would need 1024 threads: shape 10 falls back
-    # to 2 directions per thread there
+    # tiles (7): the band chunk is 32 + 8 NS bands, each lane taking one
+    # 16-byte piece and NS single bands, so 32 bands (NS = 0), 40 (NS = 1)
+    # and 48 (NS = 2). The 2D blocks of 128 cells would need 1024 threads:
+    # shape 10 falls back to 2 directions per thread there
+    shapes = (1, 7, 9, 10)
     if dim == 2:
-        d = decks.config2_deck(h_nm=6.0, n_bands=32, n_phi=4, seed=2)
-        shapes = (1, 7, 9, 10)
+        d = decks.config2_deck(h_nm=6.0, n_bands=nb, n_phi=4, seed=2)
         kw = {}
     else:
-        d = decks.config3_deck(h_nm=10.0, size_nm=(40.0, 40.0, 100.0), n_bands=40, n_theta=2, n_phi=2)
-        shapes = (1, 7, 9, 10)
+        d = decks.config3_deck(h_nm=10.0, size_nm=(40.0, 40.0, 100.0), n_bands=nb, n_theta=2, n_phi=2)
         kw = {"direction_batch": 5}
     out = {}
     for dg in shapes:
