@@ -35,10 +35,8 @@ struct gbte_handle {
     }
     // internal array of nc rows of w values -> caller's order, in place
     void to_user(double *a, int w) const {
-        const size_t nc = perm.size();
-        std::vector<double> v(a, a + nc * w);
-        for (size_t k = 0; k < nc; k++)
-            for (int j = 0; j < w; j++) a[(size_t)perm[k] * w + j] = v[k * w + j];
+        double *cols[1] = {a};
+        gbte::scatter_rows(perm, cols, 1, w);
     }
 };
 
@@ -590,12 +588,15 @@ int gbte_get_fields(gbte_handle *h, double *TE, double *TL, double *q, double *T
     gbte::Error e = h->solver.get_fields(TE, TL, q, TB);
     if (e.code) return fail(h, e), status_of(e.code);
     if (!h->perm.empty()) {
+        // the one-value columns (E, T and each band's temperature) together
         const size_t nc = h->perm.size();
-        if (TE) h->to_user(TE, 1);
-        if (TL) h->to_user(TL, 1);
-        if (q) h->to_user(q, 3);
+        std::vector<double *> cols;
+        if (TE) cols.push_back(TE);
+        if (TL) cols.push_back(TL);
         if (TB)
-            for (int b = 0; b < h->solver.bands.nb; b++) h->to_user(TB + b * nc, 1);
+            for (int b = 0; b < h->solver.bands.nb; b++) cols.push_back(TB + (size_t)b * nc);
+        gbte::scatter_rows(h->perm, cols.data(), (int)cols.size(), 1);
+        if (q) h->to_user(q, 3);
     }
     return GBTE_OK;
 }

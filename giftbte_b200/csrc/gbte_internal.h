@@ -183,6 +183,11 @@ struct SweepPlan {
 // rounding.
 void locality_order(const RawMesh &raw, std::vector<int> &perm);
 void reorder_cells(RawMesh &raw, const std::vector<int> &perm);
+// In place, for each of the ncols arrays of nc = perm.size() rows of w
+// values: row k moves to row perm[k] (internal cell order -> the caller's).
+// perm must be a permutation of 0 .. nc - 1. Columns, or ranges of rows when
+// there are few columns, run on the host's threads.
+void scatter_rows(const std::vector<int> &perm, double *const *cols, int ncols, int w);
 
 // Disjoint union of independent geometries for one batched solve: nodes,
 // cells and boundary elements concatenated, the boundary tags of geometry k

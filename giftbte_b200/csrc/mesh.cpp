@@ -834,6 +834,42 @@ void locality_order(const RawMesh &raw, std::vector<int> &perm) {
     }
 }
 
+void scatter_rows(const std::vector<int> &perm, double *const *cols, int ncols, int w) {
+    const size_t nc = perm.size();
+    if (nc == 0 || ncols <= 0 || w <= 0) return;
+    const size_t len = nc * (size_t)w;
+    auto one = [&](double *a, std::vector<double> &tmp, size_t k0, size_t k1) {
+        for (size_t k = k0; k < k1; k++)
+            for (int j = 0; j < w; j++) a[(size_t)perm[k] * w + j] = tmp[k * w + j];
+    };
+    const int hw = std::min(64, (int)std::max(1u, std::thread::hardware_concurrency()));
+    if (ncols >= 4 && hw > 1 && nc >= 4096) {
+        // whole columns per thread, each thread with its own copy buffer
+        const int nth = std::min(hw, ncols);
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nth; t++)
+            pool.emplace_back([&, t]() {
+                std::vector<double> tmp(len);
+                for (int c = t; c < ncols; c += nth) {
+                    std::copy(cols[c], cols[c] + len, tmp.begin());
+                    one(cols[c], tmp, 0, nc);
+                }
+            });
+        for (auto &th : pool) th.join();
+        return;
+    }
+    // few columns: ranges of rows per thread (perm is a permutation, so the
+    // ranges write disjoint rows)
+    std::vector<double> tmp(len);
+    for (int c = 0; c < ncols; c++) {
+        double *a = cols[c];
+        for_ranges((int)nc, [&](int lo, int hi) {
+            std::copy(a + (size_t)lo * w, a + (size_t)hi * w, tmp.begin() + (size_t)lo * w);
+        });
+        for_ranges((int)nc, [&](int lo, int hi) { one(a, tmp, lo, hi); });
+    }
+}
+
 void reorder_cells(RawMesh &raw, const std::vector<int> &perm) {
     const int nc = raw.nc();
     std::vector<int> cptr(1, 0), cverts, creg(nc);

@@ -228,3 +228,24 @@ def test_transient_deck_reads_on_the_host(tmp_path):
     with pytest.raises(g.GBTEError) as e:
         g.inspect_deck(str(tmp_path / "b"))
     assert e.value.status == -2
+
+
+def test_field_scatter_to_caller_order(tmp_path):
+    # host only: gbte_get_fields moves each field from the library's cell
+    # order to the caller's with gbte::scatter_rows, on the host's threads
+    # (whole columns per thread, or ranges of rows for few columns);
+    # tests/cpp/scatter_rows_main.cpp checks it against the serial scatter
+    # on random permutations
+    import shutil
+    import subprocess
+
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("g++ not available")
+    csrc = os.path.join(ROOT, "giftbte_b200", "csrc")
+    exe = str(tmp_path / "scatter_rows")
+    subprocess.check_call([gxx, "-std=c++17", "-O1", "-I", csrc, os.path.join(ROOT, "tests", "cpp", "scatter_rows_main.cpp")] +
+                          [os.path.join(csrc, f) for f in ("deck.cpp", "mesh.cpp", "angles.cpp")] +
+                          ["-lpthread", "-o", exe])
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.splitlines()[-1] == "OK", r.stdout + r.stderr
