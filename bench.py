@@ -365,6 +365,15 @@ def attach_shard(solver, rank: int, world: int) -> int:
     return n
 
 
+def pinned_fields(nc, nb):
+    """Pinned host arrays for StaticBTESynthetic.fields(out=...): the
+    read-back of every field copies straight into page-locked memory."""
+    import torch
+
+    return {k: torch.empty(shp, dtype=torch.float64).pin_memory().numpy()
+            for k, shp in (("E", (nc,)), ("T", (nc,)), ("q", (nc, 3)), ("Tband", (nb, nc)))}
+
+
 def e2e_iterations(args, solver, deck, world):
     """End to end through the public API on a handle already created: the
     initial field from pinned host memory (gbte_set_initial), K outer
@@ -376,6 +385,7 @@ def e2e_iterations(args, solver, deck, world):
     nc = deck.mesh.n_cells
     nb = solver.num_bands
     T0 = torch.full((nc,), float(deck.tref), dtype=torch.float64).pin_memory().numpy()
+    out = pinned_fields(nc, nb)
     reps = max(1, args.e2e_steps)
     times, ups = [], []
     for _ in range(reps):
@@ -383,7 +393,7 @@ def e2e_iterations(args, solver, deck, world):
         t0 = time.perf_counter()
         solver.set_initial(T0)
         st = solver.solve(max_iter=args.steps, err_temp=0.0, err_flux=0.0)
-        solver.fields()
+        solver.fields(out=out)
         torch.cuda.synchronize()
         times.append(time.perf_counter() - t0)
         ups.append(st["updates"])
@@ -437,7 +447,7 @@ def e2e_solves(args, deck, prec, device, world, shard_rank=None):
     if shard_rank is not None:
         attach_shard(solver, shard_rank, world)
     T0 = torch.full((nc,), float(deck.tref), dtype=torch.float64).pin_memory().numpy()
-    out = {k: np.zeros(n) for k, n in (("E", nc), ("T", nc), ("q", 3 * nc), ("Tb", nb * nc))}
+    out = pinned_fields(nc, nb)
     nsteps = max(2, min(args.steps, max(2, args.e2e_steps)))
     times, iters, ups = [], [], []
     for _ in range(nsteps):
@@ -445,7 +455,7 @@ def e2e_solves(args, deck, prec, device, world, shard_rank=None):
         t0 = time.perf_counter()
         solver.set_initial(T0)
         st = solver.solve()
-        f = solver.fields()
+        solver.fields(out=out)
         torch.cuda.synchronize()
         times.append(time.perf_counter() - t0)
         iters.append(st["iterations"])

@@ -374,12 +374,26 @@ class StaticBTESynthetic:
         self._check(rc)
         return self.stats
 
-    def fields(self) -> dict:
+    def fields(self, out: Optional[dict] = None) -> dict:
+        """The solution in the caller's cell order (gbte_get_fields): ``E``
+        and ``T`` (nc,), ``q`` (nc, 3), ``Tband`` (nb, nc). ``out`` may hold
+        arrays to fill in place under those keys (float64, C-contiguous,
+        writeable, those shapes), e.g. in pinned host memory for faster
+        copies; missing keys are allocated."""
         nc, nb = self.num_cells, self.num_bands
-        TE = np.zeros(nc); TL = np.zeros(nc); q = np.zeros(3 * nc); TB = np.zeros(nb * nc)
-        self._check(library().gbte_get_fields(self._h, _ptr(TE, ctypes.c_double), _ptr(TL, ctypes.c_double),
-                                              _ptr(q, ctypes.c_double), _ptr(TB, ctypes.c_double)))
-        return {"E": TE, "T": TL, "q": q.reshape(nc, 3), "Tband": TB.reshape(nb, nc)}
+        res = {}
+        for k, shp in (("E", (nc,)), ("T", (nc,)), ("q", (nc, 3)), ("Tband", (nb, nc))):
+            a = None if out is None else out.get(k)
+            if a is None:
+                a = np.zeros(shp)
+            elif (not isinstance(a, np.ndarray) or a.dtype != np.float64 or a.shape != shp
+                  or not a.flags.c_contiguous or not a.flags.writeable):
+                raise ValueError(f"fields: out[{k!r}] must be a writeable C-contiguous float64 array of shape {shp}")
+            res[k] = a
+        self._check(library().gbte_get_fields(self._h, _ptr(res["E"], ctypes.c_double),
+                                              _ptr(res["T"], ctypes.c_double), _ptr(res["q"], ctypes.c_double),
+                                              _ptr(res["Tband"], ctypes.c_double)))
+        return res
 
     @property
     def temperature(self):

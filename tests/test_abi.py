@@ -249,3 +249,31 @@ def test_field_scatter_to_caller_order(tmp_path):
                           ["-lpthread", "-o", exe])
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.splitlines()[-1] == "OK", r.stdout + r.stderr
+
+
+def test_fields_fill_caller_arrays(monkeypatch):
+    # StaticBTESynthetic.fields(out=...) passes the caller's arrays to
+    # gbte_get_fields (here a stand-in that writes through the pointers it
+    # gets) and refuses arrays of the wrong shape, type or layout
+    nc, nb = 7, 3
+
+    class FakeLib:
+        def gbte_get_fields(self, h, TE, TL, q, TB):
+            for p, n, base in ((TE, nc, 1.0), (TL, nc, 2.0), (q, 3 * nc, 3.0), (TB, nb * nc, 4.0)):
+                for i in range(n):
+                    p[i] = base + i
+            return g.GBTE_OK
+
+    monkeypatch.setattr(g, "library", lambda: FakeLib())
+    s = g.StaticBTESynthetic.__new__(g.StaticBTESynthetic)
+    s._h, s.num_cells, s.num_bands = None, nc, nb
+    out = {"T": np.zeros(nc), "Tband": np.zeros((nb, nc))}
+    f = s.fields(out=out)
+    assert f["T"] is out["T"] and f["Tband"] is out["Tband"]
+    assert np.array_equal(f["T"], 2.0 + np.arange(nc)) and np.array_equal(f["E"], 1.0 + np.arange(nc))
+    assert np.array_equal(f["q"], (3.0 + np.arange(3 * nc)).reshape(nc, 3))
+    assert np.array_equal(f["Tband"], (4.0 + np.arange(nb * nc)).reshape(nb, nc))
+    assert np.array_equal(s.fields()["q"], f["q"])
+    for bad in (np.zeros(nc + 1), np.zeros(nc, dtype=np.float32), np.zeros((2, nc))[:, 0]):
+        with pytest.raises(ValueError):
+            s.fields(out={"E": bad})
