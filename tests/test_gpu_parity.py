@@ -175,7 +175,7 @@ def test_benchmark_cell_converged_matches_reference():
     deck, ref = mg.load("config2_converged")
     s = StaticBTESynthetic.from_deck(deck, precision=GBTE_FP64, macro_exact=1)
     s.set_initial(ref["Tf"], ref["qf"])
-    st = s.solve(max_iter=4000)
+    st = s.solve(max_iter=4000, err_temp=1e-9, err_flux=1e-9)  # the reference run's margins
     f = s.fields()
     kk = keff_pair(s, f["q"], ref["q"])
     s.close()
