@@ -378,8 +378,8 @@ def e2e_iterations(args, solver, deck, world):
     """End to end through the public API on a handle already created: the
     initial field from pinned host memory (gbte_set_initial), K outer
     iterations (gbte_solve_with), every result field read back
-    (gbte_get_fields), repeated e2e_steps times; updates/s over the wall
-    time of the calls."""
+    (gbte_get_fields) into pinned host arrays, repeated e2e_steps times;
+    updates/s over the wall time of the calls."""
     import torch
 
     nc = deck.mesh.n_cells
