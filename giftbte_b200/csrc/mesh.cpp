@@ -845,7 +845,8 @@ void scatter_rows(const std::vector<int> &perm, double *const *cols, int ncols, 
     const int hw = std::min(64, (int)std::max(1u, std::thread::hardware_concurrency()));
     if (ncols >= 4 && hw > 1 && nc >= 4096) {
         // whole columns per thread, each thread with its own copy buffer
-        const int nth = std::min(hw, ncols);
+        // (at most 16: the scatter is bound by memory, not by threads)
+        const int nth = std::min(std::min(hw, 16), ncols);
         std::vector<std::thread> pool;
         for (int t = 0; t < nth; t++)
             pool.emplace_back([&, t]() {
