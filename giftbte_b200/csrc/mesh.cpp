@@ -80,8 +80,8 @@ void lsq_pinv(const std::vector<double> &J, int k, int dim, std::vector<double> 
 // threads (one range when n is small); f must only write entries owned by
 // its range.
 template <typename F>
-void for_ranges(int n, F &&f) {
-    const int hw = std::min(64, (int)std::max(1u, std::thread::hardware_concurrency()));
+void for_ranges(int n, F &&f, int max_threads = 64) {
+    const int hw = std::min(max_threads, (int)std::max(1u, std::thread::hardware_concurrency()));
     const int nth = std::max(1, std::min(hw, n / 4096 + 1));
     if (nth == 1) {
         f(0, n);
@@ -932,43 +932,72 @@ Error make_union(const std::vector<RawMesh> &meshes, const std::vector<BCs> &bcs
     return {0, ""};
 }
 
+// The union of block blk (cells c0 .. c1 - 1): its own cells, then the
+// other cells that `nbr(k)` names for its entries k in [k0, k1), ascending.
+// mark[] holds, per cell, the last block that listed it (blocks of one
+// thread are visited in increasing order).
+template <typename Nbr>
+static void block_halo(int blk, int c0, int c1, int k0, int k1, Nbr &&nbr, std::vector<int> &mark,
+                       std::vector<int> &halo) {
+    for (int c = c0; c < c1; c++) mark[c] = blk;
+    halo.clear();
+    for (int k = k0; k < k1; k++) {
+        const int j = nbr(k);
+        if (j >= 0 && mark[j] != blk) {
+            mark[j] = blk;
+            halo.push_back(j);
+        }
+    }
+    std::sort(halo.begin(), halo.end());
+}
+
 Error build_grad_tiles(const FlatMesh &m, int B, GradTiles &out) {
     out = GradTiles();
     if (B < 1 || B > 1024) return {-1, "gradient tile size out of range"};
     const int nc = m.nc;
     out.B = B;
     out.nblk = (nc + B - 1) / B;
-    out.ptr.assign(1, 0);
+    const int nblk = out.nblk;
     out.loc.resize(m.nbr_idx.size());
-    // mark[k] = block that last listed cell k, slot[k] = its local index there
-    std::vector<int> mark(nc, -1), slot(nc, 0), halo;
-    for (int blk = 0; blk < out.nblk; blk++) {
+    auto nbr = [&](int q) { return m.nbr_idx[q]; };
+    // union sizes per block, then the unions and local indices; blocks are
+    // independent, so ranges of blocks run on the host's threads, each
+    // thread with its own mark and slot arrays
+    std::vector<int> nu(nblk);
+    for_ranges(nblk, [&](int lo, int hi) {
+        std::vector<int> mark(nc, -1), halo;
+        for (int blk = lo; blk < hi; blk++) {
+            const int c0 = blk * B, c1 = std::min(nc, c0 + B);
+            block_halo(blk, c0, c1, m.nbr_ptr[c0], m.nbr_ptr[c1], nbr, mark, halo);
+            nu[blk] = (c1 - c0) + (int)halo.size();
+        }
+    }, 16);
+    out.ptr.assign(nblk + 1, 0);
+    for (int blk = 0; blk < nblk; blk++) {
+        if (nu[blk] > 65535) return {-8, "gradient tile union exceeds 16-bit local indices"};
         const int c0 = blk * B, c1 = std::min(nc, c0 + B);
-        for (int c = c0; c < c1; c++) {
-            mark[c] = blk;
-            slot[c] = c - c0;
-            out.cells.push_back(c);
-        }
-        halo.clear();
-        for (int q = m.nbr_ptr[c0]; q < m.nbr_ptr[c1]; q++) {
-            const int k = m.nbr_idx[q];
-            if (mark[k] != blk) {
-                mark[k] = blk;
-                halo.push_back(k);
-            }
-        }
-        std::sort(halo.begin(), halo.end());
-        const int nu = (c1 - c0) + (int)halo.size();
-        if (nu > 65535) return {-8, "gradient tile union exceeds 16-bit local indices"};
-        for (size_t h = 0; h < halo.size(); h++) {
-            slot[halo[h]] = (c1 - c0) + (int)h;
-            out.cells.push_back(halo[h]);
-        }
-        for (int q = m.nbr_ptr[c0]; q < m.nbr_ptr[c1]; q++) out.loc[q] = (unsigned short)slot[m.nbr_idx[q]];
-        out.ptr.push_back((int)out.cells.size());
-        out.umax = std::max(out.umax, nu);
+        out.ptr[blk + 1] = out.ptr[blk] + nu[blk];
+        out.umax = std::max(out.umax, nu[blk]);
         out.qmax = std::max(out.qmax, m.nbr_ptr[c1] - m.nbr_ptr[c0]);
     }
+    out.cells.resize(out.ptr[nblk]);
+    for_ranges(nblk, [&](int lo, int hi) {
+        std::vector<int> mark(nc, -1), slot(nc, 0), halo;
+        for (int blk = lo; blk < hi; blk++) {
+            const int c0 = blk * B, c1 = std::min(nc, c0 + B);
+            block_halo(blk, c0, c1, m.nbr_ptr[c0], m.nbr_ptr[c1], nbr, mark, halo);
+            int *cl = out.cells.data() + out.ptr[blk];
+            for (int c = c0; c < c1; c++) {
+                slot[c] = c - c0;
+                cl[c - c0] = c;
+            }
+            for (size_t h = 0; h < halo.size(); h++) {
+                slot[halo[h]] = (c1 - c0) + (int)h;
+                cl[(c1 - c0) + h] = halo[h];
+            }
+            for (int q = m.nbr_ptr[c0]; q < m.nbr_ptr[c1]; q++) out.loc[q] = (unsigned short)slot[m.nbr_idx[q]];
+        }
+    }, 16);
     return {0, ""};
 }
 
@@ -978,37 +1007,44 @@ Error build_face_tiles(const FlatMesh &m, int B, FaceTiles &out) {
     const int nc = m.nc;
     out.B = B;
     out.nblk = (nc + B - 1) / B;
-    out.ptr.assign(1, 0);
+    const int nblk = out.nblk;
     out.floc.assign(m.cf_ptr[nc], 0xFFFF);
-    std::vector<int> mark(nc, -1), slot(nc, 0), halo;
-    for (int blk = 0; blk < out.nblk; blk++) {
-        const int c0 = blk * B, c1 = std::min(nc, c0 + B);
-        for (int c = c0; c < c1; c++) {
-            mark[c] = blk;
-            slot[c] = c - c0;
-            out.cells.push_back(c);
+    auto nbr = [&](int k) { return m.cf_bound[k] >= 0 ? -1 : m.cf_nbr[k]; };
+    // as build_grad_tiles: union sizes, then unions and face-slot indices
+    std::vector<int> nu(nblk);
+    for_ranges(nblk, [&](int lo, int hi) {
+        std::vector<int> mark(nc, -1), halo;
+        for (int blk = lo; blk < hi; blk++) {
+            const int c0 = blk * B, c1 = std::min(nc, c0 + B);
+            block_halo(blk, c0, c1, m.cf_ptr[c0], m.cf_ptr[c1], nbr, mark, halo);
+            nu[blk] = (c1 - c0) + (int)halo.size();
         }
-        halo.clear();
-        for (int k = m.cf_ptr[c0]; k < m.cf_ptr[c1]; k++) {
-            if (m.cf_bound[k] >= 0) continue;
-            const int j = m.cf_nbr[k];
-            if (mark[j] != blk) {
-                mark[j] = blk;
-                halo.push_back(j);
-            }
-        }
-        std::sort(halo.begin(), halo.end());
-        const int nu = (c1 - c0) + (int)halo.size();
-        if (nu > 65535) return {-8, "residual tile union exceeds 16-bit local indices"};
-        for (size_t h = 0; h < halo.size(); h++) {
-            slot[halo[h]] = (c1 - c0) + (int)h;
-            out.cells.push_back(halo[h]);
-        }
-        for (int k = m.cf_ptr[c0]; k < m.cf_ptr[c1]; k++)
-            if (m.cf_bound[k] < 0) out.floc[k] = (unsigned short)slot[m.cf_nbr[k]];
-        out.ptr.push_back((int)out.cells.size());
-        out.umax = std::max(out.umax, nu);
+    }, 16);
+    out.ptr.assign(nblk + 1, 0);
+    for (int blk = 0; blk < nblk; blk++) {
+        if (nu[blk] > 65535) return {-8, "residual tile union exceeds 16-bit local indices"};
+        out.ptr[blk + 1] = out.ptr[blk] + nu[blk];
+        out.umax = std::max(out.umax, nu[blk]);
     }
+    out.cells.resize(out.ptr[nblk]);
+    for_ranges(nblk, [&](int lo, int hi) {
+        std::vector<int> mark(nc, -1), slot(nc, 0), halo;
+        for (int blk = lo; blk < hi; blk++) {
+            const int c0 = blk * B, c1 = std::min(nc, c0 + B);
+            block_halo(blk, c0, c1, m.cf_ptr[c0], m.cf_ptr[c1], nbr, mark, halo);
+            int *cl = out.cells.data() + out.ptr[blk];
+            for (int c = c0; c < c1; c++) {
+                slot[c] = c - c0;
+                cl[c - c0] = c;
+            }
+            for (size_t h = 0; h < halo.size(); h++) {
+                slot[halo[h]] = (c1 - c0) + (int)h;
+                cl[(c1 - c0) + h] = halo[h];
+            }
+            for (int k = m.cf_ptr[c0]; k < m.cf_ptr[c1]; k++)
+                if (m.cf_bound[k] < 0) out.floc[k] = (unsigned short)slot[m.cf_nbr[k]];
+        }
+    }, 16);
     return {0, ""};
 }
 
